@@ -1,0 +1,222 @@
+/*
+ * rvpoint_b200 -- C ABI of the B200 (sm_100a) point-cloud hot path.
+ *
+ * Every entry point takes plain pointers and sizes; no C++ or torch type
+ * crosses this boundary. Pointers are host or device memory as the `mem`
+ * argument says (RVP_MEM_HOST: the library stages them through pinned
+ * buffers; RVP_MEM_DEVICE: used in place, on the context's stream).
+ *
+ * Each function names the reference interface it replaces (paths inside
+ * Mumu-kun/rvpoint). The C++ drop-in of those interfaces (namespace rvpoint,
+ * include/rvpoint/...) is implemented on top of these calls.
+ *
+ * Errors: every call returns an rvp_status; rvp_last_error() gives the
+ * message of the last failure on a context. Degenerate inputs keep the
+ * reference's behaviour (empty input -> zero outputs, no error).
+ */
+#ifndef RVPOINT_B200_H
+#define RVPOINT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RVP_API __attribute__((visibility("default")))
+#else
+#define RVP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  RVP_OK = 0,
+  RVP_ERR_INVALID_ARG = 1, /* bad pointer, size or parameter */
+  RVP_ERR_OOM = 2,         /* device or pinned allocation failed */
+  RVP_ERR_CAPACITY = 3,    /* caller's output buffer too small; *total says how much */
+  RVP_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  RVP_ERR_CUDA = 5,        /* CUDA runtime error (message in rvp_last_error) */
+  RVP_ERR_NO_DEVICE = 6    /* no CUDA device / kernels not loadable */
+} rvp_status;
+
+enum { RVP_MEM_HOST = 0, RVP_MEM_DEVICE = 1 };
+
+typedef struct rvp_context rvp_context;
+typedef struct rvp_hash rvp_hash;
+typedef struct rvp_pipeline rvp_pipeline;
+
+/* ---- context ------------------------------------------------------------ */
+RVP_API rvp_status rvp_context_create(int device, rvp_context **out);
+RVP_API rvp_status rvp_context_destroy(rvp_context *ctx);
+/* stream: a cudaStream_t (NULL = legacy default stream). */
+RVP_API rvp_status rvp_context_set_stream(rvp_context *ctx, void *stream);
+RVP_API rvp_status rvp_context_synchronize(rvp_context *ctx);
+RVP_API const char *rvp_last_error(const rvp_context *ctx);
+RVP_API const char *rvp_status_string(rvp_status s);
+/* Number of kernel launches issued on this context so far. */
+RVP_API uint64_t rvp_context_launch_count(const rvp_context *ctx);
+/* Library version string. */
+RVP_API const char *rvp_version(void);
+
+/* ---- SpatialHash: search/spatial_hashing.h:12-53 ------------------------- */
+RVP_API rvp_status rvp_hash_create(rvp_context *ctx, rvp_hash **out);
+RVP_API rvp_status rvp_hash_destroy(rvp_hash *h);
+/* setHashPrimes, spatial_hashing.h:24-27 */
+RVP_API rvp_status rvp_hash_set_primes(rvp_hash *h, int64_t p1, int64_t p2);
+/* setInputCloud, spatial_hashing.cpp:76-151 (bbox, eps pad, grid dims).
+ * The cloud is copied to the device (the reference keeps a pointer). */
+RVP_API rvp_status rvp_hash_set_input_cloud(rvp_hash *h, const float *x, const float *y,
+                                    const float *z, size_t n, float cell_size,
+                                    int mem);
+/* build, spatial_hashing.cpp:153-163: radix sort of cell keys, bucket
+ * offsets, device hash table of occupied buckets. */
+RVP_API rvp_status rvp_hash_build(rvp_hash *h);
+/* 1 if two different cells share a hash key under the current primes. */
+RVP_API rvp_status rvp_hash_has_collisions(rvp_hash *h, int *out);
+/* radiusSearch, spatial_hashing.cpp:165-223, for nq queries at once.
+ * CSR result: offsets[nq+1] (int64), indices/dists hold offsets[nq] entries,
+ * each query's list sorted by (d2, index) and cut at max_nn when max_nn > 0.
+ * dists are squared distances, as in the reference. If the total exceeds
+ * capacity, returns RVP_ERR_CAPACITY with *total and offsets filled. */
+RVP_API rvp_status rvp_hash_radius_search(rvp_hash *h, const float *qx, const float *qy,
+                                  const float *qz, size_t nq, float radius,
+                                  int max_nn, int mem, int64_t *offsets,
+                                  int32_t *indices, float *dists,
+                                  size_t capacity, size_t *total);
+/* Exact k nearest neighbours (ties by index) of nq queries, k <= 64.
+ * radius > 0 bounds the search (radiusSearch with max_nn = k); radius <= 0
+ * searches the whole cloud. indices/dists: nq*k row-major; counts[nq]. */
+RVP_API rvp_status rvp_hash_knn(rvp_hash *h, const float *qx, const float *qy,
+                        const float *qz, size_t nq, int k, float radius, int mem,
+                        int32_t *indices, float *dists, int32_t *counts);
+
+/* ---- voxel grid: filters/voxel_grid.h:14-34 ------------------------------ */
+/* voxel_grid_downsamp_{sc,rvv,rvv_v2} (x86 semantics of _sc,
+ * voxel_grid_downsamp.cpp:183-213): centroids in (ix, iy, iz) order.
+ * out_aos: >= 3*n floats; keys (optional): 3 ints per voxel. */
+RVP_API rvp_status rvp_voxel_grid(rvp_context *ctx, const float *x, const float *y,
+                          const float *z, size_t n, float leaf_size, int mem,
+                          float *out_aos, int32_t *keys, size_t *out_count);
+
+/* ---- SOR: filters/statistical_outlier_removal.h:18-36 -------------------- */
+/* sor_sc / sor_rvv (statistical_outlier_removal.cpp:19-63): exact k+1 NN
+ * over all points. mean_dists (n floats) and keep (n bytes) optional. */
+RVP_API rvp_status rvp_sor(rvp_context *ctx, const float *x, const float *y,
+                   const float *z, size_t n, int k, float alpha, int mem,
+                   float *out_aos, size_t *out_count, float *mean_dists,
+                   uint8_t *keep);
+/* sor_spatial_hash (statistical_outlier_removal.cpp:246-270) on the hash's
+ * cloud: neighbours = radiusSearch(q, search_radius, k+1). */
+RVP_API rvp_status rvp_sor_spatial_hash(rvp_hash *h, int k, float alpha,
+                                float search_radius, int mem, float *out_aos,
+                                size_t *out_count, float *mean_dists,
+                                uint8_t *keep);
+
+/* ---- normals: features/normal_estimation.h:15-34 ------------------------- */
+/* normal_estimation_rvv(in, const SpatialHash&, ...) (normal_estimation.cpp
+ * :240-265) on the hash's cloud: neighbours = radiusSearch(q, radius). */
+RVP_API rvp_status rvp_normals_radius(rvp_hash *h, float radius, float vp_x,
+                              float vp_y, float vp_z, int eigen_iters, int mem,
+                              float *nx, float *ny, float *nz);
+/* normal_estimation_sc (normal_estimation.cpp:123-163): k+1 nearest incl.
+ * self (ties by index), centroid divided by k+1. */
+RVP_API rvp_status rvp_normals_knn(rvp_context *ctx, const float *x, const float *y,
+                           const float *z, size_t n, int k, float vp_x,
+                           float vp_y, float vp_z, int eigen_iters, int mem,
+                           float *nx, float *ny, float *nz);
+/* Precision mode (no reference counterpart; the reference path is
+ * rvp_normals_knn): covariance of the k+1 nearest accumulated in FP32 about
+ * the query point with compensated sums, eigenvector by converged Jacobi,
+ * redone in FP64 when the condition number exceeds cond_fp64. cond (optional)
+ * receives the condition estimate; used_fp64 (optional) 1 where FP64 ran. */
+RVP_API rvp_status rvp_normals_knn_precise(rvp_context *ctx, const float *x,
+                                   const float *y, const float *z, size_t n,
+                                   int k, float vp_x, float vp_y, float vp_z,
+                                   double cond_fp64, int mem, float *nx,
+                                   float *ny, float *nz, float *cond,
+                                   uint8_t *used_fp64);
+
+/* ---- RANSAC: segmentation/ransac_plane.h:11-45 --------------------------- */
+/* ransac_plane_sc / ransac_plane_rvv (ransac_plane.cpp:55-111).
+ * rand_stream: 3*max_iters raw rand() values (the reference's
+ * srand(0)/rand() sequence); NULL makes the library draw them from libc and
+ * leave libc's generator where the reference would leave it.
+ * counts (optional, max_iters ints): per-hypothesis inlier counts, with -1 for
+ * repeated indices, -2 for collinear triples; giving it evaluates all
+ * hypotheses (no early stop in the evaluation; the result is unchanged). */
+RVP_API rvp_status rvp_ransac_plane(rvp_context *ctx, const float *x, const float *y,
+                            const float *z, size_t n, float dist_thresh,
+                            int max_iters, float collinear_thresh,
+                            float probability, const int32_t *rand_stream,
+                            int mem, float *model, int *best_count,
+                            int *iters_run, int32_t *counts);
+/* extract_plane_inliers_outliers_rvv (ransac_plane.cpp:327-383); either
+ * output may be NULL (extract_plane_inliers_rvv / _outliers_rvv). */
+RVP_API rvp_status rvp_extract_plane(rvp_context *ctx, const float *x, const float *y,
+                             const float *z, size_t n, const float *model,
+                             float dist_thresh, int mem, float *inliers_aos,
+                             float *outliers_aos, size_t *n_inliers,
+                             size_t *n_outliers);
+
+/* ---- batched frames (no single reference counterpart: the chain
+ *      voxel_grid_downsamp_rvv_v2 -> sor_rvv -> normal_estimation_sc ->
+ *      ransac_plane_rvv of tools/pipeline_export.cpp:351-498, per frame) --- */
+typedef struct {
+  float leaf_size;       /* voxel leaf (m) */
+  int sor_k;             /* SOR neighbours */
+  float sor_alpha;       /* SOR std multiplier */
+  int normal_k;          /* normals: k+1 nearest incl. self */
+  int eigen_iters;       /* Jacobi iterations (reference default 4) */
+  float vp_x, vp_y, vp_z;/* viewpoint */
+  float ransac_thresh;   /* plane distance threshold */
+  int ransac_iters;      /* hypotheses */
+  float ransac_collinear;
+  float ransac_prob;
+  float cell_size;       /* grid cell for the neighbour searches (0 = auto) */
+  int block_threads;     /* kNN kernel block size (0 = auto) */
+  int queries_per_warp;  /* kNN queries per warp: 1 (warp/query) or 32 (0 = auto) */
+} rvp_pipeline_config;
+
+RVP_API rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
+                               size_t max_points, int max_frames,
+                               rvp_pipeline **out);
+RVP_API rvp_status rvp_pipeline_destroy(rvp_pipeline *p);
+/* Runs the chain over n_frames frames stored back to back in device memory
+ * (frame f = points frame_offsets[f] .. frame_offsets[f+1]). All sizes stay
+ * on the device; nothing is copied back. Capturable in a CUDA graph. */
+RVP_API rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x,
+                                   const float *y, const float *z,
+                                   const int64_t *frame_offsets_dev,
+                                   int n_frames, size_t n_points);
+/* Device pointers to the results of the last run (valid until the next run):
+ * voxel_aos/voxel_offsets[n_frames+1], sor_aos/sor_offsets, normals (3 SoA
+ * arrays over the SOR points), ransac_model[4*n_frames], ransac_count[n_frames],
+ * ransac_iters[n_frames]. */
+typedef struct {
+  const float *voxel_aos;
+  const int64_t *voxel_offsets;
+  const float *sor_aos;
+  const int64_t *sor_offsets;
+  const float *nx, *ny, *nz;
+  const float *ransac_model;
+  const int32_t *ransac_count;
+  const int32_t *ransac_iters;
+  const float *sor_mean_dists; /* per voxel point */
+} rvp_pipeline_outputs;
+RVP_API rvp_status rvp_pipeline_outputs_get(rvp_pipeline *p, rvp_pipeline_outputs *o);
+/* Host entry: copies host frames in, runs, copies the per-frame results out
+ * (any output pointer may be NULL). Output arrays are sized by max_points /
+ * n_frames; *_offsets are n_frames+1 entries. */
+RVP_API rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const float *y,
+                                 const float *z, const int64_t *frame_offsets,
+                                 int n_frames, float *voxel_aos,
+                                 int64_t *voxel_offsets, float *sor_aos,
+                                 int64_t *sor_offsets, float *nx, float *ny,
+                                 float *nz, float *ransac_model,
+                                 int32_t *ransac_count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RVPOINT_B200_H */

@@ -1,0 +1,154 @@
+// Test infrastructure only (the checker). This file is compiled together with
+// the UNMODIFIED reference sources (src/**/*.cpp of Mumu-kun/rvpoint) into
+// oracle/_ref/librvpoint_ref.so by oracle/Makefile. It adds nothing but a
+// plain extern "C" surface so Python tests and bench.py's CPU-baseline leg can
+// call the reference's own scalar path through ctypes. Every function below is
+// a thin forwarder: all arithmetic happens inside the reference's code.
+//
+// Built with -O3 -std=c++17 -ffp-contract=off and WITHOUT -march=native:
+// FMA contraction would change the bits of d^2 and of the plane distance.
+
+#include "core/point_types.h"
+#include "search/spatial_hashing.h"
+#include "filters/voxel_grid.h"
+#include "filters/statistical_outlier_removal.h"
+#include "features/normal_estimation.h"
+#include "segmentation/ransac_plane.h"
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+using namespace rvpoint;
+
+namespace {
+PointCloudSoA soa(const float *x, const float *y, const float *z, size_t n) {
+  PointCloudSoA c;
+  c.x = const_cast<float *>(x);
+  c.y = const_cast<float *>(y);
+  c.z = const_cast<float *>(z);
+  c.n = n;
+  return c;
+}
+}  // namespace
+
+extern "C" {
+
+// SpatialHash::setInputCloud + build + radiusSearch for every query
+// (spatial_hashing.cpp:76-223). CSR output: offsets[nq+1]; idx/d2 hold
+// offsets[nq] entries. Returns -1 when cap is too small (offsets still valid).
+long long ref_hash_radius_search(const float *x, const float *y, const float *z,
+                                 size_t n, float cell, const float *qx,
+                                 const float *qy, const float *qz, size_t nq,
+                                 float radius, int max_nn, long long *offsets,
+                                 int *idx, float *d2, long long cap) {
+  SpatialHash h;
+  h.setInputCloud(soa(x, y, z, n), cell);
+  h.build();
+  std::vector<int> ind;
+  std::vector<float> dd;
+  long long tot = 0;
+  bool overflow = false;
+  offsets[0] = 0;
+  for (size_t q = 0; q < nq; ++q) {
+    PointXYZ p{qx[q], qy[q], qz[q]};
+    size_t c = h.radiusSearch(p, radius, ind, dd, max_nn);
+    if (!overflow && tot + (long long)c <= cap) {
+      std::memcpy(idx + tot, ind.data(), c * sizeof(int));
+      std::memcpy(d2 + tot, dd.data(), c * sizeof(float));
+    } else {
+      overflow = true;
+    }
+    tot += (long long)c;
+    offsets[q + 1] = tot;
+  }
+  return overflow ? -1 : tot;
+}
+
+// voxel_grid_downsamp_rvv_v2 (voxel_grid_downsamp.cpp:284-335; on x86 it
+// falls through to voxel_grid_downsamp_sc :183-213). out: AoS [3*n].
+size_t ref_voxel_grid(const float *x, const float *y, const float *z, size_t n,
+                      float leaf, float *out) {
+#pragma GCC diagnostic push
+#pragma GCC diagnostic ignored "-Wdeprecated-declarations"
+  return voxel_grid_downsamp_rvv_v2(soa(x, y, z, n),
+                                    reinterpret_cast<PointXYZ *>(out), leaf);
+#pragma GCC diagnostic pop
+}
+
+// sor_rvv (statistical_outlier_removal.cpp:68-190 -> sor_sc :19-63 on x86).
+size_t ref_sor_rvv(const float *x, const float *y, const float *z, size_t n,
+                   int k, float alpha, float *out) {
+  return sor_rvv(soa(x, y, z, n), reinterpret_cast<PointXYZ *>(out), k, alpha);
+}
+
+// sor_spatial_hash (statistical_outlier_removal.cpp:246-270) over a
+// SpatialHash built with cell size `cell`.
+size_t ref_sor_spatial_hash(const float *x, const float *y, const float *z,
+                            size_t n, float cell, int k, float alpha,
+                            float search_radius, float *out) {
+  PointCloudSoA c = soa(x, y, z, n);
+  SpatialHash h;
+  h.setInputCloud(c, cell);
+  h.build();
+  return sor_spatial_hash(c, h, reinterpret_cast<PointXYZ *>(out), k, alpha,
+                          search_radius);
+}
+
+// normal_estimation_rvv(in, SpatialHash, ...) (normal_estimation.cpp:240-265).
+void ref_normals_hash(const float *x, const float *y, const float *z, size_t n,
+                      float cell, int k, float radius, float vpx, float vpy,
+                      float vpz, int iters, float *nx, float *ny, float *nz) {
+  PointCloudSoA c = soa(x, y, z, n);
+  SpatialHash h;
+  h.setInputCloud(c, cell);
+  h.build();
+  normal_estimation_rvv(c, h, nx, ny, nz, k, radius, vpx, vpy, vpz, iters);
+}
+
+// normal_estimation_sc (normal_estimation.cpp:123-163): brute-force k+1 NN.
+void ref_normals_sc(const float *aos, size_t n, int k, float radius, float vpx,
+                    float vpy, float vpz, int iters, float *nx, float *ny,
+                    float *nz) {
+  normal_estimation_sc(reinterpret_cast<const PointXYZ *>(aos), n, nx, ny, nz,
+                       k, radius, vpx, vpy, vpz, iters);
+}
+
+// ransac_plane_rvv (ransac_plane.cpp:116-199 -> ransac_plane_sc :55-111).
+int ref_ransac_plane(const float *x, const float *y, const float *z, size_t n,
+                     float thresh, int max_iters, float collinear, float prob,
+                     float *model) {
+  return ransac_plane_rvv(soa(x, y, z, n), thresh, max_iters, model, collinear,
+                          prob);
+}
+
+// extract_plane_inliers_outliers_rvv (ransac_plane.cpp:327-383).
+void ref_extract_plane(const float *x, const float *y, const float *z, size_t n,
+                       const float *model, float thresh, float *inliers,
+                       float *outliers, size_t *n_in, size_t *n_out) {
+  size_t a = 0, b = 0;
+  extract_plane_inliers_outliers_rvv(
+      soa(x, y, z, n), model, thresh, reinterpret_cast<PointXYZ *>(inliers),
+      reinterpret_cast<PointXYZ *>(outliers), a, b);
+  *n_in = a;
+  *n_out = b;
+}
+
+// extract_plane_inliers_rvv (ransac_plane.cpp:234-278): inlier count of one
+// plane model, used to pin per-hypothesis inlier counts.
+size_t ref_count_plane_inliers(const float *x, const float *y, const float *z,
+                               size_t n, const float *model, float thresh,
+                               float *scratch_aos) {
+  return extract_plane_inliers_rvv(soa(x, y, z, n), model, thresh,
+                                   reinterpret_cast<PointXYZ *>(scratch_aos));
+}
+
+// Raw glibc rand() stream after srand(seed): the hypothesis source of
+// ransac_plane_sc (ransac_plane.cpp:60,69-71).
+void ref_rand_stream(unsigned seed, int count, int *out) {
+  std::srand(seed);
+  for (int i = 0; i < count; ++i) out[i] = std::rand();
+}
+
+}  // extern "C"

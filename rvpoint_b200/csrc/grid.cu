@@ -1,0 +1,806 @@
+// Cell grid ("SpatialHash") build and neighbour queries for sm_100a.
+//
+// Build (spatial_hashing.cpp:76-163): bbox reduction, the reference's cell
+// function floor((x - min) / cell), one 64-bit key per point, stable radix
+// sort of (key, index), bucket heads, an open-addressing table of occupied
+// buckets {key, start | count << 32}, and the points re-laid out in bucket
+// order as float4 {x, y, z, index} so a bucket is one contiguous run.
+//
+// Key modes:
+//  * KEY_REF_HASH: the reference's hashCell ix + iy*p1 + iz*p2
+//    (spatial_hashing.h:43-45). Buckets are then exactly the reference's
+//    grid_ entries, collisions included.
+//  * KEY_DENSE: per-frame dense cell index offset by the frame's key base,
+//    so many frames share one sort and one table.
+//
+// Queries: one warp per query. Lanes look up up to 32 window cells at once,
+// a warp scan of bucket sizes flattens the window into one candidate stream,
+// and lanes walk it 32 candidates at a time (contiguous float4 loads inside a
+// bucket). The window is the tight cell range of [q - r, q + r] computed
+// with a monotone, conservative bound, which provably contains every point
+// with d2 <= r2 (so the result equals the reference's larger
+// ceil(r/cell)+1 window whenever the hash has no collisions; with
+// collisions the reference's own window is scanned instead).
+#include <math.h>
+
+#include "internal.cuh"
+
+namespace rvp {
+
+namespace {
+inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+
+__device__ __forceinline__ int frame_of_index(const int64_t *offs, int n_frames, size_t i) {
+  int lo = 0, hi = n_frames - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((size_t)offs[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------------------
+// bbox per frame
+// ---------------------------------------------------------------------------
+__global__ void k_bbox_init(GridFrame *fr, float *bb, int n_frames) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n_frames; f += gridDim.x * blockDim.x) {
+    bb[6 * f + 0] = bb[6 * f + 1] = bb[6 * f + 2] = INFINITY;
+    bb[6 * f + 3] = bb[6 * f + 4] = bb[6 * f + 5] = -INFINITY;
+  }
+}
+
+__global__ void k_bbox(const float *__restrict__ x, const float *__restrict__ y,
+                       const float *__restrict__ z, const int64_t *offs, int n_frames,
+                       size_t n_max, const u64 *n_dev, float *bb) {
+  const size_t n = n_dev ? *n_dev : n_max;
+  const int lane = threadIdx.x & 31;
+  for (size_t base = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) & ~(size_t)31; base < n;
+       base += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = base + lane;
+    const bool valid = i < n;
+    float vx = 0, vy = 0, vz = 0;
+    int f = -1;
+    if (valid) {
+      vx = x[i]; vy = y[i]; vz = z[i];
+      f = n_frames > 1 ? frame_of_index(offs, n_frames, i) : 0;
+    }
+    const int f0 = __shfl_sync(0xffffffffu, f, 0);
+    const bool uniform = __all_sync(0xffffffffu, !valid || f == f0);
+    if (uniform) {
+      float mnx = valid ? vx : INFINITY, mny = valid ? vy : INFINITY, mnz = valid ? vz : INFINITY;
+      float mxx = valid ? vx : -INFINITY, mxy = valid ? vy : -INFINITY, mxz = valid ? vz : -INFINITY;
+      for (int o = 16; o; o >>= 1) {
+        mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+        mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+        mnz = fminf(mnz, __shfl_xor_sync(0xffffffffu, mnz, o));
+        mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+        mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+        mxz = fmaxf(mxz, __shfl_xor_sync(0xffffffffu, mxz, o));
+      }
+      if (lane == 0 && f0 >= 0) {
+        float *b = bb + 6 * f0;
+        atomic_min_f(b + 0, mnx); atomic_min_f(b + 1, mny); atomic_min_f(b + 2, mnz);
+        atomic_max_f(b + 3, mxx); atomic_max_f(b + 4, mxy); atomic_max_f(b + 5, mxz);
+      }
+    } else if (valid) {
+      float *b = bb + 6 * f;
+      atomic_min_f(b + 0, vx); atomic_min_f(b + 1, vy); atomic_min_f(b + 2, vz);
+      atomic_max_f(b + 3, vx); atomic_max_f(b + 4, vy); atomic_max_f(b + 5, vz);
+    }
+  }
+}
+
+// setInputCloud's padding and grid dimensions (spatial_hashing.cpp:141-150),
+// then (dense mode) each frame's first key.
+__global__ void k_grid_params(GridFrame *fr, const float *bb, int n_frames, float cell) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  u64 base = 0;
+  for (int f = 0; f < n_frames; ++f) {
+    const float *b = bb + 6 * f;
+    GridFrame g;
+    g.cell = cell;
+    if (b[0] > b[3]) {  // empty frame
+      g.min_x = g.min_y = g.min_z = 0.0f;
+      g.gx = g.gy = g.gz = 1;
+    } else {
+      const float eps = fmul(cell, 0.01f);
+      g.min_x = fsub(b[0], eps); g.min_y = fsub(b[1], eps); g.min_z = fsub(b[2], eps);
+      const float max_x = fadd(b[3], eps), max_y = fadd(b[4], eps), max_z = fadd(b[5], eps);
+      g.gx = (int)ceilf(fdiv(fsub(max_x, g.min_x), cell)) + 1;
+      g.gy = (int)ceilf(fdiv(fsub(max_y, g.min_y), cell)) + 1;
+      g.gz = (int)ceilf(fdiv(fsub(max_z, g.min_z), cell)) + 1;
+    }
+    g.pad = 0;
+    g.key_base = base;
+    base += (u64)g.gx * (u64)g.gy * (u64)g.gz;
+    fr[f] = g;
+  }
+}
+
+// getCellIndices (spatial_hashing.h:47-52)
+__device__ __forceinline__ int cell_axis(float v, float mn, float cell) {
+  return (int)floorf(fdiv(fsub(v, mn), cell));
+}
+// Same, saturated to [lo, hi] before the int conversion (window bounds).
+__device__ __forceinline__ int cell_axis_clamped(float v, float mn, float cell, int lo, int hi) {
+  float t = floorf(fdiv(fsub(v, mn), cell));
+  t = fminf(fmaxf(t, (float)lo), (float)hi);
+  return (int)t;
+}
+
+__device__ __forceinline__ u64 key_of_cell(const GridView &g, const GridFrame &F, int cx, int cy,
+                                           int cz) {
+  if (g.mode == KEY_REF_HASH) {
+    const long long h = (long long)cx + (long long)cy * g.p1 + (long long)cz * g.p2;
+    return (u64)h ^ 0x8000000000000000ull;
+  }
+  return F.key_base + (u64)cx + (u64)F.gx * ((u64)cy + (u64)F.gy * (u64)cz);
+}
+
+__global__ void k_cell_keys(const float *__restrict__ x, const float *__restrict__ y,
+                            const float *__restrict__ z, const int64_t *offs, int n_frames,
+                            size_t n_max, const u64 *n_dev, const GridFrame *frames, int mode,
+                            long long p1, long long p2, u64 *keys, u32 *vals) {
+  const size_t n = n_dev ? *n_dev : n_max;
+  GridView gv;
+  gv.mode = mode; gv.p1 = p1; gv.p2 = p2;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int f = n_frames > 1 ? frame_of_index(offs, n_frames, i) : 0;
+    const GridFrame F = frames[f];
+    const int cx = cell_axis(x[i], F.min_x, F.cell);
+    const int cy = cell_axis(y[i], F.min_y, F.cell);
+    const int cz = cell_axis(z[i], F.min_z, F.cell);
+    keys[i] = key_of_cell(gv, F, cx, cy, cz);
+    vals[i] = (u32)i;
+  }
+}
+
+__global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, u32 *heads) {
+  const size_t n = n_dev ? *n_dev : n_max;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    heads[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_reorder(const float *__restrict__ x, const float *__restrict__ y,
+                          const float *__restrict__ z, const u32 *vals, const u32 *heads,
+                          const u64 *bucket_of, size_t n_max, const u64 *n_dev, float4 *pts,
+                          u32 *bstart, const GridFrame *frames, int mode, int *collision) {
+  const size_t n = n_dev ? *n_dev : n_max;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const u32 v = vals[i];
+    const float px = x[v], py = y[v], pz = z[v];
+    pts[i] = make_float4(px, py, pz, __uint_as_float(v));
+    if (heads[i]) {
+      bstart[bucket_of[i]] = (u32)i;
+    } else if (mode == KEY_REF_HASH) {
+      // same key as the previous point: a different cell means a collision
+      const u32 u = vals[i - 1];
+      const GridFrame F = frames[0];
+      if (cell_axis(px, F.min_x, F.cell) != cell_axis(x[u], F.min_x, F.cell) ||
+          cell_axis(py, F.min_y, F.cell) != cell_axis(y[u], F.min_y, F.cell) ||
+          cell_axis(pz, F.min_z, F.cell) != cell_axis(z[u], F.min_z, F.cell))
+        *collision = 1;
+    }
+  }
+}
+
+// one thread per bucket: {key, start | count << 32} into the open-addressing
+// table (linear probing, load factor <= 2/3).
+__global__ void k_insert(const u64 *keys, const u32 *bstart, const u64 *bucket_of, size_t n_max,
+                         const u64 *n_dev, ulonglong2 *table, u64 mask, u64 *nbuckets) {
+  const size_t n = n_dev ? *n_dev : n_max;
+  const u64 nb = bucket_of[n];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *nbuckets = nb;
+  for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nb;
+       b += (u64)gridDim.x * blockDim.x) {
+    const u32 s = bstart[b];
+    const u32 e = (b + 1 < nb) ? bstart[b + 1] : (u32)n;
+    const u64 key = keys[s];
+    const u64 ent = (u64)s | ((u64)(e - s) << 32);
+    u64 slot = mix64(key) & mask;
+    for (u64 probe = 0; probe <= mask; ++probe) {
+      const u64 prev = atomicCAS(&table[slot].x, kEmptyKey, key);
+      if (prev == kEmptyKey || prev == key) {
+        table[slot].y = ent;
+        break;
+      }
+      slot = (slot + 1) & mask;
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Grid storage
+// ---------------------------------------------------------------------------
+static u64 next_pow2(u64 v) {
+  u64 p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+void Grid::reserve(size_t n, int nf) {
+  if (n < 1) n = 1;
+  if (nf < 1) nf = 1;
+  if (n <= n_max && nf <= n_frames_max) return;
+  n_max = n > n_max ? n : n_max;
+  n_frames_max = nf > n_frames_max ? nf : n_frames_max;
+  table_cap = (size_t)next_pow2((u64)(n_max + n_max / 2 + 1024));
+  b_keys.reserve(n_max * 8);
+  b_vals.reserve(n_max * 4);
+  b_pts.reserve(n_max * 16);
+  b_table.reserve(table_cap * 16);
+  b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
+  b_begin.reserve(al((n_frames_max + 1) * 8));
+  b_sort.reserve(sort_temp_bytes(n_max) + al(n_max * 4) + al((n_max + 1) * 8) + al(n_max * 4) +
+                 scan_temp_bytes(n_max));
+  b_misc.reserve(256);
+  d_n = b_misc.as<u64>();
+  d_nbuckets = d_n + 1;
+  d_collision = reinterpret_cast<int *>(d_n + 2);
+}
+
+void Grid::release() {
+  b_keys.release(); b_vals.release(); b_pts.release(); b_table.release();
+  b_frames.release(); b_begin.release(); b_sort.release(); b_misc.release();
+  n_max = 0; n_frames_max = 0;
+}
+
+GridView Grid::view(int mode, long long p1, long long p2) const {
+  GridView v;
+  v.pts = b_pts.as<float4>();
+  v.table = b_table.as<ulonglong2>();
+  v.table_mask = (u64)table_cap - 1;
+  v.frames = b_frames.as<GridFrame>();
+  v.frame_pt_begin = b_begin.as<u64>();
+  v.mode = mode;
+  v.p1 = p1;
+  v.p2 = p2;
+  return v;
+}
+
+void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const float *z,
+                const int64_t *offs, int n_frames, size_t n_points, float cell, int mode,
+                long long p1, long long p2, const u64 *n_dev_opt) {
+  g.reserve(n_points, n_frames);
+  cudaStream_t st = ctx->stream;
+  const size_t n_max = n_points;
+  const u64 *n_dev = n_dev_opt;
+  GridFrame *frames = g.b_frames.as<GridFrame>();
+  float *bb = reinterpret_cast<float *>(g.b_frames.as<char>() + al(g.n_frames_max * sizeof(GridFrame)));
+  u64 *begin = g.b_begin.as<u64>();
+  RVP_CUDA_TRY(cudaMemcpyAsync(begin, offs, (n_frames + 1) * 8, cudaMemcpyDeviceToDevice, st));
+  char *sp = g.b_sort.as<char>();
+  SortTemp t;
+  sort_temp_carve(t, sp, g.n_max);
+  sp += sort_temp_bytes(g.n_max);
+  u32 *heads = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
+  u64 *bucket_of = reinterpret_cast<u64 *>(sp); sp += al((g.n_max + 1) * 8);
+  u32 *bstart = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
+  void *scan_tmp = sp;
+
+  const int sms = ctx->num_sms;
+  k_bbox_init<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(frames, bb, n_frames);
+  RVP_LAUNCH_CHECK(ctx);
+  k_bbox<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, bb);
+  RVP_LAUNCH_CHECK(ctx);
+  k_grid_params<<<1, 32, 0, st>>>(frames, bb, n_frames, cell);
+  RVP_LAUNCH_CHECK(ctx);
+  k_cell_keys<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(
+      x, y, z, offs, n_frames, n_max, n_dev, frames, mode, p1, p2, g.b_keys.as<u64>(),
+      g.b_vals.as<u32>());
+  RVP_LAUNCH_CHECK(ctx);
+  radix_sort_pairs(ctx, g.b_keys.as<u64>(), g.b_vals.as<u32>(), n_max, n_dev, t);
+  k_heads<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(g.b_keys.as<u64>(), n_max, n_dev, heads);
+  RVP_LAUNCH_CHECK(ctx);
+  // bucket_of[i] = number of heads before i, i.e. the bucket id of a head
+  exclusive_scan_u32_to_u64(ctx, heads, bucket_of, n_max, n_dev, scan_tmp);
+  RVP_CUDA_TRY(cudaMemsetAsync(g.b_table.ptr, 0xFF, g.table_cap * 16, st));
+  RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 16, st));  // nbuckets + collision
+  k_reorder<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(
+      x, y, z, g.b_vals.as<u32>(), heads, bucket_of, n_max, n_dev, g.b_pts.as<float4>(), bstart,
+      frames, mode, g.d_collision);
+  RVP_LAUNCH_CHECK(ctx);
+  k_insert<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(
+      g.b_keys.as<u64>(), bstart, bucket_of, n_max, n_dev, g.b_table.as<ulonglong2>(),
+      (u64)g.table_cap - 1, g.d_nbuckets);
+  RVP_LAUNCH_CHECK(ctx);
+}
+
+// ===========================================================================
+// Queries
+// ===========================================================================
+namespace {
+
+constexpr u32 kRemovedBit = 0x80000000u;
+
+struct Window {
+  int lo[3], hi[3];
+};
+
+__device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u32 &count) {
+  u64 slot = mix64(key) & g.table_mask;
+  for (u64 probe = 0; probe <= g.table_mask; ++probe) {
+    const ulonglong2 e = __ldg(&g.table[slot]);
+    if (e.x == key) {
+      start = (u32)(e.y & 0xFFFFFFFFull);
+      count = (u32)(e.y >> 32);
+      return true;
+    }
+    if (e.x == kEmptyKey) return false;
+    slot = (slot + 1) & g.table_mask;
+  }
+  return false;
+}
+
+// Tight window of all cells that can hold a point p with d2(p, q) <= rr,
+// rr = r*r. |p - q| <= r (1 + 3 * 2^-24) per axis for any such p; the bound
+// is padded to r (1 + 1e-6) and rounded outwards, and the cell function is
+// monotone, so the window is exact. Clamped to the frame's grid.
+__device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, float qy, float qz,
+                                               double r) {
+  const double rp = r * (1.0 + 1e-6) + 1e-30;
+  Window w;
+  const float q[3] = {qx, qy, qz};
+  const float mn[3] = {F.min_x, F.min_y, F.min_z};
+  const int G[3] = {F.gx, F.gy, F.gz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lo = __double2float_rd((double)q[a] - rp);
+    const float hi = __double2float_ru((double)q[a] + rp);
+    w.lo[a] = cell_axis_clamped(lo, mn[a], F.cell, -1, G[a]);
+    w.hi[a] = cell_axis_clamped(hi, mn[a], F.cell, -1, G[a]);
+    w.lo[a] = max(w.lo[a], 0);
+    w.hi[a] = min(w.hi[a], G[a] - 1);
+  }
+  return w;
+}
+
+// The reference's window: query cell +- (ceil(r/cell) + 1), unclamped
+// (spatial_hashing.cpp:174-181).
+__device__ __forceinline__ Window ref_window(const GridFrame &F, float qx, float qy, float qz,
+                                             float radius) {
+  const int R = (int)ceilf(fdiv(radius, F.cell)) + 1;
+  Window w;
+  const int c[3] = {cell_axis(qx, F.min_x, F.cell), cell_axis(qy, F.min_y, F.cell),
+                    cell_axis(qz, F.min_z, F.cell)};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) { w.lo[a] = c[a] - R; w.hi[a] = c[a] + R; }
+  return w;
+}
+
+// Window of the query's own cell +- ring, clamped.
+__device__ __forceinline__ Window ring_window(const GridFrame &F, float qx, float qy, float qz,
+                                              int ring) {
+  Window w;
+  const float q[3] = {qx, qy, qz};
+  const float mn[3] = {F.min_x, F.min_y, F.min_z};
+  const int G[3] = {F.gx, F.gy, F.gz};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1);
+    w.lo[a] = max(c - ring, 0);
+    w.hi[a] = min(c + ring, G[a] - 1);
+  }
+  return w;
+}
+
+// Lower bound on the distance from q to any point outside window w (points
+// of other cells of this frame); +inf when w spans the whole grid.
+__device__ __forceinline__ double coverage(const GridFrame &F, const Window &w, float qx, float qy,
+                                           float qz) {
+  const float q[3] = {qx, qy, qz};
+  const float mn[3] = {F.min_x, F.min_y, F.min_z};
+  const int G[3] = {F.gx, F.gy, F.gz};
+  double cov = 1e300;
+  const double u = 4.0 * 5.960464477539063e-08;  // 4 * 2^-24
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double slack = u * (fabs((double)mn[a]) + (double)(w.hi[a] + 2) * F.cell + fabs((double)q[a])) + 1e-30;
+    if (w.lo[a] > 0) {
+      const double face = (double)mn[a] + (double)w.lo[a] * (double)F.cell;
+      cov = fmin(cov, (double)q[a] - face - slack);
+    }
+    if (w.hi[a] < G[a] - 1) {
+      const double face = (double)mn[a] + (double)(w.hi[a] + 1) * (double)F.cell;
+      cov = fmin(cov, face - (double)q[a] - slack);
+    }
+  }
+  return cov;
+}
+
+__device__ __forceinline__ long long window_cells(const Window &w) {
+  long long c = 1;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (w.hi[a] < w.lo[a]) return 0;
+    c *= (long long)(w.hi[a] - w.lo[a] + 1);
+  }
+  return c;
+}
+
+// Walk every candidate of window w (or of the whole frame when brute):
+// fn(float4 p, bool valid) is called by all 32 lanes for each batch of 32.
+template <class Fn>
+__device__ __forceinline__ void for_each_candidate(const GridView &g, const GridFrame &F, int f,
+                                                   const Window &w, bool brute, Fn &&fn) {
+  const int lane = threadIdx.x & 31;
+  if (brute) {
+    const u64 a = g.frame_pt_begin[f], b = g.frame_pt_begin[f + 1];
+    for (u64 p0 = a; p0 < b; p0 += 32) {
+      const u64 p = p0 + lane;
+      const bool valid = p < b;
+      float4 v = valid ? __ldg(&g.pts[p]) : make_float4(0, 0, 0, 0);
+      fn(v, valid);
+    }
+    return;
+  }
+  const long long total = window_cells(w);
+  const int ncx = w.hi[0] - w.lo[0] + 1, ncy = w.hi[1] - w.lo[1] + 1;
+  for (long long cb = 0; cb < total; cb += 32) {
+    const long long j = cb + lane;
+    u32 start = 0, count = 0;
+    if (j < total) {
+      const int cx = w.lo[0] + (int)(j % ncx);
+      const int cy = w.lo[1] + (int)((j / ncx) % ncy);
+      const int cz = w.lo[2] + (int)(j / ((long long)ncx * ncy));
+      if (!lookup(g, key_of_cell(g, F, cx, cy, cz), start, count)) count = 0;
+    }
+    // flatten: inclusive scan of bucket sizes
+    u32 incl = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const u32 ex = incl - count;
+    const u32 M = __shfl_sync(0xffffffffu, incl, 31);
+    for (u32 p0 = 0; p0 < M; p0 += 32) {
+      const u32 p = p0 + lane;
+      // owner cell: largest lane c with ex_c <= p
+      int c = 0;
+#pragma unroll
+      for (int s = 16; s; s >>= 1) {
+        const u32 t = __shfl_sync(0xffffffffu, ex, c + s);
+        if (t <= p) c += s;
+      }
+      const u32 st = __shfl_sync(0xffffffffu, start, c);
+      const u32 ec = __shfl_sync(0xffffffffu, ex, c);
+      const bool valid = p < M;
+      float4 v = valid ? __ldg(&g.pts[st + (p - ec)]) : make_float4(0, 0, 0, 0);
+      fn(v, valid);
+    }
+  }
+}
+
+__device__ __forceinline__ u32 query_index(const QuerySet &q, size_t i) {
+  return q.order ? (u32)q.order[i] : (u32)i;
+}
+
+// ---------------------------------------------------------------------------
+// radius search: count pass
+// ---------------------------------------------------------------------------
+__global__ void k_radius_count(GridView g, QuerySet q, float radius, bool ref_win, u32 *counts) {
+  const size_t nq = q.n_dev ? *q.n_dev : q.n_max;
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const float r2 = fmul(radius, radius);
+  for (size_t wi = warp; wi < nq; wi += nwarps) {
+    const u32 qi = query_index(q, wi);
+    const int f = q.frame_of ? q.frame_of[qi] : 0;
+    const GridFrame F = g.frames[f];
+    const float qx = q.x[qi], qy = q.y[qi], qz = q.z[qi];
+    const Window w = ref_win ? ref_window(F, qx, qy, qz, radius)
+                             : tight_window(F, qx, qy, qz, (double)radius);
+    u32 cnt = 0;
+    for_each_candidate(g, F, f, w, false, [&](float4 p, bool valid) {
+      const bool pass = valid && !(__float_as_uint(p.w) & kRemovedBit) &&
+                        dist2(p.x, p.y, p.z, qx, qy, qz) <= r2;
+      cnt += __popc(__ballot_sync(0xffffffffu, pass));
+    });
+    if (lane == 0) counts[qi] = cnt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// radius search: fill pass with per-warp shared-memory staging and sort
+// ---------------------------------------------------------------------------
+constexpr int FILL_WARPS = 4;
+constexpr int FILL_CAP = 1024;  // pairs staged per warp (8 KB)
+
+__device__ __forceinline__ void warp_bitonic_smem(u64 *s, int P) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < P; i += 32) {
+        const int l = i ^ j;
+        if (l > i) {
+          const u64 a = s[i], b = s[l];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) { s[i] = b; s[l] = a; }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ __launch_bounds__(FILL_WARPS * 32) void k_radius_fill(GridView g, QuerySet q,
+                                                                 float radius, bool ref_win,
+                                                                 const u64 *offsets, u64 *out,
+                                                                 u32 *big_list, u32 *big_count) {
+  __shared__ u64 stage[FILL_WARPS][FILL_CAP];
+  const size_t nq = q.n_dev ? *q.n_dev : q.n_max;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const float r2 = fmul(radius, radius);
+  u64 *s = stage[wib];
+  for (size_t wi = warp; wi < nq; wi += nwarps) {
+    const u32 qi = query_index(q, wi);
+    const u64 off = offsets[qi];
+    const u32 cnt = (u32)(offsets[qi + 1] - off);
+    if (cnt == 0) continue;
+    const int f = q.frame_of ? q.frame_of[qi] : 0;
+    const GridFrame F = g.frames[f];
+    const float qx = q.x[qi], qy = q.y[qi], qz = q.z[qi];
+    const Window w = ref_win ? ref_window(F, qx, qy, qz, radius)
+                             : tight_window(F, qx, qy, qz, (double)radius);
+    const bool staged = cnt <= FILL_CAP;
+    u32 pos = 0;
+    for_each_candidate(g, F, f, w, false, [&](float4 p, bool valid) {
+      const u32 idx = __float_as_uint(p.w);
+      float d2 = 0.0f;
+      bool pass = false;
+      if (valid && !(idx & kRemovedBit)) {
+        d2 = dist2(p.x, p.y, p.z, qx, qy, qz);
+        pass = d2 <= r2;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, pass);
+      if (pass) {
+        const u32 at = pos + __popc(b & ((1u << lane) - 1));
+        if (at < cnt) {
+          const u64 key = pack_nbr(d2, (int)idx);
+          if (staged) s[at] = key; else out[off + at] = key;
+        }
+      }
+      pos += __popc(b);
+    });
+    if (staged) {
+      int P = 1;
+      while (P < (int)cnt) P <<= 1;
+      for (int i = (int)cnt + lane; i < P; i += 32) s[i] = ~0ull;
+      __syncwarp();
+      warp_bitonic_smem(s, P);
+      for (u32 i = lane; i < cnt; i += 32) out[off + i] = s[i];
+      __syncwarp();
+    } else if (lane == 0) {
+      const u32 slot = atomicAdd(big_count, 1u);
+      big_list[slot] = qi;
+    }
+  }
+}
+
+// one block per oversized segment: bitonic sort, in shared memory when it
+// fits (<= 8192 pairs), else in global memory.
+constexpr int BIG_SMEM = 8192;
+__global__ __launch_bounds__(1024) void k_sort_big(const u64 *offsets, u64 *pairs,
+                                                   const u32 *big_list, const u32 *big_count) {
+  extern __shared__ u64 sb[];
+  const u32 nb = *big_count;
+  for (u32 b = blockIdx.x; b < nb; b += gridDim.x) {
+    const u32 qi = big_list[b];
+    const u64 off = offsets[qi];
+    const u64 cnt = offsets[qi + 1] - off;
+    u64 P = 1;
+    while (P < cnt) P <<= 1;
+    u64 *a = pairs + off;
+    if (P <= BIG_SMEM) {
+      for (u64 i = threadIdx.x; i < P; i += blockDim.x) sb[i] = i < cnt ? a[i] : ~0ull;
+      __syncthreads();
+      for (u64 k = 2; k <= P; k <<= 1)
+        for (u64 j = k >> 1; j > 0; j >>= 1) {
+          for (u64 i = threadIdx.x; i < P; i += blockDim.x) {
+            const u64 l = i ^ j;
+            if (l > i) {
+              const u64 x = sb[i], y = sb[l];
+              if ((x > y) == ((i & k) == 0)) { sb[i] = y; sb[l] = x; }
+            }
+          }
+          __syncthreads();
+        }
+      for (u64 i = threadIdx.x; i < cnt; i += blockDim.x) a[i] = sb[i];
+      __syncthreads();
+    } else {
+      // virtual padding: indices >= cnt hold +inf and never move
+      for (u64 k = 2; k <= P; k <<= 1)
+        for (u64 j = k >> 1; j > 0; j >>= 1) {
+          for (u64 i = threadIdx.x; i < P; i += blockDim.x) {
+            const u64 l = i ^ j;
+            if (l > i) {
+              const u64 x = i < cnt ? a[i] : ~0ull;
+              const u64 y = l < cnt ? a[l] : ~0ull;
+              if ((x > y) == ((i & k) == 0)) {
+                if (i < cnt) a[i] = y;
+                if (l < cnt) a[l] = x;
+              }
+            }
+          }
+          __syncthreads();
+        }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// exact kNN: warp-resident sorted list of 32*P keys (lane i, slot s holds
+// element 32*s + i); candidates below the K-th key are inserted one by one.
+// ---------------------------------------------------------------------------
+template <int P>
+struct WarpList {
+  u64 e[P];
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int s = 0; s < P; ++s) e[s] = ~0ull;
+  }
+  __device__ __forceinline__ u64 get(int j) const {  // broadcast element j
+    u64 v = e[0];
+#pragma unroll
+    for (int s = 1; s < P; ++s)
+      if ((j >> 5) == s) v = e[s];
+    return __shfl_sync(0xffffffffu, v, j & 31);
+  }
+  __device__ __forceinline__ void insert(u64 c) {
+    const int lane = threadIdx.x & 31;
+    u64 carry = 0;  // last element of the previous slot, before the insert
+#pragma unroll
+    for (int s = 0; s < P; ++s) {
+      const u64 cur = e[s];
+      const u64 last = __shfl_sync(0xffffffffu, cur, 31);
+      u64 prev = __shfl_up_sync(0xffffffffu, cur, 1);
+      bool prev_lt;
+      if (lane == 0) prev_lt = (s == 0) ? true : (carry < c);
+      else prev_lt = prev < c;
+      if (lane == 0 && s > 0) prev = carry;
+      if (!(cur < c)) e[s] = prev_lt ? c : prev;
+      carry = last;
+    }
+  }
+};
+
+template <int P>
+__device__ __forceinline__ void knn_scan(const GridView &g, const GridFrame &F, int f,
+                                         const Window &w, bool brute, float qx, float qy,
+                                         float qz, int K, u64 bound, WarpList<P> &L,
+                                         u32 &found) {
+  const int lane = threadIdx.x & 31;
+  u64 thr = L.get(K - 1);
+  for_each_candidate(g, F, f, w, brute, [&](float4 p, bool valid) {
+    const u32 idx = __float_as_uint(p.w);
+    u64 key = ~0ull;
+    if (valid && !(idx & kRemovedBit)) key = pack_nbr(dist2(p.x, p.y, p.z, qx, qy, qz), (int)idx);
+    const bool in_bound = key <= bound;
+    found += __popc(__ballot_sync(0xffffffffu, in_bound));
+    unsigned m = __ballot_sync(0xffffffffu, in_bound && key < thr);
+    while (m) {
+      const int src = __ffs(m) - 1;
+      m &= m - 1;
+      const u64 c = __shfl_sync(0xffffffffu, key, src);
+      if (c < thr) {
+        L.insert(c);
+        thr = L.get(K - 1);
+      }
+    }
+    (void)lane;
+  });
+}
+
+template <int P>
+__global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K, float radius,
+                                                  u64 *out, int32_t *out_counts) {
+  const size_t nq = q.n_dev ? *q.n_dev : q.n_max;
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  for (size_t wi = warp; wi < nq; wi += nwarps) {
+    const u32 qi = query_index(q, wi);
+    const int f = q.frame_of ? q.frame_of[qi] : 0;
+    const GridFrame F = g.frames[f];
+    const float qx = q.x[qi], qy = q.y[qi], qz = q.z[qi];
+    WarpList<P> L;
+    L.init();
+    u32 found = 0;
+    if (radius > 0.0f) {
+      const float r2 = fmul(radius, radius);
+      const Window w = tight_window(F, qx, qy, qz, (double)radius);
+      knn_scan<P>(g, F, f, w, false, qx, qy, qz, K, pack_nbr(r2, 0x7FFFFFFF) | 0xFFFFFFFFull, L,
+                  found);
+    } else {
+      // 1) own cell +- 1
+      const Window w1 = ring_window(F, qx, qy, qz, 1);
+      knn_scan<P>(g, F, f, w1, false, qx, qy, qz, K, ~0ull - 1, L, found);
+      bool done = false;
+      if (found >= (u32)K) {
+        const float tau = nbr_d2(L.get(K - 1));
+        const double cov = coverage(F, w1, qx, qy, qz);
+        if (cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5)) done = true;
+        if (!done) {
+          // 2) every point with d2 <= tau lies in the tight window of
+          //    sqrt(tau), and there are >= K of them: exact.
+          const Window w2 = tight_window(F, qx, qy, qz, sqrt((double)tau));
+          if (window_cells(w2) <= 4096) {
+            L.init();
+            found = 0;
+            knn_scan<P>(g, F, f, w2, false, qx, qy, qz, K,
+                        pack_nbr(tau, 0x7FFFFFFF) | 0xFFFFFFFFull, L, found);
+            done = true;
+          }
+        }
+      }
+      if (!done) {  // 3) whole frame
+        L.init();
+        found = 0;
+        knn_scan<P>(g, F, f, w1, true, qx, qy, qz, K, ~0ull - 1, L, found);
+      }
+    }
+    const u32 cnt = found < (u32)K ? found : (u32)K;
+#pragma unroll
+    for (int s = 0; s < P; ++s) {
+      const int j = s * 32 + lane;
+      if (j < (int)cnt) out[(size_t)qi * K + j] = L.e[s];
+    }
+    if (lane == 0 && out_counts) out_counts[qi] = (int32_t)cnt;
+  }
+}
+
+}  // namespace
+
+void grid_radius_count(rvp_context *ctx, const GridView &g, const QuerySet &q, float radius,
+                       bool ref_window, u32 *counts) {
+  const unsigned blocks = grid_for(q.n_max * 32, 256, ctx->num_sms * 16);
+  k_radius_count<<<blocks, 256, 0, ctx->stream>>>(g, q, radius, ref_window, counts);
+  RVP_LAUNCH_CHECK(ctx);
+}
+
+void grid_radius_fill(rvp_context *ctx, const GridView &g, const QuerySet &q, float radius,
+                      bool ref_window, const u64 *offsets, int max_nn, u64 *out_pairs,
+                      u32 *big_list, u32 *big_count) {
+  (void)max_nn;
+  RVP_CUDA_TRY(cudaMemsetAsync(big_count, 0, 4, ctx->stream));
+  const unsigned blocks = grid_for(q.n_max * 32, FILL_WARPS * 32, ctx->num_sms * 16);
+  k_radius_fill<<<blocks, FILL_WARPS * 32, 0, ctx->stream>>>(g, q, radius, ref_window, offsets,
+                                                             out_pairs, big_list, big_count);
+  RVP_LAUNCH_CHECK(ctx);
+}
+
+void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs, const u32 *big_list,
+                       const u32 *big_count, u32 max_big) {
+  static bool attr[64] = {false};
+  if (ctx->device < 64 && !attr[ctx->device]) {
+    RVP_CUDA_TRY(cudaFuncSetAttribute(k_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      BIG_SMEM * 8));
+    attr[ctx->device] = true;
+  }
+  const unsigned blocks = max_big < 1 ? 1 : (max_big < 4096 ? max_big : 4096);
+  k_sort_big<<<blocks, 1024, BIG_SMEM * 8, ctx->stream>>>(offsets, pairs, big_list, big_count);
+  RVP_LAUNCH_CHECK(ctx);
+}
+
+void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k, float radius,
+              u64 *out_pairs, int32_t *out_counts, int qpw, int block_threads) {
+  (void)qpw;
+  const int bt = block_threads > 0 ? block_threads : 256;
+  const unsigned blocks = grid_for(q.n_max * 32, bt, ctx->num_sms * 32);
+  if (k <= 32)
+    k_knn_warp<1><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts);
+  else
+    k_knn_warp<2><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts);
+  RVP_LAUNCH_CHECK(ctx);
+}
+
+}  // namespace rvp

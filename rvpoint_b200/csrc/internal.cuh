@@ -1,0 +1,318 @@
+// Internal declarations of the rvpoint_b200 CUDA library (sm_100a).
+//
+// Layout in HBM (all frames of a batch back to back):
+//   * input clouds: SoA float x[], y[], z[] (what the reference's
+//     PointCloudSoA views, core/point_types.h:24-29);
+//   * grid: points re-ordered by cell key into float4 {x, y, z, idx-bits}
+//     (16 B, one vector load per candidate), bucket table of
+//     {key, start | count<<32} entries (one 16 B load per probe);
+//   * outputs: AoS PointXYZ (12 B) like the reference's PointXYZ* out.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/rvpoint_b200.h"
+
+namespace rvp {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+constexpr u64 kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error {
+  rvp_status status;
+  std::string msg;
+};
+
+#define RVP_CUDA_TRY(expr)                                                   \
+  do {                                                                       \
+    cudaError_t e_ = (expr);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      throw ::rvp::Error{e_ == cudaErrorMemoryAllocation ? RVP_ERR_OOM        \
+                                                          : RVP_ERR_CUDA,    \
+                         std::string(#expr) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+#define RVP_REQUIRE(cond, msg)                                  \
+  do {                                                          \
+    if (!(cond)) throw ::rvp::Error{RVP_ERR_INVALID_ARG, (msg)}; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t b);  // grow-only; contents are not preserved
+  void release();
+  template <class T>
+  T *as() const { return static_cast<T *>(ptr); }
+};
+
+struct HostBuf {  // pinned
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  void reserve(size_t b);
+  void release();
+  template <class T>
+  T *as() const { return static_cast<T *>(ptr); }
+};
+
+struct Grid;
+struct VoxelWork;
+}  // namespace rvp
+
+struct rvp_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  unsigned long long launches = 0;
+  // scratch owned by one-shot entry points (grow-only, reused across calls)
+  rvp::DevBuf scratch[24];
+  rvp::HostBuf pinned[4];
+  rvp::Grid *grid = nullptr;        // grid reused by one-shot kNN entry points
+  rvp::VoxelWork *vwork = nullptr;  // voxel scratch of rvp_voxel_grid
+};
+
+namespace rvp {
+
+inline void count_launch(rvp_context *ctx) {
+  ctx->launches++;
+}
+
+#define RVP_LAUNCH_CHECK(ctx)                                             \
+  do {                                                                    \
+    ::rvp::count_launch(ctx);                                             \
+    cudaError_t e_ = cudaGetLastError();                                  \
+    if (e_ != cudaSuccess)                                                \
+      throw ::rvp::Error{RVP_ERR_CUDA,                                    \
+                         std::string("kernel launch: ") + cudaGetErrorString(e_)}; \
+  } while (0)
+
+inline unsigned grid_for(size_t n, int threads, int cap_blocks) {
+  size_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (cap_blocks > 0 && b > (size_t)cap_blocks) b = (size_t)cap_blocks;
+  return (unsigned)b;
+}
+
+// ---------------------------------------------------------------------------
+// exact IEEE single-precision helpers: the reference is compiled without FP
+// contraction, so every product and sum is rounded on its own.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// d2 = dx*dx + dy*dy + dz*dz with dx = p - q (rvv_common.cpp:102-107)
+__device__ __forceinline__ float dist2(float px, float py, float pz, float qx,
+                                       float qy, float qz) {
+  const float dx = fsub(px, qx), dy = fsub(py, qy), dz = fsub(pz, qz);
+  return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+}
+
+// (d2, idx) packed so that unsigned order == std::pair<float,int> order for
+// d2 >= 0 and idx >= 0 (spatial_hashing.cpp:204-209).
+__device__ __forceinline__ u64 pack_nbr(float d2, int idx) {
+  return ((u64)__float_as_uint(d2) << 32) | (u64)(u32)idx;
+}
+__device__ __forceinline__ float nbr_d2(u64 k) { return __uint_as_float((u32)(k >> 32)); }
+__device__ __forceinline__ int nbr_idx(u64 k) { return (int)(u32)(k & 0xFFFFFFFFull); }
+
+__device__ __forceinline__ u64 mix64(u64 k) {  // splitmix64 finaliser
+  k ^= k >> 30;
+  k *= 0xbf58476d1ce4e5b9ull;
+  k ^= k >> 27;
+  k *= 0x94d049bb133111ebull;
+  k ^= k >> 31;
+  return k;
+}
+
+// float atomics on ordered int images (valid for non-NaN values)
+__device__ __forceinline__ void atomic_min_f(float *a, float v) {
+  if (v >= 0.0f) atomicMin((int *)a, __float_as_int(v));
+  else atomicMax((unsigned *)a, __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f(float *a, float v) {
+  if (v >= 0.0f) atomicMax((int *)a, __float_as_int(v));
+  else atomicMin((unsigned *)a, __float_as_uint(v));
+}
+
+// ---------------------------------------------------------------------------
+// radix sort (radix_sort.cu): stable LSD sort of (u64 key, u32 value) pairs,
+// 8-bit digits. Digits that are constant over all keys are skipped (the
+// global digit histogram shows it), so keys only pay for their live bits.
+// n may live on the device (n_dev) for graph capture; n_max sizes the grid.
+// ---------------------------------------------------------------------------
+struct SortTemp {
+  u64 *keys_alt = nullptr;
+  u32 *vals_alt = nullptr;
+  u32 *tile_hist = nullptr;    // 256 x tiles(n_max)
+  u32 *global_hist = nullptr;  // 256 digit totals of the current pass
+  int *pass_info = nullptr;    // OR and AND of all keys (2 x u64)
+};
+size_t sort_temp_bytes(size_t n_max);
+void sort_temp_carve(SortTemp &t, void *base, size_t n_max);
+void radix_sort_pairs(rvp_context *ctx, u64 *keys, u32 *vals, size_t n_max,
+                      const u64 *n_dev, const SortTemp &t);
+
+// exclusive scan of u32/u64 flags -> u64 offsets (scan.cu). n may be on the
+// device. out[n] receives the total. temp: scan_temp_bytes(n_max).
+size_t scan_temp_bytes(size_t n_max);
+void exclusive_scan_u32_to_u64(rvp_context *ctx, const u32 *in, u64 *out,
+                               size_t n_max, const u64 *n_dev, void *temp);
+
+// ---------------------------------------------------------------------------
+// cell grid (grid.cu)
+// ---------------------------------------------------------------------------
+struct GridFrame {  // per-frame grid parameters (device)
+  float min_x, min_y, min_z;
+  float cell;
+  int gx, gy, gz;
+  int pad;
+  u64 key_base;  // mode 1: frame's first key; mode 0: unused
+};
+
+enum KeyMode { KEY_REF_HASH = 0, KEY_DENSE = 1 };
+
+struct GridView {  // what the query kernels read
+  const float4 *pts;       // cell-sorted {x,y,z,idx}
+  const ulonglong2 *table; // {key, start | count<<32}
+  u64 table_mask;
+  const GridFrame *frames; // per frame
+  const u64 *frame_pt_begin;  // per frame: first sorted position
+  int mode;
+  long long p1, p2;        // mode 0 primes
+};
+
+struct Grid {
+  int n_frames_max = 0;
+  size_t n_max = 0;
+  size_t table_cap = 0;
+  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc;
+  u64 *d_n = nullptr;          // number of points (device)
+  u64 *d_nbuckets = nullptr;   // number of buckets (device)
+  int *d_collision = nullptr;  // mode 0: hash collision detected
+  GridView view(int mode, long long p1, long long p2) const;
+  void reserve(size_t n_max, int n_frames_max);
+  void release();
+};
+
+// Build a grid over frames of SoA points. frame_offsets_dev: n_frames+1
+// int64 on the device. cell: cell size (same for all frames). Mode 0 uses the
+// reference's bbox/eps/grid formulas and prime hash (single frame).
+void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y,
+                const float *z, const int64_t *frame_offsets_dev, int n_frames,
+                size_t n_points, float cell, int mode, long long p1,
+                long long p2, const u64 *n_dev_opt);
+
+// Query helpers (queries are SoA; query q belongs to frame qframe(q)).
+struct QuerySet {
+  const float *x, *y, *z;
+  size_t n_max;
+  const u64 *n_dev;              // optional device count
+  const int32_t *frame_of;       // optional: frame of each query (else 0)
+  const int32_t *order;          // optional: process queries in this order
+};
+
+// radius search, two passes. counts[nq]; then offsets via scan; then fill.
+void grid_radius_count(rvp_context *ctx, const GridView &g, const QuerySet &q,
+                       float radius, bool ref_window, u32 *counts);
+void grid_radius_fill(rvp_context *ctx, const GridView &g, const QuerySet &q,
+                      float radius, bool ref_window, const u64 *offsets,
+                      int max_nn, u64 *out_pairs, u32 *big_list, u32 *big_count);
+void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs,
+                       const u32 *big_list, const u32 *big_count, u32 max_big);
+
+// exact kNN (k <= 64) with ring expansion / brute force fallback. radius > 0
+// bounds the search. skip_flag: candidates whose idx has bit 31 set are
+// ignored (points removed by an earlier stage). out: nq * k packed pairs.
+void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
+              float radius, u64 *out_pairs, int32_t *out_counts, int qpw,
+              int block_threads);
+
+// ---------------------------------------------------------------------------
+// voxel grid (voxel.cu)
+// ---------------------------------------------------------------------------
+struct VoxelWork {
+  DevBuf keys, vals, sort, misc, heads;
+  void reserve(size_t n_max, int n_frames_max);
+  void release();
+};
+// Writes AoS centroids to out_aos, voxel count per frame prefix to
+// out_offsets (n_frames+1, int64), and optionally keys (3 ints per voxel).
+void voxel_grid_run(rvp_context *ctx, VoxelWork &w, const float *x,
+                    const float *y, const float *z,
+                    const int64_t *frame_offsets_dev, int n_frames,
+                    size_t n_max, const u64 *n_dev, float inv_leaf,
+                    float *out_aos, int64_t *out_offsets, int32_t *out_keys,
+                    int *error_flag, float *out_x, float *out_y, float *out_z);
+
+// ---------------------------------------------------------------------------
+// SOR (sor.cu)
+// ---------------------------------------------------------------------------
+// mean distance from sorted kNN lists (k+1 incl. self)
+void sor_mean_from_knn(rvp_context *ctx, const u64 *pairs, int kk,
+                       const int32_t *counts, size_t n_max, const u64 *n_dev,
+                       float *mean, float fallback_radius, bool radius_mode);
+// per-frame sequential statistics, keep mask and ordered AoS copy-out
+void sor_filter_frames(rvp_context *ctx, const float *x, const float *y,
+                       const float *z, const float *mean,
+                       const int64_t *frame_offsets_dev, int n_frames,
+                       size_t n_max, const u64 *n_dev, float alpha,
+                       uint8_t *keep, float *out_aos, int64_t *out_offsets,
+                       float *thresh, void *temp, float *out_x, float *out_y,
+                       float *out_z, u32 *src_index);
+size_t sor_filter_temp_bytes(size_t n_max, int n_frames);
+
+// ---------------------------------------------------------------------------
+// normals (normals.cu)
+// ---------------------------------------------------------------------------
+// Normals from neighbour lists (CSR, each sorted by (d2, idx)).
+// div_centroid: normal_estimation_sc's "/ (k+1)" instead of "* (1/n)".
+void normals_from_lists(rvp_context *ctx, const float *x, const float *y,
+                        const float *z, const u64 *pairs, const u64 *offsets,
+                        const int32_t *fixed_counts, int fixed_k,
+                        size_t n_max, const u64 *n_dev, bool div_centroid,
+                        int iters, float vpx, float vpy, float vpz,
+                        const float *qx, const float *qy, const float *qz,
+                        float *nx, float *ny, float *nz);
+void normals_precise(rvp_context *ctx, const float *x, const float *y,
+                     const float *z, const u64 *pairs, int kk, size_t n,
+                     float vpx, float vpy, float vpz, double cond_fp64,
+                     float *nx, float *ny, float *nz, float *cond,
+                     uint8_t *used_fp64);
+
+// ---------------------------------------------------------------------------
+// RANSAC (ransac.cu)
+// ---------------------------------------------------------------------------
+struct RansacParams {
+  float thresh;
+  int max_iters;
+  float collinear;
+  double log_p;  // log(1 - clamp(p, .5, .9999)), computed on the host
+};
+// One block per frame over SoA clouds; frame f = [off[f], off[f+1]).
+void ransac_frames(rvp_context *ctx, const float *x, const float *y,
+                   const float *z, const int64_t *frame_offsets_dev,
+                   int n_frames, const int *rand_dev, const RansacParams &p,
+                   float *model, int32_t *best, int32_t *iters_run,
+                   int32_t *counts_all, bool eval_all);
+void extract_plane_run(rvp_context *ctx, const float *x, const float *y,
+                       const float *z, size_t n, const float *model_dev,
+                       float thresh, float *in_aos, float *out_aos,
+                       u64 *counts_dev, void *temp);
+size_t extract_temp_bytes(size_t n);
+
+}  // namespace rvp

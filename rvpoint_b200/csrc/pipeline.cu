@@ -1,0 +1,309 @@
+// Batched frames: the chain tools/pipeline_export.cpp:351-498 runs per frame
+// (voxel_grid_downsamp_rvv_v2 -> sor_rvv -> normal_estimation_sc ->
+// ransac_plane_rvv), here for many frames of uneven size in one sequence of
+// kernels. Frame boundaries and every intermediate size stay in device memory
+// (offset arrays), kernels are sized by the batch's point capacity and read
+// the live counts on the device, so the whole run can be captured once in a
+// CUDA graph and replayed.
+//
+//   voxel      one sort over (frame, voxel) keys for the whole batch
+//   grid       one sort + table over (frame, cell) keys of the voxel points
+//   SOR kNN    exact k+1 nearest per voxel point (ring / tight window /
+//              brute force fallback), mean distance, per-frame sequential
+//              statistics, ordered compaction
+//   normals    the removed points are flagged in the same grid, the k+1
+//              nearest kept points of every kept point give the covariance
+//   RANSAC     one block per frame over the kept points
+#include <math.h>
+
+#include <algorithm>
+#include <new>
+
+#include "internal.cuh"
+
+using rvp::u32;
+using rvp::u64;
+
+struct rvp_pipeline {
+  rvp_context *ctx = nullptr;
+  rvp_pipeline_config cfg{};
+  size_t max_points = 0;
+  int max_frames = 0;
+  float cell = 0.0f;
+  rvp::VoxelWork vw;
+  rvp::Grid grid;
+  rvp::DevBuf in_x, in_y, in_z, in_offs;
+  rvp::DevBuf vox_aos, vox_x, vox_y, vox_z, vox_offs, vox_frame;
+  rvp::DevBuf knn_pairs, knn_counts, mean, keep, sor_tmp;
+  rvp::DevBuf sor_aos, sor_x, sor_y, sor_z, sor_offs, sor_frame, sor_src;
+  rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
+  rvp::DevBuf r_model, r_best, r_iters, r_rand;
+  int n_frames_last = 0;
+};
+
+namespace {
+template <class F>
+rvp_status guard(rvp_context *ctx, F &&f) {
+  try {
+    f();
+    return RVP_OK;
+  } catch (const rvp::Error &e) {
+    if (ctx) ctx->last_error = e.msg;
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    if (ctx) ctx->last_error = "host allocation failed";
+    return RVP_ERR_OOM;
+  } catch (...) {
+    if (ctx) ctx->last_error = "unknown error";
+    return RVP_ERR_CUDA;
+  }
+}
+
+__global__ void k_frame_ids(const int64_t *offs, int n_frames, size_t n_max, int32_t *frame) {
+  const u64 n = (u64)offs[n_frames];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n && i < n_max;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n_frames - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((u64)offs[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    frame[i] = lo;
+  }
+}
+
+// flag grid points whose source point was removed by SOR
+__global__ void k_mark_removed(float4 *pts, const uint8_t *keep, const u64 *n_dev, size_t n_max) {
+  const size_t n = n_dev ? *n_dev : n_max;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const u32 idx = __float_as_uint(pts[i].w);
+    if (!keep[idx & 0x7FFFFFFFu]) pts[i].w = __uint_as_float(idx | 0x80000000u);
+  }
+}
+}  // namespace
+
+extern "C" {
+
+rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
+                               size_t max_points, int max_frames, rvp_pipeline **out) {
+  if (!ctx || !cfg || !out) return RVP_ERR_INVALID_ARG;
+  *out = nullptr;
+  rvp_pipeline *p = new (std::nothrow) rvp_pipeline();
+  if (!p) return RVP_ERR_OOM;
+  rvp_status s = guard(ctx, [&] {
+    RVP_REQUIRE(max_points >= 1 && max_points < 0x7FFFFFFFull, "max_points out of range");
+    RVP_REQUIRE(max_frames >= 1, "max_frames must be >= 1");
+    RVP_REQUIRE(cfg->leaf_size > 0.0f, "leaf_size must be > 0");
+    RVP_REQUIRE(cfg->sor_k >= 1 && cfg->sor_k + 1 <= 64, "sor_k must be in [1, 63]");
+    RVP_REQUIRE(cfg->normal_k >= 1 && cfg->normal_k + 1 <= 64, "normal_k must be in [1, 63]");
+    RVP_REQUIRE(cfg->ransac_iters >= 0, "ransac_iters must be >= 0");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    p->ctx = ctx;
+    p->cfg = *cfg;
+    p->max_points = max_points;
+    p->max_frames = max_frames;
+    p->cell = cfg->cell_size > 0.0f ? cfg->cell_size : 2.5f * cfg->leaf_size;
+    const size_t N = max_points;
+    const size_t F1 = (size_t)max_frames + 1;
+    p->in_x.reserve(N * 4); p->in_y.reserve(N * 4); p->in_z.reserve(N * 4);
+    p->in_offs.reserve(F1 * 8);
+    p->vw.reserve(N, max_frames);
+    p->grid.reserve(N, max_frames);
+    p->vox_aos.reserve(N * 12);
+    p->vox_x.reserve(N * 4); p->vox_y.reserve(N * 4); p->vox_z.reserve(N * 4);
+    p->vox_offs.reserve(F1 * 8);
+    p->vox_frame.reserve(N * 4);
+    const int ks = cfg->sor_k + 1, kn = cfg->normal_k + 1;
+    p->knn_pairs.reserve(N * (size_t)ks * 8);
+    p->knn_counts.reserve(N * 4);
+    p->mean.reserve(N * 4);
+    p->keep.reserve(N);
+    p->sor_tmp.reserve(rvp::sor_filter_temp_bytes(N, max_frames));
+    p->sor_aos.reserve(N * 12);
+    p->sor_x.reserve(N * 4); p->sor_y.reserve(N * 4); p->sor_z.reserve(N * 4);
+    p->sor_offs.reserve(F1 * 8);
+    p->sor_frame.reserve(N * 4);
+    p->sor_src.reserve(N * 4);
+    p->nrm_pairs.reserve(N * (size_t)kn * 8);
+    p->nrm_counts.reserve(N * 4);
+    p->nx.reserve(N * 4); p->ny.reserve(N * 4); p->nz.reserve(N * 4);
+    p->r_model.reserve((size_t)max_frames * 16);
+    p->r_best.reserve((size_t)max_frames * 4);
+    p->r_iters.reserve((size_t)max_frames * 4);
+    // the reference's srand(0) + rand() stream, shared by every frame
+    const size_t R = 3 * (size_t)std::max(cfg->ransac_iters, 1);
+    std::vector<int> rs(R);
+    srand(0);
+    for (size_t i = 0; i < R; ++i) rs[i] = rand();
+    srand(0);
+    p->r_rand.reserve(R * 4);
+    RVP_CUDA_TRY(cudaMemcpy(p->r_rand.ptr, rs.data(), R * 4, cudaMemcpyHostToDevice));
+  });
+  if (s != RVP_OK) {
+    delete p;
+    return s;
+  }
+  *out = p;
+  return RVP_OK;
+}
+
+rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  rvp::DevBuf *bufs[] = {&p->in_x, &p->in_y, &p->in_z, &p->in_offs, &p->vox_aos, &p->vox_x,
+                         &p->vox_y, &p->vox_z, &p->vox_offs, &p->vox_frame, &p->knn_pairs,
+                         &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
+                         &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
+                         &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
+                         &p->r_best, &p->r_iters, &p->r_rand};
+  for (auto *b : bufs) b->release();
+  p->vw.release();
+  p->grid.release();
+  delete p;
+  return RVP_OK;
+}
+
+rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float *y,
+                                   const float *z, const int64_t *offs, int n_frames,
+                                   size_t n_points) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  rvp_context *ctx = p->ctx;
+  return guard(ctx, [&] {
+    RVP_REQUIRE(n_frames >= 1 && n_frames <= p->max_frames, "n_frames out of range");
+    RVP_REQUIRE(n_points <= p->max_points, "n_points exceeds the pipeline capacity");
+    RVP_REQUIRE(x && y && z && offs, "null pointer");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    const rvp_pipeline_config &c = p->cfg;
+    const size_t N = n_points > 0 ? n_points : 1;
+    cudaStream_t st = ctx->stream;
+    const int sms = ctx->num_sms;
+    p->n_frames_last = n_frames;
+    int64_t *vox_offs = p->vox_offs.as<int64_t>();
+    const u64 *n_vox = reinterpret_cast<const u64 *>(vox_offs + n_frames);
+    int64_t *sor_offs = p->sor_offs.as<int64_t>();
+    const u64 *n_sor = reinterpret_cast<const u64 *>(sor_offs + n_frames);
+
+    // 1) voxel grid
+    const float inv_leaf = 1.0f / c.leaf_size;
+    rvp::voxel_grid_run(ctx, p->vw, x, y, z, offs, n_frames, N, nullptr, inv_leaf,
+                        p->vox_aos.as<float>(), vox_offs, nullptr, nullptr, p->vox_x.as<float>(),
+                        p->vox_y.as<float>(), p->vox_z.as<float>());
+    // 2) grid over the voxel points of every frame
+    rvp::grid_build(ctx, p->grid, p->vox_x.as<float>(), p->vox_y.as<float>(),
+                    p->vox_z.as<float>(), vox_offs, n_frames, N, p->cell, rvp::KEY_DENSE, 0, 0,
+                    n_vox);
+    k_frame_ids<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(vox_offs, n_frames, N,
+                                                                 p->vox_frame.as<int32_t>());
+    RVP_LAUNCH_CHECK(ctx);
+    const rvp::GridView gv = p->grid.view(rvp::KEY_DENSE, 0, 0);
+    // 3) SOR: exact k+1 nearest, mean distance, per-frame statistics
+    const int ks = c.sor_k + 1;
+    rvp::QuerySet qv{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N, n_vox,
+                     p->vox_frame.as<int32_t>(), nullptr};
+    rvp::grid_knn(ctx, gv, qv, ks, 0.0f, p->knn_pairs.as<u64>(), p->knn_counts.as<int32_t>(),
+                  c.queries_per_warp, c.block_threads);
+    rvp::sor_mean_from_knn(ctx, p->knn_pairs.as<u64>(), ks, p->knn_counts.as<int32_t>(), N, n_vox,
+                           p->mean.as<float>(), 0.0f, false);
+    rvp::sor_filter_frames(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
+                           p->mean.as<float>(), vox_offs, n_frames, N, n_vox, c.sor_alpha,
+                           p->keep.as<uint8_t>(), p->sor_aos.as<float>(), sor_offs, nullptr,
+                           p->sor_tmp.ptr, p->sor_x.as<float>(), p->sor_y.as<float>(),
+                           p->sor_z.as<float>(), p->sor_src.as<u32>());
+    // 4) normals: k+1 nearest kept points of every kept point
+    k_mark_removed<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(
+        p->grid.b_pts.as<float4>(), p->keep.as<uint8_t>(), n_vox, N);
+    RVP_LAUNCH_CHECK(ctx);
+    k_frame_ids<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(sor_offs, n_frames, N,
+                                                                 p->sor_frame.as<int32_t>());
+    RVP_LAUNCH_CHECK(ctx);
+    const int kn = c.normal_k + 1;
+    rvp::QuerySet qs{p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(), N, n_sor,
+                     p->sor_frame.as<int32_t>(), nullptr};
+    rvp::grid_knn(ctx, gv, qs, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(),
+                  c.queries_per_warp, c.block_threads);
+    rvp::normals_from_lists(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
+                            p->nrm_pairs.as<u64>(), nullptr, p->nrm_counts.as<int32_t>(), kn, N,
+                            n_sor, true, c.eigen_iters, c.vp_x, c.vp_y, c.vp_z,
+                            p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(),
+                            p->nx.as<float>(), p->ny.as<float>(), p->nz.as<float>());
+    // 5) RANSAC per frame on the kept points
+    double pc = (double)c.ransac_prob;
+    pc = pc < 0.5 ? 0.5 : (pc > 0.9999 ? 0.9999 : pc);
+    rvp::RansacParams prm{c.ransac_thresh, c.ransac_iters, c.ransac_collinear, log(1.0 - pc)};
+    rvp::ransac_frames(ctx, p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(),
+                       sor_offs, n_frames, p->r_rand.as<int>(), prm, p->r_model.as<float>(),
+                       p->r_best.as<int32_t>(), p->r_iters.as<int32_t>(), nullptr, false);
+  });
+}
+
+rvp_status rvp_pipeline_outputs_get(rvp_pipeline *p, rvp_pipeline_outputs *o) {
+  if (!p || !o) return RVP_ERR_INVALID_ARG;
+  o->voxel_aos = p->vox_aos.as<float>();
+  o->voxel_offsets = p->vox_offs.as<int64_t>();
+  o->sor_aos = p->sor_aos.as<float>();
+  o->sor_offsets = p->sor_offs.as<int64_t>();
+  o->nx = p->nx.as<float>();
+  o->ny = p->ny.as<float>();
+  o->nz = p->nz.as<float>();
+  o->ransac_model = p->r_model.as<float>();
+  o->ransac_count = p->r_best.as<int32_t>();
+  o->ransac_iters = p->r_iters.as<int32_t>();
+  o->sor_mean_dists = p->mean.as<float>();
+  return RVP_OK;
+}
+
+rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const float *y, const float *z,
+                                 const int64_t *frame_offsets, int n_frames, float *voxel_aos,
+                                 int64_t *voxel_offsets, float *sor_aos, int64_t *sor_offsets,
+                                 float *nx, float *ny, float *nz, float *ransac_model,
+                                 int32_t *ransac_count) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  rvp_context *ctx = p->ctx;
+  rvp_status s = guard(ctx, [&] {
+    RVP_REQUIRE(frame_offsets && n_frames >= 1 && n_frames <= p->max_frames, "bad frames");
+    const size_t n = (size_t)frame_offsets[n_frames];
+    RVP_REQUIRE(n <= p->max_points, "batch exceeds the pipeline capacity");
+    RVP_REQUIRE(n == 0 || (x && y && z), "null pointer");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (n) {
+      RVP_CUDA_TRY(cudaMemcpyAsync(p->in_x.ptr, x, n * 4, cudaMemcpyHostToDevice, st));
+      RVP_CUDA_TRY(cudaMemcpyAsync(p->in_y.ptr, y, n * 4, cudaMemcpyHostToDevice, st));
+      RVP_CUDA_TRY(cudaMemcpyAsync(p->in_z.ptr, z, n * 4, cudaMemcpyHostToDevice, st));
+    }
+    RVP_CUDA_TRY(cudaMemcpyAsync(p->in_offs.ptr, frame_offsets, (n_frames + 1) * 8,
+                                 cudaMemcpyHostToDevice, st));
+  });
+  if (s != RVP_OK) return s;
+  const size_t n = (size_t)frame_offsets[n_frames];
+  s = rvp_pipeline_run_device(p, p->in_x.as<float>(), p->in_y.as<float>(), p->in_z.as<float>(),
+                              p->in_offs.as<int64_t>(), n_frames, n);
+  if (s != RVP_OK) return s;
+  return guard(ctx, [&] {
+    cudaStream_t st = ctx->stream;
+    std::vector<int64_t> vo(n_frames + 1), so(n_frames + 1);
+    RVP_CUDA_TRY(cudaMemcpyAsync(vo.data(), p->vox_offs.ptr, (n_frames + 1) * 8,
+                                 cudaMemcpyDeviceToHost, st));
+    RVP_CUDA_TRY(cudaMemcpyAsync(so.data(), p->sor_offs.ptr, (n_frames + 1) * 8,
+                                 cudaMemcpyDeviceToHost, st));
+    RVP_CUDA_TRY(cudaStreamSynchronize(st));
+    const size_t nv = (size_t)vo[n_frames], ns = (size_t)so[n_frames];
+    if (voxel_offsets) memcpy(voxel_offsets, vo.data(), (n_frames + 1) * 8);
+    if (sor_offsets) memcpy(sor_offsets, so.data(), (n_frames + 1) * 8);
+    auto d2h = [&](void *dst, const void *src, size_t b) {
+      if (dst && b) RVP_CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, st));
+    };
+    d2h(voxel_aos, p->vox_aos.ptr, nv * 12);
+    d2h(sor_aos, p->sor_aos.ptr, ns * 12);
+    d2h(nx, p->nx.ptr, ns * 4);
+    d2h(ny, p->ny.ptr, ns * 4);
+    d2h(nz, p->nz.ptr, ns * 4);
+    d2h(ransac_model, p->r_model.ptr, (size_t)n_frames * 16);
+    d2h(ransac_count, p->r_best.ptr, (size_t)n_frames * 4);
+    RVP_CUDA_TRY(cudaStreamSynchronize(st));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,256 @@
+// RANSAC plane fitting (segmentation/ransac_plane.cpp:18-111) for many
+// frames, one thread block per frame.
+//
+// The reference draws three rand() % n indices per iteration after
+// srand(0); the raw rand() stream is the same for every call, so it is an
+// input table here (rand_dev, 3 * max_iters values) and i = r % n is taken
+// on the device. Hypotheses are evaluated 32 at a time: each warp walks the
+// frame's points, every lane tests its point against hypothesis h and
+// __ballot_sync/__popc turns the 32 tests into one count that lane h
+// accumulates. Thread 0 then replays the reference's sequential logic
+// (strictly greater count wins, adaptive k_iters with p = 0.99 in double),
+// so best count, model and the number of executed iterations are the
+// reference's, and the loop stops as early as the reference's does.
+#include <float.h>
+#include <math.h>
+
+#include "internal.cuh"
+
+namespace rvp {
+
+namespace {
+constexpr int HB = 32;        // hypotheses per batch
+constexpr int R_THREADS = 512;
+constexpr int R_PTS = 4;      // points per lane per pass (amortises the hypothesis loads)
+
+// compute_plane_coefficients (ransac_plane.cpp:18-50), exact op order.
+__device__ __forceinline__ bool plane_coeffs(float x1, float y1, float z1, float x2, float y2,
+                                             float z2, float x3, float y3, float z3, float col,
+                                             float4 &m) {
+  const float v1x = fsub(x2, x1), v1y = fsub(y2, y1), v1z = fsub(z2, z1);
+  const float v2x = fsub(x3, x1), v2y = fsub(y3, y1), v2z = fsub(z3, z1);
+  float a = fsub(fmul(v1y, v2z), fmul(v1z, v2y));
+  float b = fsub(fmul(v1z, v2x), fmul(v1x, v2z));
+  float c = fsub(fmul(v1x, v2y), fmul(v1y, v2x));
+  const float norm = __fsqrt_rn(fadd(fadd(fmul(a, a), fmul(b, b)), fmul(c, c)));
+  if (norm < col) return false;
+  a = fdiv(a, norm);
+  b = fdiv(b, norm);
+  c = fdiv(c, norm);
+  const float d = -fadd(fadd(fmul(a, x1), fmul(b, y1)), fmul(c, z1));
+  m = make_float4(a, b, c, d);
+  return true;
+}
+
+// |a*x + b*y + c*z + d| <= t  (ransac_plane.cpp:80-87)
+__device__ __forceinline__ bool is_inlier(const float4 &m, float x, float y, float z, float t) {
+  return fabsf(fadd(fadd(fadd(fmul(m.x, x), fmul(m.y, y)), fmul(m.z, z)), m.w)) <= t;
+}
+
+__global__ __launch_bounds__(R_THREADS) void k_ransac(
+    const float *__restrict__ X, const float *__restrict__ Y, const float *__restrict__ Z,
+    const int64_t *offs, const int *__restrict__ rnd, RansacParams prm, float *model_out,
+    int32_t *best_out, int32_t *iters_out, int32_t *counts_all, bool eval_all) {
+  const int f = blockIdx.x;
+  const int64_t a0 = offs[f];
+  const u32 n = (u32)(offs[f + 1] - a0);
+  const float *x = X + a0, *y = Y + a0, *z = Z + a0;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  constexpr int NW = R_THREADS / 32;
+
+  __shared__ float4 hyp[HB];
+  __shared__ int hcode[HB];  // 0 valid, -1 repeated index, -2 collinear
+  __shared__ u32 hcnt[HB];
+  __shared__ int s_best, s_kiters, s_stop, s_iters;
+  __shared__ float4 s_model;
+
+  if (n < 3) {  // ransac_plane.cpp:59
+    if (tid == 0) {
+      model_out[4 * f + 0] = model_out[4 * f + 1] = model_out[4 * f + 2] = model_out[4 * f + 3] = 0;
+      best_out[f] = 0;
+      if (iters_out) iters_out[f] = 0;
+    }
+    if (counts_all)
+      for (int it = tid; it < prm.max_iters; it += R_THREADS)
+        counts_all[(size_t)f * prm.max_iters + it] = -3;
+    return;
+  }
+  if (tid == 0) {
+    s_best = 0;
+    s_kiters = prm.max_iters;
+    s_stop = 0;
+    s_iters = prm.max_iters;
+    s_model = make_float4(0, 0, 0, 0);
+  }
+  __syncthreads();
+
+  for (int base = 0; base < prm.max_iters; base += HB) {
+    if (s_stop && !eval_all) break;
+    if (tid < HB) {
+      const int it = base + tid;
+      float4 m = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);  // NaN: never an inlier
+      int code = -3;
+      if (it < prm.max_iters) {
+        const u32 i1 = (u32)rnd[3 * it + 0] % n;
+        const u32 i2 = (u32)rnd[3 * it + 1] % n;
+        const u32 i3 = (u32)rnd[3 * it + 2] % n;
+        if (i1 == i2 || i1 == i3 || i2 == i3) {
+          code = -1;
+        } else if (!plane_coeffs(x[i1], y[i1], z[i1], x[i2], y[i2], z[i2], x[i3], y[i3], z[i3],
+                                 prm.collinear, m)) {
+          code = -2;
+          m = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);
+        } else {
+          code = 0;
+        }
+      }
+      hyp[tid] = m;
+      hcode[tid] = code;
+      hcnt[tid] = 0;
+    }
+    __syncthreads();
+
+    u32 acc = 0;  // lane h accumulates hypothesis h
+    for (u32 p0 = (u32)wid * 32 * R_PTS; p0 < n; p0 += NW * 32 * R_PTS) {
+      float px[R_PTS], py[R_PTS], pz[R_PTS];
+      bool pv[R_PTS];
+#pragma unroll
+      for (int r = 0; r < R_PTS; ++r) {
+        const u32 i = p0 + r * 32 + lane;
+        pv[r] = i < n;
+        px[r] = pv[r] ? __ldg(&x[i]) : 0.0f;
+        py[r] = pv[r] ? __ldg(&y[i]) : 0.0f;
+        pz[r] = pv[r] ? __ldg(&z[i]) : 0.0f;
+      }
+#pragma unroll 4
+      for (int h = 0; h < HB; ++h) {
+        const float4 m = hyp[h];
+        u32 c = 0;
+#pragma unroll
+        for (int r = 0; r < R_PTS; ++r)
+          c += __popc(__ballot_sync(0xffffffffu, pv[r] && is_inlier(m, px[r], py[r], pz[r], prm.thresh)));
+        if (lane == h) acc += c;
+      }
+    }
+    atomicAdd(&hcnt[lane], acc);
+    __syncthreads();
+
+    if (tid == 0) {
+      // replay ransac_plane.cpp:67-107 for this batch, in order
+      for (int h = 0; h < HB && !s_stop; ++h) {
+        const int it = base + h;
+        if (it >= s_kiters || it >= prm.max_iters) {
+          s_stop = 1;
+          s_iters = it;
+          break;
+        }
+        if (hcode[h] != 0) continue;
+        const int cur = (int)hcnt[h];
+        if (cur > s_best) {
+          s_best = cur;
+          s_model = hyp[h];
+          const double w = (double)cur / (double)n;
+          double p_no = 1.0 - pow(w, 3.0);
+          p_no = fmax(DBL_EPSILON, p_no);
+          p_no = fmin(1.0 - DBL_EPSILON, p_no);
+          const double log_no = log(p_no);
+          if (fabs(log_no) > 1e-7) {
+            const int dyn = (int)ceil(prm.log_p / log_no);
+            if (dyn > 0 && dyn < s_kiters) s_kiters = dyn;
+          }
+        }
+      }
+      if (!s_stop && base + HB >= prm.max_iters) {
+        s_stop = 1;
+        s_iters = prm.max_iters;
+      }
+    }
+    if (counts_all && tid < HB && base + tid < prm.max_iters)
+      counts_all[(size_t)f * prm.max_iters + base + tid] =
+          hcode[tid] == 0 ? (int32_t)hcnt[tid] : hcode[tid];
+    __syncthreads();
+  }
+  if (counts_all && !eval_all) {
+    // hypotheses past the early stop were not evaluated
+    const int done = ((s_iters + HB - 1) / HB) * HB;
+    for (int it = done + tid; it < prm.max_iters; it += R_THREADS)
+      counts_all[(size_t)f * prm.max_iters + it] = -3;
+  }
+  if (tid == 0) {
+    model_out[4 * f + 0] = s_model.x;
+    model_out[4 * f + 1] = s_model.y;
+    model_out[4 * f + 2] = s_model.z;
+    model_out[4 * f + 3] = s_model.w;
+    best_out[f] = s_best;
+    if (iters_out) iters_out[f] = s_iters;
+  }
+}
+
+// extract_plane_inliers_outliers_rvv, scalar branch (ransac_plane.cpp:373-381):
+// inlier iff -t <= a*x + b*y + c*z + d <= t.
+__global__ void k_plane_flags(const float *x, const float *y, const float *z, size_t n,
+                              const float *model, float t, u32 *flags) {
+  const float4 m = make_float4(model[0], model[1], model[2], model[3]);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float d = fadd(fadd(fadd(fmul(m.x, x[i]), fmul(m.y, y[i])), fmul(m.z, z[i])), m.w);
+    flags[i] = (d >= -t && d <= t) ? 1u : 0u;
+  }
+}
+
+__global__ void k_plane_scatter(const float *x, const float *y, const float *z, size_t n,
+                                const u32 *flags, const u64 *pos, float *in_aos, float *out_aos,
+                                u64 *counts) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const u64 pi = pos[i];
+    float *dst = nullptr;
+    if (flags[i]) {
+      if (in_aos) dst = in_aos + 3 * pi;
+    } else {
+      if (out_aos) dst = out_aos + 3 * (i - pi);
+    }
+    if (dst) {
+      dst[0] = x[i];
+      dst[1] = y[i];
+      dst[2] = z[i];
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counts[0] = pos[n];
+    counts[1] = n - pos[n];
+  }
+}
+
+inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+}  // namespace
+
+void ransac_frames(rvp_context *ctx, const float *x, const float *y, const float *z,
+                   const int64_t *offs, int n_frames, const int *rand_dev, const RansacParams &p,
+                   float *model, int32_t *best, int32_t *iters_run, int32_t *counts_all,
+                   bool eval_all) {
+  if (n_frames <= 0) return;
+  k_ransac<<<n_frames, R_THREADS, 0, ctx->stream>>>(x, y, z, offs, rand_dev, p, model, best,
+                                                    iters_run, counts_all, eval_all);
+  RVP_LAUNCH_CHECK(ctx);
+}
+
+size_t extract_temp_bytes(size_t n) {
+  return al(n * 4) + al((n + 1) * 8) + scan_temp_bytes(n);
+}
+
+void extract_plane_run(rvp_context *ctx, const float *x, const float *y, const float *z, size_t n,
+                       const float *model_dev, float thresh, float *in_aos, float *out_aos,
+                       u64 *counts_dev, void *temp) {
+  char *p = static_cast<char *>(temp);
+  u32 *flags = reinterpret_cast<u32 *>(p); p += al(n * 4);
+  u64 *pos = reinterpret_cast<u64 *>(p); p += al((n + 1) * 8);
+  const unsigned g = grid_for(n, 256, ctx->num_sms * 16);
+  k_plane_flags<<<g, 256, 0, ctx->stream>>>(x, y, z, n, model_dev, thresh, flags);
+  RVP_LAUNCH_CHECK(ctx);
+  exclusive_scan_u32_to_u64(ctx, flags, pos, n, nullptr, p);
+  k_plane_scatter<<<g, 256, 0, ctx->stream>>>(x, y, z, n, flags, pos, in_aos, out_aos, counts_dev);
+  RVP_LAUNCH_CHECK(ctx);
+}
+
+}  // namespace rvp
