@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Batched point-cloud pipeline benchmark (one JSON line on rank 0).
+
+Workload: 256 synthetic spinning-LiDAR frames (64 beams x 2048 azimuths cast
+against a ground plane and 40 boxes, sigma = 2 cm, 5% drop, each thinned to
+a log-uniform size in [20k, 131k] points), the chain
+voxel(0.1 m) -> SOR(k=16, std_mul=1) -> normals(k=16) -> RANSAC(1000
+hypotheses, 0.05 m) per frame. A step is one pass of the chain over the
+whole batch. `value` is input points per second with the batch resident in
+HBM; `e2e` is the same through the host-buffer C entry point
+(rvp_pipeline_run_host) with the host<->device copies inside the timed
+region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1: launched by torch.distributed.run, one rank per GPU; every rank owns
+its own 256 frames (weak scaling, no data-path collective); time = max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "pipeline Mpts/s on 1 B200; learned-vs-plain RANSAC time at equal inlier count"
+UNIT = "Mpts/s"
+WORKLOAD = "lidar_batch_256_frames_voxel0.1_sor16_normals16_ransac1000"
+LEAF, SOR_K, SOR_ALPHA, NORMAL_K, R_THRESH, R_ITERS = 0.1, 16, 1.0, 16, 0.05, 1000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=256)
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# CPU side (the reference's scalar path; test infrastructure under oracle/)
+# ---------------------------------------------------------------------------
+def _cpu_frame(args):
+    """voxel -> sor_rvv -> normal_estimation_sc -> ransac_plane_rvv on one
+    frame with the reference's own code (or the restatement if absent)."""
+    x, y, z = args
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from oracle import oracle as O
+    from rvpoint_b200.datasets import Cloud
+    c = Cloud(np.ascontiguousarray(x), np.ascontiguousarray(y), np.ascontiguousarray(z))
+    t0 = time.perf_counter()
+    if O.reference_available():
+        R = O.Reference()
+        v = R.voxel_grid(c, LEAF)
+        vc = Cloud.from_xyz(v)
+        s = R.sor_rvv(vc, SOR_K, SOR_ALPHA)
+        sc = Cloud.from_xyz(s)
+        R.normals_sc(sc, NORMAL_K)
+        R.ransac_plane(sc, R_THRESH, R_ITERS)
+        kind = "reference"
+    else:
+        R = O.Restatement()
+        v, _ = R.voxel_grid(c, LEAF)
+        vc = Cloud.from_xyz(v)
+        s, _, _ = R.sor_exact(vc, SOR_K, SOR_ALPHA)
+        sc = Cloud.from_xyz(s)
+        R.normals_knn(sc, NORMAL_K)
+        R.ransac_plane(sc, R_THRESH, R_ITERS, O.libc_rand_stream(3 * R_ITERS))
+        kind = "port"
+    return time.perf_counter() - t0, int(x.shape[0]), kind
+
+
+def cpu_baseline(batch, budget_s: float) -> dict:
+    """Frames in order, single-threaded (the reference library is), until
+    the CPU budget is spent."""
+    from oracle import oracle as O
+    O.build() if not os.path.exists(O.RESTATEMENT_SO) else None
+    t_tot, pts, frames, kind = 0.0, 0, 0, "port"
+    for f in range(batch.n_frames):
+        fr = batch.frame(f)
+        dt, n, kind = _cpu_frame((fr.x, fr.y, fr.z))
+        t_tot += dt
+        pts += n
+        frames += 1
+        if t_tot >= budget_s:
+            break
+    return {"value": pts / t_tot / 1e6, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"first {frames} of {batch.n_frames} frames ({pts} input points), "
+                      f"full chain, one thread, {t_tot:.1f} s"}
+
+
+def reference_arm(a, rank: int) -> None:
+    if rank != 0:
+        return
+    from rvpoint_b200 import datasets as D
+    from oracle import oracle as O
+    if not os.path.exists(O.RESTATEMENT_SO):
+        O.build()
+    batch = D.lidar_batch(n_frames=a.frames)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    workers = max(1, cores)
+    ctx = mp.get_context("spawn")
+    times, pts_step = [], []
+    kind = "port"
+    with ctx.Pool(workers) as pool:
+        nxt = 0
+        for step in range(a.warmup + a.steps):
+            # one frame per worker per step, frames in order
+            sel = [(nxt + j) % batch.n_frames for j in range(min(workers, batch.n_frames))]
+            nxt = (nxt + len(sel)) % batch.n_frames
+            jobs = [(batch.frame(f).x, batch.frame(f).y, batch.frame(f).z) for f in sel]
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_frame, jobs)
+            dt = time.perf_counter() - t0
+            kind = res[0][2]
+            if step >= a.warmup:
+                times.append(dt)
+                pts_step.append(sum(r[1] for r in res))
+    value = sum(pts_step) / sum(times) / 1e6
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1e3 * statistics.mean(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames_per_step": min(workers, batch.n_frames),
+                       "leaf": LEAF, "sor_k": SOR_K, "normal_k": NORMAL_K,
+                       "ransac_iters": R_ITERS, "ransac_thresh": R_THRESH},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind,
+                             "sample": f"{min(workers, batch.n_frames)} frames per step, one "
+                                       f"frame per process, {workers} processes"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        gid = ids[gpu_index] if gpu_index < len(ids) else str(gpu_index)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gid}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [v.strip() for v in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except Exception:
+                continue
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+# algorithmic bytes per unit (what one launch of each stage must move)
+def stage_bytes(stage: str, n_in: int, n_vox: int, n_sor: int, n_frames: int) -> float:
+    ks, kn = SOR_K + 1, NORMAL_K + 1
+    return {
+        "voxel": 12.0 * n_in + 12.0 * n_vox,
+        "grid_build": 28.0 * n_vox,
+        "sor_knn": (12.0 + 8.0 * ks) * n_vox,
+        "sor_filter": 12.0 * n_vox + 1.0 * n_vox + 12.0 * n_sor,
+        "normals_knn": (12.0 + 8.0 * kn) * n_sor,
+        "normals": 24.0 * n_sor,
+        "ransac": 12.0 * n_sor + 4.0 * n_frames,
+    }[stage]
+
+
+STAGE_KERNEL = {"sor_knn": "k_knn_warp", "normals_knn": "k_knn_warp", "ransac": "k_ransac",
+                "normals": "k_normals_lists", "voxel": "voxel stage (sort + reduce)",
+                "grid_build": "grid build (sort + table)", "sor_filter": "SOR statistics"}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        reference_arm(a, rank)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from rvpoint_b200 import api, autotune
+    from rvpoint_b200 import datasets as D
+
+    batch = D.lidar_batch(n_frames=a.frames, seed=D.SEED_BASE + 2 + 7919 * rank)
+    n, nf = batch.n, batch.n_frames
+    dev = torch.device("cuda", local)
+    x = torch.from_numpy(batch.x).to(dev)
+    y = torch.from_numpy(batch.y).to(dev)
+    z = torch.from_numpy(batch.z).to(dev)
+    offs = torch.from_numpy(batch.offsets).to(dev)
+    ctx = api.Context(local)
+    pipe = api.Pipeline(max_points=n, max_frames=nf, leaf_size=LEAF, sor_k=SOR_K,
+                        sor_alpha=SOR_ALPHA, normal_k=NORMAL_K, ransac_thresh=R_THRESH,
+                        ransac_iters=R_ITERS, ctx=ctx)
+    args = (x, y, z, offs, nf, n)
+    best = None
+    if not a.no_tune:
+        best, _ = autotune.tune(pipe, *args)
+    for _ in range(max(a.warmup, 1)):
+        pipe.run_device(*args)
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    pipe.run_device(*args)
+    torch.cuda.synchronize()
+    launches_per_step = ctx.launches - launches0
+
+    # ---- timed region: inputs resident in HBM (180 MB of input > 126 MB L2)
+    pipe.set_timing(a.steps)
+    clocks = Clocks(local) if rank == 0 else None
+    time.sleep(0.3 if clocks else 0)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(a.steps):
+        pipe.run_device(*args)
+    ev1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop() if clocks else None
+    stages = pipe.stage_times()
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / a.steps
+    value = (n * world) / (ms_step / 1e3) / 1e6
+
+    # result sizes (for the algorithmic bytes)
+    import ctypes
+    from rvpoint_b200 import _lib as L
+    vo_h, so_h = pipe.frame_offsets()
+    n_vox, n_sor = int(vo_h[-1]), int(so_h[-1])
+
+    # ---- e2e: host buffers through the C entry point, copies inside
+    e2e = None
+    h2d = d2h = 0
+    if rank == 0 or world > 1:
+        pin = lambda arr: torch.from_numpy(arr).pin_memory()  # noqa: E731
+        hx, hy, hz = pin(batch.x), pin(batch.y), pin(batch.z)
+        ho = pin(batch.offsets)
+        out_vox = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+        out_sor = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+        out_vo = torch.empty(nf + 1, dtype=torch.int64).pin_memory()
+        out_so = torch.empty(nf + 1, dtype=torch.int64).pin_memory()
+        out_n = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3)]
+        out_m = torch.empty((nf, 4), dtype=torch.float32).pin_memory()
+        out_c = torch.empty(nf, dtype=torch.int32).pin_memory()
+        pipe.set_timing(0)
+        ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        P = lambda t_: ctypes.c_void_p(t_.data_ptr())  # noqa: E731
+
+        def run_host():
+            L.check(pipe.L.rvp_pipeline_run_host(pipe.h, P(hx), P(hy), P(hz), P(ho), nf,
+                                                 P(out_vox), P(out_vo), P(out_sor), P(out_so),
+                                                 P(out_n[0]), P(out_n[1]), P(out_n[2]),
+                                                 P(out_m), P(out_c)), ctx.h)
+        run_host()
+        e_steps = max(2, min(a.steps, 5))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(e_steps):
+            run_host()
+        e1.record()
+        torch.cuda.synchronize()
+        e_ms = e0.elapsed_time(e1) / e_steps
+        h2d = 12 * n + 8 * (nf + 1)
+        d2h = 8 * (nf + 1) * 2 + 12 * n_vox + 12 * n_sor + 12 * n_sor + 16 * nf + 4 * nf
+        e_t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
+        e2e = {"value": (n * world) / (float(e_t.item()) / 1e3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": float(e_t.item()), "steps": e_steps}
+
+    if world > 1:
+        dist.barrier()
+    if rank != 0:
+        dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant single-kernel stage
+    single = ["sor_knn", "normals_knn", "normals", "ransac"]
+    dom = max(single, key=lambda s_: stages[s_])
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peaks = json.load(open(peaks_path))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    alg = stage_bytes(dom, n, n_vox, n_sor, nf)
+    achieved = alg / (stages[dom] / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(dom)
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "kernel": STAGE_KERNEL[dom],
+            "stage": dom, "peak_source": peak_src,
+            "algorithmic_bytes_per_launch": alg, "launch_ms": stages[dom]}
+
+    cpu = cpu_baseline(batch, a.cpu_budget_s) if world == 1 else None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames_per_gpu": nf, "points_per_gpu": n,
+                       "voxel_points": n_vox, "sor_points": n_sor, "leaf": LEAF,
+                       "sor_k": SOR_K, "normal_k": NORMAL_K, "ransac_iters": R_ITERS,
+                       "ransac_thresh": R_THRESH, "parallelism": f"frames x{world}",
+                       "l2": "inputs larger than L2 (no flush)",
+                       "tuning": best},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_step * a.steps, "clocks": clk,
+            "stages_ms": {k: v for k, v in stages.items() if k != "runs"}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -205,6 +205,24 @@ typedef struct {
   const float *sor_mean_dists; /* per voxel point */
 } rvp_pipeline_outputs;
 RVP_API rvp_status rvp_pipeline_outputs_get(rvp_pipeline *p, rvp_pipeline_outputs *o);
+/* Host copies of the per-frame voxel and SOR offsets of the last run
+ * (n_frames+1 int64 each; either may be NULL). Synchronizes the stream. */
+RVP_API rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_offsets,
+                                              int64_t *sor_offsets);
+/* Tunables chosen by the autotuner, applied to the next run without
+ * reallocating: grid cell size (m), kNN block size (multiple of 32, 0 =
+ * default), queries per warp. A graph captured earlier keeps the values it
+ * was captured with. */
+RVP_API rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size,
+                                           int block_threads, int queries_per_warp);
+/* Stage timing with CUDA events on the context's stream: the next max_runs
+ * runs record 8 events each (stage boundaries: voxel, grid build, SOR kNN,
+ * SOR statistics, normals kNN, normals, RANSAC). rvp_pipeline_stage_times
+ * synchronizes and returns the mean ms per stage over the recorded runs
+ * (ms[7]), then resets. max_runs = 0 turns timing off. */
+RVP_API rvp_status rvp_pipeline_set_timing(rvp_pipeline *p, int max_runs);
+RVP_API rvp_status rvp_pipeline_stage_times(rvp_pipeline *p, float *ms, int n_stages,
+                                            int *runs);
 /* Host entry: copies host frames in, runs, copies the per-frame results out
  * (any output pointer may be NULL). Output arrays are sized by max_points /
  * n_frames; *_offsets are n_frames+1 entries. */

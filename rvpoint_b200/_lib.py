@@ -85,6 +85,10 @@ SIGNATURES = {
     "rvp_pipeline_run_device": (I, [P, P, P, P, P, I, SZ]),
     "rvp_pipeline_outputs_get": (I, [P, C.POINTER(PipelineOutputs)]),
     "rvp_pipeline_run_host": (I, [P, P, P, P, P, I, P, P, P, P, P, P, P, P, P]),
+    "rvp_pipeline_set_timing": (I, [P, I]),
+    "rvp_pipeline_set_tuning": (I, [P, F, I, I]),
+    "rvp_pipeline_frame_offsets": (I, [P, P, P]),
+    "rvp_pipeline_stage_times": (I, [P, C.POINTER(F), I, C.POINTER(I)]),
 }
 
 _lib = None

@@ -476,12 +476,42 @@ class Pipeline:
         self.h = h
         self.max_points = max_points
         self.max_frames = max_frames
+        self.last_frames = 0
 
     def run_device(self, x, y, z, offsets_dev, n_frames: int, n_points: int) -> None:
         """x, y, z, offsets: CUDA tensors; results stay on the device."""
         self.ctx.use_torch_stream()
+        self.last_frames = int(n_frames)
         check(self.L.rvp_pipeline_run_device(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(offsets_dev),
                                              int(n_frames), int(n_points)), self.ctx.h)
+
+    STAGES = ("voxel", "grid_build", "sor_knn", "sor_filter", "normals_knn", "normals",
+              "ransac")
+
+    def set_tuning(self, cell_size: float, block_threads: int = 0,
+                   queries_per_warp: int = 0) -> None:
+        check(self.L.rvp_pipeline_set_tuning(self.h, float(cell_size), int(block_threads),
+                                             int(queries_per_warp)), self.ctx.h)
+        self.cfg.cell_size = cell_size
+        self.cfg.block_threads = block_threads
+        self.cfg.queries_per_warp = queries_per_warp
+
+    def frame_offsets(self, n_frames: Optional[int] = None):
+        """(voxel_offsets, sor_offsets) of the last run, as host int64 arrays."""
+        nf = n_frames if n_frames is not None else self.last_frames
+        vo = np.empty(nf + 1, np.int64)
+        so = np.empty(nf + 1, np.int64)
+        check(self.L.rvp_pipeline_frame_offsets(self.h, _ptr(vo), _ptr(so)), self.ctx.h)
+        return vo, so
+
+    def set_timing(self, max_runs: int) -> None:
+        check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)
+
+    def stage_times(self) -> dict:
+        ms = (C.c_float * 7)()
+        runs = C.c_int(0)
+        check(self.L.rvp_pipeline_stage_times(self.h, ms, 7, C.byref(runs)), self.ctx.h)
+        return {"runs": runs.value, **{s: float(ms[i]) for i, s in enumerate(self.STAGES)}}
 
     def outputs(self) -> _lib.PipelineOutputs:
         o = _lib.PipelineOutputs()
@@ -494,6 +524,7 @@ class Pipeline:
         x, y, z = _f32(batch.x), _f32(batch.y), _f32(batch.z)
         offs = np.ascontiguousarray(batch.offsets, dtype=np.int64)
         nf = int(offs.shape[0] - 1)
+        self.last_frames = nf
         n = int(offs[-1])
         vox = np.empty((max(n, 1), 3), np.float32)
         vo = np.empty(nf + 1, np.int64)

@@ -1,0 +1,75 @@
+"""Autotuner for the batched pipeline.
+
+Chooses the neighbour-grid cell size, the kNN block shape and the queries
+per warp by timing candidate settings on the caller's own device-resident
+batch (CUDA events on the pipeline's stream, best of a few runs each). The
+choice is cached per workload signature so later runs reuse it.
+"""
+from __future__ import annotations
+
+import json
+import os
+from typing import Dict, Iterable, Optional, Tuple
+
+_CACHE: Dict[str, dict] = {}
+
+
+def signature(n_points: int, n_frames: int, cfg) -> str:
+    bucket = 1 << max(0, int(n_points).bit_length() - 3)  # ~12% size buckets
+    return (f"n{n_points // bucket * bucket}_f{n_frames}_leaf{cfg.leaf_size:.4g}_"
+            f"sk{cfg.sor_k}_nk{cfg.normal_k}")
+
+
+def _time_run(pipe, args, reps: int) -> float:
+    import torch
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        s.record()
+        pipe.run_device(*args)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    return best
+
+
+def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
+         cells: Optional[Iterable[float]] = None,
+         blocks: Iterable[int] = (128, 256),
+         qpws: Iterable[int] = (1,), reps: int = 2,
+         cache_file: Optional[str] = None, verbose: bool = False) -> Tuple[dict, list]:
+    """Returns (best setting, all trials) and applies the best to `pipe`."""
+    sig = signature(n_points, n_frames, pipe.cfg)
+    if cache_file and os.path.exists(cache_file) and not _CACHE:
+        try:
+            _CACHE.update(json.load(open(cache_file)))
+        except Exception:
+            pass
+    if sig in _CACHE:
+        b = _CACHE[sig]
+        pipe.set_tuning(b["cell"], b["block"], b["qpw"])
+        return b, []
+    leaf = pipe.cfg.leaf_size
+    cells = list(cells) if cells is not None else [leaf * m for m in (1.5, 2.0, 2.5, 3.0, 4.0)]
+    args = (x, y, z, offsets, n_frames, n_points)
+    trials = []
+    for c in cells:
+        for b in blocks:
+            for q in qpws:
+                pipe.set_tuning(c, b, q)
+                pipe.run_device(*args)  # warm
+                t = _time_run(pipe, args, reps)
+                trials.append({"cell": c, "block": b, "qpw": q, "ms": t})
+                if verbose:
+                    print(f"[autotune] cell={c:.3f} block={b} qpw={q}: {t:.3f} ms", flush=True)
+    best = min(trials, key=lambda r: r["ms"])
+    pipe.set_tuning(best["cell"], best["block"], best["qpw"])
+    _CACHE[sig] = best
+    if cache_file:
+        try:
+            json.dump(_CACHE, open(cache_file, "w"), indent=1)
+        except Exception:
+            pass
+    return best, trials

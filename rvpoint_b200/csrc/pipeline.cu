@@ -39,6 +39,14 @@ struct rvp_pipeline {
   rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
   int n_frames_last = 0;
+  // stage timing: a ring of event sets, one set per run
+  static constexpr int kStages = 7;
+  std::vector<cudaEvent_t> events;  // runs_cap * (kStages + 1)
+  int runs_cap = 0, runs_recorded = 0;
+  void mark(int stage) {
+    if (runs_cap == 0 || runs_recorded >= runs_cap) return;
+    cudaEventRecord(events[(size_t)runs_recorded * (kStages + 1) + stage], ctx->stream);
+  }
 };
 
 namespace {
@@ -161,6 +169,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
+  for (auto e : p->events) cudaEventDestroy(e);
   delete p;
   return RVP_OK;
 }
@@ -185,11 +194,13 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     int64_t *sor_offs = p->sor_offs.as<int64_t>();
     const u64 *n_sor = reinterpret_cast<const u64 *>(sor_offs + n_frames);
 
+    p->mark(0);
     // 1) voxel grid
     const float inv_leaf = 1.0f / c.leaf_size;
     rvp::voxel_grid_run(ctx, p->vw, x, y, z, offs, n_frames, N, nullptr, inv_leaf,
                         p->vox_aos.as<float>(), vox_offs, nullptr, nullptr, p->vox_x.as<float>(),
                         p->vox_y.as<float>(), p->vox_z.as<float>());
+    p->mark(1);
     // 2) grid over the voxel points of every frame
     rvp::grid_build(ctx, p->grid, p->vox_x.as<float>(), p->vox_y.as<float>(),
                     p->vox_z.as<float>(), vox_offs, n_frames, N, p->cell, rvp::KEY_DENSE, 0, 0,
@@ -198,12 +209,14 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                                                                  p->vox_frame.as<int32_t>());
     RVP_LAUNCH_CHECK(ctx);
     const rvp::GridView gv = p->grid.view(rvp::KEY_DENSE, 0, 0);
+    p->mark(2);
     // 3) SOR: exact k+1 nearest, mean distance, per-frame statistics
     const int ks = c.sor_k + 1;
     rvp::QuerySet qv{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N, n_vox,
                      p->vox_frame.as<int32_t>(), nullptr};
     rvp::grid_knn(ctx, gv, qv, ks, 0.0f, p->knn_pairs.as<u64>(), p->knn_counts.as<int32_t>(),
                   c.queries_per_warp, c.block_threads);
+    p->mark(3);
     rvp::sor_mean_from_knn(ctx, p->knn_pairs.as<u64>(), ks, p->knn_counts.as<int32_t>(), N, n_vox,
                            p->mean.as<float>(), 0.0f, false);
     rvp::sor_filter_frames(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
@@ -211,6 +224,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                            p->keep.as<uint8_t>(), p->sor_aos.as<float>(), sor_offs, nullptr,
                            p->sor_tmp.ptr, p->sor_x.as<float>(), p->sor_y.as<float>(),
                            p->sor_z.as<float>(), p->sor_src.as<u32>());
+    p->mark(4);
     // 4) normals: k+1 nearest kept points of every kept point
     k_mark_removed<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(
         p->grid.b_pts.as<float4>(), p->keep.as<uint8_t>(), n_vox, N);
@@ -223,11 +237,13 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                      p->sor_frame.as<int32_t>(), nullptr};
     rvp::grid_knn(ctx, gv, qs, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(),
                   c.queries_per_warp, c.block_threads);
+    p->mark(5);
     rvp::normals_from_lists(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
                             p->nrm_pairs.as<u64>(), nullptr, p->nrm_counts.as<int32_t>(), kn, N,
                             n_sor, true, c.eigen_iters, c.vp_x, c.vp_y, c.vp_z,
                             p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(),
                             p->nx.as<float>(), p->ny.as<float>(), p->nz.as<float>());
+    p->mark(6);
     // 5) RANSAC per frame on the kept points
     double pc = (double)c.ransac_prob;
     pc = pc < 0.5 ? 0.5 : (pc > 0.9999 ? 0.9999 : pc);
@@ -235,6 +251,70 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     rvp::ransac_frames(ctx, p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(),
                        sor_offs, n_frames, p->r_rand.as<int>(), prm, p->r_model.as<float>(),
                        p->r_best.as<int32_t>(), p->r_iters.as<int32_t>(), nullptr, false);
+    p->mark(7);
+    if (p->runs_cap > 0 && p->runs_recorded < p->runs_cap) p->runs_recorded++;
+  });
+}
+
+rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_offsets,
+                                      int64_t *sor_offsets) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  return guard(p->ctx, [&] {
+    const size_t b = ((size_t)p->n_frames_last + 1) * 8;
+    if (voxel_offsets)
+      RVP_CUDA_TRY(cudaMemcpyAsync(voxel_offsets, p->vox_offs.ptr, b, cudaMemcpyDeviceToHost,
+                                   p->ctx->stream));
+    if (sor_offsets)
+      RVP_CUDA_TRY(cudaMemcpyAsync(sor_offsets, p->sor_offs.ptr, b, cudaMemcpyDeviceToHost,
+                                   p->ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
+  });
+}
+
+rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size, int block_threads,
+                                   int queries_per_warp) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  if (!(cell_size > 0.0f)) return RVP_ERR_INVALID_ARG;
+  if (block_threads < 0 || block_threads > 1024 || (block_threads % 32) != 0)
+    return RVP_ERR_INVALID_ARG;
+  p->cell = cell_size;
+  p->cfg.cell_size = cell_size;
+  p->cfg.block_threads = block_threads;
+  p->cfg.queries_per_warp = queries_per_warp;
+  return RVP_OK;
+}
+
+rvp_status rvp_pipeline_set_timing(rvp_pipeline *p, int max_runs) {
+  if (!p || max_runs < 0) return RVP_ERR_INVALID_ARG;
+  return guard(p->ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    for (auto e : p->events) cudaEventDestroy(e);
+    p->events.clear();
+    p->runs_cap = 0;
+    p->runs_recorded = 0;
+    p->events.resize((size_t)max_runs * (rvp_pipeline::kStages + 1));
+    for (auto &e : p->events) RVP_CUDA_TRY(cudaEventCreate(&e));
+    p->runs_cap = max_runs;
+  });
+}
+
+rvp_status rvp_pipeline_stage_times(rvp_pipeline *p, float *ms, int n_stages, int *runs) {
+  if (!p || !ms || n_stages < rvp_pipeline::kStages) return RVP_ERR_INVALID_ARG;
+  return guard(p->ctx, [&] {
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
+    for (int s = 0; s < rvp_pipeline::kStages; ++s) ms[s] = 0.0f;
+    const int R = p->runs_recorded;
+    for (int r = 0; r < R; ++r)
+      for (int s = 0; s < rvp_pipeline::kStages; ++s) {
+        float t = 0.0f;
+        RVP_CUDA_TRY(cudaEventElapsedTime(&t, p->events[(size_t)r * (rvp_pipeline::kStages + 1) + s],
+                                          p->events[(size_t)r * (rvp_pipeline::kStages + 1) + s + 1]));
+        ms[s] += t;
+      }
+    if (R > 0)
+      for (int s = 0; s < rvp_pipeline::kStages; ++s) ms[s] /= (float)R;
+    if (runs) *runs = R;
+    p->runs_recorded = 0;
   });
 }
 
