@@ -205,6 +205,18 @@ typedef struct {
   const float *sor_mean_dists; /* per voxel point */
 } rvp_pipeline_outputs;
 RVP_API rvp_status rvp_pipeline_outputs_get(rvp_pipeline *p, rvp_pipeline_outputs *o);
+/* Re-size the neighbour grid's bucket table to the bucket count of the last
+ * run (with 2x headroom and load <= 0.4) so it stays resident in L2. Call
+ * after a first run, before capturing a graph. */
+RVP_API rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p);
+/* RVP_ERR_CAPACITY if the last run's bucket table overflowed (results of
+ * that run are then incomplete); synchronizes the stream. */
+RVP_API rvp_status rvp_pipeline_check(rvp_pipeline *p);
+/* Diagnostics: enable != 0 makes the kNN kernels count which search path
+ * settled each query (out16[0..7] SOR, [8..15] normals: fine ring, fine
+ * tight window, coarse ring, coarse tight window, whole frame, bounded).
+ * Reads (if out16) and clears the counters. */
+RVP_API rvp_status rvp_pipeline_knn_stats(rvp_pipeline *p, int enable, uint32_t *out16);
 /* Host copies of the per-frame voxel and SOR offsets of the last run
  * (n_frames+1 int64 each; either may be NULL). Synchronizes the stream. */
 RVP_API rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_offsets,

@@ -88,6 +88,9 @@ SIGNATURES = {
     "rvp_pipeline_set_timing": (I, [P, I]),
     "rvp_pipeline_set_tuning": (I, [P, F, I, I]),
     "rvp_pipeline_frame_offsets": (I, [P, P, P]),
+    "rvp_pipeline_fit_tables": (I, [P]),
+    "rvp_pipeline_check": (I, [P]),
+    "rvp_pipeline_knn_stats": (I, [P, I, P]),
     "rvp_pipeline_stage_times": (I, [P, C.POINTER(F), I, C.POINTER(I)]),
 }
 

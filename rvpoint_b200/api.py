@@ -504,6 +504,20 @@ class Pipeline:
         check(self.L.rvp_pipeline_frame_offsets(self.h, _ptr(vo), _ptr(so)), self.ctx.h)
         return vo, so
 
+    def fit_tables(self) -> None:
+        check(self.L.rvp_pipeline_fit_tables(self.h), self.ctx.h)
+
+    def check(self) -> None:
+        check(self.L.rvp_pipeline_check(self.h), self.ctx.h)
+
+    PATHS = ("fine_ring", "fine_tight", "coarse_ring", "coarse_tight", "whole_frame", "bounded")
+
+    def knn_stats(self, enable: bool = True) -> dict:
+        out = np.zeros(16, np.uint32)
+        check(self.L.rvp_pipeline_knn_stats(self.h, int(enable), _ptr(out)), self.ctx.h)
+        return {"sor": dict(zip(self.PATHS, map(int, out[:6]))),
+                "normals": dict(zip(self.PATHS, map(int, out[8:14])))}
+
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)
 

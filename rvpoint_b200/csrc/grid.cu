@@ -10,15 +10,17 @@
 //  * KEY_REF_HASH: the reference's hashCell ix + iy*p1 + iz*p2
 //    (spatial_hashing.h:43-45). Buckets are then exactly the reference's
 //    grid_ entries, collisions included.
-//  * KEY_DENSE: per-frame dense cell index offset by the frame's key base,
-//    so many frames share one sort and one table.
+//  * KEY_DENSE: per-frame dense keys for many frames in one sort and one
+//    table. Keys are hierarchical -- coarse cell (4 x 4 x 4 fine cells)
+//    times 64 plus the fine cell inside it -- so both fine and coarse cells
+//    are contiguous runs of the sorted points; the table holds both levels.
 //
 // Queries: one warp per query. Lanes look up up to 32 window cells at once,
 // a warp scan of bucket sizes flattens the window into one candidate stream,
 // and lanes walk it 32 candidates at a time (contiguous float4 loads inside a
-// bucket). The window is the tight cell range of [q - r, q + r] computed
-// with a monotone, conservative bound, which provably contains every point
-// with d2 <= r2 (so the result equals the reference's larger
+// bucket). A radius window is the tight cell range of [q - r, q + r]
+// computed with a monotone, conservative bound, which provably contains
+// every point with d2 <= r2 (so the result equals the reference's larger
 // ceil(r/cell)+1 window whenever the hash has no collisions; with
 // collisions the reference's own window is scanned instead).
 #include <math.h>
@@ -28,6 +30,7 @@
 namespace rvp {
 
 namespace {
+
 inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
 __device__ __forceinline__ int frame_of_index(const int64_t *offs, int n_frames, size_t i) {
@@ -42,7 +45,7 @@ __device__ __forceinline__ int frame_of_index(const int64_t *offs, int n_frames,
 // ---------------------------------------------------------------------------
 // bbox per frame
 // ---------------------------------------------------------------------------
-__global__ void k_bbox_init(GridFrame *fr, float *bb, int n_frames) {
+__global__ void k_bbox_init(float *bb, int n_frames) {
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n_frames; f += gridDim.x * blockDim.x) {
     bb[6 * f + 0] = bb[6 * f + 1] = bb[6 * f + 2] = INFINITY;
     bb[6 * f + 3] = bb[6 * f + 4] = bb[6 * f + 5] = -INFINITY;
@@ -110,9 +113,11 @@ __global__ void k_grid_params(GridFrame *fr, const float *bb, int n_frames, floa
       g.gy = (int)ceilf(fdiv(fsub(max_y, g.min_y), cell)) + 1;
       g.gz = (int)ceilf(fdiv(fsub(max_z, g.min_z), cell)) + 1;
     }
-    g.pad = 0;
+    g.gcx = (g.gx + 3) >> 2;
+    g.gcy = (g.gy + 3) >> 2;
+    g.gcz = (g.gz + 3) >> 2;
     g.key_base = base;
-    base += (u64)g.gx * (u64)g.gy * (u64)g.gz;
+    base += (u64)g.gcx * (u64)g.gcy * (u64)g.gcz * 64ull;
     fr[f] = g;
   }
 }
@@ -128,13 +133,19 @@ __device__ __forceinline__ int cell_axis_clamped(float v, float mn, float cell, 
   return (int)t;
 }
 
-__device__ __forceinline__ u64 key_of_cell(const GridView &g, const GridFrame &F, int cx, int cy,
-                                           int cz) {
+__device__ __forceinline__ u64 fine_key(const GridView &g, const GridFrame &F, int cx, int cy,
+                                        int cz) {
   if (g.mode == KEY_REF_HASH) {
     const long long h = (long long)cx + (long long)cy * g.p1 + (long long)cz * g.p2;
     return (u64)h ^ 0x8000000000000000ull;
   }
-  return F.key_base + (u64)cx + (u64)F.gx * ((u64)cy + (u64)F.gy * (u64)cz);
+  const u64 c = ((u64)(cz >> 2) * (u64)F.gcy + (u64)(cy >> 2)) * (u64)F.gcx + (u64)(cx >> 2);
+  return F.key_base + (c << 6) + (u64)(((cz & 3) << 4) | ((cy & 3) << 2) | (cx & 3));
+}
+
+__device__ __forceinline__ u64 coarse_key(const GridFrame &F, int X, int Y, int Z) {
+  return kCoarseKeyBit |
+         ((F.key_base >> 6) + ((u64)Z * (u64)F.gcy + (u64)Y) * (u64)F.gcx + (u64)X);
 }
 
 __global__ void k_cell_keys(const float *__restrict__ x, const float *__restrict__ y,
@@ -151,22 +162,30 @@ __global__ void k_cell_keys(const float *__restrict__ x, const float *__restrict
     const int cx = cell_axis(x[i], F.min_x, F.cell);
     const int cy = cell_axis(y[i], F.min_y, F.cell);
     const int cz = cell_axis(z[i], F.min_z, F.cell);
-    keys[i] = key_of_cell(gv, F, cx, cy, cz);
+    keys[i] = fine_key(gv, F, cx, cy, cz);
     vals[i] = (u32)i;
   }
 }
 
-__global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, u32 *heads) {
+// heads of fine buckets (key changes) and, in dense mode, of coarse buckets
+// (key >> 6 changes)
+__global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int mode, u32 *heads,
+                        u32 *cheads) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    heads[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const u64 k = keys[i];
+    const u64 p = i ? keys[i - 1] : 0;
+    heads[i] = (i == 0 || k != p) ? 1u : 0u;
+    if (mode == KEY_DENSE) cheads[i] = (i == 0 || (k >> 6) != (p >> 6)) ? 1u : 0u;
+  }
 }
 
 __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__ y,
                           const float *__restrict__ z, const u32 *vals, const u32 *heads,
-                          const u64 *bucket_of, size_t n_max, const u64 *n_dev, float4 *pts,
-                          u32 *bstart, const GridFrame *frames, int mode, int *collision) {
+                          const u64 *bucket_of, const u32 *cheads, const u64 *cbucket_of,
+                          size_t n_max, const u64 *n_dev, float4 *pts, u32 *bstart, u32 *cstart,
+                          const GridFrame *frames, int mode, int *collision) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -184,30 +203,49 @@ __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__
           cell_axis(pz, F.min_z, F.cell) != cell_axis(z[u], F.min_z, F.cell))
         *collision = 1;
     }
+    if (mode == KEY_DENSE && cheads[i]) cstart[cbucket_of[i]] = (u32)i;
   }
 }
 
+__device__ __forceinline__ void table_put(ulonglong2 *table, u64 mask, u64 key, u64 ent,
+                                          int *overflow) {
+  u64 slot = mix64(key) & mask;
+  for (u64 probe = 0; probe <= mask; ++probe) {
+    const u64 prev = atomicCAS(&table[slot].x, kEmptyKey, key);
+    if (prev == kEmptyKey || prev == key) {
+      table[slot].y = ent;
+      return;
+    }
+    slot = (slot + 1) & mask;
+  }
+  *overflow = 1;
+}
+
 // one thread per bucket: {key, start | count << 32} into the open-addressing
-// table (linear probing, load factor <= 2/3).
-__global__ void k_insert(const u64 *keys, const u32 *bstart, const u64 *bucket_of, size_t n_max,
-                         const u64 *n_dev, ulonglong2 *table, u64 mask, u64 *nbuckets) {
+// table (linear probing)
+__global__ void k_insert(const u64 *keys, const u32 *bstart, const u64 *bucket_of,
+                         const u32 *cstart, const u64 *cbucket_of, size_t n_max,
+                         const u64 *n_dev, int mode, ulonglong2 *table, u64 mask, u64 *nbuckets,
+                         int *overflow) {
   const size_t n = n_dev ? *n_dev : n_max;
   const u64 nb = bucket_of[n];
-  if (blockIdx.x == 0 && threadIdx.x == 0) *nbuckets = nb;
-  for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nb;
+  const u64 ncb = mode == KEY_DENSE ? cbucket_of[n] : 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    nbuckets[0] = nb;
+    nbuckets[1] = ncb;
+  }
+  for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nb + ncb;
        b += (u64)gridDim.x * blockDim.x) {
-    const u32 s = bstart[b];
-    const u32 e = (b + 1 < nb) ? bstart[b + 1] : (u32)n;
-    const u64 key = keys[s];
-    const u64 ent = (u64)s | ((u64)(e - s) << 32);
-    u64 slot = mix64(key) & mask;
-    for (u64 probe = 0; probe <= mask; ++probe) {
-      const u64 prev = atomicCAS(&table[slot].x, kEmptyKey, key);
-      if (prev == kEmptyKey || prev == key) {
-        table[slot].y = ent;
-        break;
-      }
-      slot = (slot + 1) & mask;
+    if (b < nb) {
+      const u32 s = bstart[b];
+      const u32 e = (b + 1 < nb) ? bstart[b + 1] : (u32)n;
+      table_put(table, mask, keys[s], (u64)s | ((u64)(e - s) << 32), overflow);
+    } else {
+      const u64 c = b - nb;
+      const u32 s = cstart[c];
+      const u32 e = (c + 1 < ncb) ? cstart[c + 1] : (u32)n;
+      table_put(table, mask, kCoarseKeyBit | (keys[s] >> 6), (u64)s | ((u64)(e - s) << 32),
+                overflow);
     }
   }
 }
@@ -226,28 +264,42 @@ static u64 next_pow2(u64 v) {
 void Grid::reserve(size_t n, int nf) {
   if (n < 1) n = 1;
   if (nf < 1) nf = 1;
-  if (n <= n_max && nf <= n_frames_max) return;
-  n_max = n > n_max ? n : n_max;
-  n_frames_max = nf > n_frames_max ? nf : n_frames_max;
-  table_cap = (size_t)next_pow2((u64)(n_max + n_max / 2 + 1024));
-  b_keys.reserve(n_max * 8);
-  b_vals.reserve(n_max * 4);
-  b_pts.reserve(n_max * 16);
-  b_table.reserve(table_cap * 16);
-  b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
-  b_begin.reserve(al((n_frames_max + 1) * 8));
-  b_sort.reserve(sort_temp_bytes(n_max) + al(n_max * 4) + al((n_max + 1) * 8) + al(n_max * 4) +
-                 scan_temp_bytes(n_max));
-  b_misc.reserve(256);
-  d_n = b_misc.as<u64>();
-  d_nbuckets = d_n + 1;
-  d_collision = reinterpret_cast<int *>(d_n + 2);
+  if (n > n_max || nf > n_frames_max) {
+    n_max = n > n_max ? n : n_max;
+    n_frames_max = nf > n_frames_max ? nf : n_frames_max;
+    b_keys.reserve(n_max * 8);
+    b_vals.reserve(n_max * 4);
+    b_pts.reserve(n_max * 16);
+    b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
+    b_begin.reserve(al((n_frames_max + 1) * 8));
+    b_sort.reserve(sort_temp_bytes(n_max) + 2 * al(n_max * 4) + 2 * al((n_max + 1) * 8) +
+                   2 * al(n_max * 4) + scan_temp_bytes(n_max));
+    b_misc.reserve(256);
+    d_n = b_misc.as<u64>();
+    d_nbuckets = d_n + 1;
+    d_collision = reinterpret_cast<int *>(d_n + 3);
+    d_overflow = d_collision + 1;
+  }
+  // fine + coarse buckets never exceed 2 n; without a measured count the
+  // table is sized for that worst case
+  const size_t want = table_cap_req ? table_cap_req
+                                    : (size_t)next_pow2((u64)(2 * n_max + n_max / 2 + 1024));
+  if (want != table_cap) {
+    table_cap = want;
+    b_table.release();
+    b_table.reserve(table_cap * 16);
+  }
+}
+
+void Grid::fit_table(size_t buckets) {
+  table_cap_req = (size_t)next_pow2((u64)(buckets * 5 / 2 + 1024));
+  reserve(n_max, n_frames_max);
 }
 
 void Grid::release() {
   b_keys.release(); b_vals.release(); b_pts.release(); b_table.release();
   b_frames.release(); b_begin.release(); b_sort.release(); b_misc.release();
-  n_max = 0; n_frames_max = 0;
+  n_max = 0; n_frames_max = 0; table_cap = 0;
 }
 
 GridView Grid::view(int mode, long long p1, long long p2) const {
@@ -279,35 +331,39 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   sort_temp_carve(t, sp, g.n_max);
   sp += sort_temp_bytes(g.n_max);
   u32 *heads = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
+  u32 *cheads = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
   u64 *bucket_of = reinterpret_cast<u64 *>(sp); sp += al((g.n_max + 1) * 8);
+  u64 *cbucket_of = reinterpret_cast<u64 *>(sp); sp += al((g.n_max + 1) * 8);
   u32 *bstart = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
+  u32 *cstart = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
   void *scan_tmp = sp;
 
   const int sms = ctx->num_sms;
-  k_bbox_init<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(frames, bb, n_frames);
+  const unsigned gb = grid_for(n_max, 256, sms * 16);
+  k_bbox_init<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(bb, n_frames);
   RVP_LAUNCH_CHECK(ctx);
-  k_bbox<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, bb);
+  k_bbox<<<gb, 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, bb);
   RVP_LAUNCH_CHECK(ctx);
   k_grid_params<<<1, 32, 0, st>>>(frames, bb, n_frames, cell);
   RVP_LAUNCH_CHECK(ctx);
-  k_cell_keys<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(
-      x, y, z, offs, n_frames, n_max, n_dev, frames, mode, p1, p2, g.b_keys.as<u64>(),
-      g.b_vals.as<u32>());
+  k_cell_keys<<<gb, 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, frames, mode, p1, p2,
+                                  g.b_keys.as<u64>(), g.b_vals.as<u32>());
   RVP_LAUNCH_CHECK(ctx);
   radix_sort_pairs(ctx, g.b_keys.as<u64>(), g.b_vals.as<u32>(), n_max, n_dev, t);
-  k_heads<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(g.b_keys.as<u64>(), n_max, n_dev, heads);
+  k_heads<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), n_max, n_dev, mode, heads, cheads);
   RVP_LAUNCH_CHECK(ctx);
   // bucket_of[i] = number of heads before i, i.e. the bucket id of a head
   exclusive_scan_u32_to_u64(ctx, heads, bucket_of, n_max, n_dev, scan_tmp);
+  if (mode == KEY_DENSE) exclusive_scan_u32_to_u64(ctx, cheads, cbucket_of, n_max, n_dev, scan_tmp);
   RVP_CUDA_TRY(cudaMemsetAsync(g.b_table.ptr, 0xFF, g.table_cap * 16, st));
-  RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 16, st));  // nbuckets + collision
-  k_reorder<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(
-      x, y, z, g.b_vals.as<u32>(), heads, bucket_of, n_max, n_dev, g.b_pts.as<float4>(), bstart,
-      frames, mode, g.d_collision);
+  RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 24, st));  // buckets, collision, overflow
+  k_reorder<<<gb, 256, 0, st>>>(x, y, z, g.b_vals.as<u32>(), heads, bucket_of, cheads, cbucket_of,
+                                n_max, n_dev, g.b_pts.as<float4>(), bstart, cstart, frames, mode,
+                                g.d_collision);
   RVP_LAUNCH_CHECK(ctx);
-  k_insert<<<grid_for(n_max, 256, sms * 16), 256, 0, st>>>(
-      g.b_keys.as<u64>(), bstart, bucket_of, n_max, n_dev, g.b_table.as<ulonglong2>(),
-      (u64)g.table_cap - 1, g.d_nbuckets);
+  k_insert<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), bstart, bucket_of, cstart, cbucket_of, n_max,
+                               n_dev, mode, g.b_table.as<ulonglong2>(), (u64)g.table_cap - 1,
+                               g.d_nbuckets, g.d_overflow);
   RVP_LAUNCH_CHECK(ctx);
 }
 
@@ -319,7 +375,8 @@ namespace {
 constexpr u32 kRemovedBit = 0x80000000u;
 
 struct Window {
-  int lo[3], hi[3];
+  int lo[3], hi[3];  // cells, inclusive, at `level`
+  int level;         // 0 fine, 1 coarse (dense mode only)
 };
 
 __device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u32 &count) {
@@ -337,14 +394,16 @@ __device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u
   return false;
 }
 
-// Tight window of all cells that can hold a point p with d2(p, q) <= rr,
-// rr = r*r. |p - q| <= r (1 + 3 * 2^-24) per axis for any such p; the bound
-// is padded to r (1 + 1e-6) and rounded outwards, and the cell function is
-// monotone, so the window is exact. Clamped to the frame's grid.
+// Tight window of all cells that can hold a point p with d2(p, q) <= r*r:
+// |p - q| <= r (1 + 3 * 2^-24) per axis for any such p; the bound is padded
+// to r (1 + 1e-6) and rounded outwards, and the cell function is monotone,
+// so the window is exact. Clamped to the frame's grid. Level 1 takes the
+// coarse cells (fine index >> 2) of the same range.
 __device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, float qy, float qz,
-                                               double r) {
+                                               double r, int level = 0) {
   const double rp = r * (1.0 + 1e-6) + 1e-30;
   Window w;
+  w.level = level;
   const float q[3] = {qx, qy, qz};
   const float mn[3] = {F.min_x, F.min_y, F.min_z};
   const int G[3] = {F.gx, F.gy, F.gz};
@@ -352,10 +411,12 @@ __device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, flo
   for (int a = 0; a < 3; ++a) {
     const float lo = __double2float_rd((double)q[a] - rp);
     const float hi = __double2float_ru((double)q[a] + rp);
-    w.lo[a] = cell_axis_clamped(lo, mn[a], F.cell, -1, G[a]);
-    w.hi[a] = cell_axis_clamped(hi, mn[a], F.cell, -1, G[a]);
-    w.lo[a] = max(w.lo[a], 0);
-    w.hi[a] = min(w.hi[a], G[a] - 1);
+    w.lo[a] = max(cell_axis_clamped(lo, mn[a], F.cell, -1, G[a]), 0);
+    w.hi[a] = min(cell_axis_clamped(hi, mn[a], F.cell, -1, G[a]), G[a] - 1);
+    if (level) {
+      w.lo[a] >>= 2;
+      w.hi[a] = w.hi[a] < 0 ? -1 : (w.hi[a] >> 2);
+    }
   }
   return w;
 }
@@ -366,6 +427,7 @@ __device__ __forceinline__ Window ref_window(const GridFrame &F, float qx, float
                                              float radius) {
   const int R = (int)ceilf(fdiv(radius, F.cell)) + 1;
   Window w;
+  w.level = 0;
   const int c[3] = {cell_axis(qx, F.min_x, F.cell), cell_axis(qy, F.min_y, F.cell),
                     cell_axis(qz, F.min_z, F.cell)};
 #pragma unroll
@@ -373,40 +435,50 @@ __device__ __forceinline__ Window ref_window(const GridFrame &F, float qx, float
   return w;
 }
 
-// Window of the query's own cell +- ring, clamped.
+// The query's own cell +- ring at `level`, clamped.
 __device__ __forceinline__ Window ring_window(const GridFrame &F, float qx, float qy, float qz,
-                                              int ring) {
+                                              int ring, int level = 0) {
   Window w;
+  w.level = level;
   const float q[3] = {qx, qy, qz};
   const float mn[3] = {F.min_x, F.min_y, F.min_z};
   const int G[3] = {F.gx, F.gy, F.gz};
+  const int GC[3] = {F.gcx, F.gcy, F.gcz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1);
+    int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1);
+    int top = G[a] - 1;
+    if (level) {
+      c >>= 2;
+      top = GC[a] - 1;
+    }
     w.lo[a] = max(c - ring, 0);
-    w.hi[a] = min(c + ring, G[a] - 1);
+    w.hi[a] = min(c + ring, top);
   }
   return w;
 }
 
-// Lower bound on the distance from q to any point outside window w (points
-// of other cells of this frame); +inf when w spans the whole grid.
+// Lower bound on the distance from q to any point of the frame outside w;
+// +inf when w spans the whole grid.
 __device__ __forceinline__ double coverage(const GridFrame &F, const Window &w, float qx, float qy,
                                            float qz) {
   const float q[3] = {qx, qy, qz};
   const float mn[3] = {F.min_x, F.min_y, F.min_z};
-  const int G[3] = {F.gx, F.gy, F.gz};
+  const int top[3] = {w.level ? F.gcx - 1 : F.gx - 1, w.level ? F.gcy - 1 : F.gy - 1,
+                      w.level ? F.gcz - 1 : F.gz - 1};
+  const double cs = w.level ? 4.0 * (double)F.cell : (double)F.cell;
   double cov = 1e300;
   const double u = 4.0 * 5.960464477539063e-08;  // 4 * 2^-24
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const double slack = u * (fabs((double)mn[a]) + (double)(w.hi[a] + 2) * F.cell + fabs((double)q[a])) + 1e-30;
+    const double slack =
+        u * (fabs((double)mn[a]) + (double)(w.hi[a] + 2) * cs + fabs((double)q[a])) + 1e-30;
     if (w.lo[a] > 0) {
-      const double face = (double)mn[a] + (double)w.lo[a] * (double)F.cell;
+      const double face = (double)mn[a] + (double)w.lo[a] * cs;
       cov = fmin(cov, (double)q[a] - face - slack);
     }
-    if (w.hi[a] < G[a] - 1) {
-      const double face = (double)mn[a] + (double)(w.hi[a] + 1) * (double)F.cell;
+    if (w.hi[a] < top[a]) {
+      const double face = (double)mn[a] + (double)(w.hi[a] + 1) * cs;
       cov = fmin(cov, face - (double)q[a] - slack);
     }
   }
@@ -448,7 +520,8 @@ __device__ __forceinline__ void for_each_candidate(const GridView &g, const Grid
       const int cx = w.lo[0] + (int)(j % ncx);
       const int cy = w.lo[1] + (int)((j / ncx) % ncy);
       const int cz = w.lo[2] + (int)(j / ((long long)ncx * ncy));
-      if (!lookup(g, key_of_cell(g, F, cx, cy, cz), start, count)) count = 0;
+      const u64 key = w.level ? coarse_key(F, cx, cy, cz) : fine_key(g, F, cx, cy, cz);
+      if (!lookup(g, key, start, count)) count = 0;
     }
     // flatten: inclusive scan of bucket sizes
     u32 incl = count;
@@ -678,7 +751,6 @@ __device__ __forceinline__ void knn_scan(const GridView &g, const GridFrame &F, 
                                          const Window &w, bool brute, float qx, float qy,
                                          float qz, int K, u64 bound, WarpList<P> &L,
                                          u32 &found) {
-  const int lane = threadIdx.x & 31;
   u64 thr = L.get(K - 1);
   for_each_candidate(g, F, f, w, brute, [&](float4 p, bool valid) {
     const u32 idx = __float_as_uint(p.w);
@@ -696,17 +768,22 @@ __device__ __forceinline__ void knn_scan(const GridView &g, const GridFrame &F, 
         thr = L.get(K - 1);
       }
     }
-    (void)lane;
   });
 }
 
+__device__ __forceinline__ u64 bound_of(float tau) { return pack_nbr(tau, 0x7FFFFFFF) | 0xFFFFFFFFull; }
+
+constexpr long long kMaxFineTight = 64;    // fine cells for a tight window
+constexpr long long kMaxCoarseTight = 512; // coarse cells for a tight window
+
 template <int P>
 __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K, float radius,
-                                                  u64 *out, int32_t *out_counts) {
+                                                  u64 *out, int32_t *out_counts, u32 *stats) {
   const size_t nq = q.n_dev ? *q.n_dev : q.n_max;
   const int lane = threadIdx.x & 31;
   const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
   const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const bool two_level = g.mode == KEY_DENSE;
   for (size_t wi = warp; wi < nq; wi += nwarps) {
     const u32 qi = query_index(q, wi);
     const int f = q.frame_of ? q.frame_of[qi] : 0;
@@ -715,37 +792,60 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
     WarpList<P> L;
     L.init();
     u32 found = 0;
+    int path = 5;
     if (radius > 0.0f) {
       const float r2 = fmul(radius, radius);
       const Window w = tight_window(F, qx, qy, qz, (double)radius);
-      knn_scan<P>(g, F, f, w, false, qx, qy, qz, K, pack_nbr(r2, 0x7FFFFFFF) | 0xFFFFFFFFull, L,
-                  found);
+      knn_scan<P>(g, F, f, w, false, qx, qy, qz, K, bound_of(r2), L, found);
     } else {
-      // 1) own cell +- 1
-      const Window w1 = ring_window(F, qx, qy, qz, 1);
+      // 1) fine ring: own cell +- 1
+      const Window w1 = ring_window(F, qx, qy, qz, 1, 0);
       knn_scan<P>(g, F, f, w1, false, qx, qy, qz, K, ~0ull - 1, L, found);
       bool done = false;
+      Window wr = w1;  // window whose candidates are in L
+      if (found < (u32)K && two_level) {
+        // 2) too few points nearby: coarse ring (12 fine cells wide)
+        wr = ring_window(F, qx, qy, qz, 1, 1);
+        L.init();
+        found = 0;
+        knn_scan<P>(g, F, f, wr, false, qx, qy, qz, K, ~0ull - 1, L, found);
+        path = 2;
+      } else {
+        path = 0;
+      }
       if (found >= (u32)K) {
         const float tau = nbr_d2(L.get(K - 1));
-        const double cov = coverage(F, w1, qx, qy, qz);
+        const double cov = coverage(F, wr, qx, qy, qz);
         if (cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5)) done = true;
         if (!done) {
-          // 2) every point with d2 <= tau lies in the tight window of
-          //    sqrt(tau), and there are >= K of them: exact.
-          const Window w2 = tight_window(F, qx, qy, qz, sqrt((double)tau));
-          if (window_cells(w2) <= 4096) {
+          // 3) every point with d2 <= tau lies in the tight window of
+          //    sqrt(tau) and there are >= K of them: exact. Scan it at the
+          //    level with the fewer cells.
+          const double rt = sqrt((double)tau);
+          const Window wf = tight_window(F, qx, qy, qz, rt, 0);
+          const long long cf = window_cells(wf);
+          Window wt = wf;
+          bool ok = cf <= kMaxFineTight;
+          path = 1;
+          if (!ok && two_level) {
+            wt = tight_window(F, qx, qy, qz, rt, 1);
+            ok = window_cells(wt) <= kMaxCoarseTight;
+            path = 3;
+          }
+          if (!ok && !two_level && cf <= 4096) ok = true;
+          if (ok) {
             L.init();
             found = 0;
-            knn_scan<P>(g, F, f, w2, false, qx, qy, qz, K,
-                        pack_nbr(tau, 0x7FFFFFFF) | 0xFFFFFFFFull, L, found);
+            knn_scan<P>(g, F, f, wt, false, qx, qy, qz, K, bound_of(tau), L, found);
             done = true;
           }
         }
       }
-      if (!done) {  // 3) whole frame
+      if (!done) {  // 4) whole frame
         L.init();
         found = 0;
         knn_scan<P>(g, F, f, w1, true, qx, qy, qz, K, ~0ull - 1, L, found);
+        path = 4;
       }
     }
     const u32 cnt = found < (u32)K ? found : (u32)K;
@@ -754,7 +854,10 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
       const int j = s * 32 + lane;
       if (j < (int)cnt) out[(size_t)qi * K + j] = L.e[s];
     }
-    if (lane == 0 && out_counts) out_counts[qi] = (int32_t)cnt;
+    if (lane == 0) {
+      if (out_counts) out_counts[qi] = (int32_t)cnt;
+      if (stats) atomicAdd(&stats[path], 1u);
+    }
   }
 }
 
@@ -792,14 +895,14 @@ void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs, const u
 }
 
 void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k, float radius,
-              u64 *out_pairs, int32_t *out_counts, int qpw, int block_threads) {
+              u64 *out_pairs, int32_t *out_counts, int qpw, int block_threads, u32 *stats) {
   (void)qpw;
   const int bt = block_threads > 0 ? block_threads : 256;
   const unsigned blocks = grid_for(q.n_max * 32, bt, ctx->num_sms * 32);
   if (k <= 32)
-    k_knn_warp<1><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts);
+    k_knn_warp<1><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts, stats);
   else
-    k_knn_warp<2><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts);
+    k_knn_warp<2><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts, stats);
   RVP_LAUNCH_CHECK(ctx);
 }
 

@@ -179,12 +179,17 @@ void exclusive_scan_u32_to_u64(rvp_context *ctx, const u32 *in, u64 *out,
 struct GridFrame {  // per-frame grid parameters (device)
   float min_x, min_y, min_z;
   float cell;
-  int gx, gy, gz;
-  int pad;
-  u64 key_base;  // mode 1: frame's first key; mode 0: unused
+  int gx, gy, gz;    // fine cells per axis
+  int gcx, gcy, gcz; // coarse cells (4 x 4 x 4 fine cells) per axis
+  u64 key_base;      // dense mode: frame's first key (a multiple of 64)
 };
 
 enum KeyMode { KEY_REF_HASH = 0, KEY_DENSE = 1 };
+
+// dense-mode keys: coarse cell (x fastest) * 64 + fine cell inside it, so a
+// coarse cell's points are one contiguous run of the sorted points too;
+// coarse buckets live in the same table under keys with bit 63 set.
+constexpr u64 kCoarseKeyBit = 0x8000000000000000ull;
 
 struct GridView {  // what the query kernels read
   const float4 *pts;       // cell-sorted {x,y,z,idx}
@@ -200,12 +205,16 @@ struct Grid {
   int n_frames_max = 0;
   size_t n_max = 0;
   size_t table_cap = 0;
+  size_t table_cap_req = 0;    // 0: sized from n_max
   DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc;
   u64 *d_n = nullptr;          // number of points (device)
-  u64 *d_nbuckets = nullptr;   // number of buckets (device)
+  u64 *d_nbuckets = nullptr;   // [0] fine buckets, [1] coarse buckets (device)
   int *d_collision = nullptr;  // mode 0: hash collision detected
+  int *d_overflow = nullptr;   // a bucket found no free table slot
   GridView view(int mode, long long p1, long long p2) const;
   void reserve(size_t n_max, int n_frames_max);
+  // shrink/grow the bucket table to hold `buckets` entries at load <= 1/2.5
+  void fit_table(size_t buckets);
   void release();
 };
 
@@ -238,9 +247,12 @@ void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs,
 // exact kNN (k <= 64) with ring expansion / brute force fallback. radius > 0
 // bounds the search. skip_flag: candidates whose idx has bit 31 set are
 // ignored (points removed by an earlier stage). out: nq * k packed pairs.
+// stats (optional, 8 counters): queries certified by the fine ring, by a
+// fine tight window, by the coarse ring, by a coarse tight window, by a
+// whole-frame scan, and the radius-bounded ones.
 void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
               float radius, u64 *out_pairs, int32_t *out_counts, int qpw,
-              int block_threads);
+              int block_threads, u32 *stats = nullptr);
 
 // ---------------------------------------------------------------------------
 // voxel grid (voxel.cu)

@@ -38,6 +38,8 @@ struct rvp_pipeline {
   rvp::DevBuf sor_aos, sor_x, sor_y, sor_z, sor_offs, sor_frame, sor_src;
   rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
+  rvp::DevBuf stats;  // 16 kNN path counters (diagnostics)
+  bool stats_on = false;
   int n_frames_last = 0;
   // stage timing: a ring of event sets, one set per run
   static constexpr int kStages = 7;
@@ -165,7 +167,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand};
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats};
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
@@ -214,8 +216,9 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     const int ks = c.sor_k + 1;
     rvp::QuerySet qv{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N, n_vox,
                      p->vox_frame.as<int32_t>(), nullptr};
+    u32 *st0 = p->stats_on ? p->stats.as<u32>() : nullptr;
     rvp::grid_knn(ctx, gv, qv, ks, 0.0f, p->knn_pairs.as<u64>(), p->knn_counts.as<int32_t>(),
-                  c.queries_per_warp, c.block_threads);
+                  c.queries_per_warp, c.block_threads, st0);
     p->mark(3);
     rvp::sor_mean_from_knn(ctx, p->knn_pairs.as<u64>(), ks, p->knn_counts.as<int32_t>(), N, n_vox,
                            p->mean.as<float>(), 0.0f, false);
@@ -236,7 +239,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     rvp::QuerySet qs{p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(), N, n_sor,
                      p->sor_frame.as<int32_t>(), nullptr};
     rvp::grid_knn(ctx, gv, qs, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(),
-                  c.queries_per_warp, c.block_threads);
+                  c.queries_per_warp, c.block_threads, st0 ? st0 + 8 : nullptr);
     p->mark(5);
     rvp::normals_from_lists(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
                             p->nrm_pairs.as<u64>(), nullptr, p->nrm_counts.as<int32_t>(), kn, N,
@@ -253,6 +256,51 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                        p->r_best.as<int32_t>(), p->r_iters.as<int32_t>(), nullptr, false);
     p->mark(7);
     if (p->runs_cap > 0 && p->runs_recorded < p->runs_cap) p->runs_recorded++;
+  });
+}
+
+rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  return guard(p->ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    u64 nb[2] = {0, 0};
+    RVP_CUDA_TRY(cudaMemcpyAsync(nb, p->grid.d_nbuckets, 16, cudaMemcpyDeviceToHost,
+                                 p->ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
+    // headroom for batches whose scenes occupy more cells than this one
+    p->grid.fit_table((size_t)((nb[0] + nb[1]) * 2));
+  });
+}
+
+rvp_status rvp_pipeline_check(rvp_pipeline *p) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  int flags[2] = {0, 0};
+  rvp_status s = guard(p->ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    RVP_CUDA_TRY(cudaMemcpyAsync(flags, p->grid.d_collision, 8, cudaMemcpyDeviceToHost,
+                                 p->ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
+  });
+  if (s != RVP_OK) return s;
+  if (flags[1]) {
+    p->ctx->last_error = "neighbour grid table overflow: refit the tables (rvp_pipeline_fit_tables)";
+    return RVP_ERR_CAPACITY;
+  }
+  return RVP_OK;
+}
+
+rvp_status rvp_pipeline_knn_stats(rvp_pipeline *p, int enable, uint32_t *out16) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  return guard(p->ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    p->stats.reserve(64);
+    if (out16) {
+      RVP_CUDA_TRY(cudaMemcpyAsync(out16, p->stats.ptr, 64, cudaMemcpyDeviceToHost,
+                                   p->ctx->stream));
+      RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
+    }
+    RVP_CUDA_TRY(cudaMemsetAsync(p->stats.ptr, 0, 64, p->ctx->stream));
+    p->stats_on = enable != 0;
   });
 }
 
