@@ -515,8 +515,8 @@ class Pipeline:
     def knn_stats(self, enable: bool = True) -> dict:
         out = np.zeros(16, np.uint32)
         check(self.L.rvp_pipeline_knn_stats(self.h, int(enable), _ptr(out)), self.ctx.h)
-        return {"sor": dict(zip(self.PATHS, map(int, out[:6]))),
-                "normals": dict(zip(self.PATHS, map(int, out[8:14])))}
+        return {"sor": dict(zip(self.PATHS, map(int, out[:6])), tile=int(out[7])),
+                "normals": dict(zip(self.PATHS, map(int, out[8:14])), tile=int(out[15]))}
 
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)

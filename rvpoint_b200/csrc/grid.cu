@@ -26,8 +26,10 @@
 #include <math.h>
 
 #include "internal.cuh"
+#include "grid_device.cuh"
 
 namespace rvp {
+using namespace gd;
 
 namespace {
 
@@ -120,32 +122,6 @@ __global__ void k_grid_params(GridFrame *fr, const float *bb, int n_frames, floa
     base += (u64)g.gcx * (u64)g.gcy * (u64)g.gcz * 64ull;
     fr[f] = g;
   }
-}
-
-// getCellIndices (spatial_hashing.h:47-52)
-__device__ __forceinline__ int cell_axis(float v, float mn, float cell) {
-  return (int)floorf(fdiv(fsub(v, mn), cell));
-}
-// Same, saturated to [lo, hi] before the int conversion (window bounds).
-__device__ __forceinline__ int cell_axis_clamped(float v, float mn, float cell, int lo, int hi) {
-  float t = floorf(fdiv(fsub(v, mn), cell));
-  t = fminf(fmaxf(t, (float)lo), (float)hi);
-  return (int)t;
-}
-
-__device__ __forceinline__ u64 fine_key(const GridView &g, const GridFrame &F, int cx, int cy,
-                                        int cz) {
-  if (g.mode == KEY_REF_HASH) {
-    const long long h = (long long)cx + (long long)cy * g.p1 + (long long)cz * g.p2;
-    return (u64)h ^ 0x8000000000000000ull;
-  }
-  const u64 c = ((u64)(cz >> 2) * (u64)F.gcy + (u64)(cy >> 2)) * (u64)F.gcx + (u64)(cx >> 2);
-  return F.key_base + (c << 6) + (u64)(((cz & 3) << 4) | ((cy & 3) << 2) | (cx & 3));
-}
-
-__device__ __forceinline__ u64 coarse_key(const GridFrame &F, int X, int Y, int Z) {
-  return kCoarseKeyBit |
-         ((F.key_base >> 6) + ((u64)Z * (u64)F.gcy + (u64)Y) * (u64)F.gcx + (u64)X);
 }
 
 __global__ void k_cell_keys(const float *__restrict__ x, const float *__restrict__ y,
@@ -250,6 +226,10 @@ __global__ void k_insert(const u64 *keys, const u32 *bstart, const u64 *bucket_o
   }
 }
 
+__global__ void k_set_count(u64 *dst, const u64 *src, u64 value) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = src ? *src : value;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -273,7 +253,8 @@ void Grid::reserve(size_t n, int nf) {
     b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
     b_begin.reserve(al((n_frames_max + 1) * 8));
     b_sort.reserve(sort_temp_bytes(n_max) + 2 * al(n_max * 4) + 2 * al((n_max + 1) * 8) +
-                   2 * al(n_max * 4) + scan_temp_bytes(n_max));
+                   al(n_max * 4) + scan_temp_bytes(n_max));
+    b_cstart.reserve(al(n_max * 4));
     b_misc.reserve(256);
     d_n = b_misc.as<u64>();
     d_nbuckets = d_n + 1;
@@ -299,6 +280,7 @@ void Grid::fit_table(size_t buckets) {
 void Grid::release() {
   b_keys.release(); b_vals.release(); b_pts.release(); b_table.release();
   b_frames.release(); b_begin.release(); b_sort.release(); b_misc.release();
+  b_cstart.release();
   n_max = 0; n_frames_max = 0; table_cap = 0;
 }
 
@@ -312,6 +294,9 @@ GridView Grid::view(int mode, long long p1, long long p2) const {
   v.mode = mode;
   v.p1 = p1;
   v.p2 = p2;
+  v.cstart = b_cstart.as<u32>();
+  v.n_coarse = d_nbuckets + 1;
+  v.n_points = d_n;
   return v;
 }
 
@@ -335,11 +320,13 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   u64 *bucket_of = reinterpret_cast<u64 *>(sp); sp += al((g.n_max + 1) * 8);
   u64 *cbucket_of = reinterpret_cast<u64 *>(sp); sp += al((g.n_max + 1) * 8);
   u32 *bstart = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
-  u32 *cstart = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
+  u32 *cstart = g.b_cstart.as<u32>();
   void *scan_tmp = sp;
 
   const int sms = ctx->num_sms;
   const unsigned gb = grid_for(n_max, 256, sms * 16);
+  k_set_count<<<1, 32, 0, st>>>(g.d_n, n_dev, (u64)n_max);
+  RVP_LAUNCH_CHECK(ctx);
   k_bbox_init<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(bb, n_frames);
   RVP_LAUNCH_CHECK(ctx);
   k_bbox<<<gb, 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, bb);
@@ -371,188 +358,6 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
 // Queries
 // ===========================================================================
 namespace {
-
-constexpr u32 kRemovedBit = 0x80000000u;
-
-struct Window {
-  int lo[3], hi[3];  // cells, inclusive, at `level`
-  int level;         // 0 fine, 1 coarse (dense mode only)
-};
-
-__device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u32 &count) {
-  u64 slot = mix64(key) & g.table_mask;
-  for (u64 probe = 0; probe <= g.table_mask; ++probe) {
-    const ulonglong2 e = __ldg(&g.table[slot]);
-    if (e.x == key) {
-      start = (u32)(e.y & 0xFFFFFFFFull);
-      count = (u32)(e.y >> 32);
-      return true;
-    }
-    if (e.x == kEmptyKey) return false;
-    slot = (slot + 1) & g.table_mask;
-  }
-  return false;
-}
-
-// Tight window of all cells that can hold a point p with d2(p, q) <= r*r:
-// |p - q| <= r (1 + 3 * 2^-24) per axis for any such p; the bound is padded
-// to r (1 + 1e-6) and rounded outwards, and the cell function is monotone,
-// so the window is exact. Clamped to the frame's grid. Level 1 takes the
-// coarse cells (fine index >> 2) of the same range.
-__device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, float qy, float qz,
-                                               double r, int level = 0) {
-  const double rp = r * (1.0 + 1e-6) + 1e-30;
-  Window w;
-  w.level = level;
-  const float q[3] = {qx, qy, qz};
-  const float mn[3] = {F.min_x, F.min_y, F.min_z};
-  const int G[3] = {F.gx, F.gy, F.gz};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float lo = __double2float_rd((double)q[a] - rp);
-    const float hi = __double2float_ru((double)q[a] + rp);
-    w.lo[a] = max(cell_axis_clamped(lo, mn[a], F.cell, -1, G[a]), 0);
-    w.hi[a] = min(cell_axis_clamped(hi, mn[a], F.cell, -1, G[a]), G[a] - 1);
-    if (level) {
-      w.lo[a] >>= 2;
-      w.hi[a] = w.hi[a] < 0 ? -1 : (w.hi[a] >> 2);
-    }
-  }
-  return w;
-}
-
-// The reference's window: query cell +- (ceil(r/cell) + 1), unclamped
-// (spatial_hashing.cpp:174-181).
-__device__ __forceinline__ Window ref_window(const GridFrame &F, float qx, float qy, float qz,
-                                             float radius) {
-  const int R = (int)ceilf(fdiv(radius, F.cell)) + 1;
-  Window w;
-  w.level = 0;
-  const int c[3] = {cell_axis(qx, F.min_x, F.cell), cell_axis(qy, F.min_y, F.cell),
-                    cell_axis(qz, F.min_z, F.cell)};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) { w.lo[a] = c[a] - R; w.hi[a] = c[a] + R; }
-  return w;
-}
-
-// The query's own cell +- ring at `level`, clamped.
-__device__ __forceinline__ Window ring_window(const GridFrame &F, float qx, float qy, float qz,
-                                              int ring, int level = 0) {
-  Window w;
-  w.level = level;
-  const float q[3] = {qx, qy, qz};
-  const float mn[3] = {F.min_x, F.min_y, F.min_z};
-  const int G[3] = {F.gx, F.gy, F.gz};
-  const int GC[3] = {F.gcx, F.gcy, F.gcz};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1);
-    int top = G[a] - 1;
-    if (level) {
-      c >>= 2;
-      top = GC[a] - 1;
-    }
-    w.lo[a] = max(c - ring, 0);
-    w.hi[a] = min(c + ring, top);
-  }
-  return w;
-}
-
-// Lower bound on the distance from q to any point of the frame outside w;
-// +inf when w spans the whole grid.
-__device__ __forceinline__ double coverage(const GridFrame &F, const Window &w, float qx, float qy,
-                                           float qz) {
-  const float q[3] = {qx, qy, qz};
-  const float mn[3] = {F.min_x, F.min_y, F.min_z};
-  const int top[3] = {w.level ? F.gcx - 1 : F.gx - 1, w.level ? F.gcy - 1 : F.gy - 1,
-                      w.level ? F.gcz - 1 : F.gz - 1};
-  const double cs = w.level ? 4.0 * (double)F.cell : (double)F.cell;
-  double cov = 1e300;
-  const double u = 4.0 * 5.960464477539063e-08;  // 4 * 2^-24
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const double slack =
-        u * (fabs((double)mn[a]) + (double)(w.hi[a] + 2) * cs + fabs((double)q[a])) + 1e-30;
-    if (w.lo[a] > 0) {
-      const double face = (double)mn[a] + (double)w.lo[a] * cs;
-      cov = fmin(cov, (double)q[a] - face - slack);
-    }
-    if (w.hi[a] < top[a]) {
-      const double face = (double)mn[a] + (double)(w.hi[a] + 1) * cs;
-      cov = fmin(cov, face - (double)q[a] - slack);
-    }
-  }
-  return cov;
-}
-
-__device__ __forceinline__ long long window_cells(const Window &w) {
-  long long c = 1;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    if (w.hi[a] < w.lo[a]) return 0;
-    c *= (long long)(w.hi[a] - w.lo[a] + 1);
-  }
-  return c;
-}
-
-// Walk every candidate of window w (or of the whole frame when brute):
-// fn(float4 p, bool valid) is called by all 32 lanes for each batch of 32.
-template <class Fn>
-__device__ __forceinline__ void for_each_candidate(const GridView &g, const GridFrame &F, int f,
-                                                   const Window &w, bool brute, Fn &&fn) {
-  const int lane = threadIdx.x & 31;
-  if (brute) {
-    const u64 a = g.frame_pt_begin[f], b = g.frame_pt_begin[f + 1];
-    for (u64 p0 = a; p0 < b; p0 += 32) {
-      const u64 p = p0 + lane;
-      const bool valid = p < b;
-      float4 v = valid ? __ldg(&g.pts[p]) : make_float4(0, 0, 0, 0);
-      fn(v, valid);
-    }
-    return;
-  }
-  const long long total = window_cells(w);
-  const int ncx = w.hi[0] - w.lo[0] + 1, ncy = w.hi[1] - w.lo[1] + 1;
-  for (long long cb = 0; cb < total; cb += 32) {
-    const long long j = cb + lane;
-    u32 start = 0, count = 0;
-    if (j < total) {
-      const int cx = w.lo[0] + (int)(j % ncx);
-      const int cy = w.lo[1] + (int)((j / ncx) % ncy);
-      const int cz = w.lo[2] + (int)(j / ((long long)ncx * ncy));
-      const u64 key = w.level ? coarse_key(F, cx, cy, cz) : fine_key(g, F, cx, cy, cz);
-      if (!lookup(g, key, start, count)) count = 0;
-    }
-    // flatten: inclusive scan of bucket sizes
-    u32 incl = count;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const u32 t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    const u32 ex = incl - count;
-    const u32 M = __shfl_sync(0xffffffffu, incl, 31);
-    for (u32 p0 = 0; p0 < M; p0 += 32) {
-      const u32 p = p0 + lane;
-      // owner cell: largest lane c with ex_c <= p
-      int c = 0;
-#pragma unroll
-      for (int s = 16; s; s >>= 1) {
-        const u32 t = __shfl_sync(0xffffffffu, ex, c + s);
-        if (t <= p) c += s;
-      }
-      const u32 st = __shfl_sync(0xffffffffu, start, c);
-      const u32 ec = __shfl_sync(0xffffffffu, ex, c);
-      const bool valid = p < M;
-      float4 v = valid ? __ldg(&g.pts[st + (p - ec)]) : make_float4(0, 0, 0, 0);
-      fn(v, valid);
-    }
-  }
-}
-
-__device__ __forceinline__ u32 query_index(const QuerySet &q, size_t i) {
-  return q.order ? (u32)q.order[i] : (u32)i;
-}
 
 // ---------------------------------------------------------------------------
 // radius search: count pass
@@ -710,67 +515,6 @@ __global__ __launch_bounds__(1024) void k_sort_big(const u64 *offsets, u64 *pair
   }
 }
 
-// ---------------------------------------------------------------------------
-// exact kNN: warp-resident sorted list of 32*P keys (lane i, slot s holds
-// element 32*s + i); candidates below the K-th key are inserted one by one.
-// ---------------------------------------------------------------------------
-template <int P>
-struct WarpList {
-  u64 e[P];
-  __device__ __forceinline__ void init() {
-#pragma unroll
-    for (int s = 0; s < P; ++s) e[s] = ~0ull;
-  }
-  __device__ __forceinline__ u64 get(int j) const {  // broadcast element j
-    u64 v = e[0];
-#pragma unroll
-    for (int s = 1; s < P; ++s)
-      if ((j >> 5) == s) v = e[s];
-    return __shfl_sync(0xffffffffu, v, j & 31);
-  }
-  __device__ __forceinline__ void insert(u64 c) {
-    const int lane = threadIdx.x & 31;
-    u64 carry = 0;  // last element of the previous slot, before the insert
-#pragma unroll
-    for (int s = 0; s < P; ++s) {
-      const u64 cur = e[s];
-      const u64 last = __shfl_sync(0xffffffffu, cur, 31);
-      u64 prev = __shfl_up_sync(0xffffffffu, cur, 1);
-      bool prev_lt;
-      if (lane == 0) prev_lt = (s == 0) ? true : (carry < c);
-      else prev_lt = prev < c;
-      if (lane == 0 && s > 0) prev = carry;
-      if (!(cur < c)) e[s] = prev_lt ? c : prev;
-      carry = last;
-    }
-  }
-};
-
-template <int P>
-__device__ __forceinline__ void knn_scan(const GridView &g, const GridFrame &F, int f,
-                                         const Window &w, bool brute, float qx, float qy,
-                                         float qz, int K, u64 bound, WarpList<P> &L,
-                                         u32 &found) {
-  u64 thr = L.get(K - 1);
-  for_each_candidate(g, F, f, w, brute, [&](float4 p, bool valid) {
-    const u32 idx = __float_as_uint(p.w);
-    u64 key = ~0ull;
-    if (valid && !(idx & kRemovedBit)) key = pack_nbr(dist2(p.x, p.y, p.z, qx, qy, qz), (int)idx);
-    const bool in_bound = key <= bound;
-    found += __popc(__ballot_sync(0xffffffffu, in_bound));
-    unsigned m = __ballot_sync(0xffffffffu, in_bound && key < thr);
-    while (m) {
-      const int src = __ffs(m) - 1;
-      m &= m - 1;
-      const u64 c = __shfl_sync(0xffffffffu, key, src);
-      if (c < thr) {
-        L.insert(c);
-        thr = L.get(K - 1);
-      }
-    }
-  });
-}
-
 __device__ __forceinline__ u64 bound_of(float tau) { return pack_nbr(tau, 0x7FFFFFFF) | 0xFFFFFFFFull; }
 
 constexpr long long kMaxFineTight = 64;    // fine cells for a tight window
@@ -778,7 +522,8 @@ constexpr long long kMaxCoarseTight = 512; // coarse cells for a tight window
 
 template <int P>
 __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K, float radius,
-                                                  u64 *out, int32_t *out_counts, u32 *stats) {
+                                                  u64 *out, int32_t *out_counts, u32 *stats,
+                                                  int out_mode, float *mean) {
   const size_t nq = q.n_dev ? *q.n_dev : q.n_max;
   const int lane = threadIdx.x & 31;
   const size_t warp = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
@@ -849,15 +594,27 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
       }
     }
     const u32 cnt = found < (u32)K ? found : (u32)K;
+    if (out_mode == KNN_OUT_SOR_MEAN) {
+      // sor_sc's mean (statistical_outlier_removal.cpp:36-40): ascending
+      // sum of sqrtf(d2_j), j = 1..k, divided by k (fewer if the frame is
+      // smaller than k+1)
+      const int valid_k = (int)cnt - 1 < K - 1 ? (int)cnt - 1 : K - 1;
+      float sum = 0.0f;
+      for (int j = 1; j < K; ++j) {
+        const float d = nbr_d2(L.get(j));
+        if (j <= valid_k) sum = fadd(sum, __fsqrt_rn(d));
+      }
+      if (lane == 0) mean[qi] = valid_k > 0 ? fdiv(sum, (float)valid_k) : 0.0f;
+    } else {
+      const size_t row = out_mode == KNN_OUT_BY_SLOT ? wi : (size_t)qi;
 #pragma unroll
-    for (int s = 0; s < P; ++s) {
-      const int j = s * 32 + lane;
-      if (j < (int)cnt) out[(size_t)qi * K + j] = L.e[s];
+      for (int s = 0; s < P; ++s) {
+        const int j = s * 32 + lane;
+        if (j < (int)cnt) out[row * K + j] = L.e[s];
+      }
+      if (lane == 0 && out_counts) out_counts[row] = (int32_t)cnt;
     }
-    if (lane == 0) {
-      if (out_counts) out_counts[qi] = (int32_t)cnt;
-      if (stats) atomicAdd(&stats[path], 1u);
-    }
+    if (lane == 0 && stats) atomicAdd(&stats[path], 1u);
   }
 }
 
@@ -895,14 +652,17 @@ void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs, const u
 }
 
 void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k, float radius,
-              u64 *out_pairs, int32_t *out_counts, int qpw, int block_threads, u32 *stats) {
+              u64 *out_pairs, int32_t *out_counts, int qpw, int block_threads, u32 *stats,
+              int out_mode, float *mean) {
   (void)qpw;
   const int bt = block_threads > 0 ? block_threads : 256;
   const unsigned blocks = grid_for(q.n_max * 32, bt, ctx->num_sms * 32);
   if (k <= 32)
-    k_knn_warp<1><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts, stats);
+    k_knn_warp<1><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts, stats,
+                                                  out_mode, mean);
   else
-    k_knn_warp<2><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts, stats);
+    k_knn_warp<2><<<blocks, bt, 0, ctx->stream>>>(g, q, k, radius, out_pairs, out_counts, stats,
+                                                  out_mode, mean);
   RVP_LAUNCH_CHECK(ctx);
 }
 

@@ -199,6 +199,9 @@ struct GridView {  // what the query kernels read
   const u64 *frame_pt_begin;  // per frame: first sorted position
   int mode;
   long long p1, p2;        // mode 0 primes
+  const u32 *cstart;       // dense mode: first sorted position of each coarse bucket
+  const u64 *n_coarse;     // dense mode: number of coarse buckets (device)
+  const u64 *n_points;     // number of grid points (device; set by grid_build)
 };
 
 struct Grid {
@@ -206,7 +209,7 @@ struct Grid {
   size_t n_max = 0;
   size_t table_cap = 0;
   size_t table_cap_req = 0;    // 0: sized from n_max
-  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc;
+  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_cstart;
   u64 *d_n = nullptr;          // number of points (device)
   u64 *d_nbuckets = nullptr;   // [0] fine buckets, [1] coarse buckets (device)
   int *d_collision = nullptr;  // mode 0: hash collision detected
@@ -250,9 +253,33 @@ void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs,
 // stats (optional, 8 counters): queries certified by the fine ring, by a
 // fine tight window, by the coarse ring, by a coarse tight window, by a
 // whole-frame scan, and the radius-bounded ones.
+enum KnnOut { KNN_OUT_BY_QUERY = 0, KNN_OUT_BY_SLOT = 1, KNN_OUT_SOR_MEAN = 2 };
 void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
               float radius, u64 *out_pairs, int32_t *out_counts, int qpw,
-              int block_threads, u32 *stats = nullptr);
+              int block_threads, u32 *stats = nullptr, int out_mode = KNN_OUT_BY_QUERY,
+              float *mean = nullptr);
+
+// Tile kNN (dense grids): one block per coarse bucket stages the 6x6x6 fine
+// cells around it in shared memory, one thread per query scans its own
+// 27-cell ring; queries the ring cannot certify go to `hard` (original
+// indices) for grid_knn. Modes: SOR mean, fused reference normals, pairs.
+enum TileMode { TILE_SOR_MEAN = 0, TILE_NORMALS = 1, TILE_PAIRS = 2 };
+struct TileArgs {
+  const int32_t *frame_of;  // frame of each original index
+  float *mean;              // TILE_SOR_MEAN: by original index
+  const float *vx, *vy, *vz;  // TILE_NORMALS: coordinates by original index
+  const u64 *out_pos;       // TILE_NORMALS: output slot of each original index
+  float *nx, *ny, *nz;
+  int iters;
+  float vpx, vpy, vpz;
+  u64 *pairs;               // TILE_PAIRS: by original index, k per row
+  int32_t *counts;
+  u32 *hard;                // uncertified queries (original indices)
+  u32 *hard_count;          // device counter (cleared by the caller)
+};
+// false if k has no tile instantiation (use grid_knn then)
+bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
+                   int blocks, u32 *stats = nullptr);
 
 // ---------------------------------------------------------------------------
 // voxel grid (voxel.cu)
@@ -287,6 +314,9 @@ void sor_filter_frames(rvp_context *ctx, const float *x, const float *y,
                        float *thresh, void *temp, float *out_x, float *out_y,
                        float *out_z, u32 *src_index);
 size_t sor_filter_temp_bytes(size_t n_max, int n_frames);
+// output slot of every input point (exclusive scan of the keep flags; valid
+// for kept points) inside a sor_filter_frames temp buffer
+u64 *sor_positions(void *temp, size_t n_max);
 
 // ---------------------------------------------------------------------------
 // normals (normals.cu)
@@ -299,7 +329,8 @@ void normals_from_lists(rvp_context *ctx, const float *x, const float *y,
                         size_t n_max, const u64 *n_dev, bool div_centroid,
                         int iters, float vpx, float vpy, float vpz,
                         const float *qx, const float *qy, const float *qz,
-                        float *nx, float *ny, float *nz);
+                        float *nx, float *ny, float *nz, const u32 *order = nullptr,
+                        const u64 *out_pos = nullptr);
 void normals_precise(rvp_context *ctx, const float *x, const float *y,
                      const float *z, const u64 *pairs, int kk, size_t n,
                      float vpx, float vpy, float vpz, double cond_fp64,

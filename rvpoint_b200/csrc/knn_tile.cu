@@ -1,0 +1,220 @@
+// Tile kNN for dense (batched) grids on sm_100a.
+//
+// One thread block per coarse bucket (4 x 4 x 4 fine cells): the block looks
+// up the 6 x 6 x 6 fine cells around it once (one lookup per thread),
+// flattens them with a prefix sum and stages their points in shared memory
+// (coalesced float4 runs). Every point of the coarse bucket is then a query
+// handled by one thread, which scans its own 27-cell ring out of shared
+// memory and keeps a register-resident sorted top-K (unrolled insertion
+// network; float keys when only distances matter, packed (d2, index) keys
+// when ties must follow the reference's (d2, index) order). The ring
+// certifies the result when the K-th distance is below the ring's coverage
+// (distance to the nearest outside cell, with rounding slack); the others go
+// to a list that the warp-per-query kernel finishes with tight windows at the
+// fine or coarse level. Epilogues are fused: SOR mean distance
+// (statistical_outlier_removal.cpp:36-40) or the reference normal
+// (normal_estimation.cpp:141-161) straight from the registers.
+#include <type_traits>
+
+#include "grid_device.cuh"
+#include "internal.cuh"
+#include "normals_device.cuh"
+
+namespace rvp {
+using namespace gd;
+using namespace nd;
+
+namespace {
+constexpr int TT = 256;                      // threads per tile block
+constexpr int SIDE = 6;                      // staged fine cells per axis
+constexpr int NCELL = SIDE * SIDE * SIDE;    // 216
+constexpr int CAP = 2560;                    // staged candidates (40 KB)
+
+template <class T, int K>
+__device__ __forceinline__ void list_insert(T (&L)[K], T key) {
+#pragma unroll
+  for (int j = K - 1; j > 0; --j) {
+    const T a = L[j - 1], b = L[j];
+    L[j] = key < a ? a : (key < b ? key : b);
+  }
+  L[0] = key < L[0] ? key : L[0];
+}
+
+template <int K, int MODE>
+__global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, u32 *stats) {
+  using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
+  __shared__ u32 c_start[NCELL];
+  __shared__ u32 c_count[NCELL];
+  __shared__ u32 c_pref[NCELL + 1];
+  __shared__ float4 cand[CAP];
+  __shared__ int s_base[4];
+  __shared__ int s_staged;
+  const u64 ncb = *g.n_coarse;
+  const u64 n = *g.n_points;
+  const int tid = threadIdx.x;
+  Key kMax;
+  if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
+  else kMax = ~0ull;
+  for (u64 cb = blockIdx.x; cb < ncb; cb += gridDim.x) {
+    const u32 qs = g.cstart[cb];
+    const u32 qe = (cb + 1 < ncb) ? g.cstart[cb + 1] : (u32)n;
+    __syncthreads();  // the previous tile's shared memory is free
+    if (tid == 0) {
+      const float4 p0 = g.pts[qs];
+      const u32 i0 = __float_as_uint(p0.w) & 0x7FFFFFFFu;
+      const int f = a.frame_of ? a.frame_of[i0] : 0;
+      const GridFrame F = g.frames[f];
+      s_base[0] = (cell_axis(p0.x, F.min_x, F.cell) >> 2) * 4 - 1;
+      s_base[1] = (cell_axis(p0.y, F.min_y, F.cell) >> 2) * 4 - 1;
+      s_base[2] = (cell_axis(p0.z, F.min_z, F.cell) >> 2) * 4 - 1;
+      s_base[3] = f;
+    }
+    __syncthreads();
+    const int bx = s_base[0], by = s_base[1], bz = s_base[2];
+    const GridFrame F = g.frames[s_base[3]];
+    // 1) the 216 fine cells around the coarse cell
+    for (int t = tid; t < NCELL; t += TT) {
+      const int cx = bx + t % SIDE, cy = by + (t / SIDE) % SIDE, cz = bz + t / (SIDE * SIDE);
+      u32 st = 0, ct = 0;
+      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < F.gx && cy < F.gy && cz < F.gz)
+        if (!lookup(g, fine_key(g, F, cx, cy, cz), st, ct)) ct = 0;
+      c_start[t] = st;
+      c_count[t] = ct;
+    }
+    __syncthreads();
+    // 2) exclusive prefix of the counts (one warp) and the staging decision
+    if (tid < 32) {
+      u32 run = 0;
+      for (int base = 0; base < NCELL; base += 32) {
+        const int t = base + tid;
+        const u32 v = t < NCELL ? c_count[t] : 0;
+        u32 incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const u32 u = __shfl_up_sync(0xffffffffu, incl, o);
+          if (tid >= o) incl += u;
+        }
+        if (t < NCELL) c_pref[t] = run + incl - v;
+        run += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (tid == 0) {
+        c_pref[NCELL] = run;
+        s_staged = run <= (u32)CAP ? 1 : 0;
+      }
+    }
+    __syncthreads();
+    const bool staged = s_staged != 0;
+    if (staged) {
+      const u32 total = c_pref[NCELL];
+      for (u32 i = tid; i < total; i += TT) {
+        int lo = 0, hi = NCELL - 1;  // owning cell: largest c with c_pref[c] <= i
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (c_pref[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        cand[i] = __ldg(&g.pts[c_start[lo] + (i - c_pref[lo])]);
+      }
+    }
+    __syncthreads();
+    // 3) one thread per query of this coarse bucket
+    for (u32 qi = qs + tid; qi < qe; qi += TT) {
+      const float4 q = g.pts[qi];
+      const u32 qidx = __float_as_uint(q.w);
+      if (MODE == TILE_NORMALS && (qidx & kRemovedBit)) continue;
+      const int lx = cell_axis(q.x, F.min_x, F.cell) - bx;  // 1..4
+      const int ly = cell_axis(q.y, F.min_y, F.cell) - by;
+      const int lz = cell_axis(q.z, F.min_z, F.cell) - bz;
+      Key L[K];
+#pragma unroll
+      for (int j = 0; j < K; ++j) L[j] = kMax;
+      Key thr = kMax;
+      u32 found = 0;
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int c = ((lz + dz) * SIDE + (ly + dy)) * SIDE + (lx + dx);
+            const u32 cnt = c_count[c];
+            const u32 st = staged ? c_pref[c] : c_start[c];
+            for (u32 j = 0; j < cnt; ++j) {
+              const float4 p = staged ? cand[st + j] : __ldg(&g.pts[st + j]);
+              const u32 pidx = __float_as_uint(p.w);
+              if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
+              ++found;
+              const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+              Key key;
+              if constexpr (MODE == TILE_SOR_MEAN) key = d2;
+              else key = pack_nbr(d2, (int)pidx);
+              if (key < thr) {
+                list_insert<Key, K>(L, key);
+                thr = L[K - 1];
+              }
+            }
+          }
+      bool ok = false;
+      if (found >= (u32)K) {
+        float tau;
+        if constexpr (MODE == TILE_SOR_MEAN) tau = L[K - 1];
+        else tau = nbr_d2(L[K - 1]);
+        const Window w1 = ring_window(F, q.x, q.y, q.z, 1, 0);
+        const double cov = coverage(F, w1, q.x, q.y, q.z);
+        ok = cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5);
+      }
+      if (!ok) {
+        a.hard[atomicAdd(a.hard_count, 1u)] = qidx & 0x7FFFFFFFu;
+        continue;
+      }
+      if (stats) atomicAdd(stats, 1u);
+      if constexpr (MODE == TILE_SOR_MEAN) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
+        a.mean[qidx] = fdiv(sum, (float)(K - 1));
+      } else if constexpr (MODE == TILE_NORMALS) {
+        float nx, ny, nz;
+        normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
+                            a.vpz, nx, ny, nz);
+        const u64 o = a.out_pos[qidx];
+        a.nx[o] = nx;
+        a.ny[o] = ny;
+        a.nz[o] = nz;
+      } else {
+#pragma unroll
+        for (int j = 0; j < K; ++j) a.pairs[(size_t)qidx * K + j] = L[j];
+        if (a.counts) a.counts[qidx] = K;
+      }
+    }
+  }
+}
+
+template <int K>
+void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
+              u32 *stats) {
+  if (mode == TILE_SOR_MEAN)
+    k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, stats);
+  else if (mode == TILE_NORMALS)
+    k_knn_tile<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, stats);
+  else
+    k_knn_tile<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, stats);
+}
+}  // namespace
+
+bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
+                   int blocks, u32 *stats) {
+  if (g.mode != KEY_DENSE) return false;
+  if (blocks <= 0) blocks = ctx->num_sms * 8;
+  switch (k) {
+    case 8: launch_k<8>(ctx, g, mode, a, blocks, stats); break;
+    case 11: launch_k<11>(ctx, g, mode, a, blocks, stats); break;
+    case 16: launch_k<16>(ctx, g, mode, a, blocks, stats); break;
+    case 17: launch_k<17>(ctx, g, mode, a, blocks, stats); break;
+    case 21: launch_k<21>(ctx, g, mode, a, blocks, stats); break;
+    case 31: launch_k<31>(ctx, g, mode, a, blocks, stats); break;
+    case 32: launch_k<32>(ctx, g, mode, a, blocks, stats); break;
+    case 33: launch_k<33>(ctx, g, mode, a, blocks, stats); break;
+    default: return false;
+  }
+  RVP_LAUNCH_CHECK(ctx);
+  return true;
+}
+
+}  // namespace rvp

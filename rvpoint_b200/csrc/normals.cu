@@ -16,52 +16,15 @@
 #include <math.h>
 
 #include "internal.cuh"
+#include "normals_device.cuh"
 
 namespace rvp {
+using namespace nd;
 
 namespace {
 
-__device__ void eigen_smallest_ref(float A[3][3], int iters, float &nx, float &ny, float &nz) {
-  float V[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
-  for (int it = 0; it < iters; ++it) {
-    int p = 0, q = 1;
-    float max_off = fabsf(A[0][1]);
-    if (fabsf(A[0][2]) > max_off) { p = 0; q = 2; max_off = fabsf(A[0][2]); }
-    if (fabsf(A[1][2]) > max_off) { p = 1; q = 2; }
-    const float app = A[p][p], aqq = A[q][q], apq = A[p][q];
-    const float phi = fmul(0.5f, atan2f(fmul(2.0f, apq), fsub(app, aqq)));
-    const float c = cosf(phi), s = sinf(phi);
-    const float cc = fmul(c, c), ss = fmul(s, s), s2c = fmul(fmul(2.0f, s), c);
-    // c*c*app - 2*s*c*apq + s*s*aqq ; s*s*app + 2*s*c*apq + c*c*aqq
-    A[p][p] = fadd(fsub(fmul(cc, app), fmul(s2c, apq)), fmul(ss, aqq));
-    A[q][q] = fadd(fadd(fmul(ss, app), fmul(s2c, apq)), fmul(cc, aqq));
-    A[p][q] = 0.0f;
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      const float vip = V[r][p], viq = V[r][q];
-      V[r][p] = fsub(fmul(c, vip), fmul(s, viq));
-      V[r][q] = fadd(fmul(s, vip), fmul(c, viq));
-    }
-  }
-  int m = 0;
-  if (A[1][1] < A[m][m]) m = 1;
-  if (A[2][2] < A[m][m]) m = 2;
-  nx = V[0][m];
-  ny = V[1][m];
-  nz = V[2][m];
-}
-
-__device__ __forceinline__ void flip_ref(float px, float py, float pz, float vpx, float vpy,
-                                         float vpz, float &nx, float &ny, float &nz) {
-  const float vx = fsub(vpx, px), vy = fsub(vpy, py), vz = fsub(vpz, pz);
-  const float dot = fadd(fadd(fmul(vx, nx), fmul(vy, ny)), fmul(vz, nz));
-  if (dot < 0.0f) {
-    nx = -nx;
-    ny = -ny;
-    nz = -nz;
-  }
-}
-
+// One thread per list slot i: query qi = order ? order[i] : i, neighbours
+// pairs[offsets[i] ..) or pairs[i*fixed_k ..), result at out_pos[qi] (or qi).
 __global__ void k_normals_lists(const float *__restrict__ x, const float *__restrict__ y,
                                 const float *__restrict__ z, const u64 *__restrict__ pairs,
                                 const u64 *__restrict__ offsets,
@@ -69,7 +32,7 @@ __global__ void k_normals_lists(const float *__restrict__ x, const float *__rest
                                 size_t n_max, const u64 *n_dev, bool div_centroid, int iters,
                                 float vpx, float vpy, float vpz, const float *qx,
                                 const float *qy, const float *qz, float *nx, float *ny,
-                                float *nz) {
+                                float *nz, const u32 *order, const u64 *out_pos) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -82,46 +45,18 @@ __global__ void k_normals_lists(const float *__restrict__ x, const float *__rest
       l = pairs + i * (size_t)fixed_k;
       m = fixed_counts ? fixed_counts[i] : fixed_k;
     }
+    const size_t qi = order ? (size_t)order[i] : i;
+    const size_t oi = out_pos ? (size_t)out_pos[qi] : qi;
     if (m < 3) {  // normal_estimation.cpp:254
-      nx[i] = ny[i] = nz[i] = 0.0f;
+      nx[oi] = ny[oi] = nz[oi] = 0.0f;
       continue;
     }
-    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    for (int t = 0; t < m; ++t) {
-      const int j = nbr_idx(l[t]) & 0x7FFFFFFF;
-      cx = fadd(cx, x[j]);
-      cy = fadd(cy, y[j]);
-      cz = fadd(cz, z[j]);
-    }
-    if (div_centroid) {
-      const float fm = (float)m;
-      cx = fdiv(cx, fm);
-      cy = fdiv(cy, fm);
-      cz = fdiv(cz, fm);
-    } else {
-      const float inv_n = fdiv(1.0f, (float)m);
-      cx = fmul(cx, inv_n);
-      cy = fmul(cy, inv_n);
-      cz = fmul(cz, inv_n);
-    }
-    float c00 = 0, c01 = 0, c02 = 0, c11 = 0, c12 = 0, c22 = 0;
-    for (int t = 0; t < m; ++t) {
-      const int j = nbr_idx(l[t]) & 0x7FFFFFFF;
-      const float dx = fsub(x[j], cx), dy = fsub(y[j], cy), dz = fsub(z[j], cz);
-      c00 = fadd(c00, fmul(dx, dx));
-      c01 = fadd(c01, fmul(dx, dy));
-      c02 = fadd(c02, fmul(dx, dz));
-      c11 = fadd(c11, fmul(dy, dy));
-      c12 = fadd(c12, fmul(dy, dz));
-      c22 = fadd(c22, fmul(dz, dz));
-    }
-    float A[3][3] = {{c00, c01, c02}, {c01, c11, c12}, {c02, c12, c22}};
     float a, b, c;
-    eigen_smallest_ref(A, iters, a, b, c);
-    flip_ref(qx[i], qy[i], qz[i], vpx, vpy, vpz, a, b, c);
-    nx[i] = a;
-    ny[i] = b;
-    nz[i] = c;
+    normal_from_list(x, y, z, [&](int t) { return nbr_idx(l[t]) & 0x7FFFFFFF; }, m, div_centroid,
+                     iters, qx[qi], qy[qi], qz[qi], vpx, vpy, vpz, a, b, c);
+    nx[oi] = a;
+    ny[oi] = b;
+    nz[oi] = c;
   }
 }
 
@@ -251,10 +186,11 @@ void normals_from_lists(rvp_context *ctx, const float *x, const float *y, const 
                         const u64 *pairs, const u64 *offsets, const int32_t *fixed_counts,
                         int fixed_k, size_t n_max, const u64 *n_dev, bool div_centroid, int iters,
                         float vpx, float vpy, float vpz, const float *qx, const float *qy,
-                        const float *qz, float *nx, float *ny, float *nz) {
+                        const float *qz, float *nx, float *ny, float *nz, const u32 *order,
+                        const u64 *out_pos) {
   k_normals_lists<<<grid_for(n_max, 128, ctx->num_sms * 32), 128, 0, ctx->stream>>>(
       x, y, z, pairs, offsets, fixed_counts, fixed_k, n_max, n_dev, div_centroid, iters, vpx, vpy,
-      vpz, qx, qy, qz, nx, ny, nz);
+      vpz, qx, qy, qz, nx, ny, nz, order, out_pos);
   RVP_LAUNCH_CHECK(ctx);
 }
 

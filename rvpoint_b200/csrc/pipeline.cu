@@ -39,6 +39,7 @@ struct rvp_pipeline {
   rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
   rvp::DevBuf stats;  // 16 kNN path counters (diagnostics)
+  rvp::DevBuf hard;   // queries the tile kernel could not certify (+ counter)
   bool stats_on = false;
   int n_frames_last = 0;
   // stage timing: a ring of event sets, one set per run
@@ -80,6 +81,18 @@ __global__ void k_frame_ids(const int64_t *offs, int n_frames, size_t n_max, int
     }
     frame[i] = lo;
   }
+}
+
+__global__ void k_widen(const u32 *a, u64 *b) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *b = *a;
+}
+
+__global__ void k_queue_kept(const uint8_t *keep, const u64 *n_dev, size_t n_max, u32 *list,
+                             u32 *count) {
+  const size_t n = n_dev ? *n_dev : n_max;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    if (keep[i]) list[atomicAdd(count, 1u)] = (u32)i;
 }
 
 // flag grid points whose source point was removed by SOR
@@ -136,6 +149,7 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->sor_frame.reserve(N * 4);
     p->sor_src.reserve(N * 4);
     p->nrm_pairs.reserve(N * (size_t)kn * 8);
+    p->hard.reserve(N * 4 + 256);
     p->nrm_counts.reserve(N * 4);
     p->nx.reserve(N * 4); p->ny.reserve(N * 4); p->nz.reserve(N * 4);
     p->r_model.reserve((size_t)max_frames * 16);
@@ -167,7 +181,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats};
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard};
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
@@ -212,40 +226,81 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     RVP_LAUNCH_CHECK(ctx);
     const rvp::GridView gv = p->grid.view(rvp::KEY_DENSE, 0, 0);
     p->mark(2);
-    // 3) SOR: exact k+1 nearest, mean distance, per-frame statistics
+    // 3) SOR: exact k+1 nearest and the mean distance, fused in the tile
+    //    kernel; the queries its 27-cell ring cannot certify are finished by
+    //    the warp kernel (tight windows, coarse level, whole frame)
     const int ks = c.sor_k + 1;
+    u64 *hard_n64 = p->hard.as<u64>();                   // widened count (grid_knn)
+    u32 *hard_n = reinterpret_cast<u32 *>(hard_n64 + 1);  // atomic counter
+    u32 *hard = reinterpret_cast<u32 *>(hard_n64 + 2);    // original indices
+    u32 *st0 = p->stats_on ? p->stats.as<u32>() : nullptr;
+    rvp::TileArgs ta{};
+    ta.frame_of = p->vox_frame.as<int32_t>();
+    ta.hard = hard;
+    ta.hard_count = hard_n;
+    const bool tiled = c.queries_per_warp != 1;
+    rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
+                     hard_n64, p->vox_frame.as<int32_t>(), reinterpret_cast<int32_t *>(hard)};
     rvp::QuerySet qv{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N, n_vox,
                      p->vox_frame.as<int32_t>(), nullptr};
-    u32 *st0 = p->stats_on ? p->stats.as<u32>() : nullptr;
-    rvp::grid_knn(ctx, gv, qv, ks, 0.0f, p->knn_pairs.as<u64>(), p->knn_counts.as<int32_t>(),
-                  c.queries_per_warp, c.block_threads, st0);
+    ta.mean = p->mean.as<float>();
+    RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
+    if (tiled && rvp::grid_knn_tile(ctx, gv, ks, rvp::TILE_SOR_MEAN, ta, 0, st0 ? st0 + 7 : nullptr)) {
+      k_widen<<<1, 32, 0, st>>>(hard_n, hard_n64);
+      RVP_LAUNCH_CHECK(ctx);
+      rvp::grid_knn(ctx, gv, qh, ks, 0.0f, nullptr, nullptr, 1, c.block_threads, st0,
+                    rvp::KNN_OUT_SOR_MEAN, p->mean.as<float>());
+    } else {
+      rvp::grid_knn(ctx, gv, qv, ks, 0.0f, nullptr, nullptr, 1, c.block_threads, st0,
+                    rvp::KNN_OUT_SOR_MEAN, p->mean.as<float>());
+    }
     p->mark(3);
-    rvp::sor_mean_from_knn(ctx, p->knn_pairs.as<u64>(), ks, p->knn_counts.as<int32_t>(), N, n_vox,
-                           p->mean.as<float>(), 0.0f, false);
     rvp::sor_filter_frames(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
                            p->mean.as<float>(), vox_offs, n_frames, N, n_vox, c.sor_alpha,
                            p->keep.as<uint8_t>(), p->sor_aos.as<float>(), sor_offs, nullptr,
                            p->sor_tmp.ptr, p->sor_x.as<float>(), p->sor_y.as<float>(),
                            p->sor_z.as<float>(), p->sor_src.as<u32>());
+    const u64 *sor_pos = rvp::sor_positions(p->sor_tmp.ptr, N);
     p->mark(4);
-    // 4) normals: k+1 nearest kept points of every kept point
+    // 4) normals: the k+1 nearest kept points of every kept point, with the
+    //    reference normal computed in the same tile kernel
     k_mark_removed<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(
         p->grid.b_pts.as<float4>(), p->keep.as<uint8_t>(), n_vox, N);
     RVP_LAUNCH_CHECK(ctx);
-    k_frame_ids<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(sor_offs, n_frames, N,
-                                                                 p->sor_frame.as<int32_t>());
-    RVP_LAUNCH_CHECK(ctx);
     const int kn = c.normal_k + 1;
-    rvp::QuerySet qs{p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(), N, n_sor,
-                     p->sor_frame.as<int32_t>(), nullptr};
-    rvp::grid_knn(ctx, gv, qs, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(),
-                  c.queries_per_warp, c.block_threads, st0 ? st0 + 8 : nullptr);
+    rvp::TileArgs tn = ta;
+    tn.mean = nullptr;
+    tn.vx = p->vox_x.as<float>();
+    tn.vy = p->vox_y.as<float>();
+    tn.vz = p->vox_z.as<float>();
+    tn.out_pos = sor_pos;
+    tn.nx = p->nx.as<float>();
+    tn.ny = p->ny.as<float>();
+    tn.nz = p->nz.as<float>();
+    tn.iters = c.eigen_iters;
+    tn.vpx = c.vp_x;
+    tn.vpy = c.vp_y;
+    tn.vpz = c.vp_z;
+    RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
+    bool tn_ok = tiled && rvp::grid_knn_tile(ctx, gv, kn, rvp::TILE_NORMALS, tn, 0,
+                                             st0 ? st0 + 15 : nullptr);
+    if (!tn_ok) {
+      // every kept point through the warp kernel: queue them all
+      k_queue_kept<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(p->keep.as<uint8_t>(), n_vox,
+                                                                    N, hard, hard_n);
+      RVP_LAUNCH_CHECK(ctx);
+    }
+    k_widen<<<1, 32, 0, st>>>(hard_n, hard_n64);
+    RVP_LAUNCH_CHECK(ctx);
+    rvp::grid_knn(ctx, gv, qh, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(), 1,
+                  c.block_threads, st0 ? st0 + 8 : nullptr, rvp::KNN_OUT_BY_SLOT, nullptr);
     p->mark(5);
     rvp::normals_from_lists(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
                             p->nrm_pairs.as<u64>(), nullptr, p->nrm_counts.as<int32_t>(), kn, N,
-                            n_sor, true, c.eigen_iters, c.vp_x, c.vp_y, c.vp_z,
-                            p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(),
-                            p->nx.as<float>(), p->ny.as<float>(), p->nz.as<float>());
+                            hard_n64, true, c.eigen_iters, c.vp_x, c.vp_y, c.vp_z,
+                            p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
+                            p->nx.as<float>(), p->ny.as<float>(), p->nz.as<float>(), hard,
+                            sor_pos);
     p->mark(6);
     // 5) RANSAC per frame on the kept points
     double pc = (double)c.ransac_prob;

@@ -5,9 +5,10 @@
 //    (sor_sc :36-40); the radius-bounded variant (sor_spatial_hash
 //    :246-270) divides by min(k, count - 1) and falls back to the search
 //    radius for isolated points;
-//  * global mean / std: the reference sums sequentially in float, so one
-//    thread per frame walks its points in order (a parallel tree sum would
-//    round differently and move the threshold);
+//  * global mean / std (:43-55): the reference sums sequentially in float,
+//    so one lane per frame adds the values in input order (a parallel tree
+//    sum would round differently and move the threshold), fed through
+//    shared memory by its warp;
 //  * keep mean <= mu + alpha * sigma and copy kept points out in input order
 //    (flag scan + scatter).
 #include "internal.cuh"
@@ -45,45 +46,49 @@ __global__ void k_sor_mean(const u64 *pairs, int kk, const int32_t *counts, size
   }
 }
 
-// one thread per frame: the reference's sequential float sums (:43-55)
-__global__ void k_sor_stats(const float *__restrict__ mean, const int64_t *offs, int n_frames,
-                            float alpha, float *thresh) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per frame: lanes stage 1024 consecutive values in shared memory
+// (coalesced), then lane 0 adds them in input order -- the same sequence of
+// roundings as the reference's loop, without one global load per add.
+constexpr int ST_CHUNK = 1024;
+__global__ __launch_bounds__(32) void k_sor_stats_warp(const float *__restrict__ mean,
+                                                       const int64_t *offs, int n_frames,
+                                                       float alpha, float *thresh) {
+  __shared__ float buf[ST_CHUNK];
+  const int f = blockIdx.x;
   if (f >= n_frames) return;
+  const int lane = threadIdx.x;
   const int64_t a = offs[f], b = offs[f + 1];
   const int64_t n = b - a;
   if (n <= 0) {
-    thresh[f] = 0.0f;
+    if (lane == 0) thresh[f] = 0.0f;
     return;
   }
   float s = 0.0f;
-  int64_t i = a;
-  for (; i + 8 <= b; i += 8) {
-    float v[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = __ldg(&mean[i + j]);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) s = fadd(s, v[j]);
+  for (int64_t base = a; base < b; base += ST_CHUNK) {
+    const int m = (int)((b - base) < ST_CHUNK ? (b - base) : ST_CHUNK);
+    for (int j = lane; j < m; j += 32) buf[j] = __ldg(&mean[base + j]);
+    __syncwarp();
+    if (lane == 0)
+      for (int t = 0; t < m; ++t) s = fadd(s, buf[t]);
+    __syncwarp();
   }
-  for (; i < b; ++i) s = fadd(s, mean[i]);
-  const float mu = fdiv(s, (float)n);
+  const float mu = __shfl_sync(0xffffffffu, fdiv(s, (float)n), 0);
   float var = 0.0f;
-  for (i = a; i + 8 <= b; i += 8) {
-    float v[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = __ldg(&mean[i + j]);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const float d = fsub(v[j], mu);
-      var = fadd(var, fmul(d, d));
-    }
+  for (int64_t base = a; base < b; base += ST_CHUNK) {
+    const int m = (int)((b - base) < ST_CHUNK ? (b - base) : ST_CHUNK);
+    for (int j = lane; j < m; j += 32) buf[j] = __ldg(&mean[base + j]);
+    __syncwarp();
+    if (lane == 0)
+      for (int t = 0; t < m; ++t) {
+        const float d = fsub(buf[t], mu);
+        var = fadd(var, fmul(d, d));
+      }
+    __syncwarp();
   }
-  for (; i < b; ++i) {
-    const float d = fsub(mean[i], mu);
-    var = fadd(var, fmul(d, d));
+  if (lane == 0) {
+    const float sd = __fsqrt_rn(fdiv(var, (float)n));
+    thresh[f] = fadd(mu, fmul(alpha, sd));
   }
-  const float sd = __fsqrt_rn(fdiv(var, (float)n));
-  thresh[f] = fadd(mu, fmul(alpha, sd));
 }
 
 __global__ void k_sor_keep(const float *mean, const int64_t *offs, int n_frames, size_t n_max,
@@ -136,6 +141,10 @@ void sor_mean_from_knn(rvp_context *ctx, const u64 *pairs, int kk, const int32_t
   RVP_LAUNCH_CHECK(ctx);
 }
 
+u64 *sor_positions(void *temp, size_t n_max) {
+  return reinterpret_cast<u64 *>(static_cast<char *>(temp) + al(n_max * 4));
+}
+
 size_t sor_filter_temp_bytes(size_t n_max, int n_frames) {
   return al(n_max * 4) + al((n_max + 1) * 8) + al((size_t)(n_frames + 1) * 4) +
          scan_temp_bytes(n_max);
@@ -153,7 +162,8 @@ void sor_filter_frames(rvp_context *ctx, const float *x, const float *y, const f
   p += al((size_t)(n_frames + 1) * 4);
   void *scan_tmp = p;
   cudaStream_t st = ctx->stream;
-  k_sor_stats<<<grid_for(n_frames, 32, 0), 32, 0, st>>>(mean, offs, n_frames, alpha, thresh);
+  k_sor_stats_warp<<<(unsigned)(n_frames > 0 ? n_frames : 1), 32, 0, st>>>(mean, offs, n_frames,
+                                                                         alpha, thresh);
   RVP_LAUNCH_CHECK(ctx);
   k_sor_keep<<<grid_for(n_max, 256, ctx->num_sms * 16), 256, 0, st>>>(mean, offs, n_frames, n_max,
                                                                      n_dev, thresh, keep, flags);

@@ -352,3 +352,33 @@ def test_pipeline_frames_match_per_frame_oracle(gpu_ctx, restatement):
         best, model, _, _, _ = restatement.ransac_plane(sc, 0.05, 1000, rs)
         assert r["ransac_count"][f] == best, f
         assert np.array_equal(bits(r["ransac_model"][f]), bits(model)), f
+
+
+def test_pipeline_tile_and_warp_paths_agree(gpu_ctx):
+    """The shared-memory tile kNN (one thread per query) and the warp-per-query
+    kernel give identical SOR output and normals on a full-size frame batch."""
+    from rvpoint_b200 import api
+    batch = D.lidar_batch(n_frames=3, seed=9)
+    outs = []
+    for qpw in (0, 1):
+        p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, cell_size=0.3,
+                         queries_per_warp=qpw)
+        outs.append(p.run_host(batch))
+    a, b = outs
+    assert np.array_equal(a["sor_offsets"], b["sor_offsets"])
+    assert np.array_equal(bits(a["sor"]), bits(b["sor"]))
+    assert np.array_equal(bits(a["normals"]), bits(b["normals"]))
+    assert np.array_equal(a["ransac_count"], b["ransac_count"])
+
+
+@pytest.mark.parametrize("cell", [0.15, 0.3, 0.8])
+def test_pipeline_cell_size_does_not_change_results(gpu_ctx, restatement, cell):
+    from rvpoint_b200 import api
+    batch = D.lidar_batch(n_frames=2, seed=13, min_pts=4000, max_pts=12000)
+    p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, cell_size=cell)
+    r = p.run_host(batch)
+    for f in range(batch.n_frames):
+        v, _ = restatement.voxel_grid(batch.frame(f), 0.1)
+        s, _, _ = restatement.sor_exact(D.Cloud.from_xyz(v), 16, 1.0)
+        a, b = r["sor_offsets"][f], r["sor_offsets"][f + 1]
+        assert np.array_equal(bits(r["sor"][a:b]), bits(s))
