@@ -510,13 +510,16 @@ class Pipeline:
     def check(self) -> None:
         check(self.L.rvp_pipeline_check(self.h), self.ctx.h)
 
-    PATHS = ("fine_ring", "fine_tight", "coarse_ring", "coarse_tight", "whole_frame", "bounded")
+    # warp kernel: ring at level 0 / tight window / ring at level 1 / ring at
+    # level 2 / whole frame; tile kernel: certified at level 0 / 1 / 2
+    PATHS = ("warp_ring0", "warp_tight", "warp_ring1", "warp_ring2", "warp_whole_frame",
+             "tile_l0", "tile_l1", "tile_l2")
 
     def knn_stats(self, enable: bool = True) -> dict:
         out = np.zeros(16, np.uint32)
         check(self.L.rvp_pipeline_knn_stats(self.h, int(enable), _ptr(out)), self.ctx.h)
-        return {"sor": dict(zip(self.PATHS, map(int, out[:6])), tile=int(out[7])),
-                "normals": dict(zip(self.PATHS, map(int, out[8:14])), tile=int(out[15]))}
+        return {"sor": dict(zip(self.PATHS, map(int, out[:8]))),
+                "normals": dict(zip(self.PATHS, map(int, out[8:16])))}
 
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)

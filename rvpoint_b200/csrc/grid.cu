@@ -115,11 +115,11 @@ __global__ void k_grid_params(GridFrame *fr, const float *bb, int n_frames, floa
       g.gy = (int)ceilf(fdiv(fsub(max_y, g.min_y), cell)) + 1;
       g.gz = (int)ceilf(fdiv(fsub(max_z, g.min_z), cell)) + 1;
     }
-    g.gcx = (g.gx + 3) >> 2;
-    g.gcy = (g.gy + 3) >> 2;
-    g.gcz = (g.gz + 3) >> 2;
+    g.g3x = (g.gx + 63) >> 6;
+    g.g3y = (g.gy + 63) >> 6;
+    g.g3z = (g.gz + 63) >> 6;
     g.key_base = base;
-    base += (u64)g.gcx * (u64)g.gcy * (u64)g.gcz * 64ull;
+    base += ((u64)g.g3x * (u64)g.g3y * (u64)g.g3z) << 18;
     fr[f] = g;
   }
 }
@@ -143,34 +143,34 @@ __global__ void k_cell_keys(const float *__restrict__ x, const float *__restrict
   }
 }
 
-// heads of fine buckets (key changes) and, in dense mode, of coarse buckets
-// (key >> 6 changes)
-__global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int mode, u32 *heads,
-                        u32 *cheads) {
+// heads of level-L buckets: key >> 6L changes (dense mode: L = 0..3; the
+// reference hash: L = 0 only)
+__global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int levels, u32 *heads) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const u64 k = keys[i];
     const u64 p = i ? keys[i - 1] : 0;
-    heads[i] = (i == 0 || k != p) ? 1u : 0u;
-    if (mode == KEY_DENSE) cheads[i] = (i == 0 || (k >> 6) != (p >> 6)) ? 1u : 0u;
+    for (int L = 0; L < levels; ++L)
+      heads[(size_t)L * n_max + i] = (i == 0 || (k >> (6 * L)) != (p >> (6 * L))) ? 1u : 0u;
   }
 }
 
 __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__ y,
                           const float *__restrict__ z, const u32 *vals, const u32 *heads,
-                          const u64 *bucket_of, const u32 *cheads, const u64 *cbucket_of,
-                          size_t n_max, const u64 *n_dev, float4 *pts, u32 *bstart, u32 *cstart,
-                          const GridFrame *frames, int mode, int *collision) {
+                          const u64 *bucket_of, size_t n_max, const u64 *n_dev, int levels,
+                          float4 *pts, u32 *lstart, const GridFrame *frames, int mode,
+                          int *collision) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const u32 v = vals[i];
     const float px = x[v], py = y[v], pz = z[v];
     pts[i] = make_float4(px, py, pz, __uint_as_float(v));
-    if (heads[i]) {
-      bstart[bucket_of[i]] = (u32)i;
-    } else if (mode == KEY_REF_HASH) {
+    for (int L = 0; L < levels; ++L)
+      if (heads[(size_t)L * n_max + i])
+        lstart[(size_t)L * n_max + bucket_of[(size_t)L * (n_max + 1) + i]] = (u32)i;
+    if (mode == KEY_REF_HASH && !heads[i]) {
       // same key as the previous point: a different cell means a collision
       const u32 u = vals[i - 1];
       const GridFrame F = frames[0];
@@ -179,7 +179,6 @@ __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__
           cell_axis(pz, F.min_z, F.cell) != cell_axis(z[u], F.min_z, F.cell))
         *collision = 1;
     }
-    if (mode == KEY_DENSE && cheads[i]) cstart[cbucket_of[i]] = (u32)i;
   }
 }
 
@@ -197,32 +196,30 @@ __device__ __forceinline__ void table_put(ulonglong2 *table, u64 mask, u64 key, 
   *overflow = 1;
 }
 
-// one thread per bucket: {key, start | count << 32} into the open-addressing
-// table (linear probing)
-__global__ void k_insert(const u64 *keys, const u32 *bstart, const u64 *bucket_of,
-                         const u32 *cstart, const u64 *cbucket_of, size_t n_max,
-                         const u64 *n_dev, int mode, ulonglong2 *table, u64 mask, u64 *nbuckets,
-                         int *overflow) {
+// one thread per bucket of levels 0 .. table_levels-1: {tagged key,
+// start | count << 32} into the open-addressing table (linear probing)
+__global__ void k_insert(const u64 *keys, const u32 *lstart, const u64 *bucket_of, size_t n_max,
+                         const u64 *n_dev, int levels, int table_levels, ulonglong2 *table,
+                         u64 mask, u64 *nbuckets, int *overflow) {
   const size_t n = n_dev ? *n_dev : n_max;
-  const u64 nb = bucket_of[n];
-  const u64 ncb = mode == KEY_DENSE ? cbucket_of[n] : 0;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    nbuckets[0] = nb;
-    nbuckets[1] = ncb;
+  u64 nb[4] = {0, 0, 0, 0};
+  u64 tot = 0;
+  for (int L = 0; L < levels; ++L) {
+    nb[L] = bucket_of[(size_t)L * (n_max + 1) + n];
+    if (L < table_levels) tot += nb[L];
   }
-  for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < nb + ncb;
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    for (int L = 0; L < 4; ++L) nbuckets[L] = nb[L];
+  for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < tot;
        b += (u64)gridDim.x * blockDim.x) {
-    if (b < nb) {
-      const u32 s = bstart[b];
-      const u32 e = (b + 1 < nb) ? bstart[b + 1] : (u32)n;
-      table_put(table, mask, keys[s], (u64)s | ((u64)(e - s) << 32), overflow);
-    } else {
-      const u64 c = b - nb;
-      const u32 s = cstart[c];
-      const u32 e = (c + 1 < ncb) ? cstart[c + 1] : (u32)n;
-      table_put(table, mask, kCoarseKeyBit | (keys[s] >> 6), (u64)s | ((u64)(e - s) << 32),
-                overflow);
-    }
+    int L = 0;
+    u64 c = b;
+    while (c >= nb[L]) c -= nb[L++];
+    const u32 *st = lstart + (size_t)L * n_max;
+    const u32 s = st[c];
+    const u32 e = (c + 1 < nb[L]) ? st[c + 1] : (u32)n;
+    const u64 key = L == 0 ? keys[s] : (((u64)L << 62) | (keys[s] >> (6 * L)));
+    table_put(table, mask, key, (u64)s | ((u64)(e - s) << 32), overflow);
   }
 }
 
@@ -252,17 +249,17 @@ void Grid::reserve(size_t n, int nf) {
     b_pts.reserve(n_max * 16);
     b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
     b_begin.reserve(al((n_frames_max + 1) * 8));
-    b_sort.reserve(sort_temp_bytes(n_max) + 2 * al(n_max * 4) + 2 * al((n_max + 1) * 8) +
-                   al(n_max * 4) + scan_temp_bytes(n_max));
-    b_cstart.reserve(al(n_max * 4));
+    b_sort.reserve(sort_temp_bytes(n_max) + al(4 * n_max * 4) + al(4 * (n_max + 1) * 8) +
+                   scan_temp_bytes(n_max));
+    b_lstart.reserve(al(4 * n_max * 4));
     b_misc.reserve(256);
     d_n = b_misc.as<u64>();
     d_nbuckets = d_n + 1;
-    d_collision = reinterpret_cast<int *>(d_n + 3);
+    d_collision = reinterpret_cast<int *>(d_n + 5);
     d_overflow = d_collision + 1;
   }
-  // fine + coarse buckets never exceed 2 n; without a measured count the
-  // table is sized for that worst case
+  // buckets of levels 0-2 never exceed 3 n (in practice ~1.2 n); without a
+  // measured count the table is sized for 2 n
   const size_t want = table_cap_req ? table_cap_req
                                     : (size_t)next_pow2((u64)(2 * n_max + n_max / 2 + 1024));
   if (want != table_cap) {
@@ -280,7 +277,7 @@ void Grid::fit_table(size_t buckets) {
 void Grid::release() {
   b_keys.release(); b_vals.release(); b_pts.release(); b_table.release();
   b_frames.release(); b_begin.release(); b_sort.release(); b_misc.release();
-  b_cstart.release();
+  b_lstart.release();
   n_max = 0; n_frames_max = 0; table_cap = 0;
 }
 
@@ -294,8 +291,8 @@ GridView Grid::view(int mode, long long p1, long long p2) const {
   v.mode = mode;
   v.p1 = p1;
   v.p2 = p2;
-  v.cstart = b_cstart.as<u32>();
-  v.n_coarse = d_nbuckets + 1;
+  for (int L = 0; L < 4; ++L) v.lstart[L] = b_lstart.as<u32>() + (size_t)L * n_max;
+  v.n_level = d_nbuckets;
   v.n_points = d_n;
   return v;
 }
@@ -307,6 +304,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   cudaStream_t st = ctx->stream;
   const size_t n_max = n_points;
   const u64 *n_dev = n_dev_opt;
+  const int levels = mode == KEY_DENSE ? 4 : 1;
+  const int table_levels = mode == KEY_DENSE ? kGridLevels : 1;
   GridFrame *frames = g.b_frames.as<GridFrame>();
   float *bb = reinterpret_cast<float *>(g.b_frames.as<char>() + al(g.n_frames_max * sizeof(GridFrame)));
   u64 *begin = g.b_begin.as<u64>();
@@ -315,13 +314,13 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   SortTemp t;
   sort_temp_carve(t, sp, g.n_max);
   sp += sort_temp_bytes(g.n_max);
-  u32 *heads = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
-  u32 *cheads = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
-  u64 *bucket_of = reinterpret_cast<u64 *>(sp); sp += al((g.n_max + 1) * 8);
-  u64 *cbucket_of = reinterpret_cast<u64 *>(sp); sp += al((g.n_max + 1) * 8);
-  u32 *bstart = reinterpret_cast<u32 *>(sp); sp += al(g.n_max * 4);
-  u32 *cstart = g.b_cstart.as<u32>();
+  // per-level arrays use stride n_max (heads, starts) / n_max + 1 (ids)
+  u32 *heads = reinterpret_cast<u32 *>(sp); sp += al(4 * g.n_max * 4);
+  u64 *bucket_of = reinterpret_cast<u64 *>(sp); sp += al(4 * (g.n_max + 1) * 8);
   void *scan_tmp = sp;
+  u32 *lstart = g.b_lstart.as<u32>();
+  // strides below are g.n_max; the kernels are given g.n_max as their n_max
+  const size_t nm = g.n_max;
 
   const int sms = ctx->num_sms;
   const unsigned gb = grid_for(n_max, 256, sms * 16);
@@ -337,19 +336,21 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
                                   g.b_keys.as<u64>(), g.b_vals.as<u32>());
   RVP_LAUNCH_CHECK(ctx);
   radix_sort_pairs(ctx, g.b_keys.as<u64>(), g.b_vals.as<u32>(), n_max, n_dev, t);
-  k_heads<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), n_max, n_dev, mode, heads, cheads);
+  // n for these kernels: the live count (n_dev) or n_max; strides: nm
+  const u64 *n_live = n_dev ? n_dev : g.d_n;
+  k_heads<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), nm, n_live, levels, heads);
   RVP_LAUNCH_CHECK(ctx);
-  // bucket_of[i] = number of heads before i, i.e. the bucket id of a head
-  exclusive_scan_u32_to_u64(ctx, heads, bucket_of, n_max, n_dev, scan_tmp);
-  if (mode == KEY_DENSE) exclusive_scan_u32_to_u64(ctx, cheads, cbucket_of, n_max, n_dev, scan_tmp);
+  // bucket_of[L][i] = number of level-L heads before i (the bucket id of a head)
+  for (int L = 0; L < levels; ++L)
+    exclusive_scan_u32_to_u64(ctx, heads + (size_t)L * nm, bucket_of + (size_t)L * (nm + 1), nm,
+                              n_live, scan_tmp);
   RVP_CUDA_TRY(cudaMemsetAsync(g.b_table.ptr, 0xFF, g.table_cap * 16, st));
-  RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 24, st));  // buckets, collision, overflow
-  k_reorder<<<gb, 256, 0, st>>>(x, y, z, g.b_vals.as<u32>(), heads, bucket_of, cheads, cbucket_of,
-                                n_max, n_dev, g.b_pts.as<float4>(), bstart, cstart, frames, mode,
-                                g.d_collision);
+  RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 40, st));  // buckets[4], collision, overflow
+  k_reorder<<<gb, 256, 0, st>>>(x, y, z, g.b_vals.as<u32>(), heads, bucket_of, nm, n_live, levels,
+                                g.b_pts.as<float4>(), lstart, frames, mode, g.d_collision);
   RVP_LAUNCH_CHECK(ctx);
-  k_insert<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), bstart, bucket_of, cstart, cbucket_of, n_max,
-                               n_dev, mode, g.b_table.as<ulonglong2>(), (u64)g.table_cap - 1,
+  k_insert<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), lstart, bucket_of, nm, n_live, levels,
+                               table_levels, g.b_table.as<ulonglong2>(), (u64)g.table_cap - 1,
                                g.d_nbuckets, g.d_overflow);
   RVP_LAUNCH_CHECK(ctx);
 }
@@ -517,8 +518,6 @@ __global__ __launch_bounds__(1024) void k_sort_big(const u64 *offsets, u64 *pair
 
 __device__ __forceinline__ u64 bound_of(float tau) { return pack_nbr(tau, 0x7FFFFFFF) | 0xFFFFFFFFull; }
 
-constexpr long long kMaxFineTight = 64;    // fine cells for a tight window
-constexpr long long kMaxCoarseTight = 512; // coarse cells for a tight window
 
 template <int P>
 __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K, float radius,
@@ -543,53 +542,46 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
       const Window w = tight_window(F, qx, qy, qz, (double)radius);
       knn_scan<P>(g, F, f, w, false, qx, qy, qz, K, bound_of(r2), L, found);
     } else {
-      // 1) fine ring: own cell +- 1
-      const Window w1 = ring_window(F, qx, qy, qz, 1, 0);
-      knn_scan<P>(g, F, f, w1, false, qx, qy, qz, K, ~0ull - 1, L, found);
-      bool done = false;
-      Window wr = w1;  // window whose candidates are in L
-      if (found < (u32)K && two_level) {
-        // 2) too few points nearby: coarse ring (12 fine cells wide)
-        wr = ring_window(F, qx, qy, qz, 1, 1);
+      // 1) rings of +- 1 cell, coarser (x4) while they hold fewer than K
+      Window wr = ring_window(F, qx, qy, qz, 1, 0);
+      knn_scan<P>(g, F, f, wr, false, qx, qy, qz, K, ~0ull - 1, L, found);
+      int lvl = 0;
+      while (found < (u32)K && two_level && lvl + 1 < kGridLevels) {
+        ++lvl;
+        wr = ring_window(F, qx, qy, qz, 1, lvl);
         L.init();
         found = 0;
         knn_scan<P>(g, F, f, wr, false, qx, qy, qz, K, ~0ull - 1, L, found);
-        path = 2;
-      } else {
-        path = 0;
       }
+      path = lvl == 0 ? 0 : (lvl == 1 ? 2 : 3);
+      bool done = false;
       if (found >= (u32)K) {
         const float tau = nbr_d2(L.get(K - 1));
         const double cov = coverage(F, wr, qx, qy, qz);
         if (cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5)) done = true;
         if (!done) {
-          // 3) every point with d2 <= tau lies in the tight window of
+          // 2) every point with d2 <= tau lies in the tight window of
           //    sqrt(tau) and there are >= K of them: exact. Scan it at the
-          //    level with the fewer cells.
+          //    finest level whose window stays small.
           const double rt = sqrt((double)tau);
-          const Window wf = tight_window(F, qx, qy, qz, rt, 0);
-          const long long cf = window_cells(wf);
-          Window wt = wf;
-          bool ok = cf <= kMaxFineTight;
-          path = 1;
-          if (!ok && two_level) {
-            wt = tight_window(F, qx, qy, qz, rt, 1);
-            ok = window_cells(wt) <= kMaxCoarseTight;
-            path = 3;
-          }
-          if (!ok && !two_level && cf <= 4096) ok = true;
-          if (ok) {
-            L.init();
-            found = 0;
-            knn_scan<P>(g, F, f, wt, false, qx, qy, qz, K, bound_of(tau), L, found);
-            done = true;
+          const int top = two_level ? kGridLevels - 1 : 0;
+          for (int lt = 0; lt <= top && !done; ++lt) {
+            const Window wt = tight_window(F, qx, qy, qz, rt, lt);
+            const long long cells = window_cells(wt);
+            if (cells <= (two_level ? (lt == top ? 512 : 125) : 4096)) {
+              L.init();
+              found = 0;
+              knn_scan<P>(g, F, f, wt, false, qx, qy, qz, K, bound_of(tau), L, found);
+              done = true;
+              path = 1;
+            }
           }
         }
       }
-      if (!done) {  // 4) whole frame
+      if (!done) {  // 3) whole frame
         L.init();
         found = 0;
-        knn_scan<P>(g, F, f, w1, true, qx, qy, qz, K, ~0ull - 1, L, found);
+        knn_scan<P>(g, F, f, wr, true, qx, qy, qz, K, ~0ull - 1, L, found);
         path = 4;
       }
     }

@@ -2,6 +2,15 @@
 // kernels (grid.cu, knn_tile.cu): the reference's cell function, dense
 // hierarchical keys, bucket-table lookup, query windows and their exact
 // coverage bounds, and the warp-cooperative candidate walk.
+//
+// Dense keys are hierarchical: a level-L cell is 4 x 4 x 4 level-(L-1) cells
+// (edge c * 4^L), and the 64-bit key of a fine cell is
+//   key_base(frame) + (level-3 cell, x fastest) << 18
+//                   + sub2 << 12 + sub1 << 6 + sub0,
+// subL = 6-bit position of the level-L cell inside its level-(L+1) parent.
+// Sorting by this key therefore makes every cell of every level one
+// contiguous run of points; level-L cells (L = 0, 1, 2) are entered in the
+// bucket table under key >> 6L tagged with L in bits 62-63.
 #pragma once
 
 #include <math.h>
@@ -10,6 +19,8 @@
 
 namespace rvp {
 namespace gd {
+
+constexpr u32 kRemovedBit = 0x80000000u;
 
 // getCellIndices (spatial_hashing.h:47-52)
 __device__ __forceinline__ int cell_axis(float v, float mn, float cell) {
@@ -22,26 +33,41 @@ __device__ __forceinline__ int cell_axis_clamped(float v, float mn, float cell, 
   return (int)t;
 }
 
+__device__ __forceinline__ int level_dim(int g, int level) {
+  return (g + (1 << (2 * level)) - 1) >> (2 * level);
+}
+
+__device__ __forceinline__ u64 sub_index(int cx, int cy, int cz, int level) {
+  const int s = 2 * level;
+  return (u64)((((cz >> s) & 3) << 4) | (((cy >> s) & 3) << 2) | ((cx >> s) & 3));
+}
+
+__device__ __forceinline__ u64 dense_key(const GridFrame &F, int cx, int cy, int cz) {
+  const u64 c3 = ((u64)(cz >> 6) * (u64)F.g3y + (u64)(cy >> 6)) * (u64)F.g3x + (u64)(cx >> 6);
+  return F.key_base + (c3 << 18) + (sub_index(cx, cy, cz, 2) << 12) +
+         (sub_index(cx, cy, cz, 1) << 6) + sub_index(cx, cy, cz, 0);
+}
+
 __device__ __forceinline__ u64 fine_key(const GridView &g, const GridFrame &F, int cx, int cy,
                                         int cz) {
   if (g.mode == KEY_REF_HASH) {
     const long long h = (long long)cx + (long long)cy * g.p1 + (long long)cz * g.p2;
     return (u64)h ^ 0x8000000000000000ull;
   }
-  const u64 c = ((u64)(cz >> 2) * (u64)F.gcy + (u64)(cy >> 2)) * (u64)F.gcx + (u64)(cx >> 2);
-  return F.key_base + (c << 6) + (u64)(((cz & 3) << 4) | ((cy & 3) << 2) | (cx & 3));
+  return dense_key(F, cx, cy, cz);
 }
 
-__device__ __forceinline__ u64 coarse_key(const GridFrame &F, int X, int Y, int Z) {
-  return kCoarseKeyBit |
-         ((F.key_base >> 6) + ((u64)Z * (u64)F.gcy + (u64)Y) * (u64)F.gcx + (u64)X);
+// table key of the level-L cell (X, Y, Z) (coordinates in level-L cells)
+__device__ __forceinline__ u64 level_key(const GridView &g, const GridFrame &F, int level, int X,
+                                         int Y, int Z) {
+  if (level == 0) return fine_key(g, F, X, Y, Z);
+  const int s = 2 * level;
+  return ((u64)level << 62) | (dense_key(F, X << s, Y << s, Z << s) >> (3 * s));
 }
-
-constexpr u32 kRemovedBit = 0x80000000u;
 
 struct Window {
   int lo[3], hi[3];  // cells, inclusive, at `level`
-  int level;         // 0 fine, 1 coarse (dense mode only)
+  int level;         // 0 fine; 1, 2 coarser (dense mode only)
 };
 
 __device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u32 &count) {
@@ -62,8 +88,8 @@ __device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u
 // Tight window of all cells that can hold a point p with d2(p, q) <= r*r:
 // |p - q| <= r (1 + 3 * 2^-24) per axis for any such p; the bound is padded
 // to r (1 + 1e-6) and rounded outwards, and the cell function is monotone,
-// so the window is exact. Clamped to the frame's grid. Level 1 takes the
-// coarse cells (fine index >> 2) of the same range.
+// so the window is exact. Clamped to the frame's grid, then taken at `level`
+// (fine index >> 2 level).
 __device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, float qy, float qz,
                                                double r, int level = 0) {
   const double rp = r * (1.0 + 1e-6) + 1e-30;
@@ -79,8 +105,8 @@ __device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, flo
     w.lo[a] = max(cell_axis_clamped(lo, mn[a], F.cell, -1, G[a]), 0);
     w.hi[a] = min(cell_axis_clamped(hi, mn[a], F.cell, -1, G[a]), G[a] - 1);
     if (level) {
-      w.lo[a] >>= 2;
-      w.hi[a] = w.hi[a] < 0 ? -1 : (w.hi[a] >> 2);
+      w.lo[a] >>= 2 * level;
+      w.hi[a] = w.hi[a] < 0 ? -1 : (w.hi[a] >> (2 * level));
     }
   }
   return w;
@@ -100,7 +126,7 @@ __device__ __forceinline__ Window ref_window(const GridFrame &F, float qx, float
   return w;
 }
 
-// The query's own cell +- ring at `level`, clamped.
+// The query's own level-L cell +- ring, clamped.
 __device__ __forceinline__ Window ring_window(const GridFrame &F, float qx, float qy, float qz,
                                               int ring, int level = 0) {
   Window w;
@@ -108,17 +134,11 @@ __device__ __forceinline__ Window ring_window(const GridFrame &F, float qx, floa
   const float q[3] = {qx, qy, qz};
   const float mn[3] = {F.min_x, F.min_y, F.min_z};
   const int G[3] = {F.gx, F.gy, F.gz};
-  const int GC[3] = {F.gcx, F.gcy, F.gcz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1);
-    int top = G[a] - 1;
-    if (level) {
-      c >>= 2;
-      top = GC[a] - 1;
-    }
+    const int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1) >> (2 * level);
     w.lo[a] = max(c - ring, 0);
-    w.hi[a] = min(c + ring, top);
+    w.hi[a] = min(c + ring, level_dim(G[a], level) - 1);
   }
   return w;
 }
@@ -129,9 +149,8 @@ __device__ __forceinline__ double coverage(const GridFrame &F, const Window &w, 
                                            float qz) {
   const float q[3] = {qx, qy, qz};
   const float mn[3] = {F.min_x, F.min_y, F.min_z};
-  const int top[3] = {w.level ? F.gcx - 1 : F.gx - 1, w.level ? F.gcy - 1 : F.gy - 1,
-                      w.level ? F.gcz - 1 : F.gz - 1};
-  const double cs = w.level ? 4.0 * (double)F.cell : (double)F.cell;
+  const int G[3] = {F.gx, F.gy, F.gz};
+  const double cs = (double)F.cell * (double)(1 << (2 * w.level));
   double cov = 1e300;
   const double u = 4.0 * 5.960464477539063e-08;  // 4 * 2^-24
 #pragma unroll
@@ -142,7 +161,7 @@ __device__ __forceinline__ double coverage(const GridFrame &F, const Window &w, 
       const double face = (double)mn[a] + (double)w.lo[a] * cs;
       cov = fmin(cov, (double)q[a] - face - slack);
     }
-    if (w.hi[a] < top[a]) {
+    if (w.hi[a] < level_dim(G[a], w.level) - 1) {
       const double face = (double)mn[a] + (double)(w.hi[a] + 1) * cs;
       cov = fmin(cov, face - (double)q[a] - slack);
     }
@@ -185,8 +204,7 @@ __device__ __forceinline__ void for_each_candidate(const GridView &g, const Grid
       const int cx = w.lo[0] + (int)(j % ncx);
       const int cy = w.lo[1] + (int)((j / ncx) % ncy);
       const int cz = w.lo[2] + (int)(j / ((long long)ncx * ncy));
-      const u64 key = w.level ? coarse_key(F, cx, cy, cz) : fine_key(g, F, cx, cy, cz);
-      if (!lookup(g, key, start, count)) count = 0;
+      if (!lookup(g, level_key(g, F, w.level, cx, cy, cz), start, count)) count = 0;
     }
     // flatten: inclusive scan of bucket sizes
     u32 incl = count;

@@ -180,16 +180,12 @@ struct GridFrame {  // per-frame grid parameters (device)
   float min_x, min_y, min_z;
   float cell;
   int gx, gy, gz;    // fine cells per axis
-  int gcx, gcy, gcz; // coarse cells (4 x 4 x 4 fine cells) per axis
-  u64 key_base;      // dense mode: frame's first key (a multiple of 64)
+  int g3x, g3y, g3z; // level-3 cells (64 x 64 x 64 fine cells) per axis
+  u64 key_base;      // dense mode: frame's first key (a multiple of 2^18)
 };
 
 enum KeyMode { KEY_REF_HASH = 0, KEY_DENSE = 1 };
-
-// dense-mode keys: coarse cell (x fastest) * 64 + fine cell inside it, so a
-// coarse cell's points are one contiguous run of the sorted points too;
-// coarse buckets live in the same table under keys with bit 63 set.
-constexpr u64 kCoarseKeyBit = 0x8000000000000000ull;
+constexpr int kGridLevels = 3;  // cell levels in the bucket table: c, 4c, 16c
 
 struct GridView {  // what the query kernels read
   const float4 *pts;       // cell-sorted {x,y,z,idx}
@@ -199,8 +195,8 @@ struct GridView {  // what the query kernels read
   const u64 *frame_pt_begin;  // per frame: first sorted position
   int mode;
   long long p1, p2;        // mode 0 primes
-  const u32 *cstart;       // dense mode: first sorted position of each coarse bucket
-  const u64 *n_coarse;     // dense mode: number of coarse buckets (device)
+  const u32 *lstart[4];    // dense mode: first sorted position of each level-L bucket
+  const u64 *n_level;      // dense mode: number of level-L buckets (device, [4])
   const u64 *n_points;     // number of grid points (device; set by grid_build)
 };
 
@@ -209,9 +205,9 @@ struct Grid {
   size_t n_max = 0;
   size_t table_cap = 0;
   size_t table_cap_req = 0;    // 0: sized from n_max
-  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_cstart;
+  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_lstart;
   u64 *d_n = nullptr;          // number of points (device)
-  u64 *d_nbuckets = nullptr;   // [0] fine buckets, [1] coarse buckets (device)
+  u64 *d_nbuckets = nullptr;   // buckets per level [4] (device)
   int *d_collision = nullptr;  // mode 0: hash collision detected
   int *d_overflow = nullptr;   // a bucket found no free table slot
   GridView view(int mode, long long p1, long long p2) const;
@@ -276,6 +272,8 @@ struct TileArgs {
   int32_t *counts;
   u32 *hard;                // uncertified queries (original indices)
   u32 *hard_count;          // device counter (cleared by the caller)
+  uint8_t *qlevel;          // per grid point: level at which it is still open
+  size_t n_max;             // size of qlevel
 };
 // false if k has no tile instantiation (use grid_knn then)
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,

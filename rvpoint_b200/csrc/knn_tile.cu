@@ -1,17 +1,17 @@
 // Tile kNN for dense (batched) grids on sm_100a.
 //
-// One thread block per coarse bucket (4 x 4 x 4 fine cells): the block looks
-// up the 6 x 6 x 6 fine cells around it once (one lookup per thread),
-// flattens them with a prefix sum and stages their points in shared memory
-// (coalesced float4 runs). Every point of the coarse bucket is then a query
-// handled by one thread, which scans its own 27-cell ring out of shared
-// memory and keeps a register-resident sorted top-K (unrolled insertion
-// network; float keys when only distances matter, packed (d2, index) keys
-// when ties must follow the reference's (d2, index) order). The ring
-// certifies the result when the K-th distance is below the ring's coverage
-// (distance to the nearest outside cell, with rounding slack); the others go
-// to a list that the warp-per-query kernel finishes with tight windows at the
-// fine or coarse level. Epilogues are fused: SOR mean distance
+// Level by level (cells of c, 4c, 16c): one thread block per bucket of the
+// next level up (a group of 4 x 4 x 4 cells) looks up the 6 x 6 x 6 cells
+// around it once (one lookup per thread), flattens them with a prefix sum
+// and stages their points in shared memory (coalesced float4 runs). Every
+// open query of the group is then handled by one thread, which scans its own
+// 27-cell ring out of shared memory and keeps a register-resident sorted
+// top-K (unrolled insertion network; float keys when only distances matter,
+// packed (d2, index) keys when ties must follow the reference's (d2, index)
+// order). The ring certifies the result when the K-th distance is below the
+// ring's coverage (distance to the nearest outside cell, with rounding
+// slack); the others stay open for the next, 4x coarser level, and after the
+// last level go to a list that the warp-per-query kernel finishes. Epilogues are fused: SOR mean distance
 // (statistical_outlier_removal.cpp:36-40) or the reference normal
 // (normal_estimation.cpp:141-161) straight from the registers.
 #include <type_traits>
@@ -41,7 +41,8 @@ __device__ __forceinline__ void list_insert(T (&L)[K], T key) {
 }
 
 template <int K, int MODE>
-__global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, u32 *stats) {
+__global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int level,
+                                                 uint8_t *qlevel, u32 *stats) {
   using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
   __shared__ u32 c_start[NCELL];
   __shared__ u32 c_count[NCELL];
@@ -49,35 +50,48 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, u32 *st
   __shared__ float4 cand[CAP];
   __shared__ int s_base[4];
   __shared__ int s_staged;
-  const u64 ncb = *g.n_coarse;
+  const u64 ngroups = g.n_level[level + 1];
+  const u32 *gstart = g.lstart[level + 1];
   const u64 n = *g.n_points;
   const int tid = threadIdx.x;
+  const int sh = 2 * level;  // level-L cell = fine index >> sh
   Key kMax;
   if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
   else kMax = ~0ull;
-  for (u64 cb = blockIdx.x; cb < ncb; cb += gridDim.x) {
-    const u32 qs = g.cstart[cb];
-    const u32 qe = (cb + 1 < ncb) ? g.cstart[cb + 1] : (u32)n;
-    __syncthreads();  // the previous tile's shared memory is free
+  for (u64 cb = blockIdx.x; cb < ngroups; cb += gridDim.x) {
+    const u32 qs = gstart[cb];
+    const u32 qe = (cb + 1 < ngroups) ? gstart[cb + 1] : (u32)n;
+    if (level > 0) {  // only the queries the previous level left open
+      int any = 0;
+      for (u32 base = qs; base < qe; base += TT) {
+        const u32 i = base + tid;
+        any |= __syncthreads_or(i < qe && qlevel[i] == level);
+      }
+      if (!any) continue;
+    }
+    __syncthreads();  // the previous group's shared memory is free
     if (tid == 0) {
       const float4 p0 = g.pts[qs];
       const u32 i0 = __float_as_uint(p0.w) & 0x7FFFFFFFu;
       const int f = a.frame_of ? a.frame_of[i0] : 0;
       const GridFrame F = g.frames[f];
-      s_base[0] = (cell_axis(p0.x, F.min_x, F.cell) >> 2) * 4 - 1;
-      s_base[1] = (cell_axis(p0.y, F.min_y, F.cell) >> 2) * 4 - 1;
-      s_base[2] = (cell_axis(p0.z, F.min_z, F.cell) >> 2) * 4 - 1;
+      const int gs = sh + 2;  // group cell = fine index >> gs
+      s_base[0] = (cell_axis(p0.x, F.min_x, F.cell) >> gs) * 4 - 1;
+      s_base[1] = (cell_axis(p0.y, F.min_y, F.cell) >> gs) * 4 - 1;
+      s_base[2] = (cell_axis(p0.z, F.min_z, F.cell) >> gs) * 4 - 1;
       s_base[3] = f;
     }
     __syncthreads();
     const int bx = s_base[0], by = s_base[1], bz = s_base[2];
     const GridFrame F = g.frames[s_base[3]];
-    // 1) the 216 fine cells around the coarse cell
+    const int dx_ = level_dim(F.gx, level), dy_ = level_dim(F.gy, level),
+              dz_ = level_dim(F.gz, level);
+    // 1) the 6 x 6 x 6 level-L cells around the group
     for (int t = tid; t < NCELL; t += TT) {
       const int cx = bx + t % SIDE, cy = by + (t / SIDE) % SIDE, cz = bz + t / (SIDE * SIDE);
       u32 st = 0, ct = 0;
-      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < F.gx && cy < F.gy && cz < F.gz)
-        if (!lookup(g, fine_key(g, F, cx, cy, cz), st, ct)) ct = 0;
+      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < dx_ && cy < dy_ && cz < dz_)
+        if (!lookup(g, level_key(g, F, level, cx, cy, cz), st, ct)) ct = 0;
       c_start[t] = st;
       c_count[t] = ct;
     }
@@ -116,14 +130,15 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, u32 *st
       }
     }
     __syncthreads();
-    // 3) one thread per query of this coarse bucket
+    // 3) one thread per open query of this group
     for (u32 qi = qs + tid; qi < qe; qi += TT) {
+      if (level > 0 && qlevel[qi] != level) continue;
       const float4 q = g.pts[qi];
       const u32 qidx = __float_as_uint(q.w);
       if (MODE == TILE_NORMALS && (qidx & kRemovedBit)) continue;
-      const int lx = cell_axis(q.x, F.min_x, F.cell) - bx;  // 1..4
-      const int ly = cell_axis(q.y, F.min_y, F.cell) - by;
-      const int lz = cell_axis(q.z, F.min_z, F.cell) - bz;
+      const int lx = (cell_axis(q.x, F.min_x, F.cell) >> sh) - bx;  // 1..4
+      const int ly = (cell_axis(q.y, F.min_y, F.cell) >> sh) - by;
+      const int lz = (cell_axis(q.z, F.min_z, F.cell) >> sh) - bz;
       Key L[K];
 #pragma unroll
       for (int j = 0; j < K; ++j) L[j] = kMax;
@@ -155,12 +170,13 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, u32 *st
         float tau;
         if constexpr (MODE == TILE_SOR_MEAN) tau = L[K - 1];
         else tau = nbr_d2(L[K - 1]);
-        const Window w1 = ring_window(F, q.x, q.y, q.z, 1, 0);
+        const Window w1 = ring_window(F, q.x, q.y, q.z, 1, level);
         const double cov = coverage(F, w1, q.x, q.y, q.z);
         ok = cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5);
       }
       if (!ok) {
-        a.hard[atomicAdd(a.hard_count, 1u)] = qidx & 0x7FFFFFFFu;
+        if (level + 1 < kGridLevels) qlevel[qi] = (uint8_t)(level + 1);
+        else a.hard[atomicAdd(a.hard_count, 1u)] = qidx & 0x7FFFFFFFu;
         continue;
       }
       if (stats) atomicAdd(stats, 1u);
@@ -188,32 +204,36 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, u32 *st
 
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
-              u32 *stats) {
-  if (mode == TILE_SOR_MEAN)
-    k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, stats);
-  else if (mode == TILE_NORMALS)
-    k_knn_tile<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, stats);
-  else
-    k_knn_tile<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, stats);
+              uint8_t *qlevel, u32 *stats) {
+  RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
+  for (int level = 0; level < kGridLevels; ++level) {
+    u32 *st = stats ? stats + level : nullptr;
+    if (mode == TILE_SOR_MEAN)
+      k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, st);
+    else if (mode == TILE_NORMALS)
+      k_knn_tile<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, st);
+    else
+      k_knn_tile<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, st);
+    RVP_LAUNCH_CHECK(ctx);
+  }
 }
 }  // namespace
 
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
                    int blocks, u32 *stats) {
-  if (g.mode != KEY_DENSE) return false;
+  if (g.mode != KEY_DENSE || !a.qlevel) return false;
   if (blocks <= 0) blocks = ctx->num_sms * 8;
   switch (k) {
-    case 8: launch_k<8>(ctx, g, mode, a, blocks, stats); break;
-    case 11: launch_k<11>(ctx, g, mode, a, blocks, stats); break;
-    case 16: launch_k<16>(ctx, g, mode, a, blocks, stats); break;
-    case 17: launch_k<17>(ctx, g, mode, a, blocks, stats); break;
-    case 21: launch_k<21>(ctx, g, mode, a, blocks, stats); break;
-    case 31: launch_k<31>(ctx, g, mode, a, blocks, stats); break;
-    case 32: launch_k<32>(ctx, g, mode, a, blocks, stats); break;
-    case 33: launch_k<33>(ctx, g, mode, a, blocks, stats); break;
+    case 8: launch_k<8>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
+    case 11: launch_k<11>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
+    case 16: launch_k<16>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
+    case 17: launch_k<17>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
+    case 21: launch_k<21>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
+    case 31: launch_k<31>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
+    case 32: launch_k<32>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
+    case 33: launch_k<33>(ctx, g, mode, a, blocks, a.qlevel, stats); break;
     default: return false;
   }
-  RVP_LAUNCH_CHECK(ctx);
   return true;
 }
 

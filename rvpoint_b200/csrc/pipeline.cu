@@ -40,6 +40,7 @@ struct rvp_pipeline {
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
   rvp::DevBuf stats;  // 16 kNN path counters (diagnostics)
   rvp::DevBuf hard;   // queries the tile kernel could not certify (+ counter)
+  rvp::DevBuf qlevel; // per grid point: level at which its kNN is still open
   bool stats_on = false;
   int n_frames_last = 0;
   // stage timing: a ring of event sets, one set per run
@@ -150,6 +151,7 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->sor_src.reserve(N * 4);
     p->nrm_pairs.reserve(N * (size_t)kn * 8);
     p->hard.reserve(N * 4 + 256);
+    p->qlevel.reserve(N);
     p->nrm_counts.reserve(N * 4);
     p->nx.reserve(N * 4); p->ny.reserve(N * 4); p->nz.reserve(N * 4);
     p->r_model.reserve((size_t)max_frames * 16);
@@ -181,7 +183,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard};
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel};
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
@@ -238,6 +240,8 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.frame_of = p->vox_frame.as<int32_t>();
     ta.hard = hard;
     ta.hard_count = hard_n;
+    ta.qlevel = p->qlevel.as<uint8_t>();
+    ta.n_max = N;
     const bool tiled = c.queries_per_warp != 1;
     rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
                      hard_n64, p->vox_frame.as<int32_t>(), reinterpret_cast<int32_t *>(hard)};
@@ -245,7 +249,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                      p->vox_frame.as<int32_t>(), nullptr};
     ta.mean = p->mean.as<float>();
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
-    if (tiled && rvp::grid_knn_tile(ctx, gv, ks, rvp::TILE_SOR_MEAN, ta, 0, st0 ? st0 + 7 : nullptr)) {
+    if (tiled && rvp::grid_knn_tile(ctx, gv, ks, rvp::TILE_SOR_MEAN, ta, 0, st0 ? st0 + 5 : nullptr)) {
       k_widen<<<1, 32, 0, st>>>(hard_n, hard_n64);
       RVP_LAUNCH_CHECK(ctx);
       rvp::grid_knn(ctx, gv, qh, ks, 0.0f, nullptr, nullptr, 1, c.block_threads, st0,
@@ -283,7 +287,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     tn.vpz = c.vp_z;
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
     bool tn_ok = tiled && rvp::grid_knn_tile(ctx, gv, kn, rvp::TILE_NORMALS, tn, 0,
-                                             st0 ? st0 + 15 : nullptr);
+                                             st0 ? st0 + 13 : nullptr);
     if (!tn_ok) {
       // every kept point through the warp kernel: queue them all
       k_queue_kept<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(p->keep.as<uint8_t>(), n_vox,
@@ -318,12 +322,12 @@ rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p) {
   if (!p) return RVP_ERR_INVALID_ARG;
   return guard(p->ctx, [&] {
     RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
-    u64 nb[2] = {0, 0};
-    RVP_CUDA_TRY(cudaMemcpyAsync(nb, p->grid.d_nbuckets, 16, cudaMemcpyDeviceToHost,
+    u64 nb[4] = {0, 0, 0, 0};
+    RVP_CUDA_TRY(cudaMemcpyAsync(nb, p->grid.d_nbuckets, 32, cudaMemcpyDeviceToHost,
                                  p->ctx->stream));
     RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
     // headroom for batches whose scenes occupy more cells than this one
-    p->grid.fit_table((size_t)((nb[0] + nb[1]) * 2));
+    p->grid.fit_table((size_t)((nb[0] + nb[1] + nb[2]) * 2));
   });
 }
 
