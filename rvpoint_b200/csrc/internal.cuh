@@ -273,7 +273,8 @@ struct TileArgs {
   u32 *hard;                // uncertified queries (original indices)
   u32 *hard_count;          // device counter (cleared by the caller)
   uint8_t *qlevel;          // per grid point: level at which it is still open
-  size_t n_max;             // size of qlevel
+  float *qtau;              // per grid point: K-th distance bound from the level below
+  size_t n_max;             // size of qlevel / qtau
 };
 // false if k has no tile instantiation (use grid_knn then)
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,

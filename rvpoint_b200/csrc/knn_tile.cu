@@ -42,7 +42,7 @@ __device__ __forceinline__ void list_insert(T (&L)[K], T key) {
 
 template <int K, int MODE>
 __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int level,
-                                                 uint8_t *qlevel, u32 *stats) {
+                                                 uint8_t *qlevel, float *qtau, u32 *stats) {
   using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
   __shared__ u32 c_start[NCELL];
   __shared__ u32 c_count[NCELL];
@@ -144,9 +144,30 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int lev
       for (int j = 0; j < K; ++j) L[j] = kMax;
       Key thr = kMax;
       u32 found = 0;
-      for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-          for (int dx = -1; dx <= 1; ++dx) {
+      // A query left open by the level below with K points found there
+      // carries tau >= its K-th distance: every point with d2 <= tau lies in
+      // the tight window of sqrt(tau) (at most the own cell +- 1 here, since
+      // sqrt(tau) < one cell of this level), so scanning that window with
+      // the bound tau is exact and needs no further check.
+      const float tb = level > 0 ? qtau[qi] : -1.0f;
+      bool bounded = tb >= 0.0f;
+      int lo[3] = {-1, -1, -1}, hi[3] = {1, 1, 1};
+      if (bounded) {
+        const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)tb), level);
+        const int own[3] = {lx + bx, ly + by, lz + bz};
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          lo[ax] = wt.lo[ax] - own[ax];
+          hi[ax] = wt.hi[ax] - own[ax];
+          if (lo[ax] < -1 || hi[ax] > 1) bounded = false;
+        }
+        if (!bounded)
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax) { lo[ax] = -1; hi[ax] = 1; }
+      }
+      for (int dz = lo[2]; dz <= hi[2]; ++dz)
+        for (int dy = lo[1]; dy <= hi[1]; ++dy)
+          for (int dx = lo[0]; dx <= hi[0]; ++dx) {
             const int c = ((lz + dz) * SIDE + (ly + dy)) * SIDE + (lx + dx);
             const u32 cnt = c_count[c];
             const u32 st = staged ? c_pref[c] : c_start[c];
@@ -154,8 +175,9 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int lev
               const float4 p = staged ? cand[st + j] : __ldg(&g.pts[st + j]);
               const u32 pidx = __float_as_uint(p.w);
               if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
-              ++found;
               const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+              if (bounded && !(d2 <= tb)) continue;
+              ++found;
               Key key;
               if constexpr (MODE == TILE_SOR_MEAN) key = d2;
               else key = pack_nbr(d2, (int)pidx);
@@ -165,9 +187,9 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int lev
               }
             }
           }
-      bool ok = false;
-      if (found >= (u32)K) {
-        float tau;
+      bool ok = bounded && found >= (u32)K;
+      float tau = -1.0f;
+      if (!ok && found >= (u32)K) {
         if constexpr (MODE == TILE_SOR_MEAN) tau = L[K - 1];
         else tau = nbr_d2(L[K - 1]);
         const Window w1 = ring_window(F, q.x, q.y, q.z, 1, level);
@@ -175,8 +197,12 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int lev
         ok = cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5);
       }
       if (!ok) {
-        if (level + 1 < kGridLevels) qlevel[qi] = (uint8_t)(level + 1);
-        else a.hard[atomicAdd(a.hard_count, 1u)] = qidx & 0x7FFFFFFFu;
+        if (level + 1 < kGridLevels) {
+          qlevel[qi] = (uint8_t)(level + 1);
+          qtau[qi] = tau;
+        } else {
+          a.hard[atomicAdd(a.hard_count, 1u)] = qidx & 0x7FFFFFFFu;
+        }
         continue;
       }
       if (stats) atomicAdd(stats, 1u);
@@ -209,11 +235,13 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
   for (int level = 0; level < kGridLevels; ++level) {
     u32 *st = stats ? stats + level : nullptr;
     if (mode == TILE_SOR_MEAN)
-      k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, st);
+      k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
+                                                                   st);
     else if (mode == TILE_NORMALS)
-      k_knn_tile<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, st);
+      k_knn_tile<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
+                                                                  st);
     else
-      k_knn_tile<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, st);
+      k_knn_tile<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau, st);
     RVP_LAUNCH_CHECK(ctx);
   }
 }
@@ -221,7 +249,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
 
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
                    int blocks, u32 *stats) {
-  if (g.mode != KEY_DENSE || !a.qlevel) return false;
+  if (g.mode != KEY_DENSE || !a.qlevel || !a.qtau) return false;
   if (blocks <= 0) blocks = ctx->num_sms * 8;
   switch (k) {
     case 8: launch_k<8>(ctx, g, mode, a, blocks, a.qlevel, stats); break;

@@ -41,6 +41,7 @@ struct rvp_pipeline {
   rvp::DevBuf stats;  // 16 kNN path counters (diagnostics)
   rvp::DevBuf hard;   // queries the tile kernel could not certify (+ counter)
   rvp::DevBuf qlevel; // per grid point: level at which its kNN is still open
+  rvp::DevBuf qtau;   // per grid point: K-th distance bound handed to the next level
   bool stats_on = false;
   int n_frames_last = 0;
   // stage timing: a ring of event sets, one set per run
@@ -152,6 +153,7 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->nrm_pairs.reserve(N * (size_t)kn * 8);
     p->hard.reserve(N * 4 + 256);
     p->qlevel.reserve(N);
+    p->qtau.reserve(N * 4);
     p->nrm_counts.reserve(N * 4);
     p->nx.reserve(N * 4); p->ny.reserve(N * 4); p->nz.reserve(N * 4);
     p->r_model.reserve((size_t)max_frames * 16);
@@ -183,7 +185,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel};
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau};
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
@@ -241,6 +243,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.hard = hard;
     ta.hard_count = hard_n;
     ta.qlevel = p->qlevel.as<uint8_t>();
+    ta.qtau = p->qtau.as<float>();
     ta.n_max = N;
     const bool tiled = c.queries_per_warp != 1;
     rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
