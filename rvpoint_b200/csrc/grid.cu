@@ -542,11 +542,18 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
       const Window w = tight_window(F, qx, qy, qz, (double)radius);
       knn_scan<P>(g, F, f, w, false, qx, qy, qz, K, bound_of(r2), L, found);
     } else {
-      // 1) rings of +- 1 cell, coarser (x4) while they hold fewer than K
+      // 0) a known bound: every point with d2 <= tb lies in the tight window
+      //    of sqrt(tb), and there are >= K of them -- scan it directly
+      const float tb = q.bound ? q.bound[wi] : -1.0f;
       Window wr = ring_window(F, qx, qy, qz, 1, 0);
-      knn_scan<P>(g, F, f, wr, false, qx, qy, qz, K, ~0ull - 1, L, found);
       int lvl = 0;
-      while (found < (u32)K && two_level && lvl + 1 < kGridLevels) {
+      if (tb >= 0.0f) {
+        found = 0;
+      } else {
+        // 1) rings of +- 1 cell, coarser (x4) while they hold fewer than K
+        knn_scan<P>(g, F, f, wr, false, qx, qy, qz, K, ~0ull - 1, L, found);
+      }
+      while (tb < 0.0f && found < (u32)K && two_level && lvl + 1 < kGridLevels) {
         ++lvl;
         wr = ring_window(F, qx, qy, qz, 1, lvl);
         L.init();
@@ -555,10 +562,12 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
       }
       path = lvl == 0 ? 0 : (lvl == 1 ? 2 : 3);
       bool done = false;
-      if (found >= (u32)K) {
-        const float tau = nbr_d2(L.get(K - 1));
-        const double cov = coverage(F, wr, qx, qy, qz);
-        if (cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5)) done = true;
+      if (found >= (u32)K || tb >= 0.0f) {
+        const float tau = tb >= 0.0f ? tb : nbr_d2(L.get(K - 1));
+        if (tb < 0.0f) {
+          const double cov = coverage(F, wr, qx, qy, qz);
+          if (cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5)) done = true;
+        }
         if (!done) {
           // 2) every point with d2 <= tau lies in the tight window of
           //    sqrt(tau) and there are >= K of them: exact. Scan it at the

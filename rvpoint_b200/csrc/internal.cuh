@@ -232,6 +232,7 @@ struct QuerySet {
   const u64 *n_dev;              // optional device count
   const int32_t *frame_of;       // optional: frame of each query (else 0)
   const int32_t *order;          // optional: process queries in this order
+  const float *bound = nullptr;  // optional, per slot: known d2 >= the K-th (< 0: none)
 };
 
 // radius search, two passes. counts[nq]; then offsets via scan; then fill.
@@ -272,6 +273,7 @@ struct TileArgs {
   int32_t *counts;
   u32 *hard;                // uncertified queries (original indices)
   u32 *hard_count;          // device counter (cleared by the caller)
+  float *hard_tau;          // per hard slot: K-th distance bound (< 0: none)
   uint8_t *qlevel;          // per grid point: level at which it is still open
   float *qtau;              // per grid point: K-th distance bound from the level below
   size_t n_max;             // size of qlevel / qtau

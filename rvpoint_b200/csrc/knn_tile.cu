@@ -30,6 +30,13 @@ constexpr int SIDE = 6;                      // staged fine cells per axis
 constexpr int NCELL = SIDE * SIDE * SIDE;    // 216
 constexpr int CAP = 2560;                    // staged candidates (40 KB)
 
+// the 27 ring cells, nearest first: own cell, 6 faces, 12 edges, 8 corners
+__constant__ signed char kRingOrder[27][3] = {
+    {0, 0, 0},   {-1, 0, 0},  {1, 0, 0},   {0, -1, 0},  {0, 1, 0},   {0, 0, -1},  {0, 0, 1},
+    {-1, -1, 0}, {1, -1, 0},  {-1, 1, 0},  {1, 1, 0},   {-1, 0, -1}, {1, 0, -1},  {-1, 0, 1},
+    {1, 0, 1},   {0, -1, -1}, {0, 1, -1},  {0, -1, 1},  {0, 1, 1},   {-1, -1, -1}, {1, -1, -1},
+    {-1, 1, -1}, {1, 1, -1},  {-1, -1, 1}, {1, -1, 1},  {-1, 1, 1},  {1, 1, 1}};
+
 template <class T, int K>
 __device__ __forceinline__ void list_insert(T (&L)[K], T key) {
 #pragma unroll
@@ -165,28 +172,59 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int lev
 #pragma unroll
           for (int ax = 0; ax < 3; ++ax) { lo[ax] = -1; hi[ax] = 1; }
       }
-      for (int dz = lo[2]; dz <= hi[2]; ++dz)
-        for (int dy = lo[1]; dy <= hi[1]; ++dy)
-          for (int dx = lo[0]; dx <= hi[0]; ++dx) {
-            const int c = ((lz + dz) * SIDE + (ly + dy)) * SIDE + (lx + dx);
-            const u32 cnt = c_count[c];
-            const u32 st = staged ? c_pref[c] : c_start[c];
-            for (u32 j = 0; j < cnt; ++j) {
-              const float4 p = staged ? cand[st + j] : __ldg(&g.pts[st + j]);
-              const u32 pidx = __float_as_uint(p.w);
-              if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
-              const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
-              if (bounded && !(d2 <= tb)) continue;
-              ++found;
-              Key key;
-              if constexpr (MODE == TILE_SOR_MEAN) key = d2;
-              else key = pack_nbr(d2, (int)pidx);
-              if (key < thr) {
-                list_insert<Key, K>(L, key);
-                thr = L[K - 1];
-              }
-            }
+      // distance from q to the faces of its own cell, shrunk by the rounding
+      // slack of the cell function: a point of a neighbour cell lies at least
+      // this far away along that axis
+      float gap_lo[3], gap_hi[3];
+      {
+        const float qq[3] = {q.x, q.y, q.z};
+        const float mn[3] = {F.min_x, F.min_y, F.min_z};
+        const int own[3] = {lx + bx, ly + by, lz + bz};
+        const double cs = (double)F.cell * (double)(1 << sh);
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          const double face0 = (double)mn[ax] + (double)own[ax] * cs;
+          const double slack = 2.4e-7 * (fabs((double)mn[ax]) + fabs((double)qq[ax]) +
+                                         (double)(own[ax] + 2) * cs) + 1e-30;
+          gap_lo[ax] = (float)fmax((double)qq[ax] - face0 - slack, 0.0);
+          gap_hi[ax] = (float)fmax(face0 + cs - (double)qq[ax] - slack, 0.0);
+        }
+      }
+      for (int t = 0; t < 27; ++t) {
+        const int dx = kRingOrder[t][0], dy = kRingOrder[t][1], dz = kRingOrder[t][2];
+        if (dx < lo[0] || dx > hi[0] || dy < lo[1] || dy > hi[1] || dz < lo[2] || dz > hi[2])
+          continue;
+        if (t > 0) {
+          // skip a cell that cannot hold anything below the current K-th
+          // distance (nothing is skipped until the list is full)
+          float thr_d2;
+          if constexpr (MODE == TILE_SOR_MEAN) thr_d2 = thr;
+          else thr_d2 = nbr_d2(thr);
+          const float gx = dx < 0 ? gap_lo[0] : (dx > 0 ? gap_hi[0] : 0.0f);
+          const float gy = dy < 0 ? gap_lo[1] : (dy > 0 ? gap_hi[1] : 0.0f);
+          const float gz = dz < 0 ? gap_lo[2] : (dz > 0 ? gap_hi[2] : 0.0f);
+          const float box2 = (gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f);
+          if (box2 > thr_d2) continue;
+        }
+        const int c = ((lz + dz) * SIDE + (ly + dy)) * SIDE + (lx + dx);
+        const u32 cnt = c_count[c];
+        const u32 st = staged ? c_pref[c] : c_start[c];
+        for (u32 j = 0; j < cnt; ++j) {
+          const float4 p = staged ? cand[st + j] : __ldg(&g.pts[st + j]);
+          const u32 pidx = __float_as_uint(p.w);
+          if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
+          const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+          if (bounded && !(d2 <= tb)) continue;
+          ++found;
+          Key key;
+          if constexpr (MODE == TILE_SOR_MEAN) key = d2;
+          else key = pack_nbr(d2, (int)pidx);
+          if (key < thr) {
+            list_insert<Key, K>(L, key);
+            thr = L[K - 1];
           }
+        }
+      }
       bool ok = bounded && found >= (u32)K;
       float tau = -1.0f;
       if (!ok && found >= (u32)K) {
@@ -201,7 +239,9 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int lev
           qlevel[qi] = (uint8_t)(level + 1);
           qtau[qi] = tau;
         } else {
-          a.hard[atomicAdd(a.hard_count, 1u)] = qidx & 0x7FFFFFFFu;
+          const u32 slot = atomicAdd(a.hard_count, 1u);
+          a.hard[slot] = qidx & 0x7FFFFFFFu;
+          if (a.hard_tau) a.hard_tau[slot] = tau;
         }
         continue;
       }

@@ -151,7 +151,7 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->sor_frame.reserve(N * 4);
     p->sor_src.reserve(N * 4);
     p->nrm_pairs.reserve(N * (size_t)kn * 8);
-    p->hard.reserve(N * 4 + 256);
+    p->hard.reserve(N * 8 + 256);
     p->qlevel.reserve(N);
     p->qtau.reserve(N * 4);
     p->nrm_counts.reserve(N * 4);
@@ -237,17 +237,20 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     u64 *hard_n64 = p->hard.as<u64>();                   // widened count (grid_knn)
     u32 *hard_n = reinterpret_cast<u32 *>(hard_n64 + 1);  // atomic counter
     u32 *hard = reinterpret_cast<u32 *>(hard_n64 + 2);    // original indices
+    float *hard_tau = reinterpret_cast<float *>(hard + N); // their K-th distance bounds
     u32 *st0 = p->stats_on ? p->stats.as<u32>() : nullptr;
     rvp::TileArgs ta{};
     ta.frame_of = p->vox_frame.as<int32_t>();
     ta.hard = hard;
     ta.hard_count = hard_n;
+    ta.hard_tau = hard_tau;
     ta.qlevel = p->qlevel.as<uint8_t>();
     ta.qtau = p->qtau.as<float>();
     ta.n_max = N;
     const bool tiled = c.queries_per_warp != 1;
     rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
                      hard_n64, p->vox_frame.as<int32_t>(), reinterpret_cast<int32_t *>(hard)};
+    qh.bound = tiled ? hard_tau : nullptr;
     rvp::QuerySet qv{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N, n_vox,
                      p->vox_frame.as<int32_t>(), nullptr};
     ta.mean = p->mean.as<float>();
@@ -299,8 +302,10 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     }
     k_widen<<<1, 32, 0, st>>>(hard_n, hard_n64);
     RVP_LAUNCH_CHECK(ctx);
-    rvp::grid_knn(ctx, gv, qh, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(), 1,
-                  c.block_threads, st0 ? st0 + 8 : nullptr, rvp::KNN_OUT_BY_SLOT, nullptr);
+    rvp::QuerySet qhn = qh;
+    qhn.bound = tn_ok ? hard_tau : nullptr;
+    rvp::grid_knn(ctx, gv, qhn, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(),
+                  1, c.block_threads, st0 ? st0 + 8 : nullptr, rvp::KNN_OUT_BY_SLOT, nullptr);
     p->mark(5);
     rvp::normals_from_lists(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
                             p->nrm_pairs.as<u64>(), nullptr, p->nrm_counts.as<int32_t>(), kn, N,
