@@ -268,11 +268,209 @@ __global__ __launch_bounds__(TT) void k_knn_tile(GridView g, TileArgs a, int lev
   }
 }
 
+// Level 0: one warp per fine cell of the group. Its lanes take the cell's
+// queries (32 at a time) and all walk the same 27-cell candidate stream, so
+// loop bounds are uniform and every candidate is one broadcast shared-memory
+// read; only the insertion into a lane's own list diverges.
+template <int K, int MODE>
+__global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile0(GridView g, TileArgs a, uint8_t *qlevel,
+                                                     float *qtau, u32 *stats) {
+  using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
+  __shared__ u32 c_start[NCELL];
+  __shared__ u32 c_count[NCELL];
+  __shared__ u32 c_pref[NCELL + 1];
+  __shared__ float4 cand[CAP];
+  __shared__ GridFrame s_F;
+  __shared__ int s_base[3];
+  __shared__ int s_staged;
+  const u64 ngroups = g.n_level[1];
+  const u32 *gstart = g.lstart[1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  Key kMax;
+  if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
+  else kMax = ~0ull;
+  for (u64 cb = blockIdx.x; cb < ngroups; cb += gridDim.x) {
+    __syncthreads();  // the previous group's shared memory is free
+    if (tid == 0) {
+      const float4 p0 = g.pts[gstart[cb]];
+      const u32 i0 = __float_as_uint(p0.w) & 0x7FFFFFFFu;
+      const GridFrame F = g.frames[a.frame_of ? a.frame_of[i0] : 0];
+      s_F = F;
+      s_base[0] = (cell_axis(p0.x, F.min_x, F.cell) >> 2) * 4 - 1;
+      s_base[1] = (cell_axis(p0.y, F.min_y, F.cell) >> 2) * 4 - 1;
+      s_base[2] = (cell_axis(p0.z, F.min_z, F.cell) >> 2) * 4 - 1;
+    }
+    __syncthreads();
+    {
+      const int bx = s_base[0], by = s_base[1], bz = s_base[2];
+      const int gx = s_F.gx, gy = s_F.gy, gz = s_F.gz;
+      for (int t = tid; t < NCELL; t += TT) {
+        const int cx = bx + t % SIDE, cy = by + (t / SIDE) % SIDE, cz = bz + t / (SIDE * SIDE);
+        u32 st = 0, ct = 0;
+        if (cx >= 0 && cy >= 0 && cz >= 0 && cx < gx && cy < gy && cz < gz)
+          if (!lookup(g, level_key(g, s_F, 0, cx, cy, cz), st, ct)) ct = 0;
+        c_start[t] = st;
+        c_count[t] = ct;
+      }
+    }
+    __syncthreads();
+    if (tid < 32) {
+      u32 run = 0;
+      for (int base = 0; base < NCELL; base += 32) {
+        const int t = base + tid;
+        const u32 v = t < NCELL ? c_count[t] : 0;
+        u32 incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const u32 u = __shfl_up_sync(0xffffffffu, incl, o);
+          if (tid >= o) incl += u;
+        }
+        if (t < NCELL) c_pref[t] = run + incl - v;
+        run += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (tid == 0) {
+        c_pref[NCELL] = run;
+        s_staged = run <= (u32)CAP ? 1 : 0;
+      }
+    }
+    __syncthreads();
+    const bool staged = s_staged != 0;
+    if (staged) {
+      const u32 total = c_pref[NCELL];
+      for (u32 i = tid; i < total; i += TT) {
+        int lo = 0, hi = NCELL - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (c_pref[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        cand[i] = __ldg(&g.pts[c_start[lo] + (i - c_pref[lo])]);
+      }
+    }
+    __syncthreads();
+    // the group's own 4 x 4 x 4 cells, one warp each
+    for (int oc = warp; oc < 64; oc += TT / 32) {
+      const int c = ((1 + (oc >> 4)) * SIDE + (1 + ((oc >> 2) & 3))) * SIDE + (1 + (oc & 3));
+      const u32 qn = c_count[c];
+      if (qn == 0) continue;
+      for (u32 q0 = 0; q0 < qn; q0 += 32) {
+        const u32 qj = q0 + lane;
+        const bool active = qj < qn;
+        float4 q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (active) q = staged ? cand[c_pref[c] + qj] : __ldg(&g.pts[c_start[c] + qj]);
+        const u32 qidx = __float_as_uint(q.w);
+        const bool live = active && !(MODE == TILE_NORMALS && (qidx & kRemovedBit));
+        if (!__any_sync(0xffffffffu, live)) continue;
+        // distance from q to its own cell's faces, less a generous rounding
+        // slack (pruning only: a pruned cell holds nothing below the K-th)
+        float glx, ghx, gly, ghy, glz, ghz;
+        {
+          const float cs = s_F.cell;
+          const int ox = s_base[0] + 1 + (oc & 3), oy = s_base[1] + 1 + ((oc >> 2) & 3),
+                    oz = s_base[2] + 1 + (oc >> 4);
+          const float fx = s_F.min_x + (float)ox * cs, fy = s_F.min_y + (float)oy * cs,
+                      fz = s_F.min_z + (float)oz * cs;
+          const float slx = 4e-6f * (fabsf(s_F.min_x) + fabsf(q.x) + (float)(ox + 2) * cs) + 1e-6f;
+          const float sly = 4e-6f * (fabsf(s_F.min_y) + fabsf(q.y) + (float)(oy + 2) * cs) + 1e-6f;
+          const float slz = 4e-6f * (fabsf(s_F.min_z) + fabsf(q.z) + (float)(oz + 2) * cs) + 1e-6f;
+          glx = fmaxf(q.x - fx - slx, 0.0f);
+          ghx = fmaxf(fx + cs - q.x - slx, 0.0f);
+          gly = fmaxf(q.y - fy - sly, 0.0f);
+          ghy = fmaxf(fy + cs - q.y - sly, 0.0f);
+          glz = fmaxf(q.z - fz - slz, 0.0f);
+          ghz = fmaxf(fz + cs - q.z - slz, 0.0f);
+        }
+        Key L[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) L[j] = kMax;
+        Key thr = kMax;
+        u32 found = 0;
+#pragma unroll 1
+        for (int t = 0; t < 27; ++t) {
+          const int dx = kRingOrder[t][0], dy = kRingOrder[t][1], dz = kRingOrder[t][2];
+          bool take = live;
+          if (t > 0) {
+            float thr_d2;
+            if constexpr (MODE == TILE_SOR_MEAN) thr_d2 = thr;
+            else thr_d2 = nbr_d2(thr);
+            const float gx = dx < 0 ? glx : (dx > 0 ? ghx : 0.0f);
+            const float gy = dy < 0 ? gly : (dy > 0 ? ghy : 0.0f);
+            const float gz = dz < 0 ? glz : (dz > 0 ? ghz : 0.0f);
+            take = take && !((gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) > thr_d2);
+          }
+          if (!__any_sync(0xffffffffu, take)) continue;
+          const int nc = c + (dz * SIDE + dy) * SIDE + dx;
+          const u32 cnt = c_count[nc];
+          const u32 st = staged ? c_pref[nc] : c_start[nc];
+          for (u32 j = 0; j < cnt; ++j) {
+            const float4 p = staged ? cand[st + j] : __ldg(&g.pts[st + j]);
+            const u32 pidx = __float_as_uint(p.w);
+            if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
+            const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+            if (take) {
+              ++found;
+              Key key;
+              if constexpr (MODE == TILE_SOR_MEAN) key = d2;
+              else key = pack_nbr(d2, (int)pidx);
+              if (key < thr) {
+                list_insert<Key, K>(L, key);
+                thr = L[K - 1];
+              }
+            }
+          }
+        }
+        if (!live) continue;
+        float tau = -1.0f;
+        bool ok = false;
+        if (found >= (u32)K) {
+          if constexpr (MODE == TILE_SOR_MEAN) tau = L[K - 1];
+          else tau = nbr_d2(L[K - 1]);
+          const GridFrame F = s_F;
+          const Window w1 = ring_window(F, q.x, q.y, q.z, 1, 0);
+          const double cov = coverage(F, w1, q.x, q.y, q.z);
+          ok = cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5);
+        }
+        const u32 pos = c_start[c] + qj;  // sorted position of the query
+        if (!ok) {
+          qlevel[pos] = 1;
+          qtau[pos] = tau;
+          continue;
+        }
+        if (stats) atomicAdd(stats, 1u);
+        if constexpr (MODE == TILE_SOR_MEAN) {
+          float sum = 0.0f;
+#pragma unroll
+          for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
+          a.mean[qidx] = fdiv(sum, (float)(K - 1));
+        } else if constexpr (MODE == TILE_NORMALS) {
+          float nx, ny, nz;
+          normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
+                              a.vpz, nx, ny, nz);
+          const u64 o = a.out_pos[qidx];
+          a.nx[o] = nx;
+          a.ny[o] = ny;
+          a.nz[o] = nz;
+        } else {
+#pragma unroll
+          for (int j = 0; j < K; ++j) a.pairs[(size_t)qidx * K + j] = L[j];
+          if (a.counts) a.counts[qidx] = K;
+        }
+      }
+    }
+  }
+}
+
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
               uint8_t *qlevel, u32 *stats) {
   RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
-  for (int level = 0; level < kGridLevels; ++level) {
+  if (mode == TILE_SOR_MEAN)
+    k_knn_tile0<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
+  else if (mode == TILE_NORMALS)
+    k_knn_tile0<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
+  else
+    k_knn_tile0<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
+  RVP_LAUNCH_CHECK(ctx);
+  for (int level = 1; level < kGridLevels; ++level) {
     u32 *st = stats ? stats + level : nullptr;
     if (mode == TILE_SOR_MEAN)
       k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
