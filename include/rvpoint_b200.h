@@ -227,6 +227,10 @@ RVP_API rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_of
  * was captured with. */
 RVP_API rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size,
                                            int block_threads, int queries_per_warp);
+/* First-pass search radius of the level-0 kNN tiles, as a factor of
+ * cell * sqrt(k / points in the query's cell) (0 disables the first pass;
+ * results never depend on it, only the work does). */
+RVP_API rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac);
 /* Stage timing with CUDA events on the context's stream: the next max_runs
  * runs record 8 events each (stage boundaries: voxel, grid build, SOR kNN,
  * SOR statistics, normals kNN, normals, RANSAC). rvp_pipeline_stage_times

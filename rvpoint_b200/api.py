@@ -496,6 +496,9 @@ class Pipeline:
         self.cfg.block_threads = block_threads
         self.cfg.queries_per_warp = queries_per_warp
 
+    def set_search_radius_factor(self, rfac: float) -> None:
+        check(self.L.rvp_pipeline_set_search_radius_factor(self.h, float(rfac)), self.ctx.h)
+
     def frame_offsets(self, n_frames: Optional[int] = None):
         """(voxel_offsets, sor_offsets) of the last run, as host int64 arrays."""
         nf = n_frames if n_frames is not None else self.last_frames

@@ -30,6 +30,7 @@ struct rvp_pipeline {
   size_t max_points = 0;
   int max_frames = 0;
   float cell = 0.0f;
+  float rfac = 0.9f;  // level-0 first-pass radius factor (tunable)
   rvp::VoxelWork vw;
   rvp::Grid grid;
   rvp::DevBuf in_x, in_y, in_z, in_offs;
@@ -246,6 +247,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.hard_tau = hard_tau;
     ta.qlevel = p->qlevel.as<uint8_t>();
     ta.qtau = p->qtau.as<float>();
+    ta.rfac = p->rfac;
     ta.n_max = N;
     const bool tiled = c.queries_per_warp != 1;
     rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
@@ -396,6 +398,12 @@ rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size, int block_t
   p->cfg.cell_size = cell_size;
   p->cfg.block_threads = block_threads;
   p->cfg.queries_per_warp = queries_per_warp;
+  return RVP_OK;
+}
+
+rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac) {
+  if (!p || !(rfac >= 0.0f)) return RVP_ERR_INVALID_ARG;
+  p->rfac = rfac;
   return RVP_OK;
 }
 

@@ -371,6 +371,19 @@ def test_pipeline_tile_and_warp_paths_agree(gpu_ctx):
     assert np.array_equal(a["ransac_count"], b["ransac_count"])
 
 
+def test_pipeline_search_radius_factor_does_not_change_results(gpu_ctx):
+    from rvpoint_b200 import api
+    batch = D.lidar_batch(n_frames=3, seed=17)
+    outs = []
+    for rf in (0.0, 0.6, 1.5):
+        p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, cell_size=0.5)
+        p.set_search_radius_factor(rf)
+        outs.append(p.run_host(batch))
+    for o in outs[1:]:
+        assert np.array_equal(bits(o["sor"]), bits(outs[0]["sor"]))
+        assert np.array_equal(bits(o["normals"]), bits(outs[0]["normals"]))
+
+
 @pytest.mark.parametrize("cell", [0.15, 0.3, 0.8])
 def test_pipeline_cell_size_does_not_change_results(gpu_ctx, restatement, cell):
     from rvpoint_b200 import api
