@@ -37,8 +37,9 @@ def _time_run(pipe, args, reps: int) -> float:
 
 def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
          cells: Optional[Iterable[float]] = None,
-         blocks: Iterable[int] = (128, 256),
-         qpws: Iterable[int] = (1,), reps: int = 2,
+         blocks: Iterable[int] = (256,),
+         qpws: Iterable[int] = (0,), rfacs: Iterable[float] = (0.7, 1.0),
+         reps: int = 2,
          cache_file: Optional[str] = None, verbose: bool = False) -> Tuple[dict, list]:
     """Returns (best setting, all trials) and applies the best to `pipe`."""
     sig = signature(n_points, n_frames, pipe.cfg)
@@ -50,22 +51,27 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
     if sig in _CACHE:
         b = _CACHE[sig]
         pipe.set_tuning(b["cell"], b["block"], b["qpw"])
+        pipe.set_search_radius_factor(b["rfac"])
         return b, []
     leaf = pipe.cfg.leaf_size
-    cells = list(cells) if cells is not None else [leaf * m for m in (1.5, 2.0, 2.5, 3.0, 4.0)]
+    cells = list(cells) if cells is not None else [leaf * m for m in (3.0, 5.0, 8.0, 12.0)]
     args = (x, y, z, offsets, n_frames, n_points)
     trials = []
     for c in cells:
         for b in blocks:
             for q in qpws:
-                pipe.set_tuning(c, b, q)
-                pipe.run_device(*args)  # warm
-                t = _time_run(pipe, args, reps)
-                trials.append({"cell": c, "block": b, "qpw": q, "ms": t})
-                if verbose:
-                    print(f"[autotune] cell={c:.3f} block={b} qpw={q}: {t:.3f} ms", flush=True)
+                for rf in rfacs:
+                    pipe.set_tuning(c, b, q)
+                    pipe.set_search_radius_factor(rf)
+                    pipe.run_device(*args)  # warm
+                    t = _time_run(pipe, args, reps)
+                    trials.append({"cell": c, "block": b, "qpw": q, "rfac": rf, "ms": t})
+                    if verbose:
+                        print(f"[autotune] cell={c:.3f} block={b} qpw={q} rfac={rf}: {t:.3f} ms",
+                              flush=True)
     best = min(trials, key=lambda r: r["ms"])
     pipe.set_tuning(best["cell"], best["block"], best["qpw"])
+    pipe.set_search_radius_factor(best["rfac"])
     _CACHE[sig] = best
     if cache_file:
         try:

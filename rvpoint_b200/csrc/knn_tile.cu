@@ -186,10 +186,13 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
             float thr_d2;
             if constexpr (MODE == TILE_SOR_MEAN) thr_d2 = thr;
             else thr_d2 = nbr_d2(thr);
+            if (bounded) thr_d2 = fminf(thr_d2, tb);
             const float gx = dx < 0 ? glx : (dx > 0 ? ghx : 0.0f);
             const float gy = dy < 0 ? gly : (dy > 0 ? ghy : 0.0f);
             const float gz = dz < 0 ? glz : (dz > 0 ? ghz : 0.0f);
             if ((gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) > thr_d2) continue;
+            // (a bounded pass never needs a point beyond tb; fminf keeps NaN
+            // from an unfilled u64 list out of the comparison)
           }
           const int c = ((lz + dz) * SIDE + (ly + dy)) * SIDE + (lx + dx);
           const u32 cnt = c_count[c];
