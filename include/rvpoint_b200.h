@@ -159,6 +159,29 @@ RVP_API rvp_status rvp_extract_plane(rvp_context *ctx, const float *x, const flo
                              float *outliers_aos, size_t *n_inliers,
                              size_t *n_outliers);
 
+/* Largest cloud rvp_extract_plane_noalloc accepts. */
+#define RVP_NOALLOC_MAX_POINTS 16777216
+
+/* Inlier / outlier split of rvp_extract_plane for callers that cannot
+ * allocate device memory at call time (a control loop that forbids
+ * allocation once it runs, a host framework that owns every device
+ * allocation). No counterpart in the reference. It allocates nothing: its
+ * only scratch, one count per 2048 points (32 KB), is a fixed array inside
+ * the library that every GPU loading the library keeps until exit and that
+ * all calls on a device share -- calls that run on the GPU at the same time
+ * race on it. All pointers are device memory: x, y, z (n floats), model
+ * (4 floats), inliers_aos / outliers_aos (3 * n floats each, either may be
+ * NULL), counts (2 uint64: inliers, outliers). Asynchronous on the context's
+ * stream. The first call on a device looks up the array's device address;
+ * make that first call before any stream capture. n above
+ * RVP_NOALLOC_MAX_POINTS returns RVP_ERR_INVALID_ARG and launches nothing;
+ * errors are reported by the status only (rvp_last_error is not updated). */
+RVP_API rvp_status rvp_extract_plane_noalloc(rvp_context *ctx, const float *x,
+                                             const float *y, const float *z,
+                                             size_t n, const float *model,
+                                             float dist_thresh, float *inliers_aos,
+                                             float *outliers_aos, uint64_t *counts);
+
 /* ---- batched frames (no single reference counterpart: the chain
  *      voxel_grid_downsamp_rvv_v2 -> sor_rvv -> normal_estimation_sc ->
  *      ransac_plane_rvv of tools/pipeline_export.cpp:351-498, per frame) --- */

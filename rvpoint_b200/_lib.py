@@ -80,6 +80,7 @@ SIGNATURES = {
     "rvp_normals_knn_precise": (I, [P, P, P, P, SZ, I, F, F, F, C.c_double, I, P, P, P, P, P]),
     "rvp_ransac_plane": (I, [P, P, P, P, SZ, F, I, F, F, P, I, P, C.POINTER(I), C.POINTER(I), P]),
     "rvp_extract_plane": (I, [P, P, P, P, SZ, P, F, I, P, P, C.POINTER(SZ), C.POINTER(SZ)]),
+    "rvp_extract_plane_noalloc": (I, [P, P, P, P, SZ, P, F, P, P, P]),
     "rvp_pipeline_create": (I, [P, C.POINTER(PipelineConfig), SZ, I, C.POINTER(P)]),
     "rvp_pipeline_destroy": (I, [P]),
     "rvp_pipeline_run_device": (I, [P, P, P, P, P, I, SZ]),
