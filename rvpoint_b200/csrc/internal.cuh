@@ -277,6 +277,7 @@ struct TileArgs {
   uint8_t *qlevel;          // per grid point: level at which it is still open
   float *qtau;              // per grid point: K-th distance bound from the level below
   float rfac;               // level-0 first-pass radius = rfac * cell * sqrt(K / own-cell count)
+  int level0_warp;          // level 0 by the barrier-free per-warp kernel
   size_t n_max;             // size of qlevel / qtau
 };
 // false if k has no tile instantiation (use grid_knn then)

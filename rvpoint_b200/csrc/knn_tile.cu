@@ -285,11 +285,198 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
   }
 }
 
+// Level 0 without block barriers: each warp takes 32 consecutive grid points
+// (cell-sorted, so spatially coherent) as queries, looks up the union of their
+// 27-cell rings once into a small per-warp table in shared memory (lanes in
+// parallel), and every lane then walks its own ring, reading candidates
+// through L1 (lanes of a cell read the same addresses). Warps never wait for
+// each other, so one slow query only holds its own warp.
+constexpr int WT_CELLS = 64;
+constexpr int WT_WARPS = TT / 32;
+
+template <int K, int MODE>
+__global__ __launch_bounds__(TT, 3) void k_knn_wt0(
+    GridView g, TileArgs a, uint8_t *qlevel, float *qtau, u32 *stats) {
+  using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
+  __shared__ uint2 wtab[WT_WARPS][WT_CELLS];
+  const u64 n = *g.n_points;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const u64 nwarps = (u64)gridDim.x * WT_WARPS;
+  Key kMax;
+  if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
+  else kMax = ~0ull;
+  for (u64 base = ((u64)blockIdx.x * WT_WARPS + wib) * 32; base < n; base += nwarps * 32) {
+    const u64 pos = base + lane;
+    const bool active = pos < n;
+    const float4 q = active ? g.pts[pos] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const u32 qidx = __float_as_uint(q.w);
+    const bool live = active && !(MODE == TILE_NORMALS && (qidx & kRemovedBit));
+    const int f = active ? (a.frame_of ? a.frame_of[qidx & 0x7FFFFFFFu] : 0) : -1;
+    const int f0 = __shfl_sync(0xffffffffu, f, 0);  // lane 0 is always active
+    const bool one_frame = __all_sync(0xffffffffu, !active || f == f0);
+    const GridFrame F = g.frames[active ? f : f0];
+    const int cx = cell_axis(q.x, F.min_x, F.cell), cy = cell_axis(q.y, F.min_y, F.cell),
+              cz = cell_axis(q.z, F.min_z, F.cell);
+    // union of the lanes' rings, clamped to the grid
+    int bx0 = __reduce_min_sync(0xffffffffu, active ? cx : 0x7FFFFFFF) - 1;
+    int by0 = __reduce_min_sync(0xffffffffu, active ? cy : 0x7FFFFFFF) - 1;
+    int bz0 = __reduce_min_sync(0xffffffffu, active ? cz : 0x7FFFFFFF) - 1;
+    int bx1 = __reduce_max_sync(0xffffffffu, active ? cx : (int)0x80000000) + 1;
+    int by1 = __reduce_max_sync(0xffffffffu, active ? cy : (int)0x80000000) + 1;
+    int bz1 = __reduce_max_sync(0xffffffffu, active ? cz : (int)0x80000000) + 1;
+    bx0 = max(bx0, 0); by0 = max(by0, 0); bz0 = max(bz0, 0);
+    bx1 = min(bx1, F.gx - 1); by1 = min(by1, F.gy - 1); bz1 = min(bz1, F.gz - 1);
+    const int wx = bx1 - bx0 + 1, wy = by1 - by0 + 1, wz = bz1 - bz0 + 1;
+    const bool use_tab = one_frame && wx > 0 && wy > 0 && wz > 0 && wx * wy * wz <= WT_CELLS;
+    if (use_tab) {
+      for (int t = lane; t < wx * wy * wz; t += 32) {
+        const int ux = bx0 + t % wx, uy = by0 + (t / wx) % wy, uz = bz0 + t / (wx * wy);
+        u32 st = 0, ct = 0;
+        if (!lookup(g, fine_key(g, F, ux, uy, uz), st, ct)) ct = 0;
+        wtab[wib][t] = make_uint2(st, ct);
+      }
+    }
+    __syncwarp();
+    if (live) {
+      auto cell_run = [&](int ux, int uy, int uz, u32 &st, u32 &ct) {
+        if (ux < 0 || uy < 0 || uz < 0 || ux >= F.gx || uy >= F.gy || uz >= F.gz) {
+          ct = 0;
+          return;
+        }
+        if (use_tab) {
+          const uint2 e = wtab[wib][((uz - bz0) * wy + (uy - by0)) * wx + (ux - bx0)];
+          st = e.x;
+          ct = e.y;
+        } else if (!lookup(g, fine_key(g, F, ux, uy, uz), st, ct)) {
+          ct = 0;
+        }
+      };
+      float glx, ghx, gly, ghy, glz, ghz;
+      {
+        const float cs = F.cell;
+        const float fx = F.min_x + (float)cx * cs, fy = F.min_y + (float)cy * cs,
+                    fz = F.min_z + (float)cz * cs;
+        const float slx = 4e-6f * (fabsf(F.min_x) + fabsf(q.x) + (float)(cx + 2) * cs) + 1e-6f;
+        const float sly = 4e-6f * (fabsf(F.min_y) + fabsf(q.y) + (float)(cy + 2) * cs) + 1e-6f;
+        const float slz = 4e-6f * (fabsf(F.min_z) + fabsf(q.z) + (float)(cz + 2) * cs) + 1e-6f;
+        glx = fmaxf(q.x - fx - slx, 0.0f);
+        ghx = fmaxf(fx + cs - q.x - slx, 0.0f);
+        gly = fmaxf(q.y - fy - sly, 0.0f);
+        ghy = fmaxf(fy + cs - q.y - sly, 0.0f);
+        glz = fmaxf(q.z - fz - slz, 0.0f);
+        ghz = fmaxf(fz + cs - q.z - slz, 0.0f);
+      }
+      Key L[K];
+      Key thr = kMax;
+      u32 found = 0;
+      auto scan = [&](int lox, int hix, int loy, int hiy, int loz, int hiz, bool bounded,
+                      float tb) {
+#pragma unroll
+        for (int j = 0; j < K; ++j) L[j] = kMax;
+        thr = kMax;
+        found = 0;
+        for (int t = 0; t < 27; ++t) {
+          const int dx = kRingOrder[t][0], dy = kRingOrder[t][1], dz = kRingOrder[t][2];
+          if (dx < lox || dx > hix || dy < loy || dy > hiy || dz < loz || dz > hiz) continue;
+          if (t > 0) {
+            float thr_d2;
+            if constexpr (MODE == TILE_SOR_MEAN) thr_d2 = thr;
+            else thr_d2 = nbr_d2(thr);
+            if (bounded) thr_d2 = fminf(thr_d2, tb);
+            const float gx = dx < 0 ? glx : (dx > 0 ? ghx : 0.0f);
+            const float gy = dy < 0 ? gly : (dy > 0 ? ghy : 0.0f);
+            const float gz = dz < 0 ? glz : (dz > 0 ? ghz : 0.0f);
+            if ((gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) > thr_d2) continue;
+          }
+          u32 st, cnt;
+          cell_run(cx + dx, cy + dy, cz + dz, st, cnt);
+          for (u32 j = 0; j < cnt; ++j) {
+            const float4 p = __ldg(&g.pts[st + j]);
+            const u32 pidx = __float_as_uint(p.w);
+            if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
+            const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+            if (bounded && !(d2 <= tb)) continue;
+            ++found;
+            Key key;
+            if constexpr (MODE == TILE_SOR_MEAN) key = d2;
+            else key = pack_nbr(d2, (int)pidx);
+            if (key < thr) {
+              list_insert<Key, K>(L, key);
+              thr = L[K - 1];
+            }
+          }
+        }
+      };
+      bool ok = false;
+      if (a.rfac > 0.0f) {
+        u32 st0, n_own;
+        cell_run(cx, cy, cz, st0, n_own);
+        const float r = fminf(a.rfac * F.cell * sqrtf((float)K / (float)max(n_own, 1u)),
+                              0.999f * F.cell);
+        const float tb = r * r;
+        const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)tb), 0);
+        const int lox = wt.lo[0] - cx, hix = wt.hi[0] - cx, loy = wt.lo[1] - cy,
+                  hiy = wt.hi[1] - cy, loz = wt.lo[2] - cz, hiz = wt.hi[2] - cz;
+        if (lox >= -1 && hix <= 1 && loy >= -1 && hiy <= 1 && loz >= -1 && hiz <= 1) {
+          scan(lox, hix, loy, hiy, loz, hiz, true, tb);
+          ok = found >= (u32)K;
+        }
+      }
+      float tau = -1.0f;
+      if (!ok) {
+        scan(-1, 1, -1, 1, -1, 1, false, 0.0f);
+        if (found >= (u32)K) {
+          if constexpr (MODE == TILE_SOR_MEAN) tau = L[K - 1];
+          else tau = nbr_d2(L[K - 1]);
+          const Window w1 = ring_window(F, q.x, q.y, q.z, 1, 0);
+          const double cov = coverage(F, w1, q.x, q.y, q.z);
+          ok = cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5);
+        }
+      }
+      if (!ok) {
+        qlevel[pos] = 1;
+        qtau[pos] = tau;
+      } else {
+        if (stats) atomicAdd(stats, 1u);
+        if constexpr (MODE == TILE_SOR_MEAN) {
+          float sum = 0.0f;
+#pragma unroll
+          for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
+          a.mean[qidx] = fdiv(sum, (float)(K - 1));
+        } else if constexpr (MODE == TILE_NORMALS) {
+          float nx, ny, nz;
+          normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
+                              a.vpz, nx, ny, nz);
+          const u64 o = a.out_pos[qidx];
+          a.nx[o] = nx;
+          a.ny[o] = ny;
+          a.nz[o] = nz;
+        } else {
+#pragma unroll
+          for (int j = 0; j < K; ++j) a.pairs[(size_t)qidx * K + j] = L[j];
+          if (a.counts) a.counts[qidx] = K;
+        }
+      }
+    }
+    __syncwarp();  // the warp's table is reused by its next 32 queries
+  }
+}
+
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
               uint8_t *qlevel, u32 *stats) {
   RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
-  for (int level = 0; level < kGridLevels; ++level) {
+  if (a.level0_warp) {
+    const int wblocks = ctx->num_sms * 3 * 4;
+    if (mode == TILE_SOR_MEAN)
+      k_knn_wt0<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
+    else if (mode == TILE_NORMALS)
+      k_knn_wt0<K, TILE_NORMALS><<<wblocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
+    else
+      k_knn_wt0<K, TILE_PAIRS><<<wblocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
+    RVP_LAUNCH_CHECK(ctx);
+  }
+  for (int level = a.level0_warp ? 1 : 0; level < kGridLevels; ++level) {
     u32 *st = stats ? stats + level : nullptr;
     if (mode == TILE_SOR_MEAN)
       k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,

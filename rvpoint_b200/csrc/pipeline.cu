@@ -248,6 +248,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.qlevel = p->qlevel.as<uint8_t>();
     ta.qtau = p->qtau.as<float>();
     ta.rfac = p->rfac;
+    ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles at level 0 too
     ta.n_max = N;
     const bool tiled = c.queries_per_warp != 1;
     rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
