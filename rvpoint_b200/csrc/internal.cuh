@@ -277,7 +277,12 @@ struct TileArgs {
   uint8_t *qlevel;          // per grid point: level at which it is still open
   float *qtau;              // per grid point: K-th distance bound from the level below
   float rfac;               // level-0 first-pass radius = rfac * cell * sqrt(K / own-cell count)
-  int level0_warp;          // level 0 by the barrier-free per-warp kernel
+  int level0_warp;          // every level by the barrier-free per-warp kernel
+  u32 *open_flags;          // n_max: open-query flags of a level
+  u64 *open_pos;            // n_max + 1: their exclusive scan
+  u32 *open_list;           // n_max: open queries in grid order
+  u64 *open_n;              // device count of open_list
+  void *scan_tmp;           // scan_temp_bytes(n_max)
   size_t n_max;             // size of qlevel / qtau
 };
 // false if k has no tile instantiation (use grid_knn then)

@@ -285,29 +285,37 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
   }
 }
 
-// Level 0 without block barriers: each warp takes 32 consecutive grid points
-// (cell-sorted, so spatially coherent) as queries, looks up the union of their
-// 27-cell rings once into a small per-warp table in shared memory (lanes in
-// parallel), and every lane then walks its own ring, reading candidates
-// through L1 (lanes of a cell read the same addresses). Warps never wait for
-// each other, so one slow query only holds its own warp.
+// Per-warp kNN without block barriers, one level at a time. Each warp takes
+// 32 consecutive queries in cell order -- at level 0 every grid point, at
+// level L > 0 the compacted list of queries the level below left open --
+// looks up the union of their 27-cell rings (level-L cells) once into a
+// small per-warp table in shared memory (lanes in parallel), and every lane
+// then walks its own ring, reading candidates through L1 (lanes of one cell
+// read the same addresses). Warps never wait for each other, so one slow
+// query only holds its own warp. A query open with a bound tau from the level
+// below scans only the tight window of sqrt(tau) (exact with the bound); at
+// level 0 a first pass uses a radius estimated from the own cell's
+// occupancy. A ring that cannot certify the K-th distance leaves the query
+// open for the next level, with tau when K points were found.
 constexpr int WT_CELLS = 64;
 constexpr int WT_WARPS = TT / 32;
 
 template <int K, int MODE>
-__global__ __launch_bounds__(TT, 3) void k_knn_wt0(
-    GridView g, TileArgs a, uint8_t *qlevel, float *qtau, u32 *stats) {
+__global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int level,
+                                                  const u32 *list, const u64 *n_list,
+                                                  uint8_t *qlevel, float *qtau, u32 *stats) {
   using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
   __shared__ uint2 wtab[WT_WARPS][WT_CELLS];
-  const u64 n = *g.n_points;
+  const u64 n = list ? *n_list : *g.n_points;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const u64 nwarps = (u64)gridDim.x * WT_WARPS;
+  const int sh = 2 * level;
   Key kMax;
   if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
   else kMax = ~0ull;
   for (u64 base = ((u64)blockIdx.x * WT_WARPS + wib) * 32; base < n; base += nwarps * 32) {
-    const u64 pos = base + lane;
-    const bool active = pos < n;
+    const bool active = base + lane < n;
+    const u64 pos = active ? (list ? (u64)list[base + lane] : base + lane) : 0;
     const float4 q = active ? g.pts[pos] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const u32 qidx = __float_as_uint(q.w);
     const bool live = active && !(MODE == TILE_NORMALS && (qidx & kRemovedBit));
@@ -315,8 +323,11 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt0(
     const int f0 = __shfl_sync(0xffffffffu, f, 0);  // lane 0 is always active
     const bool one_frame = __all_sync(0xffffffffu, !active || f == f0);
     const GridFrame F = g.frames[active ? f : f0];
-    const int cx = cell_axis(q.x, F.min_x, F.cell), cy = cell_axis(q.y, F.min_y, F.cell),
-              cz = cell_axis(q.z, F.min_z, F.cell);
+    const int GX = level_dim(F.gx, level), GY = level_dim(F.gy, level),
+              GZ = level_dim(F.gz, level);
+    const int cx = cell_axis(q.x, F.min_x, F.cell) >> sh,
+              cy = cell_axis(q.y, F.min_y, F.cell) >> sh,
+              cz = cell_axis(q.z, F.min_z, F.cell) >> sh;
     // union of the lanes' rings, clamped to the grid
     int bx0 = __reduce_min_sync(0xffffffffu, active ? cx : 0x7FFFFFFF) - 1;
     int by0 = __reduce_min_sync(0xffffffffu, active ? cy : 0x7FFFFFFF) - 1;
@@ -325,21 +336,21 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt0(
     int by1 = __reduce_max_sync(0xffffffffu, active ? cy : (int)0x80000000) + 1;
     int bz1 = __reduce_max_sync(0xffffffffu, active ? cz : (int)0x80000000) + 1;
     bx0 = max(bx0, 0); by0 = max(by0, 0); bz0 = max(bz0, 0);
-    bx1 = min(bx1, F.gx - 1); by1 = min(by1, F.gy - 1); bz1 = min(bz1, F.gz - 1);
+    bx1 = min(bx1, GX - 1); by1 = min(by1, GY - 1); bz1 = min(bz1, GZ - 1);
     const int wx = bx1 - bx0 + 1, wy = by1 - by0 + 1, wz = bz1 - bz0 + 1;
     const bool use_tab = one_frame && wx > 0 && wy > 0 && wz > 0 && wx * wy * wz <= WT_CELLS;
     if (use_tab) {
       for (int t = lane; t < wx * wy * wz; t += 32) {
         const int ux = bx0 + t % wx, uy = by0 + (t / wx) % wy, uz = bz0 + t / (wx * wy);
         u32 st = 0, ct = 0;
-        if (!lookup(g, fine_key(g, F, ux, uy, uz), st, ct)) ct = 0;
+        if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, ct)) ct = 0;
         wtab[wib][t] = make_uint2(st, ct);
       }
     }
     __syncwarp();
     if (live) {
       auto cell_run = [&](int ux, int uy, int uz, u32 &st, u32 &ct) {
-        if (ux < 0 || uy < 0 || uz < 0 || ux >= F.gx || uy >= F.gy || uz >= F.gz) {
+        if (ux < 0 || uy < 0 || uz < 0 || ux >= GX || uy >= GY || uz >= GZ) {
           ct = 0;
           return;
         }
@@ -347,13 +358,13 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt0(
           const uint2 e = wtab[wib][((uz - bz0) * wy + (uy - by0)) * wx + (ux - bx0)];
           st = e.x;
           ct = e.y;
-        } else if (!lookup(g, fine_key(g, F, ux, uy, uz), st, ct)) {
+        } else if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, ct)) {
           ct = 0;
         }
       };
       float glx, ghx, gly, ghy, glz, ghz;
       {
-        const float cs = F.cell;
+        const float cs = F.cell * (float)(1 << sh);
         const float fx = F.min_x + (float)cx * cs, fy = F.min_y + (float)cy * cs,
                     fz = F.min_z + (float)cz * cs;
         const float slx = 4e-6f * (fabsf(F.min_x) + fabsf(q.x) + (float)(cx + 2) * cs) + 1e-6f;
@@ -407,14 +418,21 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt0(
           }
         }
       };
-      bool ok = false;
-      if (a.rfac > 0.0f) {
+      // first pass with a bound: the level below's tau, or at level 0 a
+      // radius from the own cell's occupancy (kept under one cell)
+      float tb = -1.0f;
+      if (level > 0) {
+        tb = qtau[pos];
+      } else if (a.rfac > 0.0f) {
         u32 st0, n_own;
         cell_run(cx, cy, cz, st0, n_own);
         const float r = fminf(a.rfac * F.cell * sqrtf((float)K / (float)max(n_own, 1u)),
                               0.999f * F.cell);
-        const float tb = r * r;
-        const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)tb), 0);
+        tb = r * r;
+      }
+      bool ok = false;
+      if (tb >= 0.0f) {
+        const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)tb), level);
         const int lox = wt.lo[0] - cx, hix = wt.hi[0] - cx, loy = wt.lo[1] - cy,
                   hiy = wt.hi[1] - cy, loz = wt.lo[2] - cz, hiz = wt.hi[2] - cz;
         if (lox >= -1 && hix <= 1 && loy >= -1 && hiy <= 1 && loz >= -1 && hiz <= 1) {
@@ -428,14 +446,20 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt0(
         if (found >= (u32)K) {
           if constexpr (MODE == TILE_SOR_MEAN) tau = L[K - 1];
           else tau = nbr_d2(L[K - 1]);
-          const Window w1 = ring_window(F, q.x, q.y, q.z, 1, 0);
+          const Window w1 = ring_window(F, q.x, q.y, q.z, 1, level);
           const double cov = coverage(F, w1, q.x, q.y, q.z);
           ok = cov > 0.0 && (double)tau < cov * cov * (1.0 - 1e-5);
         }
       }
       if (!ok) {
-        qlevel[pos] = 1;
-        qtau[pos] = tau;
+        if (level + 1 < kGridLevels) {
+          qlevel[pos] = (uint8_t)(level + 1);
+          qtau[pos] = tau;
+        } else {
+          const u32 slot = atomicAdd(a.hard_count, 1u);
+          a.hard[slot] = qidx & 0x7FFFFFFFu;
+          if (a.hard_tau) a.hard_tau[slot] = tau;
+        }
       } else {
         if (stats) atomicAdd(stats, 1u);
         if constexpr (MODE == TILE_SOR_MEAN) {
@@ -462,21 +486,55 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt0(
   }
 }
 
+// open queries of `level`, in grid (cell) order: flags -> scan -> positions
+__global__ void k_open_flags(const uint8_t *qlevel, const u64 *n_dev, int level, u32 *flags) {
+  const u64 n = *n_dev;
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    flags[i] = qlevel[i] == level ? 1u : 0u;
+}
+__global__ void k_open_scatter(const u32 *flags, const u64 *pos, const u64 *n_dev, u32 *list,
+                               u64 *n_list) {
+  const u64 n = *n_dev;
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    if (flags[i]) list[pos[i]] = (u32)i;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_list = pos[n];
+}
+
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
               uint8_t *qlevel, u32 *stats) {
   RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
   if (a.level0_warp) {
+    // barrier-free per-warp kernels at every level; levels > 0 read the
+    // compacted list of open queries
     const int wblocks = ctx->num_sms * 3 * 4;
-    if (mode == TILE_SOR_MEAN)
-      k_knn_wt0<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
-    else if (mode == TILE_NORMALS)
-      k_knn_wt0<K, TILE_NORMALS><<<wblocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
-    else
-      k_knn_wt0<K, TILE_PAIRS><<<wblocks, TT, 0, ctx->stream>>>(g, a, qlevel, a.qtau, stats);
-    RVP_LAUNCH_CHECK(ctx);
+    for (int level = 0; level < kGridLevels; ++level) {
+      const u32 *list = nullptr;
+      if (level > 0) {
+        const unsigned gb = grid_for(a.n_max, 256, ctx->num_sms * 16);
+        k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, level, a.open_flags);
+        RVP_LAUNCH_CHECK(ctx);
+        exclusive_scan_u32_to_u64(ctx, a.open_flags, a.open_pos, a.n_max, g.n_points, a.scan_tmp);
+        k_open_scatter<<<gb, 256, 0, ctx->stream>>>(a.open_flags, a.open_pos, g.n_points,
+                                                    a.open_list, a.open_n);
+        RVP_LAUNCH_CHECK(ctx);
+        list = a.open_list;
+      }
+      u32 *st = stats ? stats + level : nullptr;
+      if (mode == TILE_SOR_MEAN)
+        k_knn_wt<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
+                                                                    qlevel, a.qtau, st);
+      else if (mode == TILE_NORMALS)
+        k_knn_wt<K, TILE_NORMALS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
+                                                                   qlevel, a.qtau, st);
+      else
+        k_knn_wt<K, TILE_PAIRS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
+                                                                 qlevel, a.qtau, st);
+      RVP_LAUNCH_CHECK(ctx);
+    }
+    return;
   }
-  for (int level = a.level0_warp ? 1 : 0; level < kGridLevels; ++level) {
+  for (int level = 0; level < kGridLevels; ++level) {
     u32 *st = stats ? stats + level : nullptr;
     if (mode == TILE_SOR_MEAN)
       k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,

@@ -43,6 +43,7 @@ struct rvp_pipeline {
   rvp::DevBuf hard;   // queries the tile kernel could not certify (+ counter)
   rvp::DevBuf qlevel; // per grid point: level at which its kNN is still open
   rvp::DevBuf qtau;   // per grid point: K-th distance bound handed to the next level
+  rvp::DevBuf open;   // open-query compaction between levels (flags, scan, list)
   bool stats_on = false;
   int n_frames_last = 0;
   // stage timing: a ring of event sets, one set per run
@@ -155,6 +156,8 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->hard.reserve(N * 8 + 256);
     p->qlevel.reserve(N);
     p->qtau.reserve(N * 4);
+    p->open.reserve(((N * 4 + 255) & ~(size_t)255) + ((N * 8 + 8 + 255) & ~(size_t)255) +
+                    ((N * 4 + 255) & ~(size_t)255) + 256 + rvp::scan_temp_bytes(N));
     p->nrm_counts.reserve(N * 4);
     p->nx.reserve(N * 4); p->ny.reserve(N * 4); p->nz.reserve(N * 4);
     p->r_model.reserve((size_t)max_frames * 16);
@@ -186,7 +189,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau};
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau, &p->open};
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
@@ -248,7 +251,16 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.qlevel = p->qlevel.as<uint8_t>();
     ta.qtau = p->qtau.as<float>();
     ta.rfac = p->rfac;
-    ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles at level 0 too
+    ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles instead
+    {
+      char *op = p->open.as<char>();
+      auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+      ta.open_flags = reinterpret_cast<u32 *>(op); op += al(N * 4);
+      ta.open_pos = reinterpret_cast<u64 *>(op); op += al(N * 8 + 8);
+      ta.open_list = reinterpret_cast<u32 *>(op); op += al(N * 4);
+      ta.open_n = reinterpret_cast<u64 *>(op); op += 256;
+      ta.scan_tmp = op;
+    }
     ta.n_max = N;
     const bool tiled = c.queries_per_warp != 1;
     rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
