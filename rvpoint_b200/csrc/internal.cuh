@@ -283,12 +283,6 @@ struct TileArgs {
   u32 *open_list;           // n_max: open queries in grid order
   u64 *open_n;              // device count of open_list
   void *scan_tmp;           // scan_temp_bytes(n_max)
-  // whole-frame pass for the queries no level certified (optional)
-  int n_frames;
-  u32 *frame_cnt;           // n_frames
-  u32 *frame_start;         // n_frames + 1
-  u32 *by_frame;            // n_max
-  const float *qx, *qy, *qz;  // query coordinates by original index (SOR / pairs)
   size_t n_max;             // size of qlevel / qtau
 };
 // false if k has no tile instantiation (use grid_knn then)

@@ -500,129 +500,6 @@ __global__ void k_open_scatter(const u32 *flags, const u64 *pos, const u64 *n_de
   if (blockIdx.x == 0 && threadIdx.x == 0) *n_list = pos[n];
 }
 
-// Last resort for the queries no level certified (isolated points with fewer
-// than K neighbours within their widest ring): one block per frame takes its
-// queries 256 at a time and streams the frame's points through shared memory
-// in chunks, each thread scanning every chunk for its own query. A frame's
-// points are loaded once per 256 queries instead of once per query.
-constexpr int FB_CHUNK = 1024;
-
-__global__ void k_hard_frame_count(const u32 *hard, const u32 *hard_n, const int32_t *frame_of,
-                                   u32 *frame_cnt) {
-  const u32 n = *hard_n;
-  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    atomicAdd(&frame_cnt[frame_of ? frame_of[hard[i]] : 0], 1u);
-}
-__global__ void k_hard_frame_scan(u32 *frame_cnt, int n_frames, u32 *frame_start) {
-  if (blockIdx.x || threadIdx.x) return;
-  u32 run = 0;
-  for (int f = 0; f < n_frames; ++f) {
-    frame_start[f] = run;
-    run += frame_cnt[f];
-    frame_cnt[f] = 0;  // reused as the fill cursor
-  }
-  frame_start[n_frames] = run;
-}
-__global__ void k_hard_frame_fill(const u32 *hard, const float *hard_tau, const u32 *hard_n,
-                                  const int32_t *frame_of, const u32 *frame_start,
-                                  u32 *frame_cnt, u32 *by_frame) {
-  const u32 n = *hard_n;
-  for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int f = frame_of ? frame_of[hard[i]] : 0;
-    by_frame[frame_start[f] + atomicAdd(&frame_cnt[f], 1u)] = hard[i];
-  }
-}
-
-template <int K, int MODE>
-__global__ __launch_bounds__(TT) void k_knn_frame_brute(GridView g, TileArgs a,
-                                                        const u32 *by_frame,
-                                                        const u32 *frame_start, int n_frames) {
-  using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
-  __shared__ float4 chunk[FB_CHUNK];
-  Key kMax;
-  if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
-  else kMax = ~0ull;
-  for (int f = blockIdx.x; f < n_frames; f += gridDim.x) {
-    const u32 qa = frame_start[f], qb = frame_start[f + 1];
-    if (qa == qb) continue;
-    const u64 pa = g.frame_pt_begin[f], pb = g.frame_pt_begin[f + 1];
-    for (u32 r0 = qa; r0 < qb; r0 += TT) {
-      const u32 slot = r0 + threadIdx.x;
-      const bool has = slot < qb;
-      const u32 qidx = has ? by_frame[slot] : 0;
-      float qx = 0.0f, qy = 0.0f, qz = 0.0f;
-      if (has) {
-        if (MODE == TILE_NORMALS) {
-          qx = a.vx[qidx]; qy = a.vy[qidx]; qz = a.vz[qidx];
-        } else {
-          qx = a.qx[qidx]; qy = a.qy[qidx]; qz = a.qz[qidx];
-        }
-      }
-      Key L[K];
-#pragma unroll
-      for (int j = 0; j < K; ++j) L[j] = kMax;
-      Key thr = kMax;
-      u32 found = 0;
-      for (u64 c0 = pa; c0 < pb; c0 += FB_CHUNK) {
-        const u32 m = (u32)((pb - c0) < FB_CHUNK ? (pb - c0) : FB_CHUNK);
-        __syncthreads();
-        for (u32 j = threadIdx.x; j < m; j += TT) chunk[j] = __ldg(&g.pts[c0 + j]);
-        __syncthreads();
-        if (has)
-          for (u32 j = 0; j < m; ++j) {
-            const float4 p = chunk[j];
-            const u32 pidx = __float_as_uint(p.w);
-            if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
-            ++found;
-            const float d2 = dist2(p.x, p.y, p.z, qx, qy, qz);
-            Key key;
-            if constexpr (MODE == TILE_SOR_MEAN) key = d2;
-            else key = pack_nbr(d2, (int)pidx);
-            if (key < thr) {
-              list_insert<Key, K>(L, key);
-              thr = L[K - 1];
-            }
-          }
-      }
-      if (!has) continue;
-      const int cnt = (int)(found < (u32)K ? found : (u32)K);
-      if constexpr (MODE == TILE_SOR_MEAN) {
-        // sor_sc's mean (fewer terms if the frame holds fewer than K points)
-        const int valid_k = cnt - 1;
-        float sum = 0.0f;
-#pragma unroll
-        for (int j = 1; j < K; ++j)
-          if (j <= valid_k) sum = fadd(sum, __fsqrt_rn(L[j]));
-        a.mean[qidx] = valid_k > 0 ? fdiv(sum, (float)valid_k) : 0.0f;
-      } else if constexpr (MODE == TILE_NORMALS) {
-        float nx = 0.0f, ny = 0.0f, nz = 0.0f;
-        if (cnt == K)
-          normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, qx, qy, qz, a.vpx, a.vpy,
-                              a.vpz, nx, ny, nz);
-        else if (cnt >= 3)
-          normal_from_list(a.vx, a.vy, a.vz,
-                           [&](int t) {
-                             u64 k = 0;
-#pragma unroll
-                             for (int j = 0; j < K; ++j)
-                               if (j == t) k = L[j];
-                             return nbr_idx(k) & 0x7FFFFFFF;
-                           },
-                           cnt, true, a.iters, qx, qy, qz, a.vpx, a.vpy, a.vpz, nx, ny, nz);
-        const u64 o = a.out_pos[qidx];
-        a.nx[o] = nx;
-        a.ny[o] = ny;
-        a.nz[o] = nz;
-      } else {
-#pragma unroll
-        for (int j = 0; j < K; ++j)
-          if (j < cnt) a.pairs[(size_t)qidx * K + j] = L[j];
-        if (a.counts) a.counts[qidx] = cnt;
-      }
-    }
-  }
-}
-
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
               uint8_t *qlevel, u32 *stats) {
@@ -654,32 +531,6 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
         k_knn_wt<K, TILE_PAIRS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                  qlevel, a.qtau, st);
       RVP_LAUNCH_CHECK(ctx);
-    }
-    if (a.frame_cnt) {
-      // whatever is still open: whole frames, one block per frame
-      RVP_CUDA_TRY(cudaMemsetAsync(a.frame_cnt, 0, (size_t)a.n_frames * 4, ctx->stream));
-      k_hard_frame_count<<<ctx->num_sms, 256, 0, ctx->stream>>>(a.hard, a.hard_count, a.frame_of,
-                                                                 a.frame_cnt);
-      RVP_LAUNCH_CHECK(ctx);
-      k_hard_frame_scan<<<1, 32, 0, ctx->stream>>>(a.frame_cnt, a.n_frames, a.frame_start);
-      RVP_LAUNCH_CHECK(ctx);
-      k_hard_frame_fill<<<ctx->num_sms, 256, 0, ctx->stream>>>(a.hard, a.hard_tau, a.hard_count,
-                                                                a.frame_of, a.frame_start,
-                                                                a.frame_cnt, a.by_frame);
-      RVP_LAUNCH_CHECK(ctx);
-      const int fb = a.n_frames < ctx->num_sms * 2 ? a.n_frames : ctx->num_sms * 2;
-      if (mode == TILE_SOR_MEAN)
-        k_knn_frame_brute<K, TILE_SOR_MEAN><<<fb, TT, 0, ctx->stream>>>(g, a, a.by_frame,
-                                                                       a.frame_start, a.n_frames);
-      else if (mode == TILE_NORMALS)
-        k_knn_frame_brute<K, TILE_NORMALS><<<fb, TT, 0, ctx->stream>>>(g, a, a.by_frame,
-                                                                      a.frame_start, a.n_frames);
-      else
-        k_knn_frame_brute<K, TILE_PAIRS><<<fb, TT, 0, ctx->stream>>>(g, a, a.by_frame,
-                                                                    a.frame_start, a.n_frames);
-      RVP_LAUNCH_CHECK(ctx);
-      // nothing is left for the caller's fallback
-      RVP_CUDA_TRY(cudaMemsetAsync(a.hard_count, 0, 4, ctx->stream));
     }
     return;
   }

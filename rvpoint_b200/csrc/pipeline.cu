@@ -44,7 +44,6 @@ struct rvp_pipeline {
   rvp::DevBuf qlevel; // per grid point: level at which its kNN is still open
   rvp::DevBuf qtau;   // per grid point: K-th distance bound handed to the next level
   rvp::DevBuf open;   // open-query compaction between levels (flags, scan, list)
-  rvp::DevBuf fbrute; // whole-frame pass: per-frame counts/starts, queries by frame
   bool stats_on = false;
   int n_frames_last = 0;
   // stage timing: a ring of event sets, one set per run
@@ -87,8 +86,6 @@ __global__ void k_frame_ids(const int64_t *offs, int n_frames, size_t n_max, int
     frame[i] = lo;
   }
 }
-
-inline size_t max_frames_align(int f) { return ((size_t)f + 64) & ~(size_t)63; }
 
 __global__ void k_widen(const u32 *a, u64 *b) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *b = *a;
@@ -159,7 +156,6 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->hard.reserve(N * 8 + 256);
     p->qlevel.reserve(N);
     p->qtau.reserve(N * 4);
-    p->fbrute.reserve(max_frames_align(max_frames) * 8 + 256 + N * 4);
     p->open.reserve(((N * 4 + 255) & ~(size_t)255) + ((N * 8 + 8 + 255) & ~(size_t)255) +
                     ((N * 4 + 255) & ~(size_t)255) + 256 + rvp::scan_temp_bytes(N));
     p->nrm_counts.reserve(N * 4);
@@ -193,7 +189,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau, &p->open, &p->fbrute};
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau, &p->open};
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
@@ -264,14 +260,6 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
       ta.open_list = reinterpret_cast<u32 *>(op); op += al(N * 4);
       ta.open_n = reinterpret_cast<u64 *>(op); op += 256;
       ta.scan_tmp = op;
-      char *fp = p->fbrute.as<char>();
-      ta.n_frames = n_frames;
-      ta.frame_cnt = reinterpret_cast<u32 *>(fp);
-      ta.frame_start = reinterpret_cast<u32 *>(fp + ((size_t)max_frames_align(p->max_frames) * 4));
-      ta.by_frame = reinterpret_cast<u32 *>(fp + ((size_t)max_frames_align(p->max_frames) * 8 + 256));
-      ta.qx = p->vox_x.as<float>();
-      ta.qy = p->vox_y.as<float>();
-      ta.qz = p->vox_z.as<float>();
     }
     ta.n_max = N;
     const bool tiled = c.queries_per_warp != 1;
