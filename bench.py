@@ -196,23 +196,31 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-# algorithmic bytes per unit (what one launch of each stage must move)
-def stage_bytes(stage: str, n_in: int, n_vox: int, n_sor: int, n_frames: int) -> float:
-    ks, kn = SOR_K + 1, NORMAL_K + 1
-    return {
-        "voxel": 12.0 * n_in + 12.0 * n_vox,
-        "grid_build": 28.0 * n_vox,
-        "sor_knn": (12.0 + 8.0 * ks) * n_vox,
-        "sor_filter": 12.0 * n_vox + 1.0 * n_vox + 12.0 * n_sor,
-        "normals_knn": (12.0 + 8.0 * kn) * n_sor,
-        "normals": 24.0 * n_sor,
-        "ransac": 12.0 * n_sor + 4.0 * n_frames,
-    }[stage]
+# kernels timed live for the roofline: the stage or per-level kernel name,
+# the kernel that runs there, and the queries / points one launch processes
+KERNELS = {
+    "sor_knn_l0": ("k_knn_wt<17,SOR_MEAN> grid level 0", "vox"),
+    "sor_knn_l1": ("k_knn_wt<17,SOR_MEAN> grid level 1", None),
+    "sor_knn_l2": ("k_knn_wt<17,SOR_MEAN> grid level 2", None),
+    "normals_knn_l0": ("k_knn_wt<17,NORMALS> grid level 0", "sor"),
+    "normals_knn_l1": ("k_knn_wt<17,NORMALS> grid level 1", None),
+    "normals_knn_l2": ("k_knn_wt<17,NORMALS> grid level 2", None),
+    "ransac": ("k_ransac", "ransac"),
+}
 
 
-STAGE_KERNEL = {"sor_knn": "k_knn_warp", "normals_knn": "k_knn_warp", "ransac": "k_ransac",
-                "normals": "k_normals_lists", "voxel": "voxel stage (sort + reduce)",
-                "grid_build": "grid build (sort + table)", "sor_filter": "SOR statistics"}
+def kernel_bytes(name: str, n_vox: int, n_sor: int, n_frames: int) -> float:
+    """Algorithmic bytes of one launch: every query of the batch passes the
+    level-0 kNN kernel (12 B query + 8 B per neighbour, k+1 = 17 neighbours);
+    RANSAC reads each kept point once and writes a count per hypothesis."""
+    kind = KERNELS[name][1]
+    if kind == "vox":
+        return (12.0 + 8.0 * (SOR_K + 1)) * n_vox
+    if kind == "sor":
+        return (12.0 + 8.0 * (NORMAL_K + 1)) * n_sor
+    if kind == "ransac":
+        return 12.0 * n_sor + 4.0 * R_ITERS * n_frames
+    raise ValueError(name)
 
 
 def main():
@@ -279,7 +287,29 @@ def main():
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop() if clocks else None
     pipe.check()
-    stages = pipe.stage_times()
+    stages = pipe.stage_times(levels=True)
+
+    # ---- the same steps replayed from one CUDA graph (no per-stage events)
+    pipe.set_timing(0)
+    graph_kernels = pipe.capture(*args)
+    for _ in range(2):
+        pipe.replay()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(a.steps):
+        pipe.replay()
+    g1.record()
+    torch.cuda.synchronize()
+    pipe.check()
+    g_t = torch.tensor([g0.elapsed_time(g1)], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(g_t, op=dist.ReduceOp.MAX)
+    graph = {"ms_per_step": float(g_t.item()) / a.steps, "kernels_per_step": graph_kernels,
+             "value": (n * world) / (float(g_t.item()) / a.steps / 1e3) / 1e6}
     t = torch.tensor([ms], device=dev, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -342,28 +372,34 @@ def main():
         dist.destroy_process_group()
         return
 
-    # ---- roofline of the dominant single-kernel stage
-    single = ["sor_knn", "normals_knn", "normals", "ransac"]
-    dom = max(single, key=lambda s_: stages[s_])
+    # ---- roofline of the longest kernel timed live (per-level kNN kernels
+    # and RANSAC; the level-1/2 kernels see only the queries left open)
+    timed = {k: stages[k] for k in KERNELS if KERNELS[k][1] and stages.get(k, 0.0) > 0.0}
+    dom = max(timed, key=timed.get)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peaks = json.load(open(peaks_path))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
-    alg = stage_bytes(dom, n, n_vox, n_sor, nf)
-    achieved = alg / (stages[dom] / 1e3) / 1e9
+    alg = kernel_bytes(dom, n_vox, n_sor, nf)
+    achieved = alg / (timed[dom] / 1e3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(dom)
+            tr = json.load(open(tf)).get(dom)
+            # captured on a smaller batch: scaled by queries (traffic grows
+            # in proportion to the queries processed)
+            if tr:
+                units = n_vox if KERNELS[dom][1] == "vox" else n_sor
+                traffic = tr["bytes"] * units / tr["units"]
         except Exception:
             traffic = None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "kernel": STAGE_KERNEL[dom],
+            "frac": achieved / peak, "traffic": traffic, "kernel": KERNELS[dom][0],
             "stage": dom, "peak_source": peak_src,
-            "algorithmic_bytes_per_launch": alg, "launch_ms": stages[dom]}
+            "algorithmic_bytes_per_launch": alg, "launch_ms": timed[dom]}
 
     cpu = cpu_baseline(batch, a.cpu_budget_s) if world == 1 else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -377,7 +413,8 @@ def main():
                        "tuning": best},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps, "clocks": clk,
-            "stages_ms": {k: v for k, v in stages.items() if k != "runs"}}
+            "stages_ms": {k: v for k, v in stages.items() if k != "runs"},
+            "graph": graph}
     print(json.dumps(line), flush=True)
 
 

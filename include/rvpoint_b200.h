@@ -212,6 +212,19 @@ RVP_API rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x,
                                    const float *y, const float *z,
                                    const int64_t *frame_offsets_dev,
                                    int n_frames, size_t n_points);
+/* Records one rvp_pipeline_run_device over these device inputs as a CUDA
+ * graph (replacing any earlier one) without running it; *kernels (may be
+ * NULL) receives the kernel launches one replay makes. The graph keeps the
+ * input pointers and n_frames / n_points: new data goes into the same
+ * buffers. A tuning change needs a new capture. Run the pipeline once
+ * before the first capture, so that every buffer has its final size. */
+RVP_API rvp_status rvp_pipeline_capture(rvp_pipeline *p, const float *x,
+                                        const float *y, const float *z,
+                                        const int64_t *frame_offsets_dev,
+                                        int n_frames, size_t n_points,
+                                        uint64_t *kernels);
+/* Launches the captured run on the context's stream. */
+RVP_API rvp_status rvp_pipeline_replay(rvp_pipeline *p);
 /* Device pointers to the results of the last run (valid until the next run):
  * voxel_aos/voxel_offsets[n_frames+1], sor_aos/sor_offsets, normals (3 SoA
  * arrays over the SOR points), ransac_model[4*n_frames], ransac_count[n_frames],
@@ -256,9 +269,12 @@ RVP_API rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size,
 RVP_API rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac);
 /* Stage timing with CUDA events on the context's stream: the next max_runs
  * runs record 8 events each (stage boundaries: voxel, grid build, SOR kNN,
- * SOR statistics, normals kNN, normals, RANSAC). rvp_pipeline_stage_times
- * synchronizes and returns the mean ms per stage over the recorded runs
- * (ms[7]), then resets. max_runs = 0 turns timing off. */
+ * SOR statistics, normals kNN, normals, RANSAC), plus a pair around each
+ * grid level's kNN kernel. rvp_pipeline_stage_times synchronizes and returns
+ * the mean ms per stage over the recorded runs (ms[0..6]); with n_stages >= 13
+ * also the mean ms of the kNN kernel of each grid level (ms[7..9] SOR levels
+ * 0-2, ms[10..12] normals levels 0-2). It then resets. max_runs = 0 turns
+ * timing off. */
 RVP_API rvp_status rvp_pipeline_set_timing(rvp_pipeline *p, int max_runs);
 RVP_API rvp_status rvp_pipeline_stage_times(rvp_pipeline *p, float *ms, int n_stages,
                                             int *runs);
@@ -272,6 +288,14 @@ RVP_API rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const 
                                  int64_t *sor_offsets, float *nx, float *ny,
                                  float *nz, float *ransac_model,
                                  int32_t *ransac_count);
+/* Copies the results of the last run (run_device, replay or run_host) of
+ * the last n_frames to host arrays, sized and laid out as for
+ * rvp_pipeline_run_host (any pointer may be NULL); synchronizes. */
+RVP_API rvp_status rvp_pipeline_copy_outputs(rvp_pipeline *p, float *voxel_aos,
+                                             int64_t *voxel_offsets, float *sor_aos,
+                                             int64_t *sor_offsets, float *nx, float *ny,
+                                             float *nz, float *ransac_model,
+                                             int32_t *ransac_count);
 
 #ifdef __cplusplus
 }

@@ -84,6 +84,9 @@ SIGNATURES = {
     "rvp_pipeline_create": (I, [P, C.POINTER(PipelineConfig), SZ, I, C.POINTER(P)]),
     "rvp_pipeline_destroy": (I, [P]),
     "rvp_pipeline_run_device": (I, [P, P, P, P, P, I, SZ]),
+    "rvp_pipeline_capture": (I, [P, P, P, P, P, I, SZ, C.POINTER(C.c_uint64)]),
+    "rvp_pipeline_replay": (I, [P]),
+    "rvp_pipeline_copy_outputs": (I, [P] * 10),
     "rvp_pipeline_outputs_get": (I, [P, C.POINTER(PipelineOutputs)]),
     "rvp_pipeline_run_host": (I, [P, P, P, P, P, I, P, P, P, P, P, P, P, P, P]),
     "rvp_pipeline_set_timing": (I, [P, I]),

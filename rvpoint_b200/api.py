@@ -485,6 +485,22 @@ class Pipeline:
         check(self.L.rvp_pipeline_run_device(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(offsets_dev),
                                              int(n_frames), int(n_points)), self.ctx.h)
 
+    def capture(self, x, y, z, offsets_dev, n_frames: int, n_points: int) -> int:
+        """Record one run over these device tensors as a CUDA graph; returns
+        the kernel launches one replay makes. Refill the same tensors and
+        call replay() for each new batch."""
+        self.ctx.use_torch_stream()
+        self.last_frames = int(n_frames)
+        k = C.c_uint64(0)
+        check(self.L.rvp_pipeline_capture(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(offsets_dev),
+                                          int(n_frames), int(n_points), C.byref(k)), self.ctx.h)
+        self._graph_inputs = (x, y, z, offsets_dev)  # the graph reads these buffers
+        return int(k.value)
+
+    def replay(self) -> None:
+        self.ctx.use_torch_stream()
+        check(self.L.rvp_pipeline_replay(self.h), self.ctx.h)
+
     STAGES = ("voxel", "grid_build", "sor_knn", "sor_filter", "normals_knn", "normals",
               "ransac")
 
@@ -527,11 +543,18 @@ class Pipeline:
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)
 
-    def stage_times(self) -> dict:
-        ms = (C.c_float * 7)()
+    LEVEL_KERNELS = ("sor_knn_l0", "sor_knn_l1", "sor_knn_l2", "normals_knn_l0",
+                     "normals_knn_l1", "normals_knn_l2")
+
+    def stage_times(self, levels: bool = False) -> dict:
+        """Mean ms per stage over the runs recorded since set_timing; with
+        levels=True also the kNN kernel of each grid level."""
+        n = len(self.STAGES) + (len(self.LEVEL_KERNELS) if levels else 0)
+        ms = (C.c_float * n)()
         runs = C.c_int(0)
-        check(self.L.rvp_pipeline_stage_times(self.h, ms, 7, C.byref(runs)), self.ctx.h)
-        return {"runs": runs.value, **{s: float(ms[i]) for i, s in enumerate(self.STAGES)}}
+        check(self.L.rvp_pipeline_stage_times(self.h, ms, n, C.byref(runs)), self.ctx.h)
+        names = self.STAGES + (self.LEVEL_KERNELS if levels else ())
+        return {"runs": runs.value, **{s: float(ms[i]) for i, s in enumerate(names)}}
 
     def outputs(self) -> _lib.PipelineOutputs:
         o = _lib.PipelineOutputs()
@@ -546,6 +569,15 @@ class Pipeline:
         nf = int(offs.shape[0] - 1)
         self.last_frames = nf
         n = int(offs[-1])
+        check(self.L.rvp_pipeline_run_host(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(offs), nf,
+                                           None, None, None, None, None, None, None, None, None),
+              self.ctx.h)
+        return self.results(n)
+
+    def results(self, max_points: int | None = None) -> dict:
+        """Per-frame results of the last run, copied to numpy."""
+        nf = int(self.last_frames)
+        n = int(max_points if max_points is not None else self.max_points)
         vox = np.empty((max(n, 1), 3), np.float32)
         vo = np.empty(nf + 1, np.int64)
         sor = np.empty((max(n, 1), 3), np.float32)
@@ -555,10 +587,9 @@ class Pipeline:
         nz = np.empty(max(n, 1), np.float32)
         model = np.empty((nf, 4), np.float32)
         cnt = np.empty(nf, np.int32)
-        check(self.L.rvp_pipeline_run_host(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(offs), nf,
-                                           _ptr(vox), _ptr(vo), _ptr(sor), _ptr(so), _ptr(nx),
-                                           _ptr(ny), _ptr(nz), _ptr(model), _ptr(cnt)),
-              self.ctx.h)
+        check(self.L.rvp_pipeline_copy_outputs(self.h, _ptr(vox), _ptr(vo), _ptr(sor), _ptr(so),
+                                               _ptr(nx), _ptr(ny), _ptr(nz), _ptr(model),
+                                               _ptr(cnt)), self.ctx.h)
         nv, ns = int(vo[-1]), int(so[-1])
         return dict(voxel=vox[:nv], voxel_offsets=vo, sor=sor[:ns], sor_offsets=so,
                     normals=np.stack([nx[:ns], ny[:ns], nz[:ns]], 1), ransac_model=model,

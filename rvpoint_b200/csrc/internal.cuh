@@ -284,6 +284,7 @@ struct TileArgs {
   u64 *open_n;              // device count of open_list
   void *scan_tmp;           // scan_temp_bytes(n_max)
   size_t n_max;             // size of qlevel / qtau
+  cudaEvent_t *level_events;  // null, or 2 per grid level: around each level's kNN kernel
 };
 // false if k has no tile instantiation (use grid_knn then)
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,

@@ -521,6 +521,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
         list = a.open_list;
       }
       u32 *st = stats ? stats + level : nullptr;
+      if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
       if (mode == TILE_SOR_MEAN)
         k_knn_wt<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                     qlevel, a.qtau, st);
@@ -531,11 +532,13 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
         k_knn_wt<K, TILE_PAIRS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                  qlevel, a.qtau, st);
       RVP_LAUNCH_CHECK(ctx);
+      if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
     }
     return;
   }
   for (int level = 0; level < kGridLevels; ++level) {
     u32 *st = stats ? stats + level : nullptr;
+    if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
     if (mode == TILE_SOR_MEAN)
       k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
                                                                    st);
@@ -545,6 +548,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
     else
       k_knn_tile<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau, st);
     RVP_LAUNCH_CHECK(ctx);
+    if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
   }
 }
 }  // namespace

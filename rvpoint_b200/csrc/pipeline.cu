@@ -47,12 +47,31 @@ struct rvp_pipeline {
   bool stats_on = false;
   int n_frames_last = 0;
   // stage timing: a ring of event sets, one set per run
+  // (stage boundaries, then a pair around each grid level's kNN kernel: SOR
+  // levels 0-2, normals levels 0-2)
   static constexpr int kStages = 7;
-  std::vector<cudaEvent_t> events;  // runs_cap * (kStages + 1)
+  static constexpr int kLevelKernels = 2 * rvp::kGridLevels;
+  static constexpr int kEventsPerRun = kStages + 1 + 2 * kLevelKernels;
+  std::vector<cudaEvent_t> events;  // runs_cap * kEventsPerRun
   int runs_cap = 0, runs_recorded = 0;
+  // one run captured as a CUDA graph (rvp_pipeline_capture / _replay)
+  cudaGraphExec_t graph = nullptr;
+  uint64_t graph_kernels = 0;
+  bool capturing = false;
   void mark(int stage) {
-    if (runs_cap == 0 || runs_recorded >= runs_cap) return;
-    cudaEventRecord(events[(size_t)runs_recorded * (kStages + 1) + stage], ctx->stream);
+    if (capturing || runs_cap == 0 || runs_recorded >= runs_cap) return;
+    cudaEventRecord(events[(size_t)runs_recorded * kEventsPerRun + stage], ctx->stream);
+  }
+  // events around the kNN kernels of the current run (first = 0 SOR, 1 normals)
+  cudaEvent_t *level_events(int first) {
+    if (capturing || runs_cap == 0 || runs_recorded >= runs_cap) return nullptr;
+    return &events[(size_t)runs_recorded * kEventsPerRun + kStages + 1 +
+                   first * 2 * rvp::kGridLevels];
+  }
+  // a run whose kNN skipped the per-level kernels records zero-length pairs
+  void empty_level_events(cudaEvent_t *ev) {
+    if (ev)
+      for (int j = 0; j < 2 * rvp::kGridLevels; ++j) cudaEventRecord(ev[j], ctx->stream);
   }
 };
 
@@ -194,6 +213,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
   p->vw.release();
   p->grid.release();
   for (auto e : p->events) cudaEventDestroy(e);
+  if (p->graph) cudaGraphExecDestroy(p->graph);
   delete p;
   return RVP_OK;
 }
@@ -262,6 +282,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
       ta.scan_tmp = op;
     }
     ta.n_max = N;
+    ta.level_events = p->level_events(0);
     const bool tiled = c.queries_per_warp != 1;
     rvp::QuerySet qh{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N,
                      hard_n64, p->vox_frame.as<int32_t>(), reinterpret_cast<int32_t *>(hard)};
@@ -276,6 +297,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
       rvp::grid_knn(ctx, gv, qh, ks, 0.0f, nullptr, nullptr, 1, c.block_threads, st0,
                     rvp::KNN_OUT_SOR_MEAN, p->mean.as<float>());
     } else {
+      p->empty_level_events(ta.level_events);
       rvp::grid_knn(ctx, gv, qv, ks, 0.0f, nullptr, nullptr, 1, c.block_threads, st0,
                     rvp::KNN_OUT_SOR_MEAN, p->mean.as<float>());
     }
@@ -306,10 +328,12 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     tn.vpx = c.vp_x;
     tn.vpy = c.vp_y;
     tn.vpz = c.vp_z;
+    tn.level_events = p->level_events(1);
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
     bool tn_ok = tiled && rvp::grid_knn_tile(ctx, gv, kn, rvp::TILE_NORMALS, tn, 0,
                                              st0 ? st0 + 13 : nullptr);
     if (!tn_ok) {
+      p->empty_level_events(tn.level_events);
       // every kept point through the warp kernel: queue them all
       k_queue_kept<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(p->keep.as<uint8_t>(), n_vox,
                                                                     N, hard, hard_n);
@@ -337,7 +361,60 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                        sor_offs, n_frames, p->r_rand.as<int>(), prm, p->r_model.as<float>(),
                        p->r_best.as<int32_t>(), p->r_iters.as<int32_t>(), nullptr, false);
     p->mark(7);
-    if (p->runs_cap > 0 && p->runs_recorded < p->runs_cap) p->runs_recorded++;
+    if (!p->capturing && p->runs_cap > 0 && p->runs_recorded < p->runs_cap) p->runs_recorded++;
+  });
+}
+
+rvp_status rvp_pipeline_capture(rvp_pipeline *p, const float *x, const float *y, const float *z,
+                                const int64_t *offs, int n_frames, size_t n_points,
+                                uint64_t *kernels) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  rvp_context *ctx = p->ctx;
+  cudaStream_t user_stream = ctx->stream;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t g = nullptr;
+  rvp_status run = RVP_OK;
+  rvp_status s = guard(ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    // the legacy default stream cannot be captured: capture on a private
+    // stream ordered after the caller's work; the replay goes to the
+    // context's stream
+    RVP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    RVP_CUDA_TRY(cudaStreamSynchronize(user_stream));
+    if (p->graph) {
+      RVP_CUDA_TRY(cudaGraphExecDestroy(p->graph));
+      p->graph = nullptr;
+    }
+    RVP_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    ctx->stream = cap;
+    p->capturing = true;
+    const uint64_t l0 = ctx->launches;
+    run = rvp_pipeline_run_device(p, x, y, z, offs, n_frames, n_points);
+    p->graph_kernels = ctx->launches - l0;
+    p->capturing = false;
+    ctx->stream = user_stream;
+    const cudaError_t e = cudaStreamEndCapture(cap, &g);
+    if (run != RVP_OK) return;
+    RVP_CUDA_TRY(e);
+    RVP_CUDA_TRY(cudaGraphInstantiate(&p->graph, g, 0));
+    RVP_CUDA_TRY(cudaGraphUpload(p->graph, user_stream));
+  });
+  p->capturing = false;
+  ctx->stream = user_stream;
+  if (g) cudaGraphDestroy(g);
+  if (cap) cudaStreamDestroy(cap);
+  if (run != RVP_OK) return run;  // its message is already in last_error
+  if (s == RVP_OK && kernels) *kernels = p->graph_kernels;
+  return s;
+}
+
+rvp_status rvp_pipeline_replay(rvp_pipeline *p) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  return guard(p->ctx, [&] {
+    RVP_REQUIRE(p->graph, "no captured run: call rvp_pipeline_capture first");
+    RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    RVP_CUDA_TRY(cudaGraphLaunch(p->graph, p->ctx->stream));
+    p->ctx->launches += p->graph_kernels;
   });
 }
 
@@ -428,27 +505,50 @@ rvp_status rvp_pipeline_set_timing(rvp_pipeline *p, int max_runs) {
     p->events.clear();
     p->runs_cap = 0;
     p->runs_recorded = 0;
-    p->events.resize((size_t)max_runs * (rvp_pipeline::kStages + 1));
+    p->events.resize((size_t)max_runs * rvp_pipeline::kEventsPerRun);
     for (auto &e : p->events) RVP_CUDA_TRY(cudaEventCreate(&e));
     p->runs_cap = max_runs;
   });
 }
 
 rvp_status rvp_pipeline_stage_times(rvp_pipeline *p, float *ms, int n_stages, int *runs) {
-  if (!p || !ms || n_stages < rvp_pipeline::kStages) return RVP_ERR_INVALID_ARG;
+  using P = rvp_pipeline;
+  if (!p || !ms || n_stages < P::kStages) return RVP_ERR_INVALID_ARG;
   return guard(p->ctx, [&] {
     RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
-    for (int s = 0; s < rvp_pipeline::kStages; ++s) ms[s] = 0.0f;
+    const int n_out = n_stages < P::kStages + P::kLevelKernels ? P::kStages
+                                                                : P::kStages + P::kLevelKernels;
+    for (int s = 0; s < n_out; ++s) ms[s] = 0.0f;
     const int R = p->runs_recorded;
-    for (int r = 0; r < R; ++r)
-      for (int s = 0; s < rvp_pipeline::kStages; ++s) {
+    // the per-level events exist only on runs whose kNN went through the
+    // per-level kernels; a run without them reports 0 there
+    int level_runs = 0;
+    for (int r = 0; r < R; ++r) {
+      cudaEvent_t *ev = &p->events[(size_t)r * P::kEventsPerRun];
+      for (int s = 0; s < P::kStages; ++s) {
         float t = 0.0f;
-        RVP_CUDA_TRY(cudaEventElapsedTime(&t, p->events[(size_t)r * (rvp_pipeline::kStages + 1) + s],
-                                          p->events[(size_t)r * (rvp_pipeline::kStages + 1) + s + 1]));
+        RVP_CUDA_TRY(cudaEventElapsedTime(&t, ev[s], ev[s + 1]));
         ms[s] += t;
       }
+      if (n_out > P::kStages) {
+        float lt[P::kLevelKernels];
+        bool ok = true;
+        for (int j = 0; j < P::kLevelKernels && ok; ++j) {
+          const cudaEvent_t *e = ev + P::kStages + 1 + 2 * j;
+          ok = cudaEventElapsedTime(&lt[j], e[0], e[1]) == cudaSuccess;
+        }
+        if (ok) {
+          for (int j = 0; j < P::kLevelKernels; ++j) ms[P::kStages + j] += lt[j];
+          ++level_runs;
+        } else {
+          cudaGetLastError();
+        }
+      }
+    }
     if (R > 0)
-      for (int s = 0; s < rvp_pipeline::kStages; ++s) ms[s] /= (float)R;
+      for (int s = 0; s < P::kStages; ++s) ms[s] /= (float)R;
+    if (level_runs > 0)
+      for (int s = P::kStages; s < n_out; ++s) ms[s] /= (float)level_runs;
     if (runs) *runs = R;
     p->runs_recorded = 0;
   });
@@ -497,7 +597,19 @@ rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const float *y
   s = rvp_pipeline_run_device(p, p->in_x.as<float>(), p->in_y.as<float>(), p->in_z.as<float>(),
                               p->in_offs.as<int64_t>(), n_frames, n);
   if (s != RVP_OK) return s;
+  return rvp_pipeline_copy_outputs(p, voxel_aos, voxel_offsets, sor_aos, sor_offsets, nx, ny, nz,
+                                   ransac_model, ransac_count);
+}
+
+rvp_status rvp_pipeline_copy_outputs(rvp_pipeline *p, float *voxel_aos, int64_t *voxel_offsets,
+                                     float *sor_aos, int64_t *sor_offsets, float *nx, float *ny,
+                                     float *nz, float *ransac_model, int32_t *ransac_count) {
+  if (!p) return RVP_ERR_INVALID_ARG;
+  rvp_context *ctx = p->ctx;
   return guard(ctx, [&] {
+    const int n_frames = p->n_frames_last;
+    RVP_REQUIRE(n_frames >= 1, "no run to copy");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     std::vector<int64_t> vo(n_frames + 1), so(n_frames + 1);
     RVP_CUDA_TRY(cudaMemcpyAsync(vo.data(), p->vox_offs.ptr, (n_frames + 1) * 8,

@@ -395,3 +395,67 @@ def test_pipeline_cell_size_does_not_change_results(gpu_ctx, restatement, cell):
         s, _, _ = restatement.sor_exact(D.Cloud.from_xyz(v), 16, 1.0)
         a, b = r["sor_offsets"][f], r["sor_offsets"][f + 1]
         assert np.array_equal(bits(r["sor"][a:b]), bits(s))
+
+
+def test_pipeline_graph_replay_matches_direct_runs(gpu_ctx):
+    """One run captured as a CUDA graph and replayed gives the direct run's
+    results bit for bit, also after new frames are copied into the captured
+    input buffers."""
+    import torch
+    from rvpoint_b200 import api
+    b1 = D.lidar_batch(n_frames=3, seed=21, min_pts=20000, max_pts=60000)
+    b2 = D.lidar_batch(n_frames=3, seed=22, min_pts=20000, max_pts=60000)
+    cap_n = max(b1.n, b2.n)
+    dev = torch.device("cuda", 0)
+    bufs = [torch.zeros(cap_n, dtype=torch.float32, device=dev) for _ in range(3)]
+    offs = torch.zeros(4, dtype=torch.int64, device=dev)
+
+    def load(b):
+        for t, a in zip(bufs, (b.x, b.y, b.z)):
+            t[:b.n].copy_(torch.from_numpy(a))
+        offs.copy_(torch.from_numpy(b.offsets))
+
+    direct = api.Pipeline(max_points=cap_n, max_frames=3)
+    ref = [direct.run_host(b) for b in (b1, b2)]
+
+    g = api.Pipeline(max_points=cap_n, max_frames=3)
+    load(b1)
+    g.run_device(*bufs, offs, 3, b1.n)  # sizes every buffer before the capture
+    kernels = g.capture(*bufs, offs, 3, b1.n)
+    assert kernels > 20
+    for b, r in zip((b1, b1), (ref[0], ref[0])):
+        load(b)
+        g.replay()
+        out = g.results()
+        for key in ("voxel", "sor", "normals", "ransac_model"):
+            assert np.array_equal(bits(out[key]), bits(r[key])), key
+        assert np.array_equal(out["ransac_count"], r["ransac_count"])
+    # the graph keeps n_points: a second batch of another size needs a new capture
+    load(b2)
+    g.capture(*bufs, offs, 3, b2.n)
+    g.replay()
+    out = g.results()
+    for key in ("voxel", "sor", "normals"):
+        assert np.array_equal(bits(out[key]), bits(ref[1][key])), key
+
+
+def test_pipeline_level_kernel_times(gpu_ctx):
+    """Per-level kNN kernel timing: positive at level 0, and each stage's
+    level kernels fit inside the stage."""
+    import torch
+    from rvpoint_b200 import api
+    b = D.lidar_batch(n_frames=4, seed=23)
+    dev = torch.device("cuda", 0)
+    x, y, z = (torch.from_numpy(a).to(dev) for a in (b.x, b.y, b.z))
+    offs = torch.from_numpy(b.offsets).to(dev)
+    p = api.Pipeline(max_points=b.n, max_frames=4)
+    p.run_device(x, y, z, offs, 4, b.n)
+    p.set_timing(2)
+    for _ in range(2):
+        p.run_device(x, y, z, offs, 4, b.n)
+    t = p.stage_times(levels=True)
+    assert t["runs"] == 2
+    assert t["sor_knn_l0"] > 0 and t["normals_knn_l0"] > 0
+    assert t["sor_knn_l0"] + t["sor_knn_l1"] + t["sor_knn_l2"] <= t["sor_knn"] * 1.001
+    assert (t["normals_knn_l0"] + t["normals_knn_l1"] + t["normals_knn_l2"]
+            <= t["normals_knn"] * 1.001)
