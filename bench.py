@@ -12,6 +12,7 @@ HBM; `e2e` is the same through the host-buffer C entry point
 region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--cell C [--rfac R]] [--no-tune] [--cpu-budget-s S]
 
 N > 1: launched by torch.distributed.run, one rank per GPU; every rank owns
 its own 256 frames (weak scaling, no data-path collective); time = max over
@@ -47,6 +48,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=256)
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--cell", type=float, default=0.0,
+                    help="fixed grid cell (m) instead of the autotuner's choice")
+    ap.add_argument("--rfac", type=float, default=1.0,
+                    help="level-0 first-pass radius factor with --cell")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     return ap.parse_args()
 
@@ -258,7 +263,11 @@ def main():
     best = None
     pipe.run_device(*args)
     pipe.fit_tables()  # bucket table sized to this workload (stays in L2)
-    if not a.no_tune:
+    if a.cell > 0:
+        pipe.set_tuning(a.cell, 256, 0)
+        pipe.set_search_radius_factor(a.rfac)
+        best = {"cell": a.cell, "block": 256, "qpw": 0, "rfac": a.rfac, "fixed": True}
+    elif not a.no_tune:
         best, _ = autotune.tune(pipe, *args)
     for _ in range(max(a.warmup, 1)):
         pipe.run_device(*args)

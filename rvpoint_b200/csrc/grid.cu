@@ -595,7 +595,7 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
       }
     }
     const u32 cnt = found < (u32)K ? found : (u32)K;
-    if (out_mode == KNN_OUT_SOR_MEAN) {
+    if (out_mode == KNN_OUT_SOR_MEAN || out_mode == KNN_OUT_SOR_MEAN_LIST) {
       // sor_sc's mean (statistical_outlier_removal.cpp:36-40): ascending
       // sum of sqrtf(d2_j), j = 1..k, divided by k (fewer if the frame is
       // smaller than k+1)
@@ -606,6 +606,14 @@ __global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K,
         if (j <= valid_k) sum = fadd(sum, __fsqrt_rn(d));
       }
       if (lane == 0) mean[qi] = valid_k > 0 ? fdiv(sum, (float)valid_k) : 0.0f;
+      if (out_mode == KNN_OUT_SOR_MEAN_LIST) {
+        u32 *row = reinterpret_cast<u32 *>(out) + (size_t)qi * K;
+#pragma unroll
+        for (int s = 0; s < P; ++s) {
+          const int j = s * 32 + lane;
+          if (j < K) row[j] = j < (int)cnt ? (u32)nbr_idx(L.e[s]) & 0x7FFFFFFFu : 0xFFFFFFFFu;
+        }
+      }
     } else {
       const size_t row = out_mode == KNN_OUT_BY_SLOT ? wi : (size_t)qi;
 #pragma unroll

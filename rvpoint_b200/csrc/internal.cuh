@@ -250,7 +250,10 @@ void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs,
 // stats (optional, 8 counters): queries certified by the fine ring, by a
 // fine tight window, by the coarse ring, by a coarse tight window, by a
 // whole-frame scan, and the radius-bounded ones.
-enum KnnOut { KNN_OUT_BY_QUERY = 0, KNN_OUT_BY_SLOT = 1, KNN_OUT_SOR_MEAN = 2 };
+// KNN_OUT_SOR_MEAN_LIST: the mean, and out_pairs (as u32 rows of k by
+// original index) receives the k nearest indices, 0xFFFFFFFF past the found
+enum KnnOut { KNN_OUT_BY_QUERY = 0, KNN_OUT_BY_SLOT = 1, KNN_OUT_SOR_MEAN = 2,
+              KNN_OUT_SOR_MEAN_LIST = 3 };
 void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
               float radius, u64 *out_pairs, int32_t *out_counts, int qpw,
               int block_threads, u32 *stats = nullptr, int out_mode = KNN_OUT_BY_QUERY,
@@ -260,10 +263,13 @@ void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
 // cells around it in shared memory, one thread per query scans its own
 // 27-cell ring; queries the ring cannot certify go to `hard` (original
 // indices) for grid_knn. Modes: SOR mean, fused reference normals, pairs.
-enum TileMode { TILE_SOR_MEAN = 0, TILE_NORMALS = 1, TILE_PAIRS = 2 };
+// TILE_SOR_LIST: the SOR mean plus the k nearest indices in (d2, index)
+// order, kept for the normal stage (sor_list)
+enum TileMode { TILE_SOR_MEAN = 0, TILE_NORMALS = 1, TILE_PAIRS = 2, TILE_SOR_LIST = 3 };
 struct TileArgs {
   const int32_t *frame_of;  // frame of each original index
-  float *mean;              // TILE_SOR_MEAN: by original index
+  float *mean;              // TILE_SOR_MEAN / _LIST: by original index
+  u32 *sor_list;            // TILE_SOR_LIST: k indices per original index
   const float *vx, *vy, *vz;  // TILE_NORMALS: coordinates by original index
   const u64 *out_pos;       // TILE_NORMALS: output slot of each original index
   float *nx, *ny, *nz;
@@ -285,8 +291,14 @@ struct TileArgs {
   void *scan_tmp;           // scan_temp_bytes(n_max)
   size_t n_max;             // size of qlevel / qtau
   cudaEvent_t *level_events;  // null, or 2 per grid level: around each level's kNN kernel
+  bool preset_open;         // qlevel already holds 0 (open) / 0xFF (done) per grid point
 };
 // false if k has no tile instantiation (use grid_knn then)
+// Normals of the kept points whose SOR neighbour list (TILE_SOR_LIST, ks per
+// point) holds kn kept points; marks the rest open (qlevel 0) and the others
+// done (0xFF). False (nothing launched) if kn > ks or kn is not instantiated.
+bool normals_from_sor_lists(rvp_context *ctx, const GridView &g, const TileArgs &a, int ks,
+                            int kn, const uint8_t *keep);
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
                    int blocks, u32 *stats = nullptr);
 

@@ -47,6 +47,20 @@ __device__ __forceinline__ void list_insert(T (&L)[K], T key) {
   L[0] = key < L[0] ? key : L[0];
 }
 
+// SOR statistics of a certified list of packed keys: the mean distance to the
+// k nearest other points (statistical_outlier_removal.cpp:36-40, ascending
+// sum), and the k+1 indices for the normal stage
+template <int K>
+__device__ __forceinline__ void sor_list_out(const TileArgs &a, u32 qidx, const u64 (&L)[K]) {
+  float sum = 0.0f;
+#pragma unroll
+  for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(nbr_d2(L[j])));
+  a.mean[qidx] = fdiv(sum, (float)(K - 1));
+  u32 *row = a.sor_list + (size_t)qidx * K;
+#pragma unroll
+  for (int j = 0; j < K; ++j) row[j] = (u32)nbr_idx(L[j]) & 0x7FFFFFFFu;
+}
+
 template <int K, int MODE>
 __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(GridView g, TileArgs a, int level,
                                                  uint8_t *qlevel, float *qtau, u32 *stats) {
@@ -268,6 +282,8 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
 #pragma unroll
         for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
         a.mean[qidx] = fdiv(sum, (float)(K - 1));
+      } else if constexpr (MODE == TILE_SOR_LIST) {
+        sor_list_out<K>(a, qidx, L);
       } else if constexpr (MODE == TILE_NORMALS) {
         float nx, ny, nz;
         normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
@@ -452,7 +468,12 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
         }
       }
       if (!ok) {
-        if (level + 1 < kGridLevels) {
+        // a bound found at the next-to-top level goes straight to the warp
+        // kernel, which scans the tight window of sqrt(tau) at the finest
+        // level where it stays small; the top-level ring would hold far more
+        // points than that window
+        const bool to_warp = level + 2 == kGridLevels && tau >= 0.0f && a.hard_tau;
+        if (level + 1 < kGridLevels && !to_warp) {
           qlevel[pos] = (uint8_t)(level + 1);
           qtau[pos] = tau;
         } else {
@@ -467,6 +488,8 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
 #pragma unroll
           for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
           a.mean[qidx] = fdiv(sum, (float)(K - 1));
+        } else if constexpr (MODE == TILE_SOR_LIST) {
+          sor_list_out<K>(a, qidx, L);
         } else if constexpr (MODE == TILE_NORMALS) {
           float nx, ny, nz;
           normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
@@ -503,14 +526,15 @@ __global__ void k_open_scatter(const u32 *flags, const u64 *pos, const u64 *n_de
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
               uint8_t *qlevel, u32 *stats) {
-  RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
+  if (!a.preset_open) RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
   if (a.level0_warp) {
-    // barrier-free per-warp kernels at every level; levels > 0 read the
-    // compacted list of open queries
+    // barrier-free per-warp kernels at every level; levels > 0 (and level 0
+    // when the caller marked the open queries) read the compacted list of
+    // open queries
     const int wblocks = ctx->num_sms * 3 * 4;
     for (int level = 0; level < kGridLevels; ++level) {
       const u32 *list = nullptr;
-      if (level > 0) {
+      if (level > 0 || a.preset_open) {
         const unsigned gb = grid_for(a.n_max, 256, ctx->num_sms * 16);
         k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, level, a.open_flags);
         RVP_LAUNCH_CHECK(ctx);
@@ -524,6 +548,9 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
       if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
       if (mode == TILE_SOR_MEAN)
         k_knn_wt<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
+                                                                    qlevel, a.qtau, st);
+      else if (mode == TILE_SOR_LIST)
+        k_knn_wt<K, TILE_SOR_LIST><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                     qlevel, a.qtau, st);
       else if (mode == TILE_NORMALS)
         k_knn_wt<K, TILE_NORMALS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
@@ -542,6 +569,9 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
     if (mode == TILE_SOR_MEAN)
       k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
                                                                    st);
+    else if (mode == TILE_SOR_LIST)
+      k_knn_tile<K, TILE_SOR_LIST><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
+                                                                   st);
     else if (mode == TILE_NORMALS)
       k_knn_tile<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
                                                                   st);
@@ -553,9 +583,73 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
 }
 }  // namespace
 
+namespace {
+// Normals from the SOR stage's neighbour lists. The k+1 nearest points of a
+// kept point are its k+1 nearest kept points whenever none of them was
+// removed (removal only takes points away, and the (d2, index) order of the
+// rest is unchanged), so the first KN entries of its SOR list, when all kept,
+// are exactly the list the normal needs. Those points get their normal here;
+// the others are marked open (qlevel 0) for the kNN search. One thread per
+// grid point.
+template <int KN>
+__global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs a, int ks,
+                                                           const uint8_t *keep) {
+  const u64 n = *g.n_points;
+  for (u64 pos = blockIdx.x * (u64)blockDim.x + threadIdx.x; pos < n;
+       pos += (u64)gridDim.x * blockDim.x) {
+    const float4 q = g.pts[pos];
+    const u32 qidx = __float_as_uint(q.w);
+    if (qidx & kRemovedBit) {
+      a.qlevel[pos] = 0xFF;
+      continue;
+    }
+    const u32 *row = a.sor_list + (size_t)qidx * ks;
+    int I[KN];
+    bool ok = true;
+#pragma unroll
+    for (int t = 0; t < KN; ++t) {
+      const u32 j = __ldg(&row[t]);
+      ok = ok && j != 0xFFFFFFFFu && keep[j];
+      I[t] = ok ? (int)j : 0;
+    }
+    if (!ok) {
+      a.qlevel[pos] = 0;
+      continue;
+    }
+    a.qlevel[pos] = 0xFF;
+    float nx, ny, nz;
+    normal_from_regs<KN>(a.vx, a.vy, a.vz, [&](int t) { return I[t]; }, true, a.iters, q.x, q.y,
+                         q.z, a.vpx, a.vpy, a.vpz, nx, ny, nz);
+    const u64 o = a.out_pos[qidx];
+    a.nx[o] = nx;
+    a.ny[o] = ny;
+    a.nz[o] = nz;
+  }
+}
+}  // namespace
+
+bool normals_from_sor_lists(rvp_context *ctx, const GridView &g, const TileArgs &a, int ks,
+                            int kn, const uint8_t *keep) {
+  if (g.mode != KEY_DENSE || !a.sor_list || !a.qlevel || kn > ks) return false;
+  const unsigned blocks = grid_for(a.n_max, 256, ctx->num_sms * 16);
+  switch (kn) {
+#define RVP_NSL(K)                                                                        \
+  case K:                                                                                 \
+    k_normals_sor_lists<K><<<blocks, 256, 0, ctx->stream>>>(g, a, ks, keep);              \
+    break;
+    RVP_NSL(8) RVP_NSL(11) RVP_NSL(16) RVP_NSL(17) RVP_NSL(21) RVP_NSL(31) RVP_NSL(32)
+    RVP_NSL(33)
+#undef RVP_NSL
+    default: return false;
+  }
+  RVP_LAUNCH_CHECK(ctx);
+  return true;
+}
+
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
                    int blocks, u32 *stats) {
   if (g.mode != KEY_DENSE || !a.qlevel || !a.qtau) return false;
+  if (a.preset_open && !a.level0_warp) return false;
   if (blocks <= 0) blocks = ctx->num_sms * 8;
   switch (k) {
     case 8: launch_k<8>(ctx, g, mode, a, blocks, a.qlevel, stats); break;

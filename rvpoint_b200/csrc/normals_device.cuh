@@ -12,34 +12,49 @@
 namespace rvp {
 namespace nd {
 
+// One Jacobi rotation of the reference's loop body on the pair (P, Q), with
+// every index static so that A and V stay in registers.
+template <int P, int Q>
+__device__ __forceinline__ void jacobi_rotate_ref(float (&A)[3][3], float (&V)[3][3]) {
+  const float app = A[P][P], aqq = A[Q][Q], apq = A[P][Q];
+  const float phi = fmul(0.5f, atan2f(fmul(2.0f, apq), fsub(app, aqq)));
+  const float c = cosf(phi), s = sinf(phi);
+  const float cc = fmul(c, c), ss = fmul(s, s), s2c = fmul(fmul(2.0f, s), c);
+  // c*c*app - 2*s*c*apq + s*s*aqq ; s*s*app + 2*s*c*apq + c*c*aqq
+  A[P][P] = fadd(fsub(fmul(cc, app), fmul(s2c, apq)), fmul(ss, aqq));
+  A[Q][Q] = fadd(fadd(fmul(ss, app), fmul(s2c, apq)), fmul(cc, aqq));
+  A[P][Q] = 0.0f;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const float vip = V[r][P], viq = V[r][Q];
+    V[r][P] = fsub(fmul(c, vip), fmul(s, viq));
+    V[r][Q] = fadd(fmul(s, vip), fmul(c, viq));
+  }
+}
+
+// The reference's Jacobi loop: each iteration rotates the pair with the
+// largest upper off-diagonal |A[p][q]| (first of equals), which it reads from
+// the upper triangle only; the lower triangle is never read.
 __device__ __forceinline__ void eigen_smallest_ref(float A[3][3], int iters, float &nx, float &ny, float &nz) {
+  float (&M)[3][3] = *reinterpret_cast<float (*)[3][3]>(A);
   float V[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
   for (int it = 0; it < iters; ++it) {
-    int p = 0, q = 1;
-    float max_off = fabsf(A[0][1]);
-    if (fabsf(A[0][2]) > max_off) { p = 0; q = 2; max_off = fabsf(A[0][2]); }
-    if (fabsf(A[1][2]) > max_off) { p = 1; q = 2; }
-    const float app = A[p][p], aqq = A[q][q], apq = A[p][q];
-    const float phi = fmul(0.5f, atan2f(fmul(2.0f, apq), fsub(app, aqq)));
-    const float c = cosf(phi), s = sinf(phi);
-    const float cc = fmul(c, c), ss = fmul(s, s), s2c = fmul(fmul(2.0f, s), c);
-    // c*c*app - 2*s*c*apq + s*s*aqq ; s*s*app + 2*s*c*apq + c*c*aqq
-    A[p][p] = fadd(fsub(fmul(cc, app), fmul(s2c, apq)), fmul(ss, aqq));
-    A[q][q] = fadd(fadd(fmul(ss, app), fmul(s2c, apq)), fmul(cc, aqq));
-    A[p][q] = 0.0f;
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      const float vip = V[r][p], viq = V[r][q];
-      V[r][p] = fsub(fmul(c, vip), fmul(s, viq));
-      V[r][q] = fadd(fmul(s, vip), fmul(c, viq));
-    }
+    int pq = 0;  // 0: (0,1), 1: (0,2), 2: (1,2)
+    float max_off = fabsf(M[0][1]);
+    if (fabsf(M[0][2]) > max_off) { pq = 1; max_off = fabsf(M[0][2]); }
+    if (fabsf(M[1][2]) > max_off) pq = 2;
+    if (pq == 0) jacobi_rotate_ref<0, 1>(M, V);
+    else if (pq == 1) jacobi_rotate_ref<0, 2>(M, V);
+    else jacobi_rotate_ref<1, 2>(M, V);
   }
+  float d0 = M[0][0], d1 = M[1][1], d2 = M[2][2];
   int m = 0;
-  if (A[1][1] < A[m][m]) m = 1;
-  if (A[2][2] < A[m][m]) m = 2;
-  nx = V[0][m];
-  ny = V[1][m];
-  nz = V[2][m];
+  float dm = d0;
+  if (d1 < dm) { m = 1; dm = d1; }
+  if (d2 < dm) m = 2;
+  nx = m == 0 ? V[0][0] : (m == 1 ? V[0][1] : V[0][2]);
+  ny = m == 0 ? V[1][0] : (m == 1 ? V[1][1] : V[1][2]);
+  nz = m == 0 ? V[2][0] : (m == 1 ? V[2][1] : V[2][2]);
 }
 
 __device__ __forceinline__ void flip_ref(float px, float py, float pz, float vpx, float vpy,
@@ -104,19 +119,20 @@ __device__ __forceinline__ void normal_from_list(const float *__restrict__ x,
 
 namespace rvp {
 namespace nd {
-// normal_from_list over a register-resident list of M packed (d2, index)
-// keys (compile-time length: every index below is static).
-template <int M>
-__device__ __forceinline__ void normal_from_keys(const float *__restrict__ x,
+// normal_from_list over a register-resident list of M neighbours
+// (compile-time length: every index below is static).
+// The same over M indices (compile-time length) given by idx(t).
+template <int M, class IdxF>
+__device__ __forceinline__ void normal_from_regs(const float *__restrict__ x,
                                                  const float *__restrict__ y,
-                                                 const float *__restrict__ z, const u64 (&L)[M],
+                                                 const float *__restrict__ z, IdxF idx,
                                                  bool div_centroid, int iters, float qx, float qy,
                                                  float qz, float vpx, float vpy, float vpz,
                                                  float &nx, float &ny, float &nz) {
   float px[M], py[M], pz[M];
 #pragma unroll
   for (int t = 0; t < M; ++t) {
-    const int j = nbr_idx(L[t]) & 0x7FFFFFFF;
+    const int j = idx(t);
     px[t] = __ldg(&x[j]);
     py[t] = __ldg(&y[j]);
     pz[t] = __ldg(&z[j]);
@@ -153,6 +169,17 @@ __device__ __forceinline__ void normal_from_keys(const float *__restrict__ x,
   float A[3][3] = {{c00, c01, c02}, {c01, c11, c12}, {c02, c12, c22}};
   eigen_smallest_ref(A, iters, nx, ny, nz);
   flip_ref(qx, qy, qz, vpx, vpy, vpz, nx, ny, nz);
+}
+
+template <int M>
+__device__ __forceinline__ void normal_from_keys(const float *__restrict__ x,
+                                                 const float *__restrict__ y,
+                                                 const float *__restrict__ z, const u64 (&L)[M],
+                                                 bool div_centroid, int iters, float qx, float qy,
+                                                 float qz, float vpx, float vpy, float vpz,
+                                                 float &nx, float &ny, float &nz) {
+  normal_from_regs<M>(x, y, z, [&](int t) { return nbr_idx(L[t]) & 0x7FFFFFFF; }, div_centroid,
+                      iters, qx, qy, qz, vpx, vpy, vpz, nx, ny, nz);
 }
 }  // namespace nd
 }  // namespace rvp

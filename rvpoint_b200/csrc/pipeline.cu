@@ -35,7 +35,7 @@ struct rvp_pipeline {
   rvp::Grid grid;
   rvp::DevBuf in_x, in_y, in_z, in_offs;
   rvp::DevBuf vox_aos, vox_x, vox_y, vox_z, vox_offs, vox_frame;
-  rvp::DevBuf knn_pairs, knn_counts, mean, keep, sor_tmp;
+  rvp::DevBuf sor_list, knn_counts, mean, keep, sor_tmp;
   rvp::DevBuf sor_aos, sor_x, sor_y, sor_z, sor_offs, sor_frame, sor_src;
   rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
@@ -161,7 +161,7 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->vox_offs.reserve(F1 * 8);
     p->vox_frame.reserve(N * 4);
     const int ks = cfg->sor_k + 1, kn = cfg->normal_k + 1;
-    p->knn_pairs.reserve(N * (size_t)ks * 8);
+    p->sor_list.reserve(N * (size_t)ks * 4);
     p->knn_counts.reserve(N * 4);
     p->mean.reserve(N * 4);
     p->keep.reserve(N);
@@ -204,7 +204,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(p->ctx->stream);
   rvp::DevBuf *bufs[] = {&p->in_x, &p->in_y, &p->in_z, &p->in_offs, &p->vox_aos, &p->vox_x,
-                         &p->vox_y, &p->vox_z, &p->vox_offs, &p->vox_frame, &p->knn_pairs,
+                         &p->vox_y, &p->vox_z, &p->vox_offs, &p->vox_frame, &p->sor_list,
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
@@ -290,12 +290,24 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     rvp::QuerySet qv{p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(), N, n_vox,
                      p->vox_frame.as<int32_t>(), nullptr};
     ta.mean = p->mean.as<float>();
+    // with the per-warp kernels the SOR stage also keeps each point's k+1
+    // nearest indices, from which the normal stage takes the lists of the
+    // points whose neighbours all survive
+    const int kn = c.normal_k + 1;
+    const bool lists = c.queries_per_warp == 0 && kn <= ks;
+    ta.sor_list = lists ? p->sor_list.as<u32>() : nullptr;
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
-    if (tiled && rvp::grid_knn_tile(ctx, gv, ks, rvp::TILE_SOR_MEAN, ta, 0, st0 ? st0 + 5 : nullptr)) {
+    bool sor_lists = false;
+    if (tiled && rvp::grid_knn_tile(ctx, gv, ks, lists ? rvp::TILE_SOR_LIST : rvp::TILE_SOR_MEAN,
+                                    ta, 0, st0 ? st0 + 5 : nullptr)) {
+      sor_lists = lists;
       k_widen<<<1, 32, 0, st>>>(hard_n, hard_n64);
       RVP_LAUNCH_CHECK(ctx);
-      rvp::grid_knn(ctx, gv, qh, ks, 0.0f, nullptr, nullptr, 1, c.block_threads, st0,
-                    rvp::KNN_OUT_SOR_MEAN, p->mean.as<float>());
+      rvp::grid_knn(ctx, gv, qh, ks, 0.0f,
+                    sor_lists ? reinterpret_cast<u64 *>(p->sor_list.ptr) : nullptr, nullptr, 1,
+                    c.block_threads, st0,
+                    sor_lists ? rvp::KNN_OUT_SOR_MEAN_LIST : rvp::KNN_OUT_SOR_MEAN,
+                    p->mean.as<float>());
     } else {
       p->empty_level_events(ta.level_events);
       rvp::grid_knn(ctx, gv, qv, ks, 0.0f, nullptr, nullptr, 1, c.block_threads, st0,
@@ -314,7 +326,6 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     k_mark_removed<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(
         p->grid.b_pts.as<float4>(), p->keep.as<uint8_t>(), n_vox, N);
     RVP_LAUNCH_CHECK(ctx);
-    const int kn = c.normal_k + 1;
     rvp::TileArgs tn = ta;
     tn.mean = nullptr;
     tn.vx = p->vox_x.as<float>();
@@ -330,6 +341,10 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     tn.vpz = c.vp_z;
     tn.level_events = p->level_events(1);
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
+    // points whose SOR list holds kn kept points: normal straight from it;
+    // the rest open for the kNN search
+    tn.preset_open = sor_lists && rvp::normals_from_sor_lists(ctx, gv, tn, ks, kn,
+                                                              p->keep.as<uint8_t>());
     bool tn_ok = tiled && rvp::grid_knn_tile(ctx, gv, kn, rvp::TILE_NORMALS, tn, 0,
                                              st0 ? st0 + 13 : nullptr);
     if (!tn_ok) {
