@@ -297,6 +297,81 @@ RVP_API rvp_status rvp_pipeline_copy_outputs(rvp_pipeline *p, float *voxel_aos,
                                              float *nz, float *ransac_model,
                                              int32_t *ransac_count);
 
+/* ---------------------------------------------------------------------------
+ * Batched plain RANSAC and the learned hypothesis proposal. None of these
+ * has a reference counterpart except rvp_ransac_frames, which is
+ * ransac_plane_rvv (segmentation/ransac_plane.cpp:116-199, scalar branch
+ * :55-111) applied to every frame of a batch. All pointers are device
+ * pointers on the context's stream; the calls synchronize before returning,
+ * except rvp_scorer_features and rvp_mlp_forward.
+ * ------------------------------------------------------------------------- */
+#define RVP_MLP_INPUTS 8
+#define RVP_MLP_HIDDEN 64
+/* W1[64][8], b1[64], W2[64][64], b2[64], w3[64], b3: 4801 floats */
+#define RVP_MLP_PARAMS 4801
+
+/* ransac_plane_rvv on every frame (one srand(0) stream shared by all, as
+ * each reference call restarts it; libc's generator is left as the last
+ * frame's call leaves it). targets (optional, per frame): stop a frame at
+ * the first hypothesis whose inlier count reaches its target, with the
+ * adaptive stop off; iters_run then counts the hypotheses drawn. */
+RVP_API rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const float *y,
+                                     const float *z, const int64_t *frame_offsets_dev,
+                                     int n_frames, int max_iters, float dist_thresh,
+                                     float collinear_thresh, float probability,
+                                     const int32_t *targets, float *models, int32_t *best,
+                                     int32_t *iters_run);
+/* RANSAC whose three points are drawn from each frame's candidates
+ * (cand[cand_offsets[f] .. cand_offsets[f+1]), global point indices inside
+ * frame f) with probability proportional to weights (one per candidate),
+ * from a counter-based generator keyed by seed. Counting, model and the
+ * strict-greater update are ransac_plane_rvv's. */
+RVP_API rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y,
+                                       const float *z, const int64_t *frame_offsets_dev,
+                                       int n_frames, const uint32_t *cand,
+                                       const int64_t *cand_offsets_dev, const float *weights,
+                                       uint64_t seed, int max_iters, float dist_thresh,
+                                       float collinear_thresh, float probability,
+                                       const int32_t *targets, float *models, int32_t *best,
+                                       int32_t *iters_run);
+/* labels[i] = 1 if point i lies within dist_thresh of its frame's model
+ * (models: 4 floats per frame), else 0. */
+RVP_API rvp_status rvp_plane_labels(rvp_context *ctx, const float *x, const float *y,
+                                    const float *z, const int64_t *frame_offsets_dev,
+                                    int n_frames, size_t n_points, const float *models,
+                                    float dist_thresh, float *labels);
+
+typedef struct rvp_scorer rvp_scorer;
+RVP_API rvp_status rvp_scorer_create(rvp_context *ctx, size_t max_points, int max_frames,
+                                     rvp_scorer **out);
+RVP_API rvp_status rvp_scorer_destroy(rvp_scorer *s);
+/* Eight features per candidate (all points if cand is NULL) from its k = 16
+ * nearest neighbours within its frame: |normal| (3), curvature, planarity,
+ * log of the 16th-neighbour distance r, distance to the local plane / r,
+ * distance to the neighbourhood centroid / r. features: n_cand x 8. */
+RVP_API rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y,
+                                       const float *z, const int64_t *frame_offsets_dev,
+                                       int n_frames, size_t n_points, float cell_size,
+                                       const uint32_t *cand, size_t n_cand, float *features);
+/* Parameters (host arrays): FP32 master weights, RVP_MLP_PARAMS floats;
+ * the network computes with their BF16 rounding. set_params resets the
+ * optimiser. set_norm: per-feature mean and standard deviation applied
+ * before the first layer. */
+RVP_API rvp_status rvp_mlp_set_params(rvp_scorer *s, const float *params);
+RVP_API rvp_status rvp_mlp_get_params(rvp_scorer *s, float *params);
+RVP_API rvp_status rvp_mlp_set_norm(rvp_scorer *s, const float *mean, const float *stddev);
+/* logits[i] of features[i] (n x 8), device arrays. */
+RVP_API rvp_status rvp_mlp_forward(rvp_scorer *s, const float *features, size_t n,
+                                   float *logits);
+/* Mean binary cross-entropy of the logits against labels (0/1 floats) and
+ * its gradient w.r.t. the parameters (host, RVP_MLP_PARAMS floats). */
+RVP_API rvp_status rvp_mlp_gradients(rvp_scorer *s, const float *features, const float *labels,
+                                     size_t n, float *grad, double *loss);
+/* One Adam step (beta 0.9 / 0.999) on that loss; loss (host, may be NULL)
+ * receives the loss before the step. */
+RVP_API rvp_status rvp_mlp_train_step(rvp_scorer *s, const float *features, const float *labels,
+                                      size_t n, float lr, double *loss);
+
 #ifdef __cplusplus
 }
 #endif

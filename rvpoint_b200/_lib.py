@@ -97,7 +97,24 @@ SIGNATURES = {
     "rvp_pipeline_check": (I, [P]),
     "rvp_pipeline_knn_stats": (I, [P, I, P]),
     "rvp_pipeline_stage_times": (I, [P, C.POINTER(F), I, C.POINTER(I)]),
+    # batched RANSAC and the learned proposal
+    "rvp_ransac_frames": (I, [P, P, P, P, P, I, I, F, F, F, P, P, P, P]),
+    "rvp_ransac_weighted": (I, [P, P, P, P, P, I, P, P, P, C.c_uint64, I, F, F, F, P, P, P, P]),
+    "rvp_plane_labels": (I, [P, P, P, P, P, I, SZ, P, F, P]),
+    "rvp_scorer_create": (I, [P, SZ, I, C.POINTER(P)]),
+    "rvp_scorer_destroy": (I, [P]),
+    "rvp_scorer_features": (I, [P, P, P, P, P, I, SZ, F, P, SZ, P]),
+    "rvp_mlp_set_params": (I, [P, P]),
+    "rvp_mlp_get_params": (I, [P, P]),
+    "rvp_mlp_set_norm": (I, [P, P, P]),
+    "rvp_mlp_forward": (I, [P, P, SZ, P]),
+    "rvp_mlp_gradients": (I, [P, P, P, SZ, P, C.POINTER(C.c_double)]),
+    "rvp_mlp_train_step": (I, [P, P, P, SZ, F, C.POINTER(C.c_double)]),
 }
+
+MLP_INPUTS = 8
+MLP_HIDDEN = 64
+MLP_PARAMS = 4801
 
 _lib = None
 

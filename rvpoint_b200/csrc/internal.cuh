@@ -367,12 +367,28 @@ struct RansacParams {
   float collinear;
   double log_p;  // log(1 - clamp(p, .5, .9999)), computed on the host
 };
+// Hypothesis source of ransac_frames. Default (cdf null): the reference's
+// rand() stream, i = r % n. Weighted: three candidates of the frame drawn
+// with probability proportional to their weight (cdf = per-frame inclusive
+// prefix sums over the candidates cand[cand_offs[f] .. cand_offs[f+1]), global
+// point indices), from a counter-based generator keyed by seed. targets
+// (optional, per frame): stop a frame at the first hypothesis whose count
+// reaches its target (the adaptive stop is then off); iters_run = hypotheses
+// drawn.
+struct RansacSampler {
+  const u32 *cand = nullptr;
+  const int64_t *cand_offs = nullptr;
+  const double *cdf = nullptr;
+  u64 seed = 0;
+  const int32_t *targets = nullptr;
+};
 // One block per frame over SoA clouds; frame f = [off[f], off[f+1]).
 void ransac_frames(rvp_context *ctx, const float *x, const float *y,
                    const float *z, const int64_t *frame_offsets_dev,
                    int n_frames, const int *rand_dev, const RansacParams &p,
                    float *model, int32_t *best, int32_t *iters_run,
-                   int32_t *counts_all, bool eval_all);
+                   int32_t *counts_all, bool eval_all,
+                   const RansacSampler &smp = RansacSampler{});
 void extract_plane_run(rvp_context *ctx, const float *x, const float *y,
                        const float *z, size_t n, const float *model_dev,
                        float thresh, float *in_aos, float *out_aos,

@@ -1,0 +1,818 @@
+// Learned hypothesis proposal for batched RANSAC plane fitting.
+//
+// Per-point features come from the k = 16 nearest neighbours (17 with the
+// point itself) found by the batched grid kNN: the shifted covariance of
+// the neighbourhood, its eigen-decomposition (cyclic Jacobi, FP32), the
+// K-th neighbour distance and the point's offset from the neighbourhood
+// centroid. A per-point MLP 8 -> 64 -> 64 -> 1 (ReLU) scores how likely
+// the point lies on the plane plain RANSAC would pick; RANSAC then draws
+// its three points with probability proportional to the score
+// (ransac.cu, RansacSampler), and the exact inlier count over every
+// point still decides between hypotheses.
+//
+// The network's weights are BF16 (rounded from FP32 master weights after
+// every optimiser step); activations, sums and gradients are FP32. Training
+// runs on the GPU: one fused kernel does the forward and backward pass of
+// 128 points per block and reduces the weight gradients of its points in
+// shared memory before one atomic add per weight, then Adam updates the
+// master weights.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "internal.cuh"
+
+using rvp::u32;
+using rvp::u64;
+
+namespace rvp {
+namespace {
+
+constexpr int MI = RVP_MLP_INPUTS;   // 8
+constexpr int MH = RVP_MLP_HIDDEN;   // 64
+constexpr int NP = RVP_MLP_PARAMS;   // 4801
+constexpr int OW1 = 0, OB1 = OW1 + MH * MI, OW2 = OB1 + MH, OB2 = OW2 + MH * MH,
+              OW3 = OB2 + MH, OB3 = OW3 + MH;
+static_assert(OB3 + 1 == NP, "parameter layout");
+constexpr int KF = 17;  // neighbours per feature point (k = 16 and the point)
+
+// ---------------------------------------------------------------------------
+// features
+// ---------------------------------------------------------------------------
+template <int P, int Q>
+__device__ __forceinline__ void jacobi_pair(float (&A)[3][3], float (&V)[3][3]) {
+  const float apq = A[P][Q];
+  if (fabsf(apq) < 1e-30f) return;
+  const float theta = (A[Q][Q] - A[P][P]) / (2.0f * apq);
+  const float t = copysignf(1.0f, theta) / (fabsf(theta) + sqrtf(theta * theta + 1.0f));
+  const float c = rsqrtf(t * t + 1.0f), s = t * c;
+  const float app = A[P][P], aqq = A[Q][Q];
+  A[P][P] = app - t * apq;
+  A[Q][Q] = aqq + t * apq;
+  A[P][Q] = A[Q][P] = 0.0f;
+  constexpr int R = 3 - P - Q;  // the third index
+  const float arp = A[R][P], arq = A[R][Q];
+  A[R][P] = A[P][R] = c * arp - s * arq;
+  A[R][Q] = A[Q][R] = s * arp + c * arq;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const float vp = V[r][P], vq = V[r][Q];
+    V[r][P] = c * vp - s * vq;
+    V[r][Q] = s * vp + c * vq;
+  }
+}
+
+// f0..2 |normal|, f3 curvature, f4 planarity, f5 log K-th distance,
+// f6 |offset from the local plane| / r, f7 |offset from the centroid| / r
+__global__ __launch_bounds__(256) void k_features(const float *__restrict__ x,
+                                                  const float *__restrict__ y,
+                                                  const float *__restrict__ z,
+                                                  const u64 *__restrict__ pairs,
+                                                  const int32_t *__restrict__ counts,
+                                                  const u32 *__restrict__ cand, size_t n_cand,
+                                                  size_t n, float *__restrict__ feat) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n_cand;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const u32 i = cand ? cand[t] : (u32)t;
+    const int m = i < n ? min((int)counts[i], KF) : 0;
+    float f[MI] = {0, 0, 0, 1, 0, 0, 0, 0};
+    if (m >= 3) {
+      const float px = x[i], py = y[i], pz = z[i];
+      float dx[KF], dy[KF], dz[KF];
+      float cx = 0, cy = 0, cz = 0;
+      float r2 = 0.0f;
+#pragma unroll
+      for (int j = 0; j < KF; ++j) {
+        if (j < m) {
+          const u64 key = pairs[(size_t)i * KF + j];
+          const int q = nbr_idx(key) & 0x7FFFFFFF;
+          dx[j] = x[q] - px;
+          dy[j] = y[q] - py;
+          dz[j] = z[q] - pz;
+          cx += dx[j];
+          cy += dy[j];
+          cz += dz[j];
+          r2 = nbr_d2(key);
+        } else {
+          dx[j] = dy[j] = dz[j] = 0.0f;
+        }
+      }
+      const float inv = 1.0f / (float)m;
+      cx *= inv; cy *= inv; cz *= inv;
+      float A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+      for (int j = 0; j < KF; ++j) {
+        if (j < m) {
+          const float ex = dx[j] - cx, ey = dy[j] - cy, ez = dz[j] - cz;
+          A[0][0] += ex * ex; A[0][1] += ex * ey; A[0][2] += ex * ez;
+          A[1][1] += ey * ey; A[1][2] += ey * ez; A[2][2] += ez * ez;
+        }
+      }
+      A[1][0] = A[0][1]; A[2][0] = A[0][2]; A[2][1] = A[1][2];
+      float V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll 1
+      for (int sweep = 0; sweep < 6; ++sweep) {
+        jacobi_pair<0, 1>(A, V);
+        jacobi_pair<0, 2>(A, V);
+        jacobi_pair<1, 2>(A, V);
+      }
+      float l0 = A[0][0], l1 = A[1][1], l2 = A[2][2];
+      float nx = V[0][0], ny = V[1][0], nz = V[2][0];
+      // smallest eigenvalue and its vector; then order the other two
+      if (l1 < l0) { const float tl = l0; l0 = l1; l1 = tl; nx = V[0][1]; ny = V[1][1]; nz = V[2][1]; }
+      if (l2 < l0) { const float tl = l0; l0 = l2; l2 = tl; nx = V[0][2]; ny = V[1][2]; nz = V[2][2]; }
+      if (l2 < l1) { const float tl = l1; l1 = l2; l2 = tl; }
+      l0 = fmaxf(l0, 0.0f);
+      const float sum = l0 + l1 + l2;
+      const float r = sqrtf(r2) + 1e-6f;
+      f[0] = fabsf(nx);
+      f[1] = fabsf(ny);
+      f[2] = fabsf(nz);
+      f[3] = sum > 0.0f ? l0 / sum : 1.0f;
+      f[4] = l2 > 0.0f ? (l1 - l0) / l2 : 0.0f;
+      f[5] = logf(r);
+      f[6] = fabsf(nx * cx + ny * cy + nz * cz) / r;
+      f[7] = sqrtf(cx * cx + cy * cy + cz * cz) / r;
+    }
+#pragma unroll
+    for (int k = 0; k < MI; ++k) feat[t * MI + k] = f[k];
+  }
+}
+
+__global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t *frame) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n_frames - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((u64)offs[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    frame[i] = lo;
+  }
+}
+
+__global__ void k_mark_cand(const u32 *cand, size_t n_cand, size_t n, uint8_t *is_cand) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n_cand;
+       t += (size_t)gridDim.x * blockDim.x)
+    if (cand[t] < n) is_cand[cand[t]] = 1;
+}
+
+// grid positions of the candidates open at level 0, the rest done
+__global__ void k_open_cand(const float4 *pts, const u64 *n_dev, const uint8_t *is_cand,
+                            uint8_t *qlevel) {
+  const u64 n = *n_dev;
+  for (u64 pos = blockIdx.x * (u64)blockDim.x + threadIdx.x; pos < n;
+       pos += (u64)gridDim.x * blockDim.x) {
+    const u32 idx = __float_as_uint(pts[pos].w) & 0x7FFFFFFFu;
+    qlevel[pos] = (!is_cand || is_cand[idx]) ? 0 : 0xFF;
+  }
+}
+
+__global__ void k_widen32(const u32 *a, u64 *b) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *b = *a;
+}
+
+// ---------------------------------------------------------------------------
+// MLP
+// ---------------------------------------------------------------------------
+__global__ void k_quantize(const float *w, __nv_bfloat16 *wq, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    wq[i] = __float2bfloat16_rn(w[i]);
+}
+
+__device__ __forceinline__ void load_weights(const __nv_bfloat16 *wq, const float *norm,
+                                             float *sw, float *snorm) {
+  for (int i = threadIdx.x; i < NP; i += blockDim.x) sw[i] = __bfloat162float(wq[i]);
+  for (int i = threadIdx.x; i < 2 * MI; i += blockDim.x) snorm[i] = norm[i];
+  __syncthreads();
+}
+
+__device__ __forceinline__ void normalise(const float *__restrict__ feat, size_t i,
+                                          const float *snorm, float (&xn)[MI]) {
+#pragma unroll
+  for (int k = 0; k < MI; ++k) xn[k] = (feat[i * MI + k] - snorm[k]) * snorm[MI + k];
+}
+
+// logits, one thread per point
+__global__ __launch_bounds__(256) void k_mlp_forward(const float *__restrict__ feat, size_t n,
+                                                     const __nv_bfloat16 *__restrict__ wq,
+                                                     const float *__restrict__ norm,
+                                                     float *__restrict__ logits) {
+  __shared__ __align__(16) float sw[NP + 3];
+  __shared__ float snorm[2 * MI];
+  load_weights(wq, norm, sw, snorm);
+  // one point per thread: a grid-stride loop would let the compiler hoist
+  // the weight loads out of it into (spilled) registers
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) {
+    float xn[MI];
+    normalise(feat, i, snorm, xn);
+    float h1[MH];
+#pragma unroll
+    for (int h = 0; h < MH; ++h) {
+      float s = sw[OB1 + h];
+#pragma unroll
+      for (int k = 0; k < MI; ++k) s = fmaf(sw[OW1 + h * MI + k], xn[k], s);
+      h1[h] = fmaxf(s, 0.0f);
+    }
+    float out = sw[OB3];
+#pragma unroll 1
+    for (int j = 0; j < MH; ++j) {
+      float s = sw[OB2 + j];
+#pragma unroll
+      for (int h = 0; h < MH; ++h) s = fmaf(sw[OW2 + j * MH + h], h1[h], s);
+      out = fmaf(sw[OW3 + j], fmaxf(s, 0.0f), out);
+    }
+    logits[i] = out;
+  }
+}
+
+constexpr int TB = 128;  // points per training block
+// rows kept per point for the gradient reduction
+constexpr int RH1 = 0, RD2 = RH1 + MH, RD1 = RD2 + MH, RH2 = RD1 + MH, RX = RH2 + MH,
+              RG = RX + MI, ROW = RG + 1;  // 265 floats
+constexpr size_t TRAIN_SMEM = (size_t)(NP + 3 + 2 * MI + TB * ROW) * sizeof(float);
+
+// Forward + backward of mean binary cross-entropy with logits over n points
+// (labels 0/1), gradients added to grad, the loss sum to loss_sum.
+__global__ __launch_bounds__(TB) void k_mlp_train(const float *__restrict__ feat,
+                                                  const float *__restrict__ labels, size_t n,
+                                                  const __nv_bfloat16 *__restrict__ wq,
+                                                  const float *__restrict__ norm, float *grad,
+                                                  double *loss_sum) {
+  extern __shared__ __align__(16) float sm[];
+  float *sw = sm;
+  float *snorm = sw + NP + 3;
+  float *rows = snorm + 2 * MI;
+  load_weights(wq, norm, sw, snorm);
+  const int tid = threadIdx.x;
+  const float inv_n = 1.0f / (float)n;
+  // this thread's share of the gradient: 32 of W2, 4 of W1, and one or two
+  // of the 193 vector entries (b1, b2, w3, b3)
+  float gw2[32], gw1[4], gv[2] = {0.0f, 0.0f};
+#pragma unroll
+  for (int r = 0; r < 32; ++r) gw2[r] = 0.0f;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) gw1[r] = 0.0f;
+  float loss = 0.0f;
+  for (size_t base = (size_t)blockIdx.x * TB; base < n; base += (size_t)gridDim.x * TB) {
+    const size_t i = base + tid;
+    float *row = rows + tid * ROW;
+    if (i < n) {
+      float xn[MI];
+      normalise(feat, i, snorm, xn);
+      float h1[MH];
+#pragma unroll
+      for (int h = 0; h < MH; ++h) {
+        float s = sw[OB1 + h];
+#pragma unroll
+        for (int k = 0; k < MI; ++k) s = fmaf(sw[OW1 + h * MI + k], xn[k], s);
+        h1[h] = fmaxf(s, 0.0f);
+        row[RH1 + h] = h1[h];
+      }
+      float out = sw[OB3];
+#pragma unroll 4
+      for (int j = 0; j < MH; ++j) {
+        float s = sw[OB2 + j];
+#pragma unroll
+        for (int h = 0; h < MH; ++h) s = fmaf(sw[OW2 + j * MH + h], h1[h], s);
+        const float a = fmaxf(s, 0.0f);
+        row[RH2 + j] = a;
+        out = fmaf(sw[OW3 + j], a, out);
+      }
+      const float yl = labels[i];
+      // softplus(out) - y*out, stable
+      loss += fmaxf(out, 0.0f) - yl * out + log1pf(expf(-fabsf(out)));
+      const float g = (1.0f / (1.0f + expf(-out)) - yl) * inv_n;
+      row[RG] = g;
+#pragma unroll
+      for (int k = 0; k < MI; ++k) row[RX + k] = xn[k];
+      // delta2_j = g * w3_j * [h2_j > 0]; delta1_h = sum_j W2[j][h] delta2_j * [h1_h > 0]
+      float d1[MH];
+#pragma unroll
+      for (int h = 0; h < MH; ++h) d1[h] = 0.0f;
+#pragma unroll 4
+      for (int j = 0; j < MH; ++j) {
+        const float d2 = row[RH2 + j] > 0.0f ? g * sw[OW3 + j] : 0.0f;
+        row[RD2 + j] = d2;
+#pragma unroll
+        for (int h = 0; h < MH; ++h) d1[h] = fmaf(sw[OW2 + j * MH + h], d2, d1[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < MH; ++h) row[RD1 + h] = h1[h] > 0.0f ? d1[h] : 0.0f;
+    } else {
+      for (int c = 0; c < ROW; ++c) row[c] = 0.0f;
+    }
+    __syncthreads();
+    {
+      // W2[j][h] += D2[b][j] * H1[b][h] for j = tid / 2, h = (tid % 2) * 32 + r
+      const int j = tid >> 1, h0 = (tid & 1) * 32;
+      for (int b = 0; b < TB; ++b) {
+        const float *rb = rows + b * ROW;
+        const float d2 = rb[RD2 + j];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) gw2[r] = fmaf(d2, rb[RH1 + h0 + r], gw2[r]);
+      }
+      // W1[h][k] += D1[b][h] * X[b][k] for h = tid / 2, k = (tid % 2) * 4 + r
+      const int h = tid >> 1, k0 = (tid & 1) * 4;
+      for (int b = 0; b < TB; ++b) {
+        const float *rb = rows + b * ROW;
+        const float d1 = rb[RD1 + h];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) gw1[r] = fmaf(d1, rb[RX + k0 + r], gw1[r]);
+      }
+      // vector entries v = tid and tid + TB over [b1 | b2 | w3 | b3]
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int v = tid + e * TB;
+        if (v > 3 * MH) continue;
+        float s = 0.0f;
+        for (int b = 0; b < TB; ++b) {
+          const float *rb = rows + b * ROW;
+          s += v < MH ? rb[RD1 + v]
+                      : (v < 2 * MH ? rb[RD2 + v - MH]
+                                    : (v < 3 * MH ? rb[RG] * rb[RH2 + v - 2 * MH] : rb[RG]));
+        }
+        gv[e] += s;
+      }
+    }
+    __syncthreads();
+  }
+  {
+    const int j = tid >> 1, h0 = (tid & 1) * 32;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) atomicAdd(&grad[OW2 + j * MH + h0 + r], gw2[r]);
+    const int h = tid >> 1, k0 = (tid & 1) * 4;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) atomicAdd(&grad[OW1 + h * MI + k0 + r], gw1[r]);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int v = tid + e * TB;
+      if (v > 3 * MH) continue;
+      const int dst = v < MH ? OB1 + v : (v < 2 * MH ? OB2 + v - MH : (v < 3 * MH ? OW3 + v - 2 * MH : OB3));
+      atomicAdd(&grad[dst], gv[e]);
+    }
+  }
+  // loss: warp sums, one double atomic per warp
+  for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+  if ((tid & 31) == 0) atomicAdd(loss_sum, (double)loss);
+}
+
+__global__ void k_adam(float *w, const float *g, float *m, float *v, int n, float lr, float b1,
+                       float b2, float eps, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  }
+}
+
+// per-frame inclusive prefix sums (double) of candidate weights; one block
+// per frame
+__global__ __launch_bounds__(256) void k_cdf(const float *w, const int64_t *coffs, double *cdf) {
+  const int f = blockIdx.x;
+  const int64_t a = coffs[f], b = coffs[f + 1];
+  __shared__ double warp_tot[8];
+  __shared__ double carry;
+  if (threadIdx.x == 0) carry = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t c0 = a; c0 < b; c0 += 256) {
+    const int64_t i = c0 + threadIdx.x;
+    double v = i < b ? (double)fmaxf(w[i], 0.0f) : 0.0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const double t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_tot[wid] = v;
+    __syncthreads();
+    double before = carry;
+    for (int k = 0; k < wid; ++k) before += warp_tot[k];
+    if (i < b) cdf[i] = before + v;
+    __syncthreads();
+    if (threadIdx.x == 255) carry = before + v;
+    __syncthreads();
+  }
+}
+
+// labels: 1 for points within thresh of their frame's model, else 0
+__global__ void k_plane_labels(const float *x, const float *y, const float *z, const int32_t *frame,
+                               size_t n, const float *models, float t, float *labels) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float *m = models + 4 * frame[i];
+    const float d = fadd(fadd(fadd(fmul(m[0], x[i]), fmul(m[1], y[i])), fmul(m[2], z[i])), m[3]);
+    labels[i] = fabsf(d) <= t ? 1.0f : 0.0f;
+  }
+}
+
+}  // namespace
+}  // namespace rvp
+
+struct rvp_scorer {
+  rvp_context *ctx = nullptr;
+  size_t max_points = 0;
+  int max_frames = 0;
+  rvp::Grid grid;
+  rvp::DevBuf frame_of, is_cand, pairs, counts, hard, qlevel, qtau, open;
+  rvp::DevBuf w, wq, m, v, grad, norm, loss;
+  int adam_step = 0;
+};
+
+namespace {
+// a temporary device buffer released on every path out of its scope
+struct TmpBuf : rvp::DevBuf {
+  TmpBuf() = default;
+  TmpBuf(const TmpBuf &) = delete;
+  TmpBuf &operator=(const TmpBuf &) = delete;
+  ~TmpBuf() { release(); }
+};
+
+template <class F>
+rvp_status sguard(rvp_context *ctx, F &&f) {
+  try {
+    f();
+    return RVP_OK;
+  } catch (const rvp::Error &e) {
+    if (ctx) ctx->last_error = e.msg;
+    return e.status;
+  } catch (const std::bad_alloc &) {
+    if (ctx) ctx->last_error = "host allocation failed";
+    return RVP_ERR_OOM;
+  } catch (...) {
+    if (ctx) ctx->last_error = "unknown error";
+    return RVP_ERR_CUDA;
+  }
+}
+size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+double clamp_prob(float p) {
+  double pc = (double)p;
+  return pc < 0.5 ? 0.5 : (pc > 0.9999 ? 0.9999 : pc);
+}
+}  // namespace
+
+extern "C" {
+
+rvp_status rvp_scorer_create(rvp_context *ctx, size_t max_points, int max_frames,
+                             rvp_scorer **out) {
+  if (!ctx || !out || max_frames < 1) return RVP_ERR_INVALID_ARG;
+  *out = nullptr;
+  rvp_scorer *s = new (std::nothrow) rvp_scorer;
+  if (!s) return RVP_ERR_OOM;
+  s->ctx = ctx;
+  s->max_points = max_points > 0 ? max_points : 1;
+  s->max_frames = max_frames;
+  rvp_status st = sguard(ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    const size_t N = s->max_points;
+    s->grid.reserve(N, max_frames);
+    s->frame_of.reserve(N * 4);
+    s->is_cand.reserve(N);
+    s->pairs.reserve(N * rvp::KF * 8);
+    s->counts.reserve(N * 4);
+    s->hard.reserve(N * 8 + 256);
+    s->qlevel.reserve(N);
+    s->qtau.reserve(N * 4);
+    s->open.reserve(al256(N * 4) + al256(N * 8 + 8) + al256(N * 4) + 256 + rvp::scan_temp_bytes(N));
+    s->w.reserve(rvp::NP * 4);
+    s->wq.reserve(rvp::NP * 2);
+    s->m.reserve(rvp::NP * 4);
+    s->v.reserve(rvp::NP * 4);
+    s->grad.reserve(rvp::NP * 4);
+    s->norm.reserve(2 * rvp::MI * 4);
+    s->loss.reserve(16);
+    // He-style uniform initial weights from a fixed seed, zero biases;
+    // identity normalisation until rvp_mlp_set_norm
+    std::vector<float> w0(rvp::NP, 0.0f);
+    unsigned long long st64 = 0x243F6A8885A308D3ull;
+    auto uni = [&] {
+      st64 = st64 * 6364136223846793005ull + 1442695040888963407ull;
+      return ((st64 >> 11) * 0x1.0p-53) * 2.0 - 1.0;
+    };
+    for (int i = 0; i < rvp::MH * rvp::MI; ++i) w0[rvp::OW1 + i] = (float)(uni() * sqrt(6.0 / rvp::MI));
+    for (int i = 0; i < rvp::MH * rvp::MH; ++i) w0[rvp::OW2 + i] = (float)(uni() * sqrt(6.0 / rvp::MH));
+    for (int i = 0; i < rvp::MH; ++i) w0[rvp::OW3 + i] = (float)(uni() * sqrt(3.0 / rvp::MH));
+    std::vector<float> nm(2 * rvp::MI);
+    for (int k = 0; k < rvp::MI; ++k) { nm[k] = 0.0f; nm[rvp::MI + k] = 1.0f; }
+    RVP_CUDA_TRY(cudaMemcpy(s->w.ptr, w0.data(), rvp::NP * 4, cudaMemcpyHostToDevice));
+    RVP_CUDA_TRY(cudaMemcpy(s->norm.ptr, nm.data(), nm.size() * 4, cudaMemcpyHostToDevice));
+    RVP_CUDA_TRY(cudaMemset(s->m.ptr, 0, rvp::NP * 4));
+    RVP_CUDA_TRY(cudaMemset(s->v.ptr, 0, rvp::NP * 4));
+    rvp::k_quantize<<<8, 256, 0, ctx->stream>>>(s->w.as<float>(), s->wq.as<__nv_bfloat16>(), rvp::NP);
+    RVP_LAUNCH_CHECK(ctx);
+    RVP_CUDA_TRY(cudaFuncSetAttribute(rvp::k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)rvp::TRAIN_SMEM));
+    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  });
+  if (st != RVP_OK) {
+    rvp_scorer_destroy(s);
+    return st;
+  }
+  *out = s;
+  return RVP_OK;
+}
+
+rvp_status rvp_scorer_destroy(rvp_scorer *s) {
+  if (!s) return RVP_ERR_INVALID_ARG;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  rvp::DevBuf *bufs[] = {&s->frame_of, &s->is_cand, &s->pairs, &s->counts, &s->hard, &s->qlevel,
+                         &s->qtau, &s->open, &s->w, &s->wq, &s->m, &s->v, &s->grad, &s->norm,
+                         &s->loss};
+  for (auto *b : bufs) b->release();
+  s->grid.release();
+  delete s;
+  return RVP_OK;
+}
+
+rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, const float *z,
+                               const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
+                               float cell_size, const uint32_t *cand, size_t n_cand,
+                               float *features) {
+  if (!s) return RVP_ERR_INVALID_ARG;
+  rvp_context *ctx = s->ctx;
+  return sguard(ctx, [&] {
+    RVP_REQUIRE(x && y && z && frame_offsets_dev && features, "null pointer");
+    RVP_REQUIRE(n_frames >= 1 && n_frames <= s->max_frames, "n_frames out of range");
+    RVP_REQUIRE(n_points >= 1 && n_points <= s->max_points, "n_points out of range");
+    RVP_REQUIRE(cell_size > 0.0f, "cell_size must be > 0");
+    if (!cand) n_cand = n_points;
+    RVP_REQUIRE(n_cand <= n_points, "more candidates than points");
+    if (n_cand == 0) return;
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t N = n_points;
+    const int sms = ctx->num_sms;
+    const unsigned gb = rvp::grid_for(N, 256, sms * 16);
+    rvp::grid_build(ctx, s->grid, x, y, z, frame_offsets_dev, n_frames, N, cell_size,
+                    rvp::KEY_DENSE, 0, 0, nullptr);
+    rvp::k_frame_of<<<gb, 256, 0, st>>>(frame_offsets_dev, n_frames, N, s->frame_of.as<int32_t>());
+    RVP_LAUNCH_CHECK(ctx);
+    const rvp::GridView gv = s->grid.view(rvp::KEY_DENSE, 0, 0);
+    uint8_t *is_cand = nullptr;
+    if (cand) {
+      is_cand = s->is_cand.as<uint8_t>();
+      RVP_CUDA_TRY(cudaMemsetAsync(is_cand, 0, N, st));
+      rvp::k_mark_cand<<<rvp::grid_for(n_cand, 256, sms * 16), 256, 0, st>>>(cand, n_cand, N,
+                                                                            is_cand);
+      RVP_LAUNCH_CHECK(ctx);
+    }
+    rvp::k_open_cand<<<gb, 256, 0, st>>>(gv.pts, gv.n_points, is_cand, s->qlevel.as<uint8_t>());
+    RVP_LAUNCH_CHECK(ctx);
+    u64 *hard_n64 = s->hard.as<u64>();
+    u32 *hard_n = reinterpret_cast<u32 *>(hard_n64 + 1);
+    u32 *hard = reinterpret_cast<u32 *>(hard_n64 + 2);
+    float *hard_tau = reinterpret_cast<float *>(hard + N);
+    RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
+    rvp::TileArgs ta{};
+    ta.frame_of = s->frame_of.as<int32_t>();
+    ta.pairs = s->pairs.as<u64>();
+    ta.counts = s->counts.as<int32_t>();
+    ta.hard = hard;
+    ta.hard_count = hard_n;
+    ta.hard_tau = hard_tau;
+    ta.qlevel = s->qlevel.as<uint8_t>();
+    ta.qtau = s->qtau.as<float>();
+    ta.rfac = 1.0f;
+    ta.level0_warp = true;
+    ta.preset_open = true;
+    char *op = s->open.as<char>();
+    ta.open_flags = reinterpret_cast<u32 *>(op); op += al256(N * 4);
+    ta.open_pos = reinterpret_cast<u64 *>(op); op += al256(N * 8 + 8);
+    ta.open_list = reinterpret_cast<u32 *>(op); op += al256(N * 4);
+    ta.open_n = reinterpret_cast<u64 *>(op); op += 256;
+    ta.scan_tmp = op;
+    ta.n_max = N;
+    RVP_REQUIRE(rvp::grid_knn_tile(ctx, gv, rvp::KF, rvp::TILE_PAIRS, ta, 0, nullptr),
+                "kNN tile path unavailable");
+    rvp::k_widen32<<<1, 32, 0, st>>>(hard_n, hard_n64);
+    RVP_LAUNCH_CHECK(ctx);
+    rvp::QuerySet qh{x, y, z, N, hard_n64, s->frame_of.as<int32_t>(),
+                     reinterpret_cast<int32_t *>(hard)};
+    qh.bound = hard_tau;
+    rvp::grid_knn(ctx, gv, qh, rvp::KF, 0.0f, s->pairs.as<u64>(), s->counts.as<int32_t>(), 1, 256,
+                  nullptr, rvp::KNN_OUT_BY_QUERY, nullptr);
+    rvp::k_features<<<rvp::grid_for(n_cand, 256, sms * 16), 256, 0, st>>>(
+        x, y, z, s->pairs.as<u64>(), s->counts.as<int32_t>(), cand, n_cand, N, features);
+    RVP_LAUNCH_CHECK(ctx);
+  });
+}
+
+rvp_status rvp_mlp_set_params(rvp_scorer *s, const float *params) {
+  if (!s || !params) return RVP_ERR_INVALID_ARG;
+  return sguard(s->ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
+    RVP_CUDA_TRY(cudaMemcpyAsync(s->w.ptr, params, rvp::NP * 4, cudaMemcpyHostToDevice,
+                                 s->ctx->stream));
+    RVP_CUDA_TRY(cudaMemsetAsync(s->m.ptr, 0, rvp::NP * 4, s->ctx->stream));
+    RVP_CUDA_TRY(cudaMemsetAsync(s->v.ptr, 0, rvp::NP * 4, s->ctx->stream));
+    s->adam_step = 0;
+    rvp::k_quantize<<<8, 256, 0, s->ctx->stream>>>(s->w.as<float>(), s->wq.as<__nv_bfloat16>(),
+                                                   rvp::NP);
+    RVP_LAUNCH_CHECK(s->ctx);
+    RVP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  });
+}
+
+rvp_status rvp_mlp_get_params(rvp_scorer *s, float *params) {
+  if (!s || !params) return RVP_ERR_INVALID_ARG;
+  return sguard(s->ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
+    RVP_CUDA_TRY(cudaMemcpyAsync(params, s->w.ptr, rvp::NP * 4, cudaMemcpyDeviceToHost,
+                                 s->ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  });
+}
+
+rvp_status rvp_mlp_set_norm(rvp_scorer *s, const float *mean, const float *stddev) {
+  if (!s || !mean || !stddev) return RVP_ERR_INVALID_ARG;
+  return sguard(s->ctx, [&] {
+    float nm[2 * rvp::MI];
+    for (int k = 0; k < rvp::MI; ++k) {
+      RVP_REQUIRE(stddev[k] > 0.0f, "stddev must be > 0");
+      nm[k] = mean[k];
+      nm[rvp::MI + k] = 1.0f / stddev[k];
+    }
+    RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
+    RVP_CUDA_TRY(cudaMemcpyAsync(s->norm.ptr, nm, sizeof(nm), cudaMemcpyHostToDevice,
+                                 s->ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+  });
+}
+
+rvp_status rvp_mlp_forward(rvp_scorer *s, const float *features, size_t n, float *logits) {
+  if (!s) return RVP_ERR_INVALID_ARG;
+  return sguard(s->ctx, [&] {
+    if (n == 0) return;
+    RVP_REQUIRE(features && logits, "null pointer");
+    RVP_REQUIRE(n <= (size_t)0xFFFFFFFFull * 256, "too many points");
+    RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
+    rvp::k_mlp_forward<<<(unsigned)((n + 255) / 256), 256, 0, s->ctx->stream>>>(
+        features, n, s->wq.as<__nv_bfloat16>(), s->norm.as<float>(), logits);
+    RVP_LAUNCH_CHECK(s->ctx);
+  });
+}
+
+namespace {
+void mlp_grad(rvp_scorer *s, const float *features, const float *labels, size_t n) {
+  rvp_context *ctx = s->ctx;
+  RVP_CUDA_TRY(cudaMemsetAsync(s->grad.ptr, 0, rvp::NP * 4, ctx->stream));
+  RVP_CUDA_TRY(cudaMemsetAsync(s->loss.ptr, 0, 8, ctx->stream));
+  const unsigned blocks =
+      (unsigned)std::min<size_t>((n + rvp::TB - 1) / rvp::TB, (size_t)ctx->num_sms);
+  rvp::k_mlp_train<<<blocks, rvp::TB, rvp::TRAIN_SMEM, ctx->stream>>>(
+      features, labels, n, s->wq.as<__nv_bfloat16>(), s->norm.as<float>(), s->grad.as<float>(),
+      s->loss.as<double>());
+  RVP_LAUNCH_CHECK(ctx);
+}
+}  // namespace
+
+rvp_status rvp_mlp_gradients(rvp_scorer *s, const float *features, const float *labels,
+                             size_t n, float *grad, double *loss) {
+  if (!s || !grad || !loss) return RVP_ERR_INVALID_ARG;
+  return sguard(s->ctx, [&] {
+    RVP_REQUIRE(n > 0 && features && labels, "empty batch");
+    RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
+    mlp_grad(s, features, labels, n);
+    double l = 0.0;
+    RVP_CUDA_TRY(cudaMemcpyAsync(grad, s->grad.ptr, rvp::NP * 4, cudaMemcpyDeviceToHost,
+                                 s->ctx->stream));
+    RVP_CUDA_TRY(cudaMemcpyAsync(&l, s->loss.ptr, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+    *loss = l / (double)n;
+  });
+}
+
+rvp_status rvp_mlp_train_step(rvp_scorer *s, const float *features, const float *labels,
+                              size_t n, float lr, double *loss) {
+  if (!s || !(lr > 0.0f)) return RVP_ERR_INVALID_ARG;
+  return sguard(s->ctx, [&] {
+    RVP_REQUIRE(n > 0 && features && labels, "empty batch");
+    RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
+    mlp_grad(s, features, labels, n);
+    s->adam_step++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f / (1.0f - powf(b1, (float)s->adam_step));
+    const float c2 = 1.0f / (1.0f - powf(b2, (float)s->adam_step));
+    rvp::k_adam<<<8, 256, 0, s->ctx->stream>>>(s->w.as<float>(), s->grad.as<float>(),
+                                               s->m.as<float>(), s->v.as<float>(), rvp::NP, lr,
+                                               b1, b2, 1e-8f, c1, c2);
+    RVP_LAUNCH_CHECK(s->ctx);
+    rvp::k_quantize<<<8, 256, 0, s->ctx->stream>>>(s->w.as<float>(), s->wq.as<__nv_bfloat16>(),
+                                                   rvp::NP);
+    RVP_LAUNCH_CHECK(s->ctx);
+    if (loss) {
+      double l = 0.0;
+      RVP_CUDA_TRY(cudaMemcpyAsync(&l, s->loss.ptr, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
+      RVP_CUDA_TRY(cudaStreamSynchronize(s->ctx->stream));
+      *loss = l / (double)n;
+    }
+  });
+}
+
+rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const float *y, const float *z,
+                             const int64_t *frame_offsets_dev, int n_frames, int max_iters,
+                             float dist_thresh, float collinear_thresh, float probability,
+                             const int32_t *targets, float *models, int32_t *best,
+                             int32_t *iters_run) {
+  if (!ctx) return RVP_ERR_INVALID_ARG;
+  return sguard(ctx, [&] {
+    RVP_REQUIRE(x && y && z && frame_offsets_dev && models && best, "null pointer");
+    RVP_REQUIRE(n_frames >= 1 && max_iters >= 1, "n_frames / max_iters must be >= 1");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    // the reference's srand(0) + rand() stream, drawn from libc, with the
+    // generator left where the reference's last call leaves it
+    const size_t R = 3 * (size_t)max_iters;
+    std::vector<int32_t> rs(R);
+    srand(0);
+    for (size_t i = 0; i < R; ++i) rs[i] = rand();
+    TmpBuf drand;
+    drand.reserve(R * 4);
+    RVP_CUDA_TRY(cudaMemcpyAsync(drand.ptr, rs.data(), R * 4, cudaMemcpyHostToDevice, ctx->stream));
+    rvp::RansacParams prm{dist_thresh, max_iters, collinear_thresh,
+                          log(1.0 - clamp_prob(probability))};
+    rvp::RansacSampler smp;
+    smp.targets = targets;
+    std::vector<int32_t> it(n_frames, 0);
+    int32_t *di = iters_run;
+    TmpBuf tmp;
+    if (!di) {
+      tmp.reserve((size_t)n_frames * 4);
+      di = tmp.as<int32_t>();
+    }
+    rvp::ransac_frames(ctx, x, y, z, frame_offsets_dev, n_frames, drand.as<int>(), prm, models,
+                       best, di, nullptr, false, smp);
+    RVP_CUDA_TRY(cudaMemcpyAsync(it.data(), di, (size_t)n_frames * 4, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    srand(0);
+    for (long i = 0; i < 3L * it[n_frames - 1]; ++i) (void)rand();
+  });
+}
+
+rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y, const float *z,
+                               const int64_t *frame_offsets_dev, int n_frames,
+                               const uint32_t *cand, const int64_t *cand_offsets_dev,
+                               const float *weights, uint64_t seed, int max_iters,
+                               float dist_thresh, float collinear_thresh, float probability,
+                               const int32_t *targets, float *models, int32_t *best,
+                               int32_t *iters_run) {
+  if (!ctx) return RVP_ERR_INVALID_ARG;
+  return sguard(ctx, [&] {
+    RVP_REQUIRE(x && y && z && frame_offsets_dev && cand && cand_offsets_dev && weights &&
+                    models && best,
+                "null pointer");
+    RVP_REQUIRE(n_frames >= 1 && max_iters >= 1, "n_frames / max_iters must be >= 1");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    int64_t n_cand = 0;
+    RVP_CUDA_TRY(cudaMemcpyAsync(&n_cand, cand_offsets_dev + n_frames, 8, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    TmpBuf cdf;
+    cdf.reserve((size_t)std::max<int64_t>(n_cand, 1) * 8);
+    rvp::k_cdf<<<n_frames, 256, 0, ctx->stream>>>(weights, cand_offsets_dev, cdf.as<double>());
+    RVP_LAUNCH_CHECK(ctx);
+    rvp::RansacParams prm{dist_thresh, max_iters, collinear_thresh,
+                          log(1.0 - clamp_prob(probability))};
+    rvp::RansacSampler smp;
+    smp.cand = cand;
+    smp.cand_offs = cand_offsets_dev;
+    smp.cdf = cdf.as<double>();
+    smp.seed = seed;
+    smp.targets = targets;
+    rvp::ransac_frames(ctx, x, y, z, frame_offsets_dev, n_frames, nullptr, prm, models, best,
+                       iters_run, nullptr, false, smp);
+    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+rvp_status rvp_plane_labels(rvp_context *ctx, const float *x, const float *y, const float *z,
+                            const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
+                            const float *models, float dist_thresh, float *labels) {
+  if (!ctx) return RVP_ERR_INVALID_ARG;
+  return sguard(ctx, [&] {
+    RVP_REQUIRE(x && y && z && frame_offsets_dev && models && labels, "null pointer");
+    RVP_REQUIRE(n_frames >= 1, "n_frames must be >= 1");
+    if (n_points == 0) return;
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    TmpBuf fr;
+    fr.reserve(n_points * 4);
+    const unsigned gb = rvp::grid_for(n_points, 256, ctx->num_sms * 16);
+    rvp::k_frame_of<<<gb, 256, 0, ctx->stream>>>(frame_offsets_dev, n_frames, n_points,
+                                                 fr.as<int32_t>());
+    RVP_LAUNCH_CHECK(ctx);
+    rvp::k_plane_labels<<<gb, 256, 0, ctx->stream>>>(x, y, z, fr.as<int32_t>(), n_points, models,
+                                                     dist_thresh, labels);
+    RVP_LAUNCH_CHECK(ctx);
+    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+}  // extern "C"

@@ -1,5 +1,6 @@
 // RANSAC plane fitting (segmentation/ransac_plane.cpp:18-111) for many
-// frames, one thread block per frame.
+// frames, one thread block per frame; optionally with hypotheses drawn by
+// per-point weight (the learned proposal) instead of the rand() stream.
 //
 // The reference draws three rand() % n indices per iteration after
 // srand(0); the raw rand() stream is the same for every call, so it is an
@@ -47,10 +48,28 @@ __device__ __forceinline__ bool is_inlier(const float4 &m, float x, float y, flo
   return fabsf(fadd(fadd(fadd(fmul(m.x, x), fmul(m.y, y)), fmul(m.z, z)), m.w)) <= t;
 }
 
+// One weighted draw: the candidate whose prefix-sum interval holds u * total,
+// returned relative to the frame's first point (a0).
+__device__ __forceinline__ u32 weighted_draw(const RansacSampler &smp, int f, int it, int k,
+                                             int64_t a0, u32 n) {
+  const int64_t c0 = smp.cand_offs[f], c1 = smp.cand_offs[f + 1];
+  const double total = smp.cdf[c1 - 1];
+  const u64 r = mix64(smp.seed ^ mix64(((u64)f << 34) ^ ((u64)it << 2) ^ (u64)k));
+  const double u = (double)(r >> 11) * 0x1.0p-53 * total;
+  int64_t lo = c0, hi = c1 - 1;  // first slot with cdf > u
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (smp.cdf[mid] > u) hi = mid; else lo = mid + 1;
+  }
+  const int64_t rel = (int64_t)smp.cand[lo] - a0;
+  return rel >= 0 && rel < (int64_t)n ? (u32)rel : 0xFFFFFFFFu;  // outside the frame: no hypothesis
+}
+
 __global__ __launch_bounds__(R_THREADS) void k_ransac(
     const float *__restrict__ X, const float *__restrict__ Y, const float *__restrict__ Z,
     const int64_t *offs, const int *__restrict__ rnd, RansacParams prm, float *model_out,
-    int32_t *best_out, int32_t *iters_out, int32_t *counts_all, bool eval_all) {
+    int32_t *best_out, int32_t *iters_out, int32_t *counts_all, bool eval_all,
+    RansacSampler smp) {
   const int f = blockIdx.x;
   const int64_t a0 = offs[f];
   const u32 n = (u32)(offs[f + 1] - a0);
@@ -64,7 +83,9 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
   __shared__ int s_best, s_kiters, s_stop, s_iters;
   __shared__ float4 s_model;
 
-  if (n < 3) {  // ransac_plane.cpp:59
+  const bool no_cand = smp.cdf && (smp.cand_offs[f + 1] - smp.cand_offs[f] < 3 ||
+                                   !(smp.cdf[smp.cand_offs[f + 1] - 1] > 0.0));
+  if (n < 3 || no_cand) {  // ransac_plane.cpp:59
     if (tid == 0) {
       model_out[4 * f + 0] = model_out[4 * f + 1] = model_out[4 * f + 2] = model_out[4 * f + 3] = 0;
       best_out[f] = 0;
@@ -91,10 +112,17 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
       float4 m = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);  // NaN: never an inlier
       int code = -3;
       if (it < prm.max_iters) {
-        const u32 i1 = (u32)rnd[3 * it + 0] % n;
-        const u32 i2 = (u32)rnd[3 * it + 1] % n;
-        const u32 i3 = (u32)rnd[3 * it + 2] % n;
-        if (i1 == i2 || i1 == i3 || i2 == i3) {
+        u32 i1, i2, i3;
+        if (smp.cdf) {
+          i1 = weighted_draw(smp, f, it, 0, a0, n);
+          i2 = weighted_draw(smp, f, it, 1, a0, n);
+          i3 = weighted_draw(smp, f, it, 2, a0, n);
+        } else {
+          i1 = (u32)rnd[3 * it + 0] % n;
+          i2 = (u32)rnd[3 * it + 1] % n;
+          i3 = (u32)rnd[3 * it + 2] % n;
+        }
+        if (i1 == i2 || i1 == i3 || i2 == i3 || i1 >= n || i2 >= n || i3 >= n) {
           code = -1;
         } else if (!plane_coeffs(x[i1], y[i1], z[i1], x[i2], y[i2], z[i2], x[i3], y[i3], z[i3],
                                  prm.collinear, m)) {
@@ -146,7 +174,14 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
         }
         if (hcode[h] != 0) continue;
         const int cur = (int)hcnt[h];
-        if (cur > s_best) {
+        if (cur > s_best && smp.targets) {
+          s_best = cur;
+          s_model = hyp[h];
+          if (cur >= smp.targets[f]) {
+            s_stop = 1;
+            s_iters = it + 1;
+          }
+        } else if (cur > s_best) {
           s_best = cur;
           s_model = hyp[h];
           const double w = (double)cur / (double)n;
@@ -228,10 +263,10 @@ inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 void ransac_frames(rvp_context *ctx, const float *x, const float *y, const float *z,
                    const int64_t *offs, int n_frames, const int *rand_dev, const RansacParams &p,
                    float *model, int32_t *best, int32_t *iters_run, int32_t *counts_all,
-                   bool eval_all) {
+                   bool eval_all, const RansacSampler &smp) {
   if (n_frames <= 0) return;
   k_ransac<<<n_frames, R_THREADS, 0, ctx->stream>>>(x, y, z, offs, rand_dev, p, model, best,
-                                                    iters_run, counts_all, eval_all);
+                                                    iters_run, counts_all, eval_all, smp);
   RVP_LAUNCH_CHECK(ctx);
 }
 
