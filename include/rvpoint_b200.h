@@ -323,14 +323,17 @@ RVP_API rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const flo
                                      int32_t *iters_run);
 /* RANSAC whose three points are drawn from each frame's candidates
  * (cand[cand_offsets[f] .. cand_offsets[f+1]), global point indices inside
- * frame f) with probability proportional to weights (one per candidate),
- * from a counter-based generator keyed by seed. Counting, model and the
+ * frame f) with probability proportional to their weight, from a
+ * counter-based generator keyed by seed. weights: one per candidate, used
+ * as given (negatives as 0) when logit_power is 0, else taken as logits and
+ * turned into sigmoid(w) ^ logit_power. Counting, model and the
  * strict-greater update are ransac_plane_rvv's. */
 RVP_API rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y,
                                        const float *z, const int64_t *frame_offsets_dev,
                                        int n_frames, const uint32_t *cand,
                                        const int64_t *cand_offsets_dev, const float *weights,
-                                       uint64_t seed, int max_iters, float dist_thresh,
+                                       float logit_power, uint64_t seed, int max_iters,
+                                       float dist_thresh,
                                        float collinear_thresh, float probability,
                                        const int32_t *targets, float *models, int32_t *best,
                                        int32_t *iters_run);

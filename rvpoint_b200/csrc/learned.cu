@@ -88,7 +88,7 @@ __global__ __launch_bounds__(256) void k_features(const float *__restrict__ x,
       for (int j = 0; j < KF; ++j) {
         if (j < m) {
           const u64 key = pairs[(size_t)i * KF + j];
-          const int q = nbr_idx(key) & 0x7FFFFFFF;
+          const u32 q = min((u32)(nbr_idx(key) & 0x7FFFFFFF), (u32)(n - 1));
           dx[j] = x[q] - px;
           dy[j] = y[q] - py;
           dz[j] = z[q] - pz;
@@ -375,7 +375,16 @@ __global__ void k_adam(float *w, const float *g, float *m, float *v, int n, floa
 
 // per-frame inclusive prefix sums (double) of candidate weights; one block
 // per frame
-__global__ __launch_bounds__(256) void k_cdf(const float *w, const int64_t *coffs, double *cdf) {
+__device__ __forceinline__ double cand_weight(float w, float logit_power) {
+  if (logit_power > 0.0f) {  // w is a logit: sigmoid(w) ^ power
+    const double p = 1.0 / (1.0 + exp(-(double)w));
+    return pow(p, (double)logit_power);
+  }
+  return (double)fmaxf(w, 0.0f);
+}
+
+__global__ __launch_bounds__(256) void k_cdf(const float *w, float logit_power,
+                                             const int64_t *coffs, double *cdf) {
   const int f = blockIdx.x;
   const int64_t a = coffs[f], b = coffs[f + 1];
   __shared__ double warp_tot[8];
@@ -385,7 +394,7 @@ __global__ __launch_bounds__(256) void k_cdf(const float *w, const int64_t *coff
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int64_t c0 = a; c0 < b; c0 += 256) {
     const int64_t i = c0 + threadIdx.x;
-    double v = i < b ? (double)fmaxf(w[i], 0.0f) : 0.0;
+    double v = i < b ? cand_weight(w[i], logit_power) : 0.0;
     for (int o = 1; o < 32; o <<= 1) {
       const double t = __shfl_up_sync(0xffffffffu, v, o);
       if (lane >= o) v += t;
@@ -571,6 +580,7 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
     u32 *hard = reinterpret_cast<u32 *>(hard_n64 + 2);
     float *hard_tau = reinterpret_cast<float *>(hard + N);
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
+    RVP_CUDA_TRY(cudaMemsetAsync(s->counts.ptr, 0, N * 4, st));
     rvp::TileArgs ta{};
     ta.frame_of = s->frame_of.as<int32_t>();
     ta.pairs = s->pairs.as<u64>();
@@ -760,10 +770,10 @@ rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const float *y, c
 rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y, const float *z,
                                const int64_t *frame_offsets_dev, int n_frames,
                                const uint32_t *cand, const int64_t *cand_offsets_dev,
-                               const float *weights, uint64_t seed, int max_iters,
-                               float dist_thresh, float collinear_thresh, float probability,
-                               const int32_t *targets, float *models, int32_t *best,
-                               int32_t *iters_run) {
+                               const float *weights, float logit_power, uint64_t seed,
+                               int max_iters, float dist_thresh, float collinear_thresh,
+                               float probability, const int32_t *targets, float *models,
+                               int32_t *best, int32_t *iters_run) {
   if (!ctx) return RVP_ERR_INVALID_ARG;
   return sguard(ctx, [&] {
     RVP_REQUIRE(x && y && z && frame_offsets_dev && cand && cand_offsets_dev && weights &&
@@ -777,7 +787,9 @@ rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y,
     RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     TmpBuf cdf;
     cdf.reserve((size_t)std::max<int64_t>(n_cand, 1) * 8);
-    rvp::k_cdf<<<n_frames, 256, 0, ctx->stream>>>(weights, cand_offsets_dev, cdf.as<double>());
+    RVP_REQUIRE(logit_power >= 0.0f, "logit_power must be >= 0");
+    rvp::k_cdf<<<n_frames, 256, 0, ctx->stream>>>(weights, logit_power, cand_offsets_dev,
+                                                  cdf.as<double>());
     RVP_LAUNCH_CHECK(ctx);
     rvp::RansacParams prm{dist_thresh, max_iters, collinear_thresh,
                           log(1.0 - clamp_prob(probability))};

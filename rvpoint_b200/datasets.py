@@ -276,3 +276,12 @@ def plane_scene(seed: int, n: int = 50_000, size: float = 10.0, sigma: float = 0
 
 def plane_scenes(n_scenes: int = 512, n: int = 50_000, seed: int = SEED_BASE + 4):
     return [plane_scene(seed * 100_003 + s, n=n) for s in range(n_scenes)]
+
+
+def plane_batch(n_scenes: int = 512, n: int = 50_000, seed: int = SEED_BASE + 4) -> Batch:
+    """plane_scenes concatenated into one Batch (scene s = frame s)."""
+    sc = plane_scenes(n_scenes=n_scenes, n=n, seed=seed)
+    offs = np.zeros(n_scenes + 1, np.int64)
+    offs[1:] = np.cumsum([c.n for c, _ in sc])
+    return Batch(np.concatenate([c.x for c, _ in sc]), np.concatenate([c.y for c, _ in sc]),
+                 np.concatenate([c.z for c, _ in sc]), offs)
