@@ -14,6 +14,11 @@ region.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--cell C [--rfac R]] [--no-tune] [--cpu-budget-s S]
 
+Rank 0 also runs the learned-vs-plain RANSAC leg (``learned_ransac`` in the
+line): 512 plane scenes of 50,000 points; plain GPU RANSAC (10,000
+hypotheses, the reference's stream and stopping rule) against the learned
+proposal (features + MLP + weighted RANSAC) to 99% of plain's best count.
+
 N > 1: launched by torch.distributed.run, one rank per GPU; every rank owns
 its own 256 frames (weak scaling, no data-path collective); time = max over
 ranks.
@@ -53,6 +58,8 @@ def parse():
     ap.add_argument("--rfac", type=float, default=1.0,
                     help="level-0 first-pass radius factor with --cell")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--learned-scenes", type=int, default=512,
+                    help="plane scenes of the learned-vs-plain RANSAC leg (0: skip)")
     return ap.parse_args()
 
 
@@ -226,6 +233,71 @@ def kernel_bytes(name: str, n_vox: int, n_sor: int, n_frames: int) -> float:
     if kind == "ransac":
         return 12.0 * n_sor + 4.0 * R_ITERS * n_frames
     raise ValueError(name)
+
+
+def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
+    """Learned-vs-plain RANSAC on n_scenes synthetic plane scenes of 50,000
+    points (1-6 planes, 30-70% outliers, 5 mm noise). The target of every
+    scene is 99% of plain RANSAC's best count after up to 10,000
+    hypotheses (the reference's rand() stream, adaptive stop p = 0.99).
+    Timed with CUDA events, inputs resident: plain RANSAC to its own stop,
+    plain RANSAC stopped at the target, and the learned proposal (features
+    + MLP + weighted RANSAC stopped at the target). The network is trained
+    first on n_train held-out scenes, on the GPU."""
+    import torch
+    from rvpoint_b200 import datasets as D
+    from rvpoint_b200 import learned as LR
+    T = 0.02
+    tr = D.plane_batch(n_train, seed=D.SEED_BASE + 4000)
+    ev = D.plane_batch(n_scenes, seed=D.SEED_BASE + 4)
+    bt, be = LR.DeviceBatch.from_host(tr), LR.DeviceBatch.from_host(ev)
+    del tr, ev
+    scorer = LR.PlaneScorer(max(bt.n, be.n), max(n_train, n_scenes), ctx=ctx)
+    info = LR.train(scorer, bt, LR.TrainConfig())
+
+    def timed(fn):
+        for _ in range(3):
+            out = fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, out
+
+    t_plain, (_, best, it_plain) = timed(lambda: LR.ransac_frames(be, 10_000, T, ctx=ctx))
+    tg = torch.ceil(best.double() * 0.99).to(torch.int32)
+    t_ptg, (_, _, it_ptg) = timed(lambda: LR.ransac_frames(be, 10_000, T, targets=tg, ctx=ctx))
+    lr = LR.LearnedRansac(scorer)
+    cand, coffs = lr.prepare(be)
+    t_l, (_, bl, it_l) = timed(lambda: lr.run(be, cand, coffs, 10_000, T, targets=tg))
+    t_f, feat = timed(lambda: LR.proposal_features(scorer, be, cand, lr._coffs_h, coffs,
+                                                   lr.cell, lr.scope))
+    t_m, logits = timed(lambda: scorer.forward(feat))
+    t_w, _ = timed(lambda: LR.ransac_weighted(be, cand, coffs, logits, 10_000, T, seed=lr.seed,
+                                              logit_power=lr.logit_power, targets=tg, ctx=ctx))
+    q = lambda t, p: float(t.double().quantile(p).item())  # noqa: E731
+    out = {"scenes": n_scenes, "points_per_scene": 50_000, "thresh": T,
+           "train_scenes": n_train, "train_seconds": info["seconds"],
+           "train_loss_first_last": [info["losses"][0][1], info["losses"][-1][1]],
+           "candidates_per_scene": lr.cand_per_frame, "feature_scope": lr.scope,
+           "plain_10k_ms": t_plain,
+           "plain_10k_hypotheses_mean": float(it_plain.double().mean().item()),
+           "plain_to_target_ms": t_ptg,
+           "plain_hypotheses_to_target": {"mean": float(it_ptg.double().mean().item()),
+                                          "median": q(it_ptg, 0.5), "p90": q(it_ptg, 0.9)},
+           "learned_to_target_ms": t_l, "learned_parts_ms": {"features": t_f, "mlp": t_m,
+                                                             "weighted_ransac": t_w},
+           "learned_hypotheses_to_target": {"mean": float(it_l.double().mean().item()),
+                                            "median": q(it_l, 0.5), "p90": q(it_l, 0.9)},
+           "learned_reached_fraction": float((bl >= tg).float().mean().item()),
+           "time_ratio_plain10k_over_learned": t_plain / t_l,
+           "time_ratio_plain_to_target_over_learned": t_ptg / t_l}
+    scorer.close()
+    return out
 
 
 def main():
@@ -411,6 +483,7 @@ def main():
             "algorithmic_bytes_per_launch": alg, "launch_ms": timed[dom]}
 
     cpu = cpu_baseline(batch, a.cpu_budget_s) if world == 1 else None
+    learned = learned_leg(ctx, a.learned_scenes, 64) if a.learned_scenes > 0 else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -423,7 +496,7 @@ def main():
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps, "clocks": clk,
             "stages_ms": {k: v for k, v in stages.items() if k != "runs"},
-            "graph": graph}
+            "graph": graph, "learned_ransac": learned}
     print(json.dumps(line), flush=True)
 
 
