@@ -211,10 +211,10 @@ class Clocks:
 # kernels timed live for the roofline: the stage or per-level kernel name,
 # the kernel that runs there, and the queries / points one launch processes
 KERNELS = {
-    "sor_knn_l0": ("k_knn_wt<17,SOR_MEAN> grid level 0", "vox"),
-    "sor_knn_l1": ("k_knn_wt<17,SOR_MEAN> grid level 1", None),
-    "sor_knn_l2": ("k_knn_wt<17,SOR_MEAN> grid level 2", None),
-    "normals_knn_l0": ("k_knn_wt<17,NORMALS> grid level 0", "sor"),
+    "sor_knn_l0": ("k_knn_wt<17,SOR_LIST> grid level 0", "vox"),
+    "sor_knn_l1": ("k_knn_wt<17,SOR_LIST> grid level 1", None),
+    "sor_knn_l2": ("k_knn_wt<17,SOR_LIST> grid level 2", None),
+    "normals_knn_l0": ("k_knn_wt<17,NORMALS> grid level 0", None),
     "normals_knn_l1": ("k_knn_wt<17,NORMALS> grid level 1", None),
     "normals_knn_l2": ("k_knn_wt<17,NORMALS> grid level 2", None),
     "ransac": ("k_ransac", "ransac"),
