@@ -302,8 +302,10 @@ RVP_API rvp_status rvp_pipeline_copy_outputs(rvp_pipeline *p, float *voxel_aos,
  * has a reference counterpart except rvp_ransac_frames, which is
  * ransac_plane_rvv (segmentation/ransac_plane.cpp:116-199, scalar branch
  * :55-111) applied to every frame of a batch. All pointers are device
- * pointers on the context's stream; the calls synchronize before returning,
- * except rvp_scorer_features and rvp_mlp_forward.
+ * pointers on the context's stream. rvp_ransac_frames (which restores
+ * libc's generator), rvp_mlp_gradients, the parameter calls and a
+ * rvp_mlp_train_step asked for its loss synchronize; the others only queue
+ * work. Scratch is kept in the context between calls.
  * ------------------------------------------------------------------------- */
 #define RVP_MLP_INPUTS 8
 #define RVP_MLP_HIDDEN 64
@@ -323,7 +325,7 @@ RVP_API rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const flo
                                      int32_t *iters_run);
 /* RANSAC whose three points are drawn from each frame's candidates
  * (cand[cand_offsets[f] .. cand_offsets[f+1]), global point indices inside
- * frame f) with probability proportional to their weight, from a
+ * frame f; n_cand = cand_offsets[n_frames]) with probability proportional to their weight, from a
  * counter-based generator keyed by seed. weights: one per candidate, used
  * as given (negatives as 0) when logit_power is 0, else taken as logits and
  * turned into sigmoid(w) ^ logit_power. Counting, model and the
@@ -331,8 +333,9 @@ RVP_API rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const flo
 RVP_API rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y,
                                        const float *z, const int64_t *frame_offsets_dev,
                                        int n_frames, const uint32_t *cand,
-                                       const int64_t *cand_offsets_dev, const float *weights,
-                                       float logit_power, uint64_t seed, int max_iters,
+                                       const int64_t *cand_offsets_dev, size_t n_cand,
+                                       const float *weights, float logit_power,
+                                       uint64_t seed, int max_iters,
                                        float dist_thresh,
                                        float collinear_thresh, float probability,
                                        const int32_t *targets, float *models, int32_t *best,

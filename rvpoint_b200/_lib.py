@@ -99,8 +99,8 @@ SIGNATURES = {
     "rvp_pipeline_stage_times": (I, [P, C.POINTER(F), I, C.POINTER(I)]),
     # batched RANSAC and the learned proposal
     "rvp_ransac_frames": (I, [P, P, P, P, P, I, I, F, F, F, P, P, P, P]),
-    "rvp_ransac_weighted": (I, [P, P, P, P, P, I, P, P, P, F, C.c_uint64, I, F, F, F, P, P, P,
-                                P]),
+    "rvp_ransac_weighted": (I, [P, P, P, P, P, I, P, P, SZ, P, F, C.c_uint64, I, F, F, F, P, P,
+                                P, P]),
     "rvp_plane_labels": (I, [P, P, P, P, P, I, SZ, P, F, P]),
     "rvp_scorer_create": (I, [P, SZ, I, C.POINTER(P)]),
     "rvp_scorer_destroy": (I, [P]),

@@ -870,7 +870,7 @@ rvp_status rvp_ransac_plane(rvp_context *ctx, const float *x, const float *y, co
     rvp::RansacParams prm{dist_thresh, max_iters, collinear_thresh, log(1.0 - pc)};
     if (max_iters > 0)
       rvp::ransac_frames(ctx, dx, dy, dz, offs, 1, drand, prm, dm, db, di, dcounts,
-                         counts != nullptr);
+                         counts != nullptr, rvp::RansacSampler{}, 8);
     float hm[4] = {0, 0, 0, 0};
     int32_t hb = 0, hi = 0;
     if (max_iters > 0) {

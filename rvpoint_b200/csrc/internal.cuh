@@ -78,7 +78,7 @@ struct rvp_context {
   std::string last_error;
   unsigned long long launches = 0;
   // scratch owned by one-shot entry points (grow-only, reused across calls)
-  rvp::DevBuf scratch[24];
+  rvp::DevBuf scratch[32];  // 0-23 one-shot entry points, 24-27 batched RANSAC
   rvp::HostBuf pinned[4];
   rvp::Grid *grid = nullptr;        // grid reused by one-shot kNN entry points
   rvp::VoxelWork *vwork = nullptr;  // voxel scratch of rvp_voxel_grid
@@ -382,13 +382,14 @@ struct RansacSampler {
   u64 seed = 0;
   const int32_t *targets = nullptr;
 };
-// One block per frame over SoA clouds; frame f = [off[f], off[f+1]).
+// One cluster of `cluster` blocks (1-8, fewer if the device cannot hold them)
+// per frame over SoA clouds; frame f = [off[f], off[f+1]).
 void ransac_frames(rvp_context *ctx, const float *x, const float *y,
                    const float *z, const int64_t *frame_offsets_dev,
                    int n_frames, const int *rand_dev, const RansacParams &p,
                    float *model, int32_t *best, int32_t *iters_run,
                    int32_t *counts_all, bool eval_all,
-                   const RansacSampler &smp = RansacSampler{});
+                   const RansacSampler &smp = RansacSampler{}, int cluster = 1);
 void extract_plane_run(rvp_context *ctx, const float *x, const float *y,
                        const float *z, size_t n, const float *model_dev,
                        float thresh, float *in_aos, float *out_aos,

@@ -435,14 +435,6 @@ struct rvp_scorer {
 };
 
 namespace {
-// a temporary device buffer released on every path out of its scope
-struct TmpBuf : rvp::DevBuf {
-  TmpBuf() = default;
-  TmpBuf(const TmpBuf &) = delete;
-  TmpBuf &operator=(const TmpBuf &) = delete;
-  ~TmpBuf() { release(); }
-};
-
 template <class F>
 rvp_status sguard(rvp_context *ctx, F &&f) {
   try {
@@ -743,7 +735,7 @@ rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const float *y, c
     std::vector<int32_t> rs(R);
     srand(0);
     for (size_t i = 0; i < R; ++i) rs[i] = rand();
-    TmpBuf drand;
+    rvp::DevBuf &drand = ctx->scratch[24];
     drand.reserve(R * 4);
     RVP_CUDA_TRY(cudaMemcpyAsync(drand.ptr, rs.data(), R * 4, cudaMemcpyHostToDevice, ctx->stream));
     rvp::RansacParams prm{dist_thresh, max_iters, collinear_thresh,
@@ -752,13 +744,12 @@ rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const float *y, c
     smp.targets = targets;
     std::vector<int32_t> it(n_frames, 0);
     int32_t *di = iters_run;
-    TmpBuf tmp;
     if (!di) {
-      tmp.reserve((size_t)n_frames * 4);
-      di = tmp.as<int32_t>();
+      ctx->scratch[25].reserve((size_t)n_frames * 4);
+      di = ctx->scratch[25].as<int32_t>();
     }
     rvp::ransac_frames(ctx, x, y, z, frame_offsets_dev, n_frames, drand.as<int>(), prm, models,
-                       best, di, nullptr, false, smp);
+                       best, di, nullptr, false, smp, 8);
     RVP_CUDA_TRY(cudaMemcpyAsync(it.data(), di, (size_t)n_frames * 4, cudaMemcpyDeviceToHost,
                                  ctx->stream));
     RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -770,7 +761,8 @@ rvp_status rvp_ransac_frames(rvp_context *ctx, const float *x, const float *y, c
 rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y, const float *z,
                                const int64_t *frame_offsets_dev, int n_frames,
                                const uint32_t *cand, const int64_t *cand_offsets_dev,
-                               const float *weights, float logit_power, uint64_t seed,
+                               size_t n_cand, const float *weights, float logit_power,
+                               uint64_t seed,
                                int max_iters, float dist_thresh, float collinear_thresh,
                                float probability, const int32_t *targets, float *models,
                                int32_t *best, int32_t *iters_run) {
@@ -781,12 +773,8 @@ rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y,
                 "null pointer");
     RVP_REQUIRE(n_frames >= 1 && max_iters >= 1, "n_frames / max_iters must be >= 1");
     RVP_CUDA_TRY(cudaSetDevice(ctx->device));
-    int64_t n_cand = 0;
-    RVP_CUDA_TRY(cudaMemcpyAsync(&n_cand, cand_offsets_dev + n_frames, 8, cudaMemcpyDeviceToHost,
-                                 ctx->stream));
-    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    TmpBuf cdf;
-    cdf.reserve((size_t)std::max<int64_t>(n_cand, 1) * 8);
+    rvp::DevBuf &cdf = ctx->scratch[26];
+    cdf.reserve(std::max<size_t>(n_cand, 1) * 8);
     RVP_REQUIRE(logit_power >= 0.0f, "logit_power must be >= 0");
     rvp::k_cdf<<<n_frames, 256, 0, ctx->stream>>>(weights, logit_power, cand_offsets_dev,
                                                   cdf.as<double>());
@@ -800,8 +788,7 @@ rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y,
     smp.seed = seed;
     smp.targets = targets;
     rvp::ransac_frames(ctx, x, y, z, frame_offsets_dev, n_frames, nullptr, prm, models, best,
-                       iters_run, nullptr, false, smp);
-    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+                       iters_run, nullptr, false, smp, 8);
   });
 }
 
@@ -814,7 +801,7 @@ rvp_status rvp_plane_labels(rvp_context *ctx, const float *x, const float *y, co
     RVP_REQUIRE(n_frames >= 1, "n_frames must be >= 1");
     if (n_points == 0) return;
     RVP_CUDA_TRY(cudaSetDevice(ctx->device));
-    TmpBuf fr;
+    rvp::DevBuf &fr = ctx->scratch[27];
     fr.reserve(n_points * 4);
     const unsigned gb = rvp::grid_for(n_points, 256, ctx->num_sms * 16);
     rvp::k_frame_of<<<gb, 256, 0, ctx->stream>>>(frame_offsets_dev, n_frames, n_points,
@@ -823,7 +810,6 @@ rvp_status rvp_plane_labels(rvp_context *ctx, const float *x, const float *y, co
     rvp::k_plane_labels<<<gb, 256, 0, ctx->stream>>>(x, y, z, fr.as<int32_t>(), n_points, models,
                                                      dist_thresh, labels);
     RVP_LAUNCH_CHECK(ctx);
-    RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   });
 }
 

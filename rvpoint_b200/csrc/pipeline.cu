@@ -374,7 +374,8 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     rvp::RansacParams prm{c.ransac_thresh, c.ransac_iters, c.ransac_collinear, log(1.0 - pc)};
     rvp::ransac_frames(ctx, p->sor_x.as<float>(), p->sor_y.as<float>(), p->sor_z.as<float>(),
                        sor_offs, n_frames, p->r_rand.as<int>(), prm, p->r_model.as<float>(),
-                       p->r_best.as<int32_t>(), p->r_iters.as<int32_t>(), nullptr, false);
+                       p->r_best.as<int32_t>(), p->r_iters.as<int32_t>(), nullptr, false,
+                       rvp::RansacSampler{}, 4);
     p->mark(7);
     if (!p->capturing && p->runs_cap > 0 && p->runs_recorded < p->runs_cap) p->runs_recorded++;
   });

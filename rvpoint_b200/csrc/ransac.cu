@@ -12,12 +12,16 @@
 // (strictly greater count wins, adaptive k_iters with p = 0.99 in double),
 // so best count, model and the number of executed iterations are the
 // reference's, and the loop stops as early as the reference's does.
+#include <cooperative_groups.h>
 #include <float.h>
+
+#include <atomic>
 #include <math.h>
 
 #include "internal.cuh"
 
 namespace rvp {
+namespace cg = cooperative_groups;
 
 namespace {
 constexpr int HB = 32;        // hypotheses per batch
@@ -70,7 +74,14 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
     const int64_t *offs, const int *__restrict__ rnd, RansacParams prm, float *model_out,
     int32_t *best_out, int32_t *iters_out, int32_t *counts_all, bool eval_all,
     RansacSampler smp) {
-  const int f = blockIdx.x;
+  // a frame is a cluster of G blocks (G = 1 without a cluster launch): every
+  // block builds the same hypotheses, counts its share of the points, and
+  // reads the others' counts through distributed shared memory; every block
+  // then replays the same decisions, so they stop together
+  cg::cluster_group cl = cg::this_cluster();
+  const u32 G = cl.num_blocks(), cr = cl.block_rank();
+  const int f = blockIdx.x / G;
+  const bool lead = cr == 0;  // writes the frame's outputs
   const int64_t a0 = offs[f];
   const u32 n = (u32)(offs[f + 1] - a0);
   const float *x = X + a0, *y = Y + a0, *z = Z + a0;
@@ -79,13 +90,15 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
 
   __shared__ float4 hyp[HB];
   __shared__ int hcode[HB];  // 0 valid, -1 repeated index, -2 collinear
-  __shared__ u32 hcnt[HB];
+  __shared__ u32 hcnt[HB];   // this block's partial counts
+  __shared__ u32 htot[HB];   // the frame's counts
   __shared__ int s_best, s_kiters, s_stop, s_iters;
   __shared__ float4 s_model;
 
   const bool no_cand = smp.cdf && (smp.cand_offs[f + 1] - smp.cand_offs[f] < 3 ||
                                    !(smp.cdf[smp.cand_offs[f + 1] - 1] > 0.0));
   if (n < 3 || no_cand) {  // ransac_plane.cpp:59
+    if (!lead) return;
     if (tid == 0) {
       model_out[4 * f + 0] = model_out[4 * f + 1] = model_out[4 * f + 2] = model_out[4 * f + 3] = 0;
       best_out[f] = 0;
@@ -139,7 +152,7 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
     __syncthreads();
 
     u32 acc = 0;  // lane h accumulates hypothesis h
-    for (u32 p0 = (u32)wid * 32 * R_PTS; p0 < n; p0 += NW * 32 * R_PTS) {
+    for (u32 p0 = (cr * NW + (u32)wid) * 32 * R_PTS; p0 < n; p0 += G * NW * 32 * R_PTS) {
       float px[R_PTS], py[R_PTS], pz[R_PTS];
       bool pv[R_PTS];
 #pragma unroll
@@ -161,7 +174,13 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
       }
     }
     atomicAdd(&hcnt[lane], acc);
-    __syncthreads();
+    cl.sync();  // every block's partial counts of this batch are complete
+    if (tid < HB) {
+      u32 t = 0;
+      for (u32 r = 0; r < G; ++r) t += cl.map_shared_rank(hcnt, r)[tid];
+      htot[tid] = t;
+    }
+    cl.sync();  // no block resets its counts while another still reads them
 
     if (tid == 0) {
       // replay ransac_plane.cpp:67-107 for this batch, in order
@@ -173,7 +192,7 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
           break;
         }
         if (hcode[h] != 0) continue;
-        const int cur = (int)hcnt[h];
+        const int cur = (int)htot[h];
         if (cur > s_best && smp.targets) {
           s_best = cur;
           s_model = hyp[h];
@@ -200,11 +219,12 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
         s_iters = prm.max_iters;
       }
     }
-    if (counts_all && tid < HB && base + tid < prm.max_iters)
+    if (lead && counts_all && tid < HB && base + tid < prm.max_iters)
       counts_all[(size_t)f * prm.max_iters + base + tid] =
-          hcode[tid] == 0 ? (int32_t)hcnt[tid] : hcode[tid];
+          hcode[tid] == 0 ? (int32_t)htot[tid] : hcode[tid];
     __syncthreads();
   }
+  if (!lead) return;
   if (counts_all && !eval_all) {
     // hypotheses past the early stop were not evaluated
     const int done = ((s_iters + HB - 1) / HB) * HB;
@@ -263,11 +283,42 @@ inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 void ransac_frames(rvp_context *ctx, const float *x, const float *y, const float *z,
                    const int64_t *offs, int n_frames, const int *rand_dev, const RansacParams &p,
                    float *model, int32_t *best, int32_t *iters_run, int32_t *counts_all,
-                   bool eval_all, const RansacSampler &smp) {
+                   bool eval_all, const RansacSampler &smp, int cluster) {
   if (n_frames <= 0) return;
-  k_ransac<<<n_frames, R_THREADS, 0, ctx->stream>>>(x, y, z, offs, rand_dev, p, model, best,
-                                                    iters_run, counts_all, eval_all, smp);
-  RVP_LAUNCH_CHECK(ctx);
+  const int want = cluster < 1 ? 1 : (cluster > 8 ? 8 : cluster);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  cfg.blockDim = dim3(R_THREADS);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = ctx->stream;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  // the largest cluster (<= want) the device holds, found once per device
+  // and request, before any stream capture that launches this kernel
+  static std::atomic<int> fitted[64][9];
+  const int dev = ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0;
+  int G = fitted[dev][want].load(std::memory_order_relaxed);
+  for (G = G ? G : want; G > 1 && !fitted[dev][want].load(std::memory_order_relaxed); G >>= 1) {
+    cfg.gridDim = dim3((unsigned)n_frames * G);
+    attr[0].val.clusterDim.x = G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int active = 0;
+    if (cudaOccupancyMaxActiveClusters(&active, k_ransac, &cfg) == cudaSuccess && active > 0) break;
+    cudaGetLastError();
+  }
+  if (G < 1) G = 1;
+  fitted[dev][want].store(G, std::memory_order_relaxed);
+  cfg.gridDim = dim3((unsigned)n_frames * G);
+  attr[0].val.clusterDim.x = G;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = G > 1 ? 1 : 0;
+  RVP_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_ransac, x, y, z, offs, rand_dev, p, model, best,
+                                  iters_run, counts_all, eval_all, smp));
+  ::rvp::count_launch(ctx);
 }
 
 size_t extract_temp_bytes(size_t n) {

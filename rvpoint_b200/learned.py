@@ -206,7 +206,8 @@ def ransac_weighted(b: DeviceBatch, cand: torch.Tensor, cand_offsets: torch.Tens
     best = torch.empty(nf, dtype=torch.int32, device=dev)
     iters = torch.empty(nf, dtype=torch.int32, device=dev)
     check(_lib.load().rvp_ransac_weighted(ctx.h, _p(b.x), _p(b.y), _p(b.z), _p(b.offsets), nf,
-                                          _p(cand), _p(cand_offsets), _p(weights),
+                                          _p(cand), _p(cand_offsets), int(cand.numel()),
+                                          _p(weights),
                                           float(logit_power), int(seed), int(max_iters),
                                           float(thresh), float(collinear), float(probability),
                                           _p(targets), _p(models), _p(best), _p(iters)), ctx.h)
