@@ -25,7 +25,8 @@ STAMP = os.path.join(LIBDIR, ".sources.sha256")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
               "-fvisibility=hidden", "--expt-relaxed-constexpr", "-I" + INCLUDE]
-CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I" + INCLUDE]
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I" + INCLUDE,
+             "-I" + os.path.join(INCLUDE, "rvpoint")]
 
 
 def nvcc() -> str:
@@ -54,7 +55,8 @@ def _digest(files) -> str:
 def build(force: bool = False, verbose: bool = False) -> str:
     cu, cpp = sources()
     headers = [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cuh", ".h"))]
-    headers += [os.path.join(INCLUDE, f) for f in sorted(os.listdir(INCLUDE)) if f.endswith(".h")]
+    for d, _, fs in sorted(os.walk(INCLUDE)):
+        headers += [os.path.join(d, f) for f in sorted(fs) if f.endswith(".h")]
     dig = _digest(cu + cpp + headers)
     if not force and os.path.exists(LIB) and os.path.exists(STAMP):
         with open(STAMP) as fh:

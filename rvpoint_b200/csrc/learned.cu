@@ -432,6 +432,8 @@ struct rvp_scorer {
   rvp::DevBuf frame_of, is_cand, pairs, counts, hard, qlevel, qtau, open;
   rvp::DevBuf w, wq, m, v, grad, norm, loss;
   int adam_step = 0;
+  size_t fitted_points = 0;  // batch size and cell the bucket table was fitted to
+  float fitted_cell = 0.0f;
 };
 
 namespace {
@@ -554,6 +556,18 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
     const unsigned gb = rvp::grid_for(N, 256, sms * 16);
     rvp::grid_build(ctx, s->grid, x, y, z, frame_offsets_dev, n_frames, N, cell_size,
                     rvp::KEY_DENSE, 0, 0, nullptr);
+    if (s->fitted_points != N || s->fitted_cell != cell_size) {
+      // size the bucket table to the cells this batch occupies (it stays in
+      // L2 instead of spanning 2.5 slots per point), then build again
+      u64 nb[4] = {0, 0, 0, 0};
+      RVP_CUDA_TRY(cudaMemcpyAsync(nb, s->grid.d_nbuckets, 32, cudaMemcpyDeviceToHost, st));
+      RVP_CUDA_TRY(cudaStreamSynchronize(st));
+      s->grid.fit_table((size_t)((nb[0] + nb[1] + nb[2]) * 2));
+      s->fitted_points = N;
+      s->fitted_cell = cell_size;
+      rvp::grid_build(ctx, s->grid, x, y, z, frame_offsets_dev, n_frames, N, cell_size,
+                      rvp::KEY_DENSE, 0, 0, nullptr);
+    }
     rvp::k_frame_of<<<gb, 256, 0, st>>>(frame_offsets_dev, n_frames, N, s->frame_of.as<int32_t>());
     RVP_LAUNCH_CHECK(ctx);
     const rvp::GridView gv = s->grid.view(rvp::KEY_DENSE, 0, 0);
