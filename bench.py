@@ -318,6 +318,7 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     from rvpoint_b200 import api, autotune
+    from rvpoint_b200.sharding import max_over_ranks
     from rvpoint_b200 import datasets as D
 
     batch = D.lidar_batch(n_frames=a.frames, seed=D.SEED_BASE + 2 + 7919 * rank)
@@ -386,15 +387,10 @@ def main():
     g1.record()
     torch.cuda.synchronize()
     pipe.check()
-    g_t = torch.tensor([g0.elapsed_time(g1)], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(g_t, op=dist.ReduceOp.MAX)
-    graph = {"ms_per_step": float(g_t.item()) / a.steps, "kernels_per_step": graph_kernels,
-             "value": (n * world) / (float(g_t.item()) / a.steps / 1e3) / 1e6}
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    g_ms = max_over_ranks(g0.elapsed_time(g1), dev)
+    graph = {"ms_per_step": g_ms / a.steps, "kernels_per_step": graph_kernels,
+             "value": (n * world) / (g_ms / a.steps / 1e3) / 1e6}
+    ms_max = max_over_ranks(ms, dev)
     ms_step = ms_max / a.steps
     value = (n * world) / (ms_step / 1e3) / 1e6
 
@@ -440,12 +436,10 @@ def main():
         e_ms = e0.elapsed_time(e1) / e_steps
         h2d = 12 * n + 8 * (nf + 1)
         d2h = 8 * (nf + 1) * 2 + 12 * n_vox + 12 * n_sor + 12 * n_sor + 16 * nf + 4 * nf
-        e_t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
-        e2e = {"value": (n * world) / (float(e_t.item()) / 1e3) / 1e6, "unit": UNIT,
+        e_max = max_over_ranks(e_ms, dev)
+        e2e = {"value": (n * world) / (e_max / 1e3) / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": float(e_t.item()), "steps": e_steps}
+               "ms_per_step": e_max, "steps": e_steps}
 
     if world > 1:
         dist.barrier()
