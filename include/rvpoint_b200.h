@@ -280,7 +280,9 @@ RVP_API rvp_status rvp_pipeline_stage_times(rvp_pipeline *p, float *ms, int n_st
                                             int *runs);
 /* Host entry: copies host frames in, runs, copies the per-frame results out
  * (any output pointer may be NULL). Output arrays are sized by max_points /
- * n_frames; *_offsets are n_frames+1 entries. */
+ * n_frames; *_offsets are n_frames+1 entries. The voxel results are copied
+ * out while SOR and the normals run, the SOR results while the normals and
+ * RANSAC run (asynchronous when the host buffers are pinned). */
 RVP_API rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const float *y,
                                  const float *z, const int64_t *frame_offsets,
                                  int n_frames, float *voxel_aos,

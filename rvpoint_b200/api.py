@@ -569,10 +569,23 @@ class Pipeline:
         nf = int(offs.shape[0] - 1)
         self.last_frames = nf
         n = int(offs[-1])
+        vox = np.empty((max(n, 1), 3), np.float32)
+        vo = np.empty(nf + 1, np.int64)
+        sor = np.empty((max(n, 1), 3), np.float32)
+        so = np.empty(nf + 1, np.int64)
+        nx = np.empty(max(n, 1), np.float32)
+        ny = np.empty(max(n, 1), np.float32)
+        nz = np.empty(max(n, 1), np.float32)
+        model = np.empty((nf, 4), np.float32)
+        cnt = np.empty(nf, np.int32)
         check(self.L.rvp_pipeline_run_host(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(offs), nf,
-                                           None, None, None, None, None, None, None, None, None),
+                                           _ptr(vox), _ptr(vo), _ptr(sor), _ptr(so), _ptr(nx),
+                                           _ptr(ny), _ptr(nz), _ptr(model), _ptr(cnt)),
               self.ctx.h)
-        return self.results(n)
+        nv, ns = int(vo[-1]), int(so[-1])
+        return dict(voxel=vox[:nv], voxel_offsets=vo, sor=sor[:ns], sor_offsets=so,
+                    normals=np.stack([nx[:ns], ny[:ns], nz[:ns]], 1), ransac_model=model,
+                    ransac_count=cnt)
 
     def results(self, max_points: int | None = None) -> dict:
         """Per-frame results of the last run, copied to numpy."""

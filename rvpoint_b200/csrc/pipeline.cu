@@ -46,6 +46,11 @@ struct rvp_pipeline {
   rvp::DevBuf open;   // open-query compaction between levels (flags, scan, list)
   bool stats_on = false;
   int n_frames_last = 0;
+  // run_host: events after the voxel and SOR stages, so that their results
+  // go down (s_out) while the later stages run; sizes read on s_meta
+  bool record_stages = false;
+  cudaEvent_t ev_stage[2] = {nullptr, nullptr};
+  cudaStream_t s_out = nullptr, s_meta = nullptr;
   // stage timing: a ring of event sets, one set per run
   // (stage boundaries, then a pair around each grid level's kNN kernel: SOR
   // levels 0-2, normals levels 0-2)
@@ -214,6 +219,10 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
   p->grid.release();
   for (auto e : p->events) cudaEventDestroy(e);
   if (p->graph) cudaGraphExecDestroy(p->graph);
+  for (auto e : p->ev_stage)
+    if (e) cudaEventDestroy(e);
+  if (p->s_out) cudaStreamDestroy(p->s_out);
+  if (p->s_meta) cudaStreamDestroy(p->s_meta);
   delete p;
   return RVP_OK;
 }
@@ -245,6 +254,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                         p->vox_aos.as<float>(), vox_offs, nullptr, nullptr, p->vox_x.as<float>(),
                         p->vox_y.as<float>(), p->vox_z.as<float>());
     p->mark(1);
+    if (p->record_stages) RVP_CUDA_TRY(cudaEventRecord(p->ev_stage[0], st));
     // 2) grid over the voxel points of every frame
     rvp::grid_build(ctx, p->grid, p->vox_x.as<float>(), p->vox_y.as<float>(),
                     p->vox_z.as<float>(), vox_offs, n_frames, N, p->cell, rvp::KEY_DENSE, 0, 0,
@@ -321,6 +331,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                            p->sor_z.as<float>(), p->sor_src.as<u32>());
     const u64 *sor_pos = rvp::sor_positions(p->sor_tmp.ptr, N);
     p->mark(4);
+    if (p->record_stages) RVP_CUDA_TRY(cudaEventRecord(p->ev_stage[1], st));
     // 4) normals: the k+1 nearest kept points of every kept point, with the
     //    reference normal computed in the same tile kernel
     k_mark_removed<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(
@@ -610,11 +621,57 @@ rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const float *y
   });
   if (s != RVP_OK) return s;
   const size_t n = (size_t)frame_offsets[n_frames];
+  s = guard(ctx, [&] {
+    if (!p->s_out) {
+      RVP_CUDA_TRY(cudaStreamCreateWithFlags(&p->s_out, cudaStreamNonBlocking));
+      RVP_CUDA_TRY(cudaStreamCreateWithFlags(&p->s_meta, cudaStreamNonBlocking));
+      for (auto &e : p->ev_stage) RVP_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+  });
+  if (s != RVP_OK) return s;
+  // queue the whole run, then bring each stage's results down as soon as
+  // that stage is done: the voxel output under SOR and normals, the SOR
+  // output under normals and RANSAC
+  p->record_stages = true;
   s = rvp_pipeline_run_device(p, p->in_x.as<float>(), p->in_y.as<float>(), p->in_z.as<float>(),
                               p->in_offs.as<int64_t>(), n_frames, n);
+  p->record_stages = false;
   if (s != RVP_OK) return s;
-  return rvp_pipeline_copy_outputs(p, voxel_aos, voxel_offsets, sor_aos, sor_offsets, nx, ny, nz,
-                                   ransac_model, ransac_count);
+  s = guard(ctx, [&] {
+    cudaStream_t st = ctx->stream;
+    std::vector<int64_t> vo(n_frames + 1), so(n_frames + 1);
+    auto d2h = [&](void *dst, const void *src, size_t b, cudaStream_t on) {
+      if (dst && b) RVP_CUDA_TRY(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, on));
+    };
+    RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_meta, p->ev_stage[0], 0));
+    RVP_CUDA_TRY(cudaMemcpyAsync(vo.data(), p->vox_offs.ptr, (n_frames + 1) * 8,
+                                 cudaMemcpyDeviceToHost, p->s_meta));
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->s_meta));
+    const size_t nv = (size_t)vo[n_frames];
+    if (voxel_offsets) memcpy(voxel_offsets, vo.data(), (n_frames + 1) * 8);
+    RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_out, p->ev_stage[0], 0));
+    d2h(voxel_aos, p->vox_aos.ptr, nv * 12, p->s_out);
+    RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_meta, p->ev_stage[1], 0));
+    RVP_CUDA_TRY(cudaMemcpyAsync(so.data(), p->sor_offs.ptr, (n_frames + 1) * 8,
+                                 cudaMemcpyDeviceToHost, p->s_meta));
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->s_meta));
+    const size_t ns = (size_t)so[n_frames];
+    if (sor_offsets) memcpy(sor_offsets, so.data(), (n_frames + 1) * 8);
+    RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_out, p->ev_stage[1], 0));
+    d2h(sor_aos, p->sor_aos.ptr, ns * 12, p->s_out);
+    d2h(nx, p->nx.ptr, ns * 4, st);
+    d2h(ny, p->ny.ptr, ns * 4, st);
+    d2h(nz, p->nz.ptr, ns * 4, st);
+    d2h(ransac_model, p->r_model.ptr, (size_t)n_frames * 16, st);
+    d2h(ransac_count, p->r_best.ptr, (size_t)n_frames * 4, st);
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->s_out));
+    RVP_CUDA_TRY(cudaStreamSynchronize(st));
+  });
+  if (s != RVP_OK) {
+    cudaStreamSynchronize(p->s_out);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  return s;
 }
 
 rvp_status rvp_pipeline_copy_outputs(rvp_pipeline *p, float *voxel_aos, int64_t *voxel_offsets,
