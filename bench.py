@@ -274,8 +274,7 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
     lr = LR.LearnedRansac(scorer)
     cand, coffs = lr.prepare(be)
     t_l, (_, bl, it_l) = timed(lambda: lr.run(be, cand, coffs, 10_000, T, targets=tg))
-    t_f, feat = timed(lambda: LR.proposal_features(scorer, be, cand, lr._coffs_h, coffs,
-                                                   lr.cell, lr.scope))
+    t_f, feat = timed(lambda: LR.proposal_features(scorer, be, cand, coffs, lr.cell, lr.scope))
     t_m, logits = timed(lambda: scorer.forward(feat))
     t_w, _ = timed(lambda: LR.ransac_weighted(be, cand, coffs, logits, 10_000, T, seed=lr.seed,
                                               logit_power=lr.logit_power, targets=tg, ctx=ctx))

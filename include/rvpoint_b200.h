@@ -356,11 +356,15 @@ RVP_API rvp_status rvp_scorer_destroy(rvp_scorer *s);
 /* Eight features per candidate (all points if cand is NULL) from its k = 16
  * nearest neighbours within its frame: |normal| (3), curvature, planarity,
  * log of the 16th-neighbour distance r, distance to the local plane / r,
- * distance to the neighbourhood centroid / r. features: n_cand x 8. */
+ * distance to the neighbourhood centroid / r. features: n_cand x 8.
+ * neighbours = 0: among all of the frame's points; 1: among the frame's
+ * candidates only (cand_offsets_dev: n_frames + 1 offsets into cand; a
+ * coarser neighbourhood for far less kNN work). */
 RVP_API rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y,
                                        const float *z, const int64_t *frame_offsets_dev,
                                        int n_frames, size_t n_points, float cell_size,
-                                       const uint32_t *cand, size_t n_cand, float *features);
+                                       const uint32_t *cand, const int64_t *cand_offsets_dev,
+                                       size_t n_cand, int neighbours, float *features);
 /* Parameters (host arrays): FP32 master weights, RVP_MLP_PARAMS floats;
  * the network computes with their BF16 rounding. set_params resets the
  * optimiser. set_norm: per-feature mean and standard deviation applied

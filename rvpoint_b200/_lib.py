@@ -104,7 +104,7 @@ SIGNATURES = {
     "rvp_plane_labels": (I, [P, P, P, P, P, I, SZ, P, F, P]),
     "rvp_scorer_create": (I, [P, SZ, I, C.POINTER(P)]),
     "rvp_scorer_destroy": (I, [P]),
-    "rvp_scorer_features": (I, [P, P, P, P, P, I, SZ, F, P, SZ, P]),
+    "rvp_scorer_features": (I, [P, P, P, P, P, I, SZ, F, P, P, SZ, I, P]),
     "rvp_mlp_set_params": (I, [P, P]),
     "rvp_mlp_get_params": (I, [P, P]),
     "rvp_mlp_set_norm": (I, [P, P, P]),

@@ -171,6 +171,17 @@ __global__ void k_open_cand(const float4 *pts, const u64 *n_dev, const uint8_t *
   }
 }
 
+__global__ void k_gather_xyz(const float *x, const float *y, const float *z, const u32 *idx,
+                             size_t n, size_t n_src, float *ox, float *oy, float *oz) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const u32 i = idx[t] < n_src ? idx[t] : 0;
+    ox[t] = x[i];
+    oy[t] = y[i];
+    oz[t] = z[i];
+  }
+}
+
 __global__ void k_widen32(const u32 *a, u64 *b) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *b = *a;
 }
@@ -431,6 +442,7 @@ struct rvp_scorer {
   rvp::Grid grid;
   rvp::DevBuf frame_of, is_cand, pairs, counts, hard, qlevel, qtau, open;
   rvp::DevBuf w, wq, m, v, grad, norm, loss;
+  rvp::DevBuf cand_xyz;  // candidates' own coordinates (neighbours among candidates)
   int adam_step = 0;
   size_t fitted_points = 0;  // batch size and cell the bucket table was fitted to
   float fitted_cell = 0.0f;
@@ -528,18 +540,17 @@ rvp_status rvp_scorer_destroy(rvp_scorer *s) {
   cudaStreamSynchronize(s->ctx->stream);
   rvp::DevBuf *bufs[] = {&s->frame_of, &s->is_cand, &s->pairs, &s->counts, &s->hard, &s->qlevel,
                          &s->qtau, &s->open, &s->w, &s->wq, &s->m, &s->v, &s->grad, &s->norm,
-                         &s->loss};
+                         &s->loss, &s->cand_xyz};
   for (auto *b : bufs) b->release();
   s->grid.release();
   delete s;
   return RVP_OK;
 }
 
-rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, const float *z,
-                               const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
-                               float cell_size, const uint32_t *cand, size_t n_cand,
-                               float *features) {
-  if (!s) return RVP_ERR_INVALID_ARG;
+namespace {
+rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const float *z,
+                         const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
+                         float cell_size, const uint32_t *cand, size_t n_cand, float *features) {
   rvp_context *ctx = s->ctx;
   return sguard(ctx, [&] {
     RVP_REQUIRE(x && y && z && frame_offsets_dev && features, "null pointer");
@@ -620,6 +631,36 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
     RVP_LAUNCH_CHECK(ctx);
   });
 }
+}  // namespace
+
+rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, const float *z,
+                               const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
+                               float cell_size, const uint32_t *cand,
+                               const int64_t *cand_offsets_dev, size_t n_cand, int neighbours,
+                               float *features) {
+  if (!s) return RVP_ERR_INVALID_ARG;
+  if (neighbours == 0) return features_impl(s, x, y, z, frame_offsets_dev, n_frames, n_points,
+                                            cell_size, cand, n_cand, features);
+  if (neighbours != 1 || !cand || !cand_offsets_dev) return RVP_ERR_INVALID_ARG;
+  // neighbourhoods among the candidates only: their coordinates, frame by
+  // frame, become the cloud
+  rvp_context *ctx = s->ctx;
+  const rvp_status st = sguard(ctx, [&] {
+    RVP_REQUIRE(x && y && z, "null pointer");
+    RVP_REQUIRE(n_cand >= 1 && n_cand <= s->max_points, "n_cand out of range");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    s->cand_xyz.reserve(n_cand * 12);
+    float *gx = s->cand_xyz.as<float>();
+    rvp::k_gather_xyz<<<rvp::grid_for(n_cand, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
+        x, y, z, cand, n_cand, n_points, gx, gx + n_cand, gx + 2 * n_cand);
+    RVP_LAUNCH_CHECK(ctx);
+  });
+  if (st != RVP_OK) return st;
+  const float *gx = s->cand_xyz.as<float>();
+  return features_impl(s, gx, gx + n_cand, gx + 2 * n_cand, cand_offsets_dev, n_frames, n_cand,
+                       cell_size, nullptr, n_cand, features);
+}
+
 
 rvp_status rvp_mlp_set_params(rvp_scorer *s, const float *params) {
   if (!s || !params) return RVP_ERR_INVALID_ARG;

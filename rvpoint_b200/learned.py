@@ -80,26 +80,14 @@ def candidates(offsets_host: np.ndarray, per_frame: int, seed: int):
     return np.concatenate(out), np.asarray(offs, np.int64)
 
 
-def candidate_batch(b: DeviceBatch, cand: torch.Tensor, cand_offsets_host: np.ndarray,
-                    cand_offsets: torch.Tensor) -> DeviceBatch:
-    """The candidates' own points as a batch (frame f = its candidates)."""
-    idx = cand.long()
-    return DeviceBatch(b.x.index_select(0, idx), b.y.index_select(0, idx),
-                       b.z.index_select(0, idx), cand_offsets, cand_offsets_host)
-
-
 def proposal_features(scorer: "PlaneScorer", b: DeviceBatch, cand: torch.Tensor,
-                      cand_offsets_host: np.ndarray, cand_offsets: torch.Tensor, cell: float,
-                      scope: str) -> torch.Tensor:
+                      cand_offsets: torch.Tensor, cell: float, scope: str) -> torch.Tensor:
     """Features of the candidates. scope "points": neighbours among all of
     the frame's points; "candidates": among the frame's candidates only (a
     coarser neighbourhood, far less kNN work)."""
-    if scope == "points":
-        return scorer.features(b, cell, cand)
-    if scope == "candidates":
-        cb = candidate_batch(b, cand, cand_offsets_host, cand_offsets)
-        return scorer.features(cb, cell)
-    raise ValueError(scope)
+    if scope not in ("points", "candidates"):
+        raise ValueError(scope)
+    return scorer.features(b, cell, cand, cand_offsets, scope == "candidates")
 
 
 class PlaneScorer:
@@ -115,12 +103,14 @@ class PlaneScorer:
         self.mean = np.zeros(8, np.float32)
         self.std = np.ones(8, np.float32)
 
-    def features(self, b: DeviceBatch, cell: float, cand: Optional[torch.Tensor] = None):
+    def features(self, b: DeviceBatch, cell: float, cand: Optional[torch.Tensor] = None,
+                 cand_offsets: Optional[torch.Tensor] = None, among_candidates: bool = False):
         self.ctx.use_torch_stream()
         n_cand = b.n if cand is None else int(cand.numel())
         feat = torch.empty((n_cand, 8), dtype=torch.float32, device=b.x.device)
         check(self.L.rvp_scorer_features(self.h, _p(b.x), _p(b.y), _p(b.z), _p(b.offsets),
-                                         b.n_frames, b.n, float(cell), _p(cand), n_cand,
+                                         b.n_frames, b.n, float(cell), _p(cand),
+                                         _p(cand_offsets), n_cand, int(among_candidates),
                                          _p(feat)), self.ctx.h)
         return feat
 
@@ -229,9 +219,9 @@ def plane_labels(b: DeviceBatch, models: torch.Tensor, thresh: float,
 class TrainConfig:
     thresh: float = 0.02          # RANSAC inlier distance (m)
     label_iters: int = 10_000     # plain RANSAC hypotheses behind the labels
-    cell: float = 0.3             # grid cell of the feature kNN (m)
+    cell: float = 1.5             # grid cell of the feature kNN (m)
     cand_per_frame: int = 1024    # feature points per frame
-    scope: str = "points"         # feature neighbourhoods: "points" or "candidates"
+    scope: str = "candidates"     # feature neighbourhoods: "candidates" or "points"
     steps: int = 400
     batch: int = 32_768
     lr: float = 3e-3
@@ -247,7 +237,7 @@ def train(scorer: PlaneScorer, b: DeviceBatch, cfg: TrainConfig = TrainConfig())
     cand_h, coffs_h = candidates(b.offsets_host, cfg.cand_per_frame, cfg.seed)
     cand = torch.from_numpy(cand_h.view(np.int32)).to(b.x.device)
     coffs = torch.from_numpy(coffs_h).to(b.x.device)
-    feat = proposal_features(scorer, b, cand, coffs_h, coffs, cfg.cell, cfg.scope)
+    feat = proposal_features(scorer, b, cand, coffs, cfg.cell, cfg.scope)
     labels = labels_all[cand.long()].contiguous()
     mean = feat.mean(0).cpu().numpy()
     std = feat.std(0).clamp_min(1e-6).cpu().numpy()
@@ -271,8 +261,8 @@ def train(scorer: PlaneScorer, b: DeviceBatch, cfg: TrainConfig = TrainConfig())
 class LearnedRansac:
     """features -> MLP -> weighted RANSAC over every frame of a batch."""
 
-    def __init__(self, scorer: PlaneScorer, cell: float = 0.3, cand_per_frame: int = 1024,
-                 logit_power: float = 1.0, seed: int = 11, scope: str = "points"):
+    def __init__(self, scorer: PlaneScorer, cell: float = 1.5, cand_per_frame: int = 1024,
+                 logit_power: float = 1.0, seed: int = 11, scope: str = "candidates"):
         self.scorer = scorer
         self.cell = cell
         self.cand_per_frame = cand_per_frame
@@ -290,8 +280,7 @@ class LearnedRansac:
 
     def run(self, b: DeviceBatch, cand, cand_offsets, max_iters: int, thresh: float,
             targets: Optional[torch.Tensor] = None):
-        feat = proposal_features(self.scorer, b, cand, self._coffs_h, cand_offsets, self.cell,
-                                 self.scope)
+        feat = proposal_features(self.scorer, b, cand, cand_offsets, self.cell, self.scope)
         logits = self.scorer.forward(feat)
         return ransac_weighted(b, cand, cand_offsets, logits, max_iters, thresh,
                                seed=self.seed, logit_power=self.logit_power, targets=targets,

@@ -143,6 +143,23 @@ def test_features_match_cpu_oracle(gpu_ctx):
 
 
 @pytest.mark.gpu
+def test_features_among_candidates_equal_features_of_their_subcloud(gpu_ctx):
+    import torch
+    from rvpoint_b200.learned import DeviceBatch, PlaneScorer, candidates
+    tr = D.plane_batch(n_scenes=3, n=20_000, seed=D.SEED_BASE + 77)
+    b = DeviceBatch.from_host(tr)
+    cand_h, coffs_h = candidates(b.offsets_host, 1500, 3)
+    sub = D.Batch(tr.x[cand_h], tr.y[cand_h], tr.z[cand_h], coffs_h)
+    s = PlaneScorer(b.n, 3, ctx=gpu_ctx)
+    cand = torch.from_numpy(cand_h.view(np.int32)).cuda()
+    coffs = torch.from_numpy(coffs_h).cuda()
+    f1 = s.features(b, 1.0, cand, coffs, among_candidates=True).cpu().numpy()
+    f2 = s.features(DeviceBatch.from_host(sub), 1.0).cpu().numpy()
+    assert np.array_equal(f1.view(np.int32), f2.view(np.int32))
+    s.close()
+
+
+@pytest.mark.gpu
 def test_batched_ransac_matches_reference_per_frame(gpu_ctx, restatement):
     import torch
     from oracle.oracle import libc_rand_stream
