@@ -57,6 +57,8 @@ def parse():
                     help="fixed grid cell (m) instead of the autotuner's choice")
     ap.add_argument("--rfac", type=float, default=1.0,
                     help="level-0 first-pass radius factor with --cell")
+    ap.add_argument("--lane-levels", type=int, default=2,
+                    help="grid levels of the one-query-per-lane kNN with --cell")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--learned-scenes", type=int, default=512,
                     help="plane scenes of the learned-vs-plain RANSAC leg (0: skip)")
@@ -343,7 +345,9 @@ def main():
     if a.cell > 0:
         pipe.set_tuning(a.cell, 256, 0)
         pipe.set_search_radius_factor(a.rfac)
-        best = {"cell": a.cell, "block": 256, "qpw": 0, "rfac": a.rfac, "fixed": True}
+        pipe.set_lane_levels(a.lane_levels)
+        best = {"cell": a.cell, "block": 256, "qpw": 0, "rfac": a.rfac,
+                "lane_levels": a.lane_levels, "fixed": True}
     elif not a.no_tune:
         best, _ = autotune.tune(pipe, *args)
     for _ in range(max(a.warmup, 1)):

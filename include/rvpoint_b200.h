@@ -267,6 +267,10 @@ RVP_API rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size,
  * cell * sqrt(k / points in the query's cell) (0 disables the first pass;
  * results never depend on it, only the work does). */
 RVP_API rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac);
+/* Grid levels (1-3; 0 = all 3) whose kNN runs one query per lane; the
+ * queries still open after them go to the warp-per-query kernel, which
+ * spreads a query's candidates over the lanes. Results never depend on it. */
+RVP_API rvp_status rvp_pipeline_set_lane_levels(rvp_pipeline *p, int levels);
 /* Stage timing with CUDA events on the context's stream: the next max_runs
  * runs record 8 events each (stage boundaries: voxel, grid build, SOR kNN,
  * SOR statistics, normals kNN, normals, RANSAC), plus a pair around each

@@ -92,6 +92,7 @@ SIGNATURES = {
     "rvp_pipeline_set_timing": (I, [P, I]),
     "rvp_pipeline_set_tuning": (I, [P, F, I, I]),
     "rvp_pipeline_set_search_radius_factor": (I, [P, F]),
+    "rvp_pipeline_set_lane_levels": (I, [P, I]),
     "rvp_pipeline_frame_offsets": (I, [P, P, P]),
     "rvp_pipeline_fit_tables": (I, [P]),
     "rvp_pipeline_check": (I, [P]),

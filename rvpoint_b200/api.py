@@ -512,6 +512,11 @@ class Pipeline:
         self.cfg.block_threads = block_threads
         self.cfg.queries_per_warp = queries_per_warp
 
+    def set_lane_levels(self, levels: int) -> None:
+        """Grid levels of the one-query-per-lane kNN kernels (0: all)."""
+        check(self.L.rvp_pipeline_set_lane_levels(self.h, int(levels)), self.ctx.h)
+        self.lane_levels = int(levels)
+
     def set_search_radius_factor(self, rfac: float) -> None:
         check(self.L.rvp_pipeline_set_search_radius_factor(self.h, float(rfac)), self.ctx.h)
 

@@ -1,8 +1,9 @@
 """Autotuner for the batched pipeline.
 
-Chooses the neighbour-grid cell size, the kNN block shape and the queries
-per warp by timing candidate settings on the caller's own device-resident
-batch (CUDA events on the pipeline's stream, best of a few runs each). The
+Chooses the neighbour-grid cell size, the kNN block shape, the queries
+per warp, the first-pass radius factor and the number of grid levels run
+one query per lane by timing candidate settings on the caller's own
+device-resident batch (CUDA events on the pipeline's stream, best of a few runs each). The
 choice is cached per workload signature so later runs reuse it.
 """
 from __future__ import annotations
@@ -39,6 +40,7 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
          cells: Optional[Iterable[float]] = None,
          blocks: Iterable[int] = (256,),
          qpws: Iterable[int] = (0,), rfacs: Iterable[float] = (0.7, 1.0),
+         lane_levels: Iterable[int] = (3, 2),
          reps: int = 2,
          cache_file: Optional[str] = None, verbose: bool = False) -> Tuple[dict, list]:
     """Returns (best setting, all trials) and applies the best to `pipe`."""
@@ -52,26 +54,31 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
         b = _CACHE[sig]
         pipe.set_tuning(b["cell"], b["block"], b["qpw"])
         pipe.set_search_radius_factor(b["rfac"])
+        pipe.set_lane_levels(b.get("lane_levels", 0))
         return b, []
     leaf = pipe.cfg.leaf_size
-    cells = list(cells) if cells is not None else [leaf * m for m in (3.0, 5.0, 8.0, 12.0)]
+    cells = list(cells) if cells is not None else [leaf * m for m in (3.0, 5.0, 8.0, 10.0, 12.0)]
     args = (x, y, z, offsets, n_frames, n_points)
     trials = []
     for c in cells:
         for b in blocks:
             for q in qpws:
                 for rf in rfacs:
-                    pipe.set_tuning(c, b, q)
-                    pipe.set_search_radius_factor(rf)
-                    pipe.run_device(*args)  # warm
-                    t = _time_run(pipe, args, reps)
-                    trials.append({"cell": c, "block": b, "qpw": q, "rfac": rf, "ms": t})
-                    if verbose:
-                        print(f"[autotune] cell={c:.3f} block={b} qpw={q} rfac={rf}: {t:.3f} ms",
-                              flush=True)
+                    for ll in lane_levels:
+                        pipe.set_tuning(c, b, q)
+                        pipe.set_search_radius_factor(rf)
+                        pipe.set_lane_levels(ll)
+                        pipe.run_device(*args)  # warm
+                        t = _time_run(pipe, args, reps)
+                        trials.append({"cell": c, "block": b, "qpw": q, "rfac": rf,
+                                       "lane_levels": ll, "ms": t})
+                        if verbose:
+                            print(f"[autotune] cell={c:.3f} block={b} qpw={q} rfac={rf} "
+                                  f"lane_levels={ll}: {t:.3f} ms", flush=True)
     best = min(trials, key=lambda r: r["ms"])
     pipe.set_tuning(best["cell"], best["block"], best["qpw"])
     pipe.set_search_radius_factor(best["rfac"])
+    pipe.set_lane_levels(best["lane_levels"])
     _CACHE[sig] = best
     if cache_file:
         try:

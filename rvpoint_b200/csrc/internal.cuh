@@ -292,6 +292,7 @@ struct TileArgs {
   size_t n_max;             // size of qlevel / qtau
   cudaEvent_t *level_events;  // null, or 2 per grid level: around each level's kNN kernel
   bool preset_open;         // qlevel already holds 0 (open) / 0xFF (done) per grid point
+  int lane_levels;          // grid levels of the per-lane kernels (0: all)
 };
 // false if k has no tile instantiation (use grid_knn then)
 // Normals of the kept points whose SOR neighbour list (TILE_SOR_LIST, ks per

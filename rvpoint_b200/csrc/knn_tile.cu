@@ -472,8 +472,12 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
         // kernel, which scans the tight window of sqrt(tau) at the finest
         // level where it stays small; the top-level ring would hold far more
         // points than that window
-        const bool to_warp = level + 2 == kGridLevels && tau >= 0.0f && a.hard_tau;
-        if (level + 1 < kGridLevels && !to_warp) {
+        // lane_levels: the levels run by these per-lane kernels; past
+        // them the warp kernel (lanes over candidates) takes the query
+        const int last = a.lane_levels > 0 && a.lane_levels < kGridLevels ? a.lane_levels - 1
+                                                                           : kGridLevels - 1;
+        const bool to_warp = level + 1 == last && tau >= 0.0f && a.hard_tau;
+        if (level < last && !to_warp) {
           qlevel[pos] = (uint8_t)(level + 1);
           qtau[pos] = tau;
         } else {
@@ -532,7 +536,9 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
     // when the caller marked the open queries) read the compacted list of
     // open queries
     const int wblocks = ctx->num_sms * 3 * 4;
-    for (int level = 0; level < kGridLevels; ++level) {
+    const int levels = a.lane_levels > 0 && a.lane_levels < kGridLevels ? a.lane_levels
+                                                                        : kGridLevels;
+    for (int level = 0; level < levels; ++level) {
       const u32 *list = nullptr;
       if (level > 0 || a.preset_open) {
         const unsigned gb = grid_for(a.n_max, 256, ctx->num_sms * 16);
@@ -560,6 +566,10 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
                                                                  qlevel, a.qtau, st);
       RVP_LAUNCH_CHECK(ctx);
       if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
+    }
+    for (int level = levels; level < kGridLevels && a.level_events; ++level) {
+      cudaEventRecord(a.level_events[2 * level], ctx->stream);  // not run: zero length
+      cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
     }
     return;
   }

@@ -30,7 +30,8 @@ struct rvp_pipeline {
   size_t max_points = 0;
   int max_frames = 0;
   float cell = 0.0f;
-  float rfac = 0.9f;  // level-0 first-pass radius factor (tunable)
+  float rfac = 0.9f;
+  int lane_levels = 0;  // grid levels of the per-lane kNN kernels (0: all)  // level-0 first-pass radius factor (tunable)
   rvp::VoxelWork vw;
   rvp::Grid grid;
   rvp::DevBuf in_x, in_y, in_z, in_offs;
@@ -281,6 +282,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.qlevel = p->qlevel.as<uint8_t>();
     ta.qtau = p->qtau.as<float>();
     ta.rfac = p->rfac;
+    ta.lane_levels = p->lane_levels;
     ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles instead
     {
       char *op = p->open.as<char>();
@@ -521,6 +523,12 @@ rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size, int block_t
 rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac) {
   if (!p || !(rfac >= 0.0f)) return RVP_ERR_INVALID_ARG;
   p->rfac = rfac;
+  return RVP_OK;
+}
+
+rvp_status rvp_pipeline_set_lane_levels(rvp_pipeline *p, int levels) {
+  if (!p || levels < 0 || levels > 3) return RVP_ERR_INVALID_ARG;
+  p->lane_levels = levels;
   return RVP_OK;
 }
 

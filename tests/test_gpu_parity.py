@@ -459,3 +459,20 @@ def test_pipeline_level_kernel_times(gpu_ctx):
     assert t["sor_knn_l0"] + t["sor_knn_l1"] + t["sor_knn_l2"] <= t["sor_knn"] * 1.001
     assert (t["normals_knn_l0"] + t["normals_knn_l1"] + t["normals_knn_l2"]
             <= t["normals_knn"] * 1.001)
+
+
+@pytest.mark.gpu
+def test_pipeline_lane_levels_do_not_change_results(gpu_ctx):
+    """Handing queries to the warp-per-query kernel after 1, 2 or 3 grid
+    levels changes the work, not the results."""
+    from rvpoint_b200 import api
+    batch = D.lidar_batch(n_frames=3, seed=29)
+    outs = []
+    for ll in (0, 1, 2):
+        p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, cell_size=0.5)
+        p.set_lane_levels(ll)
+        outs.append(p.run_host(batch))
+    for o in outs[1:]:
+        assert np.array_equal(bits(o["sor"]), bits(outs[0]["sor"]))
+        assert np.array_equal(bits(o["normals"]), bits(outs[0]["normals"]))
+        assert np.array_equal(o["ransac_count"], outs[0]["ransac_count"])
