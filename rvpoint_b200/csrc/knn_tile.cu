@@ -61,6 +61,21 @@ __device__ __forceinline__ void sor_list_out(const TileArgs &a, u32 qidx, const 
   for (int j = 0; j < K; ++j) row[j] = (u32)nbr_idx(L[j]) & 0x7FFFFFFFu;
 }
 
+// the same network over float keys carrying an index beside each: a key
+// goes after equal keys already in the list
+template <int K>
+__device__ __forceinline__ void list_insert_kv(float (&L)[K], u32 (&I)[K], float key, u32 idx) {
+#pragma unroll
+  for (int j = K - 1; j > 0; --j) {
+    const bool a = key < L[j - 1], b = key < L[j];
+    L[j] = a ? L[j - 1] : (b ? key : L[j]);
+    I[j] = a ? I[j - 1] : (b ? idx : I[j]);
+  }
+  const bool b0 = key < L[0];
+  I[0] = b0 ? idx : I[0];
+  L[0] = b0 ? key : L[0];
+}
+
 template <int K, int MODE>
 __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(GridView g, TileArgs a, int level,
                                                  uint8_t *qlevel, float *qtau, u32 *stats) {
@@ -320,14 +335,17 @@ template <int K, int MODE>
 __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int level,
                                                   const u32 *list, const u64 *n_list,
                                                   uint8_t *qlevel, float *qtau, u32 *stats) {
-  using Key = typename std::conditional<MODE == TILE_SOR_MEAN, float, u64>::type;
+  // float keys where only distances order the list (SOR); the list mode
+  // carries indices beside them and detects ties (below)
+  constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST;
+  using Key = typename std::conditional<FKEY, float, u64>::type;
   __shared__ uint2 wtab[WT_WARPS][WT_CELLS];
   const u64 n = list ? *n_list : *g.n_points;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const u64 nwarps = (u64)gridDim.x * WT_WARPS;
   const int sh = 2 * level;
   Key kMax;
-  if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
+  if constexpr (FKEY) kMax = INFINITY;
   else kMax = ~0ull;
   for (u64 base = ((u64)blockIdx.x * WT_WARPS + wib) * 32; base < n; base += nwarps * 32) {
     const bool active = base + lane < n;
@@ -396,18 +414,23 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
       Key L[K];
       Key thr = kMax;
       u32 found = 0;
+      // list mode: indices, and the value of the last tie met at the
+      // boundary (an equal key rejected or evicted)
+      u32 I[MODE == TILE_SOR_LIST ? K : 1];
+      float tie = -1.0f;
       auto scan = [&](int lox, int hix, int loy, int hiy, int loz, int hiz, bool bounded,
                       float tb) {
 #pragma unroll
         for (int j = 0; j < K; ++j) L[j] = kMax;
         thr = kMax;
         found = 0;
+        tie = -1.0f;
         for (int t = 0; t < 27; ++t) {
           const int dx = kRingOrder[t][0], dy = kRingOrder[t][1], dz = kRingOrder[t][2];
           if (dx < lox || dx > hix || dy < loy || dy > hiy || dz < loz || dz > hiz) continue;
           if (t > 0) {
             float thr_d2;
-            if constexpr (MODE == TILE_SOR_MEAN) thr_d2 = thr;
+            if constexpr (FKEY) thr_d2 = thr;
             else thr_d2 = nbr_d2(thr);
             if (bounded) thr_d2 = fminf(thr_d2, tb);
             const float gx = dx < 0 ? glx : (dx > 0 ? ghx : 0.0f);
@@ -425,11 +448,18 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
             if (bounded && !(d2 <= tb)) continue;
             ++found;
             Key key;
-            if constexpr (MODE == TILE_SOR_MEAN) key = d2;
+            if constexpr (FKEY) key = d2;
             else key = pack_nbr(d2, (int)pidx);
             if (key < thr) {
-              list_insert<Key, K>(L, key);
+              if constexpr (MODE == TILE_SOR_LIST) {
+                list_insert_kv<K>(L, I, key, pidx);
+                if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
+              } else {
+                list_insert<Key, K>(L, key);
+              }
               thr = L[K - 1];
+            } else if constexpr (MODE == TILE_SOR_LIST) {
+              if (key == thr) tie = key;
             }
           }
         }
@@ -460,7 +490,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
       if (!ok) {
         scan(-1, 1, -1, 1, -1, 1, false, 0.0f);
         if (found >= (u32)K) {
-          if constexpr (MODE == TILE_SOR_MEAN) tau = L[K - 1];
+          if constexpr (FKEY) tau = L[K - 1];
           else tau = nbr_d2(L[K - 1]);
           const Window w1 = ring_window(F, q.x, q.y, q.z, 1, level);
           const double cov = coverage(F, w1, q.x, q.y, q.z);
@@ -493,7 +523,19 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
           for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
           a.mean[qidx] = fdiv(sum, (float)(K - 1));
         } else if constexpr (MODE == TILE_SOR_LIST) {
-          sor_list_out<K>(a, qidx, L);
+          float sum = 0.0f;
+#pragma unroll
+          for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
+          a.mean[qidx] = fdiv(sum, (float)(K - 1));
+          // equal distances leave the order (and at the boundary the set)
+          // to the scan order instead of the index: such a list is marked
+          // unusable and the normal stage searches that point again
+          bool tied = tie == L[K - 1];
+#pragma unroll
+          for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
+          u32 *row = a.sor_list + (size_t)qidx * K;
+#pragma unroll
+          for (int j = 0; j < K; ++j) row[j] = tied ? 0xFFFFFFFFu : I[j];
         } else if constexpr (MODE == TILE_NORMALS) {
           float nx, ny, nz;
           normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
