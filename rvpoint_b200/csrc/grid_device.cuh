@@ -271,6 +271,30 @@ struct WarpList {
       carry = last;
     }
   }
+  // one key per lane (~0 for none) merged at once (32-slot lists): a
+  // bitonic sort of the 32 keys, then the 32 smallest of both lists as a
+  // bitonic sequence, sorted again
+  __device__ __forceinline__ void merge_lanes(u64 key) {
+    static_assert(P == 1, "batch merge is for 32-slot lists");
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        const u64 o = __shfl_xor_sync(0xffffffffu, key, j);
+        const bool up = (lane & k) == 0, low = (lane & j) == 0;
+        key = (low == up) ? (o < key ? o : key) : (o < key ? key : o);
+      }
+    }
+    const u64 rev = __shfl_sync(0xffffffffu, key, 31 - lane);
+    u64 v = e[0] < rev ? e[0] : rev;
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+      const u64 o = __shfl_xor_sync(0xffffffffu, v, j);
+      v = (lane & j) == 0 ? (o < v ? o : v) : (o < v ? v : o);
+    }
+    e[0] = v;
+  }
 };
 
 template <int P>
@@ -286,6 +310,13 @@ __device__ __forceinline__ void knn_scan(const GridView &g, const GridFrame &F, 
     const bool in_bound = key <= bound;
     found += __popc(__ballot_sync(0xffffffffu, in_bound));
     unsigned m = __ballot_sync(0xffffffffu, in_bound && key < thr);
+    if constexpr (P == 1) {
+      if (__popc(m) > 4) {  // many at once: one merge instead of serial inserts
+        L.merge_lanes((m >> (threadIdx.x & 31)) & 1u ? key : ~0ull);
+        thr = L.get(K - 1);
+        m = 0;
+      }
+    }
     while (m) {
       const int src = __ffs(m) - 1;
       m &= m - 1;
