@@ -50,44 +50,75 @@ __global__ void k_sor_mean(const u64 *pairs, int kk, const int32_t *counts, size
 // (coalesced), then lane 0 adds them in input order -- the same sequence of
 // roundings as the reference's loop, without one global load per add.
 constexpr int ST_CHUNK = 1024;
-__global__ __launch_bounds__(32) void k_sor_stats_warp(const float *__restrict__ mean,
+// One block of two warps per frame: warp 1 stages the next chunk of means
+// in shared memory while lane 0 of warp 0 adds up the current one in input
+// order (the reference's sequential float sums), four values per load.
+__global__ __launch_bounds__(64) void k_sor_stats_warp(const float *__restrict__ mean,
                                                        const int64_t *offs, int n_frames,
                                                        float alpha, float *thresh) {
-  __shared__ float buf[ST_CHUNK];
+  __shared__ __align__(16) float buf[2][ST_CHUNK];
+  __shared__ float s_mu;
   const int f = blockIdx.x;
   if (f >= n_frames) return;
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t a = offs[f], b = offs[f + 1];
   const int64_t n = b - a;
   if (n <= 0) {
-    if (lane == 0) thresh[f] = 0.0f;
+    if (tid == 0) thresh[f] = 0.0f;
     return;
   }
-  float s = 0.0f;
-  for (int64_t base = a; base < b; base += ST_CHUNK) {
+  const int nch = (int)((n + ST_CHUNK - 1) / ST_CHUNK);
+  auto stage = [&](int c) {
+    const int64_t base = a + (int64_t)c * ST_CHUNK;
     const int m = (int)((b - base) < ST_CHUNK ? (b - base) : ST_CHUNK);
-    for (int j = lane; j < m; j += 32) buf[j] = __ldg(&mean[base + j]);
-    __syncwarp();
-    if (lane == 0)
-      for (int t = 0; t < m; ++t) s = fadd(s, buf[t]);
-    __syncwarp();
-  }
-  const float mu = __shfl_sync(0xffffffffu, fdiv(s, (float)n), 0);
-  float var = 0.0f;
-  for (int64_t base = a; base < b; base += ST_CHUNK) {
-    const int m = (int)((b - base) < ST_CHUNK ? (b - base) : ST_CHUNK);
-    for (int j = lane; j < m; j += 32) buf[j] = __ldg(&mean[base + j]);
-    __syncwarp();
-    if (lane == 0)
-      for (int t = 0; t < m; ++t) {
-        const float d = fsub(buf[t], mu);
-        var = fadd(var, fmul(d, d));
+    float *dst = buf[c & 1];
+    for (int j = lane; j < m; j += 32) dst[j] = __ldg(&mean[base + j]);
+  };
+  float acc = 0.0f;
+  for (int pass = 0; pass < 2; ++pass) {
+    const float mu = pass ? s_mu : 0.0f;
+    if (warp == 1) stage(0);
+    __syncthreads();
+    for (int c = 0; c < nch; ++c) {
+      if (warp == 1 && c + 1 < nch) stage(c + 1);
+      if (tid == 0) {
+        const int m = (int)((n - (int64_t)c * ST_CHUNK) < ST_CHUNK ? (n - (int64_t)c * ST_CHUNK)
+                                                                   : ST_CHUNK);
+        const float *src = buf[c & 1];
+        const float4 *src4 = reinterpret_cast<const float4 *>(src);
+        int t = 0;
+        for (; t + 4 <= m; t += 4) {
+          const float4 v = src4[t >> 2];
+          if (pass == 0) {
+            acc = fadd(acc, v.x); acc = fadd(acc, v.y); acc = fadd(acc, v.z); acc = fadd(acc, v.w);
+          } else {
+            float d = fsub(v.x, mu); acc = fadd(acc, fmul(d, d));
+            d = fsub(v.y, mu); acc = fadd(acc, fmul(d, d));
+            d = fsub(v.z, mu); acc = fadd(acc, fmul(d, d));
+            d = fsub(v.w, mu); acc = fadd(acc, fmul(d, d));
+          }
+        }
+        for (; t < m; ++t) {
+          if (pass == 0) {
+            acc = fadd(acc, src[t]);
+          } else {
+            const float d = fsub(src[t], mu);
+            acc = fadd(acc, fmul(d, d));
+          }
+        }
       }
-    __syncwarp();
-  }
-  if (lane == 0) {
-    const float sd = __fsqrt_rn(fdiv(var, (float)n));
-    thresh[f] = fadd(mu, fmul(alpha, sd));
+      __syncthreads();
+    }
+    if (tid == 0) {
+      if (pass == 0) {
+        s_mu = fdiv(acc, (float)n);
+        acc = 0.0f;
+      } else {
+        const float sd = __fsqrt_rn(fdiv(acc, (float)n));
+        thresh[f] = fadd(s_mu, fmul(alpha, sd));
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -162,7 +193,7 @@ void sor_filter_frames(rvp_context *ctx, const float *x, const float *y, const f
   p += al((size_t)(n_frames + 1) * 4);
   void *scan_tmp = p;
   cudaStream_t st = ctx->stream;
-  k_sor_stats_warp<<<(unsigned)(n_frames > 0 ? n_frames : 1), 32, 0, st>>>(mean, offs, n_frames,
+  k_sor_stats_warp<<<(unsigned)(n_frames > 0 ? n_frames : 1), 64, 0, st>>>(mean, offs, n_frames,
                                                                          alpha, thresh);
   RVP_LAUNCH_CHECK(ctx);
   k_sor_keep<<<grid_for(n_max, 256, ctx->num_sms * 16), 256, 0, st>>>(mean, offs, n_frames, n_max,

@@ -45,38 +45,66 @@ __global__ void k_vox_init(int *mm, int n_frames) {
   }
 }
 
+// Per-frame voxel-index bounds. Each warp owns one contiguous run of points
+// and keeps its running min / max in registers, flushing them with atomics
+// only when its run crosses into the next frame (a few atomics per warp
+// instead of six per 32 points on the same frame's six words).
 __global__ void k_vox_minmax(const float *x, const float *y, const float *z, const int64_t *offs,
                              int n_frames, size_t n_max, const u64 *n_dev, float inv, int *mm) {
   const size_t n = n_dev ? *n_dev : n_max;
   const int lane = threadIdx.x & 31;
-  for (size_t base = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) & ~(size_t)31; base < n;
-       base += (size_t)gridDim.x * blockDim.x) {
-    const size_t i = base + lane;
-    const bool valid = i < n;
-    int v[3] = {0, 0, 0}, f = -1;
-    if (valid) {
-      voxel_of(x[i], y[i], z[i], inv, v[0], v[1], v[2]);
-      f = n_frames > 1 ? frame_of_index(offs, n_frames, i) : 0;
-    }
-    const int f0 = __shfl_sync(0xffffffffu, f, 0);
-    if (__all_sync(0xffffffffu, !valid || f == f0)) {
+  const size_t warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const size_t w = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t per = ((n + warps - 1) / warps + 31) & ~(size_t)31;
+  const size_t a = w * per, e = a + per < n ? a + per : n;
+  if (a >= e) return;
+  int f = n_frames > 1 ? frame_of_index(offs, n_frames, a) : 0;
+  size_t f_end = n_frames > 1 ? (size_t)offs[f + 1] : n;
+  int lo[3] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF};
+  int hi[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
+  auto flush = [&](int fr) {
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int lo = __reduce_min_sync(0xffffffffu, valid ? v[a] : 0x7FFFFFFF);
-        const int hi = __reduce_max_sync(0xffffffffu, valid ? v[a] : (int)0x80000000);
-        if (lane == 0 && f0 >= 0) {
-          atomicMin(&mm[6 * f0 + a], lo);
-          atomicMax(&mm[6 * f0 + 3 + a], hi);
-        }
+    for (int k = 0; k < 3; ++k) {
+      const int l = __reduce_min_sync(0xffffffffu, lo[k]);
+      const int h = __reduce_max_sync(0xffffffffu, hi[k]);
+      if (lane == 0 && l <= h) {
+        atomicMin(&mm[6 * fr + k], l);
+        atomicMax(&mm[6 * fr + 3 + k], h);
       }
-    } else if (valid) {
+      lo[k] = 0x7FFFFFFF;
+      hi[k] = (int)0x80000000;
+    }
+  };
+  for (size_t base = a; base < e; base += 32) {
+    // the frame changes at most a few times in a run: flush, then move on
+    while (n_frames > 1 && base >= f_end && f + 1 < n_frames) {
+      flush(f);
+      ++f;
+      f_end = (size_t)offs[f + 1];
+    }
+    const size_t i = base + lane;
+    if (i < e) {
+      if (i >= f_end) {  // this lane's point already belongs to a later frame
+        int v[3];
+        voxel_of(x[i], y[i], z[i], inv, v[0], v[1], v[2]);
+        const int fi = frame_of_index(offs, n_frames, i);
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        atomicMin(&mm[6 * f + a], v[a]);
-        atomicMax(&mm[6 * f + 3 + a], v[a]);
+        for (int k = 0; k < 3; ++k) {
+          atomicMin(&mm[6 * fi + k], v[k]);
+          atomicMax(&mm[6 * fi + 3 + k], v[k]);
+        }
+      } else {
+        int v[3];
+        voxel_of(x[i], y[i], z[i], inv, v[0], v[1], v[2]);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = min(lo[k], v[k]);
+          hi[k] = max(hi[k], v[k]);
+        }
       }
     }
   }
+  flush(f);
 }
 
 __device__ __forceinline__ int bits_for(unsigned long long r) {
