@@ -54,45 +54,60 @@ __global__ void k_bbox_init(float *bb, int n_frames) {
   }
 }
 
+// One contiguous run of points per warp; running min / max in registers,
+// flushed with atomics only where the run crosses into the next frame.
 __global__ void k_bbox(const float *__restrict__ x, const float *__restrict__ y,
                        const float *__restrict__ z, const int64_t *offs, int n_frames,
                        size_t n_max, const u64 *n_dev, float *bb) {
   const size_t n = n_dev ? *n_dev : n_max;
   const int lane = threadIdx.x & 31;
-  for (size_t base = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) & ~(size_t)31; base < n;
-       base += (size_t)gridDim.x * blockDim.x) {
-    const size_t i = base + lane;
-    const bool valid = i < n;
-    float vx = 0, vy = 0, vz = 0;
-    int f = -1;
-    if (valid) {
-      vx = x[i]; vy = y[i]; vz = z[i];
-      f = n_frames > 1 ? frame_of_index(offs, n_frames, i) : 0;
-    }
-    const int f0 = __shfl_sync(0xffffffffu, f, 0);
-    const bool uniform = __all_sync(0xffffffffu, !valid || f == f0);
-    if (uniform) {
-      float mnx = valid ? vx : INFINITY, mny = valid ? vy : INFINITY, mnz = valid ? vz : INFINITY;
-      float mxx = valid ? vx : -INFINITY, mxy = valid ? vy : -INFINITY, mxz = valid ? vz : -INFINITY;
+  const size_t warps = ((size_t)gridDim.x * blockDim.x) >> 5;
+  const size_t w = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const size_t per = ((n + warps - 1) / warps + 31) & ~(size_t)31;
+  const size_t a = w * per, e = a + per < n ? a + per : n;
+  if (a >= e) return;
+  int f = n_frames > 1 ? frame_of_index(offs, n_frames, a) : 0;
+  size_t f_end = n_frames > 1 ? (size_t)offs[f + 1] : n;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  auto flush = [&](int fr) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
       for (int o = 16; o; o >>= 1) {
-        mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
-        mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
-        mnz = fminf(mnz, __shfl_xor_sync(0xffffffffu, mnz, o));
-        mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
-        mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
-        mxz = fmaxf(mxz, __shfl_xor_sync(0xffffffffu, mxz, o));
+        mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+        mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
       }
-      if (lane == 0 && f0 >= 0) {
-        float *b = bb + 6 * f0;
-        atomic_min_f(b + 0, mnx); atomic_min_f(b + 1, mny); atomic_min_f(b + 2, mnz);
-        atomic_max_f(b + 3, mxx); atomic_max_f(b + 4, mxy); atomic_max_f(b + 5, mxz);
+      if (lane == 0 && mn[k] <= mx[k]) {
+        atomic_min_f(bb + 6 * fr + k, mn[k]);
+        atomic_max_f(bb + 6 * fr + 3 + k, mx[k]);
       }
-    } else if (valid) {
-      float *b = bb + 6 * f;
-      atomic_min_f(b + 0, vx); atomic_min_f(b + 1, vy); atomic_min_f(b + 2, vz);
-      atomic_max_f(b + 3, vx); atomic_max_f(b + 4, vy); atomic_max_f(b + 5, vz);
+      mn[k] = INFINITY;
+      mx[k] = -INFINITY;
+    }
+  };
+  for (size_t base = a; base < e; base += 32) {
+    while (n_frames > 1 && base >= f_end && f + 1 < n_frames) {
+      flush(f);
+      ++f;
+      f_end = (size_t)offs[f + 1];
+    }
+    const size_t i = base + lane;
+    if (i < e) {
+      const float v[3] = {x[i], y[i], z[i]};
+      if (i >= f_end) {  // already in a later frame
+        const int fi = frame_of_index(offs, n_frames, i);
+        float *bf = bb + 6 * fi;
+        atomic_min_f(bf + 0, v[0]); atomic_min_f(bf + 1, v[1]); atomic_min_f(bf + 2, v[2]);
+        atomic_max_f(bf + 3, v[0]); atomic_max_f(bf + 4, v[1]); atomic_max_f(bf + 5, v[2]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          mn[k] = fminf(mn[k], v[k]);
+          mx[k] = fmaxf(mx[k], v[k]);
+        }
+      }
     }
   }
+  flush(f);
 }
 
 // setInputCloud's padding and grid dimensions (spatial_hashing.cpp:141-150),
