@@ -383,10 +383,13 @@ RVP_API rvp_status rvp_mlp_forward(rvp_scorer *s, const float *features, size_t 
  * its gradient w.r.t. the parameters (host, RVP_MLP_PARAMS floats). */
 RVP_API rvp_status rvp_mlp_gradients(rvp_scorer *s, const float *features, const float *labels,
                                      size_t n, float *grad, double *loss);
-/* One Adam step (beta 0.9 / 0.999) on that loss; loss (host, may be NULL)
- * receives the loss before the step. */
+/* One Adam step (beta 0.9 / 0.999) on that loss over all n rows, or, with
+ * batch > 0, over a minibatch of `batch` rows drawn uniformly with
+ * replacement (a counter-based generator keyed by seed and the step count).
+ * loss (host, may be NULL) receives the loss before the step. */
 RVP_API rvp_status rvp_mlp_train_step(rvp_scorer *s, const float *features, const float *labels,
-                                      size_t n, float lr, double *loss);
+                                      size_t n, size_t batch, uint64_t seed, float lr,
+                                      double *loss);
 
 #ifdef __cplusplus
 }

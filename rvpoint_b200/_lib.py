@@ -111,7 +111,7 @@ SIGNATURES = {
     "rvp_mlp_set_norm": (I, [P, P, P]),
     "rvp_mlp_forward": (I, [P, P, SZ, P]),
     "rvp_mlp_gradients": (I, [P, P, P, SZ, P, C.POINTER(C.c_double)]),
-    "rvp_mlp_train_step": (I, [P, P, P, SZ, F, C.POINTER(C.c_double)]),
+    "rvp_mlp_train_step": (I, [P, P, P, SZ, SZ, C.c_uint64, F, C.POINTER(C.c_double)]),
 }
 
 MLP_INPUTS = 8

@@ -249,8 +249,11 @@ constexpr size_t TRAIN_SMEM = (size_t)(NP + 3 + 2 * MI + TB * ROW) * sizeof(floa
 
 // Forward + backward of mean binary cross-entropy with logits over n points
 // (labels 0/1), gradients added to grad, the loss sum to loss_sum.
+// With sample_seed != 0 the n rows are a minibatch drawn uniformly (with
+// replacement) from the n_src rows by a counter-based generator.
 __global__ __launch_bounds__(TB) void k_mlp_train(const float *__restrict__ feat,
                                                   const float *__restrict__ labels, size_t n,
+                                                  size_t n_src, u64 sample_seed,
                                                   const __nv_bfloat16 *__restrict__ wq,
                                                   const float *__restrict__ norm, float *grad,
                                                   double *loss_sum) {
@@ -270,9 +273,10 @@ __global__ __launch_bounds__(TB) void k_mlp_train(const float *__restrict__ feat
   for (int r = 0; r < 4; ++r) gw1[r] = 0.0f;
   float loss = 0.0f;
   for (size_t base = (size_t)blockIdx.x * TB; base < n; base += (size_t)gridDim.x * TB) {
-    const size_t i = base + tid;
+    const size_t slot = base + tid;
+    const size_t i = sample_seed ? (size_t)(mix64(sample_seed ^ mix64(slot)) % n_src) : slot;
     float *row = rows + tid * ROW;
-    if (i < n) {
+    if (slot < n) {
       float xn[MI];
       normalise(feat, i, snorm, xn);
       float h1[MH];
@@ -718,15 +722,16 @@ rvp_status rvp_mlp_forward(rvp_scorer *s, const float *features, size_t n, float
 }
 
 namespace {
-void mlp_grad(rvp_scorer *s, const float *features, const float *labels, size_t n) {
+void mlp_grad(rvp_scorer *s, const float *features, const float *labels, size_t n,
+              size_t n_src = 0, u64 sample_seed = 0) {
   rvp_context *ctx = s->ctx;
   RVP_CUDA_TRY(cudaMemsetAsync(s->grad.ptr, 0, rvp::NP * 4, ctx->stream));
   RVP_CUDA_TRY(cudaMemsetAsync(s->loss.ptr, 0, 8, ctx->stream));
   const unsigned blocks =
       (unsigned)std::min<size_t>((n + rvp::TB - 1) / rvp::TB, (size_t)ctx->num_sms);
   rvp::k_mlp_train<<<blocks, rvp::TB, rvp::TRAIN_SMEM, ctx->stream>>>(
-      features, labels, n, s->wq.as<__nv_bfloat16>(), s->norm.as<float>(), s->grad.as<float>(),
-      s->loss.as<double>());
+      features, labels, n, n_src ? n_src : n, sample_seed, s->wq.as<__nv_bfloat16>(),
+      s->norm.as<float>(), s->grad.as<float>(), s->loss.as<double>());
   RVP_LAUNCH_CHECK(ctx);
 }
 }  // namespace
@@ -748,12 +753,16 @@ rvp_status rvp_mlp_gradients(rvp_scorer *s, const float *features, const float *
 }
 
 rvp_status rvp_mlp_train_step(rvp_scorer *s, const float *features, const float *labels,
-                              size_t n, float lr, double *loss) {
+                              size_t n, size_t batch, uint64_t seed, float lr, double *loss) {
   if (!s || !(lr > 0.0f)) return RVP_ERR_INVALID_ARG;
   return sguard(s->ctx, [&] {
     RVP_REQUIRE(n > 0 && features && labels, "empty batch");
     RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
-    mlp_grad(s, features, labels, n);
+    if (batch > 0)  // a fresh minibatch every step: the key mixes seed and step
+      mlp_grad(s, features, labels, batch, n,
+               (seed ^ (0x9E3779B97F4A7C15ull * (u64)(s->adam_step + 1))) | 1ull);
+    else
+      mlp_grad(s, features, labels, n);
     s->adam_step++;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.0f / (1.0f - powf(b1, (float)s->adam_step));

@@ -145,12 +145,14 @@ class PlaneScorer:
         return float(loss.value), g
 
     def train_step(self, feat: torch.Tensor, labels: torch.Tensor, lr: float,
-                   want_loss: bool = False):
+                   want_loss: bool = False, batch: int = 0, seed: int = 1):
+        """One Adam step over all rows, or over a minibatch of `batch` rows
+        drawn on the device."""
         self.ctx.use_torch_stream()
         loss = C.c_double(0.0)
         check(self.L.rvp_mlp_train_step(self.h, _p(feat), _p(labels), int(feat.shape[0]),
-                                        float(lr), C.byref(loss) if want_loss else None),
-              self.ctx.h)
+                                        int(batch), int(seed), float(lr),
+                                        C.byref(loss) if want_loss else None), self.ctx.h)
         return float(loss.value) if want_loss else None
 
     def close(self):
@@ -242,15 +244,12 @@ def train(scorer: PlaneScorer, b: DeviceBatch, cfg: TrainConfig = TrainConfig())
     mean = feat.mean(0).cpu().numpy()
     std = feat.std(0).clamp_min(1e-6).cpu().numpy()
     scorer.set_norm(mean, std)
-    g = torch.Generator(device="cpu").manual_seed(cfg.seed)
     n = feat.shape[0]
     losses = []
     for step in range(cfg.steps):
-        idx = torch.randint(0, n, (min(cfg.batch, n),), generator=g).to(feat.device)
-        fb = feat[idx].contiguous()
-        lb = labels[idx].contiguous()
         want = step % 50 == 0 or step == cfg.steps - 1
-        l_ = scorer.train_step(fb, lb, cfg.lr, want_loss=want)
+        l_ = scorer.train_step(feat, labels, cfg.lr, want_loss=want,
+                               batch=min(cfg.batch, n), seed=cfg.seed)
         if want:
             losses.append((step, l_))
     torch.cuda.synchronize()
