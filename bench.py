@@ -283,13 +283,15 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
     t_l, (_, bl, it_l) = timed(lambda: lr.run(be, cand, coffs, 10_000, T, targets=tg))
     t_f, feat = timed(lambda: LR.proposal_features(scorer, be, cand, coffs, lr.cell, lr.scope))
     t_m, logits = timed(lambda: scorer.forward(feat))
-    t_w, _ = timed(lambda: LR.ransac_weighted(be, cand, coffs, logits, 10_000, T, seed=lr.seed,
-                                              logit_power=lr.logit_power, targets=tg, ctx=ctx))
+    t_w, _ = timed(lambda: lr.ransac(be, cand, coffs, logits, 10_000, T, targets=tg))
     q = lambda t, p: float(t.double().quantile(p).item())  # noqa: E731
     out = {"scenes": n_scenes, "points_per_scene": 50_000, "thresh": T,
            "train_scenes": n_train, "train_seconds": info["seconds"],
            "train_loss_first_last": [info["losses"][0][1], info["losses"][-1][1]],
            "candidates_per_scene": lr.cand_per_frame, "feature_scope": lr.scope,
+           "proposal": (f"preemptive: {lr.draws} draws per round ranked on the candidates, "
+                        "best 32 counted exactly" if lr.preemptive else "weighted draws, "
+                        "each counted exactly"),
            "plain_10k_ms": t_plain,
            "plain_10k_hypotheses_mean": float(it_plain.double().mean().item()),
            "plain_to_target_ms": t_ptg,
@@ -297,7 +299,7 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
                                           "median": q(it_ptg, 0.5), "p90": q(it_ptg, 0.9)},
            "learned_to_target_ms": t_l, "learned_parts_ms": {"features": t_f, "mlp": t_m,
                                                              "weighted_ransac": t_w},
-           "learned_hypotheses_to_target": {"mean": float(it_l.double().mean().item()),
+           "learned_hypotheses_drawn_to_target": {"mean": float(it_l.double().mean().item()),
                                             "median": q(it_l, 0.5), "p90": q(it_l, 0.9)},
            "learned_reached_fraction": float((bl >= tg).float().mean().item()),
            "time_ratio_plain10k_over_learned": t_plain / t_l,

@@ -346,6 +346,22 @@ RVP_API rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const f
                                        float collinear_thresh, float probability,
                                        const int32_t *targets, float *models, int32_t *best,
                                        int32_t *iters_run);
+/* The weighted proposal in preemptive rounds: each round draws `draws`
+ * (<= 512) hypotheses per frame from its candidates (at most 2048 per
+ * frame) by weight, ranks them by their inliers among the candidates, and
+ * counts the best 32 exactly over all of the frame's points, keeping the
+ * best exact count with the strict-greater rule across rounds. A frame stops
+ * when its count reaches its target (targets, optional) or after max_rounds;
+ * draws_run receives the hypotheses drawn per frame. weights as for
+ * rvp_ransac_weighted. */
+RVP_API rvp_status rvp_ransac_preemptive(rvp_context *ctx, const float *x, const float *y,
+                                         const float *z, const int64_t *frame_offsets_dev,
+                                         int n_frames, const uint32_t *cand,
+                                         const int64_t *cand_offsets_dev, size_t n_cand,
+                                         const float *weights, float logit_power, uint64_t seed,
+                                         int draws, int max_rounds, float dist_thresh,
+                                         float collinear_thresh, const int32_t *targets,
+                                         float *models, int32_t *best, int32_t *draws_run);
 /* labels[i] = 1 if point i lies within dist_thresh of its frame's model
  * (models: 4 floats per frame), else 0. */
 RVP_API rvp_status rvp_plane_labels(rvp_context *ctx, const float *x, const float *y,

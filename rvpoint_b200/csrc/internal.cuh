@@ -382,6 +382,13 @@ struct RansacSampler {
   const double *cdf = nullptr;
   u64 seed = 0;
   const int32_t *targets = nullptr;
+  // given hypotheses instead of drawn ones: n_models planes per frame (a NaN
+  // first coefficient marks an empty slot)
+  const float4 *models = nullptr;
+  int n_models = 0;
+  // start each frame from an earlier best (count and model), not from zero
+  const int32_t *best_in = nullptr;
+  const float *model_in = nullptr;
 };
 // One cluster of `cluster` blocks (1-8, fewer if the device cannot hold them)
 // per frame over SoA clouds; frame f = [off[f], off[f+1]).
@@ -391,6 +398,17 @@ void ransac_frames(rvp_context *ctx, const float *x, const float *y,
                    float *model, int32_t *best, int32_t *iters_run,
                    int32_t *counts_all, bool eval_all,
                    const RansacSampler &smp = RansacSampler{}, int cluster = 1);
+// Weighted proposal with preemptive rounds: each round draws `draws`
+// hypotheses per frame, ranks them by their inliers among the frame's
+// candidates and counts the best 32 exactly over all points (strict-greater
+// update carried over rounds); a frame stops at its target (smp.targets) or
+// after max_rounds. draws_run: hypotheses drawn per frame. scratch:
+// preemptive_temp_bytes(n_frames).
+void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const float *z,
+                       const int64_t *offs, int n_frames, const RansacSampler &smp, int draws,
+                       int max_rounds, const RansacParams &p, float *model, int32_t *best,
+                       int32_t *draws_run, void *scratch);
+size_t preemptive_temp_bytes(int n_frames);
 void extract_plane_run(rvp_context *ctx, const float *x, const float *y,
                        const float *z, size_t n, const float *model_dev,
                        float thresh, float *in_aos, float *out_aos,

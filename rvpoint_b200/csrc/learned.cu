@@ -66,7 +66,58 @@ __device__ __forceinline__ void jacobi_pair(float (&A)[3][3], float (&V)[3][3]) 
 }
 
 // f0..2 |normal|, f3 curvature, f4 planarity, f5 log K-th distance,
-// f6 |offset from the local plane| / r, f7 |offset from the centroid| / r
+// f6 |offset from the local plane| / r, f7 |offset from the centroid| / r,
+// from the offsets (neighbour - point) of the m nearest, in distance order,
+// and the squared distance r2 of the last of them
+__device__ __forceinline__ void plane_features(const float (&dx)[KF], const float (&dy)[KF],
+                                               const float (&dz)[KF], int m, float r2,
+                                               float (&f)[MI]) {
+  float cx = 0, cy = 0, cz = 0;
+#pragma unroll
+  for (int j = 0; j < KF; ++j)
+    if (j < m) {
+      cx += dx[j];
+      cy += dy[j];
+      cz += dz[j];
+    }
+  const float inv = 1.0f / (float)m;
+  cx *= inv; cy *= inv; cz *= inv;
+  float A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int j = 0; j < KF; ++j) {
+    if (j < m) {
+      const float ex = dx[j] - cx, ey = dy[j] - cy, ez = dz[j] - cz;
+      A[0][0] += ex * ex; A[0][1] += ex * ey; A[0][2] += ex * ez;
+      A[1][1] += ey * ey; A[1][2] += ey * ez; A[2][2] += ez * ez;
+    }
+  }
+  A[1][0] = A[0][1]; A[2][0] = A[0][2]; A[2][1] = A[1][2];
+  float V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll 1
+  for (int sweep = 0; sweep < 6; ++sweep) {
+    jacobi_pair<0, 1>(A, V);
+    jacobi_pair<0, 2>(A, V);
+    jacobi_pair<1, 2>(A, V);
+  }
+  float l0 = A[0][0], l1 = A[1][1], l2 = A[2][2];
+  float nx = V[0][0], ny = V[1][0], nz = V[2][0];
+  // smallest eigenvalue and its vector; then order the other two
+  if (l1 < l0) { const float tl = l0; l0 = l1; l1 = tl; nx = V[0][1]; ny = V[1][1]; nz = V[2][1]; }
+  if (l2 < l0) { const float tl = l0; l0 = l2; l2 = tl; nx = V[0][2]; ny = V[1][2]; nz = V[2][2]; }
+  if (l2 < l1) { const float tl = l1; l1 = l2; l2 = tl; }
+  l0 = fmaxf(l0, 0.0f);
+  const float sum = l0 + l1 + l2;
+  const float r = sqrtf(r2) + 1e-6f;
+  f[0] = fabsf(nx);
+  f[1] = fabsf(ny);
+  f[2] = fabsf(nz);
+  f[3] = sum > 0.0f ? l0 / sum : 1.0f;
+  f[4] = l2 > 0.0f ? (l1 - l0) / l2 : 0.0f;
+  f[5] = logf(r);
+  f[6] = fabsf(nx * cx + ny * cy + nz * cz) / r;
+  f[7] = sqrtf(cx * cx + cy * cy + cz * cz) / r;
+}
+
 __global__ __launch_bounds__(256) void k_features(const float *__restrict__ x,
                                                   const float *__restrict__ y,
                                                   const float *__restrict__ z,
@@ -82,7 +133,6 @@ __global__ __launch_bounds__(256) void k_features(const float *__restrict__ x,
     if (m >= 3) {
       const float px = x[i], py = y[i], pz = z[i];
       float dx[KF], dy[KF], dz[KF];
-      float cx = 0, cy = 0, cz = 0;
       float r2 = 0.0f;
 #pragma unroll
       for (int j = 0; j < KF; ++j) {
@@ -92,50 +142,12 @@ __global__ __launch_bounds__(256) void k_features(const float *__restrict__ x,
           dx[j] = x[q] - px;
           dy[j] = y[q] - py;
           dz[j] = z[q] - pz;
-          cx += dx[j];
-          cy += dy[j];
-          cz += dz[j];
           r2 = nbr_d2(key);
         } else {
           dx[j] = dy[j] = dz[j] = 0.0f;
         }
       }
-      const float inv = 1.0f / (float)m;
-      cx *= inv; cy *= inv; cz *= inv;
-      float A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-      for (int j = 0; j < KF; ++j) {
-        if (j < m) {
-          const float ex = dx[j] - cx, ey = dy[j] - cy, ez = dz[j] - cz;
-          A[0][0] += ex * ex; A[0][1] += ex * ey; A[0][2] += ex * ez;
-          A[1][1] += ey * ey; A[1][2] += ey * ez; A[2][2] += ez * ez;
-        }
-      }
-      A[1][0] = A[0][1]; A[2][0] = A[0][2]; A[2][1] = A[1][2];
-      float V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-#pragma unroll 1
-      for (int sweep = 0; sweep < 6; ++sweep) {
-        jacobi_pair<0, 1>(A, V);
-        jacobi_pair<0, 2>(A, V);
-        jacobi_pair<1, 2>(A, V);
-      }
-      float l0 = A[0][0], l1 = A[1][1], l2 = A[2][2];
-      float nx = V[0][0], ny = V[1][0], nz = V[2][0];
-      // smallest eigenvalue and its vector; then order the other two
-      if (l1 < l0) { const float tl = l0; l0 = l1; l1 = tl; nx = V[0][1]; ny = V[1][1]; nz = V[2][1]; }
-      if (l2 < l0) { const float tl = l0; l0 = l2; l2 = tl; nx = V[0][2]; ny = V[1][2]; nz = V[2][2]; }
-      if (l2 < l1) { const float tl = l1; l1 = l2; l2 = tl; }
-      l0 = fmaxf(l0, 0.0f);
-      const float sum = l0 + l1 + l2;
-      const float r = sqrtf(r2) + 1e-6f;
-      f[0] = fabsf(nx);
-      f[1] = fabsf(ny);
-      f[2] = fabsf(nz);
-      f[3] = sum > 0.0f ? l0 / sum : 1.0f;
-      f[4] = l2 > 0.0f ? (l1 - l0) / l2 : 0.0f;
-      f[5] = logf(r);
-      f[6] = fabsf(nx * cx + ny * cy + nz * cz) / r;
-      f[7] = sqrtf(cx * cx + cy * cy + cz * cz) / r;
+      plane_features(dx, dy, dz, m, r2, f);
     }
 #pragma unroll
     for (int k = 0; k < MI; ++k) feat[t * MI + k] = f[k];
@@ -647,7 +659,7 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
                                             cell_size, cand, n_cand, features);
   if (neighbours != 1 || !cand || !cand_offsets_dev) return RVP_ERR_INVALID_ARG;
   // neighbourhoods among the candidates only: their coordinates, frame by
-  // frame, become the cloud
+  // frame, become the cloud of the grid search
   rvp_context *ctx = s->ctx;
   const rvp_status st = sguard(ctx, [&] {
     RVP_REQUIRE(x && y && z, "null pointer");
@@ -853,6 +865,41 @@ rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const float *y,
     smp.targets = targets;
     rvp::ransac_frames(ctx, x, y, z, frame_offsets_dev, n_frames, nullptr, prm, models, best,
                        iters_run, nullptr, false, smp, 8);
+  });
+}
+
+rvp_status rvp_ransac_preemptive(rvp_context *ctx, const float *x, const float *y,
+                                 const float *z, const int64_t *frame_offsets_dev, int n_frames,
+                                 const uint32_t *cand, const int64_t *cand_offsets_dev,
+                                 size_t n_cand, const float *weights, float logit_power,
+                                 uint64_t seed, int draws, int max_rounds, float dist_thresh,
+                                 float collinear_thresh, const int32_t *targets, float *models,
+                                 int32_t *best, int32_t *draws_run) {
+  if (!ctx) return RVP_ERR_INVALID_ARG;
+  return sguard(ctx, [&] {
+    RVP_REQUIRE(x && y && z && frame_offsets_dev && cand && cand_offsets_dev && weights &&
+                    models && best && draws_run,
+                "null pointer");
+    RVP_REQUIRE(n_frames >= 1 && max_rounds >= 1, "n_frames / max_rounds must be >= 1");
+    RVP_REQUIRE(draws >= 1 && draws <= 512, "draws must be in [1, 512]");
+    RVP_REQUIRE(logit_power >= 0.0f, "logit_power must be >= 0");
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    rvp::DevBuf &cdf = ctx->scratch[26];
+    cdf.reserve(std::max<size_t>(n_cand, 1) * 8);
+    rvp::k_cdf<<<n_frames, 256, 0, ctx->stream>>>(weights, logit_power, cand_offsets_dev,
+                                                  cdf.as<double>());
+    RVP_LAUNCH_CHECK(ctx);
+    rvp::DevBuf &tmp = ctx->scratch[28];
+    tmp.reserve(rvp::preemptive_temp_bytes(n_frames));
+    rvp::RansacParams prm{dist_thresh, 32, collinear_thresh, log(1.0 - 0.9999)};
+    rvp::RansacSampler smp;
+    smp.cand = cand;
+    smp.cand_offs = cand_offsets_dev;
+    smp.cdf = cdf.as<double>();
+    smp.seed = seed;
+    smp.targets = targets;
+    rvp::ransac_preemptive(ctx, x, y, z, frame_offsets_dev, n_frames, smp, draws, max_rounds,
+                           prm, models, best, draws_run, tmp.ptr);
   });
 }
 

@@ -27,6 +27,7 @@ namespace {
 constexpr int HB = 32;        // hypotheses per batch
 constexpr int R_THREADS = 512;
 constexpr int R_PTS = 4;      // points per lane per pass (amortises the hypothesis loads)
+constexpr int PE_KEEP = HB;   // preemptive rounds: hypotheses counted exactly per round
 
 // compute_plane_coefficients (ransac_plane.cpp:18-50), exact op order.
 __device__ __forceinline__ bool plane_coeffs(float x1, float y1, float z1, float x2, float y2,
@@ -115,6 +116,15 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
     s_stop = 0;
     s_iters = prm.max_iters;
     s_model = make_float4(0, 0, 0, 0);
+    if (smp.best_in) {
+      s_best = smp.best_in[f];
+      s_model = make_float4(smp.model_in[4 * f + 0], smp.model_in[4 * f + 1],
+                            smp.model_in[4 * f + 2], smp.model_in[4 * f + 3]);
+      if (smp.targets && s_best >= smp.targets[f]) {  // reached in an earlier round
+        s_stop = 1;
+        s_iters = 0;
+      }
+    }
   }
   __syncthreads();
 
@@ -124,7 +134,10 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
       const int it = base + tid;
       float4 m = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);  // NaN: never an inlier
       int code = -3;
-      if (it < prm.max_iters) {
+      if (it < prm.max_iters && smp.models) {
+        m = smp.models[(size_t)f * smp.n_models + it];
+        code = isnan(m.x) ? -2 : 0;
+      } else if (it < prm.max_iters) {
         u32 i1, i2, i3;
         if (smp.cdf) {
           i1 = weighted_draw(smp, f, it, 0, a0, n);
@@ -241,6 +254,87 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
   }
 }
 
+// Preemptive round of the weighted proposal, one block per frame: draw
+// PE_H hypotheses from the frame's candidates by weight, count each one's
+// inliers among the candidates only (they sit in shared memory), and keep the
+// PE_KEEP best (count, then draw order) for the exact count over all points.
+// Frames that already reached their target write empty slots.
+constexpr int PE_THREADS = 256;
+constexpr int PE_MAXC = 2048;
+constexpr int PE_MAXH = 512;
+__global__ __launch_bounds__(PE_THREADS) void k_preempt(
+    const float *__restrict__ X, const float *__restrict__ Y, const float *__restrict__ Z,
+    const int64_t *offs, RansacSampler smp, int draws, int round, RansacParams prm,
+    const int32_t *best_now, float4 *out) {
+  __shared__ float4 P[PE_MAXC];
+  __shared__ float4 hyp[PE_MAXH];
+  __shared__ int hcnt[PE_MAXH];
+  const int f = blockIdx.x;
+  const int64_t a0 = offs[f];
+  const u32 n = (u32)(offs[f + 1] - a0);
+  const int64_t c0 = smp.cand_offs[f], c1 = smp.cand_offs[f + 1];
+  const int m = (int)(c1 - c0);
+  float4 *o = out + (size_t)f * PE_KEEP;
+  const float4 none = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);
+  const bool done = smp.targets && best_now && best_now[f] >= smp.targets[f];
+  if (done || n < 3 || m < 3 || m > PE_MAXC || !(smp.cdf[c1 - 1] > 0.0)) {
+    for (int t = threadIdx.x; t < PE_KEEP; t += blockDim.x) o[t] = none;
+    return;
+  }
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const u32 g = smp.cand[c0 + j];
+    P[j] = make_float4(X[g], Y[g], Z[g], 0.0f);
+  }
+  const float *x = X + a0, *y = Y + a0, *z = Z + a0;
+  for (int h = threadIdx.x; h < draws; h += blockDim.x) {
+    const int it = round * draws + h;
+    const u32 i1 = weighted_draw(smp, f, it, 0, a0, n);
+    const u32 i2 = weighted_draw(smp, f, it, 1, a0, n);
+    const u32 i3 = weighted_draw(smp, f, it, 2, a0, n);
+    float4 mdl = none;
+    if (!(i1 == i2 || i1 == i3 || i2 == i3 || i1 >= n || i2 >= n || i3 >= n) &&
+        !plane_coeffs(x[i1], y[i1], z[i1], x[i2], y[i2], z[i2], x[i3], y[i3], z[i3],
+                      prm.collinear, mdl))
+      mdl = none;
+    hyp[h] = mdl;
+  }
+  __syncthreads();
+  for (int h = threadIdx.x; h < draws; h += blockDim.x) {
+    const float4 mdl = hyp[h];
+    int c = -1;
+    if (!isnan(mdl.x)) {
+      c = 0;
+      for (int j = 0; j < m; ++j) c += is_inlier(mdl, P[j].x, P[j].y, P[j].z, prm.thresh) ? 1 : 0;
+    }
+    hcnt[h] = c;
+  }
+  __syncthreads();
+  for (int h = threadIdx.x; h < draws; h += blockDim.x) {
+    const int c = hcnt[h];
+    int rank = 0;
+    for (int g = 0; g < draws; ++g) {
+      const int cg = hcnt[g];
+      rank += (cg > c || (cg == c && g < h)) ? 1 : 0;
+    }
+    if (rank < PE_KEEP) o[rank] = c >= 0 ? hyp[h] : none;
+  }
+}
+
+// draws_run of the frames that stop after this round (reached their
+// target, or the last round); open counts the others
+__global__ void k_preempt_done(const int32_t *best, const int32_t *targets, int n_frames,
+                               int round, int draws, bool last, int32_t *draws_run, int *open) {
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n_frames; f += gridDim.x * blockDim.x) {
+    if (draws_run[f] >= 0) continue;
+    if (last || (targets && best[f] >= targets[f])) draws_run[f] = (round + 1) * draws;
+    else atomicAdd(open, 1);
+  }
+}
+
+__global__ void k_fill_i32(int32_t *p, int n, int v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
 // extract_plane_inliers_outliers_rvv, scalar branch (ransac_plane.cpp:373-381):
 // inlier iff -t <= a*x + b*y + c*z + d <= t.
 __global__ void k_plane_flags(const float *x, const float *y, const float *z, size_t n,
@@ -319,6 +413,49 @@ void ransac_frames(rvp_context *ctx, const float *x, const float *y, const float
   RVP_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_ransac, x, y, z, offs, rand_dev, p, model, best,
                                   iters_run, counts_all, eval_all, smp));
   ::rvp::count_launch(ctx);
+}
+
+void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const float *z,
+                       const int64_t *offs, int n_frames, const RansacSampler &smp0, int draws,
+                       int max_rounds, const RansacParams &p, float *model, int32_t *best,
+                       int32_t *draws_run, void *scratch) {
+  if (n_frames <= 0) return;
+  RVP_REQUIRE(draws >= 1 && draws <= PE_MAXH, "draws per round must be in [1, 512]");
+  char *sp = static_cast<char *>(scratch);
+  float4 *models = reinterpret_cast<float4 *>(sp);
+  int *open = reinterpret_cast<int *>(sp + al((size_t)n_frames * PE_KEEP * 16));
+  int32_t *dummy_iters = reinterpret_cast<int32_t *>(sp + al((size_t)n_frames * PE_KEEP * 16) + 256);
+  cudaStream_t st = ctx->stream;
+  k_fill_i32<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(draws_run, n_frames, -1);
+  RVP_LAUNCH_CHECK(ctx);
+  RansacParams pe = p;
+  pe.max_iters = PE_KEEP;
+  for (int r = 0; r < max_rounds; ++r) {
+    k_preempt<<<n_frames, PE_THREADS, 0, st>>>(x, y, z, offs, smp0, draws, r, p,
+                                               r > 0 ? best : nullptr, models);
+    RVP_LAUNCH_CHECK(ctx);
+    RansacSampler sm = smp0;
+    sm.models = models;
+    sm.n_models = PE_KEEP;
+    sm.best_in = r > 0 ? best : nullptr;
+    sm.model_in = r > 0 ? model : nullptr;
+    ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, pe, model, best, dummy_iters, nullptr,
+                  false, sm, 8);
+    RVP_CUDA_TRY(cudaMemsetAsync(open, 0, 4, st));
+    k_preempt_done<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(
+        best, smp0.targets, n_frames, r, draws, r + 1 == max_rounds, draws_run, open);
+    RVP_LAUNCH_CHECK(ctx);
+    if (smp0.targets) {
+      int h_open = 0;
+      RVP_CUDA_TRY(cudaMemcpyAsync(&h_open, open, 4, cudaMemcpyDeviceToHost, st));
+      RVP_CUDA_TRY(cudaStreamSynchronize(st));
+      if (h_open == 0) return;
+    }
+  }
+}
+
+size_t preemptive_temp_bytes(int n_frames) {
+  return al((size_t)n_frames * PE_KEEP * 16) + 256 + al((size_t)n_frames * 4);
 }
 
 size_t extract_temp_bytes(size_t n) {

@@ -206,6 +206,29 @@ def ransac_weighted(b: DeviceBatch, cand: torch.Tensor, cand_offsets: torch.Tens
     return models, best, iters
 
 
+def ransac_preemptive(b: DeviceBatch, cand: torch.Tensor, cand_offsets: torch.Tensor,
+                      weights: torch.Tensor, thresh: float, draws: int = 256,
+                      max_rounds: int = 40, seed: int = 1, logit_power: float = 0.0,
+                      collinear: float = 1e-6, targets: Optional[torch.Tensor] = None,
+                      ctx: Optional[Context] = None):
+    """Weighted proposal in preemptive rounds (rvp_ransac_preemptive):
+    returns (models, best, hypotheses drawn per frame)."""
+    ctx = ctx or default_context()
+    ctx.use_torch_stream()
+    dev = b.x.device
+    nf = b.n_frames
+    models = torch.empty((nf, 4), dtype=torch.float32, device=dev)
+    best = torch.empty(nf, dtype=torch.int32, device=dev)
+    drawn = torch.empty(nf, dtype=torch.int32, device=dev)
+    check(_lib.load().rvp_ransac_preemptive(ctx.h, _p(b.x), _p(b.y), _p(b.z), _p(b.offsets), nf,
+                                            _p(cand), _p(cand_offsets), int(cand.numel()),
+                                            _p(weights), float(logit_power), int(seed),
+                                            int(draws), int(max_rounds), float(thresh),
+                                            float(collinear), _p(targets), _p(models), _p(best),
+                                            _p(drawn)), ctx.h)
+    return models, best, drawn
+
+
 def plane_labels(b: DeviceBatch, models: torch.Tensor, thresh: float,
                  ctx: Optional[Context] = None) -> torch.Tensor:
     ctx = ctx or default_context()
@@ -261,7 +284,13 @@ class LearnedRansac:
     """features -> MLP -> weighted RANSAC over every frame of a batch."""
 
     def __init__(self, scorer: PlaneScorer, cell: float = 1.5, cand_per_frame: int = 1024,
-                 logit_power: float = 1.0, seed: int = 11, scope: str = "candidates"):
+                 logit_power: float = 1.0, seed: int = 11, scope: str = "candidates",
+                 preemptive: bool = True, draws: int = 512):
+        """preemptive: hypotheses ranked among the candidates first, the best
+        32 of every `draws` counted exactly (else every hypothesis is counted
+        exactly, 32 at a time)."""
+        self.preemptive = preemptive
+        self.draws = draws
         self.scorer = scorer
         self.cell = cell
         self.cand_per_frame = cand_per_frame
@@ -281,6 +310,16 @@ class LearnedRansac:
             targets: Optional[torch.Tensor] = None):
         feat = proposal_features(self.scorer, b, cand, cand_offsets, self.cell, self.scope)
         logits = self.scorer.forward(feat)
+        return self.ransac(b, cand, cand_offsets, logits, max_iters, thresh, targets)
+
+    def ransac(self, b: DeviceBatch, cand, cand_offsets, logits, max_iters: int, thresh: float,
+               targets: Optional[torch.Tensor] = None):
+        if self.preemptive:
+            rounds = max(1, (max_iters + self.draws - 1) // self.draws)
+            return ransac_preemptive(b, cand, cand_offsets, logits, thresh, draws=self.draws,
+                                     max_rounds=rounds, seed=self.seed,
+                                     logit_power=self.logit_power, targets=targets,
+                                     ctx=self.scorer.ctx)
         return ransac_weighted(b, cand, cand_offsets, logits, max_iters, thresh,
                                seed=self.seed, logit_power=self.logit_power, targets=targets,
                                ctx=self.scorer.ctx)

@@ -226,6 +226,31 @@ def test_weighted_ransac_counts_are_exact(gpu_ctx):
 
 
 @pytest.mark.gpu
+def test_preemptive_rounds_count_exactly_and_stop_at_targets(gpu_ctx):
+    import torch
+    from rvpoint_b200.learned import DeviceBatch, candidates, ransac_preemptive
+    tr = D.plane_batch(n_scenes=4, n=20_000, seed=D.SEED_BASE + 91)
+    b = DeviceBatch.from_host(tr)
+    cand_h, coffs_h = candidates(b.offsets_host, 1024, 5)
+    cand = torch.from_numpy(cand_h.view(np.int32)).cuda()
+    coffs = torch.from_numpy(coffs_h).cuda()
+    w = torch.ones(cand.numel(), dtype=torch.float32, device="cuda")
+    models, best, drawn = ransac_preemptive(b, cand, coffs, w, 0.02, draws=128, max_rounds=3,
+                                            seed=9, ctx=gpu_ctx)
+    models, best, drawn = models.cpu().numpy(), best.cpu().numpy(), drawn.cpu().numpy()
+    for f in range(4):
+        assert best[f] > 0
+        assert _recount(tr.frame(f), models[f], 0.02) == best[f]
+        assert drawn[f] == 3 * 128
+    tg = torch.from_numpy((best // 2).astype(np.int32)).cuda()
+    _, b2, d2 = ransac_preemptive(b, cand, coffs, w, 0.02, draws=128, max_rounds=3, seed=9,
+                                  targets=tg, ctx=gpu_ctx)
+    assert np.all(b2.cpu().numpy() >= best // 2)
+    d2 = d2.cpu().numpy()  # whole rounds, stopping at the round that reached the target
+    assert np.all((d2 % 128 == 0) & (d2 >= 128) & (d2 <= 384))
+
+
+@pytest.mark.gpu
 def test_trained_proposal_needs_fewer_hypotheses(gpu_ctx):
     """Trained on held-out scenes, the learned proposal reaches 99% of the
     plain 10k-hypothesis best count with fewer hypotheses than uniform
@@ -242,11 +267,14 @@ def test_trained_proposal_needs_fewer_hypotheses(gpu_ctx):
     _, best, _ = ransac_frames(be, 10_000, 0.02, ctx=gpu_ctx)
     tg = torch.ceil(best.double() * 0.99).to(torch.int32)
     _, bp, itp = ransac_frames(be, 10_000, 0.02, targets=tg, ctx=gpu_ctx)
-    lr = LearnedRansac(s)
+    lr = LearnedRansac(s, preemptive=False)
     cand, coffs = lr.prepare(be)
     _, bl, itl = lr.run(be, cand, coffs, 10_000, 0.02, targets=tg)
     reached = (bl >= tg).float().mean().item()
     assert reached >= 0.9
+    # the preemptive rounds reach the same targets
+    _, bp2, _ = LearnedRansac(s).run(be, cand, coffs, 10_000, 0.02, targets=tg)
+    assert (bp2 >= tg).float().mean().item() >= 0.9
     # typical scene: the median over scenes (a scene whose best plane the
     # proposal misses falls back to the hypothesis budget)
     assert itl.double().median().item() < itp.double().median().item()
