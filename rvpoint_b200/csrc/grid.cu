@@ -112,30 +112,56 @@ __global__ void k_bbox(const float *__restrict__ x, const float *__restrict__ y,
 
 // setInputCloud's padding and grid dimensions (spatial_hashing.cpp:141-150),
 // then (dense mode) each frame's first key.
-__global__ void k_grid_params(GridFrame *fr, const float *bb, int n_frames, float cell) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  u64 base = 0;
-  for (int f = 0; f < n_frames; ++f) {
-    const float *b = bb + 6 * f;
+// One block: a thread per frame computes its grid, then a block-wide
+// exclusive scan of the level-3 group counts gives each frame's key_base.
+__global__ __launch_bounds__(1024) void k_grid_params(GridFrame *fr, const float *bb,
+                                                      int n_frames, float cell) {
+  __shared__ u64 warp_sum[32];
+  __shared__ u64 carry;
+  if (blockIdx.x != 0) return;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) carry = 0;
+  __syncthreads();
+  for (int f0 = 0; f0 < n_frames; f0 += blockDim.x) {
+    const int f = f0 + tid;
     GridFrame g;
-    g.cell = cell;
-    if (b[0] > b[3]) {  // empty frame
-      g.min_x = g.min_y = g.min_z = 0.0f;
-      g.gx = g.gy = g.gz = 1;
-    } else {
-      const float eps = fmul(cell, 0.01f);
-      g.min_x = fsub(b[0], eps); g.min_y = fsub(b[1], eps); g.min_z = fsub(b[2], eps);
-      const float max_x = fadd(b[3], eps), max_y = fadd(b[4], eps), max_z = fadd(b[5], eps);
-      g.gx = (int)ceilf(fdiv(fsub(max_x, g.min_x), cell)) + 1;
-      g.gy = (int)ceilf(fdiv(fsub(max_y, g.min_y), cell)) + 1;
-      g.gz = (int)ceilf(fdiv(fsub(max_z, g.min_z), cell)) + 1;
+    u64 groups = 0;
+    if (f < n_frames) {
+      const float *b = bb + 6 * f;
+      g.cell = cell;
+      if (b[0] > b[3]) {  // empty frame
+        g.min_x = g.min_y = g.min_z = 0.0f;
+        g.gx = g.gy = g.gz = 1;
+      } else {
+        const float eps = fmul(cell, 0.01f);
+        g.min_x = fsub(b[0], eps); g.min_y = fsub(b[1], eps); g.min_z = fsub(b[2], eps);
+        const float max_x = fadd(b[3], eps), max_y = fadd(b[4], eps), max_z = fadd(b[5], eps);
+        g.gx = (int)ceilf(fdiv(fsub(max_x, g.min_x), cell)) + 1;
+        g.gy = (int)ceilf(fdiv(fsub(max_y, g.min_y), cell)) + 1;
+        g.gz = (int)ceilf(fdiv(fsub(max_z, g.min_z), cell)) + 1;
+      }
+      g.g3x = (g.gx + 63) >> 6;
+      g.g3y = (g.gy + 63) >> 6;
+      g.g3z = (g.gz + 63) >> 6;
+      groups = ((u64)g.g3x * (u64)g.g3y * (u64)g.g3z) << 18;
     }
-    g.g3x = (g.gx + 63) >> 6;
-    g.g3y = (g.gy + 63) >> 6;
-    g.g3z = (g.gz + 63) >> 6;
-    g.key_base = base;
-    base += ((u64)g.g3x * (u64)g.g3y * (u64)g.g3z) << 18;
-    fr[f] = g;
+    // inclusive scan of groups over the block
+    u64 v = groups;
+    for (int o = 1; o < 32; o <<= 1) {
+      const u64 t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_sum[wid] = v;
+    __syncthreads();
+    u64 before = carry;
+    for (int k = 0; k < wid; ++k) before += warp_sum[k];
+    if (f < n_frames) {
+      g.key_base = before + v - groups;
+      fr[f] = g;
+    }
+    __syncthreads();
+    if (tid == blockDim.x - 1) carry = before + v;
+    __syncthreads();
   }
 }
 
@@ -345,7 +371,7 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   RVP_LAUNCH_CHECK(ctx);
   k_bbox<<<gb, 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, bb);
   RVP_LAUNCH_CHECK(ctx);
-  k_grid_params<<<1, 32, 0, st>>>(frames, bb, n_frames, cell);
+  k_grid_params<<<1, 1024, 0, st>>>(frames, bb, n_frames, cell);
   RVP_LAUNCH_CHECK(ctx);
   k_cell_keys<<<gb, 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, frames, mode, p1, p2,
                                   g.b_keys.as<u64>(), g.b_vals.as<u32>());

@@ -566,7 +566,8 @@ rvp_status rvp_scorer_destroy(rvp_scorer *s) {
 namespace {
 rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const float *z,
                          const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
-                         float cell_size, const uint32_t *cand, size_t n_cand, float *features) {
+                         float cell_size, const uint32_t *cand, size_t n_cand, float *features,
+                         int lane_levels = 0) {
   rvp_context *ctx = s->ctx;
   return sguard(ctx, [&] {
     RVP_REQUIRE(x && y && z && frame_offsets_dev && features, "null pointer");
@@ -626,6 +627,7 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
     ta.rfac = 1.0f;
     ta.level0_warp = true;
     ta.preset_open = true;
+    ta.lane_levels = lane_levels;
     char *op = s->open.as<char>();
     ta.open_flags = reinterpret_cast<u32 *>(op); op += al256(N * 4);
     ta.open_pos = reinterpret_cast<u64 *>(op); op += al256(N * 8 + 8);
@@ -673,8 +675,9 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
   });
   if (st != RVP_OK) return st;
   const float *gx = s->cand_xyz.as<float>();
+  // sparse clouds: after one per-lane level the warp kernel is cheaper
   return features_impl(s, gx, gx + n_cand, gx + 2 * n_cand, cand_offsets_dev, n_frames, n_cand,
-                       cell_size, nullptr, n_cand, features);
+                       cell_size, nullptr, n_cand, features, 1);
 }
 
 
