@@ -353,6 +353,9 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     tn.vpy = c.vp_y;
     tn.vpz = c.vp_z;
     tn.level_events = p->level_events(1);
+    // the normals' open queries sit next to removed points, where rings are
+    // sparse: after one per-lane level the warp kernel is cheaper
+    tn.lane_levels = 1;
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
     // points whose SOR list holds kn kept points: normal straight from it;
     // the rest open for the kNN search
