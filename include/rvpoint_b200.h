@@ -159,6 +159,18 @@ RVP_API rvp_status rvp_extract_plane(rvp_context *ctx, const float *x, const flo
                              float *outliers_aos, size_t *n_inliers,
                              size_t *n_outliers);
 
+/* ---- Euclidean clustering: segmentation/euclidean_clustering.h:17-70 ---- */
+/* EuclideanClustering::extract (euclidean_clustering.cpp:113-189, without a
+ * neighbour searcher): the connected components of "squared distance <=
+ * tolerance^2", listed by their lowest index, each sorted ascending, kept
+ * when min_size <= size <= max_size. CSR output: offsets (capacity n + 1,
+ * n_clusters + 1 written) and indices (capacity n). */
+RVP_API rvp_status rvp_euclidean_clusters(rvp_context *ctx, const float *x, const float *y,
+                                          const float *z, size_t n, float tolerance,
+                                          int min_size, int max_size, int mem,
+                                          int64_t *offsets, int32_t *indices,
+                                          size_t *n_clusters);
+
 /* Largest cloud rvp_extract_plane_noalloc accepts. */
 #define RVP_NOALLOC_MAX_POINTS 16777216
 

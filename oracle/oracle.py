@@ -59,6 +59,16 @@ def _lib(path):
     return _libs[path]
 
 
+def _clusters(fn, c, tolerance, min_size, max_size):
+    x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+    n = x.shape[0]
+    offs = np.zeros(n + 1, np.int64)
+    idx = np.zeros(max(n, 1), np.int32)
+    k = fn(xp, yp, zp, n, tolerance, int(min_size), int(max_size), _ptr(offs, _lp),
+           _ptr(idx, _ip))
+    return [idx[offs[i]:offs[i + 1]].copy() for i in range(k)]
+
+
 def reference_available() -> bool:
     return os.path.exists(REFERENCE_SO)
 
@@ -93,6 +103,9 @@ class Restatement:
         L.rvo_extract_plane.restype = None
         L.rvo_extract_plane.argtypes = [_fp, _fp, _fp, _sz, _fp, C.c_float, _fp, _fp,
                                         C.POINTER(_sz), C.POINTER(_sz)]
+        L.rvo_euclidean_clusters.restype = C.c_long
+        L.rvo_euclidean_clusters.argtypes = [_fp, _fp, _fp, _sz, C.c_float, C.c_int, C.c_int,
+                                             _lp, _ip]
         L.rvo_normals_knn_exact_f64.restype = None
         L.rvo_normals_knn_exact_f64.argtypes = [_fp, _fp, _fp, _sz, _ip, C.c_int, C.c_float,
                                                 C.c_float, C.c_float, _dp, _dp, _dp, _dp]
@@ -175,6 +188,10 @@ class Restatement:
                                  _ptr(b, _fp), C.byref(ni), C.byref(no))
         return a[: ni.value].copy(), b[: no.value].copy()
 
+    def euclidean_clusters(self, c, tolerance, min_size=1, max_size=2**31 - 1):
+        """List of sorted index arrays, in the reference's cluster order."""
+        return _clusters(self.L.rvo_euclidean_clusters, c, tolerance, min_size, max_size)
+
     def normals_exact_f64(self, c, nbr_idx, vp=(0, 0, 0)):
         x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
         nbr = np.ascontiguousarray(nbr_idx, np.int32)
@@ -215,6 +232,9 @@ class Reference:
                                         C.POINTER(_sz), C.POINTER(_sz)]
         L.ref_count_plane_inliers.restype = _sz
         L.ref_count_plane_inliers.argtypes = [_fp, _fp, _fp, _sz, _fp, C.c_float, _fp]
+        L.ref_euclidean_clusters.restype = C.c_long
+        L.ref_euclidean_clusters.argtypes = [_fp, _fp, _fp, _sz, C.c_float, C.c_int, C.c_int,
+                                             _lp, _ip]
         L.ref_rand_stream.restype = None
         L.ref_rand_stream.argtypes = [C.c_uint, C.c_int, _ip]
 
@@ -275,6 +295,9 @@ class Reference:
         best = self.L.ref_ransac_plane(xp, yp, zp, x.shape[0], thresh, max_iters, collinear,
                                        prob, _ptr(model, _fp))
         return best, model
+
+    def euclidean_clusters(self, c, tolerance, min_size=1, max_size=2**31 - 1):
+        return _clusters(self.L.ref_euclidean_clusters, c, tolerance, min_size, max_size)
 
     def extract_plane(self, c, model, thresh):
         x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)

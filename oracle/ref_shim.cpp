@@ -14,6 +14,7 @@
 #include "filters/statistical_outlier_removal.h"
 #include "features/normal_estimation.h"
 #include "segmentation/ransac_plane.h"
+#include "segmentation/euclidean_clustering.h"
 
 #include <cstdint>
 #include <cstdlib>
@@ -142,6 +143,28 @@ size_t ref_count_plane_inliers(const float *x, const float *y, const float *z,
                                float *scratch_aos) {
   return extract_plane_inliers_rvv(soa(x, y, z, n), model, thresh,
                                    reinterpret_cast<PointXYZ *>(scratch_aos));
+}
+
+// EuclideanClustering::extract (euclidean_clustering.cpp:113-189) without a
+// neighbour searcher. CSR output: offsets[n_clusters+1] and indices; returns
+// the number of clusters (offsets / indices sized by the caller: n + 1, n).
+long ref_euclidean_clusters(const float *x, const float *y, const float *z, size_t n,
+                            float tolerance, int min_size, int max_size, long long *offsets,
+                            int *indices) {
+  const PointCloudSoA c = soa(x, y, z, n);
+  EuclideanClustering ec;
+  ec.setInputCloud(c);
+  ec.setClusterTolerance(tolerance);
+  ec.setMinClusterSize(min_size);
+  ec.setMaxClusterSize(max_size);
+  const std::vector<ClusterIndices> cl = ec.extract();
+  long long o = 0;
+  offsets[0] = 0;
+  for (size_t k = 0; k < cl.size(); ++k) {
+    for (int i : cl[k].indices) indices[o++] = i;
+    offsets[k + 1] = o;
+  }
+  return (long)cl.size();
 }
 
 // Raw glibc rand() stream after srand(seed): the hypothesis source of

@@ -785,3 +785,55 @@ void rvo_extract_plane(const float *x, const float *y, const float *z,
   *n_in = ni;
   *n_out = no;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Euclidean clustering                                                     */
+/* ------------------------------------------------------------------------ */
+static int cmp_int(const void *a, const void *b) {
+  const int x = *(const int *)a, y = *(const int *)b;
+  return (x > y) - (x < y);
+}
+
+/* euclidean_clustering.cpp:113-189 with radiusQueryUnvisited's scalar branch
+ * (:88-98): neighbours of the current point are the unvisited points with
+ * ((px - qx)^2 + (py - qy)^2) + (pz - qz)^2 <= tol^2, in index order, pushed
+ * to a FIFO queue; a cluster is every point the BFS from a seed reaches. */
+long rvo_euclidean_clusters(const float *x, const float *y, const float *z, size_t n,
+                            float tolerance, int min_size, int max_size, long long *offsets,
+                            int *indices) {
+  const float tol_sq = tolerance * tolerance;
+  unsigned char *visited = calloc(n ? n : 1, 1);
+  int *queue = malloc(sizeof(int) * (n ? n : 1));
+  long n_cl = 0;
+  long long o = 0;
+  offsets[0] = 0;
+  for (size_t seed = 0; seed < n; ++seed) {
+    if (visited[seed]) continue;
+    size_t head = 0, tail = 0;
+    visited[seed] = 1;
+    queue[tail++] = (int)seed;
+    while (head < tail) {
+      const int cur = queue[head++];
+      const float qx = x[cur], qy = y[cur], qz = z[cur];
+      for (size_t i = 0; i < n; ++i) {
+        if (visited[i]) continue;
+        const float dx = x[i] - qx, dy = y[i] - qy, dz = z[i] - qz;
+        if (dx * dx + dy * dy + dz * dz <= tol_sq) {
+          visited[i] = 1;
+          queue[tail++] = (int)i;
+        }
+      }
+    }
+    /* the BFS order (queue[0..tail)) is the cluster's membership */
+    const int sz = (int)tail;
+    if (sz >= min_size && sz <= max_size) {
+      memcpy(indices + o, queue, sizeof(int) * tail);
+      qsort(indices + o, tail, sizeof(int), cmp_int);
+      o += (long long)tail;
+      offsets[++n_cl] = o;
+    }
+  }
+  free(visited);
+  free(queue);
+  return n_cl;
+}

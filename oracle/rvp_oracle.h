@@ -81,6 +81,15 @@ void rvo_normals_knn_exact_f64(const float *x, const float *y, const float *z,
                                float vpy, float vpz, double *nx, double *ny,
                                double *nz, double *cond);
 
+/* EuclideanClustering::extract without a searcher
+ * (segmentation/euclidean_clustering.cpp:113-189): BFS from the lowest
+ * unvisited index over points with squared distance <= tolerance^2,
+ * clusters kept when min_size <= size <= max_size, each sorted. CSR output
+ * (offsets n + 1, indices n); returns the number of clusters. */
+long rvo_euclidean_clusters(const float *x, const float *y, const float *z, size_t n,
+                            float tolerance, int min_size, int max_size, long long *offsets,
+                            int *indices);
+
 #ifdef __cplusplus
 }
 #endif

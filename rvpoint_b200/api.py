@@ -456,6 +456,58 @@ def extract_plane_outliers_rvv(cloud, model, dist_thresh: float, ctx=None):
 # ---------------------------------------------------------------------------
 # batched frames
 # ---------------------------------------------------------------------------
+def euclidean_clusters(cloud, tolerance: float, min_size: int = 1,
+                       max_size: int = 2**31 - 1, ctx: Optional[Context] = None):
+    """EuclideanClustering::extract (segmentation/euclidean_clustering.cpp
+    :113-189): list of sorted index arrays, by lowest index."""
+    ctx = ctx or default_context()
+    x, y, z = _xyz(cloud)
+    mem = _mem_of(x, y, z)
+    _prep(ctx, mem)
+    n = int(x.shape[0])
+    dev = mem == MEM_DEVICE
+    device = x.device if dev else None
+    offs = _empty((n + 1,), np.int64, dev, device)
+    idx = _empty((max(n, 1),), np.int32, dev, device)
+    k = C.c_size_t(0)
+    check(ctx.L.rvp_euclidean_clusters(ctx.h, _ptr(x), _ptr(y), _ptr(z), n, float(tolerance),
+                                       int(min_size), int(max_size), mem, _ptr(offs), _ptr(idx),
+                                       C.byref(k)), ctx.h)
+    k = int(k.value)
+    if dev:
+        offs, idx = offs.cpu().numpy(), idx.cpu().numpy()
+    return [idx[offs[i]:offs[i + 1]].copy() for i in range(k)]
+
+
+class EuclideanClustering:
+    """segmentation/euclidean_clustering.h:17-70 (no neighbour searcher)."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx
+        self.cloud = None
+        self.tolerance = 0.05
+        self.min_size = 1
+        self.max_size = 2**31 - 1
+
+    def setInputCloud(self, cloud):
+        self.cloud = cloud
+
+    def setClusterTolerance(self, tolerance: float):
+        self.tolerance = float(tolerance)
+
+    def setMinClusterSize(self, n: int):
+        self.min_size = int(n)
+
+    def setMaxClusterSize(self, n: int):
+        self.max_size = int(n)
+
+    def extract(self):
+        if self.cloud is None:
+            return []
+        return euclidean_clusters(self.cloud, self.tolerance, self.min_size, self.max_size,
+                                  ctx=self.ctx)
+
+
 class Pipeline:
     """voxel -> SOR -> normals(k+1 NN) -> RANSAC over many frames at once."""
 

@@ -896,6 +896,56 @@ rvp_status rvp_ransac_plane(rvp_context *ctx, const float *x, const float *y, co
   });
 }
 
+// ===========================================================================
+// Euclidean clustering
+// ===========================================================================
+rvp_status rvp_euclidean_clusters(rvp_context *ctx, const float *x, const float *y,
+                                  const float *z, size_t n, float tolerance, int min_size,
+                                  int max_size, int mem, int64_t *offsets, int32_t *indices,
+                                  size_t *n_clusters) {
+  if (!ctx) return RVP_ERR_INVALID_ARG;
+  return guard(ctx, [&] {
+    RVP_REQUIRE(offsets && n_clusters, "offsets / n_clusters required");
+    *n_clusters = 0;
+    if (n == 0) {  // euclidean_clustering.cpp:116-118
+      if (mem == RVP_MEM_DEVICE) {
+        set_device(ctx);
+        RVP_CUDA_TRY(cudaMemsetAsync(offsets, 0, 8, ctx->stream));
+        sync(ctx);
+      } else {
+        offsets[0] = 0;
+      }
+      return;
+    }
+    RVP_REQUIRE(x && y && z && indices, "null pointer");
+    RVP_REQUIRE(tolerance > 0.0f, "tolerance must be > 0");
+    RVP_REQUIRE(n < 0x7FFFFFFFull, "clouds are limited to 2^31 - 1 points");
+    set_device(ctx);
+    const float *dx = in_dev(ctx, 1, x, n, mem);
+    const float *dy = in_dev(ctx, 2, y, n, mem);
+    const float *dz = in_dev(ctx, 3, z, n, mem);
+    int64_t *doffs = out_dev(ctx, 4, offsets, n + 1, mem);
+    int32_t *didx = out_dev(ctx, 5, indices, n, mem);
+    int64_t *fo = single_frame_offsets(ctx, 6, n);
+    u64 *dcount = static_cast<u64 *>(scratch(ctx, 7, 64));
+    rvp::euclidean_clusters_run(ctx, ctx_grid(ctx), dx, dy, dz, n, fo, tolerance, min_size,
+                                max_size, doffs, didx, dcount,
+                                scratch(ctx, 8, rvp::euclidean_temp_bytes(n)));
+    u64 k = 0;
+    RVP_CUDA_TRY(cudaMemcpyAsync(&k, dcount, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    *n_clusters = (size_t)k;
+    if (mem != RVP_MEM_DEVICE) {
+      out_copy(ctx, offsets, doffs, (size_t)k + 1, mem);
+      int64_t total = 0;
+      RVP_CUDA_TRY(cudaMemcpyAsync(&total, doffs + k, 8, cudaMemcpyDeviceToHost, ctx->stream));
+      sync(ctx);
+      out_copy(ctx, indices, didx, (size_t)total, mem);
+      sync(ctx);
+    }
+  });
+}
+
 rvp_status rvp_extract_plane(rvp_context *ctx, const float *x, const float *y, const float *z,
                              size_t n, const float *model, float dist_thresh, int mem,
                              float *inliers_aos, float *outliers_aos, size_t *n_inliers,

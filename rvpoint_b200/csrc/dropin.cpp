@@ -25,6 +25,7 @@
 #include "rvpoint/filters/voxel_grid.h"
 #include "rvpoint/search/spatial_hashing.h"
 #include "rvpoint/segmentation/ransac_plane.h"
+#include "rvpoint/segmentation/euclidean_clustering.h"
 
 namespace {
 
@@ -270,6 +271,32 @@ void extract_plane_inliers_outliers_rvv(const PointCloudSoA &cloud, const float 
                                         PointXYZ *outliers, std::size_t &n_inliers,
                                         std::size_t &n_outliers) {
   extract(cloud, model, dist_thresh, inliers, outliers, n_inliers, n_outliers);
+}
+
+// ---- Euclidean clustering (euclidean_clustering.cpp) -----------------------
+void EuclideanClustering::setInputCloud(const PointCloudSoA &cloud) { cloud_ = &cloud; }
+void EuclideanClustering::setClusterTolerance(float tolerance) { clusterTolerance_ = tolerance; }
+void EuclideanClustering::setMinClusterSize(int min_size) { minClusterSize_ = min_size; }
+void EuclideanClustering::setMaxClusterSize(int max_size) { maxClusterSize_ = max_size; }
+
+std::vector<ClusterIndices> EuclideanClustering::extract() const {
+  std::vector<ClusterIndices> result;
+  if (!cloud_ || cloud_->n == 0) return result;
+  const std::size_t n = cloud_->n;
+  std::vector<int64_t> offs(n + 1);
+  std::vector<int32_t> idx(n);
+  size_t k = 0;
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!ok(rvp_euclidean_clusters(ctx(), cloud_->x, cloud_->y, cloud_->z, n, clusterTolerance_,
+                                   minClusterSize_, maxClusterSize_, RVP_MEM_HOST, offs.data(),
+                                   idx.data(), &k)))
+      return result;
+  }
+  result.resize(k);
+  for (size_t c = 0; c < k; ++c)
+    result[c].indices.assign(idx.begin() + offs[c], idx.begin() + offs[c + 1]);
+  return result;
 }
 
 }  // namespace rvpoint

@@ -398,6 +398,15 @@ void ransac_frames(rvp_context *ctx, const float *x, const float *y,
                    float *model, int32_t *best, int32_t *iters_run,
                    int32_t *counts_all, bool eval_all,
                    const RansacSampler &smp = RansacSampler{}, int cluster = 1);
+// Euclidean clusters of one cloud (cluster.cu): CSR offsets (capacity
+// n + 1) and indices (capacity n) on the device, count in n_clusters_dev.
+// temp: euclidean_temp_bytes(n). Synchronizes.
+size_t euclidean_temp_bytes(size_t n);
+void euclidean_clusters_run(rvp_context *ctx, Grid &grid, const float *x, const float *y,
+                            const float *z, size_t n, const int64_t *offs_dev, float tolerance,
+                            int min_size, int max_size, int64_t *offsets, int32_t *indices,
+                            u64 *n_clusters_dev, void *temp);
+
 // Weighted proposal with preemptive rounds: each round draws `draws`
 // hypotheses per frame, ranks them by their inliers among the frame's
 // candidates and counts the best 32 exactly over all points (strict-greater

@@ -14,6 +14,7 @@
 #include "filters/statistical_outlier_removal.h"
 #include "filters/voxel_grid.h"
 #include "search/spatial_hashing.h"
+#include "segmentation/euclidean_clustering.h"
 #include "segmentation/ransac_plane.h"
 
 using namespace rvpoint;
@@ -113,6 +114,20 @@ int main(int argc, char **argv) {
   extract_plane_inliers_outliers_rvv(sc, model, 0.01f, pin.data(), pout.data(), ni, no);
   put(reinterpret_cast<float *>(pin.data()), 3 * ni);
   put(reinterpret_cast<float *>(pout.data()), 3 * no);
+  // Euclidean clusters of the SOR output
+  EuclideanClustering ec;
+  ec.setInputCloud(sc);
+  ec.setClusterTolerance(0.08f);
+  ec.setMinClusterSize(2);
+  const std::vector<ClusterIndices> cl = ec.extract();
+  std::vector<int64_t> coffs{0};
+  std::vector<int> cidx;
+  for (const auto &c : cl) {
+    cidx.insert(cidx.end(), c.indices.begin(), c.indices.end());
+    coffs.push_back((int64_t)cidx.size());
+  }
+  put(coffs.data(), coffs.size());
+  put(cidx.data(), cidx.size());
   // degenerate inputs return 0 as in the reference
   PointCloudSoA empty{};
   float m0[4] = {9, 9, 9, 9};

@@ -58,6 +58,11 @@ def main():
         out[f"ransac_{name}_best"] = np.array([best], np.int32)
         out[f"ransac_{name}_model"] = model
     out["rand_stream_3000"] = R.rand_stream(3000)
+    # Euclidean clustering (euclidean_clustering.cpp:113-189), CSR
+    for name, c, tol, mn, mx in [("room", room, 0.02, 3, 100000), ("lidar", lid, 0.5, 1, 200)]:
+        cl = R.euclidean_clusters(c, tol, mn, mx)
+        out[f"ec_{name}_offsets"] = np.cumsum([0] + [len(k) for k in cl]).astype(np.int64)
+        out[f"ec_{name}_idx"] = (np.concatenate(cl) if cl else np.zeros(0)).astype(np.int32)
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
     print("wrote", os.path.join(HERE, "golden.npz"), len(out), "arrays")
 

@@ -70,9 +70,9 @@ def test_dropin_chain_matches_oracle(tmp_path, restatement):
     assert r.returncode == 0, r.stderr
     f32, i32, i64 = np.float32, np.int32, np.int64
     (vox, vox_sc, sor, sor2, counts, idx, d2, nx, ny, nz, kx, ky, kz, filt, rb, model,
-     best_sc, model_sc, pin, pout, degen) = _arrays(
+     best_sc, model_sc, pin, pout, coffs, cidx, degen) = _arrays(
         outp.read_bytes(), [f32, f32, f32, f32, i64, i32, f32, f32, f32, f32, f32, f32, f32,
-                            f32, i32, f32, i32, f32, f32, f32, i64])
+                            f32, i32, f32, i32, f32, f32, f32, i64, i32, i64])
     bits = lambda a: np.ascontiguousarray(a, np.float32).view(np.int32)  # noqa: E731
     v, _ = restatement.voxel_grid(c, 0.05)
     assert np.array_equal(bits(vox), bits(v.ravel()))
@@ -113,4 +113,7 @@ def test_dropin_chain_matches_oracle(tmp_path, restatement):
     a, b = restatement.extract_plane(sc, m, 0.01)
     assert np.array_equal(bits(pin), bits(a.ravel()))
     assert np.array_equal(bits(pout), bits(b.ravel()))
+    cl = restatement.euclidean_clusters(sc, 0.08, 2)
+    assert np.array_equal(coffs, np.cumsum([0] + [len(k) for k in cl]))
+    assert np.array_equal(cidx, np.concatenate(cl))
     assert list(degen) == [0, 0, 1]

@@ -476,3 +476,41 @@ def test_pipeline_lane_levels_do_not_change_results(gpu_ctx):
         assert np.array_equal(bits(o["sor"]), bits(outs[0]["sor"]))
         assert np.array_equal(bits(o["normals"]), bits(outs[0]["normals"]))
         assert np.array_equal(o["ransac_count"], outs[0]["ransac_count"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("src,tol,mn,mx", [("room", 0.02, 3, 100000), ("lidar", 0.5, 1, 200)])
+def test_euclidean_clusters_match_golden(gpu_ctx, src, tol, mn, mx):
+    """EuclideanClustering::extract: the same clusters, in the same order,
+    with the same sorted indices as the reference (golden fixtures)."""
+    import os
+    from rvpoint_b200 import api
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden.npz"))
+    a = g[src]
+    c = D.Cloud(np.ascontiguousarray(a[:, 0]), np.ascontiguousarray(a[:, 1]),
+                np.ascontiguousarray(a[:, 2]))
+    cl = api.euclidean_clusters(c, tol, mn, mx, ctx=gpu_ctx)
+    offs = np.cumsum([0] + [len(k) for k in cl]).astype(np.int64)
+    assert np.array_equal(offs, g[f"ec_{src}_offsets"])
+    assert np.array_equal(np.concatenate(cl).astype(np.int32), g[f"ec_{src}_idx"])
+
+
+@pytest.mark.gpu
+def test_euclidean_clusters_match_oracle_larger(gpu_ctx, restatement):
+    from rvpoint_b200 import api
+    fr = D.lidar_frame(seed=777)
+    c = fr.subset(np.arange(0, fr.n, 5))
+    for tol, mn, mx in ((0.3, 1, 2**31 - 1), (0.6, 5, 5000), (0.05, 1, 3)):
+        got = api.euclidean_clusters(c, tol, mn, mx, ctx=gpu_ctx)
+        ref = restatement.euclidean_clusters(c, tol, mn, mx)
+        assert len(got) == len(ref)
+        for u, v in zip(got, ref):
+            assert np.array_equal(u, v)
+    # device arrays in place; empty cloud
+    import torch
+    xs = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (c.x, c.y, c.z)]
+    got = api.euclidean_clusters(tuple(xs), 0.3, ctx=gpu_ctx)
+    ref = restatement.euclidean_clusters(c, 0.3)
+    assert len(got) == len(ref) and all(np.array_equal(u, v) for u, v in zip(got, ref))
+    e = np.zeros(0, np.float32)
+    assert api.euclidean_clusters((e, e, e), 0.3, ctx=gpu_ctx) == []

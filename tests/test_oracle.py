@@ -144,3 +144,13 @@ def test_reference_lidar_frame(reference, restatement):
     vc = cloud(v1)
     s1, _, _ = restatement.sor_exact(vc, 16, 1.0)
     assert np.array_equal(bits(s1), bits(reference.sor_rvv(vc, 16, 1.0)))
+
+
+@pytest.mark.parametrize("name,src,tol,mn,mx", [("room", "room", 0.02, 3, 100000),
+                                                ("lidar", "lidar", 0.5, 1, 200)])
+def test_golden_euclidean_clusters(golden, restatement, name, src, tol, mn, mx):
+    cl = restatement.euclidean_clusters(cloud(golden[src]), tol, mn, mx)
+    offs = np.cumsum([0] + [len(k) for k in cl]).astype(np.int64)
+    assert np.array_equal(offs, golden[f"ec_{name}_offsets"])
+    idx = np.concatenate(cl).astype(np.int32) if cl else np.zeros(0, np.int32)
+    assert np.array_equal(idx, golden[f"ec_{name}_idx"])
