@@ -171,6 +171,14 @@ RVP_API rvp_status rvp_euclidean_clusters(rvp_context *ctx, const float *x, cons
                                           int64_t *offsets, int32_t *indices,
                                           size_t *n_clusters);
 
+/* ---- PCD input: io/simple_pcd_loader.h:143-291 ---------------------------- */
+/* loadPCD's parsing (ascii, binary, binary_compressed) into SoA x, y, z
+ * (device arrays with mem = RVP_MEM_DEVICE: binary records are split on the
+ * GPU). *n_points receives the point count; when it exceeds capacity the
+ * call returns RVP_ERR_CAPACITY and writes nothing. Synchronizes. */
+RVP_API rvp_status rvp_pcd_load(rvp_context *ctx, const char *path, int mem, float *x,
+                                float *y, float *z, size_t capacity, size_t *n_points);
+
 /* Largest cloud rvp_extract_plane_noalloc accepts. */
 #define RVP_NOALLOC_MAX_POINTS 16777216
 

@@ -232,6 +232,12 @@ class Reference:
                                         C.POINTER(_sz), C.POINTER(_sz)]
         L.ref_count_plane_inliers.restype = _sz
         L.ref_count_plane_inliers.argtypes = [_fp, _fp, _fp, _sz, _fp, C.c_float, _fp]
+        L.ref_load_pcd.restype = C.c_long
+        L.ref_load_pcd.argtypes = [C.c_char_p, _fp, _sz]
+        L.ref_save_pcd.restype = None
+        L.ref_save_pcd.argtypes = [C.c_char_p, _fp, _sz, C.c_int]
+        L.ref_save_pcd_rgb.restype = None
+        L.ref_save_pcd_rgb.argtypes = [C.c_char_p, _fp, C.POINTER(C.c_ubyte), _sz, C.c_int]
         L.ref_euclidean_clusters.restype = C.c_long
         L.ref_euclidean_clusters.argtypes = [_fp, _fp, _fp, _sz, C.c_float, C.c_int, C.c_int,
                                              _lp, _ip]
@@ -295,6 +301,20 @@ class Reference:
         best = self.L.ref_ransac_plane(xp, yp, zp, x.shape[0], thresh, max_iters, collinear,
                                        prob, _ptr(model, _fp))
         return best, model
+
+    def save_pcd(self, path, xyz, binary, rgb=None):
+        a = np.ascontiguousarray(xyz, np.float32)
+        if rgb is None:
+            self.L.ref_save_pcd(path.encode(), _ptr(a, _fp), a.shape[0], int(binary))
+        else:
+            c = np.ascontiguousarray(rgb, np.uint8)
+            self.L.ref_save_pcd_rgb(path.encode(), _ptr(a, _fp), _ptr(c, C.POINTER(C.c_ubyte)),
+                                    a.shape[0], int(binary))
+
+    def load_pcd(self, path, cap):
+        out = np.zeros((max(cap, 1), 3), np.float32)
+        k = self.L.ref_load_pcd(path.encode(), _ptr(out, _fp), cap)
+        return out[:max(k, 0)].copy() if k >= 0 else None
 
     def euclidean_clusters(self, c, tolerance, min_size=1, max_size=2**31 - 1):
         return _clusters(self.L.ref_euclidean_clusters, c, tolerance, min_size, max_size)

@@ -15,6 +15,7 @@
 #include "features/normal_estimation.h"
 #include "segmentation/ransac_plane.h"
 #include "segmentation/euclidean_clustering.h"
+#include "io/simple_pcd_loader.h"
 
 #include <cstdint>
 #include <cstdlib>
@@ -165,6 +166,36 @@ long ref_euclidean_clusters(const float *x, const float *y, const float *z, size
     offsets[k + 1] = o;
   }
   return (long)cl.size();
+}
+
+// loadPCD (io/simple_pcd_loader.h:143-291): AoS points into out (capacity
+// cap); returns the reference's count (-1 on failure).
+long ref_load_pcd(const char *path, float *out, size_t cap) {
+  std::vector<PointXYZ> pts;
+  const int k = loadPCD(path, pts);
+  if (k < 0) return k;
+  for (size_t i = 0; i < pts.size() && i < cap; ++i) {
+    out[3 * i + 0] = pts[i].x;
+    out[3 * i + 1] = pts[i].y;
+    out[3 * i + 2] = pts[i].z;
+  }
+  return (long)pts.size();
+}
+
+// savePCD / savePCDRGB (io/simple_pcd_loader.h:295-386)
+void ref_save_pcd(const char *path, const float *aos, size_t n, int binary) {
+  std::vector<PointXYZ> pts(n);
+  for (size_t i = 0; i < n; ++i) pts[i] = {aos[3 * i], aos[3 * i + 1], aos[3 * i + 2]};
+  savePCD(path, pts, binary != 0);
+}
+
+void ref_save_pcd_rgb(const char *path, const float *aos, const unsigned char *rgb, size_t n,
+                      int binary) {
+  std::vector<PointXYZRGB> pts(n);
+  for (size_t i = 0; i < n; ++i)
+    pts[i] = {aos[3 * i], aos[3 * i + 1], aos[3 * i + 2], rgb[3 * i], rgb[3 * i + 1],
+              rgb[3 * i + 2]};
+  savePCDRGB(path, pts, binary != 0);
 }
 
 // Raw glibc rand() stream after srand(seed): the hypothesis source of

@@ -104,6 +104,7 @@ SIGNATURES = {
                                 P, P]),
     "rvp_plane_labels": (I, [P, P, P, P, P, I, SZ, P, F, P]),
     "rvp_euclidean_clusters": (I, [P, P, P, P, SZ, F, I, I, I, P, P, C.POINTER(SZ)]),
+    "rvp_pcd_load": (I, [P, C.c_char_p, I, P, P, P, SZ, C.POINTER(SZ)]),
     "rvp_ransac_preemptive": (I, [P, P, P, P, P, I, P, P, SZ, P, F, C.c_uint64, I, I, F, F, P, P,
                                   P, P]),
     "rvp_scorer_create": (I, [P, SZ, I, C.POINTER(P)]),

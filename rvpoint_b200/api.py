@@ -479,6 +479,25 @@ def euclidean_clusters(cloud, tolerance: float, min_size: int = 1,
     return [idx[offs[i]:offs[i + 1]].copy() for i in range(k)]
 
 
+def load_pcd(path: str, device: bool = False, ctx: Optional[Context] = None):
+    """io/simple_pcd_loader.h loadPCD: (x, y, z) float32 arrays (CUDA tensors
+    with device=True)."""
+    ctx = ctx or default_context()
+    n = C.c_size_t(0)
+    st = ctx.L.rvp_pcd_load(ctx.h, path.encode(), MEM_HOST, None, None, None, 0, C.byref(n))
+    if st not in (_lib.RVP_OK, _lib.RVP_ERR_CAPACITY):
+        check(st, ctx.h)
+    cap = int(n.value)
+    mem = MEM_DEVICE if device else MEM_HOST
+    _prep(ctx, mem)
+    x, y, z = (_empty((max(cap, 1),), np.float32, device, torch.device("cuda", ctx.device)
+                      if device else None) for _ in range(3))
+    check(ctx.L.rvp_pcd_load(ctx.h, path.encode(), mem, _ptr(x), _ptr(y), _ptr(z), max(cap, 1),
+                             C.byref(n)), ctx.h)
+    k = int(n.value)
+    return x[:k], y[:k], z[:k]
+
+
 class EuclideanClustering:
     """segmentation/euclidean_clustering.h:17-70 (no neighbour searcher)."""
 

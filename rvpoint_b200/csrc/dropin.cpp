@@ -10,6 +10,9 @@
 // GPU itself throws std::runtime_error with the library's message (the
 // reference cannot fail that way, and a silent 0 would hide it).
 #include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
 #include <mutex>
 #include <new>
 #include <stdexcept>
@@ -23,6 +26,7 @@
 #include "rvpoint/features/normal_estimation.h"
 #include "rvpoint/filters/statistical_outlier_removal.h"
 #include "rvpoint/filters/voxel_grid.h"
+#include "rvpoint/io/simple_pcd_loader.h"
 #include "rvpoint/search/spatial_hashing.h"
 #include "rvpoint/segmentation/ransac_plane.h"
 #include "rvpoint/segmentation/euclidean_clustering.h"
@@ -297,6 +301,81 @@ std::vector<ClusterIndices> EuclideanClustering::extract() const {
   for (size_t c = 0; c < k; ++c)
     result[c].indices.assign(idx.begin() + offs[c], idx.begin() + offs[c + 1]);
   return result;
+}
+
+// ---- PCD files (io/simple_pcd_loader.h) -----------------------------------
+int loadPCD(const std::string &file_path, std::vector<PointXYZ> &points) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  rvp_context *c = ctx();
+  size_t n = 0;
+  // first the count (binary files: from the header alone), then the points
+  rvp_status s = rvp_pcd_load(c, file_path.c_str(), RVP_MEM_HOST, nullptr, nullptr, nullptr,
+                              0, &n);
+  if (s == RVP_ERR_CAPACITY) {
+    std::vector<float> x(n), y(n), z(n);
+    s = rvp_pcd_load(c, file_path.c_str(), RVP_MEM_HOST, x.data(), y.data(), z.data(), n, &n);
+    if (s == RVP_OK) {
+      points.resize(n);
+      for (size_t i = 0; i < n; ++i) points[i] = {x[i], y[i], z[i]};
+    }
+  } else if (s == RVP_OK) {
+    points.clear();  // an ascii file without a readable point line
+  }
+  if (s == RVP_OK) return static_cast<int>(points.size());
+  if (s == RVP_ERR_OOM) throw std::bad_alloc();
+  std::cerr << "Error: " << rvp_last_error(c) << std::endl;
+  return -1;
+}
+
+namespace {
+
+bool pcd_head(std::ofstream &f, const std::string &name, size_t n, bool rgb, bool binary) {
+  if (!f.is_open()) {
+    std::cerr << "Error: Could not open file " << name << " for writing." << std::endl;
+    return false;
+  }
+  f << "# .PCD v.7 - Point Cloud Data file format\nVERSION .7\n"
+    << (rgb ? "FIELDS x y z rgb\nSIZE 4 4 4 4\nTYPE F F F F\nCOUNT 1 1 1 1\n"
+            : "FIELDS x y z\nSIZE 4 4 4\nTYPE F F F\nCOUNT 1 1 1\n")
+    << "WIDTH " << n << "\nHEIGHT 1\nVIEWPOINT 0 0 0 1 0 0 0\nPOINTS " << n << "\nDATA "
+    << (binary ? "binary" : "ascii") << "\n";
+  return true;
+}
+
+}  // namespace
+
+void savePCD(const std::string &filename, const std::vector<PointXYZ> &points, bool binary) {
+  std::ofstream f(filename, binary ? (std::ios::binary | std::ios::out) : std::ios::out);
+  if (!pcd_head(f, filename, points.size(), false, binary)) return;
+  if (binary) {
+    if (!points.empty())
+      f.write(reinterpret_cast<const char *>(points.data()),
+              static_cast<std::streamsize>(points.size() * sizeof(PointXYZ)));
+  } else {
+    for (const PointXYZ &p : points) f << p.x << " " << p.y << " " << p.z << "\n";
+  }
+  f.close();
+  std::cout << "Saved " << points.size() << " points to " << filename << std::endl;
+}
+
+void savePCDRGB(const std::string &filename, const std::vector<PointXYZRGB> &points,
+                bool binary) {
+  std::ofstream f(filename, binary ? (std::ios::binary | std::ios::out) : std::ios::out);
+  if (!pcd_head(f, filename, points.size(), true, binary)) return;
+  for (const PointXYZRGB &p : points) {
+    // packed 0x00RRGGBB, stored as the bits of a float
+    const std::uint32_t bits = (std::uint32_t(p.r) << 16) | (std::uint32_t(p.g) << 8) | p.b;
+    float rgb;
+    std::memcpy(&rgb, &bits, 4);
+    if (binary) {
+      const float rec[4] = {p.x, p.y, p.z, rgb};
+      f.write(reinterpret_cast<const char *>(rec), sizeof rec);
+    } else {
+      f << p.x << " " << p.y << " " << p.z << " " << rgb << "\n";
+    }
+  }
+  f.close();
+  std::cout << "Saved " << points.size() << " colored points to " << filename << std::endl;
 }
 
 }  // namespace rvpoint
