@@ -106,6 +106,23 @@ class Restatement:
         L.rvo_euclidean_clusters.restype = C.c_long
         L.rvo_euclidean_clusters.argtypes = [_fp, _fp, _fp, _sz, C.c_float, C.c_int, C.c_int,
                                              _lp, _ip]
+        L.rvo_octree_order.restype = None
+        L.rvo_octree_order.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int,
+                                       C.c_float, _ip]
+        L.rvo_octree_radius_search.restype = C.c_longlong
+        L.rvo_octree_radius_search.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int,
+                                               C.c_float, _fp, _fp, _fp, _sz, C.c_float, _lp,
+                                               _ip, _fp, C.c_longlong]
+        L.rvo_nth_element.restype = C.c_int
+        L.rvo_nth_element.argtypes = [_fp, _sz, _sz]
+        L.rvo_sor_octree.restype = _sz
+        L.rvo_sor_octree.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int, C.c_float,
+                                     C.c_int, C.c_float, C.c_float, _fp, _fp,
+                                     C.POINTER(C.c_ubyte)]
+        L.rvo_normals_octree.restype = None
+        L.rvo_normals_octree.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int,
+                                         C.c_float, C.c_float, C.c_float, C.c_float,
+                                         C.c_float, C.c_int, _fp, _fp, _fp]
         L.rvo_normals_knn_exact_f64.restype = None
         L.rvo_normals_knn_exact_f64.argtypes = [_fp, _fp, _fp, _sz, _ip, C.c_int, C.c_float,
                                                 C.c_float, C.c_float, _dp, _dp, _dp, _dp]
@@ -192,6 +209,55 @@ class Restatement:
         """List of sorted index arrays, in the reference's cluster order."""
         return _clusters(self.L.rvo_euclidean_clusters, c, tolerance, min_size, max_size)
 
+    # Octree (kind 0) / PointerOctree (kind 1); tree = (cap, max_depth, eps)
+    def octree_order(self, kind, c, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        order = np.zeros(max(x.shape[0], 1), np.int32)
+        self.L.rvo_octree_order(kind, xp, yp, zp, x.shape[0], tree[0], tree[1], tree[2],
+                                _ptr(order, _ip))
+        return order[:x.shape[0]]
+
+    def octree_radius(self, kind, c, radius, queries=None, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        q = queries if queries is not None else c
+        qx, qxp = _f(q.x); qy, qyp = _f(q.y); qz, qzp = _f(q.z)
+        nq = qx.shape[0]
+        offs = np.zeros(nq + 1, np.int64)
+        cap = 1 << 16
+        while True:
+            idx = np.zeros(cap, np.int32); d2 = np.zeros(cap, np.float32)
+            t = self.L.rvo_octree_radius_search(kind, xp, yp, zp, x.shape[0], tree[0], tree[1],
+                                                tree[2], qxp, qyp, qzp, nq, radius,
+                                                _ptr(offs, _lp), _ptr(idx, _ip), _ptr(d2, _fp),
+                                                cap)
+            if t >= 0:
+                return offs, idx[:t].copy(), d2[:t].copy()
+            cap = int(offs[-1]) + 1
+
+    def nth_element(self, a, nth):
+        a = np.ascontiguousarray(a, np.float32).copy()
+        heap = self.L.rvo_nth_element(_ptr(a, _fp), a.shape[0], nth)
+        return a, bool(heap)
+
+    def sor_octree(self, kind, c, k, alpha, search_radius, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        n = x.shape[0]
+        out = np.zeros((max(n, 1), 3), np.float32)
+        md = np.zeros(max(n, 1), np.float32); keep = np.zeros(max(n, 1), np.uint8)
+        m = self.L.rvo_sor_octree(kind, xp, yp, zp, n, tree[0], tree[1], tree[2], k, alpha,
+                                  search_radius, _ptr(out, _fp), _ptr(md, _fp),
+                                  _ptr(keep, C.POINTER(C.c_ubyte)))
+        return out[:m].copy(), md[:n], keep[:n].astype(bool)
+
+    def normals_octree(self, kind, c, radius, vp=(0, 0, 0), iters=4, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        n = x.shape[0]
+        nx, ny, nz = (np.zeros(max(n, 1), np.float32) for _ in range(3))
+        self.L.rvo_normals_octree(kind, xp, yp, zp, n, tree[0], tree[1], tree[2], radius,
+                                  vp[0], vp[1], vp[2], iters, _ptr(nx, _fp), _ptr(ny, _fp),
+                                  _ptr(nz, _fp))
+        return np.stack([nx[:n], ny[:n], nz[:n]], 1)
+
     def normals_exact_f64(self, c, nbr_idx, vp=(0, 0, 0)):
         x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
         nbr = np.ascontiguousarray(nbr_idx, np.int32)
@@ -238,6 +304,22 @@ class Reference:
         L.ref_save_pcd.argtypes = [C.c_char_p, _fp, _sz, C.c_int]
         L.ref_save_pcd_rgb.restype = None
         L.ref_save_pcd_rgb.argtypes = [C.c_char_p, _fp, C.POINTER(C.c_ubyte), _sz, C.c_int]
+        L.ref_octree_radius.restype = C.c_long
+        L.ref_octree_radius.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int,
+                                        C.c_float, _fp, _fp, _fp, _sz, C.c_float, _lp, _ip,
+                                        _fp, _sz]
+        L.ref_sor_octree.restype = _sz
+        L.ref_sor_octree.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int, C.c_float,
+                                     C.c_int, C.c_float, C.c_float, _fp]
+        L.ref_normals_octree.restype = None
+        L.ref_normals_octree.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int,
+                                         C.c_float, C.c_float, C.c_float, C.c_float,
+                                         C.c_float, C.c_int, _fp, _fp, _fp]
+        L.ref_pointer_octree_leaves.restype = C.c_long
+        L.ref_pointer_octree_leaves.argtypes = [_fp, _fp, _fp, _sz, C.c_int, C.c_int,
+                                                C.c_float, _ip, _lp]
+        L.ref_nth_element.restype = None
+        L.ref_nth_element.argtypes = [_fp, _sz, _sz]
         L.ref_euclidean_clusters.restype = C.c_long
         L.ref_euclidean_clusters.argtypes = [_fp, _fp, _fp, _sz, C.c_float, C.c_int, C.c_int,
                                              _lp, _ip]
@@ -315,6 +397,53 @@ class Reference:
         out = np.zeros((max(cap, 1), 3), np.float32)
         k = self.L.ref_load_pcd(path.encode(), _ptr(out, _fp), cap)
         return out[:max(k, 0)].copy() if k >= 0 else None
+
+    # kind 0: Octree, 1: PointerOctree::radiusSearch, 2: radiusSearchScalar
+    def octree_radius(self, kind, c, radius, queries=None, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        q = queries if queries is not None else c
+        qx, qxp = _f(q.x); qy, qyp = _f(q.y); qz, qzp = _f(q.z)
+        nq = qx.shape[0]
+        offs = np.zeros(nq + 1, np.int64)
+        cap = 1 << 16
+        while True:
+            idx = np.zeros(cap, np.int32); d2 = np.zeros(cap, np.float32)
+            t = self.L.ref_octree_radius(kind, xp, yp, zp, x.shape[0], tree[0], tree[1],
+                                         tree[2], qxp, qyp, qzp, nq, radius, _ptr(offs, _lp),
+                                         _ptr(idx, _ip), _ptr(d2, _fp), cap)
+            if t <= cap:
+                return offs, idx[:t].copy(), d2[:t].copy()
+            cap = t
+
+    def sor_octree(self, kind, c, k, alpha, search_radius, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        out = np.zeros((max(x.shape[0], 1), 3), np.float32)
+        m = self.L.ref_sor_octree(kind, xp, yp, zp, x.shape[0], tree[0], tree[1], tree[2], k,
+                                  alpha, search_radius, _ptr(out, _fp))
+        return out[:m].copy()
+
+    # kind 0: Octree, 1: PointerOctree, 2: the self-building overload
+    def normals_octree(self, kind, c, radius, vp=(0, 0, 0), iters=4, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        n = x.shape[0]
+        nx, ny, nz = (np.zeros(max(n, 1), np.float32) for _ in range(3))
+        self.L.ref_normals_octree(kind, xp, yp, zp, n, tree[0], tree[1], tree[2], radius,
+                                  vp[0], vp[1], vp[2], iters, _ptr(nx, _fp), _ptr(ny, _fp),
+                                  _ptr(nz, _fp))
+        return np.stack([nx[:n], ny[:n], nz[:n]], 1)
+
+    def pointer_octree_leaves(self, c, tree=(64, 8, 1e-4)):
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        n = x.shape[0]
+        order = np.zeros(max(n, 1), np.int32); offs = np.zeros(n + 2, np.int64)
+        L = self.L.ref_pointer_octree_leaves(xp, yp, zp, n, tree[0], tree[1], tree[2],
+                                             _ptr(order, _ip), _ptr(offs, _lp))
+        return order[:n], offs[:L + 1]
+
+    def nth_element(self, a, nth):
+        a = np.ascontiguousarray(a, np.float32).copy()
+        self.L.ref_nth_element(_ptr(a, _fp), a.shape[0], nth)
+        return a
 
     def euclidean_clusters(self, c, tolerance, min_size=1, max_size=2**31 - 1):
         return _clusters(self.L.ref_euclidean_clusters, c, tolerance, min_size, max_size)

@@ -16,6 +16,10 @@
 #include "segmentation/ransac_plane.h"
 #include "segmentation/euclidean_clustering.h"
 #include "io/simple_pcd_loader.h"
+#include "search/octree.h"
+#include "search/pointer_octree.h"
+
+#include <algorithm>
 
 #include <cstdint>
 #include <cstdlib>
@@ -197,6 +201,134 @@ void ref_save_pcd_rgb(const char *path, const float *aos, const unsigned char *r
               rgb[3 * i + 2]};
   savePCDRGB(path, pts, binary != 0);
 }
+
+// Octree (kind 0), PointerOctree::radiusSearch (kind 1) and
+// PointerOctree::radiusSearchScalar (kind 2) for every query; the trees'
+// parameters through their setters. Returns the total (entries past
+// capacity are dropped).
+long ref_octree_radius(int kind, const float *x, const float *y, const float *z, size_t n,
+                       int cap, int depth, float eps, const float *qx, const float *qy,
+                       const float *qz, size_t nq, float radius, int64_t *offsets,
+                       int32_t *idx, float *d2, size_t capacity) {
+  const PointCloudSoA c = soa(x, y, z, n);
+  Octree ot;
+  PointerOctree pt;
+  if (kind == 0) {
+    ot.setMaxPointsPerLeaf(cap);
+    ot.setMaxDepth(depth);
+    ot.setBuildEpsilon(eps);
+    ot.setInputCloud(c);
+    ot.build();
+  } else {
+    pt.setMaxPointsPerLeaf(cap);
+    pt.setMaxDepth(depth);
+    pt.setBuildEpsilon(eps);
+    pt.setInputCloud(c);
+    pt.build();
+  }
+  std::vector<int> ind;
+  std::vector<float> dst;
+  size_t tot = 0;
+  offsets[0] = 0;
+  for (size_t q = 0; q < nq; ++q) {
+    PointXYZ p{qx[q], qy[q], qz[q]};
+    if (kind == 0) ot.radiusSearch(p, radius, ind, dst);
+    else if (kind == 1) pt.radiusSearch(p, radius, ind, dst);
+    else pt.radiusSearchScalar(p, radius, ind, dst);
+    for (size_t t = 0; t < ind.size(); ++t, ++tot) {
+      if (tot < capacity) {
+        idx[tot] = ind[t];
+        d2[tot] = dst[t];
+      }
+    }
+    offsets[q + 1] = (int64_t)tot;
+  }
+  return (long)tot;
+}
+
+// sor_octree (kind 0) / sor_pointer_octree (kind 1) on a tree of the cloud
+size_t ref_sor_octree(int kind, const float *x, const float *y, const float *z, size_t n,
+                      int cap, int depth, float eps, int k, float alpha, float radius,
+                      float *out) {
+  const PointCloudSoA c = soa(x, y, z, n);
+  if (kind == 0) {
+    Octree t;
+    t.setMaxPointsPerLeaf(cap);
+    t.setMaxDepth(depth);
+    t.setBuildEpsilon(eps);
+    t.setInputCloud(c);
+    t.build();
+    return sor_octree(c, t, reinterpret_cast<PointXYZ *>(out), k, alpha, radius);
+  }
+  PointerOctree t;
+  t.setMaxPointsPerLeaf(cap);
+  t.setMaxDepth(depth);
+  t.setBuildEpsilon(eps);
+  t.setInputCloud(c);
+  t.build();
+  return sor_pointer_octree(c, t, reinterpret_cast<PointXYZ *>(out), k, alpha, radius);
+}
+
+// normal_estimation_rvv with an Octree (kind 0), a PointerOctree (kind 1),
+// or the self-building overload (kind 2, default tree parameters)
+void ref_normals_octree(int kind, const float *x, const float *y, const float *z, size_t n,
+                        int cap, int depth, float eps, float radius, float vx, float vy,
+                        float vz, int iters, float *nx, float *ny, float *nz) {
+  const PointCloudSoA c = soa(x, y, z, n);
+  if (kind == 0) {
+    Octree t;
+    t.setMaxPointsPerLeaf(cap);
+    t.setMaxDepth(depth);
+    t.setBuildEpsilon(eps);
+    t.setInputCloud(c);
+    t.build();
+    normal_estimation_rvv(c, t, nx, ny, nz, 10, radius, vx, vy, vz, iters);
+  } else if (kind == 1) {
+    PointerOctree t;
+    t.setMaxPointsPerLeaf(cap);
+    t.setMaxDepth(depth);
+    t.setBuildEpsilon(eps);
+    t.setInputCloud(c);
+    t.build();
+    normal_estimation_rvv(c, t, nx, ny, nz, 10, radius, vx, vy, vz, iters);
+  } else {
+    normal_estimation_rvv(c, nx, ny, nz, 10, radius, vx, vy, vz, iters);
+  }
+}
+
+// PointerOctree::getRoot: the leaves in depth-first order (children 0..7)
+// with their points; returns the number of leaves
+long ref_pointer_octree_leaves(const float *x, const float *y, const float *z, size_t n,
+                               int cap, int depth, float eps, int32_t *order,
+                               int64_t *leaf_offsets) {
+  PointerOctree t;
+  t.setMaxPointsPerLeaf(cap);
+  t.setMaxDepth(depth);
+  t.setBuildEpsilon(eps);
+  t.setInputCloud(soa(x, y, z, n));
+  t.build();
+  long leaves = 0;
+  size_t pos = 0;
+  leaf_offsets[0] = 0;
+  std::vector<const PointerOctreeNode *> stack;
+  if (t.getRoot()) stack.push_back(t.getRoot());
+  while (!stack.empty()) {
+    const PointerOctreeNode *nd = stack.back();
+    stack.pop_back();
+    if (nd->is_leaf) {
+      for (int i : nd->indices) order[pos++] = i;
+      leaf_offsets[++leaves] = (int64_t)pos;
+    } else {
+      for (int c = 7; c >= 0; --c)
+        if (nd->children[c]) stack.push_back(nd->children[c]);
+    }
+  }
+  return leaves;
+}
+
+// std::nth_element of the reference's C++ library (the step of
+// sor_pointer_octree, statistical_outlier_removal.cpp:290)
+void ref_nth_element(float *a, size_t n, size_t nth) { std::nth_element(a, a + nth, a + n); }
 
 // Raw glibc rand() stream after srand(seed): the hypothesis source of
 // ransac_plane_sc (ransac_plane.cpp:60,69-71).

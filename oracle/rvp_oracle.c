@@ -837,3 +837,295 @@ long rvo_euclidean_clusters(const float *x, const float *y, const float *z, size
   free(queue);
   return n_cl;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Octree / PointerOctree                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Root box: octree.cpp:36-53 (min, max + eps) and pointer_octree.cpp:36-63
+ * (min - eps, max + eps). */
+static void oct_root(int kind, const float *x, const float *y, const float *z, size_t n,
+                     float eps, float b[6]) {
+  const float *c[3] = {x, y, z};
+  for (int a = 0; a < 3; ++a) {
+    float lo = FLT_MAX, hi = -FLT_MAX;
+    for (size_t i = 0; i < n; ++i) {
+      if (c[a][i] < lo) lo = c[a][i];
+      if (c[a][i] > hi) hi = c[a][i];
+    }
+    b[a] = kind == 0 ? lo : lo - eps;
+    b[3 + a] = hi + eps;
+  }
+}
+
+/* buildParams (octree.cpp:59-94): a node with <= cap points, or at
+ * max_depth, is a leaf; otherwise its points go to child
+ * (x >= mid) | (y >= mid) << 1 | (z >= mid) << 2 in index order, with
+ * mid = (min + max) * 0.5f per axis, and the children are visited 0..7. */
+static void oct_split(const float *x, const float *y, const float *z, int *idx, int *tmp,
+                      size_t cnt, const float b[6], int depth, size_t cap, int max_depth,
+                      int *out, size_t *pos) {
+  if (cnt <= cap || depth >= max_depth) {
+    memcpy(out + *pos, idx, cnt * sizeof(int));
+    *pos += cnt;
+    return;
+  }
+  const float mx = (b[0] + b[3]) * 0.5f, my = (b[1] + b[4]) * 0.5f,
+              mz = (b[2] + b[5]) * 0.5f;
+  size_t count[8] = {0}, start[8];
+  for (size_t t = 0; t < cnt; ++t) {
+    const int i = idx[t];
+    const int code = (x[i] >= mx) | ((y[i] >= my) << 1) | ((z[i] >= mz) << 2);
+    count[code]++;
+  }
+  start[0] = 0;
+  for (int c = 1; c < 8; ++c) start[c] = start[c - 1] + count[c - 1];
+  size_t fill[8];
+  memcpy(fill, start, sizeof(fill));
+  for (size_t t = 0; t < cnt; ++t) {
+    const int i = idx[t];
+    const int code = (x[i] >= mx) | ((y[i] >= my) << 1) | ((z[i] >= mz) << 2);
+    tmp[fill[code]++] = i;
+  }
+  memcpy(idx, tmp, cnt * sizeof(int));
+  for (int c = 0; c < 8; ++c) {
+    if (!count[c]) continue;
+    float cb[6];
+    cb[0] = (c & 1) ? mx : b[0];
+    cb[3] = (c & 1) ? b[3] : mx;
+    cb[1] = (c & 2) ? my : b[1];
+    cb[4] = (c & 2) ? b[4] : my;
+    cb[2] = (c & 4) ? mz : b[2];
+    cb[5] = (c & 4) ? b[5] : mz;
+    oct_split(x, y, z, idx + start[c], tmp + start[c], count[c], cb, depth + 1, cap,
+              max_depth, out, pos);
+  }
+}
+
+void rvo_octree_order(int kind, const float *x, const float *y, const float *z, size_t n,
+                      int cap, int max_depth, float eps, int *order) {
+  if (n == 0) return;
+  float b[6];
+  oct_root(kind, x, y, z, n, eps, b);
+  int *idx = (int *)malloc(n * sizeof(int)), *tmp = (int *)malloc(n * sizeof(int));
+  for (size_t i = 0; i < n; ++i) idx[i] = (int)i;
+  size_t pos = 0;
+  /* (size_t)max_points_per_leaf_, as the reference compares */
+  oct_split(x, y, z, idx, tmp, n, b, 0, (size_t)(long long)cap, max_depth, order, &pos);
+  free(idx);
+  free(tmp);
+}
+
+long long rvo_octree_radius_search(int kind, const float *x, const float *y, const float *z,
+                                   size_t n, int cap_leaf, int max_depth, float eps,
+                                   const float *qx, const float *qy, const float *qz,
+                                   size_t nq, float radius, long long *offsets, int *idx,
+                                   float *d2, long long cap) {
+  int *order = (int *)malloc((n ? n : 1) * sizeof(int));
+  rvo_octree_order(kind, x, y, z, n, cap_leaf, max_depth, eps, order);
+  const float r2 = radius * radius;
+  long long tot = 0;
+  offsets[0] = 0;
+  for (size_t q = 0; q < nq; ++q) {
+    for (size_t p = 0; p < n; ++p) {
+      const int j = order[p];
+      const float dx = x[j] - qx[q], dy = y[j] - qy[q], dz = z[j] - qz[q];
+      const float d = dx * dx + dy * dy + dz * dz;
+      if (d <= r2) {
+        if (tot < cap) {
+          idx[tot] = j;
+          d2[tot] = d;
+        }
+        ++tot;
+      }
+    }
+    offsets[q + 1] = tot;
+  }
+  free(order);
+  return tot > cap ? -1 : tot;
+}
+
+/* --- std::nth_element (libstdc++ 13, bits/stl_algo.h / stl_heap.h) -------
+ * Introselect: while the range holds more than 3 elements, move the median
+ * of (first + 1, middle, last - 1) to first, partition the rest around it
+ * (Hoare, unguarded) and keep the side holding nth; after 2 * floor(log2 n)
+ * rounds fall back to a binary-heap selection of the nth + 1 smallest.
+ * The last range is insertion-sorted. Only operator< is used. */
+static void fswap(float *a, long i, long j) {
+  const float t = a[i];
+  a[i] = a[j];
+  a[j] = t;
+}
+
+/* percolate v up from hole towards top in the max-heap a */
+static void heap_up(float *a, long hole, long top, float v) {
+  long parent = (hole - 1) / 2;
+  while (hole > top && a[parent] < v) {
+    a[hole] = a[parent];
+    hole = parent;
+    parent = (hole - 1) / 2;
+  }
+  a[hole] = v;
+}
+
+/* move the hole down to a leaf along the larger children, then put v in
+ * by percolating it up (the bottom-up sift of libstdc++'s __adjust_heap) */
+static void heap_adjust(float *a, long hole, long len, float v) {
+  const long top = hole;
+  long child = hole;
+  while (child < (len - 1) / 2) {
+    child = 2 * (child + 1);
+    if (a[child] < a[child - 1]) child--;
+    a[hole] = a[child];
+    hole = child;
+  }
+  if ((len & 1) == 0 && child == (len - 2) / 2) {
+    child = 2 * (child + 1);
+    a[hole] = a[child - 1];
+    hole = child - 1;
+  }
+  heap_up(a, hole, top, v);
+}
+
+static void heap_select(float *a, long middle, long last) {
+  if (middle >= 2) {
+    for (long parent = (middle - 2) / 2;; --parent) {
+      heap_adjust(a, parent, middle, a[parent]);
+      if (parent == 0) break;
+    }
+  }
+  for (long i = middle; i < last; ++i) {
+    if (a[i] < a[0]) {
+      const float v = a[i];
+      a[i] = a[0];
+      heap_adjust(a, 0, middle, v);
+    }
+  }
+}
+
+int rvo_nth_element(float *a, size_t n, size_t nth) {
+  if (n == 0 || nth >= n) return 0;
+  long first = 0, last = (long)n;
+  int lg = 0;
+  while (((size_t)1 << (lg + 1)) <= n) ++lg;
+  int depth = 2 * lg;
+  while (last - first > 3) {
+    if (depth == 0) {
+      heap_select(a + first, (long)nth + 1 - first, last - first);
+      fswap(a, first, (long)nth);
+      return 1;
+    }
+    --depth;
+    /* median of three to first */
+    const long x = first + 1, y = first + (last - first) / 2, z = last - 1;
+    if (a[x] < a[y]) {
+      if (a[y] < a[z]) fswap(a, first, y);
+      else if (a[x] < a[z]) fswap(a, first, z);
+      else fswap(a, first, x);
+    } else if (a[x] < a[z]) {
+      fswap(a, first, x);
+    } else if (a[y] < a[z]) {
+      fswap(a, first, z);
+    } else {
+      fswap(a, first, y);
+    }
+    /* unguarded partition of [first + 1, last) around a[first] */
+    long lo = first + 1, hi = last;
+    for (;;) {
+      while (a[lo] < a[first]) ++lo;
+      --hi;
+      while (a[first] < a[hi]) --hi;
+      if (!(lo < hi)) break;
+      fswap(a, lo, hi);
+      ++lo;
+    }
+    if (lo <= (long)nth) first = lo;
+    else last = lo;
+  }
+  for (long i = first + 1; i < last; ++i) {
+    const float v = a[i];
+    if (v < a[first]) {
+      memmove(a + first + 1, a + first, (size_t)(i - first) * sizeof(float));
+      a[first] = v;
+    } else {
+      long j = i;
+      while (v < a[j - 1]) {
+        a[j] = a[j - 1];
+        --j;
+      }
+      a[j] = v;
+    }
+  }
+  return 0;
+}
+
+static int cmp_f32(const void *a, const void *b) {
+  const float p = *(const float *)a, q = *(const float *)b;
+  return (p > q) - (p < q);
+}
+
+size_t rvo_sor_octree(int kind, const float *x, const float *y, const float *z, size_t n,
+                      int cap_leaf, int max_depth, float eps, int k, float alpha,
+                      float search_radius, float *out, float *mean_dists, unsigned char *keep) {
+  if (n == 0) return 0;
+  int *order = (int *)malloc(n * sizeof(int));
+  rvo_octree_order(kind, x, y, z, n, cap_leaf, max_depth, eps, order);
+  float *md = mean_dists ? mean_dists : (float *)malloc(n * sizeof(float));
+  float *d = (float *)malloc(n * sizeof(float));
+  const float r2 = search_radius * search_radius;
+  for (size_t i = 0; i < n; ++i) {
+    size_t c = 0;
+    for (size_t p = 0; p < n; ++p) {
+      const int j = order[p];
+      const float dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      const float v = dx * dx + dy * dy + dz * dz;
+      if (v <= r2) d[c++] = v;
+    }
+    if (c > 1) {
+      const int valid_k = k < (int)c - 1 ? k : (int)c - 1;
+      if (kind == 0) qsort(d, c, sizeof(float), cmp_f32);
+      else rvo_nth_element(d, c, (size_t)valid_k);
+      float sum = 0.0f;
+      for (int j = 1; j <= valid_k; ++j) sum += sqrtf(d[j]);
+      md[i] = sum / (float)valid_k;
+    } else {
+      md[i] = search_radius;
+    }
+  }
+  free(d);
+  free(order);
+  size_t kept = sor_filter(x, y, z, n, md, alpha, out, keep);
+  if (!mean_dists) free(md);
+  return kept;
+}
+
+void rvo_normals_octree(int kind, const float *x, const float *y, const float *z, size_t n,
+                        int cap_leaf, int max_depth, float eps, float radius, float vpx,
+                        float vpy, float vpz, int iters, float *nx, float *ny, float *nz) {
+  if (n == 0) return;
+  int *order = (int *)malloc(n * sizeof(int));
+  rvo_octree_order(kind, x, y, z, n, cap_leaf, max_depth, eps, order);
+  nbr *l = (nbr *)malloc(n * sizeof(nbr));
+  const float r2 = radius * radius;
+  for (size_t i = 0; i < n; ++i) {
+    size_t m = 0;
+    for (size_t p = 0; p < n; ++p) {
+      const int j = order[p];
+      const float dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      const float v = dx * dx + dy * dy + dz * dz;
+      if (v <= r2) {
+        l[m].d2 = v;
+        l[m].idx = j;
+        ++m;
+      }
+    }
+    if (m < 3) {
+      nx[i] = ny[i] = nz[i] = 0;
+      continue;
+    }
+    normal_from_list_f(x, y, z, l, m, 0, x[i], y[i], z[i], vpx, vpy, vpz, iters, nx + i,
+                       ny + i, nz + i);
+  }
+  free(l);
+  free(order);
+}

@@ -90,6 +90,44 @@ long rvo_euclidean_clusters(const float *x, const float *y, const float *z, size
                             float tolerance, int min_size, int max_size, long long *offsets,
                             int *indices);
 
+/* Octree (search/octree.cpp:32-94) and PointerOctree
+ * (search/pointer_octree.cpp:30-116), kind 0 and 1: the points in the
+ * trees' depth-first leaf order (children 0..7, each leaf's points in index
+ * order), which is the order of their radiusSearch output. cap, max_depth,
+ * eps: setMaxPointsPerLeaf / setMaxDepth / setBuildEpsilon (64, 8, 1e-4). */
+void rvo_octree_order(int kind, const float *x, const float *y, const float *z, size_t n,
+                      int cap, int max_depth, float eps, int *order);
+
+/* Octree::radiusSearch (octree.cpp:111-143) / PointerOctree::radiusSearch
+ * (pointer_octree.cpp:201-240): every point with d2 <= radius^2 in the tree's
+ * leaf order, max_nn ignored. CSR as rvo_hash_radius_search; returns the
+ * total, or -1 if cap was too small. */
+long long rvo_octree_radius_search(int kind, const float *x, const float *y, const float *z,
+                                   size_t n, int cap_leaf, int max_depth, float eps,
+                                   const float *qx, const float *qy, const float *qz,
+                                   size_t nq, float radius, long long *offsets, int *idx,
+                                   float *d2, long long cap);
+
+/* std::nth_element on floats as libstdc++ (GCC 13) does it: introselect
+ * with median-of-three pivots, heap selection when the depth limit
+ * 2 * floor(log2 n) runs out, insertion sort of the last range of <= 3.
+ * Returns 1 if the heap selection ran. */
+int rvo_nth_element(float *a, size_t n, size_t nth);
+
+/* sor_octree (kind 0, statistical_outlier_removal.cpp:220-244: all
+ * neighbours in the radius, sorted) and sor_pointer_octree (kind 1,
+ * :272-301: nth_element on the tree-ordered distances), then
+ * filter_by_mean_dists. mean_dists/keep optional. */
+size_t rvo_sor_octree(int kind, const float *x, const float *y, const float *z, size_t n,
+                      int cap_leaf, int max_depth, float eps, int k, float alpha,
+                      float search_radius, float *out, float *mean_dists, unsigned char *keep);
+
+/* normal_estimation_rvv(in, Octree / PointerOctree, ...) (normal_estimation
+ * .cpp:155-187, 216-244): neighbours = the tree's radiusSearch, in its order. */
+void rvo_normals_octree(int kind, const float *x, const float *y, const float *z, size_t n,
+                        int cap_leaf, int max_depth, float eps, float radius, float vpx,
+                        float vpy, float vpz, int iters, float *nx, float *ny, float *nz);
+
 #ifdef __cplusplus
 }
 #endif

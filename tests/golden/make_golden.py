@@ -63,6 +63,30 @@ def main():
         cl = R.euclidean_clusters(c, tol, mn, mx)
         out[f"ec_{name}_offsets"] = np.cumsum([0] + [len(k) for k in cl]).astype(np.int64)
         out[f"ec_{name}_idx"] = (np.concatenate(cl) if cl else np.zeros(0)).astype(np.int32)
+    # Octree / PointerOctree: leaf order (radiusSearch over everything),
+    # radius lists in tree order, sor_octree / sor_pointer_octree, normals
+    big = D.Cloud.from_xyz(np.array([[0.0, 0.0, 0.0]], np.float32))
+    for kind in (0, 1):
+        for tname, tree in (("d", (64, 8, 1e-4)), ("s", (8, 5, 1e-3))):
+            _, i, _ = R.octree_radius(kind, room, 1e6, queries=big, tree=tree)
+            out[f"oct{kind}_order_{tname}"] = i
+        o, i, d = R.octree_radius(kind, room, 0.05)
+        out[f"oct{kind}_r05_offsets"] = o
+        out[f"oct{kind}_r05_idx"] = i
+        out[f"oct{kind}_r05_d2"] = d
+        out[f"oct{kind}_sor_k20"] = R.sor_octree(kind, room, 20, 1.0, 0.1)
+        out[f"oct{kind}_nrm_r05"] = R.normals_octree(kind, room, 0.05)
+    # std::nth_element (sor_pointer_octree's step): inputs and results
+    rng = np.random.default_rng(7)
+    nth_in = [rng.random(257).astype(np.float32), rng.integers(0, 5, 100).astype(np.float32),
+              np.concatenate([np.arange(150), np.arange(150)[::-1]]).astype(np.float32),
+              # organ pipe of 85 with nth 35: the depth limit runs out (heap selection)
+              np.concatenate([np.arange(42), np.arange(43)[::-1]]).astype(np.float32)]
+    for t, a in enumerate(nth_in):
+        nth = [100, 37, 120, 35][t]
+        out[f"nth{t}_in"] = a
+        out[f"nth{t}_k"] = np.array([nth], np.int64)
+        out[f"nth{t}_out"] = R.nth_element(a, nth)
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
     print("wrote", os.path.join(HERE, "golden.npz"), len(out), "arrays")
 

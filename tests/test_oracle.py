@@ -154,3 +154,84 @@ def test_golden_euclidean_clusters(golden, restatement, name, src, tol, mn, mx):
     assert np.array_equal(offs, golden[f"ec_{name}_offsets"])
     idx = np.concatenate(cl).astype(np.int32) if cl else np.zeros(0, np.int32)
     assert np.array_equal(idx, golden[f"ec_{name}_idx"])
+
+
+# ---- Octree / PointerOctree ------------------------------------------------
+@pytest.mark.parametrize("kind", [0, 1])
+def test_golden_octree(golden, restatement, kind):
+    room = cloud(golden["room"])
+    for tname, tree in (("d", (64, 8, 1e-4)), ("s", (8, 5, 1e-3))):
+        assert np.array_equal(restatement.octree_order(kind, room, tree),
+                              golden[f"oct{kind}_order_{tname}"])
+    o, i, d = restatement.octree_radius(kind, room, 0.05)
+    assert np.array_equal(o, golden[f"oct{kind}_r05_offsets"])
+    assert np.array_equal(i, golden[f"oct{kind}_r05_idx"])
+    assert np.array_equal(bits(d), bits(golden[f"oct{kind}_r05_d2"]))
+    s, _, _ = restatement.sor_octree(kind, room, 20, 1.0, 0.1)
+    assert np.array_equal(bits(s), bits(golden[f"oct{kind}_sor_k20"]))
+    n = restatement.normals_octree(kind, room, 0.05)
+    assert np.array_equal(bits(n), bits(golden[f"oct{kind}_nrm_r05"]))
+
+
+def test_golden_nth_element(golden, restatement):
+    heap = False
+    for t in range(4):
+        r, h = restatement.nth_element(golden[f"nth{t}_in"], int(golden[f"nth{t}_k"][0]))
+        assert np.array_equal(bits(r), bits(golden[f"nth{t}_out"]))
+        heap |= h
+    assert heap  # the heap-selection branch is pinned too
+
+
+def test_reference_nth_element(reference, restatement):
+    """The restated introselect against the C++ library's nth_element on
+    random, few-valued, sorted, reversed and organ-pipe arrays (the last ones
+    reach the heap selection)."""
+    rng = np.random.default_rng(0)
+    heaps = 0
+    for t in range(3000):
+        n = int(rng.integers(1, 300))
+        kind = t % 5
+        if kind == 0:
+            a = rng.random(n).astype(np.float32)
+        elif kind == 1:
+            a = rng.integers(0, 4, n).astype(np.float32)
+        elif kind == 2:
+            a = np.sort(rng.random(n)).astype(np.float32)
+        elif kind == 3:
+            a = np.sort(rng.random(n))[::-1].astype(np.float32)
+        else:
+            h = n // 2
+            a = np.concatenate([np.arange(h), np.arange(n - h)[::-1]]).astype(np.float32)
+        nth = int(rng.integers(0, n))
+        s, hp = restatement.nth_element(a, nth)
+        heaps += hp
+        assert np.array_equal(bits(reference.nth_element(a, nth)), bits(s)), (t, n, nth)
+    assert heaps > 0
+
+
+@pytest.mark.parametrize("seed", [5, 6])
+def test_reference_octrees(reference, restatement, seed):
+    c = D.room_cloud(n=2500, seed=seed)
+    q = D.Cloud.from_xyz(np.array([[0.5, 0.5, 0.5]], np.float32))
+    for kind in (0, 1):
+        for tree in ((64, 8, 1e-4), (8, 8, 1e-4), (16, 3, 1e-3), (1, 12, 1e-4), (-1, 8, 1e-4)):
+            _, i, _ = reference.octree_radius(kind, c, 1e6, queries=q, tree=tree)
+            assert np.array_equal(restatement.octree_order(kind, c, tree), i)
+        for r in (0.05, 0.2):
+            a = reference.octree_radius(kind, c, r)
+            b = restatement.octree_radius(kind, c, r)
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+            assert np.array_equal(bits(a[2]), bits(b[2]))
+        for k, al, r in ((10, 1.0, 0.1), (5, 0.5, 0.05)):
+            assert np.array_equal(bits(reference.sor_octree(kind, c, k, al, r)),
+                                  bits(restatement.sor_octree(kind, c, k, al, r)[0]))
+        assert np.array_equal(bits(reference.normals_octree(kind, c, 0.08)),
+                              bits(restatement.normals_octree(kind, c, 0.08)))
+    # radiusSearchScalar and the self-building normals overload
+    a = reference.octree_radius(2, c, 0.1)
+    b = restatement.octree_radius(1, c, 0.1)
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(bits(reference.normals_octree(2, c, 0.08)),
+                          bits(restatement.normals_octree(1, c, 0.08)))
+    o, l = reference.pointer_octree_leaves(c)
+    assert np.array_equal(o, restatement.octree_order(1, c))
