@@ -45,6 +45,7 @@ enum { RVP_MEM_HOST = 0, RVP_MEM_DEVICE = 1 };
 typedef struct rvp_context rvp_context;
 typedef struct rvp_hash rvp_hash;
 typedef struct rvp_pipeline rvp_pipeline;
+typedef struct rvp_octree rvp_octree;
 
 /* ---- context ------------------------------------------------------------ */
 RVP_API rvp_status rvp_context_create(int device, rvp_context **out);
@@ -170,6 +171,48 @@ RVP_API rvp_status rvp_euclidean_clusters(rvp_context *ctx, const float *x, cons
                                           int min_size, int max_size, int mem,
                                           int64_t *offsets, int32_t *indices,
                                           size_t *n_clusters);
+
+/* ---- Octree / PointerOctree: search/octree.h:20-48, pointer_octree.h:26-62 */
+/* Both trees return every point with squared distance <= radius^2 (max_nn
+ * ignored, octree.cpp:111-114), in the tree's depth-first leaf order
+ * (children 0..7, each leaf's points by index). The tree is not built as
+ * nodes: build gives every point its rank in that order (root box by the
+ * tree's epsilon rule, float midpoints, leaves of <= max_points_per_leaf
+ * points or at max_depth), and searches sort the grid's radius lists by rank.
+ * The cloud is copied to the device (the reference keeps a pointer). */
+enum { RVP_OCTREE = 0, RVP_POINTER_OCTREE = 1 };
+RVP_API rvp_status rvp_octree_create(rvp_context *ctx, int kind, rvp_octree **out);
+RVP_API rvp_status rvp_octree_destroy(rvp_octree *o);
+/* setMaxPointsPerLeaf / setMaxDepth / setBuildEpsilon (64, 8, 1e-4 by
+ * default; octree.h:33-35). max_depth > 21 is rejected. */
+RVP_API rvp_status rvp_octree_set_params(rvp_octree *o, int max_points_per_leaf, int max_depth,
+                                         float build_epsilon);
+/* setInputCloud (octree.cpp:28-30, pointer_octree.cpp:26-28) */
+RVP_API rvp_status rvp_octree_set_input_cloud(rvp_octree *o, const float *x, const float *y,
+                                              const float *z, size_t n, int mem);
+/* build (octree.cpp:32-57, pointer_octree.cpp:30-69) */
+RVP_API rvp_status rvp_octree_build(rvp_octree *o);
+/* the points in the tree's leaf order (n ints) */
+RVP_API rvp_status rvp_octree_order(rvp_octree *o, int mem, int32_t *order);
+/* radiusSearch for nq queries (octree.cpp:111-143, pointer_octree.cpp
+ * :201-282 incl. radiusSearchScalar). CSR as rvp_hash_radius_search. */
+RVP_API rvp_status rvp_octree_radius_search(rvp_octree *o, const float *qx, const float *qy,
+                                            const float *qz, size_t nq, float radius, int mem,
+                                            int64_t *offsets, int32_t *indices, float *dists,
+                                            size_t capacity, size_t *total);
+/* sor_octree (RVP_OCTREE, statistical_outlier_removal.cpp:220-244: sorted
+ * distances) / sor_pointer_octree (RVP_POINTER_OCTREE, :272-301: the C++
+ * library's nth_element on the tree-ordered distances, as the reference
+ * runs it) on the tree's cloud; outputs as rvp_sor_spatial_hash. */
+RVP_API rvp_status rvp_sor_octree(rvp_octree *o, int k, float alpha, float search_radius,
+                                  int mem, float *out_aos, size_t *out_count, float *mean_dists,
+                                  uint8_t *keep);
+/* normal_estimation_rvv(in, Octree / PointerOctree, ...) (normal_estimation
+ * .cpp:155-187, 216-253) on the tree's cloud: covariance over the tree's
+ * radiusSearch list, in its order. */
+RVP_API rvp_status rvp_normals_octree(rvp_octree *o, float radius, float vp_x, float vp_y,
+                                      float vp_z, int eigen_iters, int mem, float *nx,
+                                      float *ny, float *nz);
 
 /* ---- PCD input: io/simple_pcd_loader.h:143-291 ---------------------------- */
 /* loadPCD's parsing (ascii, binary, binary_compressed) into SoA x, y, z

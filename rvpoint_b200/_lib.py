@@ -104,6 +104,17 @@ SIGNATURES = {
                                 P, P]),
     "rvp_plane_labels": (I, [P, P, P, P, P, I, SZ, P, F, P]),
     "rvp_euclidean_clusters": (I, [P, P, P, P, SZ, F, I, I, I, P, P, C.POINTER(SZ)]),
+    "rvp_octree_create": (I, [P, C.c_int, C.POINTER(P)]),
+    "rvp_octree_destroy": (I, [P]),
+    "rvp_octree_set_params": (I, [P, C.c_int, C.c_int, C.c_float]),
+    "rvp_octree_set_input_cloud": (I, [P, P, P, P, SZ, I]),
+    "rvp_octree_build": (I, [P]),
+    "rvp_octree_order": (I, [P, I, P]),
+    "rvp_octree_radius_search": (I, [P, P, P, P, SZ, C.c_float, I, P, P, P, SZ,
+                                     C.POINTER(SZ)]),
+    "rvp_sor_octree": (I, [P, C.c_int, C.c_float, C.c_float, I, P, C.POINTER(SZ), P, P]),
+    "rvp_normals_octree": (I, [P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, I, P,
+                               P, P]),
     "rvp_pcd_load": (I, [P, C.c_char_p, I, P, P, P, SZ, C.POINTER(SZ)]),
     "rvp_ransac_preemptive": (I, [P, P, P, P, P, I, P, P, SZ, P, F, C.c_uint64, I, I, F, F, P, P,
                                   P, P]),

@@ -321,6 +321,173 @@ def sor_spatial_hash(cloud, hash_: SpatialHash, k: int, alpha: float,
 
 
 # ---------------------------------------------------------------------------
+# Octree / PointerOctree
+# ---------------------------------------------------------------------------
+class Octree:
+    """search/octree.h:20-48 on the GPU: radiusSearch returns every point
+    with d2 <= radius^2 in the tree's depth-first leaf order (max_nn is
+    ignored, as in the reference)."""
+
+    KIND = 0
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.L = self.ctx.L
+        h = C.c_void_p()
+        check(self.L.rvp_octree_create(self.ctx.h, self.KIND, C.byref(h)), self.ctx.h)
+        self.h = h
+        self.n = 0
+        self._params = [64, 8, 1e-4]
+
+    def _set_params(self):
+        check(self.L.rvp_octree_set_params(self.h, int(self._params[0]), int(self._params[1]),
+                                           float(self._params[2])), self.ctx.h)
+
+    def setMaxPointsPerLeaf(self, n: int) -> None:
+        self._params[0] = n
+        self._set_params()
+
+    def setMaxDepth(self, d: int) -> None:
+        self._params[1] = d
+        self._set_params()
+
+    def setBuildEpsilon(self, eps: float) -> None:
+        self._params[2] = eps
+        self._set_params()
+
+    def setInputCloud(self, cloud) -> None:
+        x, y, z = _xyz(cloud)
+        mem = _mem_of(x, y, z)
+        _prep(self.ctx, mem)
+        n = int(x.shape[0])
+        check(self.L.rvp_octree_set_input_cloud(self.h, _ptr(x), _ptr(y), _ptr(z), n, mem),
+              self.ctx.h)
+        self.n = n
+
+    def build(self) -> None:
+        _prep(self.ctx, MEM_HOST)
+        check(self.L.rvp_octree_build(self.h), self.ctx.h)
+
+    def order(self) -> np.ndarray:
+        """The points in the tree's leaf order."""
+        _prep(self.ctx, MEM_HOST)
+        o = np.empty(max(self.n, 1), np.int32)
+        check(self.L.rvp_octree_order(self.h, MEM_HOST, _ptr(o)), self.ctx.h)
+        return o[:self.n]
+
+    def radiusSearch(self, query: Sequence[float], radius: float, indices: Optional[list] = None,
+                     dists: Optional[list] = None, max_nn: int = 0) -> int:
+        q = np.asarray(query, dtype=np.float32).reshape(3)
+        offs, idx, d2 = self.radiusSearchBatch(q[0:1], q[1:2], q[2:3], radius)
+        if indices is not None:
+            indices.clear()
+            indices.extend(int(v) for v in idx)
+        if dists is not None:
+            dists.clear()
+            dists.extend(float(v) for v in d2)
+        return int(offs[-1])
+
+    def radiusSearchBatch(self, qx, qy, qz, radius: float, capacity: Optional[int] = None):
+        """All queries at once. Returns (offsets[nq+1], indices, dists) CSR."""
+        qx, qy, qz = _f32(qx), _f32(qy), _f32(qz)
+        mem = _mem_of(qx, qy, qz)
+        _prep(self.ctx, mem)
+        nq = int(qx.shape[0])
+        dev = mem == MEM_DEVICE
+        device = qx.device if dev else None
+        offs = _empty((nq + 1,), np.int64, dev, device)
+        cap = capacity if capacity is not None else 0
+        total = C.c_size_t(0)
+        while True:
+            idx = _empty((max(cap, 1),), np.int32, dev, device)
+            d2 = _empty((max(cap, 1),), np.float32, dev, device)
+            st = self.L.rvp_octree_radius_search(self.h, _ptr(qx), _ptr(qy), _ptr(qz), nq,
+                                                 float(radius), mem, _ptr(offs), _ptr(idx),
+                                                 _ptr(d2), cap, C.byref(total))
+            if st == _lib.RVP_ERR_CAPACITY:
+                cap = int(total.value)
+                continue
+            check(st, self.ctx.h)
+            t = int(total.value)
+            return offs, idx[:t], d2[:t]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.rvp_octree_destroy(self.h)
+            self.h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PointerOctree(Octree):
+    """search/pointer_octree.h:26-62 (root box [min - eps, max + eps])."""
+
+    KIND = 1
+
+    def radiusSearchScalar(self, query, radius, indices=None, dists=None) -> int:
+        """pointer_octree.cpp:242-282: the same list as radiusSearch."""
+        return self.radiusSearch(query, radius, indices, dists)
+
+
+def _sor_tree(tree, k, alpha, search_radius, return_stats):
+    ctx = tree.ctx
+    _prep(ctx, MEM_HOST)
+    n = tree.n
+    out = np.empty((max(n, 1), 3), np.float32)
+    md = np.empty(max(n, 1), np.float32)
+    keep = np.empty(max(n, 1), np.uint8)
+    cnt = C.c_size_t(0)
+    check(ctx.L.rvp_sor_octree(tree.h, int(k), float(alpha), float(search_radius), MEM_HOST,
+                               _ptr(out), C.byref(cnt), _ptr(md), _ptr(keep)), ctx.h)
+    v = int(cnt.value)
+    if return_stats:
+        return out[:v], md[:n], keep[:n]
+    return out[:v]
+
+
+def sor_octree(cloud, tree: Octree, k: int, alpha: float, search_radius: float = 0.5,
+               return_stats=False):
+    """filters/statistical_outlier_removal.h:29 over the tree's cloud."""
+    return _sor_tree(tree, k, alpha, search_radius, return_stats)
+
+
+def sor_pointer_octree(cloud, tree: PointerOctree, k: int, alpha: float,
+                       search_radius: float = 0.5, return_stats=False):
+    """filters/statistical_outlier_removal.h:41 over the tree's cloud (the
+    reference's nth_element step included)."""
+    return _sor_tree(tree, k, alpha, search_radius, return_stats)
+
+
+def normal_estimation_tree(cloud, tree: Octree, k: int, radius: float, vp_x: float = 0.0,
+                           vp_y: float = 0.0, vp_z: float = 0.0, eigen_iters: int = 4):
+    """features/normal_estimation.h:23/39 (Octree / PointerOctree overloads)
+    over the tree's cloud. Returns (nx, ny, nz)."""
+    ctx = tree.ctx
+    _prep(ctx, MEM_HOST)
+    n = tree.n
+    nx, ny, nz = (np.empty(max(n, 1), np.float32) for _ in range(3))
+    check(ctx.L.rvp_normals_octree(tree.h, float(radius), vp_x, vp_y, vp_z, int(eigen_iters),
+                                   MEM_HOST, _ptr(nx), _ptr(ny), _ptr(nz)), ctx.h)
+    return nx[:n], ny[:n], nz[:n]
+
+
+def normal_estimation_self(cloud, k: int, radius: float, vp_x: float = 0.0, vp_y: float = 0.0,
+                           vp_z: float = 0.0, eigen_iters: int = 4, ctx=None):
+    """features/normal_estimation.h:47 (builds a PointerOctree itself)."""
+    t = PointerOctree(ctx)
+    try:
+        t.setInputCloud(cloud)
+        t.build()
+        return normal_estimation_tree(cloud, t, k, radius, vp_x, vp_y, vp_z, eigen_iters)
+    finally:
+        t.close()
+
+
+# ---------------------------------------------------------------------------
 # normals
 # ---------------------------------------------------------------------------
 def normal_estimation_rvv(cloud, hash_: SpatialHash, k: int, radius: float, vp_x: float = 0.0,
