@@ -27,6 +27,8 @@
 #include "rvpoint/filters/statistical_outlier_removal.h"
 #include "rvpoint/filters/voxel_grid.h"
 #include "rvpoint/io/simple_pcd_loader.h"
+#include "rvpoint/search/octree.h"
+#include "rvpoint/search/pointer_octree.h"
 #include "rvpoint/search/spatial_hashing.h"
 #include "rvpoint/segmentation/ransac_plane.h"
 #include "rvpoint/segmentation/euclidean_clustering.h"
@@ -179,6 +181,80 @@ std::size_t SpatialHash::radiusSearch(const PointXYZ &query, float radius,
   return total;
 }
 
+// ---- Octree / PointerOctree (octree.cpp, pointer_octree.cpp) --------------
+namespace {
+
+void tree_build(rvp_octree *&t, int kind, const PointCloudSoA &c, int cap, int depth, float eps) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (!t && !ok(rvp_octree_create(ctx(), kind, &t))) return;
+  if (rvp_octree_set_params(t, cap, depth, eps) != RVP_OK)
+    throw std::runtime_error(std::string("rvpoint: ") + rvp_last_error(ctx()));
+  if (!ok(rvp_octree_set_input_cloud(t, c.x, c.y, c.z, c.n, RVP_MEM_HOST))) return;
+  ok(rvp_octree_build(t));
+}
+
+std::size_t tree_search(rvp_octree *t, std::size_t n, const PointXYZ &query, float radius,
+                        std::vector<int> &indices, std::vector<float> &dists) {
+  indices.clear();
+  dists.clear();
+  if (!t || n == 0) return 0;
+  std::lock_guard<std::mutex> lock(g_mu);
+  int64_t offs[2] = {0, 0};
+  size_t cap = 256, total = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    indices.resize(cap);
+    dists.resize(cap);
+    const rvp_status s = rvp_octree_radius_search(t, &query.x, &query.y, &query.z, 1, radius,
+                                                  RVP_MEM_HOST, offs, indices.data(),
+                                                  dists.data(), cap, &total);
+    if (s == RVP_ERR_CAPACITY && attempt == 0) {
+      cap = total;
+      continue;
+    }
+    if (!ok(s)) total = 0;
+    break;
+  }
+  indices.resize(total);
+  dists.resize(total);
+  return total;
+}
+
+void tree_destroy(rvp_octree *t) {
+  if (t) rvp_octree_destroy(t);
+}
+
+}  // namespace
+
+Octree::Octree() = default;
+Octree::~Octree() { tree_destroy(t_); }
+// octree.cpp:28-30: the view is kept; build() reads the points
+void Octree::setInputCloud(const PointCloudSoA &cloud) { cloud_ = cloud; }
+void Octree::build() {
+  tree_build(t_, RVP_OCTREE, cloud_, max_points_per_leaf_, max_depth_, build_epsilon_);
+}
+std::size_t Octree::radiusSearch(const PointXYZ &query, float radius, std::vector<int> &indices,
+                                 std::vector<float> &dists, int max_nn) const {
+  (void)max_nn;  // octree.cpp:114
+  return tree_search(t_, cloud_.n, query, radius, indices, dists);
+}
+
+PointerOctree::PointerOctree() = default;
+PointerOctree::~PointerOctree() { tree_destroy(t_); }
+void PointerOctree::setInputCloud(const PointCloudSoA &cloud) { cloud_ = cloud; }
+void PointerOctree::build() {
+  tree_build(t_, RVP_POINTER_OCTREE, cloud_, max_points_per_leaf_, max_depth_, build_epsilon_);
+}
+std::size_t PointerOctree::radiusSearch(const PointXYZ &query, float radius,
+                                        std::vector<int> &indices,
+                                        std::vector<float> &dists) const {
+  return tree_search(t_, cloud_.n, query, radius, indices, dists);
+}
+std::size_t PointerOctree::radiusSearchScalar(const PointXYZ &query, float radius,
+                                              std::vector<int> &indices,
+                                              std::vector<float> &dists) const {
+  return tree_search(t_, cloud_.n, query, radius, indices, dists);
+}
+
 // ---- voxel grid (voxel_grid_downsamp.cpp) ----------------------------------
 std::size_t voxel_grid_downsamp_sc(const PointXYZ *in, std::size_t n, PointXYZ *out,
                                    float leaf_size) {
@@ -219,6 +295,30 @@ std::size_t sor_spatial_hash(const PointCloudSoA &in, const SpatialHash &hash, P
   return cnt;
 }
 
+namespace {
+std::size_t sor_tree(const PointCloudSoA &in, rvp_octree *t, PointXYZ *out, int k, float alpha,
+                     float search_radius) {
+  if (in.n == 0 || !t) return 0;
+  std::lock_guard<std::mutex> lock(g_mu);
+  size_t cnt = 0;
+  if (!ok(rvp_sor_octree(t, k, alpha, search_radius, RVP_MEM_HOST, reinterpret_cast<float *>(out),
+                         &cnt, nullptr, nullptr)))
+    return 0;
+  return cnt;
+}
+}  // namespace
+
+// `in` is the cloud `tree` was built on, as in the reference's callers
+std::size_t sor_octree(const PointCloudSoA &in, const Octree &tree, PointXYZ *out, int k,
+                       float alpha, float search_radius) {
+  return sor_tree(in, tree.device_tree(), out, k, alpha, search_radius);
+}
+
+std::size_t sor_pointer_octree(const PointCloudSoA &in, const PointerOctree &tree, PointXYZ *out,
+                               int k, float alpha, float search_radius) {
+  return sor_tree(in, tree.device_tree(), out, k, alpha, search_radius);
+}
+
 // ---- normals (normal_estimation.cpp) ---------------------------------------
 void normal_estimation_sc(const PointXYZ *in, std::size_t n, float *nx, float *ny, float *nz,
                           int k, float radius, float vp_x, float vp_y, float vp_z,
@@ -239,6 +339,37 @@ void normal_estimation_rvv(const PointCloudSoA &in, const SpatialHash &hash, flo
   std::lock_guard<std::mutex> lock(g_mu);
   ok(rvp_normals_radius(hash.device_hash(), radius, vp_x, vp_y, vp_z, eigen_iters, RVP_MEM_HOST,
                         nx, ny, nz));
+}
+
+namespace {
+void normals_tree(const PointCloudSoA &in, rvp_octree *t, float *nx, float *ny, float *nz,
+                  float radius, float vp_x, float vp_y, float vp_z, int eigen_iters) {
+  if (in.n == 0 || !t) return;
+  std::lock_guard<std::mutex> lock(g_mu);
+  ok(rvp_normals_octree(t, radius, vp_x, vp_y, vp_z, eigen_iters, RVP_MEM_HOST, nx, ny, nz));
+}
+}  // namespace
+
+void normal_estimation_rvv(const PointCloudSoA &in, const Octree &octree, float *nx, float *ny,
+                           float *nz, int k, float radius, float vp_x, float vp_y, float vp_z,
+                           int eigen_iters) {
+  (void)k;  // the radius search decides the neighbours, as in the reference
+  normals_tree(in, octree.device_tree(), nx, ny, nz, radius, vp_x, vp_y, vp_z, eigen_iters);
+}
+
+void normal_estimation_rvv(const PointCloudSoA &in, const PointerOctree &octree, float *nx,
+                           float *ny, float *nz, int k, float radius, float vp_x, float vp_y,
+                           float vp_z, int eigen_iters) {
+  (void)k;
+  normals_tree(in, octree.device_tree(), nx, ny, nz, radius, vp_x, vp_y, vp_z, eigen_iters);
+}
+
+void normal_estimation_rvv(const PointCloudSoA &in, float *nx, float *ny, float *nz, int k,
+                           float radius, float vp_x, float vp_y, float vp_z, int eigen_iters) {
+  PointerOctree octree;
+  octree.setInputCloud(in);
+  octree.build();
+  normal_estimation_rvv(in, octree, nx, ny, nz, k, radius, vp_x, vp_y, vp_z, eigen_iters);
 }
 
 // ---- RANSAC (ransac_plane.cpp) ---------------------------------------------
@@ -282,6 +413,16 @@ void EuclideanClustering::setInputCloud(const PointCloudSoA &cloud) { cloud_ = &
 void EuclideanClustering::setClusterTolerance(float tolerance) { clusterTolerance_ = tolerance; }
 void EuclideanClustering::setMinClusterSize(int min_size) { minClusterSize_ = min_size; }
 void EuclideanClustering::setMaxClusterSize(int max_size) { maxClusterSize_ = max_size; }
+// euclidean_clustering.cpp:35-43: a searcher built on the same cloud lists
+// the same neighbours, so the clusters do not depend on it
+void EuclideanClustering::setNeighborSearch(const Octree *search) {
+  searcher_ = search;
+  ptr_searcher_ = nullptr;
+}
+void EuclideanClustering::setNeighborSearch(const PointerOctree *search) {
+  ptr_searcher_ = search;
+  searcher_ = nullptr;
+}
 
 std::vector<ClusterIndices> EuclideanClustering::extract() const {
   std::vector<ClusterIndices> result;

@@ -48,8 +48,10 @@ def _arrays(buf, dtypes):
 
 
 def _angle(a, b):
-    c = np.abs(np.sum(a * b, 1)) / (np.linalg.norm(a, axis=1) * np.linalg.norm(b, axis=1) + 1e-30)
-    return np.arccos(np.clip(c, -1, 1))
+    """Angle between lines (sign-free), in double: atan2(|a x b|, |a . b|)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), np.abs(np.sum(a * b, 1)))
 
 
 @pytest.mark.gpu
@@ -117,3 +119,72 @@ def test_dropin_chain_matches_oracle(tmp_path, restatement):
     assert np.array_equal(coffs, np.cumsum([0] + [len(k) for k in cl]))
     assert np.array_equal(cidx, np.concatenate(cl))
     assert list(degen) == [0, 0, 1]
+
+
+def _build_octree_driver(tmp_path):
+    from rvpoint_b200 import build as B
+    B.build()
+    exe = str(tmp_path / "dropin_octree")
+    cmd = ["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include", "rvpoint"),
+           os.path.join(ROOT, "tests", "dropin_octree.cpp"), "-o", exe, "-L", LIBDIR,
+           "-lrvpoint_b200", "-Wl,-rpath," + LIBDIR]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_dropin_octree_compiles_and_links(tmp_path):
+    assert os.path.exists(_build_octree_driver(tmp_path))
+
+
+@pytest.mark.gpu
+def test_dropin_octree_matches_oracle(tmp_path, restatement):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rvpoint_b200 import api
+    exe = _build_octree_driver(tmp_path)
+    c = D.room_cloud(n=6000, seed=91)
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as f:
+        f.write(np.uint64(c.n).tobytes())
+        for a in (c.x, c.y, c.z):
+            f.write(np.ascontiguousarray(a, np.float32).tobytes())
+    outp = tmp_path / "out.bin"
+    r = subprocess.run([exe, str(inp), str(outp)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    f32, i32, i64 = np.float32, np.int32, np.int64
+    (cnt, li, ld, s0, s1, ox, oy, oz, px, py, pz, sx, sy, sz, coffs, cidx, threw) = _arrays(
+        outp.read_bytes(), [i64, i32, f32, f32, f32] + [f32] * 9 + [i64, i32, i64])
+    bits = lambda a: np.ascontiguousarray(a, np.float32).view(np.int32)  # noqa: E731
+    q = c.subset(np.arange(50))
+    pos = 0
+    for t, (kind, tree) in enumerate(((0, (16, 8, 1e-4)), (1, (64, 8, 1e-4)),
+                                      (1, (64, 8, 1e-4)))):
+        o, i, d = restatement.octree_radius(kind, c, 0.1, queries=q, tree=tree)
+        assert np.array_equal(cnt[50 * t:50 * t + 50], np.diff(o))
+        m = int(o[-1])
+        assert np.array_equal(li[pos:pos + m], i)
+        assert np.array_equal(bits(ld[pos:pos + m]), bits(d))
+        pos += m
+    r0, _, _ = restatement.sor_octree(0, c, 20, 1.0, 0.25, (16, 8, 1e-4))
+    r1, _, _ = restatement.sor_octree(1, c, 20, 1.0, 0.25)
+    assert np.array_equal(bits(s0), bits(r0.ravel()))
+    assert np.array_equal(bits(s1), bits(r1.ravel()))
+    # normals: the same GPU results as the Python API over the same trees
+    for (nx_, ny_, nz_), (kind, tree) in (((ox, oy, oz), (0, (16, 8, 1e-4))),
+                                          ((px, py, pz), (1, (64, 8, 1e-4))),
+                                          ((sx, sy, sz), (1, (64, 8, 1e-4)))):
+        t = (api.Octree if kind == 0 else api.PointerOctree)()
+        t.setMaxPointsPerLeaf(tree[0])
+        t.setInputCloud(c)
+        t.build()
+        g = np.stack(api.normal_estimation_tree(c, t, 10, 0.1), 1)
+        assert np.array_equal(bits(np.stack([nx_, ny_, nz_], 1)), bits(g))
+        f32n = restatement.normals_octree(kind, c, 0.1, tree=tree)
+        assert (_angle(g, f32n) < 1e-4).mean() > 0.99
+        t.close()
+    cl = restatement.euclidean_clusters(c, 0.05, 3)
+    assert np.array_equal(coffs, np.cumsum([0] + [len(k) for k in cl]))
+    assert np.array_equal(cidx, np.concatenate(cl))
+    assert int(threw[0]) == 1

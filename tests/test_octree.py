@@ -36,8 +36,10 @@ def _tree(api, kind, c, tree):
 
 
 def _angle_err(a, b):
-    c = np.abs(np.sum(a * b, 1)) / (np.linalg.norm(a, axis=1) * np.linalg.norm(b, axis=1) + 1e-30)
-    return np.arccos(np.clip(c, -1, 1))
+    """Angle between lines (sign-free), in double: atan2(|a x b|, |a . b|)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), np.abs(np.sum(a * b, 1)))
 
 
 def test_octree_entry_points_exported():
