@@ -567,7 +567,7 @@ namespace {
 rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const float *z,
                          const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
                          float cell_size, const uint32_t *cand, size_t n_cand, float *features,
-                         int lane_levels = 0) {
+                         int lane_levels = 0, float rfac = 1.0f) {
   rvp_context *ctx = s->ctx;
   return sguard(ctx, [&] {
     RVP_REQUIRE(x && y && z && frame_offsets_dev && features, "null pointer");
@@ -624,7 +624,7 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
     ta.hard_tau = hard_tau;
     ta.qlevel = s->qlevel.as<uint8_t>();
     ta.qtau = s->qtau.as<float>();
-    ta.rfac = 1.0f;
+    ta.rfac = rfac;
     ta.level0_warp = true;
     ta.preset_open = true;
     ta.lane_levels = lane_levels;
@@ -675,9 +675,11 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
   });
   if (st != RVP_OK) return st;
   const float *gx = s->cand_xyz.as<float>();
-  // sparse clouds: after one per-lane level the warp kernel is cheaper
+  // sparse clouds: after one per-lane level the warp kernel is cheaper, and
+  // the first pass bounded by the own cell's occupancy rarely certifies a
+  // query there (it scans the ring at once)
   return features_impl(s, gx, gx + n_cand, gx + 2 * n_cand, cand_offsets_dev, n_frames, n_cand,
-                       cell_size, nullptr, n_cand, features, 1);
+                       cell_size, nullptr, n_cand, features, 1, 0.0f);
 }
 
 

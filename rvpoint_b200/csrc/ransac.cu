@@ -53,6 +53,14 @@ __device__ __forceinline__ bool is_inlier(const float4 &m, float x, float y, flo
   return fabsf(fadd(fadd(fadd(fmul(m.x, x), fmul(m.y, y)), fmul(m.z, z)), m.w)) <= t;
 }
 
+// The same test with fused multiply-adds, for the preemptive ranking on the
+// candidates only: an estimate that orders hypotheses for the exact count,
+// which alone decides the result
+__device__ __forceinline__ bool is_inlier_fast(const float4 &m, float x, float y, float z,
+                                               float t) {
+  return fabsf(fmaf(m.x, x, fmaf(m.y, y, fmaf(m.z, z, m.w)))) <= t;
+}
+
 // One weighted draw: the candidate whose prefix-sum interval holds u * total,
 // returned relative to the frame's first point (a0).
 __device__ __forceinline__ u32 weighted_draw(const RansacSampler &smp, int f, int it, int k,
@@ -164,6 +172,10 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
     }
     __syncthreads();
 
+    // hypotheses to count: all of a full batch, else only the valid ones
+    // (given models past their end, or frames short of hypotheses, leave
+    // empty slots whose counts nothing reads)
+    const u32 vmask = __ballot_sync(0xffffffffu, hcode[lane] == 0);
     u32 acc = 0;  // lane h accumulates hypothesis h
     for (u32 p0 = (cr * NW + (u32)wid) * 32 * R_PTS; p0 < n; p0 += G * NW * 32 * R_PTS) {
       float px[R_PTS], py[R_PTS], pz[R_PTS];
@@ -176,14 +188,19 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
         py[r] = pv[r] ? __ldg(&y[i]) : 0.0f;
         pz[r] = pv[r] ? __ldg(&z[i]) : 0.0f;
       }
-#pragma unroll 4
-      for (int h = 0; h < HB; ++h) {
+      auto count = [&](int h) {
         const float4 m = hyp[h];
         u32 c = 0;
 #pragma unroll
         for (int r = 0; r < R_PTS; ++r)
           c += __popc(__ballot_sync(0xffffffffu, pv[r] && is_inlier(m, px[r], py[r], pz[r], prm.thresh)));
         if (lane == h) acc += c;
+      };
+      if (vmask == 0xffffffffu) {
+#pragma unroll 4
+        for (int h = 0; h < HB; ++h) count(h);
+      } else {
+        for (u32 b = vmask; b; b &= b - 1) count(__ffs(b) - 1);
       }
     }
     atomicAdd(&hcnt[lane], acc);
@@ -255,13 +272,16 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
 }
 
 // Preemptive round of the weighted proposal, one block per frame: draw
-// PE_H hypotheses from the frame's candidates by weight, count each one's
-// inliers among the candidates only (they sit in shared memory), and keep the
-// PE_KEEP best (count, then draw order) for the exact count over all points.
-// Frames that already reached their target write empty slots.
-constexpr int PE_THREADS = 256;
+// `draws` hypotheses from the frame's candidates by weight, count each one's
+// inliers among the candidates only (they sit in shared memory), and keep
+// the PE_KEEP best (count, then draw order) for the exact count over all
+// points. The candidate counts are an estimate that orders hypotheses (fused
+// multiply-adds); the exact count alone decides the result. Frames that
+// already reached their target write empty slots.
+constexpr int PE_THREADS = 1024;  // a frame's ranking spread wide: late rounds hold few frames
 constexpr int PE_MAXC = 2048;
 constexpr int PE_MAXH = 512;
+constexpr int PE_FIRST = 4;  // with targets: exact counts of the best-ranked few first
 __global__ __launch_bounds__(PE_THREADS) void k_preempt(
     const float *__restrict__ X, const float *__restrict__ Y, const float *__restrict__ Z,
     const int64_t *offs, RansacSampler smp, int draws, int round, RansacParams prm,
@@ -269,6 +289,8 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt(
   __shared__ float4 P[PE_MAXC];
   __shared__ float4 hyp[PE_MAXH];
   __shared__ int hcnt[PE_MAXH];
+  __shared__ int hist[PE_MAXC / 2 + 2];  // counts in pairs: (count + 1) >> 1
+  __shared__ int s_thr;
   const int f = blockIdx.x;
   const int64_t a0 = offs[f];
   const u32 n = (u32)(offs[f + 1] - a0);
@@ -276,11 +298,9 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt(
   const int m = (int)(c1 - c0);
   float4 *o = out + (size_t)f * PE_KEEP;
   const float4 none = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);
+  for (int t = threadIdx.x; t < PE_KEEP; t += blockDim.x) o[t] = none;
   const bool done = smp.targets && best_now && best_now[f] >= smp.targets[f];
-  if (done || n < 3 || m < 3 || m > PE_MAXC || !(smp.cdf[c1 - 1] > 0.0)) {
-    for (int t = threadIdx.x; t < PE_KEEP; t += blockDim.x) o[t] = none;
-    return;
-  }
+  if (done || n < 3 || m < 3 || m > PE_MAXC || !(smp.cdf[c1 - 1] > 0.0)) return;
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
     const u32 g = smp.cand[c0 + j];
     P[j] = make_float4(X[g], Y[g], Z[g], 0.0f);
@@ -297,20 +317,56 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt(
                       prm.collinear, mdl))
       mdl = none;
     hyp[h] = mdl;
+    hcnt[h] = isnan(mdl.x) ? -1 : 0;
   }
+  const int nbins = ((m + 1) >> 1) + 1;
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) hist[b] = 0;
   __syncthreads();
-  for (int h = threadIdx.x; h < draws; h += blockDim.x) {
+  // S threads per hypothesis, each over every S-th candidate (a warp shares
+  // the slice, so its lanes read the same candidate: a shared-memory
+  // broadcast); the integer counts add up to the same totals in any order
+  const int S = max(1, (int)blockDim.x / draws);
+  const int slots = draws * S;
+  for (int u = threadIdx.x; u < slots; u += blockDim.x) {
+    const int h = u % draws, sl = u / draws;
     const float4 mdl = hyp[h];
-    int c = -1;
-    if (!isnan(mdl.x)) {
-      c = 0;
-      for (int j = 0; j < m; ++j) c += is_inlier(mdl, P[j].x, P[j].y, P[j].z, prm.thresh) ? 1 : 0;
-    }
-    hcnt[h] = c;
+    if (isnan(mdl.x)) continue;
+    int c = 0;
+    for (int j = sl; j < m; j += S)
+      c += is_inlier_fast(mdl, P[j].x, P[j].y, P[j].z, prm.thresh) ? 1 : 0;
+    if (c) atomicAdd(&hcnt[h], c);
   }
   __syncthreads();
+  // rank = #(greater count) + #(equal count, earlier draw). Only the
+  // hypotheses at or above the PE_KEEP-th largest count can rank below
+  // PE_KEEP: a histogram of the counts finds that count first.
+  for (int h = threadIdx.x; h < draws; h += blockDim.x) atomicAdd(&hist[(hcnt[h] + 1) >> 1], 1);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int above = 0, thr = 0;  // thr: histogram bin; 0 keeps every hypothesis
+    for (int top = nbins - 1; top >= 0; top -= 32) {
+      const int bb = top - lane;
+      int sfx = bb >= 0 ? hist[bb] : 0;  // becomes the sum of bins top .. bb
+#pragma unroll
+      for (int sh = 1; sh < 32; sh <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, sfx, sh);
+        if (lane >= sh) sfx += t;
+      }
+      const unsigned hit = __ballot_sync(0xffffffffu, bb >= 0 && above + sfx >= PE_KEEP);
+      if (hit) {
+        thr = top - (__ffs(hit) - 1);
+        break;
+      }
+      above += __shfl_sync(0xffffffffu, sfx, 31);
+    }
+    if (lane == 0) s_thr = thr;
+  }
+  __syncthreads();
+  const int cthr = 2 * s_thr - 1;  // the lowest count of bin s_thr
   for (int h = threadIdx.x; h < draws; h += blockDim.x) {
     const int c = hcnt[h];
+    if (c < cthr) continue;
     int rank = 0;
     for (int g = 0; g < draws; ++g) {
       const int cg = hcnt[g];
@@ -323,10 +379,10 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt(
 // draws_run of the frames that stop after this round (reached their
 // target, or the last round); open counts the others
 __global__ void k_preempt_done(const int32_t *best, const int32_t *targets, int n_frames,
-                               int round, int draws, bool last, int32_t *draws_run, int *open) {
+                               int drawn, bool last, int32_t *draws_run, int *open) {
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < n_frames; f += gridDim.x * blockDim.x) {
     if (draws_run[f] >= 0) continue;
-    if (last || (targets && best[f] >= targets[f])) draws_run[f] = (round + 1) * draws;
+    if (last || (targets && best[f] >= targets[f])) draws_run[f] = drawn;
     else atomicAdd(open, 1);
   }
 }
@@ -439,11 +495,27 @@ void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const f
     sm.n_models = PE_KEEP;
     sm.best_in = r > 0 ? best : nullptr;
     sm.model_in = r > 0 ? model : nullptr;
-    ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, pe, model, best, dummy_iters, nullptr,
-                  false, sm, 8);
+    if (smp0.targets) {
+      // the best-ranked PE_FIRST first: most frames reach their target
+      // there; the others go on with the rest, in the same rank order (so
+      // the result is the single pass's)
+      RansacParams p1 = pe;
+      p1.max_iters = PE_FIRST;
+      ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, p1, model, best, dummy_iters, nullptr,
+                    false, sm, 8);
+      sm.models = models + PE_FIRST;
+      sm.best_in = best;
+      sm.model_in = model;
+      p1.max_iters = PE_KEEP - PE_FIRST;
+      ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, p1, model, best, dummy_iters, nullptr,
+                    false, sm, 8);
+    } else {
+      ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, pe, model, best, dummy_iters, nullptr,
+                    false, sm, 8);
+    }
     RVP_CUDA_TRY(cudaMemsetAsync(open, 0, 4, st));
     k_preempt_done<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(
-        best, smp0.targets, n_frames, r, draws, r + 1 == max_rounds, draws_run, open);
+        best, smp0.targets, n_frames, (r + 1) * draws, r + 1 == max_rounds, draws_run, open);
     RVP_LAUNCH_CHECK(ctx);
     if (smp0.targets) {
       int h_open = 0;

@@ -244,7 +244,7 @@ def plane_labels(b: DeviceBatch, models: torch.Tensor, thresh: float,
 class TrainConfig:
     thresh: float = 0.02          # RANSAC inlier distance (m)
     label_iters: int = 10_000     # plain RANSAC hypotheses behind the labels
-    cell: float = 3.0             # grid cell of the feature kNN (m; speed only)
+    cell: float = 2.5             # grid cell of the feature kNN (m; speed only)
     cand_per_frame: int = 1024    # feature points per frame
     scope: str = "candidates"     # feature neighbourhoods: "candidates" or "points"
     steps: int = 400
@@ -283,7 +283,7 @@ def train(scorer: PlaneScorer, b: DeviceBatch, cfg: TrainConfig = TrainConfig())
 class LearnedRansac:
     """features -> MLP -> weighted RANSAC over every frame of a batch."""
 
-    def __init__(self, scorer: PlaneScorer, cell: float = 3.0, cand_per_frame: int = 1024,
+    def __init__(self, scorer: PlaneScorer, cell: float = 2.5, cand_per_frame: int = 1024,
                  logit_power: float = 1.0, seed: int = 11, scope: str = "candidates",
                  preemptive: bool = True, draws: int = 512):
         """preemptive: hypotheses ranked among the candidates first, the best
