@@ -19,6 +19,11 @@ line): 512 plane scenes of 50,000 points; plain GPU RANSAC (10,000
 hypotheses, the reference's stream and stopping rule) against the learned
 proposal (features + MLP + weighted RANSAC) to 99% of plain's best count.
 
+Rank 0 also times the calls around the path (``next_rows``): PCD input,
+PointerOctree SOR and normals and Euclidean clustering on the reference
+pipeline driver's settings, through the public API with host arrays, beside
+the reference's own CPU code on the same input (one thread).
+
 N > 1: launched by torch.distributed.run, one rank per GPU; every rank owns
 its own 256 frames (weak scaling, no data-path collective); time = max over
 ranks.
@@ -60,6 +65,8 @@ def parse():
     ap.add_argument("--lane-levels", type=int, default=2,
                     help="grid levels of the one-query-per-lane kNN with --cell")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--no-next-rows", action="store_true",
+                    help="skip the PCD / octree / clustering timings")
     ap.add_argument("--learned-scenes", type=int, default=512,
                     help="plane scenes of the learned-vs-plain RANSAC leg (0: skip)")
     return ap.parse_args()
@@ -240,6 +247,96 @@ def kernel_bytes(name: str, n_vox: int, n_sor: int, n_frames: int) -> float:
     if kind == "ransac":
         return 12.0 * n_sor + 4.0 * R_ITERS * n_frames
     raise ValueError(name)
+
+
+def _write_pcd_binary(path: str, x, y, z) -> None:
+    """A PCD file of fields x y z, DATA binary (io/simple_pcd_loader.h)."""
+    import numpy as np
+    n = int(x.shape[0])
+    head = ("# .PCD v.7 - Point Cloud Data file format\nVERSION .7\nFIELDS x y z\n"
+            "SIZE 4 4 4\nTYPE F F F\nCOUNT 1 1 1\n"
+            f"WIDTH {n}\nHEIGHT 1\nVIEWPOINT 0 0 0 1 0 0 0\nPOINTS {n}\nDATA binary\n")
+    with open(path, "wb") as f:
+        f.write(head.encode())
+        f.write(np.ascontiguousarray(np.stack([x, y, z], 1), np.float32).tobytes())
+
+
+def next_rows_leg(ctx, batch) -> dict:
+    """The calls around the hot path on the reference pipeline driver's
+    settings (pipeline_export.cpp:37-67): loadPCD of the batch (binary),
+    then on a 100k-point room cloud thinned by voxel 0.01: PointerOctree
+    build + sor_pointer_octree (k 20, std 1, radius 0.25), PointerOctree
+    normals (radius 0.03), Euclidean clustering (tolerance 0.15, 50 to
+    100,000 points; the reference's quadratic search on a 20,000-point
+    subset, the GPU on the same subset and on the whole cloud). GPU times are
+    wall clock around the public API call with host arrays in and out; the
+    CPU times are the reference's own code (oracle/_ref), one thread."""
+    import numpy as np
+    from oracle import oracle as O
+    from rvpoint_b200 import api
+    from rvpoint_b200 import datasets as D
+    if not O.reference_available():
+        return {"unavailable": "reference library not built"}
+    R = O.Reference()
+    out = {}
+
+    def wall(fn, reps=3):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = fn()
+        return (time.perf_counter() - t0) / reps * 1e3, r
+
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "batch.pcd")
+        _write_pcd_binary(path, batch.x, batch.y, batch.z)
+        n = int(batch.x.shape[0])
+        g_ms, _ = wall(lambda: api.load_pcd(path, device=True, ctx=ctx))
+        c_ms, _ = wall(lambda: R.load_pcd(path, n), reps=1)
+        out["pcd_load_binary"] = {"points": n, "bytes": os.path.getsize(path),
+                                  "gpu_ms": g_ms, "cpu_ms": c_ms,
+                                  "gpu_mpts_s": n / g_ms / 1e3, "cpu_mpts_s": n / c_ms / 1e3,
+                                  "note": "file in page cache; GPU: into device arrays"}
+    v = api.voxel_grid_downsamp_rvv_v2(D.room_cloud(n=100_000), 0.01, ctx=ctx)
+    c = D.Cloud.from_xyz(v)
+    nv = c.n
+
+    def gpu_sor():
+        t = api.PointerOctree(ctx)
+        t.setInputCloud(c)
+        t.build()
+        r = api.sor_pointer_octree(c, t, 20, 1.0, 0.25)
+        t.close()
+        return r
+    g_ms, g_out = wall(gpu_sor)
+    c_ms, c_out = wall(lambda: R.sor_octree(1, c, 20, 1.0, 0.25), reps=1)
+    same = bool(np.array_equal(np.ascontiguousarray(g_out).view(np.int32),
+                               np.ascontiguousarray(c_out).view(np.int32)))
+    out["sor_pointer_octree"] = {"points": nv, "gpu_ms": g_ms, "cpu_ms": c_ms,
+                                 "speedup": c_ms / g_ms, "kept": int(g_out.shape[0]),
+                                 "bit_exact": same}
+
+    def gpu_normals():
+        t = api.PointerOctree(ctx)
+        t.setInputCloud(c)
+        t.build()
+        r = api.normal_estimation_tree(c, t, 10, 0.03)
+        t.close()
+        return r
+    g_ms, _ = wall(gpu_normals)
+    c_ms, _ = wall(lambda: R.normals_octree(1, c, 0.03), reps=1)
+    out["normals_pointer_octree"] = {"points": nv, "gpu_ms": g_ms, "cpu_ms": c_ms,
+                                     "speedup": c_ms / g_ms}
+    sub = c.subset(np.arange(min(nv, 20_000)))
+    g_ms, g_cl = wall(lambda: api.euclidean_clusters(sub, 0.15, 50, 100_000, ctx=ctx))
+    c_ms, c_cl = wall(lambda: R.euclidean_clusters(sub, 0.15, 50, 100_000), reps=1)
+    same = len(g_cl) == len(c_cl) and all(np.array_equal(a, b) for a, b in zip(g_cl, c_cl))
+    gf_ms, _ = wall(lambda: api.euclidean_clusters(c, 0.15, 50, 100_000, ctx=ctx))
+    out["euclidean_clustering"] = {"points": int(sub.n), "gpu_ms": g_ms, "cpu_ms": c_ms,
+                                   "speedup": c_ms / g_ms, "clusters": len(g_cl),
+                                   "same_clusters": same, "gpu_ms_full_cloud": gf_ms,
+                                   "full_cloud_points": nv}
+    return out
 
 
 def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
@@ -488,6 +585,7 @@ def main():
 
     cpu = cpu_baseline(batch, a.cpu_budget_s) if world == 1 else None
     learned = learned_leg(ctx, a.learned_scenes, 64) if a.learned_scenes > 0 else None
+    nxt = next_rows_leg(ctx, batch) if world == 1 and not a.no_next_rows else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -500,7 +598,7 @@ def main():
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps, "clocks": clk,
             "stages_ms": {k: v for k, v in stages.items() if k != "runs"},
-            "graph": graph, "learned_ransac": learned}
+            "graph": graph, "learned_ransac": learned, "next_rows": nxt}
     print(json.dumps(line), flush=True)
 
 

@@ -36,20 +36,29 @@ struct rvp_octree {
   int kind = RVP_OCTREE;
   int cap = 64, depth = 8;
   float eps = 1e-4f;
+  // the tree itself: its copy of the cloud and every point's rank
   rvp::DevBuf x, y, z, offs, rank, order, root;
   size_t n = 0;
   bool has_cloud = false, built = false;
   float box[6] = {0, 0, 0, 0, 0, 0};  // root box (host copy)
-  rvp::Grid grid;
-  float grid_cell = -1.0f;
-  // working buffers (grow-only)
-  rvp::DevBuf keys, vals, sortb, cnt, loffs, pairs, pairs2, big, scan, work, stage[6];
 };
 
 namespace rvp {
 namespace {
 
-inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
+// Working buffers live in the context's one-shot scratch (grow-only, shared
+// by the entry points of a context, which run one at a time), and the radius
+// grid is the context's shared grid: a tree made per call, as the
+// reference's callers do, allocates only its own ranks.
+enum {
+  W_KEYS = 0, W_VALS, W_SORT, W_CNT, W_LOFFS, W_PAIRS, W_PAIRS2, W_BIG, W_SCAN, W_WORK,
+  W_STAGE  // W_STAGE + 0..5: staged inputs and outputs
+};
+inline DevBuf &wb(rvp_context *ctx, int slot) { return ctx->scratch[slot]; }
+inline Grid &ctx_grid(rvp_context *ctx) {
+  if (!ctx->grid) ctx->grid = new Grid();
+  return *ctx->grid;
+}
 
 constexpr int kMaxDepth = 21;  // 3 bits per level in a 64-bit key
 
@@ -365,18 +374,18 @@ T oct_read(rvp_context *ctx, const T *dev) {
 template <class T>
 const T *oct_in(rvp_octree *o, int slot, const T *p, size_t n, int mem) {
   if (mem == RVP_MEM_DEVICE || n == 0) return p;
-  o->stage[slot].reserve(n * sizeof(T));
-  RVP_CUDA_TRY(cudaMemcpyAsync(o->stage[slot].ptr, p, n * sizeof(T), cudaMemcpyHostToDevice,
-                               o->ctx->stream));
-  return o->stage[slot].as<T>();
+  DevBuf &b = wb(o->ctx, W_STAGE + slot);
+  b.reserve(n * sizeof(T));
+  RVP_CUDA_TRY(cudaMemcpyAsync(b.ptr, p, n * sizeof(T), cudaMemcpyHostToDevice, o->ctx->stream));
+  return b.as<T>();
 }
 
 template <class T>
 T *oct_out(rvp_octree *o, int slot, T *p, size_t n, int mem) {
   if (p == nullptr) return nullptr;
   if (mem == RVP_MEM_DEVICE) return p;
-  o->stage[slot].reserve((n ? n : 1) * sizeof(T));
-  return o->stage[slot].as<T>();
+  wb(o->ctx, W_STAGE + slot).reserve((n ? n : 1) * sizeof(T));
+  return wb(o->ctx, W_STAGE + slot).as<T>();
 }
 
 template <class T>
@@ -386,9 +395,9 @@ void oct_copy(rvp_octree *o, T *user, const T *dev, size_t n, int mem) {
 }
 
 void sort_pairs(rvp_octree *o, u64 *keys, u32 *vals, size_t n) {
-  o->sortb.reserve(sort_temp_bytes(n));
+  wb(o->ctx, W_SORT).reserve(sort_temp_bytes(n));
   SortTemp st;
-  sort_temp_carve(st, o->sortb.ptr, n);
+  sort_temp_carve(st, wb(o->ctx, W_SORT).ptr, n);
   radix_sort_pairs(o->ctx, keys, vals, n, nullptr, st);
 }
 
@@ -406,26 +415,27 @@ u64 oct_lists(rvp_octree *o, const float *qx, const float *qy, const float *qz, 
   const float cmin = ext > 0.0f ? ext / 1048576.0f : 0.0f;
   if (!(cell >= cmin)) cell = cmin;
   if (!(cell > 0.0f)) cell = 1.0f;
-  if (cell != o->grid_cell) {
-    grid_build(ctx, o->grid, o->x.as<float>(), o->y.as<float>(), o->z.as<float>(),
-               o->offs.as<int64_t>(), 1, o->n, cell, KEY_DENSE, 0, 0, nullptr);
-    o->grid_cell = cell;
-  }
-  const GridView gv = o->grid.view(KEY_DENSE, 0, 0);
+  Grid &grid = ctx_grid(ctx);
+  grid_build(ctx, grid, o->x.as<float>(), o->y.as<float>(), o->z.as<float>(),
+             o->offs.as<int64_t>(), 1, o->n, cell, KEY_DENSE, 0, 0, nullptr);
+  const GridView gv = grid.view(KEY_DENSE, 0, 0);
   QuerySet qs{qx, qy, qz, nq, nullptr, nullptr, nullptr};
-  o->cnt.reserve(nq * 4 + 16);
-  u32 *cnt = o->cnt.as<u32>();
+  DevBuf &bcnt = wb(ctx, W_CNT), &boffs = wb(ctx, W_LOFFS), &bscan = wb(ctx, W_SCAN);
+  bcnt.reserve(nq * 4 + 16);
+  u32 *cnt = bcnt.as<u32>();
   grid_radius_count(ctx, gv, qs, radius, false, cnt);
-  o->loffs.reserve((nq + 1) * 8);
-  u64 *offs = o->loffs.as<u64>();
-  o->scan.reserve(scan_temp_bytes(nq + 1));
-  exclusive_scan_u32_to_u64(ctx, cnt, offs, nq, nullptr, o->scan.ptr);
+  boffs.reserve((nq + 1) * 8);
+  u64 *offs = boffs.as<u64>();
+  bscan.reserve(scan_temp_bytes(nq + 1));
+  exclusive_scan_u32_to_u64(ctx, cnt, offs, nq, nullptr, bscan.ptr);
   const u64 tot = oct_read(ctx, offs + nq);
-  if (tot >= 0xFFFFFFFFull) throw Error{RVP_ERR_INVALID_ARG, "radius lists exceed 2^32 - 1 entries"};
-  o->pairs.reserve((tot ? tot : 1) * 8);
-  u64 *pairs = o->pairs.as<u64>();
-  o->big.reserve(nq * 4 + 16);
-  u32 *big = o->big.as<u32>();
+  if (tot >= 0xFFFFFFFFull)
+    throw Error{RVP_ERR_INVALID_ARG, "radius lists exceed 2^32 - 1 entries"};
+  DevBuf &bpairs = wb(ctx, W_PAIRS), &bbig = wb(ctx, W_BIG);
+  bpairs.reserve((tot ? tot : 1) * 8);
+  u64 *pairs = bpairs.as<u64>();
+  bbig.reserve(nq * 4 + 16);
+  u32 *big = bbig.as<u32>();
   grid_radius_fill(ctx, gv, qs, radius, false, offs, 0, pairs, big, big + nq);
   if (!by_rank) {
     sort_big_segments(ctx, offs, pairs, big, big + nq, (u32)std::min<size_t>(nq, 4096));
@@ -434,17 +444,18 @@ u64 oct_lists(rvp_octree *o, const float *qx, const float *qy, const float *qz, 
     return tot;
   }
   if (tot) {
-    o->keys.reserve(tot * 8);
-    o->vals.reserve(tot * 4);
+    DevBuf &bkeys = wb(ctx, W_KEYS), &bvals = wb(ctx, W_VALS), &bp2 = wb(ctx, W_PAIRS2);
+    bkeys.reserve(tot * 8);
+    bvals.reserve(tot * 4);
     k_oct_list_keys<<<grid_for(nq * 32, 256, ctx->num_sms * 32), 256, 0, st>>>(
-        pairs, offs, nq, o->rank.as<u32>(), o->keys.as<u64>(), o->vals.as<u32>());
+        pairs, offs, nq, o->rank.as<u32>(), bkeys.as<u64>(), bvals.as<u32>());
     RVP_LAUNCH_CHECK(ctx);
-    sort_pairs(o, o->keys.as<u64>(), o->vals.as<u32>(), tot);
-    o->pairs2.reserve(tot * 8);
-    k_gather_u64<<<grid_for(tot, 256, ctx->num_sms * 16), 256, 0, st>>>(
-        pairs, o->vals.as<u32>(), tot, o->pairs2.as<u64>());
+    sort_pairs(o, bkeys.as<u64>(), bvals.as<u32>(), tot);
+    bp2.reserve(tot * 8);
+    k_gather_u64<<<grid_for(tot, 256, ctx->num_sms * 16), 256, 0, st>>>(pairs, bvals.as<u32>(),
+                                                                        tot, bp2.as<u64>());
     RVP_LAUNCH_CHECK(ctx);
-    pairs = o->pairs2.as<u64>();
+    pairs = bp2.as<u64>();
   }
   *offs_out = offs;
   *pairs_out = pairs;
@@ -470,12 +481,7 @@ rvp_status rvp_octree_destroy(rvp_octree *o) {
   if (!o) return RVP_ERR_INVALID_ARG;
   cudaSetDevice(o->ctx->device);
   cudaStreamSynchronize(o->ctx->stream);
-  for (DevBuf *b : {&o->x, &o->y, &o->z, &o->offs, &o->rank, &o->order, &o->root, &o->keys,
-                    &o->vals, &o->sortb, &o->cnt, &o->loffs, &o->pairs, &o->pairs2, &o->big,
-                    &o->scan, &o->work})
-    b->release();
-  for (DevBuf &b : o->stage) b.release();
-  o->grid.release();
+  for (DevBuf *b : {&o->x, &o->y, &o->z, &o->offs, &o->rank, &o->order, &o->root}) b->release();
   delete o;
   return RVP_OK;
 }
@@ -519,7 +525,6 @@ rvp_status rvp_octree_set_input_cloud(rvp_octree *o, const float *x, const float
     o->n = n;
     o->has_cloud = true;
     o->built = false;
-    o->grid_cell = -1.0f;
   });
 }
 
@@ -531,7 +536,6 @@ rvp_status rvp_octree_build(rvp_octree *o) {
     RVP_CUDA_TRY(cudaSetDevice(ctx->device));
     const size_t n = o->n;
     o->built = true;
-    o->grid_cell = -1.0f;
     if (n == 0) return;  // octree.cpp:35: no root, every search returns 0
     cudaStream_t st = ctx->stream;
     const int D = o->depth > 0 ? o->depth : 0;
@@ -548,17 +552,17 @@ rvp_status rvp_octree_build(rvp_octree *o) {
     k_oct_root<<<1, 32, 0, st>>>(enc, o->kind, o->eps, root);
     RVP_LAUNCH_CHECK(ctx);
     RVP_CUDA_TRY(cudaMemcpyAsync(o->box, root, 24, cudaMemcpyDeviceToHost, st));
-    o->keys.reserve(n * 8);
-    o->vals.reserve(n * 4);
-    u64 *keys = o->keys.as<u64>();
-    u32 *vals = o->vals.as<u32>();
+    wb(o->ctx, W_KEYS).reserve(n * 8);
+    wb(o->ctx, W_VALS).reserve(n * 4);
+    u64 *keys = wb(o->ctx, W_KEYS).as<u64>();
+    u32 *vals = wb(o->ctx, W_VALS).as<u32>();
     k_oct_keys<<<gb, 256, 0, st>>>(o->x.as<float>(), o->y.as<float>(), o->z.as<float>(), n, root,
                                    D, keys, vals);
     RVP_LAUNCH_CHECK(ctx);
     sort_pairs(o, keys, vals, n);
     // leaf keys by point index, then the stable sort of (leaf key, index)
-    o->pairs.reserve(n * 8);
-    u64 *leaf = o->pairs.as<u64>();
+    wb(o->ctx, W_PAIRS).reserve(n * 8);
+    u64 *leaf = wb(o->ctx, W_PAIRS).as<u64>();
     k_oct_leaf<<<gb, 256, 0, st>>>(keys, vals, n, D, cap, leaf);
     RVP_LAUNCH_CHECK(ctx);
     RVP_CUDA_TRY(cudaMemcpyAsync(keys, leaf, n * 8, cudaMemcpyDeviceToDevice, st));
@@ -662,20 +666,22 @@ rvp_status rvp_sor_octree(rvp_octree *o, int k, float alpha, float search_radius
     const u64 tot = oct_lists(o, x, y, z, n, search_radius, nth, &offs, &pairs);
     float *mean = oct_out(o, 0, mean_dists, n, mem);
     if (!mean) {
-      o->stage[0].reserve(n * 4);
-      mean = o->stage[0].as<float>();
+      wb(o->ctx, W_STAGE + 0).reserve(n * 4);
+      mean = wb(o->ctx, W_STAGE + 0).as<float>();
     }
-    if (nth) o->work.reserve((tot ? tot : 1) * 4);
+    DevBuf &work = wb(ctx, W_WORK);
+    if (nth) work.reserve((tot ? tot : 1) * 4);
     k_oct_sor_mean<<<grid_for(n, 128, ctx->num_sms * 16), 128, 0, st>>>(
-        pairs, offs, n, k, search_radius, nth, nth ? o->work.as<float>() : nullptr, mean);
+        pairs, offs, n, k, search_radius, nth, nth ? work.as<float>() : nullptr, mean);
     RVP_LAUNCH_CHECK(ctx);
     uint8_t *dkeep = oct_out(o, 1, keep, n, mem);
     float *dout = oct_out(o, 2, out_aos, 3 * n, mem);
-    o->stage[3].reserve(64);
-    int64_t *so = o->stage[3].as<int64_t>();
-    o->stage[4].reserve(sor_filter_temp_bytes(n, 1));
+    wb(ctx, W_STAGE + 3).reserve(64);
+    int64_t *so = wb(ctx, W_STAGE + 3).as<int64_t>();
+    DevBuf &tmp = wb(ctx, W_STAGE + 4);
+    tmp.reserve(sor_filter_temp_bytes(n, 1));
     sor_filter_frames(ctx, x, y, z, mean, o->offs.as<int64_t>(), 1, n, nullptr, alpha, dkeep,
-                      dout, so, nullptr, o->stage[4].ptr, nullptr, nullptr, nullptr, nullptr);
+                      dout, so, nullptr, tmp.ptr, nullptr, nullptr, nullptr, nullptr);
     int64_t hs[2];
     RVP_CUDA_TRY(cudaMemcpyAsync(hs, so, 16, cudaMemcpyDeviceToHost, st));
     oct_sync(ctx);

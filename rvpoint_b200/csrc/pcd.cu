@@ -5,8 +5,10 @@
 // COUNT defaults to 1). The payload goes to the device in the form the file
 // holds it and is split there:
 //   binary             records of all fields back to back: the records are
-//                      copied up and one thread per point picks x, y, z from
-//                      its record (the AoS -> SoA transpose runs on the GPU);
+//                      read in chunks into pinned buffers and copied up while
+//                      the next chunk is read; one thread per point picks
+//                      x, y, z from its record (the AoS -> SoA transpose runs
+//                      on the GPU);
 //   binary_compressed  one LZF block holding each field's column in turn:
 //                      decoded on the host (LZF is a sequential byte stream),
 //                      then the x, y, z columns are copied up as they are;
@@ -15,6 +17,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -178,18 +181,48 @@ extern "C" rvp_status rvp_pcd_load(rvp_context *ctx, const char *path, int mem, 
       stride += (size_t)h.sizes[i] * (size_t)h.counts[i];
     }
     if (h.data == "binary") {
-      std::vector<unsigned char> raw(stride * n);
-      f.read(reinterpret_cast<char *>(raw.data()), (std::streamsize)raw.size());
-      RVP_REQUIRE((size_t)f.gcount() == raw.size(), "short binary PCD payload");
       if (mem == RVP_MEM_DEVICE) {
+        // the records go up as they lie in the file: read in chunks into two
+        // pinned buffers, each chunk's copy overlapping the next read
+        const size_t total = stride * n;
         DevBuf &d = ctx->scratch[29];
-        d.reserve(raw.size());
-        RVP_CUDA_TRY(cudaMemcpyAsync(d.ptr, raw.data(), raw.size(), cudaMemcpyHostToDevice, st));
+        d.reserve(total);
+        constexpr size_t CH = (size_t)8 << 20;
+        HostBuf *hb[2] = {&ctx->pinned[0], &ctx->pinned[1]};
+        hb[0]->reserve(CH);
+        hb[1]->reserve(CH);
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        struct Events {  // destroyed on every way out
+          cudaEvent_t *e;
+          ~Events() {
+            for (int i = 0; i < 2; ++i)
+              if (e[i]) cudaEventDestroy(e[i]);
+          }
+        } guard_ev{ev};
+        for (int i = 0; i < 2; ++i)
+          RVP_CUDA_TRY(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+        size_t i = 0;
+        for (size_t at = 0; at < total; at += CH, ++i) {
+          const size_t len = std::min(CH, total - at);
+          HostBuf &b = *hb[i & 1];
+          if (i >= 2) RVP_CUDA_TRY(cudaEventSynchronize(ev[i & 1]));  // its last copy is done
+          f.read(static_cast<char *>(b.ptr), (std::streamsize)len);
+          if ((size_t)f.gcount() != len) {
+            RVP_CUDA_TRY(cudaStreamSynchronize(st));
+            throw Error{RVP_ERR_INVALID_ARG, "short binary PCD payload"};
+          }
+          RVP_CUDA_TRY(cudaMemcpyAsync(d.as<unsigned char>() + at, b.ptr, len,
+                                       cudaMemcpyHostToDevice, st));
+          RVP_CUDA_TRY(cudaEventRecord(ev[i & 1], st));
+        }
         k_pcd_records<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, st>>>(
             d.as<unsigned char>(), n, stride, off[xi], off[yi], off[zi], x, y, z);
         RVP_LAUNCH_CHECK(ctx);
         RVP_CUDA_TRY(cudaStreamSynchronize(st));
       } else {
+        std::vector<unsigned char> raw(stride * n);
+        f.read(reinterpret_cast<char *>(raw.data()), (std::streamsize)raw.size());
+        RVP_REQUIRE((size_t)f.gcount() == raw.size(), "short binary PCD payload");
         for (size_t i = 0; i < n; ++i) {
           const unsigned char *r = raw.data() + i * stride;
           memcpy(&x[i], r + off[xi], 4);
