@@ -357,6 +357,19 @@ RVP_API rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const 
                                  int64_t *sor_offsets, float *nx, float *ny,
                                  float *nz, float *ransac_model,
                                  int32_t *ransac_count);
+/* rvp_pipeline_run_host over n_batches batches in a row (every argument an
+ * array of n_batches entries; output entries may be NULL). Batch i + 1 goes
+ * up into a second device input set while batch i runs, and batch i's
+ * results come down while batch i + 1 runs, so the copies hide behind the
+ * work; outputs are the ones rvp_pipeline_run_host writes, bit for bit.
+ * Host arrays should be pinned for the copies to overlap. Synchronizes at
+ * the end. */
+RVP_API rvp_status rvp_pipeline_run_host_batches(
+    rvp_pipeline *p, int n_batches, const float *const *x, const float *const *y,
+    const float *const *z, const int64_t *const *frame_offsets, const int *n_frames,
+    float *const *voxel_aos, int64_t *const *voxel_offsets, float *const *sor_aos,
+    int64_t *const *sor_offsets, float *const *nx, float *const *ny, float *const *nz,
+    float *const *ransac_model, int32_t *const *ransac_count);
 /* Copies the results of the last run (run_device, replay or run_host) of
  * the last n_frames to host arrays, sized and laid out as for
  * rvp_pipeline_run_host (any pointer may be NULL); synchronizes. */

@@ -89,6 +89,7 @@ SIGNATURES = {
     "rvp_pipeline_copy_outputs": (I, [P] * 10),
     "rvp_pipeline_outputs_get": (I, [P, C.POINTER(PipelineOutputs)]),
     "rvp_pipeline_run_host": (I, [P, P, P, P, P, I, P, P, P, P, P, P, P, P, P]),
+    "rvp_pipeline_run_host_batches": (I, [P, I] + [P] * 14),
     "rvp_pipeline_set_timing": (I, [P, I]),
     "rvp_pipeline_set_tuning": (I, [P, F, I, I]),
     "rvp_pipeline_set_search_radius_factor": (I, [P, F]),

@@ -830,6 +830,48 @@ class Pipeline:
                     normals=np.stack([nx[:ns], ny[:ns], nz[:ns]], 1), ransac_model=model,
                     ransac_count=cnt)
 
+    def run_host_batches(self, batches):
+        """Several host batches in a row (rvp_pipeline_run_host_batches: the
+        next batch goes up and the previous results come down while a batch
+        runs). Returns one result dict per batch, as run_host."""
+        self.ctx.set_stream(0)
+        nb = len(batches)
+        arrs = {k: [] for k in ("x", "y", "z", "o", "vox", "vo", "sor", "so", "nx", "ny", "nz",
+                                "m", "c")}
+        nfs = []
+        for b in batches:
+            x, y, z = _f32(b.x), _f32(b.y), _f32(b.z)
+            offs = np.ascontiguousarray(b.offsets, dtype=np.int64)
+            nf = int(offs.shape[0] - 1)
+            n = int(offs[-1])
+            nfs.append(nf)
+            for k, v in (("x", x), ("y", y), ("z", z), ("o", offs),
+                         ("vox", np.empty((max(n, 1), 3), np.float32)),
+                         ("vo", np.empty(nf + 1, np.int64)),
+                         ("sor", np.empty((max(n, 1), 3), np.float32)),
+                         ("so", np.empty(nf + 1, np.int64)),
+                         ("nx", np.empty(max(n, 1), np.float32)),
+                         ("ny", np.empty(max(n, 1), np.float32)),
+                         ("nz", np.empty(max(n, 1), np.float32)),
+                         ("m", np.empty((nf, 4), np.float32)), ("c", np.empty(nf, np.int32))):
+                arrs[k].append(v)
+        ptrs = {k: (C.c_void_p * nb)(*[a.ctypes.data for a in v]) for k, v in arrs.items()}
+        nfa = (C.c_int * nb)(*nfs)
+        self.last_frames = nfs[-1] if nfs else 0
+        check(self.L.rvp_pipeline_run_host_batches(
+            self.h, nb, ptrs["x"], ptrs["y"], ptrs["z"], ptrs["o"], nfa, ptrs["vox"], ptrs["vo"],
+            ptrs["sor"], ptrs["so"], ptrs["nx"], ptrs["ny"], ptrs["nz"], ptrs["m"], ptrs["c"]),
+            self.ctx.h)
+        out = []
+        for i in range(nb):
+            nv, ns = int(arrs["vo"][i][-1]), int(arrs["so"][i][-1])
+            out.append(dict(voxel=arrs["vox"][i][:nv], voxel_offsets=arrs["vo"][i],
+                            sor=arrs["sor"][i][:ns], sor_offsets=arrs["so"][i],
+                            normals=np.stack([arrs["nx"][i][:ns], arrs["ny"][i][:ns],
+                                              arrs["nz"][i][:ns]], 1),
+                            ransac_model=arrs["m"][i], ransac_count=arrs["c"][i]))
+        return out
+
     def results(self, max_points: int | None = None) -> dict:
         """Per-frame results of the last run, copied to numpy."""
         nf = int(self.last_frames)

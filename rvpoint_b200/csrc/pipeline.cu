@@ -52,6 +52,15 @@ struct rvp_pipeline {
   bool record_stages = false;
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};
   cudaStream_t s_out = nullptr, s_meta = nullptr;
+  // run_host_batches: a second input set (batch i + 1 goes up while batch i
+  // runs), the copy-in stream, and events for the copies; wait_before holds
+  // the events run_device waits for at the voxel, SOR-filter, normal and
+  // RANSAC stages (the previous batch's results of that stage are down)
+  rvp::DevBuf in2_x, in2_y, in2_z, in2_offs;
+  cudaStream_t s_in = nullptr;
+  cudaEvent_t ev_h2d[2] = {nullptr, nullptr};
+  cudaEvent_t ev_end = nullptr, ev_dv = nullptr, ev_ds = nullptr, ev_dn = nullptr;
+  cudaEvent_t wait_before[4] = {nullptr, nullptr, nullptr, nullptr};
   // stage timing: a ring of event sets, one set per run
   // (stage boundaries, then a pair around each grid level's kNN kernel: SOR
   // levels 0-2, normals levels 0-2)
@@ -224,6 +233,10 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
     if (e) cudaEventDestroy(e);
   if (p->s_out) cudaStreamDestroy(p->s_out);
   if (p->s_meta) cudaStreamDestroy(p->s_meta);
+  if (p->s_in) cudaStreamDestroy(p->s_in);
+  for (cudaEvent_t e : {p->ev_h2d[0], p->ev_h2d[1], p->ev_end, p->ev_dv, p->ev_ds, p->ev_dn})
+    if (e) cudaEventDestroy(e);
+  for (auto *b : {&p->in2_x, &p->in2_y, &p->in2_z, &p->in2_offs}) b->release();
   delete p;
   return RVP_OK;
 }
@@ -249,6 +262,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     const u64 *n_sor = reinterpret_cast<const u64 *>(sor_offs + n_frames);
 
     p->mark(0);
+    if (p->wait_before[0]) RVP_CUDA_TRY(cudaStreamWaitEvent(st, p->wait_before[0], 0));
     // 1) voxel grid
     const float inv_leaf = 1.0f / c.leaf_size;
     rvp::voxel_grid_run(ctx, p->vw, x, y, z, offs, n_frames, N, nullptr, inv_leaf,
@@ -326,6 +340,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                     rvp::KNN_OUT_SOR_MEAN, p->mean.as<float>());
     }
     p->mark(3);
+    if (p->wait_before[1]) RVP_CUDA_TRY(cudaStreamWaitEvent(st, p->wait_before[1], 0));
     rvp::sor_filter_frames(ctx, p->vox_x.as<float>(), p->vox_y.as<float>(), p->vox_z.as<float>(),
                            p->mean.as<float>(), vox_offs, n_frames, N, n_vox, c.sor_alpha,
                            p->keep.as<uint8_t>(), p->sor_aos.as<float>(), sor_offs, nullptr,
@@ -334,6 +349,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     const u64 *sor_pos = rvp::sor_positions(p->sor_tmp.ptr, N);
     p->mark(4);
     if (p->record_stages) RVP_CUDA_TRY(cudaEventRecord(p->ev_stage[1], st));
+    if (p->wait_before[2]) RVP_CUDA_TRY(cudaStreamWaitEvent(st, p->wait_before[2], 0));
     // 4) normals: the k+1 nearest kept points of every kept point, with the
     //    reference normal computed in the same tile kernel
     k_mark_removed<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(
@@ -384,6 +400,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                             p->nx.as<float>(), p->ny.as<float>(), p->nz.as<float>(), hard,
                             sor_pos);
     p->mark(6);
+    if (p->wait_before[3]) RVP_CUDA_TRY(cudaStreamWaitEvent(st, p->wait_before[3], 0));
     // 5) RANSAC per frame on the kept points
     double pc = (double)c.ransac_prob;
     pc = pc < 0.5 ? 0.5 : (pc > 0.9999 ? 0.9999 : pc);
@@ -681,6 +698,126 @@ rvp_status rvp_pipeline_run_host(rvp_pipeline *p, const float *x, const float *y
   if (s != RVP_OK) {
     cudaStreamSynchronize(p->s_out);
     cudaStreamSynchronize(ctx->stream);
+  }
+  return s;
+}
+
+rvp_status rvp_pipeline_run_host_batches(
+    rvp_pipeline *p, int n_batches, const float *const *x, const float *const *y,
+    const float *const *z, const int64_t *const *frame_offsets, const int *n_frames,
+    float *const *voxel_aos, int64_t *const *voxel_offsets, float *const *sor_aos,
+    int64_t *const *sor_offsets, float *const *nx, float *const *ny, float *const *nz,
+    float *const *ransac_model, int32_t *const *ransac_count) {
+  if (!p || n_batches < 0) return RVP_ERR_INVALID_ARG;
+  if (n_batches == 0) return RVP_OK;
+  rvp_context *ctx = p->ctx;
+  cudaStream_t st = ctx->stream;
+  rvp_status s = guard(ctx, [&] {
+    RVP_REQUIRE(x && y && z && frame_offsets && n_frames, "null batch arrays");
+    for (int i = 0; i < n_batches; ++i) {
+      RVP_REQUIRE(frame_offsets[i] && n_frames[i] >= 1 && n_frames[i] <= p->max_frames,
+                  "bad frames");
+      const size_t n = (size_t)frame_offsets[i][n_frames[i]];
+      RVP_REQUIRE(n <= p->max_points, "batch exceeds the pipeline capacity");
+      RVP_REQUIRE(n == 0 || (x[i] && y[i] && z[i]), "null pointer");
+    }
+    RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    if (!p->s_out) {
+      RVP_CUDA_TRY(cudaStreamCreateWithFlags(&p->s_out, cudaStreamNonBlocking));
+      RVP_CUDA_TRY(cudaStreamCreateWithFlags(&p->s_meta, cudaStreamNonBlocking));
+      for (auto &e : p->ev_stage) RVP_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (!p->s_in) {
+      RVP_CUDA_TRY(cudaStreamCreateWithFlags(&p->s_in, cudaStreamNonBlocking));
+      for (cudaEvent_t *e : {&p->ev_h2d[0], &p->ev_h2d[1], &p->ev_end, &p->ev_dv, &p->ev_ds,
+                             &p->ev_dn})
+        RVP_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    const size_t N = p->max_points, F1 = (size_t)p->max_frames + 1;
+    p->in2_x.reserve(N * 4); p->in2_y.reserve(N * 4); p->in2_z.reserve(N * 4);
+    p->in2_offs.reserve(F1 * 8);
+  });
+  if (s != RVP_OK) return s;
+  rvp::DevBuf *in[2][4] = {{&p->in_x, &p->in_y, &p->in_z, &p->in_offs},
+                           {&p->in2_x, &p->in2_y, &p->in2_z, &p->in2_offs}};
+  auto h2d = [&](int i) {  // batch i into input set i % 2, on the copy-in stream
+    rvp::DevBuf **b = in[i & 1];
+    const size_t n = (size_t)frame_offsets[i][n_frames[i]];
+    if (n) {
+      RVP_CUDA_TRY(cudaMemcpyAsync(b[0]->ptr, x[i], n * 4, cudaMemcpyHostToDevice, p->s_in));
+      RVP_CUDA_TRY(cudaMemcpyAsync(b[1]->ptr, y[i], n * 4, cudaMemcpyHostToDevice, p->s_in));
+      RVP_CUDA_TRY(cudaMemcpyAsync(b[2]->ptr, z[i], n * 4, cudaMemcpyHostToDevice, p->s_in));
+    }
+    RVP_CUDA_TRY(cudaMemcpyAsync(b[3]->ptr, frame_offsets[i], (n_frames[i] + 1) * 8,
+                                 cudaMemcpyHostToDevice, p->s_in));
+    RVP_CUDA_TRY(cudaEventRecord(p->ev_h2d[i & 1], p->s_in));
+  };
+  auto pick = [&](auto *const *arr, int i) { return arr ? arr[i] : nullptr; };
+  for (int i = 0; i < n_batches && s == RVP_OK; ++i) {
+    s = guard(ctx, [&] {
+      if (i == 0) {
+        RVP_CUDA_TRY(cudaEventRecord(p->ev_end, st));  // earlier work on the stream
+        RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_in, p->ev_end, 0));
+        h2d(0);
+      }
+      if (i + 1 < n_batches) {
+        // input set (i + 1) % 2 is free once batch i - 1's voxel stage is done
+        if (i >= 1) RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_in, p->ev_stage[0], 0));
+        h2d(i + 1);
+      }
+      RVP_CUDA_TRY(cudaStreamWaitEvent(st, p->ev_h2d[i & 1], 0));
+      cudaEvent_t w[4] = {p->ev_dv, p->ev_ds, p->ev_dn, p->ev_dn};
+      for (int k = 0; k < 4; ++k) p->wait_before[k] = i > 0 ? w[k] : nullptr;
+    });
+    if (s != RVP_OK) break;
+    rvp::DevBuf **b = in[i & 1];
+    const size_t n = (size_t)frame_offsets[i][n_frames[i]];
+    p->record_stages = true;
+    s = rvp_pipeline_run_device(p, b[0]->as<float>(), b[1]->as<float>(), b[2]->as<float>(),
+                                b[3]->as<int64_t>(), n_frames[i], n);
+    p->record_stages = false;
+    for (auto &e : p->wait_before) e = nullptr;
+    if (s != RVP_OK) break;
+    s = guard(ctx, [&] {
+      const int nf = n_frames[i];
+      RVP_CUDA_TRY(cudaEventRecord(p->ev_end, st));
+      std::vector<int64_t> vo(nf + 1), so(nf + 1);
+      auto d2h = [&](void *dst, const void *src, size_t bytes) {
+        if (dst && bytes)
+          RVP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, p->s_out));
+      };
+      RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_meta, p->ev_stage[0], 0));
+      RVP_CUDA_TRY(cudaMemcpyAsync(vo.data(), p->vox_offs.ptr, (nf + 1) * 8,
+                                   cudaMemcpyDeviceToHost, p->s_meta));
+      RVP_CUDA_TRY(cudaStreamSynchronize(p->s_meta));
+      if (pick(voxel_offsets, i)) memcpy(voxel_offsets[i], vo.data(), (nf + 1) * 8);
+      RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_out, p->ev_stage[0], 0));
+      d2h(pick(voxel_aos, i), p->vox_aos.ptr, (size_t)vo[nf] * 12);
+      RVP_CUDA_TRY(cudaEventRecord(p->ev_dv, p->s_out));
+      RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_meta, p->ev_stage[1], 0));
+      RVP_CUDA_TRY(cudaMemcpyAsync(so.data(), p->sor_offs.ptr, (nf + 1) * 8,
+                                   cudaMemcpyDeviceToHost, p->s_meta));
+      RVP_CUDA_TRY(cudaStreamSynchronize(p->s_meta));
+      const size_t ns = (size_t)so[nf];
+      if (pick(sor_offsets, i)) memcpy(sor_offsets[i], so.data(), (nf + 1) * 8);
+      RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_out, p->ev_stage[1], 0));
+      d2h(pick(sor_aos, i), p->sor_aos.ptr, ns * 12);
+      RVP_CUDA_TRY(cudaEventRecord(p->ev_ds, p->s_out));
+      RVP_CUDA_TRY(cudaStreamWaitEvent(p->s_out, p->ev_end, 0));
+      d2h(pick(nx, i), p->nx.ptr, ns * 4);
+      d2h(pick(ny, i), p->ny.ptr, ns * 4);
+      d2h(pick(nz, i), p->nz.ptr, ns * 4);
+      d2h(pick(ransac_model, i), p->r_model.ptr, (size_t)nf * 16);
+      d2h(pick(ransac_count, i), p->r_best.ptr, (size_t)nf * 4);
+      RVP_CUDA_TRY(cudaEventRecord(p->ev_dn, p->s_out));
+    });
+  }
+  const cudaError_t e1 = cudaStreamSynchronize(p->s_out);
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  const cudaError_t e3 = p->s_in ? cudaStreamSynchronize(p->s_in) : cudaSuccess;
+  if (s == RVP_OK && (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)) {
+    ctx->last_error = "batched host run: CUDA error";
+    return RVP_ERR_CUDA;
   }
   return s;
 }

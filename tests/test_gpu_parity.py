@@ -514,3 +514,26 @@ def test_euclidean_clusters_match_oracle_larger(gpu_ctx, restatement):
     assert len(got) == len(ref) and all(np.array_equal(u, v) for u, v in zip(got, ref))
     e = np.zeros(0, np.float32)
     assert api.euclidean_clusters((e, e, e), 0.3, ctx=gpu_ctx) == []
+
+
+@pytest.mark.gpu
+def test_pipeline_host_batches_equal_single_runs(gpu_ctx):
+    """rvp_pipeline_run_host_batches (inputs double-buffered, results coming
+    down while the next batch runs) returns, batch by batch, what
+    rvp_pipeline_run_host returns for each batch alone: batches of different
+    sizes in a row, one repeated."""
+    from rvpoint_b200 import api
+    bs = [D.lidar_batch(n_frames=4, seed=s, min_pts=20000, max_pts=80000) for s in (31, 32, 33)]
+    seq = [bs[0], bs[1], bs[0], bs[2]]
+    cap_n = max(b.n for b in bs)
+    p = api.Pipeline(max_points=cap_n, max_frames=4)
+    ref = {id(b): p.run_host(b) for b in bs}
+    outs = p.run_host_batches(seq)
+    assert len(outs) == len(seq)
+    for b, out in zip(seq, outs):
+        r = ref[id(b)]
+        for key in ("voxel", "sor", "normals", "ransac_model"):
+            assert np.array_equal(bits(out[key]), bits(r[key])), key
+        for key in ("voxel_offsets", "sor_offsets", "ransac_count"):
+            assert np.array_equal(out[key], r[key]), key
+    p.close()
