@@ -267,8 +267,14 @@ __global__ __launch_bounds__(TB) void k_mlp_train(const float *__restrict__ feat
                                                   const float *__restrict__ labels, size_t n,
                                                   size_t n_src, u64 sample_seed,
                                                   const __nv_bfloat16 *__restrict__ wq,
-                                                  const float *__restrict__ norm, float *grad,
-                                                  double *loss_sum) {
+                                                  const float *__restrict__ norm, float *part,
+                                                  double *part_loss) {
+  // part: this block's gradient (NP floats at blockIdx.x * NP), part_loss
+  // its loss sum; every entry is written by one thread, and the blocks'
+  // shares are added in block order afterwards (k_grad_reduce): the same
+  // batch always gives the same gradient
+  __shared__ double warp_loss[TB / 32];
+  float *grad = part + (size_t)blockIdx.x * NP;
   extern __shared__ __align__(16) float sm[];
   float *sw = sm;
   float *snorm = sw + NP + 3;
@@ -371,21 +377,42 @@ __global__ __launch_bounds__(TB) void k_mlp_train(const float *__restrict__ feat
   {
     const int j = tid >> 1, h0 = (tid & 1) * 32;
 #pragma unroll
-    for (int r = 0; r < 32; ++r) atomicAdd(&grad[OW2 + j * MH + h0 + r], gw2[r]);
+    for (int r = 0; r < 32; ++r) grad[OW2 + j * MH + h0 + r] = gw2[r];
     const int h = tid >> 1, k0 = (tid & 1) * 4;
 #pragma unroll
-    for (int r = 0; r < 4; ++r) atomicAdd(&grad[OW1 + h * MI + k0 + r], gw1[r]);
+    for (int r = 0; r < 4; ++r) grad[OW1 + h * MI + k0 + r] = gw1[r];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const int v = tid + e * TB;
       if (v > 3 * MH) continue;
       const int dst = v < MH ? OB1 + v : (v < 2 * MH ? OB2 + v - MH : (v < 3 * MH ? OW3 + v - 2 * MH : OB3));
-      atomicAdd(&grad[dst], gv[e]);
+      grad[dst] = gv[e];
     }
   }
-  // loss: warp sums, one double atomic per warp
+  // loss: warp sums, then the warps in order
   for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
-  if ((tid & 31) == 0) atomicAdd(loss_sum, (double)loss);
+  if ((tid & 31) == 0) warp_loss[tid >> 5] = (double)loss;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < TB / 32; ++w) t += warp_loss[w];
+    part_loss[blockIdx.x] = t;
+  }
+}
+
+// the blocks' gradient shares and losses, added in block order
+__global__ void k_grad_reduce(const float *part, const double *part_loss, int blocks, float *grad,
+                              double *loss_sum) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < NP; p += gridDim.x * blockDim.x) {
+    float t = 0.0f;
+    for (int b = 0; b < blocks; ++b) t += part[(size_t)b * NP + p];
+    grad[p] = t;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double t = 0.0;
+    for (int b = 0; b < blocks; ++b) t += part_loss[b];
+    *loss_sum = t;
+  }
 }
 
 __global__ void k_adam(float *w, const float *g, float *m, float *v, int n, float lr, float b1,
@@ -459,6 +486,7 @@ struct rvp_scorer {
   rvp::DevBuf frame_of, is_cand, pairs, counts, hard, qlevel, qtau, open;
   rvp::DevBuf w, wq, m, v, grad, norm, loss;
   rvp::DevBuf cand_xyz;  // candidates' own coordinates (neighbours among candidates)
+  rvp::DevBuf gpart;     // per-block gradient shares of a training step
   int adam_step = 0;
   size_t fitted_points = 0;  // batch size and cell the bucket table was fitted to
   float fitted_cell = 0.0f;
@@ -556,7 +584,7 @@ rvp_status rvp_scorer_destroy(rvp_scorer *s) {
   cudaStreamSynchronize(s->ctx->stream);
   rvp::DevBuf *bufs[] = {&s->frame_of, &s->is_cand, &s->pairs, &s->counts, &s->hard, &s->qlevel,
                          &s->qtau, &s->open, &s->w, &s->wq, &s->m, &s->v, &s->grad, &s->norm,
-                         &s->loss, &s->cand_xyz};
+                         &s->loss, &s->cand_xyz, &s->gpart};
   for (auto *b : bufs) b->release();
   s->grid.release();
   delete s;
@@ -742,13 +770,18 @@ namespace {
 void mlp_grad(rvp_scorer *s, const float *features, const float *labels, size_t n,
               size_t n_src = 0, u64 sample_seed = 0) {
   rvp_context *ctx = s->ctx;
-  RVP_CUDA_TRY(cudaMemsetAsync(s->grad.ptr, 0, rvp::NP * 4, ctx->stream));
-  RVP_CUDA_TRY(cudaMemsetAsync(s->loss.ptr, 0, 8, ctx->stream));
   const unsigned blocks =
       (unsigned)std::min<size_t>((n + rvp::TB - 1) / rvp::TB, (size_t)ctx->num_sms);
+  s->gpart.reserve((size_t)blocks * rvp::NP * 4 + (size_t)blocks * 8 + 256);
+  float *part = s->gpart.as<float>();
+  double *part_loss = reinterpret_cast<double *>(
+      s->gpart.as<char>() + (((size_t)blocks * rvp::NP * 4 + 255) & ~(size_t)255));
   rvp::k_mlp_train<<<blocks, rvp::TB, rvp::TRAIN_SMEM, ctx->stream>>>(
       features, labels, n, n_src ? n_src : n, sample_seed, s->wq.as<__nv_bfloat16>(),
-      s->norm.as<float>(), s->grad.as<float>(), s->loss.as<double>());
+      s->norm.as<float>(), part, part_loss);
+  RVP_LAUNCH_CHECK(ctx);
+  rvp::k_grad_reduce<<<(rvp::NP + 255) / 256, 256, 0, ctx->stream>>>(
+      part, part_loss, (int)blocks, s->grad.as<float>(), s->loss.as<double>());
   RVP_LAUNCH_CHECK(ctx);
 }
 }  // namespace

@@ -271,43 +271,53 @@ __global__ __launch_bounds__(R_THREADS) void k_ransac(
   }
 }
 
-// Preemptive round of the weighted proposal, one block per frame: draw
-// `draws` hypotheses from the frame's candidates by weight, count each one's
-// inliers among the candidates only (they sit in shared memory), and keep
-// the PE_KEEP best (count, then draw order) for the exact count over all
-// points. The candidate counts are an estimate that orders hypotheses (fused
-// multiply-adds); the exact count alone decides the result. Frames that
-// already reached their target write empty slots.
-constexpr int PE_THREADS = 1024;  // a frame's ranking spread wide: late rounds hold few frames
+// Preemptive round of the weighted proposal, in two kernels. k_preempt_count:
+// block (frame, slice) draws the slice's share of the round's `draws`
+// hypotheses from the frame's candidates by weight and counts each one's
+// inliers among the candidates only (they sit in shared memory); a round
+// with few open frames splits each frame over several slices (blocks).
+// k_preempt_rank: per frame, the PE_KEEP best (count, then draw order) for
+// the exact count over all points. The candidate counts are an estimate that
+// orders hypotheses (fused multiply-adds); the exact count alone decides the
+// result. Frames that already reached their target write empty slots.
+constexpr int PE_THREADS = 1024;
 constexpr int PE_MAXC = 2048;
 constexpr int PE_MAXH = 512;
-constexpr int PE_FIRST = 4;  // with targets: exact counts of the best-ranked few first
-__global__ __launch_bounds__(PE_THREADS) void k_preempt(
+constexpr int PE_FIRST = 4;   // with targets: exact counts of the best-ranked few first
+constexpr int PE_SLICES = 8;  // blocks per frame in the rounds after the first
+
+__device__ __forceinline__ bool pe_skip(const RansacSampler &smp, const int64_t *offs,
+                                        const int32_t *best_now, int f) {
+  const u32 n = (u32)(offs[f + 1] - offs[f]);
+  const int64_t c0 = smp.cand_offs[f], c1 = smp.cand_offs[f + 1];
+  const int m = (int)(c1 - c0);
+  const bool done = smp.targets && best_now && best_now[f] >= smp.targets[f];
+  return done || n < 3 || m < 3 || m > PE_MAXC || !(smp.cdf[c1 - 1] > 0.0);
+}
+
+__global__ __launch_bounds__(PE_THREADS) void k_preempt_count(
     const float *__restrict__ X, const float *__restrict__ Y, const float *__restrict__ Z,
-    const int64_t *offs, RansacSampler smp, int draws, int round, RansacParams prm,
-    const int32_t *best_now, float4 *out) {
+    const int64_t *offs, RansacSampler smp, int draws, int slices, int round, RansacParams prm,
+    const int32_t *best_now, float4 *hyp_out, int *cnt_out) {
   __shared__ float4 P[PE_MAXC];
   __shared__ float4 hyp[PE_MAXH];
   __shared__ int hcnt[PE_MAXH];
-  __shared__ int hist[PE_MAXC / 2 + 2];  // counts in pairs: (count + 1) >> 1
-  __shared__ int s_thr;
-  const int f = blockIdx.x;
+  const int f = blockIdx.x / slices, sl = blockIdx.x % slices;
+  const int dg = (draws + slices - 1) / slices, h0 = sl * dg;
+  const int nh = min(draws, h0 + dg) - h0;
+  if (nh <= 0 || pe_skip(smp, offs, best_now, f)) return;
   const int64_t a0 = offs[f];
   const u32 n = (u32)(offs[f + 1] - a0);
-  const int64_t c0 = smp.cand_offs[f], c1 = smp.cand_offs[f + 1];
-  const int m = (int)(c1 - c0);
-  float4 *o = out + (size_t)f * PE_KEEP;
+  const int64_t c0 = smp.cand_offs[f];
+  const int m = (int)(smp.cand_offs[f + 1] - c0);
   const float4 none = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);
-  for (int t = threadIdx.x; t < PE_KEEP; t += blockDim.x) o[t] = none;
-  const bool done = smp.targets && best_now && best_now[f] >= smp.targets[f];
-  if (done || n < 3 || m < 3 || m > PE_MAXC || !(smp.cdf[c1 - 1] > 0.0)) return;
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
     const u32 g = smp.cand[c0 + j];
     P[j] = make_float4(X[g], Y[g], Z[g], 0.0f);
   }
   const float *x = X + a0, *y = Y + a0, *z = Z + a0;
-  for (int h = threadIdx.x; h < draws; h += blockDim.x) {
-    const int it = round * draws + h;
+  for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+    const int it = round * draws + h0 + h;
     const u32 i1 = weighted_draw(smp, f, it, 0, a0, n);
     const u32 i2 = weighted_draw(smp, f, it, 1, a0, n);
     const u32 i3 = weighted_draw(smp, f, it, 2, a0, n);
@@ -319,27 +329,48 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt(
     hyp[h] = mdl;
     hcnt[h] = isnan(mdl.x) ? -1 : 0;
   }
-  const int nbins = ((m + 1) >> 1) + 1;
-  for (int b = threadIdx.x; b < nbins; b += blockDim.x) hist[b] = 0;
   __syncthreads();
   // S threads per hypothesis, each over every S-th candidate (a warp shares
-  // the slice, so its lanes read the same candidate: a shared-memory
-  // broadcast); the integer counts add up to the same totals in any order
-  const int S = max(1, (int)blockDim.x / draws);
-  const int slots = draws * S;
+  // the slice of candidates, so its lanes read the same candidate: a
+  // shared-memory broadcast); integer counts add up the same in any order
+  const int S = max(1, (int)blockDim.x / nh);
+  const int slots = nh * S;
   for (int u = threadIdx.x; u < slots; u += blockDim.x) {
-    const int h = u % draws, sl = u / draws;
+    const int h = u % nh, cs = u / nh;
     const float4 mdl = hyp[h];
     if (isnan(mdl.x)) continue;
     int c = 0;
-    for (int j = sl; j < m; j += S)
+    for (int j = cs; j < m; j += S)
       c += is_inlier_fast(mdl, P[j].x, P[j].y, P[j].z, prm.thresh) ? 1 : 0;
     if (c) atomicAdd(&hcnt[h], c);
   }
   __syncthreads();
-  // rank = #(greater count) + #(equal count, earlier draw). Only the
-  // hypotheses at or above the PE_KEEP-th largest count can rank below
-  // PE_KEEP: a histogram of the counts finds that count first.
+  for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+    hyp_out[(size_t)f * PE_MAXH + h0 + h] = hyp[h];
+    cnt_out[(size_t)f * PE_MAXH + h0 + h] = hcnt[h];
+  }
+}
+
+// rank = #(greater count) + #(equal count, earlier draw). Only the
+// hypotheses at or above the PE_KEEP-th largest count can rank below
+// PE_KEEP: a histogram of the counts finds that count first.
+constexpr int PR_THREADS = 512;
+__global__ __launch_bounds__(PR_THREADS) void k_preempt_rank(
+    const int64_t *offs, RansacSampler smp, int draws, const int32_t *best_now,
+    const float4 *hyp_in, const int *cnt_in, float4 *out) {
+  __shared__ int hcnt[PE_MAXH];
+  __shared__ int hist[PE_MAXC / 2 + 2];  // counts in pairs: (count + 1) >> 1
+  __shared__ int s_thr;
+  const int f = blockIdx.x;
+  float4 *o = out + (size_t)f * PE_KEEP;
+  const float4 none = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);
+  for (int t = threadIdx.x; t < PE_KEEP; t += blockDim.x) o[t] = none;
+  if (pe_skip(smp, offs, best_now, f)) return;
+  const int m = (int)(smp.cand_offs[f + 1] - smp.cand_offs[f]);
+  const int nbins = ((m + 1) >> 1) + 1;
+  for (int h = threadIdx.x; h < draws; h += blockDim.x) hcnt[h] = cnt_in[(size_t)f * PE_MAXH + h];
+  for (int b = threadIdx.x; b < nbins; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
   for (int h = threadIdx.x; h < draws; h += blockDim.x) atomicAdd(&hist[(hcnt[h] + 1) >> 1], 1);
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -372,7 +403,7 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt(
       const int cg = hcnt[g];
       rank += (cg > c || (cg == c && g < h)) ? 1 : 0;
     }
-    if (rank < PE_KEEP) o[rank] = c >= 0 ? hyp[h] : none;
+    if (rank < PE_KEEP) o[rank] = c >= 0 ? hyp_in[(size_t)f * PE_MAXH + h] : none;
   }
 }
 
@@ -481,24 +512,34 @@ void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const f
   float4 *models = reinterpret_cast<float4 *>(sp);
   int *open = reinterpret_cast<int *>(sp + al((size_t)n_frames * PE_KEEP * 16));
   int32_t *dummy_iters = reinterpret_cast<int32_t *>(sp + al((size_t)n_frames * PE_KEEP * 16) + 256);
+  char *sp2 = sp + al((size_t)n_frames * PE_KEEP * 16) + 256 + al((size_t)n_frames * 4);
+  float4 *hyp_all = reinterpret_cast<float4 *>(sp2);  // a round's hypotheses, PE_MAXH per frame
+  int *cnt_all = reinterpret_cast<int *>(sp2 + al((size_t)n_frames * PE_MAXH * 16));
   cudaStream_t st = ctx->stream;
   k_fill_i32<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(draws_run, n_frames, -1);
   RVP_LAUNCH_CHECK(ctx);
   RansacParams pe = p;
   pe.max_iters = PE_KEEP;
   for (int r = 0; r < max_rounds; ++r) {
-    k_preempt<<<n_frames, PE_THREADS, 0, st>>>(x, y, z, offs, smp0, draws, r, p,
-                                               r > 0 ? best : nullptr, models);
+    // the first round holds every frame; later ones only the frames still
+    // short of their target, each spread over PE_SLICES blocks
+    const int slices = r == 0 ? 1 : PE_SLICES;
+    k_preempt_count<<<(unsigned)n_frames * slices, PE_THREADS, 0, st>>>(
+        x, y, z, offs, smp0, draws, slices, r, p, r > 0 ? best : nullptr, hyp_all, cnt_all);
+    RVP_LAUNCH_CHECK(ctx);
+    k_preempt_rank<<<n_frames, PR_THREADS, 0, st>>>(offs, smp0, draws, r > 0 ? best : nullptr,
+                                                    hyp_all, cnt_all, models);
     RVP_LAUNCH_CHECK(ctx);
     RansacSampler sm = smp0;
     sm.models = models;
     sm.n_models = PE_KEEP;
     sm.best_in = r > 0 ? best : nullptr;
     sm.model_in = r > 0 ? model : nullptr;
-    if (smp0.targets) {
+    if (smp0.targets && r == 0) {
       // the best-ranked PE_FIRST first: most frames reach their target
       // there; the others go on with the rest, in the same rank order (so
-      // the result is the single pass's)
+      // the result is the single pass's). Later rounds hold the frames the
+      // first could not finish, which rarely stop within the first few.
       RansacParams p1 = pe;
       p1.max_iters = PE_FIRST;
       ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, p1, model, best, dummy_iters, nullptr,
@@ -527,7 +568,8 @@ void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const f
 }
 
 size_t preemptive_temp_bytes(int n_frames) {
-  return al((size_t)n_frames * PE_KEEP * 16) + 256 + al((size_t)n_frames * 4);
+  return al((size_t)n_frames * PE_KEEP * 16) + 256 + al((size_t)n_frames * 4) +
+         al((size_t)n_frames * PE_MAXH * 16) + al((size_t)n_frames * PE_MAXH * 4);
 }
 
 size_t extract_temp_bytes(size_t n) {

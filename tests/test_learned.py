@@ -114,6 +114,34 @@ def test_training_lowers_the_loss(gpu_ctx):
 
 
 @pytest.mark.gpu
+def test_training_is_deterministic(gpu_ctx):
+    """The blocks' gradient shares are added in block order (no float
+    atomics): the same data, start and seeds give bit-identical weights."""
+    import torch
+    from rvpoint_b200.learned import PlaneScorer
+    rng = np.random.default_rng(10)
+    n = 50000
+    feat = rng.normal(size=(n, 8)).astype(np.float32)
+    y = (feat[:, 2] > 0.3).astype(np.float32)
+    fd, yd = torch.from_numpy(feat).cuda(), torch.from_numpy(y).cuda()
+    out = []
+    for _ in range(2):
+        s = PlaneScorer(n, 1, ctx=gpu_ctx)
+        s.set_norm(np.zeros(8, np.float32), np.ones(8, np.float32))
+        s.set_params(rng_params := np.random.default_rng(3).normal(
+            scale=0.1, size=s.get_params().shape).astype(np.float32))
+        for k in range(20):
+            s.train_step(fd, yd, 3e-3, batch=8192, seed=k + 1)
+        loss, g = s.gradients(fd, yd)
+        out.append((s.get_params(), g, loss))
+        s.close()
+    assert np.array_equal(out[0][0].view(np.int32), out[1][0].view(np.int32))
+    assert np.array_equal(out[0][1].view(np.int32), out[1][1].view(np.int32))
+    assert out[0][2] == out[1][2]
+    del rng_params
+
+
+@pytest.mark.gpu
 def test_features_match_cpu_oracle(gpu_ctx):
     import torch
     from rvpoint_b200.learned import DeviceBatch, PlaneScorer
