@@ -561,7 +561,7 @@ __device__ __forceinline__ u64 bound_of(float tau) { return pack_nbr(tau, 0x7FFF
 
 
 template <int P>
-__global__ __launch_bounds__(256) void k_knn_warp(GridView g, QuerySet q, int K, float radius,
+__global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int K, float radius,
                                                   u64 *out, int32_t *out_counts, u32 *stats,
                                                   int out_mode, float *mean) {
   const size_t nq = q.n_dev ? *q.n_dev : q.n_max;
