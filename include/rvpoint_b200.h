@@ -422,10 +422,11 @@ RVP_API rvp_status rvp_ransac_weighted(rvp_context *ctx, const float *x, const f
                                        float collinear_thresh, float probability,
                                        const int32_t *targets, float *models, int32_t *best,
                                        int32_t *iters_run);
-/* The weighted proposal in preemptive rounds: each round draws `draws`
+/* The weighted proposal in preemptive rounds: the first round draws `draws`
  * (<= 512) hypotheses per frame from its candidates (at most 2048 per
  * frame) by weight, ranks them by their inliers among the candidates, and
- * counts the best 32 exactly over all of the frame's points, keeping the
+ * counts the best 32 exactly over all of the frame's points; each later
+ * round draws 2 * draws and counts the best 64 (the same share), keeping the
  * best exact count with the strict-greater rule across rounds. A frame stops
  * when its count reaches its target (targets, optional) or after max_rounds;
  * draws_run receives the hypotheses drawn per frame. weights as for

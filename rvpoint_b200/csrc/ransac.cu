@@ -285,6 +285,9 @@ constexpr int PE_MAXC = 2048;
 constexpr int PE_MAXH = 512;
 constexpr int PE_FIRST = 4;   // with targets: exact counts of the best-ranked few first
 constexpr int PE_SLICES = 8;  // blocks per frame in the rounds after the first
+constexpr int PE_GROWTH = 2;  // later rounds: this many times the draws and the exact counts
+constexpr int PE_HALL = PE_MAXH * PE_GROWTH;  // hypotheses of a round, per frame (stride)
+constexpr int PE_KALL = PE_KEEP * PE_GROWTH;  // exactly counted hypotheses of a round (stride)
 
 __device__ __forceinline__ bool pe_skip(const RansacSampler &smp, const int64_t *offs,
                                         const int32_t *best_now, int f) {
@@ -297,7 +300,7 @@ __device__ __forceinline__ bool pe_skip(const RansacSampler &smp, const int64_t 
 
 __global__ __launch_bounds__(PE_THREADS) void k_preempt_count(
     const float *__restrict__ X, const float *__restrict__ Y, const float *__restrict__ Z,
-    const int64_t *offs, RansacSampler smp, int draws, int slices, int round, RansacParams prm,
+    const int64_t *offs, RansacSampler smp, int draws, int slices, int it_base, RansacParams prm,
     const int32_t *best_now, float4 *hyp_out, int *cnt_out) {
   __shared__ float4 P[PE_MAXC];
   __shared__ float4 hyp[PE_MAXH];
@@ -317,7 +320,7 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt_count(
   }
   const float *x = X + a0, *y = Y + a0, *z = Z + a0;
   for (int h = threadIdx.x; h < nh; h += blockDim.x) {
-    const int it = round * draws + h0 + h;
+    const int it = it_base + h0 + h;
     const u32 i1 = weighted_draw(smp, f, it, 0, a0, n);
     const u32 i2 = weighted_draw(smp, f, it, 1, a0, n);
     const u32 i3 = weighted_draw(smp, f, it, 2, a0, n);
@@ -346,29 +349,29 @@ __global__ __launch_bounds__(PE_THREADS) void k_preempt_count(
   }
   __syncthreads();
   for (int h = threadIdx.x; h < nh; h += blockDim.x) {
-    hyp_out[(size_t)f * PE_MAXH + h0 + h] = hyp[h];
-    cnt_out[(size_t)f * PE_MAXH + h0 + h] = hcnt[h];
+    hyp_out[(size_t)f * PE_HALL + h0 + h] = hyp[h];
+    cnt_out[(size_t)f * PE_HALL + h0 + h] = hcnt[h];
   }
 }
 
 // rank = #(greater count) + #(equal count, earlier draw). Only the
-// hypotheses at or above the PE_KEEP-th largest count can rank below
-// PE_KEEP: a histogram of the counts finds that count first.
+// hypotheses at or above the keep-th largest count can rank below keep: a
+// histogram of the counts finds that count first.
 constexpr int PR_THREADS = 512;
 __global__ __launch_bounds__(PR_THREADS) void k_preempt_rank(
-    const int64_t *offs, RansacSampler smp, int draws, const int32_t *best_now,
+    const int64_t *offs, RansacSampler smp, int draws, int keep, const int32_t *best_now,
     const float4 *hyp_in, const int *cnt_in, float4 *out) {
-  __shared__ int hcnt[PE_MAXH];
+  __shared__ int hcnt[PE_HALL];
   __shared__ int hist[PE_MAXC / 2 + 2];  // counts in pairs: (count + 1) >> 1
   __shared__ int s_thr;
   const int f = blockIdx.x;
-  float4 *o = out + (size_t)f * PE_KEEP;
+  float4 *o = out + (size_t)f * PE_KALL;
   const float4 none = make_float4(__int_as_float(0x7fc00000), 0, 0, 0);
-  for (int t = threadIdx.x; t < PE_KEEP; t += blockDim.x) o[t] = none;
+  for (int t = threadIdx.x; t < PE_KALL; t += blockDim.x) o[t] = none;
   if (pe_skip(smp, offs, best_now, f)) return;
   const int m = (int)(smp.cand_offs[f + 1] - smp.cand_offs[f]);
   const int nbins = ((m + 1) >> 1) + 1;
-  for (int h = threadIdx.x; h < draws; h += blockDim.x) hcnt[h] = cnt_in[(size_t)f * PE_MAXH + h];
+  for (int h = threadIdx.x; h < draws; h += blockDim.x) hcnt[h] = cnt_in[(size_t)f * PE_HALL + h];
   for (int b = threadIdx.x; b < nbins; b += blockDim.x) hist[b] = 0;
   __syncthreads();
   for (int h = threadIdx.x; h < draws; h += blockDim.x) atomicAdd(&hist[(hcnt[h] + 1) >> 1], 1);
@@ -384,7 +387,7 @@ __global__ __launch_bounds__(PR_THREADS) void k_preempt_rank(
         const int t = __shfl_up_sync(0xffffffffu, sfx, sh);
         if (lane >= sh) sfx += t;
       }
-      const unsigned hit = __ballot_sync(0xffffffffu, bb >= 0 && above + sfx >= PE_KEEP);
+      const unsigned hit = __ballot_sync(0xffffffffu, bb >= 0 && above + sfx >= keep);
       if (hit) {
         thr = top - (__ffs(hit) - 1);
         break;
@@ -403,7 +406,7 @@ __global__ __launch_bounds__(PR_THREADS) void k_preempt_rank(
       const int cg = hcnt[g];
       rank += (cg > c || (cg == c && g < h)) ? 1 : 0;
     }
-    if (rank < PE_KEEP) o[rank] = c >= 0 ? hyp_in[(size_t)f * PE_MAXH + h] : none;
+    if (rank < keep) o[rank] = c >= 0 ? hyp_in[(size_t)f * PE_HALL + h] : none;
   }
 }
 
@@ -509,54 +512,62 @@ void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const f
   if (n_frames <= 0) return;
   RVP_REQUIRE(draws >= 1 && draws <= PE_MAXH, "draws per round must be in [1, 512]");
   char *sp = static_cast<char *>(scratch);
-  float4 *models = reinterpret_cast<float4 *>(sp);
-  int *open = reinterpret_cast<int *>(sp + al((size_t)n_frames * PE_KEEP * 16));
-  int32_t *dummy_iters = reinterpret_cast<int32_t *>(sp + al((size_t)n_frames * PE_KEEP * 16) + 256);
-  char *sp2 = sp + al((size_t)n_frames * PE_KEEP * 16) + 256 + al((size_t)n_frames * 4);
-  float4 *hyp_all = reinterpret_cast<float4 *>(sp2);  // a round's hypotheses, PE_MAXH per frame
-  int *cnt_all = reinterpret_cast<int *>(sp2 + al((size_t)n_frames * PE_MAXH * 16));
+  float4 *models = reinterpret_cast<float4 *>(sp);  // a round's best, PE_KALL per frame
+  sp += al((size_t)n_frames * PE_KALL * 16);
+  int *open = reinterpret_cast<int *>(sp);
+  int32_t *dummy_iters = reinterpret_cast<int32_t *>(sp + 256);
+  sp += 256 + al((size_t)n_frames * 4);
+  float4 *hyp_all = reinterpret_cast<float4 *>(sp);  // a round's hypotheses, PE_HALL per frame
+  int *cnt_all = reinterpret_cast<int *>(sp + al((size_t)n_frames * PE_HALL * 16));
   cudaStream_t st = ctx->stream;
   k_fill_i32<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(draws_run, n_frames, -1);
   RVP_LAUNCH_CHECK(ctx);
-  RansacParams pe = p;
-  pe.max_iters = PE_KEEP;
+  int it_base = 0;
   for (int r = 0; r < max_rounds; ++r) {
     // the first round holds every frame; later ones only the frames still
-    // short of their target, each spread over PE_SLICES blocks
+    // short of their target: they draw PE_GROWTH times as many hypotheses
+    // and count PE_GROWTH times as many exactly (the same share), each frame
+    // spread over PE_SLICES blocks
+    const int grow = r == 0 ? 1 : PE_GROWTH;
+    const int draws_r = draws * grow, keep_r = PE_KEEP * grow;
     const int slices = r == 0 ? 1 : PE_SLICES;
     k_preempt_count<<<(unsigned)n_frames * slices, PE_THREADS, 0, st>>>(
-        x, y, z, offs, smp0, draws, slices, r, p, r > 0 ? best : nullptr, hyp_all, cnt_all);
+        x, y, z, offs, smp0, draws_r, slices, it_base, p, r > 0 ? best : nullptr, hyp_all,
+        cnt_all);
     RVP_LAUNCH_CHECK(ctx);
-    k_preempt_rank<<<n_frames, PR_THREADS, 0, st>>>(offs, smp0, draws, r > 0 ? best : nullptr,
-                                                    hyp_all, cnt_all, models);
+    k_preempt_rank<<<n_frames, PR_THREADS, 0, st>>>(offs, smp0, draws_r, keep_r,
+                                                    r > 0 ? best : nullptr, hyp_all, cnt_all,
+                                                    models);
     RVP_LAUNCH_CHECK(ctx);
+    it_base += draws_r;
     RansacSampler sm = smp0;
     sm.models = models;
-    sm.n_models = PE_KEEP;
+    sm.n_models = PE_KALL;
     sm.best_in = r > 0 ? best : nullptr;
     sm.model_in = r > 0 ? model : nullptr;
+    RansacParams pe = p;
     if (smp0.targets && r == 0) {
       // the best-ranked PE_FIRST first: most frames reach their target
       // there; the others go on with the rest, in the same rank order (so
       // the result is the single pass's). Later rounds hold the frames the
       // first could not finish, which rarely stop within the first few.
-      RansacParams p1 = pe;
-      p1.max_iters = PE_FIRST;
-      ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, p1, model, best, dummy_iters, nullptr,
+      pe.max_iters = PE_FIRST;
+      ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, pe, model, best, dummy_iters, nullptr,
                     false, sm, 8);
       sm.models = models + PE_FIRST;
       sm.best_in = best;
       sm.model_in = model;
-      p1.max_iters = PE_KEEP - PE_FIRST;
-      ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, p1, model, best, dummy_iters, nullptr,
+      pe.max_iters = keep_r - PE_FIRST;
+      ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, pe, model, best, dummy_iters, nullptr,
                     false, sm, 8);
     } else {
+      pe.max_iters = keep_r;
       ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, pe, model, best, dummy_iters, nullptr,
                     false, sm, 8);
     }
     RVP_CUDA_TRY(cudaMemsetAsync(open, 0, 4, st));
     k_preempt_done<<<grid_for(n_frames, 256, 64), 256, 0, st>>>(
-        best, smp0.targets, n_frames, (r + 1) * draws, r + 1 == max_rounds, draws_run, open);
+        best, smp0.targets, n_frames, it_base, r + 1 == max_rounds, draws_run, open);
     RVP_LAUNCH_CHECK(ctx);
     if (smp0.targets) {
       int h_open = 0;
@@ -568,8 +579,8 @@ void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const f
 }
 
 size_t preemptive_temp_bytes(int n_frames) {
-  return al((size_t)n_frames * PE_KEEP * 16) + 256 + al((size_t)n_frames * 4) +
-         al((size_t)n_frames * PE_MAXH * 16) + al((size_t)n_frames * PE_MAXH * 4);
+  return al((size_t)n_frames * PE_KALL * 16) + 256 + al((size_t)n_frames * 4) +
+         al((size_t)n_frames * PE_HALL * 16) + al((size_t)n_frames * PE_HALL * 4);
 }
 
 size_t extract_temp_bytes(size_t n) {

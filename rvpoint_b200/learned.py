@@ -206,13 +206,24 @@ def ransac_weighted(b: DeviceBatch, cand: torch.Tensor, cand_offsets: torch.Tens
     return models, best, iters
 
 
+PREEMPT_GROWTH = 2  # rvp_ransac_preemptive: later rounds draw (and count) this many times more
+
+
+def preemptive_rounds(max_iters: int, draws: int) -> int:
+    """Rounds of rvp_ransac_preemptive whose hypotheses first reach max_iters."""
+    rest = max(0, max_iters - draws)
+    step = PREEMPT_GROWTH * draws
+    return 1 + (rest + step - 1) // step
+
+
 def ransac_preemptive(b: DeviceBatch, cand: torch.Tensor, cand_offsets: torch.Tensor,
                       weights: torch.Tensor, thresh: float, draws: int = 256,
                       max_rounds: int = 40, seed: int = 1, logit_power: float = 0.0,
                       collinear: float = 1e-6, targets: Optional[torch.Tensor] = None,
                       ctx: Optional[Context] = None):
-    """Weighted proposal in preemptive rounds (rvp_ransac_preemptive):
-    returns (models, best, hypotheses drawn per frame)."""
+    """Weighted proposal in preemptive rounds (rvp_ransac_preemptive: the
+    first round draws `draws` hypotheses, each later one PREEMPT_GROWTH times
+    as many): returns (models, best, hypotheses drawn per frame)."""
     ctx = ctx or default_context()
     ctx.use_torch_stream()
     dev = b.x.device
@@ -315,7 +326,7 @@ class LearnedRansac:
     def ransac(self, b: DeviceBatch, cand, cand_offsets, logits, max_iters: int, thresh: float,
                targets: Optional[torch.Tensor] = None):
         if self.preemptive:
-            rounds = max(1, (max_iters + self.draws - 1) // self.draws)
+            rounds = preemptive_rounds(max_iters, self.draws)
             return ransac_preemptive(b, cand, cand_offsets, logits, thresh, draws=self.draws,
                                      max_rounds=rounds, seed=self.seed,
                                      logit_power=self.logit_power, targets=targets,
