@@ -551,9 +551,9 @@ void ransac_preemptive(rvp_context *ctx, const float *x, const float *y, const f
       // there; the others go on with the rest, in the same rank order (so
       // the result is the single pass's). Later rounds hold the frames the
       // first could not finish, which rarely stop within the first few.
-      pe.max_iters = PE_FIRST;
+      pe.max_iters = PE_FIRST;  // a light pass over every frame: one block per frame
       ransac_frames(ctx, x, y, z, offs, n_frames, nullptr, pe, model, best, dummy_iters, nullptr,
-                    false, sm, 8);
+                    false, sm, 1);
       sm.models = models + PE_FIRST;
       sm.best_in = best;
       sm.model_in = model;
