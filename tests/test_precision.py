@@ -30,7 +30,7 @@ def test_precise_normals_against_fp64(gpu_ctx, restatement):
     e_prec = _angle(n_prec, ref)
     e_plain = _angle(n_plain, ref)
     # neighbourhoods whose smallest eigenvalues nearly coincide have no
-    # well-defined normal: judge where the oracle's gap is clear
+    # well-defined normal: assess where the oracle's gap is clear
     ok = np.isfinite(ref_cond)
     stats = {"max": float(e_prec[ok].max()), "p99": float(np.percentile(e_prec[ok], 99)),
              "plain_p99": float(np.percentile(e_plain[ok], 99)),
