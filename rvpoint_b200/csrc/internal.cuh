@@ -265,7 +265,11 @@ void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
 // indices) for grid_knn. Modes: SOR mean, fused reference normals, pairs.
 // TILE_SOR_LIST: the SOR mean plus the k nearest indices in (d2, index)
 // order, kept for the normal stage (sor_list)
-enum TileMode { TILE_SOR_MEAN = 0, TILE_NORMALS = 1, TILE_PAIRS = 2, TILE_SOR_LIST = 3 };
+// TILE_PAIRS_F: the TILE_PAIRS output from float distances with an index
+// beside each (per-warp kernels only); a list with equal distances, whose
+// order the scan would decide, goes to the hard list for the exact search
+enum TileMode { TILE_SOR_MEAN = 0, TILE_NORMALS = 1, TILE_PAIRS = 2, TILE_SOR_LIST = 3,
+                TILE_PAIRS_F = 4 };
 struct TileArgs {
   const int32_t *frame_of;  // frame of each original index
   float *mean;              // TILE_SOR_MEAN / _LIST: by original index

@@ -337,7 +337,8 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
                                                   uint8_t *qlevel, float *qtau, u32 *stats) {
   // float keys where only distances order the list (SOR); the list mode
   // carries indices beside them and detects ties (below)
-  constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST;
+  constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
+  constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;  // indices beside
   using Key = typename std::conditional<FKEY, float, u64>::type;
   __shared__ uint2 wtab[WT_WARPS][WT_CELLS];
   const u64 n = list ? *n_list : *g.n_points;
@@ -416,7 +417,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
       u32 found = 0;
       // list mode: indices, and the value of the last tie met at the
       // boundary (an equal key rejected or evicted)
-      u32 I[MODE == TILE_SOR_LIST ? K : 1];
+      u32 I[KV ? K : 1];
       float tie = -1.0f;
       auto scan = [&](int lox, int hix, int loy, int hiy, int loz, int hiz, bool bounded,
                       float tb) {
@@ -451,14 +452,14 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
             if constexpr (FKEY) key = d2;
             else key = pack_nbr(d2, (int)pidx);
             if (key < thr) {
-              if constexpr (MODE == TILE_SOR_LIST) {
+              if constexpr (KV) {
                 list_insert_kv<K>(L, I, key, pidx);
                 if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
               } else {
                 list_insert<Key, K>(L, key);
               }
               thr = L[K - 1];
-            } else if constexpr (MODE == TILE_SOR_LIST) {
+            } else if constexpr (KV) {
               if (key == thr) tie = key;
             }
           }
@@ -544,6 +545,19 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
           a.nx[o] = nx;
           a.ny[o] = ny;
           a.nz[o] = nz;
+        } else if constexpr (MODE == TILE_PAIRS_F) {
+          bool tied = tie == L[K - 1];
+#pragma unroll
+          for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
+          if (tied) {  // the exact (d2, index) list from the warp kernel
+            const u32 slot = atomicAdd(a.hard_count, 1u);
+            a.hard[slot] = qidx & 0x7FFFFFFFu;
+            if (a.hard_tau) a.hard_tau[slot] = L[K - 1];
+          } else {
+#pragma unroll
+            for (int j = 0; j < K; ++j) a.pairs[(size_t)qidx * K + j] = pack_nbr(L[j], (int)I[j]);
+            if (a.counts) a.counts[qidx] = K;
+          }
         } else {
 #pragma unroll
           for (int j = 0; j < K; ++j) a.pairs[(size_t)qidx * K + j] = L[j];
@@ -602,6 +616,9 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
                                                                     qlevel, a.qtau, st);
       else if (mode == TILE_NORMALS)
         k_knn_wt<K, TILE_NORMALS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
+                                                                   qlevel, a.qtau, st);
+      else if (mode == TILE_PAIRS_F)
+        k_knn_wt<K, TILE_PAIRS_F><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                    qlevel, a.qtau, st);
       else
         k_knn_wt<K, TILE_PAIRS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,

@@ -663,7 +663,7 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
     ta.open_n = reinterpret_cast<u64 *>(op); op += 256;
     ta.scan_tmp = op;
     ta.n_max = N;
-    RVP_REQUIRE(rvp::grid_knn_tile(ctx, gv, rvp::KF, rvp::TILE_PAIRS, ta, 0, nullptr),
+    RVP_REQUIRE(rvp::grid_knn_tile(ctx, gv, rvp::KF, rvp::TILE_PAIRS_F, ta, 0, nullptr),
                 "kNN tile path unavailable");
     rvp::k_widen32<<<1, 32, 0, st>>>(hard_n, hard_n64);
     RVP_LAUNCH_CHECK(ctx);
