@@ -5,10 +5,10 @@
 // COUNT defaults to 1). The payload goes to the device in the form the file
 // holds it and is split there:
 //   binary             records of all fields back to back: the records are
-//                      read in chunks into pinned buffers and copied up while
-//                      the next chunk is read; one thread per point picks
-//                      x, y, z from its record (the AoS -> SoA transpose runs
-//                      on the GPU);
+//                      read in chunks by several threads into pinned buffers
+//                      and copied up while the next chunks are read; one
+//                      thread per point picks x, y, z from its record (the
+//                      AoS -> SoA transpose runs on the GPU);
 //   binary_compressed  one LZF block holding each field's column in turn:
 //                      decoded on the host (LZF is a sequential byte stream),
 //                      then the x, y, z columns are copied up as they are;
@@ -17,10 +17,15 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <fcntl.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <atomic>
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.cuh"
@@ -182,38 +187,65 @@ extern "C" rvp_status rvp_pcd_load(rvp_context *ctx, const char *path, int mem, 
     }
     if (h.data == "binary") {
       if (mem == RVP_MEM_DEVICE) {
-        // the records go up as they lie in the file: read in chunks into two
-        // pinned buffers, each chunk's copy overlapping the next read
+        // the records go up as they lie in the file: NB threads read NB
+        // chunks at a time (pread) into pinned buffers, and each wave's
+        // copies overlap the next wave's reads
         const size_t total = stride * n;
+        const long long at0 = (long long)f.tellg();
+        RVP_REQUIRE(at0 >= 0, "cannot locate the binary PCD payload");
         DevBuf &d = ctx->scratch[29];
         d.reserve(total);
         constexpr size_t CH = (size_t)8 << 20;
-        HostBuf *hb[2] = {&ctx->pinned[0], &ctx->pinned[1]};
-        hb[0]->reserve(CH);
-        hb[1]->reserve(CH);
-        cudaEvent_t ev[2] = {nullptr, nullptr};
+        constexpr int NB = 4;
+        cudaEvent_t ev[NB] = {};
         struct Events {  // destroyed on every way out
           cudaEvent_t *e;
           ~Events() {
-            for (int i = 0; i < 2; ++i)
+            for (int i = 0; i < NB; ++i)
               if (e[i]) cudaEventDestroy(e[i]);
           }
         } guard_ev{ev};
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < NB; ++i) {
+          ctx->pinned[i].reserve(CH);
           RVP_CUDA_TRY(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
-        size_t i = 0;
-        for (size_t at = 0; at < total; at += CH, ++i) {
-          const size_t len = std::min(CH, total - at);
-          HostBuf &b = *hb[i & 1];
-          if (i >= 2) RVP_CUDA_TRY(cudaEventSynchronize(ev[i & 1]));  // its last copy is done
-          f.read(static_cast<char *>(b.ptr), (std::streamsize)len);
-          if ((size_t)f.gcount() != len) {
+        }
+        const int fd = open(path, O_RDONLY);
+        RVP_REQUIRE(fd >= 0, std::string("cannot open ") + path);
+        struct Fd {
+          int fd;
+          ~Fd() { close(fd); }
+        } guard_fd{fd};
+        const size_t chunks = (total + CH - 1) / CH;
+        for (size_t w = 0; w < chunks; w += NB) {
+          const int nw = (int)std::min<size_t>(NB, chunks - w);
+          if (w > 0)  // the buffers' previous copies are done
+            for (int i = 0; i < nw; ++i) RVP_CUDA_TRY(cudaEventSynchronize(ev[i]));
+          std::atomic<bool> short_read{false};
+          auto read_chunk = [&](int i) {
+            const size_t at = (w + i) * CH, len = std::min(CH, total - at);
+            char *dst = static_cast<char *>(ctx->pinned[i].ptr);
+            size_t got = 0;
+            while (got < len) {
+              const ssize_t r = pread(fd, dst + got, len - got, (off_t)(at0 + at + got));
+              if (r <= 0) break;
+              got += (size_t)r;
+            }
+            if (got != len) short_read.store(true);
+          };
+          std::vector<std::thread> th;
+          for (int i = 1; i < nw; ++i) th.emplace_back(read_chunk, i);
+          read_chunk(0);
+          for (auto &t : th) t.join();
+          if (short_read.load()) {
             RVP_CUDA_TRY(cudaStreamSynchronize(st));
             throw Error{RVP_ERR_INVALID_ARG, "short binary PCD payload"};
           }
-          RVP_CUDA_TRY(cudaMemcpyAsync(d.as<unsigned char>() + at, b.ptr, len,
-                                       cudaMemcpyHostToDevice, st));
-          RVP_CUDA_TRY(cudaEventRecord(ev[i & 1], st));
+          for (int i = 0; i < nw; ++i) {
+            const size_t at = (w + i) * CH, len = std::min(CH, total - at);
+            RVP_CUDA_TRY(cudaMemcpyAsync(d.as<unsigned char>() + at, ctx->pinned[i].ptr, len,
+                                         cudaMemcpyHostToDevice, st));
+            RVP_CUDA_TRY(cudaEventRecord(ev[i], st));
+          }
         }
         k_pcd_records<<<grid_for(n, 256, ctx->num_sms * 16), 256, 0, st>>>(
             d.as<unsigned char>(), n, stride, off[xi], off[yi], off[zi], x, y, z);
