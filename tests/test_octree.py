@@ -174,3 +174,26 @@ def test_octree_large_lists_are_hash_sets_in_rank_order(gpu_ctx, kind):
         assert np.array_equal(seg[srt], hi[s:e]) and np.array_equal(bits(d[s:e][srt]), bits(hd[s:e]))
     h.close()
     t.close()
+
+
+@pytest.mark.gpu
+def test_octree_edge_cases(gpu_ctx, restatement):
+    """One point, all points equal (held together by the depth limit), a flat
+    plane, depth 21 (the deepest key) with a zero epsilon."""
+    from rvpoint_b200 import api
+    rng = np.random.default_rng(12)
+    clouds = [np.array([[1.0, 2.0, 3.0]], np.float32),
+              np.tile(np.array([[0.5, 0.5, 0.5]], np.float32), (300, 1)),
+              np.concatenate([rng.uniform(0, 2, (500, 2)), np.zeros((500, 1))], 1).astype(np.float32),
+              rng.normal(size=(700, 3)).astype(np.float32)]
+    for pts in clouds:
+        c = D.Cloud.from_xyz(pts)
+        for kind in (0, 1):
+            for tree in ((64, 8, 1e-4), (2, 6, 1e-6), (1, 21, 0.0)):
+                t = _tree(api, kind, c, tree)
+                assert np.array_equal(t.order(), restatement.octree_order(kind, c, tree)), tree
+                o, i, d = t.radiusSearchBatch(c.x, c.y, c.z, 0.3)
+                ro, ri, rd = restatement.octree_radius(kind, c, 0.3, tree=tree)
+                assert np.array_equal(o, ro) and np.array_equal(i, ri)
+                assert np.array_equal(bits(d), bits(rd))
+                t.close()

@@ -235,3 +235,23 @@ def test_reference_octrees(reference, restatement, seed):
                           bits(restatement.normals_octree(1, c, 0.08)))
     o, l = reference.pointer_octree_leaves(c)
     assert np.array_equal(o, restatement.octree_order(1, c))
+
+
+def test_reference_octree_edge_cases(reference, restatement):
+    """One point, all points equal (the depth limit holds them in one leaf),
+    a flat plane (z splits put everything on one side) and a tiny epsilon."""
+    rng = np.random.default_rng(12)
+    clouds = [np.array([[1.0, 2.0, 3.0]], np.float32),
+              np.tile(np.array([[0.5, 0.5, 0.5]], np.float32), (300, 1)),
+              np.concatenate([rng.uniform(0, 2, (500, 2)), np.zeros((500, 1))], 1).astype(np.float32),
+              rng.normal(size=(700, 3)).astype(np.float32)]
+    q = D.Cloud.from_xyz(np.array([[0.0, 0.0, 0.0]], np.float32))
+    for pts in clouds:
+        c = D.Cloud.from_xyz(pts)
+        for kind in (0, 1):
+            for tree in ((64, 8, 1e-4), (2, 6, 1e-6), (1, 21, 0.0)):
+                _, i, _ = reference.octree_radius(kind, c, 1e6, queries=q, tree=tree)
+                assert np.array_equal(restatement.octree_order(kind, c, tree), i), (kind, tree)
+            a = reference.octree_radius(kind, c, 0.3)
+            b = restatement.octree_radius(kind, c, 0.3)
+            assert np.array_equal(a[1], b[1]) and np.array_equal(bits(a[2]), bits(b[2]))
