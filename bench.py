@@ -13,7 +13,7 @@ results come down, overlapped with the neighbouring steps' work) with the
 host<->device copies inside the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--cell C [--rfac R]] [--no-tune] [--cpu-budget-s S]
+                    [--cell C [--rfac R]] [--no-tune] [--cpu-frames F]
 
 Rank 0 also runs the learned-vs-plain RANSAC leg (``learned_ransac`` in the
 line): 512 plane scenes of 50,000 points; plain GPU RANSAC (10,000
@@ -65,7 +65,14 @@ def parse():
                     help="level-0 first-pass radius factor with --cell")
     ap.add_argument("--lane-levels", type=int, default=2,
                     help="grid levels of the one-query-per-lane kNN with --cell")
-    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--qpw", type=int, default=3,
+                    help="kNN kernel mode with --cell (0 per-lane, 3 cooperative level 0)")
+    ap.add_argument("--block", type=int, default=0,
+                    help="warp-per-query kernel block size with --cell (0: 256)")
+    ap.add_argument("--cpu-frames", type=int, default=5,
+                    help="frames of the CPU baseline (and of the parity check)")
+    ap.add_argument("--no-singles", action="store_true",
+                    help="skip the single-cloud workloads (room chain, LiDAR radius, 2M normals)")
     ap.add_argument("--no-next-rows", action="store_true",
                     help="skip the PCD / octree / clustering timings")
     ap.add_argument("--learned-scenes", type=int, default=512,
@@ -78,12 +85,15 @@ def parse():
 # ---------------------------------------------------------------------------
 def _cpu_frame(args):
     """voxel -> sor_rvv -> normal_estimation_sc -> ransac_plane_rvv on one
-    frame with the reference's own code (or the restatement if absent)."""
+    frame with the reference's own code (or the restatement if absent), one
+    thread. Returns the time, the input size, the kind, and the outputs (for
+    the comparison with the GPU's results of the same frame)."""
     x, y, z = args
     sys.path.insert(0, ROOT)
     import numpy as np
     from oracle import oracle as O
     from rvpoint_b200.datasets import Cloud
+    os.environ["RVO_THREADS"] = "1"
     c = Cloud(np.ascontiguousarray(x), np.ascontiguousarray(y), np.ascontiguousarray(z))
     t0 = time.perf_counter()
     if O.reference_available():
@@ -92,8 +102,8 @@ def _cpu_frame(args):
         vc = Cloud.from_xyz(v)
         s = R.sor_rvv(vc, SOR_K, SOR_ALPHA)
         sc = Cloud.from_xyz(s)
-        R.normals_sc(sc, NORMAL_K)
-        R.ransac_plane(sc, R_THRESH, R_ITERS)
+        nrm = R.normals_sc(sc, NORMAL_K)
+        best, model = R.ransac_plane(sc, R_THRESH, R_ITERS)
         kind = "reference"
     else:
         R = O.Restatement()
@@ -101,29 +111,215 @@ def _cpu_frame(args):
         vc = Cloud.from_xyz(v)
         s, _, _ = R.sor_exact(vc, SOR_K, SOR_ALPHA)
         sc = Cloud.from_xyz(s)
-        R.normals_knn(sc, NORMAL_K)
-        R.ransac_plane(sc, R_THRESH, R_ITERS, O.libc_rand_stream(3 * R_ITERS))
+        nrm = R.normals_knn(sc, NORMAL_K)
+        best, model, _, _, _ = R.ransac_plane(sc, R_THRESH, R_ITERS,
+                                              O.libc_rand_stream(3 * R_ITERS))
         kind = "port"
-    return time.perf_counter() - t0, int(x.shape[0]), kind
+    dt = time.perf_counter() - t0
+    return dt, int(x.shape[0]), kind, {"voxel": v, "sor": s, "normals": nrm, "best": int(best),
+                                       "model": np.asarray(model, np.float32)}
 
 
-def cpu_baseline(batch, budget_s: float) -> dict:
-    """Frames in order, single-threaded (the reference library is), until
-    the CPU budget is spent."""
+def _cpu_room_chain(_=None):
+    """The 100,000-point room chain with the reference's own code, one thread:
+    voxel 0.01 -> sor_rvv k=30 -> normal_estimation_rvv(SpatialHash, r=0.03)
+    -> ransac_plane_rvv 1000 / 0.01. Returns per-stage seconds."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from rvpoint_b200 import datasets as D
+    os.environ["RVO_THREADS"] = "1"
+    if not O.reference_available():
+        return None
+    R = O.Reference()
+    c = D.room_cloud(n=100_000)
+    t = {}
+    t0 = time.perf_counter()
+    v = R.voxel_grid(c, 0.01)
+    t["voxel"] = time.perf_counter() - t0
+    vc = D.Cloud.from_xyz(v)
+    t0 = time.perf_counter()
+    s = R.sor_rvv(vc, 30, 1.0)
+    t["sor"] = time.perf_counter() - t0
+    sc = D.Cloud.from_xyz(s)
+    t0 = time.perf_counter()
+    R.normals_hash(sc, 0.03, 0.03)
+    t["normals"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    best, _ = R.ransac_plane(sc, 0.01, 1000)
+    t["ransac"] = time.perf_counter() - t0
+    return {"seconds": t, "voxels": int(v.shape[0]), "kept": int(s.shape[0]), "ransac": best}
+
+
+def _cpu_lidar_radius(_=None):
+    """All-point radiusSearch r = 0.5 and the radius-bounded kNN (max_nn = 16)
+    on the whole 64 x 2048-ray frame with the reference's SpatialHash (cell
+    0.5), one thread."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from rvpoint_b200 import datasets as D
+    if not O.reference_available():
+        return None
+    R = O.Reference()
+    f = D.lidar_frame()
+    t0 = time.perf_counter()
+    o, _, _ = R.radius_search(f, 0.5, 0.5)
+    t_r = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    R.radius_search(f, 0.5, 0.5, max_nn=16)
+    t_k = time.perf_counter() - t0
+    return {"radius_s": t_r, "knn16_s": t_k, "points": f.n, "pairs": int(o[-1])}
+
+
+def single_cloud_legs(ctx) -> dict:
+    """The single-cloud workloads through the public API with host arrays in
+    and out (wall clock, mean of 3 calls after one warm-up): the 100k room
+    chain, all-point radius search r = 0.5 and kNN 16 on one whole LiDAR
+    frame, and precision-mode normals (k = 32) of the 2,000,000-point
+    translated room with their error against float64 on 100,000 sampled
+    points."""
+    import numpy as np
+    from rvpoint_b200 import api
+    from rvpoint_b200 import datasets as D
+
+    def wall(fn, reps=3):
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            r = fn()
+        return (time.perf_counter() - t0) / reps * 1e3, r
+
+    out = {}
+    c = D.room_cloud(n=100_000)
+
+    def room_chain():
+        v = api.voxel_grid_downsamp_rvv_v2(c, 0.01, ctx=ctx)
+        vc = D.Cloud.from_xyz(v)
+        s = api.sor_rvv(vc, 30, 1.0, ctx=ctx)
+        sc = D.Cloud.from_xyz(s)
+        h = api.SpatialHash(ctx)
+        h.setInputCloud(sc, 0.03)
+        h.build()
+        api.normal_estimation_rvv(sc, h, 10, 0.03, ctx=ctx)
+        h.close()
+        best, _ = api.ransac_plane_rvv(sc, 0.01, 1000, ctx=ctx)
+        return len(v), len(s), best
+    ms, (nv, ns, best) = wall(room_chain)
+    out["room_chain_100k"] = {"workload": "room 100k: voxel 0.01 -> sor_rvv k=30 -> "
+                                          "SpatialHash normals r=0.03 -> RANSAC 1000 / 0.01",
+                              "gpu_ms": ms, "gpu_mpts_s": c.n / ms / 1e3, "voxels": nv,
+                              "kept": ns, "ransac": best}
+    f = D.lidar_frame()
+    h = api.SpatialHash(ctx)
+    h.setInputCloud(f, 0.5)
+    h.build()
+    ms_r, (offs, _, _) = wall(lambda: h.radiusSearchBatch(f.x, f.y, f.z, 0.5))
+    ms_k, _ = wall(lambda: h.radiusSearchBatch(f.x, f.y, f.z, 0.5, max_nn=16))
+    ms_kk, _ = wall(lambda: h.knn(f.x, f.y, f.z, 16))
+    h.close()
+    out["lidar_frame_radius"] = {"workload": "one 64 x 2048-ray frame, every point: "
+                                             "radiusSearch r=0.5 (cell 0.5), max_nn=16, kNN 16",
+                                 "points": f.n, "pairs_r05": int(offs[-1]),
+                                 "radius_gpu_ms": ms_r, "radius_gpu_mqueries_s": f.n / ms_r / 1e3,
+                                 "max_nn16_gpu_ms": ms_k, "knn16_gpu_ms": ms_kk}
+    p = D.precision_room()
+    ms, (nrm, cond, used) = wall(lambda: api.normal_estimation_precise(p, 32, ctx=ctx), reps=2)
+    out["precision_normals_2m"] = {"workload": "2M-point room shifted by (1e4, 1e4, 0), k=32, "
+                                               "precision mode", "gpu_ms": ms,
+                                   "gpu_mpts_s": p.n / ms / 1e3,
+                                   "fp64_eigen_fraction": float(np.mean(used > 0))}
+    try:
+        from scipy.spatial import cKDTree
+        rng = np.random.default_rng(5)
+        q = rng.choice(p.n, size=100_000, replace=False)
+        P = np.stack([p.x, p.y, p.z], 1).astype(np.float64)
+        _, nbr = cKDTree(P).query(P[q], k=33, workers=-1)
+        X = P[nbr]
+        Xc = X - X.mean(1, keepdims=True)
+        w, V = np.linalg.eigh(np.einsum("nki,nkj->nij", Xc, Xc))
+        ref = V[:, :, 0]
+        g = nrm[q].astype(np.float64)
+        cosang = np.abs((g * ref).sum(1)) / np.maximum(np.linalg.norm(g, axis=1), 1e-300)
+        ang = np.arccos(np.clip(cosang, 0, 1))
+        gap = w[:, 1] / np.maximum(w[:, 0], 1e-300)
+        ok = gap > 1.0 + 1e-9
+        out["precision_normals_2m"].update(
+            {"angle_err_rad_vs_fp64": {"sampled_points": int(ok.sum()),
+                                       "max": float(ang[ok].max()),
+                                       "p99": float(np.percentile(ang[ok], 99))}})
+    except Exception as e:  # pragma: no cover
+        out["precision_normals_2m"]["angle_err_rad_vs_fp64"] = {"unavailable": str(e)}
+    return out
+
+
+def sample_frames(sizes, count: int):
+    """Frames at evenly spaced quantiles of the batch's size distribution
+    (the CPU cost is quadratic in the frame size, so a sample of the first
+    frames would weight the mix by chance)."""
+    import numpy as np
+    order = np.argsort(sizes, kind="stable")
+    qs = [(i + 0.5) / count for i in range(count)]
+    return [int(order[min(len(order) - 1, int(q * len(order)))]) for q in qs]
+
+
+def cpu_baseline(batch, n_frames_sample: int, gpu_results=None, singles: bool = True):
+    """The reference's chain on a sample of frames spread over the batch's
+    size range, each frame on one thread (the reference library is
+    single-threaded); the frames run in separate processes at the same time
+    to save wall clock, each timed on its own. The reference's outputs of
+    those frames are compared with the GPU's results of the same frames
+    (``parity``). With `singles`, the single-cloud workloads (the 100k room
+    chain, the LiDAR frame's radius search) run beside them, one process
+    each. Returns (cpu_baseline, single-cloud CPU times)."""
+    import numpy as np
     from oracle import oracle as O
     O.build() if not os.path.exists(O.RESTATEMENT_SO) else None
-    t_tot, pts, frames, kind = 0.0, 0, 0, "port"
-    for f in range(batch.n_frames):
-        fr = batch.frame(f)
-        dt, n, kind = _cpu_frame((fr.x, fr.y, fr.z))
-        t_tot += dt
-        pts += n
-        frames += 1
-        if t_tot >= budget_s:
-            break
-    return {"value": pts / t_tot / 1e6, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"first {frames} of {batch.n_frames} frames ({pts} input points), "
-                      f"full chain, one thread, {t_tot:.1f} s"}
+    sizes = np.diff(batch.offsets)
+    pick = sample_frames(sizes, n_frames_sample)
+    jobs = [(batch.frame(f).x, batch.frame(f).y, batch.frame(f).z) for f in pick]
+    with mp.get_context("spawn").Pool(len(jobs) + (2 if singles else 0)) as pool:
+        room = pool.apply_async(_cpu_room_chain) if singles else None
+        lidar = pool.apply_async(_cpu_lidar_radius) if singles else None
+        res = pool.map(_cpu_frame, jobs)
+        cpu_single = {"room_chain_100k": room.get(), "lidar_frame_radius": lidar.get()} \
+            if singles else None
+    t_tot = sum(r[0] for r in res)
+    pts = sum(r[1] for r in res)
+    kind = res[0][2]
+    out = {"value": pts / t_tot / 1e6, "unit": UNIT, "cores": 1, "kind": kind,
+           "sample": (f"{len(pick)} of {batch.n_frames} frames at evenly spaced size "
+                      f"quantiles ({pts} input points; frame sizes "
+                      f"{[int(sizes[f]) for f in pick]}), full chain, each frame on one "
+                      f"thread; {t_tot:.1f} s of CPU time summed over the frames"),
+           "frames": pick}
+    if gpu_results is not None:
+        out["parity"] = compare_frames(gpu_results, pick, [r[3] for r in res])
+    return out, cpu_single
+
+
+def compare_frames(g, frames, ref) -> dict:
+    """The GPU's per-frame results against the reference's outputs of the
+    same frames: voxel centroids, SOR output and the RANSAC count / model bit
+    for bit; normals within 1e-4 rad of the reference's FP32 normals."""
+    import numpy as np
+    bits = lambda a: np.ascontiguousarray(a, np.float32).view(np.int32)  # noqa: E731
+    vox = sor = ran = True
+    close = []
+    for f, r in zip(frames, ref):
+        a, b = g["voxel_offsets"][f], g["voxel_offsets"][f + 1]
+        vox &= np.array_equal(bits(g["voxel"][a:b]), bits(r["voxel"]))
+        a, b = g["sor_offsets"][f], g["sor_offsets"][f + 1]
+        same_sor = np.array_equal(bits(g["sor"][a:b]), bits(r["sor"]))
+        sor &= same_sor
+        ran &= int(g["ransac_count"][f]) == r["best"] and np.array_equal(
+            bits(g["ransac_model"][f]), bits(r["model"]))
+        if same_sor:
+            u, v = g["normals"][a:b], r["normals"]
+            cosang = np.abs((u * v).sum(1)) / np.maximum(
+                np.linalg.norm(u, axis=1) * np.linalg.norm(v, axis=1), 1e-30)
+            close.append(float((np.arccos(np.clip(cosang, 0, 1)) < 1e-4).mean()))
+    return {"frames_checked": len(frames), "voxel_bit_exact": bool(vox),
+            "sor_bit_exact": bool(sor), "ransac_bit_exact": bool(ran),
+            "normals_within_1e-4_rad_min_fraction": min(close) if close else None}
 
 
 def reference_arm(a, rank: int) -> None:
@@ -137,22 +333,28 @@ def reference_arm(a, rank: int) -> None:
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     workers = max(1, cores)
     ctx = mp.get_context("spawn")
-    times, pts_step = [], []
+    times, pts_step, sizes_seen = [], [], []
     kind = "port"
     # a step is one frame per process; frames take seconds each on one core
     # (the reference's exact SOR is quadratic in the frame size), so the run
     # is bounded to at most 1 + 3 steps, whatever --steps / --warmup ask
     warm, steps = min(a.warmup, 1), min(a.steps, 3)
+    # frames in a seeded random order, so that every step's sample has the
+    # batch's size mix rather than the first frames'
+    import numpy as np
+    perm = np.random.default_rng(0).permutation(batch.n_frames)
     with ctx.Pool(workers) as pool:
         nxt = 0
         for step in range(warm + steps):
             # one frame per worker per step, frames in order
-            sel = [(nxt + j) % batch.n_frames for j in range(min(workers, batch.n_frames))]
+            sel = [int(perm[(nxt + j) % batch.n_frames])
+                   for j in range(min(workers, batch.n_frames))]
             nxt = (nxt + len(sel)) % batch.n_frames
             jobs = [(batch.frame(f).x, batch.frame(f).y, batch.frame(f).z) for f in sel]
             t0 = time.perf_counter()
             res = pool.map(_cpu_frame, jobs)
             dt = time.perf_counter() - t0
+            sizes_seen.extend(r[1] for r in res)
             kind = res[0][2]
             if step >= warm:
                 times.append(dt)
@@ -167,8 +369,9 @@ def reference_arm(a, rank: int) -> None:
                        "leaf": LEAF, "sor_k": SOR_K, "normal_k": NORMAL_K,
                        "ransac_iters": R_ITERS, "ransac_thresh": R_THRESH},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind,
-                             "sample": f"{min(workers, batch.n_frames)} frames per step, one "
-                                       f"frame per process, {workers} processes"},
+                             "sample": f"{min(workers, batch.n_frames)} frames per step in a "
+                                       f"seeded random order, one frame per process, "
+                                       f"{workers} processes; frame sizes {sizes_seen}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -342,13 +545,23 @@ def next_rows_leg(ctx, batch) -> dict:
 
 def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
     """Learned-vs-plain RANSAC on n_scenes synthetic plane scenes of 50,000
-    points (1-6 planes, 30-70% outliers, 5 mm noise). The target of every
-    scene is 99% of plain RANSAC's best count after up to 10,000
-    hypotheses (the reference's rand() stream, adaptive stop p = 0.99).
-    Timed with CUDA events, inputs resident: plain RANSAC to its own stop,
-    plain RANSAC stopped at the target, and the learned proposal (features
-    + MLP + weighted RANSAC stopped at the target). The network is trained
-    first on n_train held-out scenes, on the GPU."""
+    points (1-6 planes, 30-70% outliers, 5 mm noise), timed with CUDA events,
+    inputs resident. The network is trained first on n_train held-out scenes,
+    on the GPU.
+
+    Equal inlier count, one stopping rule for every arm: each scene's target
+    is 99% of the best count plain RANSAC reaches with up to 10,000
+    hypotheses (the reference's rand() stream and adaptive stop, p = 0.99),
+    and every arm stops a scene at the first hypothesis whose exact count
+    over all 50,000 points reaches it:
+      plain_to_count     uniform draws from the reference's stream;
+      learned_to_count   features + MLP + preemptive weighted proposal;
+      preemptive_uniform_to_count
+                         the same preemptive rounds over the same candidates
+                         with equal weights (what the preemption alone buys).
+    Without a target (the learned arm's own budget): one preemptive round,
+    its best hypotheses counted exactly; the fraction of scenes within 1% of
+    plain's 10,000-hypothesis best."""
     import torch
     from rvpoint_b200 import datasets as D
     from rvpoint_b200 import learned as LR
@@ -375,14 +588,26 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
 
     t_plain, (_, best, it_plain) = timed(lambda: LR.ransac_frames(be, 10_000, T, ctx=ctx))
     tg = torch.ceil(best.double() * 0.99).to(torch.int32)
-    t_ptg, (_, _, it_ptg) = timed(lambda: LR.ransac_frames(be, 10_000, T, targets=tg, ctx=ctx))
+    t_ptg, (_, bp, it_ptg) = timed(lambda: LR.ransac_frames(be, 10_000, T, targets=tg, ctx=ctx))
     lr = LR.LearnedRansac(scorer)
     cand, coffs = lr.prepare(be)
     t_l, (_, bl, it_l) = timed(lambda: lr.run(be, cand, coffs, 10_000, T, targets=tg))
     t_f, feat = timed(lambda: LR.proposal_features(scorer, be, cand, coffs, lr.cell, lr.scope))
     t_m, logits = timed(lambda: scorer.forward(feat))
     t_w, _ = timed(lambda: lr.ransac(be, cand, coffs, logits, 10_000, T, targets=tg))
+    flat = torch.zeros_like(logits)
+    t_u, (_, bu, it_u) = timed(lambda: lr.ransac(be, cand, coffs, flat, 10_000, T, targets=tg))
+    # the learned arm on its own budget: one preemptive round, no target
+    one = LR.LearnedRansac(scorer, draws=lr.draws)
+
+    def one_round():
+        f_ = LR.proposal_features(scorer, be, cand, coffs, one.cell, one.scope)
+        lg = scorer.forward(f_)
+        return LR.ransac_preemptive(be, cand, coffs, lg, T, draws=one.draws, max_rounds=1,
+                                    seed=one.seed, logit_power=one.logit_power, ctx=ctx)
+    t_1, (_, b1, _) = timed(one_round)
     q = lambda t, p: float(t.double().quantile(p).item())  # noqa: E731
+    within = lambda b: float((b.double() >= 0.99 * best.double()).float().mean().item())  # noqa: E731
     out = {"scenes": n_scenes, "points_per_scene": 50_000, "thresh": T,
            "train_scenes": n_train, "train_seconds": info["seconds"],
            "train_loss_first_last": [info["losses"][0][1], info["losses"][-1][1]],
@@ -390,18 +615,30 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
            "proposal": (f"preemptive: {lr.draws} draws per round ranked on the candidates, "
                         "best 32 counted exactly" if lr.preemptive else "weighted draws, "
                         "each counted exactly"),
+           "stopping_rule": "every arm stops a scene at 99% of plain RANSAC's "
+                            "10,000-hypothesis best count",
            "plain_10k_ms": t_plain,
            "plain_10k_hypotheses_mean": float(it_plain.double().mean().item()),
-           "plain_to_target_ms": t_ptg,
-           "plain_hypotheses_to_target": {"mean": float(it_ptg.double().mean().item()),
-                                          "median": q(it_ptg, 0.5), "p90": q(it_ptg, 0.9)},
-           "learned_to_target_ms": t_l, "learned_parts_ms": {"features": t_f, "mlp": t_m,
-                                                             "weighted_ransac": t_w},
-           "learned_hypotheses_drawn_to_target": {"mean": float(it_l.double().mean().item()),
-                                            "median": q(it_l, 0.5), "p90": q(it_l, 0.9)},
+           "plain_to_count_ms": t_ptg,
+           "plain_hypotheses_to_count": {"mean": float(it_ptg.double().mean().item()),
+                                         "median": q(it_ptg, 0.5), "p90": q(it_ptg, 0.9)},
+           "learned_to_count_ms": t_l,
+           "learned_parts_ms": {"features": t_f, "mlp": t_m, "weighted_ransac": t_w},
+           "learned_hypotheses_drawn_to_count": {"mean": float(it_l.double().mean().item()),
+                                                 "median": q(it_l, 0.5), "p90": q(it_l, 0.9)},
            "learned_reached_fraction": float((bl >= tg).float().mean().item()),
+           "preemptive_uniform_to_count_ms": t_u,
+           "preemptive_uniform_hypotheses_drawn_to_count": {
+               "mean": float(it_u.double().mean().item()), "median": q(it_u, 0.5),
+               "p90": q(it_u, 0.9)},
+           "preemptive_uniform_reached_fraction": float((bu >= tg).float().mean().item()),
+           "time_ratio_plain_to_count_over_learned": t_ptg / t_l,
+           "time_ratio_preemptive_uniform_over_learned": t_u / t_l,
            "time_ratio_plain10k_over_learned": t_plain / t_l,
-           "time_ratio_plain_to_target_over_learned": t_ptg / t_l}
+           "learned_one_round_no_target": {
+               "ms": t_1, "draws_per_scene": one.draws,
+               "scenes_within_1pct_of_plain_10k": within(b1),
+               "mean_count_over_plain_10k": float((b1.double() / best.double()).mean().item())}}
     scorer.close()
     return out
 
@@ -443,10 +680,10 @@ def main():
     pipe.run_device(*args)
     pipe.fit_tables()  # bucket table sized to this workload (stays in L2)
     if a.cell > 0:
-        pipe.set_tuning(a.cell, 256, 0)
+        pipe.set_tuning(a.cell, a.block, a.qpw)
         pipe.set_search_radius_factor(a.rfac)
         pipe.set_lane_levels(a.lane_levels)
-        best = {"cell": a.cell, "block": 256, "qpw": 0, "rfac": a.rfac,
+        best = {"cell": a.cell, "block": a.block, "qpw": a.qpw, "rfac": a.rfac,
                 "lane_levels": a.lane_levels, "fixed": True}
     elif not a.no_tune:
         best, _ = autotune.tune(pipe, *args)
@@ -606,7 +843,28 @@ def main():
             "stage": dom, "peak_source": peak_src,
             "algorithmic_bytes_per_launch": alg, "launch_ms": timed[dom]}
 
-    cpu = cpu_baseline(batch, a.cpu_budget_s) if world == 1 else None
+    cpu = singles = None
+    if world == 1:
+        pipe.run_device(*args)  # the timed batch once more, then its results to the host
+        torch.cuda.synchronize()
+        singles = single_cloud_legs(ctx) if not a.no_singles else None
+        cpu, cpu_single = cpu_baseline(batch, a.cpu_frames, pipe.results(),
+                                       singles=singles is not None)
+        if singles is not None and cpu_single:
+            rc = cpu_single.get("room_chain_100k")
+            if rc:
+                t = sum(rc["seconds"].values())
+                singles["room_chain_100k"].update(
+                    {"cpu_ms": t * 1e3, "cpu_mpts_s": 0.1 / t, "cpu_stage_s": rc["seconds"],
+                     "cpu_cores": 1, "cpu_same_sizes": rc["voxels"] == singles[
+                         "room_chain_100k"]["voxels"] and rc["kept"] == singles[
+                         "room_chain_100k"]["kept"] and rc["ransac"] == singles[
+                         "room_chain_100k"]["ransac"]})
+            lr = cpu_single.get("lidar_frame_radius")
+            if lr:
+                singles["lidar_frame_radius"].update(
+                    {"radius_cpu_ms": lr["radius_s"] * 1e3, "max_nn16_cpu_ms": lr["knn16_s"] * 1e3,
+                     "cpu_cores": 1, "cpu_pairs_r05": lr["pairs"]})
     learned = learned_leg(ctx, a.learned_scenes, 64) if a.learned_scenes > 0 else None
     nxt = next_rows_leg(ctx, batch) if world == 1 and not a.no_next_rows else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -621,7 +879,8 @@ def main():
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps, "clocks": clk,
             "stages_ms": {k: v for k, v in stages.items() if k != "runs"},
-            "graph": graph, "learned_ransac": learned, "next_rows": nxt}
+            "graph": graph, "learned_ransac": learned, "next_rows": nxt,
+            "single_cloud": singles}
     print(json.dumps(line), flush=True)
 
 

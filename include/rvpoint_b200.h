@@ -35,7 +35,9 @@ typedef enum {
   RVP_ERR_INVALID_ARG = 1, /* bad pointer, size or parameter */
   RVP_ERR_OOM = 2,         /* device or pinned allocation failed */
   RVP_ERR_CAPACITY = 3,    /* caller's output buffer too small; *total says how much */
-  RVP_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  RVP_ERR_TIMEOUT = 4,     /* reserved for a bounded device-side wait that gives up; no
+                              kernel of this version waits on another, so no entry
+                              point returns it */
   RVP_ERR_CUDA = 5,        /* CUDA runtime error (message in rvp_last_error) */
   RVP_ERR_NO_DEVICE = 6    /* no CUDA device / kernels not loadable */
 } rvp_status;
@@ -60,22 +62,31 @@ RVP_API uint64_t rvp_context_launch_count(const rvp_context *ctx);
 /* Library version string. */
 RVP_API const char *rvp_version(void);
 
+/* ---- test hooks (no counterpart in the reference) ------------------------- */
+/* After `after` more successful device or pinned allocations, every further
+ * allocation of the library fails as an out-of-memory would (the entry point
+ * returns RVP_ERR_OOM, having freed what it allocated); after < 0 turns the
+ * injection off. Process-wide; for tests of the error paths. */
+RVP_API rvp_status rvp_debug_fail_allocation(long long after);
+/* Bytes of device memory and of pinned host memory the library holds now. */
+RVP_API rvp_status rvp_debug_live_bytes(long long *device_bytes, long long *pinned_bytes);
+
 /* ---- SpatialHash: search/spatial_hashing.h:12-53 ------------------------- */
 RVP_API rvp_status rvp_hash_create(rvp_context *ctx, rvp_hash **out);
 RVP_API rvp_status rvp_hash_destroy(rvp_hash *h);
 /* setHashPrimes, spatial_hashing.h:24-27 */
 RVP_API rvp_status rvp_hash_set_primes(rvp_hash *h, int64_t p1, int64_t p2);
-/* setInputCloud, spatial_hashing.cpp:76-151 (bbox, eps pad, grid dims).
+/* setInputCloud, spatial_hashing.cpp:21-96 (bbox, eps pad, grid dims).
  * The cloud is copied to the device (the reference keeps a pointer). */
 RVP_API rvp_status rvp_hash_set_input_cloud(rvp_hash *h, const float *x, const float *y,
                                     const float *z, size_t n, float cell_size,
                                     int mem);
-/* build, spatial_hashing.cpp:153-163: radix sort of cell keys, bucket
+/* build, spatial_hashing.cpp:98-108: radix sort of cell keys, bucket
  * offsets, device hash table of occupied buckets. */
 RVP_API rvp_status rvp_hash_build(rvp_hash *h);
 /* 1 if two different cells share a hash key under the current primes. */
 RVP_API rvp_status rvp_hash_has_collisions(rvp_hash *h, int *out);
-/* radiusSearch, spatial_hashing.cpp:165-223, for nq queries at once.
+/* radiusSearch, spatial_hashing.cpp:110-168, for nq queries at once.
  * CSR result: offsets[nq+1] (int64), indices/dists hold offsets[nq] entries,
  * each query's list sorted by (d2, index) and cut at max_nn when max_nn > 0.
  * dists are squared distances, as in the reference. If the total exceeds
@@ -116,11 +127,11 @@ RVP_API rvp_status rvp_sor_spatial_hash(rvp_hash *h, int k, float alpha,
 
 /* ---- normals: features/normal_estimation.h:15-34 ------------------------- */
 /* normal_estimation_rvv(in, const SpatialHash&, ...) (normal_estimation.cpp
- * :240-265) on the hash's cloud: neighbours = radiusSearch(q, radius). */
+ * :189-214) on the hash's cloud: neighbours = radiusSearch(q, radius). */
 RVP_API rvp_status rvp_normals_radius(rvp_hash *h, float radius, float vp_x,
                               float vp_y, float vp_z, int eigen_iters, int mem,
                               float *nx, float *ny, float *nz);
-/* normal_estimation_sc (normal_estimation.cpp:123-163): k+1 nearest incl.
+/* normal_estimation_sc (normal_estimation.cpp:72-112): k+1 nearest incl.
  * self (ties by index), centroid divided by k+1. */
 RVP_API rvp_status rvp_normals_knn(rvp_context *ctx, const float *x, const float *y,
                            const float *z, size_t n, int k, float vp_x,
@@ -261,7 +272,10 @@ typedef struct {
   float ransac_prob;
   float cell_size;       /* grid cell for the neighbour searches (0 = auto) */
   int block_threads;     /* kNN kernel block size (0 = auto) */
-  int queries_per_warp;  /* kNN queries per warp: 1 (warp/query) or 32 (0 = auto) */
+  int queries_per_warp;  /* kNN kernel mode: 0 one query per lane at every grid level
+                            (default), 1 one warp per query, 2 shared-memory tiles,
+                            3 a cooperative level-0 pass (all lanes test the same
+                            candidate) before the per-lane kernels */
 } rvp_pipeline_config;
 
 RVP_API rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,

@@ -50,12 +50,33 @@ def unpack(params: np.ndarray):
     return W1, b1, W2, b2, w3, b3
 
 
-def forward(params, mean, std, feat):
-    """Logits (float64) of feat (n x 8) with the BF16-rounded weights."""
+def tf32_round(x: np.ndarray) -> np.ndarray:
+    """float32 -> TF32 (10 mantissa bits, round to nearest, ties away from
+    zero: cvt.rna.tf32.f32) -> float32."""
+    b = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x1000) & 0xFFFFE000
+    return b.astype(np.uint32).view(np.float32)
+
+
+def forward(params, mean, std, feat, tensor_core: bool = False):
+    """Logits (float64) of feat (n x 8) with the BF16-rounded weights.
+
+    tensor_core: the roundings of the GPU's tensor-core forward pass --
+    normalised inputs computed in float32 ((feat - mean) * (1 / std)) and
+    rounded to TF32, hidden layer 1 rounded to BF16 after its bias and ReLU;
+    every sum in float64."""
     W1, b1, W2, b2, w3, b3 = unpack(bf16_round(params))
-    xn = (np.asarray(feat, np.float64) - np.asarray(mean, np.float64)) / np.asarray(std, np.float64)
+    if tensor_core:
+        inv = (np.float32(1.0) / np.asarray(std, np.float32)).astype(np.float32)
+        x32 = (np.asarray(feat, np.float32) - np.asarray(mean, np.float32)) * inv
+        xn = tf32_round(x32.astype(np.float32)).astype(np.float64)
+    else:
+        xn = (np.asarray(feat, np.float64) - np.asarray(mean, np.float64)) / \
+            np.asarray(std, np.float64)
     z1 = xn @ W1.T + b1
     h1 = np.maximum(z1, 0.0)
+    if tensor_core:
+        h1 = bf16_round(h1.astype(np.float32)).astype(np.float64)
     z2 = h1 @ W2.T + b2
     h2 = np.maximum(z2, 0.0)
     return h2 @ w3 + b3

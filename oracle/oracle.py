@@ -30,10 +30,23 @@ _dp = C.POINTER(C.c_double)
 _sz = C.c_size_t
 
 
+# where the reference checkout is looked for when RVP_REFERENCE is not set
+_REFERENCE_CHECKOUT = "/root/reference"
+
+
+def reference_checkout():
+    """The reference checkout to compile oracle/_ref from (None if absent)."""
+    ref = os.environ.get("RVP_REFERENCE", _REFERENCE_CHECKOUT)
+    return ref if os.path.exists(os.path.join(ref, "src", "core", "point_types.h")) else None
+
+
 def build(quiet: bool = True) -> None:
     """Compile the restatement (and the reference, when its sources exist)."""
-    subprocess.run(["make", "-C", HERE], check=True,
-                   stdout=subprocess.DEVNULL if quiet else None)
+    cmd = ["make", "-C", HERE]
+    ref = reference_checkout()
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL if quiet else None)
 
 
 def _f(a):
@@ -123,6 +136,8 @@ class Restatement:
         L.rvo_normals_octree.argtypes = [C.c_int, _fp, _fp, _fp, _sz, C.c_int, C.c_int,
                                          C.c_float, C.c_float, C.c_float, C.c_float,
                                          C.c_float, C.c_int, _fp, _fp, _fp]
+        L.rvo_knn_lists.restype = None
+        L.rvo_knn_lists.argtypes = [_fp, _fp, _fp, _sz, C.c_int, _ip, _fp]
         L.rvo_normals_knn_exact_f64.restype = None
         L.rvo_normals_knn_exact_f64.argtypes = [_fp, _fp, _fp, _sz, _ip, C.c_int, C.c_float,
                                                 C.c_float, C.c_float, _dp, _dp, _dp, _dp]
@@ -257,6 +272,15 @@ class Restatement:
                                   vp[0], vp[1], vp[2], iters, _ptr(nx, _fp), _ptr(ny, _fp),
                                   _ptr(nz, _fp))
         return np.stack([nx[:n], ny[:n], nz[:n]], 1)
+
+    def knn_lists(self, c, kk):
+        """(n, kk) indices and squared distances of every point's kk nearest
+        (self included), ordered by (d2, index); brute force over threads."""
+        x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)
+        n = x.shape[0]
+        idx = np.zeros((max(n, 1), kk), np.int32); d2 = np.zeros((max(n, 1), kk), np.float32)
+        self.L.rvo_knn_lists(xp, yp, zp, n, kk, _ptr(idx, _ip), _ptr(d2, _fp))
+        return idx[:n], d2[:n]
 
     def normals_exact_f64(self, c, nbr_idx, vp=(0, 0, 0)):
         x, xp = _f(c.x); y, yp = _f(c.y); z, zp = _f(c.z)

@@ -42,7 +42,7 @@ PointCloudSoA soa(const float *x, const float *y, const float *z, size_t n) {
 extern "C" {
 
 // SpatialHash::setInputCloud + build + radiusSearch for every query
-// (spatial_hashing.cpp:76-223). CSR output: offsets[nq+1]; idx/d2 hold
+// (spatial_hashing.cpp:21-168). CSR output: offsets[nq+1]; idx/d2 hold
 // offsets[nq] entries. Returns -1 when cap is too small (offsets still valid).
 long long ref_hash_radius_search(const float *x, const float *y, const float *z,
                                  size_t n, float cell, const float *qx,
@@ -102,7 +102,7 @@ size_t ref_sor_spatial_hash(const float *x, const float *y, const float *z,
                           search_radius);
 }
 
-// normal_estimation_rvv(in, SpatialHash, ...) (normal_estimation.cpp:240-265).
+// normal_estimation_rvv(in, SpatialHash, ...) (normal_estimation.cpp:189-214).
 void ref_normals_hash(const float *x, const float *y, const float *z, size_t n,
                       float cell, int k, float radius, float vpx, float vpy,
                       float vpz, int iters, float *nx, float *ny, float *nz) {
@@ -113,7 +113,7 @@ void ref_normals_hash(const float *x, const float *y, const float *z, size_t n,
   normal_estimation_rvv(c, h, nx, ny, nz, k, radius, vpx, vpy, vpz, iters);
 }
 
-// normal_estimation_sc (normal_estimation.cpp:123-163): brute-force k+1 NN.
+// normal_estimation_sc (normal_estimation.cpp:72-112): brute-force k+1 NN.
 void ref_normals_sc(const float *aos, size_t n, int k, float radius, float vpx,
                     float vpy, float vpz, int iters, float *nx, float *ny,
                     float *nz) {

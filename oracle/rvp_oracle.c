@@ -5,12 +5,15 @@
  * Arithmetic is written in the reference's evaluation order; the Makefile
  * compiles with -ffp-contract=off so that no FMA changes a rounding.
  */
+#define _GNU_SOURCE
 #include "rvp_oracle.h"
 
 #include <float.h>
+#include <pthread.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 /* ------------------------------------------------------------------------ */
 /* SpatialHash                                                              */
@@ -49,8 +52,8 @@ static int64_t hash_cell(const rvo_hash *h, int ix, int iy, int iz) {
   return (int64_t)ix + (int64_t)iy * h->p1 + (int64_t)iz * h->p2;
 }
 
-/* setInputCloud (spatial_hashing.cpp:76-151, scalar branch :131-138) and
- * build (:153-163). Buckets keep input order, like push_back. */
+/* setInputCloud (spatial_hashing.cpp:21-96, scalar branch :76-83) and
+ * build (:98-108). Buckets keep input order, like push_back. */
 static void hash_build(rvo_hash *h, const float *x, const float *y,
                        const float *z, size_t n, float cell, int64_t p1,
                        int64_t p2) {
@@ -124,7 +127,7 @@ typedef struct {
   int idx;
 } nbr;
 
-/* std::pair<float,int> operator< : spatial_hashing.cpp:204-209. */
+/* std::pair<float,int> operator< : spatial_hashing.cpp:149-154. */
 static int cmp_nbr(const void *a, const void *b) {
   const nbr *p = (const nbr *)a, *q = (const nbr *)b;
   if (p->d2 < q->d2) return -1;
@@ -147,8 +150,8 @@ static void nv_push(nbr_vec *v, float d2, int idx) {
   v->n++;
 }
 
-/* radiusSearch: spatial_hashing.cpp:165-223, with the gather-filter of
- * rvv_common.cpp:114-133 (d2 = dx*dx + dy*dy + dz*dz, keep d2 <= r2). */
+/* radiusSearch: spatial_hashing.cpp:110-168, with the gather-filter of
+ * rvv_common.cpp:49-68 (d2 = dx*dx + dy*dy + dz*dz, keep d2 <= r2). */
 static size_t hash_radius(const rvo_hash *h, const float *x, const float *y,
                           const float *z, float qx, float qy, float qz,
                           float radius, int max_nn, nbr_vec *out) {
@@ -297,17 +300,66 @@ static size_t sor_filter(const float *x, const float *y, const float *z,
   return count;
 }
 
-/* sor_sc (statistical_outlier_removal.cpp:19-63): the k+1 smallest d2 over
- * all n points (self included), then mean of sqrt over ranks 1..k. */
-size_t rvo_sor_exact(const float *x, const float *y, const float *z, size_t n,
-                     int k, float alpha, float *out, float *mean_dists,
-                     unsigned char *keep) {
-  if (n == 0) return 0;
-  if (k < 1 || (size_t)k + 1 > n) return 0; /* reference: partial_sort past end */
-  float *md = mean_dists ? mean_dists : (float *)malloc(n * sizeof(float));
-  float *best = (float *)malloc((size_t)(k + 1) * sizeof(float));
-  const int kk = k + 1;
-  for (size_t i = 0; i < n; ++i) {
+/* ------------------------------------------------------------------------ */
+/* Row-parallel driver for the brute-force searches: every query's result is  */
+/* independent of the others, so the rows are split over threads (count from  */
+/* RVO_THREADS, else the online cores); the arithmetic of each row stays the  */
+/* sequential restatement.                                                    */
+/* ------------------------------------------------------------------------ */
+typedef void (*row_fn)(void *job, size_t lo, size_t hi);
+typedef struct {
+  row_fn fn;
+  void *job;
+  size_t n;
+  size_t next; /* next unclaimed row, taken in chunks under the lock */
+  pthread_mutex_t lock;
+} par_ctx;
+
+static void *par_worker(void *arg) {
+  par_ctx *c = (par_ctx *)arg;
+  const size_t chunk = 64;
+  for (;;) {
+    pthread_mutex_lock(&c->lock);
+    const size_t lo = c->next;
+    c->next = lo + chunk < c->n ? lo + chunk : c->n;
+    const size_t hi = c->next;
+    pthread_mutex_unlock(&c->lock);
+    if (lo >= hi) return NULL;
+    c->fn(c->job, lo, hi);
+  }
+}
+
+static void run_parallel(size_t n, row_fn fn, void *job) {
+  long t = 0;
+  const char *env = getenv("RVO_THREADS");
+  if (env) t = strtol(env, NULL, 10);
+  if (t <= 0) t = sysconf(_SC_NPROCESSORS_ONLN);
+  if (t < 1) t = 1;
+  if (t > 256) t = 256;
+  if ((size_t)t > n / 64 + 1) t = (long)(n / 64 + 1);
+  par_ctx c = {fn, job, n, 0, PTHREAD_MUTEX_INITIALIZER};
+  pthread_t th[256];
+  long started = 0;
+  for (long i = 1; i < t; ++i)
+    if (pthread_create(&th[started], NULL, par_worker, &c) == 0) ++started;
+  par_worker(&c);
+  for (long i = 0; i < started; ++i) pthread_join(th[i], NULL);
+}
+
+typedef struct {
+  const float *x, *y, *z;
+  size_t n;
+  int k;
+  float *md;
+} sor_job;
+
+static void sor_rows(void *arg, size_t lo, size_t hi) {
+  const sor_job *J = (const sor_job *)arg;
+  const float *x = J->x, *y = J->y, *z = J->z;
+  const size_t n = J->n;
+  const int k = J->k, kk = k + 1;
+  float *best = (float *)malloc((size_t)kk * sizeof(float));
+  for (size_t i = lo; i < hi; ++i) {
     int cnt = 0;
     for (size_t j = 0; j < n; ++j) {
       const float dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
@@ -322,9 +374,21 @@ size_t rvo_sor_exact(const float *x, const float *y, const float *z, size_t n,
     }
     float sum = 0.0f;
     for (int j = 1; j <= k; ++j) sum += sqrtf(best[j]);
-    md[i] = sum / (float)k;
+    J->md[i] = sum / (float)k;
   }
   free(best);
+}
+
+/* sor_sc (statistical_outlier_removal.cpp:19-63): the k+1 smallest d2 over
+ * all n points (self included), then mean of sqrt over ranks 1..k. */
+size_t rvo_sor_exact(const float *x, const float *y, const float *z, size_t n,
+                     int k, float alpha, float *out, float *mean_dists,
+                     unsigned char *keep) {
+  if (n == 0) return 0;
+  if (k < 1 || (size_t)k + 1 > n) return 0; /* reference: partial_sort past end */
+  float *md = mean_dists ? mean_dists : (float *)malloc(n * sizeof(float));
+  sor_job job = {x, y, z, n, k, md};
+  run_parallel(n, sor_rows, &job);
   size_t c = sor_filter(x, y, z, n, md, alpha, out, keep);
   if (!mean_dists) free(md);
   return c;
@@ -361,7 +425,7 @@ size_t rvo_sor_radius(const float *x, const float *y, const float *z, size_t n,
 /* Normals                                                                  */
 /* ------------------------------------------------------------------------ */
 
-/* simple_eigen3x3_smallest (normal_estimation.cpp:67-103), float. The
+/* simple_eigen3x3_smallest (normal_estimation.cpp:16-52), float. The
  * rotation updates only A[p][p], A[q][q] and A[p][q], as the reference does. */
 static void eigen_smallest_f(float cov[3][3], float *nx, float *ny, float *nz,
                              int iters) {
@@ -421,7 +485,7 @@ static void eigen_smallest_d(double cov[3][3], double *nx, double *ny,
   *nz = V[2][m];
 }
 
-/* flipNormalTowardsViewpoint (normal_estimation.cpp:106-118). */
+/* flipNormalTowardsViewpoint (normal_estimation.cpp:55-67). */
 static void flip_f(float px, float py, float pz, float vpx, float vpy,
                    float vpz, float *nx, float *ny, float *nz) {
   const float vx = vpx - px, vy = vpy - py, vz = vpz - pz;
@@ -445,7 +509,7 @@ static void flip_d(double px, double py, double pz, double vpx, double vpy,
 }
 
 /* Covariance of a neighbour list: compute_covariance_rvv
- * (normal_estimation.cpp:168-193) when div_centroid == 0 (centroid scaled by
+ * (normal_estimation.cpp:117-142) when div_centroid == 0 (centroid scaled by
  * 1.0f/n), normal_estimation_sc (:141-158) when div_centroid != 0 (divided by
  * n). Then eigen + flip. */
 static void normal_from_list_f(const float *x, const float *y, const float *z,
@@ -513,7 +577,7 @@ static void normal_from_list_d(const float *x, const float *y, const float *z,
 }
 
 /* normal_estimation_rvv(in, const SpatialHash&, ...) (normal_estimation.cpp
- * :240-265): radius neighbours sorted by (d2, idx); fewer than 3 -> zero. */
+ * :189-214): radius neighbours sorted by (d2, idx); fewer than 3 -> zero. */
 void rvo_normals_radius(const float *x, const float *y, const float *z,
                         size_t n, float cell, float radius, float vpx,
                         float vpy, float vpz, int iters, int use_f64,
@@ -558,7 +622,41 @@ static void knn_brute(const float *x, const float *y, const float *z, size_t n,
   }
 }
 
-/* normal_estimation_sc (normal_estimation.cpp:123-163). The reference's
+typedef struct {
+  const float *x, *y, *z;
+  size_t n;
+  int kk;
+  float vpx, vpy, vpz;
+  int iters, use_f64;
+  float *nx, *ny, *nz; /* normals, or */
+  int *idx;            /* the lists themselves (n * kk) */
+  float *d2;
+} normals_job;
+
+static void normals_rows(void *arg, size_t lo, size_t hi) {
+  const normals_job *J = (const normals_job *)arg;
+  const float *x = J->x, *y = J->y, *z = J->z;
+  const int kk = J->kk;
+  nbr *best = (nbr *)malloc((size_t)kk * sizeof(nbr));
+  for (size_t i = lo; i < hi; ++i) {
+    knn_brute(x, y, z, J->n, i, kk, best);
+    if (J->idx) {
+      for (int t = 0; t < kk; ++t) {
+        J->idx[i * (size_t)kk + t] = best[t].idx;
+        J->d2[i * (size_t)kk + t] = best[t].d2;
+      }
+    } else if (J->use_f64) {
+      normal_from_list_d(x, y, z, best, (size_t)kk, 1, x[i], y[i], z[i], J->vpx, J->vpy,
+                         J->vpz, J->iters, J->nx + i, J->ny + i, J->nz + i);
+    } else {
+      normal_from_list_f(x, y, z, best, (size_t)kk, 1, x[i], y[i], z[i], J->vpx, J->vpy,
+                         J->vpz, J->iters, J->nx + i, J->ny + i, J->nz + i);
+    }
+  }
+  free(best);
+}
+
+/* normal_estimation_sc (normal_estimation.cpp:72-112). The reference's
  * partial_sort leaves the order of equal distances unspecified; this
  * restatement (and the GPU path) breaks ties by index. */
 void rvo_normals_knn(const float *x, const float *y, const float *z, size_t n,
@@ -567,17 +665,18 @@ void rvo_normals_knn(const float *x, const float *y, const float *z, size_t n,
   if (n == 0) return;
   const int kk = k + 1;
   if ((size_t)kk > n) return;
-  nbr *best = (nbr *)malloc((size_t)kk * sizeof(nbr));
-  for (size_t i = 0; i < n; ++i) {
-    knn_brute(x, y, z, n, i, kk, best);
-    if (use_f64)
-      normal_from_list_d(x, y, z, best, (size_t)kk, 1, x[i], y[i], z[i], vpx,
-                         vpy, vpz, iters, nx + i, ny + i, nz + i);
-    else
-      normal_from_list_f(x, y, z, best, (size_t)kk, 1, x[i], y[i], z[i], vpx,
-                         vpy, vpz, iters, nx + i, ny + i, nz + i);
-  }
-  free(best);
+  normals_job job = {x, y, z, n, kk, vpx, vpy, vpz, iters, use_f64, nx, ny, nz, NULL, NULL};
+  run_parallel(n, normals_rows, &job);
+}
+
+/* The k+1 nearest of every point (self included) by brute force, ordered by
+ * (d2, idx): the neighbour sets normal_estimation_sc (normal_estimation.cpp:
+ * 79-88) selects, with ties broken by index. idx/d2: n * (k+1) each. */
+void rvo_knn_lists(const float *x, const float *y, const float *z, size_t n,
+                   int kk, int *idx, float *d2) {
+  if (n == 0 || kk < 1 || (size_t)kk > n) return;
+  normals_job job = {x, y, z, n, kk, 0, 0, 0, 0, 0, NULL, NULL, NULL, idx, d2};
+  run_parallel(n, normals_rows, &job);
 }
 
 /* Cyclic Jacobi on a symmetric 3x3 (double), iterated until the off-diagonal

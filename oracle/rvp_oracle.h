@@ -128,6 +128,11 @@ void rvo_normals_octree(int kind, const float *x, const float *y, const float *z
                         int cap_leaf, int max_depth, float eps, float radius, float vpx,
                         float vpy, float vpz, int iters, float *nx, float *ny, float *nz);
 
+/* The k+1 (= kk) nearest of every point, self included, by brute force,
+ * ordered by (d2, idx): idx and d2 hold n * kk entries each. */
+void rvo_knn_lists(const float *x, const float *y, const float *z, size_t n, int kk,
+                   int *idx, float *d2);
+
 #ifdef __cplusplus
 }
 #endif

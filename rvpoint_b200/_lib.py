@@ -57,6 +57,8 @@ I = C.c_int
 # name -> (restype, argtypes)
 SIGNATURES = {
     "rvp_context_create": (I, [I, C.POINTER(P)]),
+    "rvp_debug_fail_allocation": (I, [C.c_longlong]),
+    "rvp_debug_live_bytes": (I, [C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "rvp_context_destroy": (I, [P]),
     "rvp_context_set_stream": (I, [P, P]),
     "rvp_context_synchronize": (I, [P]),

@@ -38,12 +38,18 @@ def _time_run(pipe, args, reps: int) -> float:
 
 def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
          cells: Optional[Iterable[float]] = None,
-         blocks: Iterable[int] = (256,),
-         qpws: Iterable[int] = (0,), rfacs: Iterable[float] = (0.7, 1.0),
+         blocks: Iterable[int] = (128, 256, 512),
+         qpws: Iterable[int] = (0, 3), rfacs: Iterable[float] = (0.7, 0.85, 1.0),
          lane_levels: Iterable[int] = (3, 2),
          reps: int = 2,
          cache_file: Optional[str] = None, verbose: bool = False) -> Tuple[dict, list]:
-    """Returns (best setting, all trials) and applies the best to `pipe`."""
+    """Returns (best setting, all trials) and applies the best to `pipe`.
+
+    Two stages: every combination of cell size, kNN kernel mode
+    (queries_per_warp: 0 one query per lane at every grid level, 3 a
+    cooperative level-0 pass first), first-pass radius factor and per-lane
+    grid levels at the default block shape; then the block shape of the
+    warp-per-query kernel at the best of those."""
     sig = signature(n_points, n_frames, pipe.cfg)
     if cache_file and os.path.exists(cache_file) and not _CACHE:
         try:
@@ -52,33 +58,34 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
             pass
     if sig in _CACHE:
         b = _CACHE[sig]
-        pipe.set_tuning(b["cell"], b["block"], b["qpw"])
-        pipe.set_search_radius_factor(b["rfac"])
-        pipe.set_lane_levels(b.get("lane_levels", 0))
+        _apply(pipe, b)
         return b, []
     leaf = pipe.cfg.leaf_size
     cells = list(cells) if cells is not None else [leaf * m for m in (3.0, 5.0, 8.0, 10.0, 12.0)]
     args = (x, y, z, offsets, n_frames, n_points)
     trials = []
+
+    def trial(setting):
+        _apply(pipe, setting)
+        pipe.run_device(*args)  # warm
+        t = _time_run(pipe, args, reps)
+        r = dict(setting, ms=t)
+        trials.append(r)
+        if verbose:
+            print(f"[autotune] {r}", flush=True)
+        return r
+
     for c in cells:
-        for b in blocks:
-            for q in qpws:
-                for rf in rfacs:
-                    for ll in lane_levels:
-                        pipe.set_tuning(c, b, q)
-                        pipe.set_search_radius_factor(rf)
-                        pipe.set_lane_levels(ll)
-                        pipe.run_device(*args)  # warm
-                        t = _time_run(pipe, args, reps)
-                        trials.append({"cell": c, "block": b, "qpw": q, "rfac": rf,
-                                       "lane_levels": ll, "ms": t})
-                        if verbose:
-                            print(f"[autotune] cell={c:.3f} block={b} qpw={q} rfac={rf} "
-                                  f"lane_levels={ll}: {t:.3f} ms", flush=True)
+        for q in qpws:
+            for rf in rfacs:
+                for ll in lane_levels:
+                    trial({"cell": c, "block": 0, "qpw": q, "rfac": rf, "lane_levels": ll})
     best = min(trials, key=lambda r: r["ms"])
-    pipe.set_tuning(best["cell"], best["block"], best["qpw"])
-    pipe.set_search_radius_factor(best["rfac"])
-    pipe.set_lane_levels(best["lane_levels"])
+    for b in blocks:
+        trial(dict({k: v for k, v in best.items() if k != "ms"}, block=b))
+    best = dict(min(trials, key=lambda r: r["ms"]))
+    best["trials"] = len(trials)
+    _apply(pipe, best)
     _CACHE[sig] = best
     if cache_file:
         try:
@@ -86,3 +93,9 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
         except Exception:
             pass
     return best, trials
+
+
+def _apply(pipe, s: dict) -> None:
+    pipe.set_tuning(s["cell"], s["block"], s["qpw"])
+    pipe.set_search_radius_factor(s["rfac"])
+    pipe.set_lane_levels(s.get("lane_levels", 0))

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <new>
 
 #include "internal.cuh"
@@ -17,35 +18,71 @@ using rvp::u64;
 // buffers
 // ---------------------------------------------------------------------------
 namespace rvp {
+// Every device and pinned allocation of the library goes through DevBuf /
+// HostBuf: the live byte counts are kept here, and a test hook
+// (rvp_debug_fail_allocation) can make the allocations after the next n
+// fail as an out-of-memory would.
+namespace {
+std::atomic<long long> g_live_device{0}, g_live_pinned{0};
+std::atomic<long long> g_fail_after{-1};  // < 0: off
+
+void check_injected_failure() {
+  long long left = g_fail_after.load();
+  while (left >= 0) {
+    if (left == 0) throw Error{RVP_ERR_OOM, "allocation failed (injected by rvp_debug_fail_allocation)"};
+    if (g_fail_after.compare_exchange_weak(left, left - 1)) return;
+  }
+}
+}  // namespace
+
 void DevBuf::reserve(size_t b) {
   if (b <= bytes && ptr) return;
-  if (ptr) cudaFree(ptr);
-  ptr = nullptr;
-  bytes = 0;
+  release();
   if (b == 0) b = 256;
+  check_injected_failure();
   RVP_CUDA_TRY(cudaMalloc(&ptr, b));
   bytes = b;
+  g_live_device += (long long)b;
 }
 void DevBuf::release() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    cudaFree(ptr);
+    g_live_device -= (long long)bytes;
+  }
   ptr = nullptr;
   bytes = 0;
 }
 void HostBuf::reserve(size_t b) {
   if (b <= bytes && ptr) return;
-  if (ptr) cudaFreeHost(ptr);
-  ptr = nullptr;
-  bytes = 0;
+  release();
   if (b == 0) b = 256;
+  check_injected_failure();
   RVP_CUDA_TRY(cudaMallocHost(&ptr, b));
   bytes = b;
+  g_live_pinned += (long long)b;
 }
 void HostBuf::release() {
-  if (ptr) cudaFreeHost(ptr);
+  if (ptr) {
+    cudaFreeHost(ptr);
+    g_live_pinned -= (long long)bytes;
+  }
   ptr = nullptr;
   bytes = 0;
 }
 }  // namespace rvp
+
+extern "C" {
+rvp_status rvp_debug_fail_allocation(long long after) {
+  rvp::g_fail_after = after < 0 ? -1 : after;
+  return RVP_OK;
+}
+
+rvp_status rvp_debug_live_bytes(long long *device_bytes, long long *pinned_bytes) {
+  if (device_bytes) *device_bytes = rvp::g_live_device.load();
+  if (pinned_bytes) *pinned_bytes = rvp::g_live_pinned.load();
+  return RVP_OK;
+}
+}
 
 struct rvp_hash {
   rvp_context *ctx = nullptr;
@@ -413,6 +450,11 @@ rvp_status rvp_hash_set_input_cloud(rvp_hash *h, const float *x, const float *y,
     RVP_REQUIRE(n < 0x7FFFFFFFull, "clouds are limited to 2^31 - 1 points");
     RVP_REQUIRE(cell_size > 0.0f && isfinite(cell_size), "cell_size must be > 0");
     set_device(ctx);
+    // no cloud until this call has completed (a failed allocation below
+    // leaves the hash without one, not with the previous cloud's size)
+    h->has_cloud = false;
+    h->built = false;
+    h->n = 0;
     h->x.reserve(n * 4 + 16); h->y.reserve(n * 4 + 16); h->z.reserve(n * 4 + 16);
     h->offs.reserve(16);
     if (n) {
@@ -437,6 +479,7 @@ rvp_status rvp_hash_build(rvp_hash *h) {
   return guard(ctx, [&] {
     RVP_REQUIRE(h->has_cloud, "setInputCloud before build");
     set_device(ctx);
+    h->built = false;  // set again only when this build has completed
     h->collision = 0;
     if (h->n > 0) {
       rvp::grid_build(ctx, h->grid, h->x.as<float>(), h->y.as<float>(), h->z.as<float>(),
@@ -730,7 +773,7 @@ rvp_status rvp_normals_radius(rvp_hash *h, float radius, float vp_x, float vp_y,
   return guard(ctx, [&] {
     RVP_REQUIRE(h->built, "build before normal estimation");
     const size_t n = h->n;
-    if (n == 0) return;  // normal_estimation.cpp:244
+    if (n == 0) return;  // normal_estimation.cpp:193
     RVP_REQUIRE(nx && ny && nz, "null output");
     set_device(ctx);
     const float *dx = h->x.as<float>(), *dy = h->y.as<float>(), *dz = h->z.as<float>();
@@ -762,7 +805,7 @@ rvp_status rvp_normals_knn(rvp_context *ctx, const float *x, const float *y, con
                            int mem, float *nx, float *ny, float *nz) {
   if (!ctx) return RVP_ERR_INVALID_ARG;
   return guard(ctx, [&] {
-    if (n == 0) return;  // normal_estimation.cpp:126
+    if (n == 0) return;  // normal_estimation.cpp:75
     RVP_REQUIRE(x && y && z && nx && ny && nz, "null pointer");
     RVP_REQUIRE(k >= 1 && k + 1 <= 64, "k must be in [1, 63]");
     RVP_REQUIRE((size_t)k + 1 <= n, "k+1 must not exceed the number of points");

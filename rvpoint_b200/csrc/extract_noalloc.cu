@@ -13,7 +13,11 @@
 // until the process exits, and every call on a device uses the same array:
 // calls whose kernels overlap on the GPU (different streams, no ordering)
 // race on it. Each call writes every count it reads before reading it, so
-// nothing has to be cleared between calls.
+// nothing has to be cleared between calls. The array's device address is
+// looked up on the first call on each device (cudaGetSymbolAddress, which
+// allocates nothing) and kept: make that first call before any stream
+// capture, and do not reset the device (cudaDeviceReset) while the library is
+// loaded, since the kept address would then be stale.
 #include <atomic>
 #include <mutex>
 
@@ -76,6 +80,10 @@ __device__ __forceinline__ u32 block_sum(u32 v, u32 *red) {
   return s;  // valid in thread 0
 }
 
+// Points of a tile are read strided (item j of thread t is point
+// base + j * NA_THREADS + t), so every load is coalesced; input order inside
+// the tile is then (j, warp, lane).
+
 // pass 1: inliers of each tile into the scratch
 __global__ __launch_bounds__(NA_THREADS) void k_na_count(const float *__restrict__ x,
                                                          const float *__restrict__ y,
@@ -95,66 +103,106 @@ __global__ __launch_bounds__(NA_THREADS) void k_na_count(const float *__restrict
   if (threadIdx.x == 0) tile_inliers[blockIdx.x] = s;
 }
 
-// pass 2: each tile adds up the tiles before it, ranks its points in input
-// order and writes inliers and outliers (AoS) to their final positions
+// pass 2: exclusive scan of the tile counts, in place (one block of 1024
+// threads, 8 consecutive counts each)
+constexpr int NA_SCAN_THREADS = 1024;
+static_assert(NA_MAX_TILES == NA_SCAN_THREADS * 8, "scan covers the scratch");
+__global__ __launch_bounds__(NA_SCAN_THREADS) void k_na_scan(u32 *tile_inliers, u32 tiles) {
+  __shared__ u32 warp_sums[NA_SCAN_THREADS / 32];
+  const u32 tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  u32 v[8];
+  u32 s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const u32 k = tid * 8 + j;
+    v[j] = k < tiles ? tile_inliers[k] : 0;
+    s += v[j];
+  }
+  u32 incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u32 u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (u32)o) incl += u;
+  }
+  if (lane == 31) warp_sums[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    u32 ws = warp_sums[lane];
+    u32 wi = ws;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 u = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= (u32)o) wi += u;
+    }
+    warp_sums[lane] = wi - ws;  // exclusive prefix of the warps
+  }
+  __syncthreads();
+  u32 run = warp_sums[w] + incl - s;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const u32 k = tid * 8 + j;
+    if (k < tiles) tile_inliers[k] = run;
+    run += v[j];
+  }
+}
+
+// pass 3: every point's rank among the inliers (or outliers) of the cloud,
+// in input order, and its AoS copy at that position
 __global__ __launch_bounds__(NA_THREADS) void k_na_scatter(
     const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-    size_t n, const float *__restrict__ model, float t, const u32 *tile_inliers,
+    size_t n, const float *__restrict__ model, float t, const u32 *tile_before,
     float *in_aos, float *out_aos, unsigned long long *counts) {
-  __shared__ u32 red[NA_THREADS / 32];
-  __shared__ u32 scan[NA_THREADS];
-  __shared__ u32 s_before;
+  constexpr int W = NA_THREADS / 32;
+  __shared__ u32 pre[NA_ITEMS * W + 1];  // inliers before (item j, warp w), j-major
   const float4 m = make_float4(model[0], model[1], model[2], model[3]);
-  const u32 tile = blockIdx.x;
-  u32 part = 0;
-  for (u32 k = threadIdx.x; k < tile; k += NA_THREADS) part += tile_inliers[k];
-  const u32 before = block_sum(part, red);
-  if (threadIdx.x == 0) s_before = before;
-  // thread t owns NA_ITEMS consecutive points, so a scan over threads keeps
-  // input order
+  const u32 tile = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const size_t base = (size_t)tile * NA_TILE;
-  const size_t first = base + (size_t)threadIdx.x * NA_ITEMS;
-  bool f[NA_ITEMS];
-  u32 c = 0;
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned bal[NA_ITEMS];
 #pragma unroll
   for (int j = 0; j < NA_ITEMS; ++j) {
-    const size_t i = first + j;
-    f[j] = i < n && plane_inlier(m, x[i], y[i], z[i], t);
-    c += f[j] ? 1u : 0u;
+    const size_t i = base + (size_t)j * NA_THREADS + threadIdx.x;
+    const bool f = i < n && plane_inlier(m, x[i], y[i], z[i], t);
+    bal[j] = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) pre[j * W + w] = __popc(bal[j]);
   }
-  scan[threadIdx.x] = c;
   __syncthreads();
-  for (int o = 1; o < NA_THREADS; o <<= 1) {
-    const u32 v = threadIdx.x >= (u32)o ? scan[threadIdx.x - o] : 0;
-    __syncthreads();
-    scan[threadIdx.x] += v;
-    __syncthreads();
+  if (w == 0) {  // exclusive scan of the NA_ITEMS * W warp counts (2 per lane)
+    const u32 a0 = pre[2 * lane], a1 = pre[2 * lane + 1];
+    u32 incl = a0 + a1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const u32 u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (u32)o) incl += u;
+    }
+    const u32 ex = incl - a0 - a1;
+    __syncwarp();
+    pre[2 * lane] = ex;
+    pre[2 * lane + 1] = ex + a0;
+    if (lane == 31) pre[NA_ITEMS * W] = incl;
   }
-  const u32 in_before_tile = s_before;
-  u32 rin = in_before_tile + scan[threadIdx.x] - c;           // inliers before my first point
-  u64 rout = (first - rin);                                   // outliers before my first point
+  __syncthreads();
+  const u32 before = tile_before[tile];
 #pragma unroll
   for (int j = 0; j < NA_ITEMS; ++j) {
-    const size_t i = first + j;
+    const size_t i = base + (size_t)j * NA_THREADS + threadIdx.x;
     if (i >= n) break;
-    if (f[j]) {
+    const u64 rin = (u64)before + pre[j * W + w] + __popc(bal[j] & lt);  // inliers before i
+    if ((bal[j] >> lane) & 1u) {
       if (in_aos) {
-        in_aos[3 * (size_t)rin + 0] = x[i];
-        in_aos[3 * (size_t)rin + 1] = y[i];
-        in_aos[3 * (size_t)rin + 2] = z[i];
+        in_aos[3 * rin + 0] = x[i];
+        in_aos[3 * rin + 1] = y[i];
+        in_aos[3 * rin + 2] = z[i];
       }
-      ++rin;
-    } else {
-      if (out_aos) {
-        out_aos[3 * rout + 0] = x[i];
-        out_aos[3 * rout + 1] = y[i];
-        out_aos[3 * rout + 2] = z[i];
-      }
-      ++rout;
+    } else if (out_aos) {
+      const u64 rout = (u64)i - rin;  // outliers before i
+      out_aos[3 * rout + 0] = x[i];
+      out_aos[3 * rout + 1] = y[i];
+      out_aos[3 * rout + 2] = z[i];
     }
   }
-  if (tile == gridDim.x - 1 && threadIdx.x == NA_THREADS - 1) {
-    const u64 total_in = (u64)in_before_tile + scan[NA_THREADS - 1];
+  if (tile == gridDim.x - 1 && threadIdx.x == 0) {
+    const u64 total_in = (u64)before + pre[NA_ITEMS * W];
     counts[0] = total_in;
     counts[1] = (u64)n - total_in;
   }
@@ -172,30 +220,38 @@ extern "C" rvp_status rvp_extract_plane_noalloc(rvp_context *ctx, const float *x
   if (n > (size_t)RVP_NOALLOC_MAX_POINTS) return RVP_ERR_INVALID_ARG;
   if (n > 0 && (!x || !y || !z)) return RVP_ERR_INVALID_ARG;
   if (ctx->device < 0 || ctx->device >= kMaxDevices) return RVP_ERR_INVALID_ARG;
-  if (cudaSetDevice(ctx->device) != cudaSuccess) {
+  // the caller's current device is put back before returning
+  int caller_device = -1;
+  if (cudaGetDevice(&caller_device) != cudaSuccess) {
     cudaGetLastError();
     return RVP_ERR_CUDA;
   }
+  const bool switch_device = caller_device != ctx->device;
+  if (switch_device && cudaSetDevice(ctx->device) != cudaSuccess) {
+    cudaGetLastError();
+    return RVP_ERR_CUDA;
+  }
+  rvp_status status = RVP_OK;
   u32 *scratch = nullptr;
+  cudaStream_t st = ctx->stream;
   if (scratch_address(ctx->device, &scratch) != cudaSuccess) {
     cudaGetLastError();
-    return RVP_ERR_CUDA;
-  }
-  cudaStream_t st = ctx->stream;
-  if (n == 0) {
+    status = RVP_ERR_CUDA;
+  } else if (n == 0) {
     if (cudaMemsetAsync(counts, 0, 2 * sizeof(uint64_t), st) != cudaSuccess) {
       cudaGetLastError();
-      return RVP_ERR_CUDA;
+      status = RVP_ERR_CUDA;
     }
-    return RVP_OK;
+  } else {
+    const unsigned tiles = (unsigned)((n + NA_TILE - 1) / NA_TILE);
+    k_na_count<<<tiles, NA_THREADS, 0, st>>>(x, y, z, n, model, dist_thresh, scratch);
+    k_na_scan<<<1, NA_SCAN_THREADS, 0, st>>>(scratch, tiles);
+    k_na_scatter<<<tiles, NA_THREADS, 0, st>>>(x, y, z, n, model, dist_thresh, scratch,
+                                               inliers_aos, outliers_aos,
+                                               reinterpret_cast<unsigned long long *>(counts));
+    ctx->launches += 3;
+    if (cudaGetLastError() != cudaSuccess) status = RVP_ERR_CUDA;
   }
-  const unsigned tiles = (unsigned)((n + NA_TILE - 1) / NA_TILE);
-  k_na_count<<<tiles, NA_THREADS, 0, st>>>(x, y, z, n, model, dist_thresh, scratch);
-  ctx->launches++;
-  k_na_scatter<<<tiles, NA_THREADS, 0, st>>>(x, y, z, n, model, dist_thresh, scratch,
-                                             inliers_aos, outliers_aos,
-                                             reinterpret_cast<unsigned long long *>(counts));
-  ctx->launches++;
-  if (cudaGetLastError() != cudaSuccess) return RVP_ERR_CUDA;
-  return RVP_OK;
+  if (switch_device) cudaSetDevice(caller_device);
+  return status;
 }

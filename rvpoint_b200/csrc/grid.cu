@@ -1,6 +1,6 @@
 // Cell grid ("SpatialHash") build and neighbour queries for sm_100a.
 //
-// Build (spatial_hashing.cpp:76-163): bbox reduction, the reference's cell
+// Build (spatial_hashing.cpp:21-108): bbox reduction, the reference's cell
 // function floor((x - min) / cell), one 64-bit key per point, stable radix
 // sort of (key, index), bucket heads, an open-addressing table of occupied
 // buckets {key, start | count << 32}, and the points re-laid out in bucket
@@ -110,7 +110,7 @@ __global__ void k_bbox(const float *__restrict__ x, const float *__restrict__ y,
   flush(f);
 }
 
-// setInputCloud's padding and grid dimensions (spatial_hashing.cpp:141-150),
+// setInputCloud's padding and grid dimensions (spatial_hashing.cpp:86-95),
 // then (dense mode) each frame's first key.
 // One block: a thread per frame computes its grid, then a block-wide
 // exclusive scan of the level-3 group counts gives each frame's key_base.
@@ -282,31 +282,33 @@ static u64 next_pow2(u64 v) {
 void Grid::reserve(size_t n, int nf) {
   if (n < 1) n = 1;
   if (nf < 1) nf = 1;
-  if (n > n_max || nf > n_frames_max) {
-    n_max = n > n_max ? n : n_max;
-    n_frames_max = nf > n_frames_max ? nf : n_frames_max;
-    b_keys.reserve(n_max * 8);
-    b_vals.reserve(n_max * 4);
-    b_pts.reserve(n_max * 16);
-    b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
-    b_begin.reserve(al((n_frames_max + 1) * 8));
-    b_sort.reserve(sort_temp_bytes(n_max) + al(4 * n_max * 4) + al(4 * (n_max + 1) * 8) +
-                   scan_temp_bytes(n_max));
-    b_lstart.reserve(al(4 * n_max * 4));
-    b_misc.reserve(256);
-    d_n = b_misc.as<u64>();
-    d_nbuckets = d_n + 1;
-    d_collision = reinterpret_cast<int *>(d_n + 5);
-    d_overflow = d_collision + 1;
-  }
+  // every buffer is asked for its size on every call (a no-op when it is
+  // large enough), so an allocation that failed part-way leaves nothing
+  // marked as reserved that is not
+  n_max = n > n_max ? n : n_max;
+  n_frames_max = nf > n_frames_max ? nf : n_frames_max;
+  b_keys.reserve(n_max * 8);
+  b_vals.reserve(n_max * 4);
+  b_pts.reserve(n_max * 16);
+  b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
+  b_begin.reserve(al((n_frames_max + 1) * 8));
+  b_sort.reserve(sort_temp_bytes(n_max) + al(4 * n_max * 4) + al(4 * (n_max + 1) * 8) +
+                 scan_temp_bytes(n_max));
+  b_lstart.reserve(al(4 * n_max * 4));
+  b_misc.reserve(256);
+  d_n = b_misc.as<u64>();
+  d_nbuckets = d_n + 1;
+  d_collision = reinterpret_cast<int *>(d_n + 5);
+  d_overflow = d_collision + 1;
   // buckets of levels 0-2 never exceed 3 n (in practice ~1.2 n); without a
   // measured count the table is sized for 2 n
   const size_t want = table_cap_req ? table_cap_req
                                     : (size_t)next_pow2((u64)(2 * n_max + n_max / 2 + 1024));
-  if (want != table_cap) {
-    table_cap = want;
+  if (want != table_cap || !b_table.ptr) {
+    table_cap = 0;
     b_table.release();
-    b_table.reserve(table_cap * 16);
+    b_table.reserve(want * 16);
+    table_cap = want;
   }
 }
 

@@ -113,7 +113,7 @@ __device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, flo
 }
 
 // The reference's window: query cell +- (ceil(r/cell) + 1), unclamped
-// (spatial_hashing.cpp:174-181).
+// (spatial_hashing.cpp:122-129).
 __device__ __forceinline__ Window ref_window(const GridFrame &F, float qx, float qy, float qz,
                                              float radius) {
   const int R = (int)ceilf(fdiv(radius, F.cell)) + 1;

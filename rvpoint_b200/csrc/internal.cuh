@@ -115,7 +115,7 @@ __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b)
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
 
-// d2 = dx*dx + dy*dy + dz*dz with dx = p - q (rvv_common.cpp:102-107)
+// d2 = dx*dx + dy*dy + dz*dz with dx = p - q (rvv_common.cpp:37-41)
 __device__ __forceinline__ float dist2(float px, float py, float pz, float qx,
                                        float qy, float qz) {
   const float dx = fsub(px, qx), dy = fsub(py, qy), dz = fsub(pz, qz);
@@ -123,7 +123,7 @@ __device__ __forceinline__ float dist2(float px, float py, float pz, float qx,
 }
 
 // (d2, idx) packed so that unsigned order == std::pair<float,int> order for
-// d2 >= 0 and idx >= 0 (spatial_hashing.cpp:204-209).
+// d2 >= 0 and idx >= 0 (spatial_hashing.cpp:149-154).
 __device__ __forceinline__ u64 pack_nbr(float d2, int idx) {
   return ((u64)__float_as_uint(d2) << 32) | (u64)(u32)idx;
 }
@@ -297,6 +297,7 @@ struct TileArgs {
   cudaEvent_t *level_events;  // null, or 2 per grid level: around each level's kNN kernel
   bool preset_open;         // qlevel already holds 0 (open) / 0xFF (done) per grid point
   int lane_levels;          // grid levels of the per-lane kernels (0: all)
+  int coop;                 // cooperative level-0 pass (k_knn_coop) before the per-lane kernels
 };
 // false if k has no tile instantiation (use grid_knn then)
 // Normals of the kept points whose SOR neighbour list (TILE_SOR_LIST, ks per

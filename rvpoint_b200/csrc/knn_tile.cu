@@ -13,7 +13,7 @@
 // slack); the others stay open for the next, 4x coarser level, and after the
 // last level go to a list that the warp-per-query kernel finishes. Epilogues are fused: SOR mean distance
 // (statistical_outlier_removal.cpp:36-40) or the reference normal
-// (normal_estimation.cpp:141-161) straight from the registers.
+// (normal_estimation.cpp:90-110) straight from the registers.
 #include <type_traits>
 
 #include "grid_device.cuh"
@@ -569,6 +569,183 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
   }
 }
 
+// Cooperative level-0 kNN: one warp per 32 consecutive grid points, every
+// lane testing the same candidate at the same time. The union of the lanes'
+// 27-cell rings is looked up once (per-warp table, as in k_knn_wt); each
+// lane takes a bound tb from its own cell's occupancy (radius rfac * cell *
+// sqrt(K / count), under one cell). The warp then walks only the cells some
+// lane can still use (box distance below that lane's min(tb, K-th key)): 32
+// candidates of such a cell go up coalesced into a per-warp staging row,
+// and every lane tests all of them against its query (broadcast shared
+// memory reads, all lanes converged), collecting the ones within tb in a
+// bit mask; the masked ones are then inserted into the lane's register list
+// (insertion network). Every point with d2 <= tb lies in the lane's tight
+// window of sqrt(tb), inside its ring, and every cell that can hold one is
+// walked, so a lane that found K such points is exact. The others (and
+// warps whose queries span more than the table) stay open at level 0 for
+// the per-lane kernel's ring pass.
+constexpr int CP_WARPS = TT / 32;
+
+template <int K, int MODE>
+__global__ __launch_bounds__(TT, 3) void k_knn_coop(GridView g, TileArgs a, uint8_t *qlevel,
+                                                    u32 *stats) {
+  static_assert(MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F,
+                "float-key modes only");
+  constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
+  __shared__ uint2 wtab[CP_WARPS][WT_CELLS];
+  __shared__ float4 stage[CP_WARPS][32];
+  const u64 n = *g.n_points;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const u64 nwarps = (u64)gridDim.x * CP_WARPS;
+  for (u64 base = ((u64)blockIdx.x * CP_WARPS + wib) * 32; base < n; base += nwarps * 32) {
+    const bool active = base + lane < n;
+    const u64 pos = base + lane;
+    const float4 q = active ? g.pts[pos] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const u32 qidx = __float_as_uint(q.w);
+    const int f = active ? (a.frame_of ? a.frame_of[qidx & 0x7FFFFFFFu] : 0) : -1;
+    const int f0 = __shfl_sync(0xffffffffu, f, 0);  // lane 0 is always active
+    const bool one_frame = __all_sync(0xffffffffu, !active || f == f0);
+    const GridFrame F = g.frames[active ? f : f0];
+    const int cx = cell_axis(q.x, F.min_x, F.cell), cy = cell_axis(q.y, F.min_y, F.cell),
+              cz = cell_axis(q.z, F.min_z, F.cell);
+    int bx0 = __reduce_min_sync(0xffffffffu, active ? cx : 0x7FFFFFFF) - 1;
+    int by0 = __reduce_min_sync(0xffffffffu, active ? cy : 0x7FFFFFFF) - 1;
+    int bz0 = __reduce_min_sync(0xffffffffu, active ? cz : 0x7FFFFFFF) - 1;
+    int bx1 = __reduce_max_sync(0xffffffffu, active ? cx : (int)0x80000000) + 1;
+    int by1 = __reduce_max_sync(0xffffffffu, active ? cy : (int)0x80000000) + 1;
+    int bz1 = __reduce_max_sync(0xffffffffu, active ? cz : (int)0x80000000) + 1;
+    bx0 = max(bx0, 0); by0 = max(by0, 0); bz0 = max(bz0, 0);
+    bx1 = min(bx1, F.gx - 1); by1 = min(by1, F.gy - 1); bz1 = min(bz1, F.gz - 1);
+    const int wx = bx1 - bx0 + 1, wy = by1 - by0 + 1, wz = bz1 - bz0 + 1;
+    const bool use_tab = one_frame && wx > 0 && wy > 0 && wz > 0 && wx * wy * wz <= WT_CELLS;
+    if (!use_tab) {  // the per-lane kernel takes the whole warp
+      if (active) qlevel[pos] = 0;
+      continue;
+    }
+    const int ncells = wx * wy * wz;
+    for (int t = lane; t < ncells; t += 32) {
+      const int ux = bx0 + t % wx, uy = by0 + (t / wx) % wy, uz = bz0 + t / (wx * wy);
+      u32 st = 0, ct = 0;
+      if (!lookup(g, level_key(g, F, 0, ux, uy, uz), st, ct)) ct = 0;
+      wtab[wib][t] = make_uint2(st, ct);
+    }
+    __syncwarp();
+    // the lane's bound and the distances from q to its own cell's faces
+    // (shrunk by the cell function's rounding slack)
+    float tb = -1.0f;
+    float glx = 0.0f, ghx = 0.0f, gly = 0.0f, ghy = 0.0f, glz = 0.0f, ghz = 0.0f;
+    const float cs = F.cell;
+    if (active) {
+      const u32 n_own = wtab[wib][((cz - bz0) * wy + (cy - by0)) * wx + (cx - bx0)].y;
+      const float r = fminf(a.rfac * F.cell * sqrtf((float)K / (float)max(n_own, 1u)),
+                            0.999f * F.cell);
+      const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)(r * r)), 0);
+      if (wt.lo[0] >= cx - 1 && wt.hi[0] <= cx + 1 && wt.lo[1] >= cy - 1 &&
+          wt.hi[1] <= cy + 1 && wt.lo[2] >= cz - 1 && wt.hi[2] <= cz + 1)
+        tb = r * r;
+      const float fx = F.min_x + (float)cx * cs, fy = F.min_y + (float)cy * cs,
+                  fz = F.min_z + (float)cz * cs;
+      const float slx = 4e-6f * (fabsf(F.min_x) + fabsf(q.x) + (float)(cx + 2) * cs) + 1e-6f;
+      const float sly = 4e-6f * (fabsf(F.min_y) + fabsf(q.y) + (float)(cy + 2) * cs) + 1e-6f;
+      const float slz = 4e-6f * (fabsf(F.min_z) + fabsf(q.z) + (float)(cz + 2) * cs) + 1e-6f;
+      glx = fmaxf(q.x - fx - slx, 0.0f);
+      ghx = fmaxf(fx + cs - q.x - slx, 0.0f);
+      gly = fmaxf(q.y - fy - sly, 0.0f);
+      ghy = fmaxf(fy + cs - q.y - sly, 0.0f);
+      glz = fmaxf(q.z - fz - slz, 0.0f);
+      ghz = fmaxf(fz + cs - q.z - slz, 0.0f);
+    }
+    float L[K];
+    u32 I[KV ? K : 1];
+#pragma unroll
+    for (int j = 0; j < K; ++j) L[j] = INFINITY;
+    float thr = INFINITY;
+    float tie = -1.0f;
+    u32 found = 0;
+    for (int t = 0; t < ncells; ++t) {
+      const uint2 e = wtab[wib][t];
+      if (e.y == 0) continue;
+      const int ux = bx0 + t % wx, uy = by0 + (t / wx) % wy, uz = bz0 + t / (wx * wy);
+      // lower bound on the distance from q to the cell (whole cells between
+      // q's cell and it add their edge)
+      const int dx = ux - cx, dy = uy - cy, dz = uz - cz;
+      const float gx = dx < 0 ? glx + (float)(-dx - 1) * cs : (dx > 0 ? ghx + (float)(dx - 1) * cs : 0.0f);
+      const float gy = dy < 0 ? gly + (float)(-dy - 1) * cs : (dy > 0 ? ghy + (float)(dy - 1) * cs : 0.0f);
+      const float gz = dz < 0 ? glz + (float)(-dz - 1) * cs : (dz > 0 ? ghz + (float)(dz - 1) * cs : 0.0f);
+      const bool need = tb >= 0.0f && (gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) <= fminf(thr, tb);
+      if (!__any_sync(0xffffffffu, need)) continue;
+      for (u32 j0 = 0; j0 < e.y; j0 += 32) {
+        const u32 m = min(32u, e.y - j0);
+        if ((u32)lane < m) stage[wib][lane] = __ldg(&g.pts[e.x + j0 + lane]);
+        __syncwarp();
+        unsigned acc = 0;
+        if (need) {
+          for (u32 s2 = 0; s2 < m; ++s2) {
+            const float4 p = stage[wib][s2];
+            const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+            acc |= (d2 <= tb ? 1u : 0u) << s2;
+          }
+        }
+        found += __popc(acc);
+        while (acc) {
+          const int s2 = __ffs(acc) - 1;
+          acc &= acc - 1;
+          const float4 p = stage[wib][s2];
+          const float key = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+          if (key < thr) {
+            if constexpr (KV) {
+              list_insert_kv<K>(L, I, key, __float_as_uint(p.w));
+              if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
+            } else {
+              list_insert<float, K>(L, key);
+            }
+            thr = L[K - 1];
+          } else if constexpr (KV) {
+            if (key == thr) tie = key;
+          }
+        }
+        __syncwarp();  // the staging row is refilled next
+      }
+    }
+    if (active) {
+      if (found < (u32)K) {
+        qlevel[pos] = 0;  // open: the per-lane kernel's ring pass
+      } else {
+        qlevel[pos] = 0xFF;
+        if (stats) atomicAdd(stats, 1u);
+        float sum = 0.0f;
+#pragma unroll
+        for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
+        if constexpr (MODE != TILE_PAIRS_F) a.mean[qidx] = fdiv(sum, (float)(K - 1));
+        if constexpr (KV) {
+          // equal distances leave the order (and at the boundary the set) to
+          // the scan order instead of the index: marked for the exact search
+          bool tied = tie == L[K - 1];
+#pragma unroll
+          for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
+          if constexpr (MODE == TILE_SOR_LIST) {
+            u32 *row = a.sor_list + (size_t)qidx * K;
+#pragma unroll
+            for (int j = 0; j < K; ++j) row[j] = tied ? 0xFFFFFFFFu : I[j];
+          } else {
+            if (tied) {
+              const u32 slot = atomicAdd(a.hard_count, 1u);
+              a.hard[slot] = qidx & 0x7FFFFFFFu;
+              if (a.hard_tau) a.hard_tau[slot] = L[K - 1];
+            } else {
+#pragma unroll
+              for (int j = 0; j < K; ++j)
+                a.pairs[(size_t)qidx * K + j] = pack_nbr(L[j], (int)I[j]);
+              if (a.counts) a.counts[qidx] = K;
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();  // the warp's table is reused by its next 32 queries
+  }
+}
+
 // open queries of `level`, in grid (cell) order: flags -> scan -> positions
 __global__ void k_open_flags(const uint8_t *qlevel, const u64 *n_dev, int level, u32 *flags) {
   const u64 n = *n_dev;
@@ -584,8 +761,28 @@ __global__ void k_open_scatter(const u32 *flags, const u64 *pos, const u64 *n_de
 }
 
 template <int K>
-void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, int blocks,
+void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_in, int blocks,
               uint8_t *qlevel, u32 *stats) {
+  TileArgs a = a_in;
+  // cooperative level-0 pass first (float-key modes over every grid point):
+  // it marks each point done or open, and the per-lane kernels take the open
+  // ones from their ring pass on (no second bounded pass at level 0)
+  const bool coop = a.coop && a.level0_warp && !a.preset_open &&
+                    (mode == TILE_SOR_MEAN || mode == TILE_SOR_LIST || mode == TILE_PAIRS_F);
+  if (coop) {
+    if (a.level_events) cudaEventRecord(a.level_events[0], ctx->stream);
+    const int cblocks = ctx->num_sms * 3;
+    u32 *st = stats;  // counted with the level-0 certifications
+    if (mode == TILE_SOR_MEAN)
+      k_knn_coop<K, TILE_SOR_MEAN><<<cblocks, TT, 0, ctx->stream>>>(g, a, qlevel, st);
+    else if (mode == TILE_SOR_LIST)
+      k_knn_coop<K, TILE_SOR_LIST><<<cblocks, TT, 0, ctx->stream>>>(g, a, qlevel, st);
+    else
+      k_knn_coop<K, TILE_PAIRS_F><<<cblocks, TT, 0, ctx->stream>>>(g, a, qlevel, st);
+    RVP_LAUNCH_CHECK(ctx);
+    a.preset_open = true;
+    a.rfac = 0.0f;
+  }
   if (!a.preset_open) RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
   if (a.level0_warp) {
     // barrier-free per-warp kernels at every level; levels > 0 (and level 0
@@ -607,7 +804,8 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a, 
         list = a.open_list;
       }
       u32 *st = stats ? stats + level : nullptr;
-      if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
+      if (a.level_events && !(coop && level == 0))
+        cudaEventRecord(a.level_events[2 * level], ctx->stream);
       if (mode == TILE_SOR_MEAN)
         k_knn_wt<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                     qlevel, a.qtau, st);

@@ -219,37 +219,122 @@ __device__ __forceinline__ void normalise(const float *__restrict__ feat, size_t
   for (int k = 0; k < MI; ++k) xn[k] = (feat[i * MI + k] - snorm[k]) * snorm[MI + k];
 }
 
-// logits, one thread per point
-__global__ __launch_bounds__(256) void k_mlp_forward(const float *__restrict__ feat, size_t n,
-                                                     const __nv_bfloat16 *__restrict__ wq,
-                                                     const float *__restrict__ norm,
-                                                     float *__restrict__ logits) {
-  __shared__ __align__(16) float sw[NP + 3];
+// ---------------------------------------------------------------------------
+// Tensor-core forward pass (mma.sync, FP32 accumulation): one warp per tile
+// of 16 points. Layer 1 (8 -> 64) is one m16n8k8 TF32 MMA per 8 hidden
+// units (inputs rounded to TF32, the BF16 weights exactly representable);
+// layer 2 (64 -> 64) four m16n8k16 BF16 MMAs per 8 units, its A fragments
+// being layer 1's accumulators (bias, ReLU, rounded to BF16) in place --
+// the C layout of two n8 tiles is the A layout of one k16 step; layer 3
+// (64 -> 1) is a dot product of the accumulators with w3, reduced over the
+// four lanes that share a row. Both weight matrices stay in registers as
+// MMA fragments for the warp's whole run.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ u32 to_tf32(float f) {
+  u32 r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
+  return r;
+}
+__device__ __forceinline__ u32 pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // lo in the low half
+  return *reinterpret_cast<const u32 *>(&v);
+}
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&c)[4], const u32 (&a)[4], u32 b0, u32 b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ void mma_bf16_16x8x16(float (&c)[4], const u32 (&a)[4], u32 b0,
+                                                 u32 b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+constexpr int FWD_THREADS = 128;
+
+__global__ __launch_bounds__(FWD_THREADS) void k_mlp_forward(const float *__restrict__ feat,
+                                                             size_t n,
+                                                             const __nv_bfloat16 *__restrict__ wq,
+                                                             const float *__restrict__ norm,
+                                                             float *__restrict__ logits) {
+  __shared__ float sv[3 * MH + 1];  // b1 | b2 | w3 | b3
   __shared__ float snorm[2 * MI];
-  load_weights(wq, norm, sw, snorm);
-  // one point per thread: a grid-stride loop would let the compiler hoist
-  // the weight loads out of it into (spilled) registers
-  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i < n) {
-    float xn[MI];
-    normalise(feat, i, snorm, xn);
-    float h1[MH];
+  // b1 sits before W2, b2 | w3 | b3 after it
+  for (int i = threadIdx.x; i < 3 * MH + 1; i += blockDim.x)
+    sv[i] = __bfloat162float(wq[i < MH ? OB1 + i : OB2 + (i - MH)]);
+  for (int i = threadIdx.x; i < 2 * MI; i += blockDim.x) snorm[i] = norm[i];
+  __syncthreads();
+  const float *b1 = sv, *b2 = sv + MH, *w3 = sv + 2 * MH;
+  const float b3 = sv[3 * MH];
+  const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+  // B fragments: W1 (TF32, k = input, n = hidden unit), W2 (BF16 pairs)
+  u32 w1f[8][2];
 #pragma unroll
-    for (int h = 0; h < MH; ++h) {
-      float s = sw[OB1 + h];
+  for (int nt = 0; nt < 8; ++nt) {
+    const int h = nt * 8 + g;
+    w1f[nt][0] = to_tf32(__bfloat162float(wq[OW1 + h * MI + tig]));
+    w1f[nt][1] = to_tf32(__bfloat162float(wq[OW1 + h * MI + tig + 4]));
+  }
+  u32 w2f[8][4][2];
+  const u32 *wq32 = reinterpret_cast<const u32 *>(wq);
 #pragma unroll
-      for (int k = 0; k < MI; ++k) s = fmaf(sw[OW1 + h * MI + k], xn[k], s);
-      h1[h] = fmaxf(s, 0.0f);
+  for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      const int e = OW2 + (nt * 8 + g) * MH + ks * 16 + 2 * tig;  // even: a BF16 pair
+      w2f[nt][ks][0] = __ldg(&wq32[e >> 1]);
+      w2f[nt][ks][1] = __ldg(&wq32[(e + 8) >> 1]);
     }
-    float out = sw[OB3];
-#pragma unroll 1
-    for (int j = 0; j < MH; ++j) {
-      float s = sw[OB2 + j];
+  const float m0 = snorm[tig], m1 = snorm[tig + 4];
+  const float s0 = snorm[MI + tig], s1 = snorm[MI + tig + 4];
+  const size_t tiles = (n + 15) / 16;
+  const size_t warps = (size_t)gridDim.x * (FWD_THREADS / 32);
+  for (size_t tile = (size_t)blockIdx.x * (FWD_THREADS / 32) + (threadIdx.x >> 5); tile < tiles;
+       tile += warps) {
+    const size_t r0 = tile * 16 + g, r1 = r0 + 8;
+    const bool v0 = r0 < n, v1 = r1 < n;
+    u32 a1[4];
+    a1[0] = to_tf32(v0 ? (feat[r0 * MI + tig] - m0) * s0 : 0.0f);
+    a1[1] = to_tf32(v1 ? (feat[r1 * MI + tig] - m0) * s0 : 0.0f);
+    a1[2] = to_tf32(v0 ? (feat[r0 * MI + tig + 4] - m1) * s1 : 0.0f);
+    a1[3] = to_tf32(v1 ? (feat[r1 * MI + tig + 4] - m1) * s1 : 0.0f);
+    u32 a2[4][4];
 #pragma unroll
-      for (int h = 0; h < MH; ++h) s = fmaf(sw[OW2 + j * MH + h], h1[h], s);
-      out = fmaf(sw[OW3 + j], fmaxf(s, 0.0f), out);
+    for (int ks = 0; ks < 4; ++ks) {
+      float c0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, c1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      mma_tf32_16x8x8(c0, a1, w1f[2 * ks][0], w1f[2 * ks][1]);
+      mma_tf32_16x8x8(c1, a1, w1f[2 * ks + 1][0], w1f[2 * ks + 1][1]);
+      const int j0 = 16 * ks + 2 * tig, j1 = j0 + 8;
+      a2[ks][0] = pack_bf16x2(fmaxf(c0[0] + b1[j0], 0.0f), fmaxf(c0[1] + b1[j0 + 1], 0.0f));
+      a2[ks][1] = pack_bf16x2(fmaxf(c0[2] + b1[j0], 0.0f), fmaxf(c0[3] + b1[j0 + 1], 0.0f));
+      a2[ks][2] = pack_bf16x2(fmaxf(c1[0] + b1[j1], 0.0f), fmaxf(c1[1] + b1[j1 + 1], 0.0f));
+      a2[ks][3] = pack_bf16x2(fmaxf(c1[2] + b1[j1], 0.0f), fmaxf(c1[3] + b1[j1 + 1], 0.0f));
     }
-    logits[i] = out;
+    float o0 = 0.0f, o1 = 0.0f;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) mma_bf16_16x8x16(c, a2[ks], w2f[nt][ks][0], w2f[nt][ks][1]);
+      const int j = nt * 8 + 2 * tig;
+      o0 = fmaf(w3[j], fmaxf(c[0] + b2[j], 0.0f), o0);
+      o0 = fmaf(w3[j + 1], fmaxf(c[1] + b2[j + 1], 0.0f), o0);
+      o1 = fmaf(w3[j], fmaxf(c[2] + b2[j], 0.0f), o1);
+      o1 = fmaf(w3[j + 1], fmaxf(c[3] + b2[j + 1], 0.0f), o1);
+    }
+    o0 += __shfl_xor_sync(0xffffffffu, o0, 1);
+    o0 += __shfl_xor_sync(0xffffffffu, o0, 2);
+    o1 += __shfl_xor_sync(0xffffffffu, o1, 1);
+    o1 += __shfl_xor_sync(0xffffffffu, o1, 2);
+    if (tig == 0) {
+      if (v0) logits[r0] = o0 + b3;
+      if (v1) logits[r1] = o1 + b3;
+    }
   }
 }
 
@@ -758,9 +843,10 @@ rvp_status rvp_mlp_forward(rvp_scorer *s, const float *features, size_t n, float
   return sguard(s->ctx, [&] {
     if (n == 0) return;
     RVP_REQUIRE(features && logits, "null pointer");
-    RVP_REQUIRE(n <= (size_t)0xFFFFFFFFull * 256, "too many points");
     RVP_CUDA_TRY(cudaSetDevice(s->ctx->device));
-    rvp::k_mlp_forward<<<(unsigned)((n + 255) / 256), 256, 0, s->ctx->stream>>>(
+    const unsigned blocks = rvp::grid_for((n + 15) / 16, rvp::FWD_THREADS / 32,
+                                          s->ctx->num_sms * 8);
+    rvp::k_mlp_forward<<<blocks, rvp::FWD_THREADS, 0, s->ctx->stream>>>(
         features, n, s->wq.as<__nv_bfloat16>(), s->norm.as<float>(), logits);
     RVP_LAUNCH_CHECK(s->ctx);
   });

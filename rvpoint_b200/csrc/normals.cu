@@ -1,11 +1,11 @@
 // PCA normals (features/normal_estimation.cpp).
 //
 // Reference path: per point, the neighbour list in (d2, index) order,
-// centroid (sum then "* (1.0f / n)" in compute_covariance_rvv :168-193, or
-// "/ (k+1)" in normal_estimation_sc :141-146), six covariance sums, then
-// simple_eigen3x3_smallest (:67-103: `iters` rotations on the largest
+// centroid (sum then "* (1.0f / n)" in compute_covariance_rvv :117-142, or
+// "/ (k+1)" in normal_estimation_sc :90-95), six covariance sums, then
+// simple_eigen3x3_smallest (:16-52: `iters` rotations on the largest
 // off-diagonal entry, updating only A[p][p], A[q][q], A[p][q] and V) and the
-// viewpoint flip (:106-118). Every step keeps the reference's operation order
+// viewpoint flip (:55-67). Every step keeps the reference's operation order
 // with separately rounded products and sums; atan2f/cosf/sinf are CUDA's,
 // which is why normals are compared within a tolerance.
 //
@@ -47,7 +47,7 @@ __global__ void k_normals_lists(const float *__restrict__ x, const float *__rest
     }
     const size_t qi = order ? (size_t)order[i] : i;
     const size_t oi = out_pos ? (size_t)out_pos[qi] : qi;
-    if (m < 3) {  // normal_estimation.cpp:254
+    if (m < 3) {  // normal_estimation.cpp:203
       nx[oi] = ny[oi] = nz[oi] = 0.0f;
       continue;
     }

@@ -1,7 +1,7 @@
 // Reference normal arithmetic shared by the normal kernels (normals.cu) and
 // the fused kNN + normal tile kernel (knn_tile.cu):
-// simple_eigen3x3_smallest (normal_estimation.cpp:67-103) and
-// flipNormalTowardsViewpoint (:106-118), every product and sum rounded on its
+// simple_eigen3x3_smallest (normal_estimation.cpp:16-52) and
+// flipNormalTowardsViewpoint (:55-67), every product and sum rounded on its
 // own in the reference's order.
 #pragma once
 
@@ -72,7 +72,7 @@ __device__ __forceinline__ void flip_ref(float px, float py, float pz, float vpx
 // Centroid, six covariance sums, eigen-solve and flip over the neighbour
 // list nb(0..m-1) (indices into x, y, z), in list order. div_centroid:
 // normal_estimation_sc's "/ (k+1)"; else compute_covariance_rvv's
-// "* (1.0f / n)" (normal_estimation.cpp:141-146 / :168-193).
+// "* (1.0f / n)" (normal_estimation.cpp:90-95 / :117-142).
 template <class Idx>
 __device__ __forceinline__ void normal_from_list(const float *__restrict__ x,
                                                  const float *__restrict__ y,

@@ -508,6 +508,10 @@ rvp_status rvp_octree_set_input_cloud(rvp_octree *o, const float *x, const float
     RVP_REQUIRE(n == 0 || (x && y && z), "null cloud pointer");
     RVP_REQUIRE(n < 0x7FFFFFFFull, "clouds are limited to 2^31 - 1 points");
     RVP_CUDA_TRY(cudaSetDevice(ctx->device));
+    // no cloud until this call has completed (see rvp_hash_set_input_cloud)
+    o->has_cloud = false;
+    o->built = false;
+    o->n = 0;
     o->x.reserve(n * 4 + 16);
     o->y.reserve(n * 4 + 16);
     o->z.reserve(n * 4 + 16);
@@ -535,8 +539,11 @@ rvp_status rvp_octree_build(rvp_octree *o) {
     RVP_REQUIRE(o->has_cloud, "setInputCloud before build");
     RVP_CUDA_TRY(cudaSetDevice(ctx->device));
     const size_t n = o->n;
-    o->built = true;
-    if (n == 0) return;  // octree.cpp:35: no root, every search returns 0
+    o->built = false;  // set again only when this build has completed
+    if (n == 0) {      // octree.cpp:35: no root, every search returns 0
+      o->built = true;
+      return;
+    }
     cudaStream_t st = ctx->stream;
     const int D = o->depth > 0 ? o->depth : 0;
     // (size_t)max_points_per_leaf_, as octree.cpp:60 compares it
@@ -575,6 +582,7 @@ rvp_status rvp_octree_build(rvp_octree *o) {
     k_oct_rank<<<gb, 256, 0, st>>>(vals, n, o->rank.as<u32>());
     RVP_LAUNCH_CHECK(ctx);
     oct_sync(ctx);
+    o->built = true;
   });
 }
 

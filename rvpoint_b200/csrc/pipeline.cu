@@ -144,6 +144,33 @@ __global__ void k_mark_removed(float4 *pts, const uint8_t *keep, const u64 *n_de
 }
 }  // namespace
 
+namespace {
+// frees everything a pipeline holds (also a partly created one) and the
+// pipeline itself
+void release_pipeline(rvp_pipeline *p) {
+  rvp::DevBuf *bufs[] = {&p->in_x, &p->in_y, &p->in_z, &p->in_offs, &p->vox_aos, &p->vox_x,
+                         &p->vox_y, &p->vox_z, &p->vox_offs, &p->vox_frame, &p->sor_list,
+                         &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
+                         &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
+                         &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau, &p->open};
+  for (auto *b : bufs) b->release();
+  p->vw.release();
+  p->grid.release();
+  for (auto e : p->events) cudaEventDestroy(e);
+  if (p->graph) cudaGraphExecDestroy(p->graph);
+  for (auto e : p->ev_stage)
+    if (e) cudaEventDestroy(e);
+  if (p->s_out) cudaStreamDestroy(p->s_out);
+  if (p->s_meta) cudaStreamDestroy(p->s_meta);
+  if (p->s_in) cudaStreamDestroy(p->s_in);
+  for (cudaEvent_t e : {p->ev_h2d[0], p->ev_h2d[1], p->ev_end, p->ev_dv, p->ev_ds, p->ev_dn})
+    if (e) cudaEventDestroy(e);
+  for (auto *b : {&p->in2_x, &p->in2_y, &p->in2_z, &p->in2_offs}) b->release();
+  delete p;
+}
+}  // namespace
+
 extern "C" {
 
 rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
@@ -207,7 +234,7 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     RVP_CUDA_TRY(cudaMemcpy(p->r_rand.ptr, rs.data(), R * 4, cudaMemcpyHostToDevice));
   });
   if (s != RVP_OK) {
-    delete p;
+    release_pipeline(p);
     return s;
   }
   *out = p;
@@ -218,26 +245,7 @@ rvp_status rvp_pipeline_destroy(rvp_pipeline *p) {
   if (!p) return RVP_ERR_INVALID_ARG;
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(p->ctx->stream);
-  rvp::DevBuf *bufs[] = {&p->in_x, &p->in_y, &p->in_z, &p->in_offs, &p->vox_aos, &p->vox_x,
-                         &p->vox_y, &p->vox_z, &p->vox_offs, &p->vox_frame, &p->sor_list,
-                         &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
-                         &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
-                         &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau, &p->open};
-  for (auto *b : bufs) b->release();
-  p->vw.release();
-  p->grid.release();
-  for (auto e : p->events) cudaEventDestroy(e);
-  if (p->graph) cudaGraphExecDestroy(p->graph);
-  for (auto e : p->ev_stage)
-    if (e) cudaEventDestroy(e);
-  if (p->s_out) cudaStreamDestroy(p->s_out);
-  if (p->s_meta) cudaStreamDestroy(p->s_meta);
-  if (p->s_in) cudaStreamDestroy(p->s_in);
-  for (cudaEvent_t e : {p->ev_h2d[0], p->ev_h2d[1], p->ev_end, p->ev_dv, p->ev_ds, p->ev_dn})
-    if (e) cudaEventDestroy(e);
-  for (auto *b : {&p->in2_x, &p->in2_y, &p->in2_z, &p->in2_offs}) b->release();
-  delete p;
+  release_pipeline(p);
   return RVP_OK;
 }
 
@@ -298,6 +306,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.rfac = p->rfac;
     ta.lane_levels = p->lane_levels;
     ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles instead
+    ta.coop = c.queries_per_warp == 3;         // 3: cooperative level-0 pass first
     {
       char *op = p->open.as<char>();
       auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -320,7 +329,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     // nearest indices, from which the normal stage takes the lists of the
     // points whose neighbours all survive
     const int kn = c.normal_k + 1;
-    const bool lists = c.queries_per_warp == 0 && kn <= ks;
+    const bool lists = (c.queries_per_warp == 0 || c.queries_per_warp == 3) && kn <= ks;
     ta.sor_list = lists ? p->sor_list.as<u32>() : nullptr;
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
     bool sor_lists = false;

@@ -72,6 +72,15 @@ class Batch:
         a, b = int(self.offsets[f]), int(self.offsets[f + 1])
         return Cloud(self.x[a:b], self.y[a:b], self.z[a:b])
 
+    @staticmethod
+    def from_frames(frames) -> "Batch":
+        """Concatenate clouds into one batch, in the given order."""
+        offs = np.zeros(len(frames) + 1, np.int64)
+        offs[1:] = np.cumsum([f.n for f in frames])
+        cat = lambda a: np.ascontiguousarray(np.concatenate(a), np.float32)  # noqa: E731
+        return Batch(cat([f.x for f in frames]), cat([f.y for f in frames]),
+                     cat([f.z for f in frames]), offs)
+
 
 def _f32(p: np.ndarray) -> Cloud:
     return Cloud.from_xyz(p.astype(np.float32))

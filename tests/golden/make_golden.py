@@ -31,7 +31,7 @@ def main():
     lid = lid.subset(np.sort(rng.choice(lid.n, 5000, replace=False)))
     out["room"] = room.aos()
     out["lidar"] = lid.aos()
-    # SpatialHash radiusSearch (spatial_hashing.cpp:165-223)
+    # SpatialHash radiusSearch (spatial_hashing.cpp:110-168)
     for name, c, cell, r, mnn in [("room_r03", room, 0.03, 0.03, 0),
                                   ("room_r05_c02", room, 0.02, 0.05, 0),
                                   ("lidar_r5", lid, 0.5, 0.5, 0),

@@ -1,0 +1,231 @@
+"""GPU parity at the configured workload sizes, through the C ABI, against the
+CPU oracle (the restatement, pinned bit for bit to the reference in
+test_oracle.py; its brute-force searches run one query per thread row, the
+arithmetic of each query unchanged):
+
+* 256-frame LiDAR batch (voxel 0.1 -> SOR k=16 -> normals k=16 -> RANSAC
+  1000 / 0.05): frames of the benchmark's own batch across its size range
+  (the largest included) plus one whole 64 x 2048-ray frame, run through
+  Pipeline at the benchmark's tuned setting and at every cell size the tuner
+  tries;
+* one whole 64 x 2048-ray LiDAR frame: radiusSearch r = 0.5 m (CSR) and the
+  radius-bounded kNN max_nn = 16, and the exact 16 nearest;
+* the 100,000-point room chain: voxel 0.01 -> sor_rvv k=30 -> hash normals
+  r = 0.03 -> RANSAC 1000 / 0.01;
+* the 2,000,000-point translated room: precision-mode normals (k = 32)
+  against the float64 oracle.
+
+Bit-exact: voxel centroids, SOR outputs, neighbour lists (index and d2
+bits), RANSAC count and model. Normals: as close to the float64 oracle as the
+reference's own FP32 arithmetic (CUDA's atan2f/cosf/sinf differ from glibc's
+by ulps).
+"""
+import numpy as np
+import pytest
+
+from rvpoint_b200 import datasets as D
+
+pytestmark = pytest.mark.gpu
+
+LEAF, SOR_K, NORMAL_K, R_THRESH, R_ITERS = 0.1, 16, 16, 0.05, 1000
+
+
+def bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.int32)
+
+
+def _angle_err(a, b):
+    a = a / np.maximum(np.linalg.norm(a, axis=1, keepdims=True), 1e-30)
+    b = b / np.maximum(np.linalg.norm(b, axis=1, keepdims=True), 1e-30)
+    return np.arccos(np.clip(np.abs((a * b).sum(1)), 0, 1))
+
+
+@pytest.fixture(scope="module")
+def bench_frames():
+    """Frames of the benchmark batch (256 frames, default seed) spread over
+    its size range, largest first, plus one whole 64 x 2048-ray frame."""
+    b = D.lidar_batch(n_frames=256)
+    sizes = np.diff(b.offsets)
+    order = np.argsort(sizes, kind="stable")
+    m = len(order)
+    pick = [order[-1], order[0], order[m // 2], order[m // 4], order[(3 * m) // 4], order[-2]]
+    frames = [b.frame(int(f)) for f in pick] + [D.lidar_frame()]
+    return D.Batch.from_frames(frames), [int(f) for f in pick]
+
+
+@pytest.fixture(scope="module")
+def bench_oracle(bench_frames, restatement):
+    """Per frame: voxel, SOR output, normals (FP32 and FP64 arithmetic of the
+    reference over the exact k+1 lists) and RANSAC (best, model)."""
+    from oracle.oracle import libc_rand_stream
+    batch, _ = bench_frames
+    rs = libc_rand_stream(3 * R_ITERS)
+    out = []
+    for f in range(batch.n_frames):
+        v, _ = restatement.voxel_grid(batch.frame(f), LEAF)
+        s, _, _ = restatement.sor_exact(D.Cloud.from_xyz(v), SOR_K, 1.0)
+        sc = D.Cloud.from_xyz(s)
+        n32 = restatement.normals_knn(sc, NORMAL_K)
+        n64 = restatement.normals_knn(sc, NORMAL_K, f64=True)
+        best, model, _, _, _ = restatement.ransac_plane(sc, R_THRESH, R_ITERS, rs)
+        out.append(dict(voxel=v, sor=s, n32=n32, n64=n64, best=best, model=model))
+    return out
+
+
+def _check_batch(r, oracle_frames):
+    for f, o in enumerate(oracle_frames):
+        a, b = r["voxel_offsets"][f], r["voxel_offsets"][f + 1]
+        assert np.array_equal(bits(r["voxel"][a:b]), bits(o["voxel"])), f
+        a, b = r["sor_offsets"][f], r["sor_offsets"][f + 1]
+        assert np.array_equal(bits(r["sor"][a:b]), bits(o["sor"])), f
+        g = r["normals"][a:b]
+        e_gpu = _angle_err(g, o["n64"])
+        e_cpu = _angle_err(o["n32"], o["n64"])
+        # FP32 tolerance against FP64: 1e-3 rad, as often as the reference's
+        # own FP32 path meets it
+        assert (e_gpu > 1e-3).mean() <= (e_cpu > 1e-3).mean() + 0.005, f
+        assert (_angle_err(g, o["n32"]) < 1e-4).mean() > 0.99, f
+        assert r["ransac_count"][f] == o["best"], f
+        assert np.array_equal(bits(r["ransac_model"][f]), bits(o["model"])), f
+
+
+def test_batch_frames_at_tuned_setting(gpu_ctx, bench_frames, bench_oracle):
+    """The benchmark's autotuned setting: cell 1.0 m, first-pass radius
+    factor 1.0, two per-lane grid levels."""
+    from rvpoint_b200 import api
+    batch, _ = bench_frames
+    p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, leaf_size=LEAF, sor_k=SOR_K,
+                     normal_k=NORMAL_K, ransac_thresh=R_THRESH, ransac_iters=R_ITERS)
+    p.set_tuning(1.0, 256, 0)
+    p.set_search_radius_factor(1.0)
+    p.set_lane_levels(2)
+    _check_batch(p.run_host(batch), bench_oracle)
+
+
+@pytest.mark.parametrize("qpw", [0, 3])
+@pytest.mark.parametrize("cell", [0.3, 0.5, 0.8, 1.0, 1.2])
+@pytest.mark.parametrize("rfac,lane_levels", [(0.7, 3), (1.0, 2)])
+def test_batch_frames_at_every_tuner_setting(gpu_ctx, bench_frames, bench_oracle, cell, rfac,
+                                             lane_levels, qpw):
+    """The cells the tuner tries (3, 5, 8, 10, 12 voxel leaves) with both
+    kNN kernel modes (per-lane, cooperative level 0), radius factors and
+    level counts: identical outputs."""
+    from rvpoint_b200 import api
+    batch, _ = bench_frames
+    p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, leaf_size=LEAF, sor_k=SOR_K,
+                     normal_k=NORMAL_K, ransac_thresh=R_THRESH, ransac_iters=R_ITERS)
+    p.set_tuning(cell, 0, qpw)
+    p.set_search_radius_factor(rfac)
+    p.set_lane_levels(lane_levels)
+    _check_batch(p.run_host(batch), bench_oracle)
+
+
+# ---------------------------------------------------------------------------
+# one whole LiDAR frame: radius search r = 0.5 and kNN 16
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def lidar_full():
+    return D.lidar_frame()
+
+
+def test_lidar_frame_radius_search_r05(gpu_ctx, restatement, lidar_full):
+    from rvpoint_b200.api import SpatialHash
+    c = lidar_full
+    assert c.n > 100_000  # rays that hit nothing within range return no point
+    h = SpatialHash()
+    h.setInputCloud(c, 0.5)
+    h.build()
+    assert not h.hasCollisions()
+    offs, idx, d2 = h.radiusSearchBatch(c.x, c.y, c.z, 0.5)
+    o2, i2, e2 = restatement.radius_search(c, 0.5, 0.5)
+    assert np.array_equal(offs, o2)
+    assert np.array_equal(idx, i2)
+    assert np.array_equal(bits(d2), bits(e2))
+    # the radius-bounded kNN (radiusSearch(q, 0.5, ..., max_nn = 16))
+    offs, idx, d2 = h.radiusSearchBatch(c.x, c.y, c.z, 0.5, max_nn=16)
+    o2, i2, e2 = restatement.radius_search(c, 0.5, 0.5, max_nn=16)
+    assert np.array_equal(offs, o2)
+    assert np.array_equal(idx, i2)
+    assert np.array_equal(bits(d2), bits(e2))
+
+
+def test_lidar_frame_knn16(gpu_ctx, restatement, lidar_full):
+    """The exact 16 nearest of every point (self included), ties by index."""
+    from rvpoint_b200.api import SpatialHash
+    c = lidar_full
+    h = SpatialHash()
+    h.setInputCloud(c, 0.5)
+    h.build()
+    idx, d2, cnt = h.knn(c.x, c.y, c.z, 16)
+    i2, e2 = restatement.knn_lists(c, 16)
+    assert np.all(cnt == 16)
+    assert np.array_equal(idx, i2)
+    assert np.array_equal(bits(d2), bits(e2))
+
+
+# ---------------------------------------------------------------------------
+# the 100k-point room chain
+# ---------------------------------------------------------------------------
+def test_room_chain_100k(gpu_ctx, restatement):
+    from oracle.oracle import libc_rand_stream
+    from rvpoint_b200 import api
+    c = D.room_cloud(n=100_000)
+    v = api.voxel_grid_downsamp_rvv_v2(c, 0.01)
+    v2, _ = restatement.voxel_grid(c, 0.01)
+    assert np.array_equal(bits(v), bits(v2))
+    vc = D.Cloud.from_xyz(v2)
+    s, md, keep = api.sor_rvv(vc, 30, 1.0, return_stats=True)
+    s2, md2, keep2 = restatement.sor_exact(vc, 30, 1.0)
+    assert np.array_equal(bits(md), bits(md2))
+    assert np.array_equal(keep.astype(bool), keep2)
+    assert np.array_equal(bits(s), bits(s2))
+    sc = D.Cloud.from_xyz(s2)
+    h = api.SpatialHash()
+    h.setInputCloud(sc, 0.03)
+    h.build()
+    g = np.stack(api.normal_estimation_rvv(sc, h, 10, 0.03), 1)
+    f32 = restatement.normals_radius(sc, 0.03, 0.03)
+    f64 = restatement.normals_radius(sc, 0.03, 0.03, f64=True)
+    zero = np.all(f32 == 0, axis=1)
+    assert np.array_equal(np.all(g == 0, axis=1), zero)
+    e_gpu = _angle_err(g[~zero], f64[~zero])
+    e_cpu = _angle_err(f32[~zero], f64[~zero])
+    assert (e_gpu > 1e-3).mean() <= (e_cpu > 1e-3).mean() + 0.002
+    assert (_angle_err(g[~zero], f32[~zero]) < 1e-4).mean() > 0.99
+    rs = libc_rand_stream(3000)
+    best, model, counts, it = api.ransac_plane_rvv(sc, 0.01, 1000, rand_stream=rs,
+                                                   return_counts=True)
+    b2, m2, c2, _, it2 = restatement.ransac_plane(sc, 0.01, 1000, rs)
+    assert best == b2 and it == it2
+    assert np.array_equal(bits(model), bits(m2))
+    assert np.array_equal(counts, c2)
+
+
+# ---------------------------------------------------------------------------
+# the 2M-point translated room: precision-mode normals
+# ---------------------------------------------------------------------------
+def _angle(a, b):
+    c = np.abs(np.sum(a * b, 1)) / (np.linalg.norm(a, axis=1) * np.linalg.norm(b, axis=1) + 1e-300)
+    return np.arccos(np.clip(c, -1.0, 1.0))
+
+
+def test_precision_room_2m(gpu_ctx, restatement):
+    """k = 32 on all 2,000,000 points, against the float64 oracle over the
+    same neighbour sets (the exact 33 nearest from a k-d tree)."""
+    from scipy.spatial import cKDTree
+    from rvpoint_b200 import api
+    c = D.precision_room()
+    assert c.n == 2_000_000
+    k = 32
+    n_prec, cond, used = api.normal_estimation_precise(c, k, ctx=gpu_ctx)
+    P = np.stack([c.x, c.y, c.z], 1).astype(np.float64)
+    _, nbr = cKDTree(P).query(P, k=k + 1, workers=-1)
+    ref, ref_cond = restatement.normals_exact_f64(c, nbr.astype(np.int32))
+    e = _angle(n_prec, ref)
+    ok = np.isfinite(ref_cond)
+    assert ok.mean() > 0.99
+    stats = {"max": float(e[ok].max()), "p99": float(np.percentile(e[ok], 99)),
+             "fp64_fraction": float(np.mean(used > 0))}
+    print("precision 2M", stats)
+    assert stats["p99"] < 1e-3
+    assert np.array_equal(used > 0, cond > 1e6)

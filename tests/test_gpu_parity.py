@@ -355,20 +355,22 @@ def test_pipeline_frames_match_per_frame_oracle(gpu_ctx, restatement):
 
 
 def test_pipeline_tile_and_warp_paths_agree(gpu_ctx):
-    """The shared-memory tile kNN (one thread per query) and the warp-per-query
-    kernel give identical SOR output and normals on a full-size frame batch."""
+    """The per-lane kNN kernels, the warp-per-query kernel and the cooperative
+    level-0 pass give identical SOR output and normals on a full-size frame
+    batch."""
     from rvpoint_b200 import api
     batch = D.lidar_batch(n_frames=3, seed=9)
     outs = []
-    for qpw in (0, 1):
+    for qpw in (0, 1, 3):
         p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, cell_size=0.3,
                          queries_per_warp=qpw)
         outs.append(p.run_host(batch))
-    a, b = outs
-    assert np.array_equal(a["sor_offsets"], b["sor_offsets"])
-    assert np.array_equal(bits(a["sor"]), bits(b["sor"]))
-    assert np.array_equal(bits(a["normals"]), bits(b["normals"]))
-    assert np.array_equal(a["ransac_count"], b["ransac_count"])
+    a = outs[0]
+    for b in outs[1:]:
+        assert np.array_equal(a["sor_offsets"], b["sor_offsets"])
+        assert np.array_equal(bits(a["sor"]), bits(b["sor"]))
+        assert np.array_equal(bits(a["normals"]), bits(b["normals"]))
+        assert np.array_equal(a["ransac_count"], b["ransac_count"])
 
 
 def test_pipeline_search_radius_factor_does_not_change_results(gpu_ctx):
