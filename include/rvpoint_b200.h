@@ -476,6 +476,12 @@ RVP_API rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const floa
                                        int n_frames, size_t n_points, float cell_size,
                                        const uint32_t *cand, const int64_t *cand_offsets_dev,
                                        size_t n_cand, int neighbours, float *features);
+/* kNN kernels of the features among the candidates (neighbours = 1):
+ * queries_per_warp 0 one query per lane (default), 3 a cooperative first
+ * pass over the grid's finest level with the bound rfac * cell *
+ * sqrt(17 / own-cell count) (rfac > 0), the per-lane kernels after it. The
+ * features do not depend on the choice. */
+RVP_API rvp_status rvp_scorer_set_knn(rvp_scorer *s, int queries_per_warp, float rfac);
 /* Parameters (host arrays): FP32 master weights, RVP_MLP_PARAMS floats;
  * the network computes with their BF16 rounding. set_params resets the
  * optimiser. set_norm: per-feature mean and standard deviation applied

@@ -82,22 +82,50 @@ def forward(params, mean, std, feat, tensor_core: bool = False):
     return h2 @ w3 + b3
 
 
-def loss_and_grad(params, mean, std, feat, labels):
-    """Mean BCE-with-logits and its gradient (NP floats, float64)."""
+def _b(a):
+    """float64 -> float32 -> BF16 -> float64."""
+    return bf16_round(np.asarray(a, np.float32)).astype(np.float64)
+
+
+def loss_and_grad(params, mean, std, feat, labels, tensor_core: bool = False):
+    """Mean BCE-with-logits and its gradient (NP floats, float64).
+
+    tensor_core: the roundings of the GPU's tensor-core training step -- the
+    forward pass's (see forward), delta2 rounded to BF16 before it meets W2,
+    and the operands of the weight-gradient products (delta2, h1, delta1 and
+    the normalised inputs) rounded to BF16; the bias and w3 sums use the
+    unrounded values. Every sum in float64."""
     W1, b1, W2, b2, w3, b3 = unpack(bf16_round(params))
-    xn = (np.asarray(feat, np.float64) - np.asarray(mean, np.float64)) / np.asarray(std, np.float64)
+    if tensor_core:
+        inv = (np.float32(1.0) / np.asarray(std, np.float32)).astype(np.float32)
+        x32 = ((np.asarray(feat, np.float32) - np.asarray(mean, np.float32)) * inv).astype(
+            np.float32)
+        xn = tf32_round(x32).astype(np.float64)
+    else:
+        xn = (np.asarray(feat, np.float64) - np.asarray(mean, np.float64)) / \
+            np.asarray(std, np.float64)
     y = np.asarray(labels, np.float64)
     n = xn.shape[0]
     z1 = xn @ W1.T + b1
     h1 = np.maximum(z1, 0.0)
+    if tensor_core:
+        h1 = _b(h1)
     z2 = h1 @ W2.T + b2
     h2 = np.maximum(z2, 0.0)
     out = h2 @ w3 + b3
     loss = np.mean(np.maximum(out, 0.0) - y * out + np.log1p(np.exp(-np.abs(out))))
     g = (1.0 / (1.0 + np.exp(-out)) - y) / n
     d2 = np.outer(g, w3) * (h2 > 0)
-    d1 = (d2 @ W2) * (h1 > 0)
+    d1 = ((_b(d2) if tensor_core else d2) @ W2) * (h1 > 0)
     grad = np.zeros(NP)
+    if tensor_core:
+        grad[OW1:OB1] = (_b(d1).T @ _b(x32)).ravel()
+        grad[OB1:OW2] = d1.sum(0)
+        grad[OW2:OB2] = (_b(d2).T @ h1).ravel()
+        grad[OB2:OW3] = d2.sum(0)
+        grad[OW3:OB3] = h2.T @ g
+        grad[OB3] = g.sum()
+        return loss, grad
     grad[OW1:OB1] = (d1.T @ xn).ravel()
     grad[OB1:OW2] = d1.sum(0)
     grad[OW2:OB2] = (d2.T @ h1).ravel()

@@ -123,6 +123,7 @@ SIGNATURES = {
                                   P, P]),
     "rvp_scorer_create": (I, [P, SZ, I, C.POINTER(P)]),
     "rvp_scorer_destroy": (I, [P]),
+    "rvp_scorer_set_knn": (I, [P, I, F]),
     "rvp_scorer_features": (I, [P, P, P, P, P, I, SZ, F, P, P, SZ, I, P]),
     "rvp_mlp_set_params": (I, [P, P]),
     "rvp_mlp_get_params": (I, [P, P]),

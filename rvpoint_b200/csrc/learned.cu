@@ -338,149 +338,287 @@ __global__ __launch_bounds__(FWD_THREADS) void k_mlp_forward(const float *__rest
   }
 }
 
-constexpr int TB = 128;  // points per training block
-// rows kept per point for the gradient reduction
-constexpr int RH1 = 0, RD2 = RH1 + MH, RD1 = RD2 + MH, RH2 = RD1 + MH, RX = RH2 + MH,
-              RG = RX + MI, ROW = RG + 1;  // 265 floats
-constexpr size_t TRAIN_SMEM = (size_t)(NP + 3 + 2 * MI + TB * ROW) * sizeof(float);
+// ---------------------------------------------------------------------------
+// Training step on tensor cores: forward and backward of the mean binary
+// cross-entropy with logits, 64 points per block iteration (4 warps x 16).
+// Phase A (each warp, its 16 points): the forward pass as in k_mlp_forward,
+// the output gradient g = (sigmoid(out) - y) / n, delta2 = g * w3 * [h2 > 0]
+// and delta1 = (delta2 W2) * [h1 > 0], the latter as m16n8k16 BF16 MMAs
+// with delta2's accumulators as A fragments and W2 transposed in shared
+// memory as B; delta2, h1, delta1 and the normalised inputs go to shared
+// memory transposed (BF16), the bias and w3 sums of the 16 points (FP32) too.
+// Phase B (warp w owns rows 16w..16w+15 of dW2 and dW1): dW2 = delta2^T H1
+// and dW1 = delta1^T X as MMAs over the iteration's 64 points, accumulated in
+// registers across iterations; the vector entries are added in warp order.
+// Every gradient entry of a block is written by one thread, and the blocks'
+// shares are added in block order afterwards (k_grad_reduce): the same batch
+// always gives the same gradient.
+// ---------------------------------------------------------------------------
+constexpr int TB = 128;                 // threads per training block
+constexpr int TP = 64;                  // points per block iteration
+constexpr int TS = 72;                  // row stride (BF16) of the shared tiles: no bank conflicts
+constexpr int NV = 3 * MH + 1;          // b1 | b2 | w3 | b3
+struct TrainSmem {
+  __nv_bfloat16 w2[MH * TS];   // W2[j][h]
+  __nv_bfloat16 w2t[MH * TS];  // W2[j][h] at [h][j]
+  __nv_bfloat16 d2t[MH * TS];  // delta2[m][j] at [j][m]
+  __nv_bfloat16 h1t[MH * TS];  // h1[m][h] at [h][m]
+  __nv_bfloat16 d1t[MH * TS];  // delta1[m][h] at [h][m]
+  __nv_bfloat16 xt[MI * TS];   // x[m][k] at [k][m]
+  float vec[NV + 3];
+  float norm[2 * MI];
+  float vpart[TB / 32][NV + 3];  // per warp: sums of the vector gradients over its points
+  double warp_loss[TB / 32];
+};
+constexpr size_t TRAIN_SMEM = sizeof(TrainSmem);
 
-// Forward + backward of mean binary cross-entropy with logits over n points
-// (labels 0/1), gradients added to grad, the loss sum to loss_sum.
-// With sample_seed != 0 the n rows are a minibatch drawn uniformly (with
-// replacement) from the n_src rows by a counter-based generator.
+__device__ __forceinline__ u32 lds32(const __nv_bfloat16 *p) {
+  return *reinterpret_cast<const u32 *>(p);
+}
+
 __global__ __launch_bounds__(TB) void k_mlp_train(const float *__restrict__ feat,
                                                   const float *__restrict__ labels, size_t n,
                                                   size_t n_src, u64 sample_seed,
                                                   const __nv_bfloat16 *__restrict__ wq,
                                                   const float *__restrict__ norm, float *part,
                                                   double *part_loss) {
-  // part: this block's gradient (NP floats at blockIdx.x * NP), part_loss
-  // its loss sum; every entry is written by one thread, and the blocks'
-  // shares are added in block order afterwards (k_grad_reduce): the same
-  // batch always gives the same gradient
-  __shared__ double warp_loss[TB / 32];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TrainSmem &S = *reinterpret_cast<TrainSmem *>(smraw);
   float *grad = part + (size_t)blockIdx.x * NP;
-  extern __shared__ __align__(16) float sm[];
-  float *sw = sm;
-  float *snorm = sw + NP + 3;
-  float *rows = snorm + 2 * MI;
-  load_weights(wq, norm, sw, snorm);
-  const int tid = threadIdx.x;
-  const float inv_n = 1.0f / (float)n;
-  // this thread's share of the gradient: 32 of W2, 4 of W1, and one or two
-  // of the 193 vector entries (b1, b2, w3, b3)
-  float gw2[32], gw1[4], gv[2] = {0.0f, 0.0f};
-#pragma unroll
-  for (int r = 0; r < 32; ++r) gw2[r] = 0.0f;
-#pragma unroll
-  for (int r = 0; r < 4; ++r) gw1[r] = 0.0f;
-  float loss = 0.0f;
-  for (size_t base = (size_t)blockIdx.x * TB; base < n; base += (size_t)gridDim.x * TB) {
-    const size_t slot = base + tid;
-    const size_t i = sample_seed ? (size_t)(mix64(sample_seed ^ mix64(slot)) % n_src) : slot;
-    float *row = rows + tid * ROW;
-    if (slot < n) {
-      float xn[MI];
-      normalise(feat, i, snorm, xn);
-      float h1[MH];
-#pragma unroll
-      for (int h = 0; h < MH; ++h) {
-        float s = sw[OB1 + h];
-#pragma unroll
-        for (int k = 0; k < MI; ++k) s = fmaf(sw[OW1 + h * MI + k], xn[k], s);
-        h1[h] = fmaxf(s, 0.0f);
-        row[RH1 + h] = h1[h];
-      }
-      float out = sw[OB3];
-#pragma unroll 4
-      for (int j = 0; j < MH; ++j) {
-        float s = sw[OB2 + j];
-#pragma unroll
-        for (int h = 0; h < MH; ++h) s = fmaf(sw[OW2 + j * MH + h], h1[h], s);
-        const float a = fmaxf(s, 0.0f);
-        row[RH2 + j] = a;
-        out = fmaf(sw[OW3 + j], a, out);
-      }
-      const float yl = labels[i];
-      // softplus(out) - y*out, stable
-      loss += fmaxf(out, 0.0f) - yl * out + log1pf(expf(-fabsf(out)));
-      const float g = (1.0f / (1.0f + expf(-out)) - yl) * inv_n;
-      row[RG] = g;
-#pragma unroll
-      for (int k = 0; k < MI; ++k) row[RX + k] = xn[k];
-      // delta2_j = g * w3_j * [h2_j > 0]; delta1_h = sum_j W2[j][h] delta2_j * [h1_h > 0]
-      float d1[MH];
-#pragma unroll
-      for (int h = 0; h < MH; ++h) d1[h] = 0.0f;
-#pragma unroll 4
-      for (int j = 0; j < MH; ++j) {
-        const float d2 = row[RH2 + j] > 0.0f ? g * sw[OW3 + j] : 0.0f;
-        row[RD2 + j] = d2;
-#pragma unroll
-        for (int h = 0; h < MH; ++h) d1[h] = fmaf(sw[OW2 + j * MH + h], d2, d1[h]);
-      }
-#pragma unroll
-      for (int h = 0; h < MH; ++h) row[RD1 + h] = h1[h] > 0.0f ? d1[h] : 0.0f;
-    } else {
-      for (int c = 0; c < ROW; ++c) row[c] = 0.0f;
-    }
-    __syncthreads();
-    {
-      // W2[j][h] += D2[b][j] * H1[b][h] for j = tid / 2, h = (tid % 2) * 32 + r
-      const int j = tid >> 1, h0 = (tid & 1) * 32;
-      for (int b = 0; b < TB; ++b) {
-        const float *rb = rows + b * ROW;
-        const float d2 = rb[RD2 + j];
-#pragma unroll
-        for (int r = 0; r < 32; ++r) gw2[r] = fmaf(d2, rb[RH1 + h0 + r], gw2[r]);
-      }
-      // W1[h][k] += D1[b][h] * X[b][k] for h = tid / 2, k = (tid % 2) * 4 + r
-      const int h = tid >> 1, k0 = (tid & 1) * 4;
-      for (int b = 0; b < TB; ++b) {
-        const float *rb = rows + b * ROW;
-        const float d1 = rb[RD1 + h];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) gw1[r] = fmaf(d1, rb[RX + k0 + r], gw1[r]);
-      }
-      // vector entries v = tid and tid + TB over [b1 | b2 | w3 | b3]
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int v = tid + e * TB;
-        if (v > 3 * MH) continue;
-        float s = 0.0f;
-        for (int b = 0; b < TB; ++b) {
-          const float *rb = rows + b * ROW;
-          s += v < MH ? rb[RD1 + v]
-                      : (v < 2 * MH ? rb[RD2 + v - MH]
-                                    : (v < 3 * MH ? rb[RG] * rb[RH2 + v - 2 * MH] : rb[RG]));
-        }
-        gv[e] += s;
-      }
-    }
-    __syncthreads();
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, tig = lane & 3;
+  for (int i = tid; i < MH * MH; i += TB) {
+    const int j = i / MH, h = i % MH;
+    const __nv_bfloat16 v = wq[OW2 + i];
+    S.w2[j * TS + h] = v;
+    S.w2t[h * TS + j] = v;
   }
-  {
-    const int j = tid >> 1, h0 = (tid & 1) * 32;
+  for (int i = tid; i < NV; i += TB) S.vec[i] = __bfloat162float(wq[i < MH ? OB1 + i : OB2 + (i - MH)]);
+  for (int i = tid; i < 2 * MI; i += TB) S.norm[i] = norm[i];
+  __syncthreads();
+  const float *b1 = S.vec, *b2 = S.vec + MH, *w3 = S.vec + 2 * MH;
+  const float b3 = S.vec[3 * MH];
+  u32 w1f[8][2];
 #pragma unroll
-    for (int r = 0; r < 32; ++r) grad[OW2 + j * MH + h0 + r] = gw2[r];
-    const int h = tid >> 1, k0 = (tid & 1) * 4;
+  for (int nt = 0; nt < 8; ++nt) {
+    const int h = nt * 8 + g;
+    w1f[nt][0] = to_tf32(__bfloat162float(wq[OW1 + h * MI + tig]));
+    w1f[nt][1] = to_tf32(__bfloat162float(wq[OW1 + h * MI + tig + 4]));
+  }
+  const float m0 = S.norm[tig], m1 = S.norm[tig + 4];
+  const float s0 = S.norm[MI + tig], s1 = S.norm[MI + tig + 4];
+  const float inv_n = 1.0f / (float)n;
+  float gw2[8][4], gw1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, gv[2] = {0.0f, 0.0f};
 #pragma unroll
-    for (int r = 0; r < 4; ++r) grad[OW1 + h * MI + k0 + r] = gw1[r];
+  for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) gw2[nt][r] = 0.0f;
+  float loss = 0.0f;
+  const int mr0 = 16 * w + g, mr1 = mr0 + 8;  // this thread's rows within the iteration
+  for (size_t base = (size_t)blockIdx.x * TP; base < n; base += (size_t)gridDim.x * TP) {
+    // ---- phase A: forward and backward of this warp's 16 points
+    const size_t slot0 = base + mr0, slot1 = base + mr1;
+    const bool v0 = slot0 < n, v1 = slot1 < n;
+    const size_t i0 = sample_seed ? (size_t)(mix64(sample_seed ^ mix64(slot0)) % n_src) : slot0;
+    const size_t i1 = sample_seed ? (size_t)(mix64(sample_seed ^ mix64(slot1)) % n_src) : slot1;
+    const float x00 = v0 ? (feat[i0 * MI + tig] - m0) * s0 : 0.0f;
+    const float x10 = v1 ? (feat[i1 * MI + tig] - m0) * s0 : 0.0f;
+    const float x01 = v0 ? (feat[i0 * MI + tig + 4] - m1) * s1 : 0.0f;
+    const float x11 = v1 ? (feat[i1 * MI + tig + 4] - m1) * s1 : 0.0f;
+    S.xt[tig * TS + mr0] = __float2bfloat16_rn(x00);
+    S.xt[tig * TS + mr1] = __float2bfloat16_rn(x10);
+    S.xt[(tig + 4) * TS + mr0] = __float2bfloat16_rn(x01);
+    S.xt[(tig + 4) * TS + mr1] = __float2bfloat16_rn(x11);
+    const u32 a1[4] = {to_tf32(x00), to_tf32(x10), to_tf32(x01), to_tf32(x11)};
+    u32 a2[4][4];  // h1 as layer-2 A fragments (BF16)
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      float c0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, c1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      mma_tf32_16x8x8(c0, a1, w1f[2 * ks][0], w1f[2 * ks][1]);
+      mma_tf32_16x8x8(c1, a1, w1f[2 * ks + 1][0], w1f[2 * ks + 1][1]);
+      const int j0 = 16 * ks + 2 * tig, j1 = j0 + 8;
+      a2[ks][0] = pack_bf16x2(fmaxf(c0[0] + b1[j0], 0.0f), fmaxf(c0[1] + b1[j0 + 1], 0.0f));
+      a2[ks][1] = pack_bf16x2(fmaxf(c0[2] + b1[j0], 0.0f), fmaxf(c0[3] + b1[j0 + 1], 0.0f));
+      a2[ks][2] = pack_bf16x2(fmaxf(c1[0] + b1[j1], 0.0f), fmaxf(c1[1] + b1[j1 + 1], 0.0f));
+      a2[ks][3] = pack_bf16x2(fmaxf(c1[2] + b1[j1], 0.0f), fmaxf(c1[3] + b1[j1 + 1], 0.0f));
+      // h1 transposed for dW2: (h, m) pairs of this thread
+      const __nv_bfloat162 *q = reinterpret_cast<const __nv_bfloat162 *>(a2[ks]);
+      S.h1t[j0 * TS + mr0] = q[0].x; S.h1t[(j0 + 1) * TS + mr0] = q[0].y;
+      S.h1t[j0 * TS + mr1] = q[1].x; S.h1t[(j0 + 1) * TS + mr1] = q[1].y;
+      S.h1t[j1 * TS + mr0] = q[2].x; S.h1t[(j1 + 1) * TS + mr0] = q[2].y;
+      S.h1t[j1 * TS + mr1] = q[3].x; S.h1t[(j1 + 1) * TS + mr1] = q[3].y;
+    }
+    float h2[8][4];
+    float o0 = 0.0f, o1 = 0.0f;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) h2[nt][r] = 0.0f;
+      const __nv_bfloat16 *wr = S.w2 + (nt * 8 + g) * TS + 2 * tig;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        mma_bf16_16x8x16(h2[nt], a2[ks], lds32(wr + 16 * ks), lds32(wr + 16 * ks + 8));
+      const int j = nt * 8 + 2 * tig;
+      h2[nt][0] = fmaxf(h2[nt][0] + b2[j], 0.0f);
+      h2[nt][1] = fmaxf(h2[nt][1] + b2[j + 1], 0.0f);
+      h2[nt][2] = fmaxf(h2[nt][2] + b2[j], 0.0f);
+      h2[nt][3] = fmaxf(h2[nt][3] + b2[j + 1], 0.0f);
+      o0 = fmaf(w3[j], h2[nt][0], fmaf(w3[j + 1], h2[nt][1], o0));
+      o1 = fmaf(w3[j], h2[nt][2], fmaf(w3[j + 1], h2[nt][3], o1));
+    }
+    o0 += __shfl_xor_sync(0xffffffffu, o0, 1);
+    o0 += __shfl_xor_sync(0xffffffffu, o0, 2);
+    o1 += __shfl_xor_sync(0xffffffffu, o1, 1);
+    o1 += __shfl_xor_sync(0xffffffffu, o1, 2);
+    o0 += b3;
+    o1 += b3;
+    float g0 = 0.0f, g1 = 0.0f;
+    if (v0) {
+      const float yl = labels[i0];
+      if (tig == 0) loss += fmaxf(o0, 0.0f) - yl * o0 + log1pf(expf(-fabsf(o0)));
+      g0 = (1.0f / (1.0f + expf(-o0)) - yl) * inv_n;
+    }
+    if (v1) {
+      const float yl = labels[i1];
+      if (tig == 0) loss += fmaxf(o1, 0.0f) - yl * o1 + log1pf(expf(-fabsf(o1)));
+      g1 = (1.0f / (1.0f + expf(-o1)) - yl) * inv_n;
+    }
+    // delta2 (in h2's place), its sums and w3's gradient sums over the rows
+    float sb2[16], sw3[16];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      const int j = nt * 8 + 2 * tig;
+      const float d00 = h2[nt][0] > 0.0f ? g0 * w3[j] : 0.0f;
+      const float d01 = h2[nt][1] > 0.0f ? g0 * w3[j + 1] : 0.0f;
+      const float d10 = h2[nt][2] > 0.0f ? g1 * w3[j] : 0.0f;
+      const float d11 = h2[nt][3] > 0.0f ? g1 * w3[j + 1] : 0.0f;
+      sw3[2 * nt] = g0 * h2[nt][0] + g1 * h2[nt][2];
+      sw3[2 * nt + 1] = g0 * h2[nt][1] + g1 * h2[nt][3];
+      sb2[2 * nt] = d00 + d10;
+      sb2[2 * nt + 1] = d01 + d11;
+      h2[nt][0] = d00; h2[nt][1] = d01; h2[nt][2] = d10; h2[nt][3] = d11;
+    }
+    u32 ad[4][4];  // delta2 as A fragments (BF16), and transposed for dW2
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      ad[ks][0] = pack_bf16x2(h2[2 * ks][0], h2[2 * ks][1]);
+      ad[ks][1] = pack_bf16x2(h2[2 * ks][2], h2[2 * ks][3]);
+      ad[ks][2] = pack_bf16x2(h2[2 * ks + 1][0], h2[2 * ks + 1][1]);
+      ad[ks][3] = pack_bf16x2(h2[2 * ks + 1][2], h2[2 * ks + 1][3]);
+      const int j0 = 16 * ks + 2 * tig, j1 = j0 + 8;
+      const __nv_bfloat162 *q = reinterpret_cast<const __nv_bfloat162 *>(ad[ks]);
+      S.d2t[j0 * TS + mr0] = q[0].x; S.d2t[(j0 + 1) * TS + mr0] = q[0].y;
+      S.d2t[j0 * TS + mr1] = q[1].x; S.d2t[(j0 + 1) * TS + mr1] = q[1].y;
+      S.d2t[j1 * TS + mr0] = q[2].x; S.d2t[(j1 + 1) * TS + mr0] = q[2].y;
+      S.d2t[j1 * TS + mr1] = q[3].x; S.d2t[(j1 + 1) * TS + mr1] = q[3].y;
+    }
+    // delta1 = (delta2 W2) * [h1 > 0]; its sums
+    float sb1[16];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      const __nv_bfloat16 *wr = S.w2t + (nt * 8 + g) * TS + 2 * tig;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        mma_bf16_16x8x16(c, ad[ks], lds32(wr + 16 * ks), lds32(wr + 16 * ks + 8));
+      // h1 > 0 at (rows, cols nt*8 + 2 tig + {0, 1}): from the A fragments
+      const __nv_bfloat162 *q = reinterpret_cast<const __nv_bfloat162 *>(a2[nt >> 1]);
+      const int o = (nt & 1) * 2;
+      const float d00 = __bfloat162float(q[o].x) > 0.0f ? c[0] : 0.0f;
+      const float d01 = __bfloat162float(q[o].y) > 0.0f ? c[1] : 0.0f;
+      const float d10 = __bfloat162float(q[o + 1].x) > 0.0f ? c[2] : 0.0f;
+      const float d11 = __bfloat162float(q[o + 1].y) > 0.0f ? c[3] : 0.0f;
+      sb1[2 * nt] = d00 + d10;
+      sb1[2 * nt + 1] = d01 + d11;
+      const int h = nt * 8 + 2 * tig;
+      S.d1t[h * TS + mr0] = __float2bfloat16_rn(d00);
+      S.d1t[(h + 1) * TS + mr0] = __float2bfloat16_rn(d01);
+      S.d1t[h * TS + mr1] = __float2bfloat16_rn(d10);
+      S.d1t[(h + 1) * TS + mr1] = __float2bfloat16_rn(d11);
+    }
+    // the warp's vector sums: rows of the lanes with the same tig, then one
+    // lane per column writes
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        sb1[e] += __shfl_xor_sync(0xffffffffu, sb1[e], o);
+        sb2[e] += __shfl_xor_sync(0xffffffffu, sb2[e], o);
+        sw3[e] += __shfl_xor_sync(0xffffffffu, sw3[e], o);
+      }
+    }
+    float gs = g0 + g1;  // b3: the 16 rows' g
+#pragma unroll
+    for (int o = 4; o < 32; o <<= 1) gs += __shfl_xor_sync(0xffffffffu, gs, o);
+    if (g == 0) {
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const int c = nt * 8 + 2 * tig;
+        S.vpart[w][c] = sb1[2 * nt];
+        S.vpart[w][c + 1] = sb1[2 * nt + 1];
+        S.vpart[w][MH + c] = sb2[2 * nt];
+        S.vpart[w][MH + c + 1] = sb2[2 * nt + 1];
+        S.vpart[w][2 * MH + c] = sw3[2 * nt];
+        S.vpart[w][2 * MH + c + 1] = sw3[2 * nt + 1];
+      }
+      if (tig == 0) S.vpart[w][3 * MH] = gs;
+    }
+    __syncthreads();
+    // ---- phase B: this warp's rows of dW2 and dW1 over the 64 points
+#pragma unroll
+    for (int ks = 0; ks < TP / 16; ++ks) {
+      const __nv_bfloat16 *ar = S.d2t + (16 * w + g) * TS + 16 * ks + 2 * tig;
+      const u32 a[4] = {lds32(ar), lds32(ar + 8 * TS), lds32(ar + 8), lds32(ar + 8 * TS + 8)};
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        const __nv_bfloat16 *br = S.h1t + (nt * 8 + g) * TS + 16 * ks + 2 * tig;
+        mma_bf16_16x8x16(gw2[nt], a, lds32(br), lds32(br + 8));
+      }
+      const __nv_bfloat16 *dr = S.d1t + (16 * w + g) * TS + 16 * ks + 2 * tig;
+      const u32 ad1[4] = {lds32(dr), lds32(dr + 8 * TS), lds32(dr + 8), lds32(dr + 8 * TS + 8)};
+      const __nv_bfloat16 *xr = S.xt + g * TS + 16 * ks + 2 * tig;
+      mma_bf16_16x8x16(gw1, ad1, lds32(xr), lds32(xr + 8));
+    }
+    // vector entries tid and tid + TB, the warps' sums in warp order
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
       const int v = tid + e * TB;
-      if (v > 3 * MH) continue;
-      const int dst = v < MH ? OB1 + v : (v < 2 * MH ? OB2 + v - MH : (v < 3 * MH ? OW3 + v - 2 * MH : OB3));
-      grad[dst] = gv[e];
+      if (v < NV) {
+        float t = 0.0f;
+#pragma unroll
+        for (int q = 0; q < TB / 32; ++q) t += S.vpart[q][v];
+        gv[e] += t;
+      }
     }
+    __syncthreads();  // the tiles are rewritten next iteration
+  }
+  // this block's share of the gradient: each entry written by one thread
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt) {
+    const int j = 16 * w + g, h = nt * 8 + 2 * tig;
+    grad[OW2 + j * MH + h] = gw2[nt][0];
+    grad[OW2 + j * MH + h + 1] = gw2[nt][1];
+    grad[OW2 + (j + 8) * MH + h] = gw2[nt][2];
+    grad[OW2 + (j + 8) * MH + h + 1] = gw2[nt][3];
+  }
+  {
+    const int h = 16 * w + g, k = 2 * tig;
+    grad[OW1 + h * MI + k] = gw1[0];
+    grad[OW1 + h * MI + k + 1] = gw1[1];
+    grad[OW1 + (h + 8) * MI + k] = gw1[2];
+    grad[OW1 + (h + 8) * MI + k + 1] = gw1[3];
+  }
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int v = tid + e * TB;
+    if (v < NV) grad[v < MH ? OB1 + v : OB2 + (v - MH)] = gv[e];
   }
   // loss: warp sums, then the warps in order
   for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
-  if ((tid & 31) == 0) warp_loss[tid >> 5] = (double)loss;
+  if (lane == 0) S.warp_loss[w] = (double)loss;
   __syncthreads();
   if (tid == 0) {
     double t = 0.0;
-    for (int w = 0; w < TB / 32; ++w) t += warp_loss[w];
+    for (int q = 0; q < TB / 32; ++q) t += S.warp_loss[q];
     part_loss[blockIdx.x] = t;
   }
 }
@@ -575,6 +713,8 @@ struct rvp_scorer {
   int adam_step = 0;
   size_t fitted_points = 0;  // batch size and cell the bucket table was fitted to
   float fitted_cell = 0.0f;
+  int knn_coop = 0;          // features among candidates: cooperative first pass
+  float knn_rfac = 1.0f;     // its bound factor
 };
 
 namespace {
@@ -680,7 +820,7 @@ namespace {
 rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const float *z,
                          const int64_t *frame_offsets_dev, int n_frames, size_t n_points,
                          float cell_size, const uint32_t *cand, size_t n_cand, float *features,
-                         int lane_levels = 0, float rfac = 1.0f) {
+                         int lane_levels = 0, float rfac = 1.0f, bool coop = false) {
   rvp_context *ctx = s->ctx;
   return sguard(ctx, [&] {
     RVP_REQUIRE(x && y && z && frame_offsets_dev && features, "null pointer");
@@ -720,8 +860,13 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
                                                                             is_cand);
       RVP_LAUNCH_CHECK(ctx);
     }
-    rvp::k_open_cand<<<gb, 256, 0, st>>>(gv.pts, gv.n_points, is_cand, s->qlevel.as<uint8_t>());
-    RVP_LAUNCH_CHECK(ctx);
+    // every grid point a query: the cooperative pass marks them itself
+    const bool coop_pass = coop && !cand;
+    if (!coop_pass) {
+      rvp::k_open_cand<<<gb, 256, 0, st>>>(gv.pts, gv.n_points, is_cand,
+                                           s->qlevel.as<uint8_t>());
+      RVP_LAUNCH_CHECK(ctx);
+    }
     u64 *hard_n64 = s->hard.as<u64>();
     u32 *hard_n = reinterpret_cast<u32 *>(hard_n64 + 1);
     u32 *hard = reinterpret_cast<u32 *>(hard_n64 + 2);
@@ -739,7 +884,8 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
     ta.qtau = s->qtau.as<float>();
     ta.rfac = rfac;
     ta.level0_warp = true;
-    ta.preset_open = true;
+    ta.preset_open = !coop_pass;
+    ta.coop = coop_pass ? 1 : 0;
     ta.lane_levels = lane_levels;
     char *op = s->open.as<char>();
     ta.open_flags = reinterpret_cast<u32 *>(op); op += al256(N * 4);
@@ -792,7 +938,16 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
   // the first pass bounded by the own cell's occupancy rarely certifies a
   // query there (it scans the ring at once)
   return features_impl(s, gx, gx + n_cand, gx + 2 * n_cand, cand_offsets_dev, n_frames, n_cand,
-                       cell_size, nullptr, n_cand, features, 1, 0.0f);
+                       cell_size, nullptr, n_cand, features, 1,
+                       s->knn_coop ? s->knn_rfac : 0.0f, s->knn_coop != 0);
+}
+
+rvp_status rvp_scorer_set_knn(rvp_scorer *s, int queries_per_warp, float rfac) {
+  if (!s || (queries_per_warp != 0 && queries_per_warp != 3)) return RVP_ERR_INVALID_ARG;
+  if (queries_per_warp == 3 && !(rfac > 0.0f)) return RVP_ERR_INVALID_ARG;
+  s->knn_coop = queries_per_warp == 3;
+  s->knn_rfac = rfac;
+  return RVP_OK;
 }
 
 
@@ -857,7 +1012,7 @@ void mlp_grad(rvp_scorer *s, const float *features, const float *labels, size_t 
               size_t n_src = 0, u64 sample_seed = 0) {
   rvp_context *ctx = s->ctx;
   const unsigned blocks =
-      (unsigned)std::min<size_t>((n + rvp::TB - 1) / rvp::TB, (size_t)ctx->num_sms);
+      (unsigned)std::min<size_t>((n + rvp::TP - 1) / rvp::TP, (size_t)ctx->num_sms);
   s->gpart.reserve((size_t)blocks * rvp::NP * 4 + (size_t)blocks * 8 + 256);
   float *part = s->gpart.as<float>();
   double *part_loss = reinterpret_cast<double *>(

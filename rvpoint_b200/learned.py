@@ -114,6 +114,11 @@ class PlaneScorer:
                                          _p(feat)), self.ctx.h)
         return feat
 
+    def set_knn(self, queries_per_warp: int, rfac: float = 1.0) -> None:
+        """kNN kernels of the features among candidates: 0 one query per
+        lane, 3 a cooperative first pass (rvp_scorer_set_knn)."""
+        check(self.L.rvp_scorer_set_knn(self.h, int(queries_per_warp), float(rfac)), self.ctx.h)
+
     def set_params(self, params: np.ndarray) -> None:
         p = np.ascontiguousarray(params, np.float32)
         assert p.shape == (_lib.MLP_PARAMS,)

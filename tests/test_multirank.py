@@ -1,7 +1,8 @@
-"""Multi-rank host logic on CPU: two gloo ranks split a batch of LiDAR
-frames with partition_frames, each runs the voxel stage of its own frames
-(CPU oracle), and the gathered per-frame results equal one process's; the
-timing reduction returns the slowest rank's time."""
+"""Multi-rank host logic on CPU: gloo ranks (2 and 3) split a batch of LiDAR
+frames with partition_frames, each runs the whole chain (voxel -> SOR ->
+normals -> RANSAC, CPU oracle) on its own frames, and the gathered
+per-frame results equal one process's; the timing reduction returns the
+slowest rank's time."""
 import os
 import socket
 
@@ -33,6 +34,17 @@ def _free_port():
     return p
 
 
+def _chain(R, frame):
+    """voxel 0.1 -> SOR k=16 -> normals k=16 -> RANSAC 1000 / 0.05 (oracle)."""
+    from oracle.oracle import libc_rand_stream
+    v, _ = R.voxel_grid(frame, 0.1)
+    s, _, _ = R.sor_exact(D.Cloud.from_xyz(v), 16, 1.0)
+    sc = D.Cloud.from_xyz(s)
+    n = R.normals_knn(sc, 16)
+    best, model, _, _, _ = R.ransac_plane(sc, 0.05, 1000, libc_rand_stream(3000))
+    return v, s, n, best, model
+
+
 def _worker(rank, world, port, batch, q):
     import torch.distributed as dist
     from datetime import timedelta
@@ -48,8 +60,7 @@ def _worker(rank, world, port, batch, q):
         sub = rank_batch(batch, mine)
         res = {}
         for j, f in enumerate(mine):
-            v, _ = R.voxel_grid(sub.frame(j), 0.1)
-            res[f] = v
+            res[f] = _chain(R, sub.frame(j))
         gathered = [None] * world
         dist.all_gather_object(gathered, res)
         slowest = max_over_ranks(10.0 + rank)
@@ -62,21 +73,26 @@ def _worker(rank, world, port, batch, q):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_split_frames_like_one_process(restatement):
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_split_frames_like_one_process(restatement, world):
     import torch.multiprocessing as mp
-    batch = D.lidar_batch(n_frames=6, seed=31, min_pts=3000, max_pts=9000)
+    batch = D.lidar_batch(n_frames=7, seed=31, min_pts=3000, max_pts=9000)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, batch, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, batch, q)) for r in range(world)]
     for p in procs:
         p.start()
-    merged, slowest = q.get(timeout=120)
+    merged, slowest = q.get(timeout=180)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert sorted(merged) == list(range(6))
-    for f in range(6):
-        v, _ = restatement.voxel_grid(batch.frame(f), 0.1)
-        assert np.array_equal(merged[f].view(np.int32), v.view(np.int32))
-    assert slowest == 11.0
+    assert sorted(merged) == list(range(7))
+    for f in range(7):
+        want = _chain(restatement, batch.frame(f))
+        got = merged[f]
+        for a, b in zip(got[:3], want[:3]):
+            assert np.array_equal(np.asarray(a).view(np.int32), np.asarray(b).view(np.int32))
+        assert got[3] == want[3]
+        assert np.array_equal(got[4].view(np.int32), want[4].view(np.int32))
+    assert slowest == 10.0 + world - 1
