@@ -426,31 +426,37 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-# kernels timed live for the roofline: the stage or per-level kernel name,
-# the kernel that runs there, and the queries / points one launch processes
-KERNELS = {
-    "sor_knn_l0": ("k_knn_wt<17,SOR_LIST> grid level 0", "vox"),
-    "sor_knn_l1": ("k_knn_wt<17,SOR_LIST> grid level 1", None),
-    "sor_knn_l2": ("k_knn_wt<17,SOR_LIST> grid level 2", None),
-    "normals_knn_l0": ("k_knn_wt<17,NORMALS> grid level 0", None),
-    "normals_knn_l1": ("k_knn_wt<17,NORMALS> grid level 1", None),
-    "normals_knn_l2": ("k_knn_wt<17,NORMALS> grid level 2", None),
-    "ransac": ("k_ransac", "ransac"),
-}
+# kernels timed live for the roofline (CUDA events around each launch): the
+# SOR kNN kernel of each grid level and RANSAC
+LEVEL_STAGES = ("sor_knn_l0", "sor_knn_l1", "sor_knn_l2")
 
 
-def kernel_bytes(name: str, n_vox: int, n_sor: int, n_frames: int) -> float:
-    """Algorithmic bytes of one launch: every query of the batch passes the
-    level-0 kNN kernel (12 B query + 8 B per neighbour, k+1 = 17 neighbours);
-    RANSAC reads each kept point once and writes a count per hypothesis."""
-    kind = KERNELS[name][1]
-    if kind == "vox":
-        return (12.0 + 8.0 * (SOR_K + 1)) * n_vox
-    if kind == "sor":
-        return (12.0 + 8.0 * (NORMAL_K + 1)) * n_sor
-    if kind == "ransac":
+def kernel_name(stage: str, coop: bool) -> str:
+    if stage == "ransac":
+        return "k_ransac"
+    level = stage[-1]
+    return (f"k_knn_coop<17,SOR_LIST> grid level {level}" if coop
+            else f"k_knn_wt<17,SOR_LIST> grid level {level}")
+
+
+def kernel_units(stage: str, coop: bool, routed, n_vox: int):
+    """Queries one launch of a SOR kNN kernel processes: with the
+    cooperative pass, the queries routed to its level; else every query at
+    level 0 (the coarser per-lane levels see only the ones left open, a
+    count the line does not carry, so they are not candidates)."""
+    level = int(stage[-1])
+    if coop:
+        return routed[level]
+    return n_vox if level == 0 else None
+
+
+def kernel_bytes(stage: str, units: int, n_sor: int, n_frames: int) -> float:
+    """Algorithmic bytes of one launch: 12 B per query + 8 B per neighbour
+    (k+1 = 17 neighbours) for a kNN kernel; RANSAC reads each kept point once
+    and writes a count per hypothesis."""
+    if stage == "ransac":
         return 12.0 * n_sor + 4.0 * R_ITERS * n_frames
-    raise ValueError(name)
+    return (12.0 + 8.0 * (SOR_K + 1)) * units
 
 
 def _write_pcd_binary(path: str, x, y, z) -> None:
@@ -814,34 +820,43 @@ def main():
         dist.destroy_process_group()
         return
 
-    # ---- roofline of the longest kernel timed live (per-level kNN kernels
-    # and RANSAC; the level-1/2 kernels see only the queries left open)
-    timed = {k: stages[k] for k in KERNELS if KERNELS[k][1] and stages.get(k, 0.0) > 0.0}
-    dom = max(timed, key=timed.get)
+    # ---- roofline of the longest kernel timed live (per-level SOR kNN
+    # kernels and RANSAC)
+    coop = int(pipe.cfg.queries_per_warp) == 3
+    routed = pipe.knn_routed() if coop else None
+    cand = {}
+    for k in LEVEL_STAGES + ("ransac",):
+        if stages.get(k, 0.0) <= 0.0:
+            continue
+        u = None if k == "ransac" else kernel_units(k, coop, routed, n_vox)
+        if k == "ransac" or u:
+            cand[k] = u
+    dom = max(cand, key=lambda k: stages[k])
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peaks = json.load(open(peaks_path))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
-    alg = kernel_bytes(dom, n_vox, n_sor, nf)
-    achieved = alg / (timed[dom] / 1e3) / 1e9
+    alg = kernel_bytes(dom, cand[dom], n_sor, nf)
+    achieved = alg / (stages[dom] / 1e3) / 1e9
+    dom_name = kernel_name(dom, coop)
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
             tr = json.load(open(tf)).get(dom)
-            # captured on a smaller batch: scaled by queries (traffic grows
-            # in proportion to the queries processed)
-            if tr:
-                units = n_vox if KERNELS[dom][1] == "vox" else n_sor
-                traffic = tr["bytes"] * units / tr["units"]
+            # captured on a smaller case: scaled by the queries processed
+            # (traffic grows in proportion to them)
+            if tr and tr.get("kernel") == dom_name and cand[dom]:
+                traffic = tr["bytes"] * cand[dom] / tr["units"]
         except Exception:
             traffic = None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "kernel": KERNELS[dom][0],
-            "stage": dom, "peak_source": peak_src,
-            "algorithmic_bytes_per_launch": alg, "launch_ms": timed[dom]}
+            "frac": achieved / peak, "traffic": traffic, "kernel": dom_name,
+            "stage": dom, "peak_source": peak_src, "queries": cand[dom],
+            "algorithmic_bytes_per_launch": alg, "launch_ms": stages[dom],
+            "routed_queries_per_level": routed}
 
     cpu = singles = None
     if world == 1:

@@ -271,7 +271,8 @@ typedef struct {
   float ransac_collinear;
   float ransac_prob;
   float cell_size;       /* grid cell for the neighbour searches (0 = auto) */
-  int block_threads;     /* kNN kernel block size (0 = auto) */
+  int block_threads;     /* warp-per-query kNN kernel block size: 32..256, a multiple
+                            of 32 (0 = 256) */
   int queries_per_warp;  /* kNN kernel mode: 0 one query per lane at every grid level
                             (default), 1 one warp per query, 2 shared-memory tiles,
                             3 a cooperative level-0 pass (all lanes test the same
@@ -325,6 +326,9 @@ RVP_API rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p);
 /* RVP_ERR_CAPACITY if the last run's bucket table overflowed (results of
  * that run are then incomplete); synchronizes the stream. */
 RVP_API rvp_status rvp_pipeline_check(rvp_pipeline *p);
+/* Queries of the SOR kNN the last run's cooperative pass routed to each of
+ * the three grid levels (queries_per_warp 3; zeros otherwise). out[3]. */
+RVP_API rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out);
 /* Diagnostics: enable != 0 makes the kNN kernels count which search path
  * settled each query (out16[0..7] SOR, [8..15] normals: fine ring, fine
  * tight window, coarse ring, coarse tight window, whole frame, bounded).

@@ -99,6 +99,7 @@ SIGNATURES = {
     "rvp_pipeline_frame_offsets": (I, [P, P, P]),
     "rvp_pipeline_fit_tables": (I, [P]),
     "rvp_pipeline_check": (I, [P]),
+    "rvp_pipeline_knn_routed": (I, [P, P]),
     "rvp_pipeline_knn_stats": (I, [P, I, P]),
     "rvp_pipeline_stage_times": (I, [P, C.POINTER(F), I, C.POINTER(I)]),
     # batched RANSAC and the learned proposal

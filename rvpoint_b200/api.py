@@ -783,6 +783,13 @@ class Pipeline:
         return {"sor": dict(zip(self.PATHS, map(int, out[:8]))),
                 "normals": dict(zip(self.PATHS, map(int, out[8:16])))}
 
+    def knn_routed(self) -> list:
+        """SOR kNN queries the last run's cooperative pass routed to grid
+        levels 0, 1, 2 (zeros without it)."""
+        out = np.zeros(3, np.uint64)
+        check(self.L.rvp_pipeline_knn_routed(self.h, _ptr(out)), self.ctx.h)
+        return [int(v) for v in out]
+
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)
 

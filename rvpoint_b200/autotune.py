@@ -38,7 +38,7 @@ def _time_run(pipe, args, reps: int) -> float:
 
 def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
          cells: Optional[Iterable[float]] = None,
-         blocks: Iterable[int] = (128, 256, 512),
+         blocks: Iterable[int] = (64, 128, 256),
          qpws: Iterable[int] = (0, 3), rfacs: Iterable[float] = (0.7, 0.85, 1.0),
          lane_levels: Iterable[int] = (3, 2),
          reps: int = 2,

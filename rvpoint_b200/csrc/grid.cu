@@ -201,13 +201,14 @@ __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__
                           const float *__restrict__ z, const u32 *vals, const u32 *heads,
                           const u64 *bucket_of, size_t n_max, const u64 *n_dev, int levels,
                           float4 *pts, u32 *lstart, const GridFrame *frames, int mode,
-                          int *collision) {
+                          int *collision, u32 *pos_of) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const u32 v = vals[i];
     const float px = x[v], py = y[v], pz = z[v];
     pts[i] = make_float4(px, py, pz, __uint_as_float(v));
+    pos_of[v] = (u32)i;
     for (int L = 0; L < levels; ++L)
       if (heads[(size_t)L * n_max + i])
         lstart[(size_t)L * n_max + bucket_of[(size_t)L * (n_max + 1) + i]] = (u32)i;
@@ -295,6 +296,7 @@ void Grid::reserve(size_t n, int nf) {
   b_sort.reserve(sort_temp_bytes(n_max) + al(4 * n_max * 4) + al(4 * (n_max + 1) * 8) +
                  scan_temp_bytes(n_max));
   b_lstart.reserve(al(4 * n_max * 4));
+  b_pos.reserve(n_max * 4);
   b_misc.reserve(256);
   d_n = b_misc.as<u64>();
   d_nbuckets = d_n + 1;
@@ -320,7 +322,7 @@ void Grid::fit_table(size_t buckets) {
 void Grid::release() {
   b_keys.release(); b_vals.release(); b_pts.release(); b_table.release();
   b_frames.release(); b_begin.release(); b_sort.release(); b_misc.release();
-  b_lstart.release();
+  b_lstart.release(); b_pos.release();
   n_max = 0; n_frames_max = 0; table_cap = 0;
 }
 
@@ -337,6 +339,7 @@ GridView Grid::view(int mode, long long p1, long long p2) const {
   for (int L = 0; L < 4; ++L) v.lstart[L] = b_lstart.as<u32>() + (size_t)L * n_max;
   v.n_level = d_nbuckets;
   v.n_points = d_n;
+  v.pos_of = b_pos.as<u32>();
   return v;
 }
 
@@ -390,7 +393,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   RVP_CUDA_TRY(cudaMemsetAsync(g.b_table.ptr, 0xFF, g.table_cap * 16, st));
   RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 40, st));  // buckets[4], collision, overflow
   k_reorder<<<gb, 256, 0, st>>>(x, y, z, g.b_vals.as<u32>(), heads, bucket_of, nm, n_live, levels,
-                                g.b_pts.as<float4>(), lstart, frames, mode, g.d_collision);
+                                g.b_pts.as<float4>(), lstart, frames, mode, g.d_collision,
+                                g.b_pos.as<u32>());
   RVP_LAUNCH_CHECK(ctx);
   k_insert<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), lstart, bucket_of, nm, n_live, levels,
                                table_levels, g.b_table.as<ulonglong2>(), (u64)g.table_cap - 1,
@@ -649,12 +653,13 @@ __global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int
         if (j <= valid_k) sum = fadd(sum, __fsqrt_rn(d));
       }
       if (lane == 0) mean[qi] = valid_k > 0 ? fdiv(sum, (float)valid_k) : 0.0f;
-      if (out_mode == KNN_OUT_SOR_MEAN_LIST) {
-        u32 *row = reinterpret_cast<u32 *>(out) + (size_t)qi * K;
+      if (out_mode == KNN_OUT_SOR_MEAN_LIST) {  // by grid position, of grid positions
+        u32 *row = reinterpret_cast<u32 *>(out) + (size_t)g.pos_of[qi] * K;
 #pragma unroll
         for (int s = 0; s < P; ++s) {
           const int j = s * 32 + lane;
-          if (j < K) row[j] = j < (int)cnt ? (u32)nbr_idx(L.e[s]) & 0x7FFFFFFFu : 0xFFFFFFFFu;
+          if (j < K)
+            row[j] = j < (int)cnt ? g.pos_of[(u32)nbr_idx(L.e[s]) & 0x7FFFFFFFu] : 0xFFFFFFFFu;
         }
       }
     } else {

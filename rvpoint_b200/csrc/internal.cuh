@@ -198,6 +198,7 @@ struct GridView {  // what the query kernels read
   const u32 *lstart[4];    // dense mode: first sorted position of each level-L bucket
   const u64 *n_level;      // dense mode: number of level-L buckets (device, [4])
   const u64 *n_points;     // number of grid points (device; set by grid_build)
+  const u32 *pos_of;       // sorted position of each point (by original index)
 };
 
 struct Grid {
@@ -205,7 +206,7 @@ struct Grid {
   size_t n_max = 0;
   size_t table_cap = 0;
   size_t table_cap_req = 0;    // 0: sized from n_max
-  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_lstart;
+  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_lstart, b_pos;
   u64 *d_n = nullptr;          // number of points (device)
   u64 *d_nbuckets = nullptr;   // buckets per level [4] (device)
   int *d_collision = nullptr;  // mode 0: hash collision detected
@@ -250,8 +251,9 @@ void sort_big_segments(rvp_context *ctx, const u64 *offsets, u64 *pairs,
 // stats (optional, 8 counters): queries certified by the fine ring, by a
 // fine tight window, by the coarse ring, by a coarse tight window, by a
 // whole-frame scan, and the radius-bounded ones.
-// KNN_OUT_SOR_MEAN_LIST: the mean, and out_pairs (as u32 rows of k by
-// original index) receives the k nearest indices, 0xFFFFFFFF past the found
+// KNN_OUT_SOR_MEAN_LIST: the mean, and out_pairs (as u32 rows of k, one row
+// per grid position) receives the grid positions of the k nearest,
+// 0xFFFFFFFF past the found
 enum KnnOut { KNN_OUT_BY_QUERY = 0, KNN_OUT_BY_SLOT = 1, KNN_OUT_SOR_MEAN = 2,
               KNN_OUT_SOR_MEAN_LIST = 3 };
 void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
@@ -263,8 +265,9 @@ void grid_knn(rvp_context *ctx, const GridView &g, const QuerySet &q, int k,
 // cells around it in shared memory, one thread per query scans its own
 // 27-cell ring; queries the ring cannot certify go to `hard` (original
 // indices) for grid_knn. Modes: SOR mean, fused reference normals, pairs.
-// TILE_SOR_LIST: the SOR mean plus the k nearest indices in (d2, index)
-// order, kept for the normal stage (sor_list)
+// TILE_SOR_LIST: the SOR mean plus the k nearest in (d2, index) order, kept
+// for the normal stage (sor_list: one row of k per grid position, holding
+// the neighbours' grid positions)
 // TILE_PAIRS_F: the TILE_PAIRS output from float distances with an index
 // beside each (per-warp kernels only); a list with equal distances, whose
 // order the scan would decide, goes to the hard list for the exact search
@@ -297,14 +300,15 @@ struct TileArgs {
   cudaEvent_t *level_events;  // null, or 2 per grid level: around each level's kNN kernel
   bool preset_open;         // qlevel already holds 0 (open) / 0xFF (done) per grid point
   int lane_levels;          // grid levels of the per-lane kernels (0: all)
-  int coop;                 // cooperative level-0 pass (k_knn_coop) before the per-lane kernels
+  int coop;                 // cooperative passes (k_knn_coop) before the per-lane kernels
+  u64 *routed;              // optional, [kGridLevels]: queries the cooperative pass routed to each level
 };
 // false if k has no tile instantiation (use grid_knn then)
 // Normals of the kept points whose SOR neighbour list (TILE_SOR_LIST, ks per
 // point) holds kn kept points; marks the rest open (qlevel 0) and the others
 // done (0xFF). False (nothing launched) if kn > ks or kn is not instantiated.
 bool normals_from_sor_lists(rvp_context *ctx, const GridView &g, const TileArgs &a, int ks,
-                            int kn, const uint8_t *keep);
+                            int kn);
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
                    int blocks, u32 *stats = nullptr);
 

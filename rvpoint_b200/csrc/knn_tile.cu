@@ -51,14 +51,15 @@ __device__ __forceinline__ void list_insert(T (&L)[K], T key) {
 // k nearest other points (statistical_outlier_removal.cpp:36-40, ascending
 // sum), and the k+1 indices for the normal stage
 template <int K>
-__device__ __forceinline__ void sor_list_out(const TileArgs &a, u32 qidx, const u64 (&L)[K]) {
+__device__ __forceinline__ void sor_list_out(const GridView &g, const TileArgs &a, u32 qidx,
+                                             u64 qpos, const u64 (&L)[K]) {
   float sum = 0.0f;
 #pragma unroll
   for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(nbr_d2(L[j])));
   a.mean[qidx] = fdiv(sum, (float)(K - 1));
-  u32 *row = a.sor_list + (size_t)qidx * K;
+  u32 *row = a.sor_list + (size_t)qpos * K;
 #pragma unroll
-  for (int j = 0; j < K; ++j) row[j] = (u32)nbr_idx(L[j]) & 0x7FFFFFFFu;
+  for (int j = 0; j < K; ++j) row[j] = g.pos_of[(u32)nbr_idx(L[j]) & 0x7FFFFFFFu];
 }
 
 // the same network over float keys carrying an index beside each: a key
@@ -298,7 +299,7 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
         for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
         a.mean[qidx] = fdiv(sum, (float)(K - 1));
       } else if constexpr (MODE == TILE_SOR_LIST) {
-        sor_list_out<K>(a, qidx, L);
+        sor_list_out<K>(g, a, qidx, qi, L);
       } else if constexpr (MODE == TILE_NORMALS) {
         float nx, ny, nz;
         normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
@@ -453,7 +454,8 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
             else key = pack_nbr(d2, (int)pidx);
             if (key < thr) {
               if constexpr (KV) {
-                list_insert_kv<K>(L, I, key, pidx);
+                // the SOR list keeps grid positions, the feature pairs indices
+                list_insert_kv<K>(L, I, key, MODE == TILE_SOR_LIST ? st + j : pidx);
                 if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
               } else {
                 list_insert<Key, K>(L, key);
@@ -534,7 +536,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
           bool tied = tie == L[K - 1];
 #pragma unroll
           for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
-          u32 *row = a.sor_list + (size_t)qidx * K;
+          u32 *row = a.sor_list + (size_t)pos * K;
 #pragma unroll
           for (int j = 0; j < K; ++j) row[j] = tied ? 0xFFFFFFFFu : I[j];
         } else if constexpr (MODE == TILE_NORMALS) {
@@ -569,45 +571,66 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
   }
 }
 
-// Cooperative level-0 kNN: one warp per 32 consecutive grid points, every
-// lane testing the same candidate at the same time. The union of the lanes'
-// 27-cell rings is looked up once (per-warp table, as in k_knn_wt); each
-// lane takes a bound tb from its own cell's occupancy (radius rfac * cell *
-// sqrt(K / count), under one cell). The warp then walks only the cells some
-// lane can still use (box distance below that lane's min(tb, K-th key)): 32
-// candidates of such a cell go up coalesced into a per-warp staging row,
-// and every lane tests all of them against its query (broadcast shared
-// memory reads, all lanes converged), collecting the ones within tb in a
-// bit mask; the masked ones are then inserted into the lane's register list
-// (insertion network). Every point with d2 <= tb lies in the lane's tight
-// window of sqrt(tb), inside its ring, and every cell that can hold one is
-// walked, so a lane that found K such points is exact. The others (and
-// warps whose queries span more than the table) stay open at level 0 for
-// the per-lane kernel's ring pass.
+// Cooperative kNN over routed queries. Every grid point is first routed to
+// the finest grid level whose own cell holds at least `min_own` points
+// (k_knn_route), so that a radius from that cell's occupancy is likely to
+// hold K points inside the cell's 27-cell ring. Per level, one warp takes 32
+// consecutive routed queries (a compacted list in grid order, so they lie
+// close together), looks up the union of their rings once (per-warp table,
+// as in k_knn_wt), and every lane takes the bound tb = r^2 with
+// r = rfac * cell * sqrt(K / own-cell count), under one cell. The warp walks
+// only the cells some lane can still use (box distance below that lane's
+// min(tb, K-th key)): 32 candidates of such a cell go up coalesced into a
+// per-warp staging row and every lane tests all of them against its query
+// (broadcast shared-memory reads, all lanes converged). A candidate within
+// tb (and not beyond the lane's K-th key) goes, as its grid position, into
+// the lane's buffer in shared memory; the buffers are merged into the lanes'
+// register lists (insertion network) when one of them fills and at the
+// end, so the warp pays for each lane's insertions once, not for the
+// busiest lane of every batch of 32. Every point with d2 <= tb lies in the
+// lane's tight window of sqrt(tb), inside its ring, and every cell that can
+// hold one is walked, so a lane that found K such points is exact. The
+// others (and warps whose queries span more than the table) stay open at
+// their level for the per-lane kernels' ring pass, or go to the
+// warp-per-query kernel when that level is past the per-lane levels.
 constexpr int CP_WARPS = TT / 32;
+constexpr int CP_BUF = 64;  // buffered candidates per lane
+constexpr size_t CP_SMEM = (size_t)CP_WARPS * (WT_CELLS * sizeof(uint2) + 32 * sizeof(float4) +
+                                               CP_BUF * 32 * sizeof(u32));
 
 template <int K, int MODE>
-__global__ __launch_bounds__(TT, 3) void k_knn_coop(GridView g, TileArgs a, uint8_t *qlevel,
-                                                    u32 *stats) {
+__global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int level,
+                                                    const u32 *list, const u64 *n_list,
+                                                    uint8_t *qlevel, float *qtau, u32 *stats) {
   static_assert(MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F,
                 "float-key modes only");
   constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
-  __shared__ uint2 wtab[CP_WARPS][WT_CELLS];
-  __shared__ float4 stage[CP_WARPS][32];
-  const u64 n = *g.n_points;
+  extern __shared__ __align__(16) unsigned char cp_smem[];
+  uint2 (*wtab)[WT_CELLS] = reinterpret_cast<uint2 (*)[WT_CELLS]>(cp_smem);
+  float4 (*stage)[32] =
+      reinterpret_cast<float4 (*)[32]>(cp_smem + CP_WARPS * WT_CELLS * sizeof(uint2));
+  u32 (*sbuf)[CP_BUF][32] = reinterpret_cast<u32 (*)[CP_BUF][32]>(
+      cp_smem + CP_WARPS * (WT_CELLS * sizeof(uint2) + 32 * sizeof(float4)));
+  const u64 n = *n_list;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const u64 nwarps = (u64)gridDim.x * CP_WARPS;
+  const int sh = 2 * level;
+  const int last = a.lane_levels > 0 && a.lane_levels < kGridLevels ? a.lane_levels - 1
+                                                                     : kGridLevels - 1;
   for (u64 base = ((u64)blockIdx.x * CP_WARPS + wib) * 32; base < n; base += nwarps * 32) {
     const bool active = base + lane < n;
-    const u64 pos = base + lane;
+    const u64 pos = active ? (u64)list[base + lane] : 0;
     const float4 q = active ? g.pts[pos] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const u32 qidx = __float_as_uint(q.w);
     const int f = active ? (a.frame_of ? a.frame_of[qidx & 0x7FFFFFFFu] : 0) : -1;
     const int f0 = __shfl_sync(0xffffffffu, f, 0);  // lane 0 is always active
     const bool one_frame = __all_sync(0xffffffffu, !active || f == f0);
     const GridFrame F = g.frames[active ? f : f0];
-    const int cx = cell_axis(q.x, F.min_x, F.cell), cy = cell_axis(q.y, F.min_y, F.cell),
-              cz = cell_axis(q.z, F.min_z, F.cell);
+    const int GX = level_dim(F.gx, level), GY = level_dim(F.gy, level),
+              GZ = level_dim(F.gz, level);
+    const int cx = cell_axis(q.x, F.min_x, F.cell) >> sh,
+              cy = cell_axis(q.y, F.min_y, F.cell) >> sh,
+              cz = cell_axis(q.z, F.min_z, F.cell) >> sh;
     int bx0 = __reduce_min_sync(0xffffffffu, active ? cx : 0x7FFFFFFF) - 1;
     int by0 = __reduce_min_sync(0xffffffffu, active ? cy : 0x7FFFFFFF) - 1;
     int bz0 = __reduce_min_sync(0xffffffffu, active ? cz : 0x7FFFFFFF) - 1;
@@ -615,31 +638,42 @@ __global__ __launch_bounds__(TT, 3) void k_knn_coop(GridView g, TileArgs a, uint
     int by1 = __reduce_max_sync(0xffffffffu, active ? cy : (int)0x80000000) + 1;
     int bz1 = __reduce_max_sync(0xffffffffu, active ? cz : (int)0x80000000) + 1;
     bx0 = max(bx0, 0); by0 = max(by0, 0); bz0 = max(bz0, 0);
-    bx1 = min(bx1, F.gx - 1); by1 = min(by1, F.gy - 1); bz1 = min(bz1, F.gz - 1);
+    bx1 = min(bx1, GX - 1); by1 = min(by1, GY - 1); bz1 = min(bz1, GZ - 1);
     const int wx = bx1 - bx0 + 1, wy = by1 - by0 + 1, wz = bz1 - bz0 + 1;
     const bool use_tab = one_frame && wx > 0 && wy > 0 && wz > 0 && wx * wy * wz <= WT_CELLS;
-    if (!use_tab) {  // the per-lane kernel takes the whole warp
-      if (active) qlevel[pos] = 0;
+    // a query this pass cannot finish: the per-lane kernels' ring at its
+    // level, or the warp-per-query kernel past the per-lane levels
+    auto leave_open = [&]() {
+      if (level <= last) {
+        qlevel[pos] = (uint8_t)level;
+        qtau[pos] = -1.0f;
+      } else {
+        const u32 slot = atomicAdd(a.hard_count, 1u);
+        a.hard[slot] = qidx & 0x7FFFFFFFu;
+        if (a.hard_tau) a.hard_tau[slot] = -1.0f;
+      }
+    };
+    if (!use_tab) {
+      if (active) leave_open();
       continue;
     }
     const int ncells = wx * wy * wz;
     for (int t = lane; t < ncells; t += 32) {
       const int ux = bx0 + t % wx, uy = by0 + (t / wx) % wy, uz = bz0 + t / (wx * wy);
       u32 st = 0, ct = 0;
-      if (!lookup(g, level_key(g, F, 0, ux, uy, uz), st, ct)) ct = 0;
+      if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, ct)) ct = 0;
       wtab[wib][t] = make_uint2(st, ct);
     }
     __syncwarp();
     // the lane's bound and the distances from q to its own cell's faces
     // (shrunk by the cell function's rounding slack)
+    const float cs = F.cell * (float)(1 << sh);
     float tb = -1.0f;
     float glx = 0.0f, ghx = 0.0f, gly = 0.0f, ghy = 0.0f, glz = 0.0f, ghz = 0.0f;
-    const float cs = F.cell;
     if (active) {
       const u32 n_own = wtab[wib][((cz - bz0) * wy + (cy - by0)) * wx + (cx - bx0)].y;
-      const float r = fminf(a.rfac * F.cell * sqrtf((float)K / (float)max(n_own, 1u)),
-                            0.999f * F.cell);
-      const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)(r * r)), 0);
+      const float r = fminf(a.rfac * cs * sqrtf((float)K / (float)max(n_own, 1u)), 0.999f * cs);
+      const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)(r * r)), level);
       if (wt.lo[0] >= cx - 1 && wt.hi[0] <= cx + 1 && wt.lo[1] >= cy - 1 &&
           wt.hi[1] <= cy + 1 && wt.lo[2] >= cz - 1 && wt.hi[2] <= cz + 1)
         tb = r * r;
@@ -662,6 +696,30 @@ __global__ __launch_bounds__(TT, 3) void k_knn_coop(GridView g, TileArgs a, uint
     float thr = INFINITY;
     float tie = -1.0f;
     u32 found = 0;
+    int cnt = 0;  // buffered candidates of this lane
+    // merge the buffered candidates into the register list, in buffer order
+    auto flush = [&]() {
+      for (int i = 0; __any_sync(0xffffffffu, i < cnt); ++i) {
+        if (i < cnt) {
+          const u32 j = sbuf[wib][i][lane];
+          const float4 p = __ldg(&g.pts[j]);
+          const float key = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+          if (key < thr) {
+            if constexpr (KV) {
+              // the SOR list keeps grid positions, the feature pairs indices
+              list_insert_kv<K>(L, I, key, MODE == TILE_SOR_LIST ? j : __float_as_uint(p.w));
+              if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
+            } else {
+              list_insert<float, K>(L, key);
+            }
+            thr = L[K - 1];
+          } else if constexpr (KV) {
+            if (key == thr) tie = key;
+          }
+        }
+      }
+      cnt = 0;
+    };
     for (int t = 0; t < ncells; ++t) {
       const uint2 e = wtab[wib][t];
       if (e.y == 0) continue;
@@ -678,38 +736,25 @@ __global__ __launch_bounds__(TT, 3) void k_knn_coop(GridView g, TileArgs a, uint
         const u32 m = min(32u, e.y - j0);
         if ((u32)lane < m) stage[wib][lane] = __ldg(&g.pts[e.x + j0 + lane]);
         __syncwarp();
-        unsigned acc = 0;
         if (need) {
           for (u32 s2 = 0; s2 < m; ++s2) {
             const float4 p = stage[wib][s2];
             const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
-            acc |= (d2 <= tb ? 1u : 0u) << s2;
-          }
-        }
-        found += __popc(acc);
-        while (acc) {
-          const int s2 = __ffs(acc) - 1;
-          acc &= acc - 1;
-          const float4 p = stage[wib][s2];
-          const float key = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
-          if (key < thr) {
-            if constexpr (KV) {
-              list_insert_kv<K>(L, I, key, __float_as_uint(p.w));
-              if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
-            } else {
-              list_insert<float, K>(L, key);
+            if (d2 <= tb) {
+              ++found;
+              // a key equal to the K-th still goes in: it marks a tie
+              if (d2 <= thr) sbuf[wib][cnt++][lane] = e.x + j0 + s2;
             }
-            thr = L[K - 1];
-          } else if constexpr (KV) {
-            if (key == thr) tie = key;
           }
         }
         __syncwarp();  // the staging row is refilled next
+        if (__any_sync(0xffffffffu, cnt > CP_BUF - 32)) flush();
       }
     }
+    flush();
     if (active) {
       if (found < (u32)K) {
-        qlevel[pos] = 0;  // open: the per-lane kernel's ring pass
+        leave_open();
       } else {
         qlevel[pos] = 0xFF;
         if (stats) atomicAdd(stats, 1u);
@@ -724,7 +769,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_coop(GridView g, TileArgs a, uint
 #pragma unroll
           for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
           if constexpr (MODE == TILE_SOR_LIST) {
-            u32 *row = a.sor_list + (size_t)qidx * K;
+            u32 *row = a.sor_list + (size_t)pos * K;
 #pragma unroll
             for (int j = 0; j < K; ++j) row[j] = tied ? 0xFFFFFFFFu : I[j];
           } else {
@@ -742,7 +787,32 @@ __global__ __launch_bounds__(TT, 3) void k_knn_coop(GridView g, TileArgs a, uint
         }
       }
     }
-    __syncwarp();  // the warp's table is reused by its next 32 queries
+    __syncwarp();  // the warp's table and buffers are reused by its next 32 queries
+  }
+}
+
+// the finest grid level whose own cell holds at least min_own points (the
+// top level otherwise), per grid point
+__global__ void k_knn_route(GridView g, const int32_t *frame_of, u32 min_own, uint8_t *qlevel) {
+  const u64 n = *g.n_points;
+  for (u64 pos = blockIdx.x * (u64)blockDim.x + threadIdx.x; pos < n;
+       pos += (u64)gridDim.x * blockDim.x) {
+    const float4 q = g.pts[pos];
+    const u32 qidx = __float_as_uint(q.w) & 0x7FFFFFFFu;
+    const GridFrame F = g.frames[frame_of ? frame_of[qidx] : 0];
+    const int cx = cell_axis(q.x, F.min_x, F.cell), cy = cell_axis(q.y, F.min_y, F.cell),
+              cz = cell_axis(q.z, F.min_z, F.cell);
+    int lv = kGridLevels - 1;
+    for (int l = 0; l < kGridLevels - 1; ++l) {
+      u32 st = 0, ct = 0;
+      const int s = 2 * l;
+      if (!lookup(g, level_key(g, F, l, cx >> s, cy >> s, cz >> s), st, ct)) ct = 0;
+      if (ct >= min_own) {
+        lv = l;
+        break;
+      }
+    }
+    qlevel[pos] = (uint8_t)lv;
   }
 }
 
@@ -753,35 +823,71 @@ __global__ void k_open_flags(const uint8_t *qlevel, const u64 *n_dev, int level,
     flags[i] = qlevel[i] == level ? 1u : 0u;
 }
 __global__ void k_open_scatter(const u32 *flags, const u64 *pos, const u64 *n_dev, u32 *list,
-                               u64 *n_list) {
+                               u64 *n_list, u64 *n_copy = nullptr) {
   const u64 n = *n_dev;
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
     if (flags[i]) list[pos[i]] = (u32)i;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *n_list = pos[n];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *n_list = pos[n];
+    if (n_copy) *n_copy = pos[n];
+  }
 }
 
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_in, int blocks,
               uint8_t *qlevel, u32 *stats) {
   TileArgs a = a_in;
-  // cooperative level-0 pass first (float-key modes over every grid point):
-  // it marks each point done or open, and the per-lane kernels take the open
-  // ones from their ring pass on (no second bounded pass at level 0)
+  // cooperative passes first (float-key modes over every grid point): each
+  // point is routed to a level and the warps of each level work on their
+  // queries together; the per-lane kernels then take what stays open, from
+  // their ring pass on (no second bounded pass at level 0)
   const bool coop = a.coop && a.level0_warp && !a.preset_open &&
                     (mode == TILE_SOR_MEAN || mode == TILE_SOR_LIST || mode == TILE_PAIRS_F);
   if (coop) {
-    if (a.level_events) cudaEventRecord(a.level_events[0], ctx->stream);
-    const int cblocks = ctx->num_sms * 3;
-    u32 *st = stats;  // counted with the level-0 certifications
-    if (mode == TILE_SOR_MEAN)
-      k_knn_coop<K, TILE_SOR_MEAN><<<cblocks, TT, 0, ctx->stream>>>(g, a, qlevel, st);
-    else if (mode == TILE_SOR_LIST)
-      k_knn_coop<K, TILE_SOR_LIST><<<cblocks, TT, 0, ctx->stream>>>(g, a, qlevel, st);
-    else
-      k_knn_coop<K, TILE_PAIRS_F><<<cblocks, TT, 0, ctx->stream>>>(g, a, qlevel, st);
+    static bool attr_set[64] = {false};
+    if (ctx->device < 64 && !attr_set[ctx->device]) {
+      RVP_CUDA_TRY(cudaFuncSetAttribute(k_knn_coop<K, TILE_SOR_MEAN>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)CP_SMEM));
+      RVP_CUDA_TRY(cudaFuncSetAttribute(k_knn_coop<K, TILE_SOR_LIST>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)CP_SMEM));
+      RVP_CUDA_TRY(cudaFuncSetAttribute(k_knn_coop<K, TILE_PAIRS_F>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)CP_SMEM));
+      attr_set[ctx->device] = true;
+    }
+    const unsigned gb = grid_for(a.n_max, 256, ctx->num_sms * 16);
+    const float rf = a.rfac > 0.0f ? a.rfac : 1.0f;
+    const u32 min_own = (u32)ceilf(rf * rf * (float)K / 0.998f);
+    k_knn_route<<<gb, 256, 0, ctx->stream>>>(g, a.frame_of, min_own, qlevel);
     RVP_LAUNCH_CHECK(ctx);
+    const int cblocks = ctx->num_sms * 2;
+    for (int level = 0; level < kGridLevels; ++level) {
+      k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, level, a.open_flags);
+      RVP_LAUNCH_CHECK(ctx);
+      exclusive_scan_u32_to_u64(ctx, a.open_flags, a.open_pos, a.n_max, g.n_points, a.scan_tmp);
+      k_open_scatter<<<gb, 256, 0, ctx->stream>>>(a.open_flags, a.open_pos, g.n_points,
+                                                  a.open_list, a.open_n,
+                                                  a.routed ? a.routed + level : nullptr);
+      RVP_LAUNCH_CHECK(ctx);
+      u32 *st = stats ? stats + level : nullptr;  // certified at this level
+      if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
+      if (mode == TILE_SOR_MEAN)
+        k_knn_coop<K, TILE_SOR_MEAN><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
+            g, a, level, a.open_list, a.open_n, qlevel, a.qtau, st);
+      else if (mode == TILE_SOR_LIST)
+        k_knn_coop<K, TILE_SOR_LIST><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
+            g, a, level, a.open_list, a.open_n, qlevel, a.qtau, st);
+      else
+        k_knn_coop<K, TILE_PAIRS_F><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
+            g, a, level, a.open_list, a.open_n, qlevel, a.qtau, st);
+      RVP_LAUNCH_CHECK(ctx);
+      if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
+    }
     a.preset_open = true;
     a.rfac = 0.0f;
+    a.level_events = nullptr;  // the per-lane kernels after it are not timed apart
   }
   if (!a.preset_open) RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
   if (a.level0_warp) {
@@ -804,8 +910,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
         list = a.open_list;
       }
       u32 *st = stats ? stats + level : nullptr;
-      if (a.level_events && !(coop && level == 0))
-        cudaEventRecord(a.level_events[2 * level], ctx->stream);
+      if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
       if (mode == TILE_SOR_MEAN)
         k_knn_wt<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                     qlevel, a.qtau, st);
@@ -857,10 +962,11 @@ namespace {
 // rest is unchanged), so the first KN entries of its SOR list, when all kept,
 // are exactly the list the normal needs. Those points get their normal here;
 // the others are marked open (qlevel 0) for the kNN search. One thread per
-// grid point.
+// grid point: its row of the list (rows by grid position, so a warp reads
+// consecutive rows) and its neighbours' float4 grid records (spatially close,
+// so mostly cached), whose index word carries the removed flag.
 template <int KN>
-__global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs a, int ks,
-                                                           const uint8_t *keep) {
+__global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs a, int ks) {
   const u64 n = *g.n_points;
   for (u64 pos = blockIdx.x * (u64)blockDim.x + threadIdx.x; pos < n;
        pos += (u64)gridDim.x * blockDim.x) {
@@ -870,14 +976,18 @@ __global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs 
       a.qlevel[pos] = 0xFF;
       continue;
     }
-    const u32 *row = a.sor_list + (size_t)qidx * ks;
-    int I[KN];
+    const u32 *row = a.sor_list + (size_t)pos * ks;
+    float px[KN], py[KN], pz[KN];
     bool ok = true;
 #pragma unroll
     for (int t = 0; t < KN; ++t) {
       const u32 j = __ldg(&row[t]);
-      ok = ok && j != 0xFFFFFFFFu && keep[j];
-      I[t] = ok ? (int)j : 0;
+      ok = ok && j != 0xFFFFFFFFu;
+      const float4 p = ok ? __ldg(&g.pts[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      ok = ok && !(__float_as_uint(p.w) & kRemovedBit);
+      px[t] = p.x;
+      py[t] = p.y;
+      pz[t] = p.z;
     }
     if (!ok) {
       a.qlevel[pos] = 0;
@@ -885,8 +995,8 @@ __global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs 
     }
     a.qlevel[pos] = 0xFF;
     float nx, ny, nz;
-    normal_from_regs<KN>(a.vx, a.vy, a.vz, [&](int t) { return I[t]; }, true, a.iters, q.x, q.y,
-                         q.z, a.vpx, a.vpy, a.vpz, nx, ny, nz);
+    normal_from_coords<KN>(px, py, pz, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy, a.vpz, nx,
+                           ny, nz);
     const u64 o = a.out_pos[qidx];
     a.nx[o] = nx;
     a.ny[o] = ny;
@@ -896,13 +1006,13 @@ __global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs 
 }  // namespace
 
 bool normals_from_sor_lists(rvp_context *ctx, const GridView &g, const TileArgs &a, int ks,
-                            int kn, const uint8_t *keep) {
+                            int kn) {
   if (g.mode != KEY_DENSE || !a.sor_list || !a.qlevel || kn > ks) return false;
   const unsigned blocks = grid_for(a.n_max, 256, ctx->num_sms * 16);
   switch (kn) {
 #define RVP_NSL(K)                                                                        \
   case K:                                                                                 \
-    k_normals_sor_lists<K><<<blocks, 256, 0, ctx->stream>>>(g, a, ks, keep);              \
+    k_normals_sor_lists<K><<<blocks, 256, 0, ctx->stream>>>(g, a, ks);                    \
     break;
     RVP_NSL(8) RVP_NSL(11) RVP_NSL(16) RVP_NSL(17) RVP_NSL(21) RVP_NSL(31) RVP_NSL(32)
     RVP_NSL(33)

@@ -119,24 +119,14 @@ __device__ __forceinline__ void normal_from_list(const float *__restrict__ x,
 
 namespace rvp {
 namespace nd {
-// normal_from_list over a register-resident list of M neighbours
-// (compile-time length: every index below is static).
-// The same over M indices (compile-time length) given by idx(t).
-template <int M, class IdxF>
-__device__ __forceinline__ void normal_from_regs(const float *__restrict__ x,
-                                                 const float *__restrict__ y,
-                                                 const float *__restrict__ z, IdxF idx,
-                                                 bool div_centroid, int iters, float qx, float qy,
-                                                 float qz, float vpx, float vpy, float vpz,
-                                                 float &nx, float &ny, float &nz) {
-  float px[M], py[M], pz[M];
-#pragma unroll
-  for (int t = 0; t < M; ++t) {
-    const int j = idx(t);
-    px[t] = __ldg(&x[j]);
-    py[t] = __ldg(&y[j]);
-    pz[t] = __ldg(&z[j]);
-  }
+// normal_from_list over a register-resident list of M neighbours'
+// coordinates (compile-time length: every index below is static).
+template <int M>
+__device__ __forceinline__ void normal_from_coords(const float (&px)[M], const float (&py)[M],
+                                                   const float (&pz)[M], bool div_centroid,
+                                                   int iters, float qx, float qy, float qz,
+                                                   float vpx, float vpy, float vpz, float &nx,
+                                                   float &ny, float &nz) {
   float cx = 0.0f, cy = 0.0f, cz = 0.0f;
 #pragma unroll
   for (int t = 0; t < M; ++t) {
@@ -169,6 +159,25 @@ __device__ __forceinline__ void normal_from_regs(const float *__restrict__ x,
   float A[3][3] = {{c00, c01, c02}, {c01, c11, c12}, {c02, c12, c22}};
   eigen_smallest_ref(A, iters, nx, ny, nz);
   flip_ref(qx, qy, qz, vpx, vpy, vpz, nx, ny, nz);
+}
+
+// The same over M indices (compile-time length) given by idx(t) into x, y, z.
+template <int M, class IdxF>
+__device__ __forceinline__ void normal_from_regs(const float *__restrict__ x,
+                                                 const float *__restrict__ y,
+                                                 const float *__restrict__ z, IdxF idx,
+                                                 bool div_centroid, int iters, float qx, float qy,
+                                                 float qz, float vpx, float vpy, float vpz,
+                                                 float &nx, float &ny, float &nz) {
+  float px[M], py[M], pz[M];
+#pragma unroll
+  for (int t = 0; t < M; ++t) {
+    const int j = idx(t);
+    px[t] = __ldg(&x[j]);
+    py[t] = __ldg(&y[j]);
+    pz[t] = __ldg(&z[j]);
+  }
+  normal_from_coords<M>(px, py, pz, div_centroid, iters, qx, qy, qz, vpx, vpy, vpz, nx, ny, nz);
 }
 
 template <int M>

@@ -41,6 +41,7 @@ struct rvp_pipeline {
   rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
   rvp::DevBuf stats;  // 16 kNN path counters (diagnostics)
+  rvp::DevBuf routed; // SOR queries the cooperative kNN routed to each grid level
   rvp::DevBuf hard;   // queries the tile kernel could not certify (+ counter)
   rvp::DevBuf qlevel; // per grid point: level at which its kNN is still open
   rvp::DevBuf qtau;   // per grid point: K-th distance bound handed to the next level
@@ -153,7 +154,8 @@ void release_pipeline(rvp_pipeline *p) {
                          &p->knn_counts, &p->mean, &p->keep, &p->sor_tmp, &p->sor_aos, &p->sor_x,
                          &p->sor_y, &p->sor_z, &p->sor_offs, &p->sor_frame, &p->sor_src,
                          &p->nrm_pairs, &p->nrm_counts, &p->nx, &p->ny, &p->nz, &p->r_model,
-                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel, &p->qtau, &p->open};
+                         &p->r_best, &p->r_iters, &p->r_rand, &p->stats, &p->hard, &p->qlevel,
+                         &p->qtau, &p->open, &p->routed};
   for (auto *b : bufs) b->release();
   p->vw.release();
   p->grid.release();
@@ -186,6 +188,9 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     RVP_REQUIRE(cfg->sor_k >= 1 && cfg->sor_k + 1 <= 64, "sor_k must be in [1, 63]");
     RVP_REQUIRE(cfg->normal_k >= 1 && cfg->normal_k + 1 <= 64, "normal_k must be in [1, 63]");
     RVP_REQUIRE(cfg->ransac_iters >= 0, "ransac_iters must be >= 0");
+    RVP_REQUIRE(cfg->block_threads >= 0 && cfg->block_threads <= 256 &&
+                    cfg->block_threads % 32 == 0,
+                "block_threads must be 0 or a multiple of 32 up to 256");
     RVP_CUDA_TRY(cudaSetDevice(ctx->device));
     p->ctx = ctx;
     p->cfg = *cfg;
@@ -217,6 +222,7 @@ rvp_status rvp_pipeline_create(rvp_context *ctx, const rvp_pipeline_config *cfg,
     p->hard.reserve(N * 8 + 256);
     p->qlevel.reserve(N);
     p->qtau.reserve(N * 4);
+    p->routed.reserve(256);
     p->open.reserve(((N * 4 + 255) & ~(size_t)255) + ((N * 8 + 8 + 255) & ~(size_t)255) +
                     ((N * 4 + 255) & ~(size_t)255) + 256 + rvp::scan_temp_bytes(N));
     p->nrm_counts.reserve(N * 4);
@@ -306,7 +312,9 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.rfac = p->rfac;
     ta.lane_levels = p->lane_levels;
     ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles instead
-    ta.coop = c.queries_per_warp == 3;         // 3: cooperative level-0 pass first
+    ta.coop = c.queries_per_warp == 3;         // 3: cooperative passes first
+    ta.routed = p->routed.as<u64>();
+    if (ta.coop) RVP_CUDA_TRY(cudaMemsetAsync(ta.routed, 0, 8 * rvp::kGridLevels, st));
     {
       char *op = p->open.as<char>();
       auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -365,6 +373,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
         p->grid.b_pts.as<float4>(), p->keep.as<uint8_t>(), n_vox, N);
     RVP_LAUNCH_CHECK(ctx);
     rvp::TileArgs tn = ta;
+    tn.routed = nullptr;
     tn.mean = nullptr;
     tn.vx = p->vox_x.as<float>();
     tn.vy = p->vox_y.as<float>();
@@ -384,8 +393,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     RVP_CUDA_TRY(cudaMemsetAsync(hard_n64, 0, 16, st));
     // points whose SOR list holds kn kept points: normal straight from it;
     // the rest open for the kNN search
-    tn.preset_open = sor_lists && rvp::normals_from_sor_lists(ctx, gv, tn, ks, kn,
-                                                              p->keep.as<uint8_t>());
+    tn.preset_open = sor_lists && rvp::normals_from_sor_lists(ctx, gv, tn, ks, kn);
     bool tn_ok = tiled && rvp::grid_knn_tile(ctx, gv, kn, rvp::TILE_NORMALS, tn, 0,
                                              st0 ? st0 + 13 : nullptr);
     if (!tn_ok) {
@@ -521,6 +529,20 @@ rvp_status rvp_pipeline_knn_stats(rvp_pipeline *p, int enable, uint32_t *out16) 
   });
 }
 
+rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out) {
+  if (!p || !out) return RVP_ERR_INVALID_ARG;
+  return guard(p->ctx, [&] {
+    RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
+    if (!p->routed.ptr) {
+      for (int l = 0; l < rvp::kGridLevels; ++l) out[l] = 0;
+      return;
+    }
+    RVP_CUDA_TRY(cudaMemcpyAsync(out, p->routed.ptr, 8 * rvp::kGridLevels,
+                                 cudaMemcpyDeviceToHost, p->ctx->stream));
+    RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
+  });
+}
+
 rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_offsets,
                                       int64_t *sor_offsets) {
   if (!p) return RVP_ERR_INVALID_ARG;
@@ -540,7 +562,8 @@ rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size, int block_t
                                    int queries_per_warp) {
   if (!p) return RVP_ERR_INVALID_ARG;
   if (!(cell_size > 0.0f)) return RVP_ERR_INVALID_ARG;
-  if (block_threads < 0 || block_threads > 1024 || (block_threads % 32) != 0)
+  // the warp-per-query kernel is compiled for blocks of at most 256 threads
+  if (block_threads < 0 || block_threads > 256 || (block_threads % 32) != 0)
     return RVP_ERR_INVALID_ARG;
   p->cell = cell_size;
   p->cfg.cell_size = cell_size;
