@@ -428,7 +428,7 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # kernels timed live for the roofline (CUDA events around each launch): the
 # SOR kNN kernel of each grid level and RANSAC
-LEVEL_STAGES = ("sor_knn_l0", "sor_knn_l1", "sor_knn_l2")
+LEVEL_STAGES = tuple(f"sor_knn_l{lv}" for lv in range(5))
 
 
 def kernel_name(stage: str, coop: bool) -> str:
@@ -597,6 +597,15 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
     t_ptg, (_, bp, it_ptg) = timed(lambda: LR.ransac_frames(be, 10_000, T, targets=tg, ctx=ctx))
     lr = LR.LearnedRansac(scorer)
     cand, coffs = lr.prepare(be)
+    # the feature kNN's kernels: one query per lane, or the cooperative pass
+    # (same features); the faster one serves the learned arm
+    knn_modes = {}
+    for mode, rf in ((0, 1.0), (3, 1.0), (3, 0.7)):
+        scorer.set_knn(mode, rf)
+        knn_modes[f"qpw{mode}_rfac{rf}"] = timed(
+            lambda: LR.proposal_features(scorer, be, cand, coffs, lr.cell, lr.scope))[0]
+    best_mode = min(knn_modes, key=knn_modes.get)
+    scorer.set_knn(int(best_mode[3]), float(best_mode.split("rfac")[1]))
     t_l, (_, bl, it_l) = timed(lambda: lr.run(be, cand, coffs, 10_000, T, targets=tg))
     t_f, feat = timed(lambda: LR.proposal_features(scorer, be, cand, coffs, lr.cell, lr.scope))
     t_m, logits = timed(lambda: scorer.forward(feat))
@@ -630,6 +639,7 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
                                          "median": q(it_ptg, 0.5), "p90": q(it_ptg, 0.9)},
            "learned_to_count_ms": t_l,
            "learned_parts_ms": {"features": t_f, "mlp": t_m, "weighted_ransac": t_w},
+           "feature_knn_ms_by_mode": knn_modes, "feature_knn_mode": best_mode,
            "learned_hypotheses_drawn_to_count": {"mean": float(it_l.double().mean().item()),
                                                  "median": q(it_l, 0.5), "p90": q(it_l, 0.9)},
            "learned_reached_fraction": float((bl >= tg).float().mean().item()),

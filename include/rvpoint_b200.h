@@ -326,8 +326,11 @@ RVP_API rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p);
 /* RVP_ERR_CAPACITY if the last run's bucket table overflowed (results of
  * that run are then incomplete); synchronizes the stream. */
 RVP_API rvp_status rvp_pipeline_check(rvp_pipeline *p);
-/* Queries of the SOR kNN the last run's cooperative pass routed to each of
- * the three grid levels (queries_per_warp 3; zeros otherwise). out[3]. */
+/* Grid levels of the batched neighbour grid: cells of edge c, 2c, 4c, 8c,
+ * 16c (c = the pipeline's cell size). */
+#define RVP_GRID_LEVELS 5
+/* Queries of the SOR kNN the last run's cooperative pass routed to each
+ * grid level (queries_per_warp 3; zeros otherwise). out[RVP_GRID_LEVELS]. */
 RVP_API rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out);
 /* Diagnostics: enable != 0 makes the kNN kernels count which search path
  * settled each query (out16[0..7] SOR, [8..15] normals: fine ring, fine
@@ -344,11 +347,13 @@ RVP_API rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_of
  * was captured with. */
 RVP_API rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size,
                                            int block_threads, int queries_per_warp);
-/* First-pass search radius of the level-0 kNN tiles, as a factor of
- * cell * sqrt(k / points in the query's cell) (0 disables the first pass;
+/* First-pass search radius of the kNN, as a factor of cell * sqrt(k /
+ * points in the query's cell); with the cooperative kernels (queries_per_warp
+ * 3) a query also goes to the finest grid level whose own cell holds at least
+ * ceil(rfac^2 k) points (0 disables the first pass of the per-lane kernels;
  * results never depend on it, only the work does). */
 RVP_API rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac);
-/* Grid levels (1-3; 0 = all 3) whose kNN runs one query per lane; the
+/* Grid levels (1 to RVP_GRID_LEVELS; 0 = all) whose kNN runs one query per lane; the
  * queries still open after them go to the warp-per-query kernel, which
  * spreads a query's candidates over the lanes. Results never depend on it. */
 RVP_API rvp_status rvp_pipeline_set_lane_levels(rvp_pipeline *p, int levels);

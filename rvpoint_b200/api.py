@@ -784,17 +784,18 @@ class Pipeline:
                 "normals": dict(zip(self.PATHS, map(int, out[8:16])))}
 
     def knn_routed(self) -> list:
-        """SOR kNN queries the last run's cooperative pass routed to grid
-        levels 0, 1, 2 (zeros without it)."""
-        out = np.zeros(3, np.uint64)
+        """SOR kNN queries the last run's cooperative pass routed to each grid
+        level (zeros without it)."""
+        out = np.zeros(self.GRID_LEVELS, np.uint64)
         check(self.L.rvp_pipeline_knn_routed(self.h, _ptr(out)), self.ctx.h)
         return [int(v) for v in out]
 
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)
 
-    LEVEL_KERNELS = ("sor_knn_l0", "sor_knn_l1", "sor_knn_l2", "normals_knn_l0",
-                     "normals_knn_l1", "normals_knn_l2")
+    GRID_LEVELS = 5  # RVP_GRID_LEVELS: cells of c, 2c, 4c, 8c, 16c
+    LEVEL_KERNELS = tuple(f"{st}_knn_l{lv}" for st in ("sor", "normals")
+                          for lv in range(GRID_LEVELS))
 
     def stage_times(self, levels: bool = False) -> dict:
         """Mean ms per stage over the runs recorded since set_timing; with

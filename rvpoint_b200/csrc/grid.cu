@@ -11,9 +11,9 @@
 //    (spatial_hashing.h:43-45). Buckets are then exactly the reference's
 //    grid_ entries, collisions included.
 //  * KEY_DENSE: per-frame dense keys for many frames in one sort and one
-//    table. Keys are hierarchical -- coarse cell (4 x 4 x 4 fine cells)
-//    times 64 plus the fine cell inside it -- so both fine and coarse cells
-//    are contiguous runs of the sorted points; the table holds both levels.
+//    table. Keys are hierarchical (a Morton code of the fine cell inside a
+//    group of 64 x 64 x 64), so the cells of every level c, 2c, 4c, ... are
+//    contiguous runs of the sorted points; the table holds five levels.
 //
 // Queries: one warp per query. Lanes look up up to 32 window cells at once,
 // a warp scan of bucket sizes flattens the window into one candidate stream,
@@ -184,8 +184,8 @@ __global__ void k_cell_keys(const float *__restrict__ x, const float *__restrict
   }
 }
 
-// heads of level-L buckets: key >> 6L changes (dense mode: L = 0..3; the
-// reference hash: L = 0 only)
+// heads of level-L buckets: key >> 3L changes (dense mode: L = 0 ..
+// kHeadLevels - 1; the reference hash: L = 0 only)
 __global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int levels, u32 *heads) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -193,7 +193,7 @@ __global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int lev
     const u64 k = keys[i];
     const u64 p = i ? keys[i - 1] : 0;
     for (int L = 0; L < levels; ++L)
-      heads[(size_t)L * n_max + i] = (i == 0 || (k >> (6 * L)) != (p >> (6 * L))) ? 1u : 0u;
+      heads[(size_t)L * n_max + i] = (i == 0 || (k >> (3 * L)) != (p >> (3 * L))) ? 1u : 0u;
   }
 }
 
@@ -244,14 +244,14 @@ __global__ void k_insert(const u64 *keys, const u32 *lstart, const u64 *bucket_o
                          const u64 *n_dev, int levels, int table_levels, ulonglong2 *table,
                          u64 mask, u64 *nbuckets, int *overflow) {
   const size_t n = n_dev ? *n_dev : n_max;
-  u64 nb[4] = {0, 0, 0, 0};
+  u64 nb[kHeadLevels] = {};
   u64 tot = 0;
   for (int L = 0; L < levels; ++L) {
     nb[L] = bucket_of[(size_t)L * (n_max + 1) + n];
     if (L < table_levels) tot += nb[L];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0)
-    for (int L = 0; L < 4; ++L) nbuckets[L] = nb[L];
+    for (int L = 0; L < kHeadLevels; ++L) nbuckets[L] = nb[L];
   for (u64 b = blockIdx.x * (u64)blockDim.x + threadIdx.x; b < tot;
        b += (u64)gridDim.x * blockDim.x) {
     int L = 0;
@@ -260,7 +260,7 @@ __global__ void k_insert(const u64 *keys, const u32 *lstart, const u64 *bucket_o
     const u32 *st = lstart + (size_t)L * n_max;
     const u32 s = st[c];
     const u32 e = (c + 1 < nb[L]) ? st[c + 1] : (u32)n;
-    const u64 key = L == 0 ? keys[s] : (((u64)L << 62) | (keys[s] >> (6 * L)));
+    const u64 key = L == 0 ? keys[s] : (((u64)L << 60) | (keys[s] >> (3 * L)));
     table_put(table, mask, key, (u64)s | ((u64)(e - s) << 32), overflow);
   }
 }
@@ -293,19 +293,23 @@ void Grid::reserve(size_t n, int nf) {
   b_pts.reserve(n_max * 16);
   b_frames.reserve(al(n_frames_max * sizeof(GridFrame)) + al(n_frames_max * 6 * 4));
   b_begin.reserve(al((n_frames_max + 1) * 8));
-  b_sort.reserve(sort_temp_bytes(n_max) + al(4 * n_max * 4) + al(4 * (n_max + 1) * 8) +
+  b_sort.reserve(sort_temp_bytes(n_max) + al(kHeadLevels * n_max * 4) +
+                 al(kHeadLevels * (n_max + 1) * 8) +
                  scan_temp_bytes(n_max));
-  b_lstart.reserve(al(4 * n_max * 4));
+  b_lstart.reserve(al(kHeadLevels * n_max * 4));
   b_pos.reserve(n_max * 4);
   b_misc.reserve(256);
   d_n = b_misc.as<u64>();
   d_nbuckets = d_n + 1;
-  d_collision = reinterpret_cast<int *>(d_n + 5);
+  d_collision = reinterpret_cast<int *>(d_n + 1 + kHeadLevels);
   d_overflow = d_collision + 1;
-  // buckets of levels 0-2 never exceed 3 n (in practice ~1.2 n); without a
-  // measured count the table is sized for 2 n
-  const size_t want = table_cap_req ? table_cap_req
-                                    : (size_t)next_pow2((u64)(2 * n_max + n_max / 2 + 1024));
+  // the buckets of the table levels never exceed kGridLevels n (each holds a
+  // point; in practice ~1.4 n): without a measured count the table holds
+  // that many, so no insert can fail; rvp_pipeline_fit_tables and the
+  // scorer shrink it to the measured count so that it stays in L2
+  const size_t want =
+      table_cap_req ? table_cap_req
+                    : (size_t)next_pow2((u64)(kGridLevels * n_max + n_max / 4 + 1024));
   if (want != table_cap || !b_table.ptr) {
     table_cap = 0;
     b_table.release();
@@ -336,7 +340,7 @@ GridView Grid::view(int mode, long long p1, long long p2) const {
   v.mode = mode;
   v.p1 = p1;
   v.p2 = p2;
-  for (int L = 0; L < 4; ++L) v.lstart[L] = b_lstart.as<u32>() + (size_t)L * n_max;
+  for (int L = 0; L < kHeadLevels; ++L) v.lstart[L] = b_lstart.as<u32>() + (size_t)L * n_max;
   v.n_level = d_nbuckets;
   v.n_points = d_n;
   v.pos_of = b_pos.as<u32>();
@@ -350,7 +354,7 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   cudaStream_t st = ctx->stream;
   const size_t n_max = n_points;
   const u64 *n_dev = n_dev_opt;
-  const int levels = mode == KEY_DENSE ? 4 : 1;
+  const int levels = mode == KEY_DENSE ? kHeadLevels : 1;
   const int table_levels = mode == KEY_DENSE ? kGridLevels : 1;
   GridFrame *frames = g.b_frames.as<GridFrame>();
   float *bb = reinterpret_cast<float *>(g.b_frames.as<char>() + al(g.n_frames_max * sizeof(GridFrame)));
@@ -361,8 +365,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   sort_temp_carve(t, sp, g.n_max);
   sp += sort_temp_bytes(g.n_max);
   // per-level arrays use stride n_max (heads, starts) / n_max + 1 (ids)
-  u32 *heads = reinterpret_cast<u32 *>(sp); sp += al(4 * g.n_max * 4);
-  u64 *bucket_of = reinterpret_cast<u64 *>(sp); sp += al(4 * (g.n_max + 1) * 8);
+  u32 *heads = reinterpret_cast<u32 *>(sp); sp += al(kHeadLevels * g.n_max * 4);
+  u64 *bucket_of = reinterpret_cast<u64 *>(sp); sp += al(kHeadLevels * (g.n_max + 1) * 8);
   void *scan_tmp = sp;
   u32 *lstart = g.b_lstart.as<u32>();
   // strides below are g.n_max; the kernels are given g.n_max as their n_max
@@ -391,7 +395,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
     exclusive_scan_u32_to_u64(ctx, heads + (size_t)L * nm, bucket_of + (size_t)L * (nm + 1), nm,
                               n_live, scan_tmp);
   RVP_CUDA_TRY(cudaMemsetAsync(g.b_table.ptr, 0xFF, g.table_cap * 16, st));
-  RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 40, st));  // buckets[4], collision, overflow
+  // buckets per level, collision, overflow
+  RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 8 * kHeadLevels + 8, st));
   k_reorder<<<gb, 256, 0, st>>>(x, y, z, g.b_vals.as<u32>(), heads, bucket_of, nm, n_live, levels,
                                 g.b_pts.as<float4>(), lstart, frames, mode, g.d_collision,
                                 g.b_pos.as<u32>());

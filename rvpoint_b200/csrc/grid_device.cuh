@@ -3,14 +3,14 @@
 // hierarchical keys, bucket-table lookup, query windows and their exact
 // coverage bounds, and the warp-cooperative candidate walk.
 //
-// Dense keys are hierarchical: a level-L cell is 4 x 4 x 4 level-(L-1) cells
-// (edge c * 4^L), and the 64-bit key of a fine cell is
-//   key_base(frame) + (level-3 cell, x fastest) << 18
-//                   + sub2 << 12 + sub1 << 6 + sub0,
-// subL = 6-bit position of the level-L cell inside its level-(L+1) parent.
-// Sorting by this key therefore makes every cell of every level one
-// contiguous run of points; level-L cells (L = 0, 1, 2) are entered in the
-// bucket table under key >> 6L tagged with L in bits 62-63.
+// Dense keys are hierarchical: a level-L cell is 2 x 2 x 2 level-(L-1) cells
+// (edge c * 2^L), and the 64-bit key of a fine cell is
+//   key_base(frame) + (group cell, x fastest) << 18 + morton(cx, cy, cz),
+// a group being 64 x 64 x 64 fine cells and morton the 18-bit interleave of
+// the low 6 bits of the cell indices (bit 3i + a = bit i of axis a).
+// Sorting by this key makes every cell of every level one contiguous run of
+// points; level-L cells are entered in the bucket table under key >> 3L
+// tagged with L in bits 60-63.
 #pragma once
 
 #include <math.h>
@@ -34,18 +34,24 @@ __device__ __forceinline__ int cell_axis_clamped(float v, float mn, float cell, 
 }
 
 __device__ __forceinline__ int level_dim(int g, int level) {
-  return (g + (1 << (2 * level)) - 1) >> (2 * level);
+  return (g + (1 << level) - 1) >> level;
 }
 
-__device__ __forceinline__ u64 sub_index(int cx, int cy, int cz, int level) {
-  const int s = 2 * level;
-  return (u64)((((cz >> s) & 3) << 4) | (((cy >> s) & 3) << 2) | ((cx >> s) & 3));
+// the low 6 bits of x, y, z interleaved (x in bits 0, 3, 6, ...)
+__device__ __forceinline__ u32 spread3(u32 v) {
+  v &= 63u;
+  v = (v | (v << 8)) & 0x0300Fu;
+  v = (v | (v << 4)) & 0x030C3u;
+  v = (v | (v << 2)) & 0x09249u;
+  return v;
+}
+__device__ __forceinline__ u64 morton18(int cx, int cy, int cz) {
+  return (u64)(spread3((u32)cx) | (spread3((u32)cy) << 1) | (spread3((u32)cz) << 2));
 }
 
 __device__ __forceinline__ u64 dense_key(const GridFrame &F, int cx, int cy, int cz) {
   const u64 c3 = ((u64)(cz >> 6) * (u64)F.g3y + (u64)(cy >> 6)) * (u64)F.g3x + (u64)(cx >> 6);
-  return F.key_base + (c3 << 18) + (sub_index(cx, cy, cz, 2) << 12) +
-         (sub_index(cx, cy, cz, 1) << 6) + sub_index(cx, cy, cz, 0);
+  return F.key_base + (c3 << 18) + morton18(cx, cy, cz);
 }
 
 __device__ __forceinline__ u64 fine_key(const GridView &g, const GridFrame &F, int cx, int cy,
@@ -61,13 +67,12 @@ __device__ __forceinline__ u64 fine_key(const GridView &g, const GridFrame &F, i
 __device__ __forceinline__ u64 level_key(const GridView &g, const GridFrame &F, int level, int X,
                                          int Y, int Z) {
   if (level == 0) return fine_key(g, F, X, Y, Z);
-  const int s = 2 * level;
-  return ((u64)level << 62) | (dense_key(F, X << s, Y << s, Z << s) >> (3 * s));
+  return ((u64)level << 60) | (dense_key(F, X << level, Y << level, Z << level) >> (3 * level));
 }
 
 struct Window {
   int lo[3], hi[3];  // cells, inclusive, at `level`
-  int level;         // 0 fine; 1, 2 coarser (dense mode only)
+  int level;         // 0 fine; 1 .. kGridLevels - 1 coarser (dense mode only)
 };
 
 __device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u32 &count) {
@@ -89,7 +94,7 @@ __device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u
 // |p - q| <= r (1 + 3 * 2^-24) per axis for any such p; the bound is padded
 // to r (1 + 1e-6) and rounded outwards, and the cell function is monotone,
 // so the window is exact. Clamped to the frame's grid, then taken at `level`
-// (fine index >> 2 level).
+// (fine index >> level).
 __device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, float qy, float qz,
                                                double r, int level = 0) {
   const double rp = r * (1.0 + 1e-6) + 1e-30;
@@ -105,8 +110,8 @@ __device__ __forceinline__ Window tight_window(const GridFrame &F, float qx, flo
     w.lo[a] = max(cell_axis_clamped(lo, mn[a], F.cell, -1, G[a]), 0);
     w.hi[a] = min(cell_axis_clamped(hi, mn[a], F.cell, -1, G[a]), G[a] - 1);
     if (level) {
-      w.lo[a] >>= 2 * level;
-      w.hi[a] = w.hi[a] < 0 ? -1 : (w.hi[a] >> (2 * level));
+      w.lo[a] >>= level;
+      w.hi[a] = w.hi[a] < 0 ? -1 : (w.hi[a] >> level);
     }
   }
   return w;
@@ -136,7 +141,7 @@ __device__ __forceinline__ Window ring_window(const GridFrame &F, float qx, floa
   const int G[3] = {F.gx, F.gy, F.gz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1) >> (2 * level);
+    const int c = cell_axis_clamped(q[a], mn[a], F.cell, 0, G[a] - 1) >> level;
     w.lo[a] = max(c - ring, 0);
     w.hi[a] = min(c + ring, level_dim(G[a], level) - 1);
   }
@@ -150,7 +155,7 @@ __device__ __forceinline__ double coverage(const GridFrame &F, const Window &w, 
   const float q[3] = {qx, qy, qz};
   const float mn[3] = {F.min_x, F.min_y, F.min_z};
   const int G[3] = {F.gx, F.gy, F.gz};
-  const double cs = (double)F.cell * (double)(1 << (2 * w.level));
+  const double cs = (double)F.cell * (double)(1 << w.level);
   double cov = 1e300;
   const double u = 4.0 * 5.960464477539063e-08;  // 4 * 2^-24
 #pragma unroll

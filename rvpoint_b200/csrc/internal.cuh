@@ -185,7 +185,11 @@ struct GridFrame {  // per-frame grid parameters (device)
 };
 
 enum KeyMode { KEY_REF_HASH = 0, KEY_DENSE = 1 };
-constexpr int kGridLevels = 3;  // cell levels in the bucket table: c, 4c, 16c
+// The dense grid is a binary hierarchy: a level-L cell is 2 x 2 x 2 level-(L-1)
+// cells (edge c * 2^L); the bucket table holds levels 0 .. kGridLevels - 1
+// (c .. 16c), and the run starts of one level more are kept (kHeadLevels).
+constexpr int kGridLevels = RVP_GRID_LEVELS;
+constexpr int kHeadLevels = kGridLevels + 1;
 
 struct GridView {  // what the query kernels read
   const float4 *pts;       // cell-sorted {x,y,z,idx}
@@ -195,7 +199,7 @@ struct GridView {  // what the query kernels read
   const u64 *frame_pt_begin;  // per frame: first sorted position
   int mode;
   long long p1, p2;        // mode 0 primes
-  const u32 *lstart[4];    // dense mode: first sorted position of each level-L bucket
+  const u32 *lstart[kHeadLevels];  // dense mode: first sorted position of each level-L bucket
   const u64 *n_level;      // dense mode: number of level-L buckets (device, [4])
   const u64 *n_points;     // number of grid points (device; set by grid_build)
   const u32 *pos_of;       // sorted position of each point (by original index)
@@ -208,7 +212,7 @@ struct Grid {
   size_t table_cap_req = 0;    // 0: sized from n_max
   DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_lstart, b_pos;
   u64 *d_n = nullptr;          // number of points (device)
-  u64 *d_nbuckets = nullptr;   // buckets per level [4] (device)
+  u64 *d_nbuckets = nullptr;   // buckets per level [kHeadLevels] (device)
   int *d_collision = nullptr;  // mode 0: hash collision detected
   int *d_overflow = nullptr;   // a bucket found no free table slot
   GridView view(int mode, long long p1, long long p2) const;

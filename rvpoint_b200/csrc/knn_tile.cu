@@ -1,8 +1,8 @@
 // Tile kNN for dense (batched) grids on sm_100a.
 //
-// Level by level (cells of c, 4c, 16c): one thread block per bucket of the
-// next level up (a group of 4 x 4 x 4 cells) looks up the 6 x 6 x 6 cells
-// around it once (one lookup per thread), flattens them with a prefix sum
+// Level by level (cells of c, 2c, 4c, ...): one thread block per bucket of
+// the next level up (a group of 2 x 2 x 2 cells) looks up the 4 x 4 x 4
+// cells around it once (one lookup per thread), flattens them with a prefix sum
 // and stages their points in shared memory (coalesced float4 runs). Every
 // open query of the group is then handled by one thread, which scans its own
 // 27-cell ring out of shared memory and keeps a register-resident sorted
@@ -10,7 +10,7 @@
 // packed (d2, index) keys when ties must follow the reference's (d2, index)
 // order). The ring certifies the result when the K-th distance is below the
 // ring's coverage (distance to the nearest outside cell, with rounding
-// slack); the others stay open for the next, 4x coarser level, and after the
+// slack); the others stay open for the next, 2x coarser level, and after the
 // last level go to a list that the warp-per-query kernel finishes. Epilogues are fused: SOR mean distance
 // (statistical_outlier_removal.cpp:36-40) or the reference normal
 // (normal_estimation.cpp:90-110) straight from the registers.
@@ -26,8 +26,8 @@ using namespace nd;
 
 namespace {
 constexpr int TT = 256;                      // threads per tile block
-constexpr int SIDE = 6;                      // staged fine cells per axis
-constexpr int NCELL = SIDE * SIDE * SIDE;    // 216
+constexpr int SIDE = 4;                      // staged cells per axis: a group and its halo
+constexpr int NCELL = SIDE * SIDE * SIDE;    // 64
 constexpr int CAP = 2560;                    // staged candidates (40 KB)
 
 // the 27 ring cells, nearest first: own cell, 6 faces, 12 edges, 8 corners
@@ -92,7 +92,7 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
   const u32 *gstart = g.lstart[level + 1];
   const u64 n = *g.n_points;
   const int tid = threadIdx.x;
-  const int sh = 2 * level;  // level-L cell = fine index >> sh
+  const int sh = level;  // level-L cell = fine index >> sh
   Key kMax;
   if constexpr (MODE == TILE_SOR_MEAN) kMax = INFINITY;
   else kMax = ~0ull;
@@ -113,10 +113,10 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
       const u32 i0 = __float_as_uint(p0.w) & 0x7FFFFFFFu;
       const int f = a.frame_of ? a.frame_of[i0] : 0;
       const GridFrame F = g.frames[f];
-      const int gs = sh + 2;  // group cell = fine index >> gs
-      s_base[0] = (cell_axis(p0.x, F.min_x, F.cell) >> gs) * 4 - 1;
-      s_base[1] = (cell_axis(p0.y, F.min_y, F.cell) >> gs) * 4 - 1;
-      s_base[2] = (cell_axis(p0.z, F.min_z, F.cell) >> gs) * 4 - 1;
+      const int gs = sh + 1;  // group cell = fine index >> gs
+      s_base[0] = (cell_axis(p0.x, F.min_x, F.cell) >> gs) * 2 - 1;
+      s_base[1] = (cell_axis(p0.y, F.min_y, F.cell) >> gs) * 2 - 1;
+      s_base[2] = (cell_axis(p0.z, F.min_z, F.cell) >> gs) * 2 - 1;
       s_base[3] = f;
       s_F = F;
     }
@@ -125,7 +125,7 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
     const GridFrame &F = s_F;
     const int dx_ = level_dim(F.gx, level), dy_ = level_dim(F.gy, level),
               dz_ = level_dim(F.gz, level);
-    // 1) the 6 x 6 x 6 level-L cells around the group
+    // 1) the 4 x 4 x 4 level-L cells around the group
     for (int t = tid; t < NCELL; t += TT) {
       const int cx = bx + t % SIDE, cy = by + (t / SIDE) % SIDE, cz = bz + t / (SIDE * SIDE);
       u32 st = 0, ct = 0;
@@ -175,7 +175,7 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
       const float4 q = g.pts[qi];
       const u32 qidx = __float_as_uint(q.w);
       if (MODE == TILE_NORMALS && (qidx & kRemovedBit)) continue;
-      const int lx = (cell_axis(q.x, F.min_x, F.cell) >> sh) - bx;  // 1..4
+      const int lx = (cell_axis(q.x, F.min_x, F.cell) >> sh) - bx;  // 1..2
       const int ly = (cell_axis(q.y, F.min_y, F.cell) >> sh) - by;
       const int lz = (cell_axis(q.z, F.min_z, F.cell) >> sh) - bz;
       Key L[K];
@@ -345,7 +345,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
   const u64 n = list ? *n_list : *g.n_points;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const u64 nwarps = (u64)gridDim.x * WT_WARPS;
-  const int sh = 2 * level;
+  const int sh = level;
   Key kMax;
   if constexpr (FKEY) kMax = INFINITY;
   else kMax = ~0ull;
@@ -614,7 +614,7 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
   const u64 n = *n_list;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const u64 nwarps = (u64)gridDim.x * CP_WARPS;
-  const int sh = 2 * level;
+  const int sh = level;
   const int last = a.lane_levels > 0 && a.lane_levels < kGridLevels ? a.lane_levels - 1
                                                                      : kGridLevels - 1;
   for (u64 base = ((u64)blockIdx.x * CP_WARPS + wib) * 32; base < n; base += nwarps * 32) {
@@ -805,7 +805,7 @@ __global__ void k_knn_route(GridView g, const int32_t *frame_of, u32 min_own, ui
     int lv = kGridLevels - 1;
     for (int l = 0; l < kGridLevels - 1; ++l) {
       u32 st = 0, ct = 0;
-      const int s = 2 * l;
+      const int s = l;
       if (!lookup(g, level_key(g, F, l, cx >> s, cy >> s, cz >> s), st, ct)) ct = 0;
       if (ct >= min_own) {
         lv = l;
@@ -871,7 +871,8 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
                                                   a.open_list, a.open_n,
                                                   a.routed ? a.routed + level : nullptr);
       RVP_LAUNCH_CHECK(ctx);
-      u32 *st = stats ? stats + level : nullptr;  // certified at this level
+      // certified at this level (levels past 1 share the third counter)
+      u32 *st = stats ? stats + (level < 2 ? level : 2) : nullptr;
       if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
       if (mode == TILE_SOR_MEAN)
         k_knn_coop<K, TILE_SOR_MEAN><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
@@ -909,7 +910,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
         RVP_LAUNCH_CHECK(ctx);
         list = a.open_list;
       }
-      u32 *st = stats ? stats + level : nullptr;
+      u32 *st = stats ? stats + (level < 2 ? level : 2) : nullptr;
       if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
       if (mode == TILE_SOR_MEAN)
         k_knn_wt<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
@@ -936,7 +937,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
     return;
   }
   for (int level = 0; level < kGridLevels; ++level) {
-    u32 *st = stats ? stats + level : nullptr;
+    u32 *st = stats ? stats + (level < 2 ? level : 2) : nullptr;
     if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
     if (mode == TILE_SOR_MEAN)
       k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,

@@ -840,10 +840,12 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
     if (s->fitted_points != N || s->fitted_cell != cell_size) {
       // size the bucket table to the cells this batch occupies (it stays in
       // L2 instead of spanning 2.5 slots per point), then build again
-      u64 nb[4] = {0, 0, 0, 0};
-      RVP_CUDA_TRY(cudaMemcpyAsync(nb, s->grid.d_nbuckets, 32, cudaMemcpyDeviceToHost, st));
+      u64 nb[rvp::kHeadLevels] = {};
+      RVP_CUDA_TRY(cudaMemcpyAsync(nb, s->grid.d_nbuckets, 8 * rvp::kHeadLevels, cudaMemcpyDeviceToHost, st));
       RVP_CUDA_TRY(cudaStreamSynchronize(st));
-      s->grid.fit_table((size_t)((nb[0] + nb[1] + nb[2]) * 2));
+      size_t tot = 0;
+      for (int l = 0; l < rvp::kGridLevels; ++l) tot += (size_t)nb[l];
+      s->grid.fit_table(tot * 2);
       s->fitted_points = N;
       s->fitted_cell = cell_size;
       rvp::grid_build(ctx, s->grid, x, y, z, frame_offsets_dev, n_frames, N, cell_size,

@@ -31,7 +31,7 @@ struct rvp_pipeline {
   int max_frames = 0;
   float cell = 0.0f;
   float rfac = 0.9f;
-  int lane_levels = 0;  // grid levels of the per-lane kNN kernels (0: all)  // level-0 first-pass radius factor (tunable)
+  int lane_levels = 0;  // grid levels of the per-lane kNN kernels (0: all)
   rvp::VoxelWork vw;
   rvp::Grid grid;
   rvp::DevBuf in_x, in_y, in_z, in_offs;
@@ -488,12 +488,14 @@ rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p) {
   if (!p) return RVP_ERR_INVALID_ARG;
   return guard(p->ctx, [&] {
     RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
-    u64 nb[4] = {0, 0, 0, 0};
-    RVP_CUDA_TRY(cudaMemcpyAsync(nb, p->grid.d_nbuckets, 32, cudaMemcpyDeviceToHost,
+    u64 nb[rvp::kHeadLevels] = {};
+    RVP_CUDA_TRY(cudaMemcpyAsync(nb, p->grid.d_nbuckets, 8 * rvp::kHeadLevels, cudaMemcpyDeviceToHost,
                                  p->ctx->stream));
     RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
     // headroom for batches whose scenes occupy more cells than this one
-    p->grid.fit_table((size_t)((nb[0] + nb[1] + nb[2]) * 2));
+    size_t tot = 0;
+    for (int l = 0; l < rvp::kGridLevels; ++l) tot += (size_t)nb[l];
+    p->grid.fit_table(tot * 2);
   });
 }
 
@@ -579,7 +581,7 @@ rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac) {
 }
 
 rvp_status rvp_pipeline_set_lane_levels(rvp_pipeline *p, int levels) {
-  if (!p || levels < 0 || levels > 3) return RVP_ERR_INVALID_ARG;
+  if (!p || levels < 0 || levels > rvp::kGridLevels) return RVP_ERR_INVALID_ARG;
   p->lane_levels = levels;
   return RVP_OK;
 }
