@@ -199,7 +199,7 @@ def single_cloud_legs(ctx) -> dict:
         h = api.SpatialHash(ctx)
         h.setInputCloud(sc, 0.03)
         h.build()
-        api.normal_estimation_rvv(sc, h, 10, 0.03, ctx=ctx)
+        api.normal_estimation_rvv(sc, h, 10, 0.03)  # on the hash's context
         h.close()
         best, _ = api.ransac_plane_rvv(sc, 0.01, 1000, ctx=ctx)
         return len(v), len(s), best

@@ -694,6 +694,9 @@ class EuclideanClustering:
                                   ctx=self.ctx)
 
 
+GRID_LEVELS = 5  # RVP_GRID_LEVELS: neighbour-grid cells of c, 2c, 4c, 8c, 16c
+
+
 class Pipeline:
     """voxel -> SOR -> normals(k+1 NN) -> RANSAC over many frames at once."""
 
@@ -793,7 +796,7 @@ class Pipeline:
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)
 
-    GRID_LEVELS = 5  # RVP_GRID_LEVELS: cells of c, 2c, 4c, 8c, 16c
+    GRID_LEVELS = GRID_LEVELS
     LEVEL_KERNELS = tuple(f"{st}_knn_l{lv}" for st in ("sor", "normals")
                           for lv in range(GRID_LEVELS))
 

@@ -66,3 +66,13 @@ def test_api_fails_loudly_when_library_missing(tmp_path):
     with pytest.raises(OSError):
         C.CDLL(str(tmp_path / "nope.so"))
     assert os.path.exists(_lib.LIB_PATH)
+
+
+def test_python_front_end_imports():
+    """The host modules load without a device (their module-level code runs)."""
+    import importlib
+    for m in ("rvpoint_b200.api", "rvpoint_b200.learned", "rvpoint_b200.autotune",
+              "rvpoint_b200.sharding", "rvpoint_b200.datasets"):
+        importlib.import_module(m)
+    from rvpoint_b200 import api
+    assert len(api.Pipeline.LEVEL_KERNELS) == 2 * api.GRID_LEVELS
