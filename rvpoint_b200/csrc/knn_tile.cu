@@ -590,9 +590,8 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
 // busiest lane of every batch of 32. Every point with d2 <= tb lies in the
 // lane's tight window of sqrt(tb), inside its ring, and every cell that can
 // hold one is walked, so a lane that found K such points is exact. The
-// others (and warps whose queries span more than the table) stay open at
-// their level for the per-lane kernels' ring pass, or go to the
-// warp-per-query kernel when that level is past the per-lane levels.
+// others (and warps whose queries span more than the table) move up to the
+// next level's pass, and past the top level to the warp-per-query kernel.
 constexpr int CP_WARPS = TT / 32;
 constexpr int CP_BUF = 64;  // buffered candidates per lane
 constexpr size_t CP_SMEM = (size_t)CP_WARPS * (WT_CELLS * sizeof(uint2) + 32 * sizeof(float4) +
@@ -615,8 +614,6 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const u64 nwarps = (u64)gridDim.x * CP_WARPS;
   const int sh = level;
-  const int last = a.lane_levels > 0 && a.lane_levels < kGridLevels ? a.lane_levels - 1
-                                                                     : kGridLevels - 1;
   for (u64 base = ((u64)blockIdx.x * CP_WARPS + wib) * 32; base < n; base += nwarps * 32) {
     const bool active = base + lane < n;
     const u64 pos = active ? (u64)list[base + lane] : 0;
@@ -641,12 +638,12 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
     bx1 = min(bx1, GX - 1); by1 = min(by1, GY - 1); bz1 = min(bz1, GZ - 1);
     const int wx = bx1 - bx0 + 1, wy = by1 - by0 + 1, wz = bz1 - bz0 + 1;
     const bool use_tab = one_frame && wx > 0 && wy > 0 && wz > 0 && wx * wy * wz <= WT_CELLS;
-    // a query this pass cannot finish: the per-lane kernels' ring at its
-    // level, or the warp-per-query kernel past the per-lane levels
+    // a query this pass cannot finish: the next level's cooperative pass
+    // (its compaction comes after this kernel), or past the top level the
+    // warp-per-query kernel
     auto leave_open = [&]() {
-      if (level <= last) {
-        qlevel[pos] = (uint8_t)level;
-        qtau[pos] = -1.0f;
+      if (level + 1 < kGridLevels) {
+        qlevel[pos] = (uint8_t)(level + 1);
       } else {
         const u32 slot = atomicAdd(a.hard_count, 1u);
         a.hard[slot] = qidx & 0x7FFFFFFFu;
@@ -886,9 +883,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
       RVP_LAUNCH_CHECK(ctx);
       if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
     }
-    a.preset_open = true;
-    a.rfac = 0.0f;
-    a.level_events = nullptr;  // the per-lane kernels after it are not timed apart
+    return;  // nothing stays open: the top level's leftovers are in the hard list
   }
   if (!a.preset_open) RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
   if (a.level0_warp) {
