@@ -428,26 +428,28 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # kernels timed live for the roofline (CUDA events around each launch): the
 # SOR kNN kernel of each grid level and RANSAC
-LEVEL_STAGES = tuple(f"sor_knn_l{lv}" for lv in range(5))
+LEVEL_STAGES = ("sor_knn_l0", "sor_knn_l1", "sor_knn_l2", "sor_knn_coop")
 
 
 def kernel_name(stage: str, coop: bool) -> str:
     if stage == "ransac":
         return "k_ransac"
-    level = stage[-1]
-    return (f"k_knn_coop<17,SOR_LIST> grid level {level}" if coop
-            else f"k_knn_wt<17,SOR_LIST> grid level {level}")
+    if stage == "sor_knn_coop":
+        return "k_knn_coop<17,SOR_LIST> (cells of c)"
+    cells = {"sor_knn_l0": "c", "sor_knn_l1": "4c", "sor_knn_l2": "16c"}[stage]
+    return f"k_knn_wt<17,SOR_LIST> (cells of {cells})"
 
 
 def kernel_units(stage: str, coop: bool, routed, n_vox: int):
-    """Queries one launch of a SOR kNN kernel processes: with the
-    cooperative pass, the queries routed to its level; else every query at
-    level 0 (the coarser per-lane levels see only the ones left open, a
-    count the line does not carry, so they are not candidates)."""
-    level = int(stage[-1])
-    if coop:
-        return routed[level]
-    return n_vox if level == 0 else None
+    """Queries one launch of a SOR kNN kernel processes: the cooperative
+    pass, the queries it took; the per-lane kernel on cells of c, every query
+    without the cooperative pass (with it, and on the coarser cells, only the
+    ones left open, a count the line does not carry: not candidates)."""
+    if stage == "sor_knn_coop":
+        return routed if coop else None
+    if stage == "sor_knn_l0" and not coop:
+        return n_vox
+    return None
 
 
 def kernel_bytes(stage: str, units: int, n_sor: int, n_frames: int) -> float:
@@ -866,7 +868,7 @@ def main():
             "frac": achieved / peak, "traffic": traffic, "kernel": dom_name,
             "stage": dom, "peak_source": peak_src, "queries": cand[dom],
             "algorithmic_bytes_per_launch": alg, "launch_ms": stages[dom],
-            "routed_queries_per_level": routed}
+            "cooperative_queries": routed}
 
     cpu = singles = None
     if world == 1:

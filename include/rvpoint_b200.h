@@ -329,8 +329,9 @@ RVP_API rvp_status rvp_pipeline_check(rvp_pipeline *p);
 /* Grid levels of the batched neighbour grid: cells of edge c, 2c, 4c, 8c,
  * 16c (c = the pipeline's cell size). */
 #define RVP_GRID_LEVELS 5
-/* Queries of the SOR kNN the last run's cooperative pass routed to each
- * grid level (queries_per_warp 3; zeros otherwise). out[RVP_GRID_LEVELS]. */
+/* Queries of the SOR kNN the last run's cooperative pass took (points whose
+ * own cell holds at least ceil(rfac^2 k) points; queries_per_warp 3; 0
+ * otherwise). out[1]. */
 RVP_API rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out);
 /* Diagnostics: enable != 0 makes the kNN kernels count which search path
  * settled each query (out16[0..7] SOR, [8..15] normals: fine ring, fine
@@ -348,23 +349,24 @@ RVP_API rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_of
 RVP_API rvp_status rvp_pipeline_set_tuning(rvp_pipeline *p, float cell_size,
                                            int block_threads, int queries_per_warp);
 /* First-pass search radius of the kNN, as a factor of cell * sqrt(k /
- * points in the query's cell); with the cooperative kernels (queries_per_warp
- * 3) a query also goes to the finest grid level whose own cell holds at least
- * ceil(rfac^2 k) points (0 disables the first pass of the per-lane kernels;
- * results never depend on it, only the work does). */
+ * points in the query's cell); with the cooperative pass (queries_per_warp 3)
+ * it takes the queries whose own cell holds at least ceil(rfac^2 k) points
+ * (0 disables the first pass of the per-lane kernels; results never depend on
+ * it, only the work does). */
 RVP_API rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac);
-/* Grid levels (1 to RVP_GRID_LEVELS; 0 = all) whose kNN runs one query per lane; the
- * queries still open after them go to the warp-per-query kernel, which
- * spreads a query's candidates over the lanes. Results never depend on it. */
+/* Levels of the kNN chain (cells of c, 4c and 16c: 1 to 3; 0 = all 3) that
+ * run one query per lane; the queries still open after them go to the
+ * warp-per-query kernel, which spreads a query's candidates over the lanes.
+ * Results never depend on it. */
 RVP_API rvp_status rvp_pipeline_set_lane_levels(rvp_pipeline *p, int levels);
 /* Stage timing with CUDA events on the context's stream: the next max_runs
  * runs record 8 events each (stage boundaries: voxel, grid build, SOR kNN,
  * SOR statistics, normals kNN, normals, RANSAC), plus a pair around each
- * grid level's kNN kernel. rvp_pipeline_stage_times synchronizes and returns
- * the mean ms per stage over the recorded runs (ms[0..6]); with n_stages >= 13
- * also the mean ms of the kNN kernel of each grid level (ms[7..9] SOR levels
- * 0-2, ms[10..12] normals levels 0-2). It then resets. max_runs = 0 turns
- * timing off. */
+ * timed kNN kernel. rvp_pipeline_stage_times synchronizes and returns the
+ * mean ms per stage over the recorded runs (ms[0..6]); with n_stages >= 15
+ * also the mean ms of the timed kNN kernels (ms[7..10] SOR: the per-lane
+ * kernels on cells of c, 4c and 16c, then the cooperative pass; ms[11..14]
+ * the same for the normals). It then resets. max_runs = 0 turns timing off. */
 RVP_API rvp_status rvp_pipeline_set_timing(rvp_pipeline *p, int max_runs);
 RVP_API rvp_status rvp_pipeline_stage_times(rvp_pipeline *p, float *ms, int n_stages,
                                             int *runs);

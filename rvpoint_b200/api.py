@@ -695,6 +695,9 @@ class EuclideanClustering:
 
 
 GRID_LEVELS = 5  # RVP_GRID_LEVELS: neighbour-grid cells of c, 2c, 4c, 8c, 16c
+# kNN kernels timed per search stage: the per-lane kernels on cells of c, 4c
+# and 16c, and the cooperative pass
+TIMED_KNN = ("knn_l0", "knn_l1", "knn_l2", "knn_coop")
 
 
 class Pipeline:
@@ -754,7 +757,8 @@ class Pipeline:
         self.cfg.queries_per_warp = queries_per_warp
 
     def set_lane_levels(self, levels: int) -> None:
-        """Grid levels of the one-query-per-lane kNN kernels (0: all)."""
+        """Chain levels (cells of c, 4c, 16c) of the one-query-per-lane kNN
+        kernels, 1 to 3 (0: all)."""
         check(self.L.rvp_pipeline_set_lane_levels(self.h, int(levels)), self.ctx.h)
         self.lane_levels = int(levels)
 
@@ -786,19 +790,17 @@ class Pipeline:
         return {"sor": dict(zip(self.PATHS, map(int, out[:8]))),
                 "normals": dict(zip(self.PATHS, map(int, out[8:16])))}
 
-    def knn_routed(self) -> list:
-        """SOR kNN queries the last run's cooperative pass routed to each grid
-        level (zeros without it)."""
-        out = np.zeros(self.GRID_LEVELS, np.uint64)
+    def knn_routed(self) -> int:
+        """SOR kNN queries the last run's cooperative pass took (0 without it)."""
+        out = np.zeros(1, np.uint64)
         check(self.L.rvp_pipeline_knn_routed(self.h, _ptr(out)), self.ctx.h)
-        return [int(v) for v in out]
+        return int(out[0])
 
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)
 
     GRID_LEVELS = GRID_LEVELS
-    LEVEL_KERNELS = tuple(f"{st}_knn_l{lv}" for st in ("sor", "normals")
-                          for lv in range(GRID_LEVELS))
+    LEVEL_KERNELS = tuple(f"{st}_{k}" for st in ("sor", "normals") for k in TIMED_KNN)
 
     def stage_times(self, levels: bool = False) -> dict:
         """Mean ms per stage over the runs recorded since set_timing; with

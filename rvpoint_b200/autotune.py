@@ -40,7 +40,7 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
          cells: Optional[Iterable[float]] = None,
          blocks: Iterable[int] = (64, 128, 256),
          qpws: Iterable[int] = (0, 3), rfacs: Iterable[float] = (0.7, 0.85, 1.0),
-         lane_levels: Iterable[int] = (3, 4),
+         lane_levels: Iterable[int] = (3, 2),
          reps: int = 2,
          cache_file: Optional[str] = None, verbose: bool = False) -> Tuple[dict, list]:
     """Returns (best setting, all trials) and applies the best to `pipe`.

@@ -184,16 +184,19 @@ __global__ void k_cell_keys(const float *__restrict__ x, const float *__restrict
   }
 }
 
-// heads of level-L buckets: key >> 3L changes (dense mode: L = 0 ..
-// kHeadLevels - 1; the reference hash: L = 0 only)
-__global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int levels, u32 *heads) {
+// heads of the buckets of level base + j: key >> 3 (base + j) changes
+// (dense mode: j = 0 .. kHeadLevels - 1; the reference hash: base 0, j = 0)
+__global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int levels, int base,
+                        u32 *heads) {
   const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const u64 k = keys[i];
     const u64 p = i ? keys[i - 1] : 0;
-    for (int L = 0; L < levels; ++L)
-      heads[(size_t)L * n_max + i] = (i == 0 || (k >> (3 * L)) != (p >> (3 * L))) ? 1u : 0u;
+    for (int j = 0; j < levels; ++j) {
+      const int sh = 3 * (base + j);
+      heads[(size_t)j * n_max + i] = (i == 0 || (k >> sh) != (p >> sh)) ? 1u : 0u;
+    }
   }
 }
 
@@ -241,8 +244,8 @@ __device__ __forceinline__ void table_put(ulonglong2 *table, u64 mask, u64 key, 
 // one thread per bucket of levels 0 .. table_levels-1: {tagged key,
 // start | count << 32} into the open-addressing table (linear probing)
 __global__ void k_insert(const u64 *keys, const u32 *lstart, const u64 *bucket_of, size_t n_max,
-                         const u64 *n_dev, int levels, int table_levels, ulonglong2 *table,
-                         u64 mask, u64 *nbuckets, int *overflow) {
+                         const u64 *n_dev, int levels, int table_levels, int base,
+                         ulonglong2 *table, u64 mask, u64 *nbuckets, int *overflow) {
   const size_t n = n_dev ? *n_dev : n_max;
   u64 nb[kHeadLevels] = {};
   u64 tot = 0;
@@ -260,7 +263,8 @@ __global__ void k_insert(const u64 *keys, const u32 *lstart, const u64 *bucket_o
     const u32 *st = lstart + (size_t)L * n_max;
     const u32 s = st[c];
     const u32 e = (c + 1 < nb[L]) ? st[c + 1] : (u32)n;
-    const u64 key = L == 0 ? keys[s] : (((u64)L << 60) | (keys[s] >> (3 * L)));
+    const int La = base + L;  // the bucket's level
+    const u64 key = La == 0 ? keys[s] : (((u64)La << 60) | (keys[s] >> (3 * La)));
     table_put(table, mask, key, (u64)s | ((u64)(e - s) << 32), overflow);
   }
 }
@@ -344,13 +348,16 @@ GridView Grid::view(int mode, long long p1, long long p2) const {
   v.n_level = d_nbuckets;
   v.n_points = d_n;
   v.pos_of = b_pos.as<u32>();
+  v.lbase = lbase;
   return v;
 }
 
 void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const float *z,
                 const int64_t *offs, int n_frames, size_t n_points, float cell, int mode,
-                long long p1, long long p2, const u64 *n_dev_opt) {
+                long long p1, long long p2, const u64 *n_dev_opt, int base_level) {
   g.reserve(n_points, n_frames);
+  const int base = mode == KEY_DENSE ? base_level : 0;
+  g.lbase = base;
   cudaStream_t st = ctx->stream;
   const size_t n_max = n_points;
   const u64 *n_dev = n_dev_opt;
@@ -380,7 +387,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   RVP_LAUNCH_CHECK(ctx);
   k_bbox<<<gb, 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, bb);
   RVP_LAUNCH_CHECK(ctx);
-  k_grid_params<<<1, 1024, 0, st>>>(frames, bb, n_frames, cell);
+  // the sort cell: the query cell over 2^base (exact in float)
+  k_grid_params<<<1, 1024, 0, st>>>(frames, bb, n_frames, ldexpf(cell, -base));
   RVP_LAUNCH_CHECK(ctx);
   k_cell_keys<<<gb, 256, 0, st>>>(x, y, z, offs, n_frames, n_max, n_dev, frames, mode, p1, p2,
                                   g.b_keys.as<u64>(), g.b_vals.as<u32>());
@@ -388,7 +396,7 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   radix_sort_pairs(ctx, g.b_keys.as<u64>(), g.b_vals.as<u32>(), n_max, n_dev, t);
   // n for these kernels: the live count (n_dev) or n_max; strides: nm
   const u64 *n_live = n_dev ? n_dev : g.d_n;
-  k_heads<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), nm, n_live, levels, heads);
+  k_heads<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), nm, n_live, levels, base, heads);
   RVP_LAUNCH_CHECK(ctx);
   // bucket_of[L][i] = number of level-L heads before i (the bucket id of a head)
   for (int L = 0; L < levels; ++L)
@@ -402,7 +410,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
                                 g.b_pos.as<u32>());
   RVP_LAUNCH_CHECK(ctx);
   k_insert<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), lstart, bucket_of, nm, n_live, levels,
-                               table_levels, g.b_table.as<ulonglong2>(), (u64)g.table_cap - 1,
+                               table_levels, base, g.b_table.as<ulonglong2>(),
+                               (u64)g.table_cap - 1,
                                g.d_nbuckets, g.d_overflow);
   RVP_LAUNCH_CHECK(ctx);
 }
@@ -597,22 +606,22 @@ __global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int
       // 0) a known bound: every point with d2 <= tb lies in the tight window
       //    of sqrt(tb), and there are >= K of them -- scan it directly
       const float tb = q.bound ? q.bound[wi] : -1.0f;
-      Window wr = ring_window(F, qx, qy, qz, 1, 0);
-      int lvl = 0;
+      Window wr = ring_window(F, qx, qy, qz, 1, g.lbase);
+      int lvl = g.lbase;
       if (tb >= 0.0f) {
         found = 0;
       } else {
         // 1) rings of +- 1 cell, coarser (x4) while they hold fewer than K
         knn_scan<P>(g, F, f, wr, false, qx, qy, qz, K, ~0ull - 1, L, found);
       }
-      while (tb < 0.0f && found < (u32)K && two_level && lvl + 1 < kGridLevels) {
+      while (tb < 0.0f && found < (u32)K && two_level && lvl + 1 < g.lbase + kGridLevels) {
         ++lvl;
         wr = ring_window(F, qx, qy, qz, 1, lvl);
         L.init();
         found = 0;
         knn_scan<P>(g, F, f, wr, false, qx, qy, qz, K, ~0ull - 1, L, found);
       }
-      path = lvl == 0 ? 0 : (lvl == 1 ? 2 : 3);
+      path = lvl == g.lbase ? 0 : (lvl == g.lbase + 1 ? 2 : 3);
       bool done = false;
       if (found >= (u32)K || tb >= 0.0f) {
         const float tau = tb >= 0.0f ? tb : nbr_d2(L.get(K - 1));
@@ -625,8 +634,8 @@ __global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int
           //    sqrt(tau) and there are >= K of them: exact. Scan it at the
           //    finest level whose window stays small.
           const double rt = sqrt((double)tau);
-          const int top = two_level ? kGridLevels - 1 : 0;
-          for (int lt = 0; lt <= top && !done; ++lt) {
+          const int top = two_level ? g.lbase + kGridLevels - 1 : 0;
+          for (int lt = two_level ? g.lbase : 0; lt <= top && !done; ++lt) {
             const Window wt = tight_window(F, qx, qy, qz, rt, lt);
             const long long cells = window_cells(wt);
             if (cells <= (two_level ? (lt == top ? 512 : 125) : 4096)) {

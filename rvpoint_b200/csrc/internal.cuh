@@ -190,6 +190,14 @@ enum KeyMode { KEY_REF_HASH = 0, KEY_DENSE = 1 };
 // (c .. 16c), and the run starts of one level more are kept (kHeadLevels).
 constexpr int kGridLevels = RVP_GRID_LEVELS;
 constexpr int kHeadLevels = kGridLevels + 1;
+// The neighbour searches of a batch run on three levels 4x apart (cells of
+// c, 4c, 16c: table levels lbase, lbase + 2, lbase + 4), one query per
+// lane on each in turn; a grid may be sorted finer than its query cell
+// (lbase > 0) so that consecutive points lie close together inside a cell.
+constexpr int kChainLevels = 3;
+constexpr int kChainStep = 2;
+// timed kernels per search stage: the three chain levels and the cooperative pass
+constexpr int kTimedKernels = kChainLevels + 1;
 
 struct GridView {  // what the query kernels read
   const float4 *pts;       // cell-sorted {x,y,z,idx}
@@ -203,6 +211,7 @@ struct GridView {  // what the query kernels read
   const u64 *n_level;      // dense mode: number of level-L buckets (device, [4])
   const u64 *n_points;     // number of grid points (device; set by grid_build)
   const u32 *pos_of;       // sorted position of each point (by original index)
+  int lbase;               // dense mode: the finest table level (query cell = fine cell << lbase)
 };
 
 struct Grid {
@@ -210,6 +219,7 @@ struct Grid {
   size_t n_max = 0;
   size_t table_cap = 0;
   size_t table_cap_req = 0;    // 0: sized from n_max
+  int lbase = 0;               // see GridView::lbase
   DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_lstart, b_pos;
   u64 *d_n = nullptr;          // number of points (device)
   u64 *d_nbuckets = nullptr;   // buckets per level [kHeadLevels] (device)
@@ -225,10 +235,13 @@ struct Grid {
 // Build a grid over frames of SoA points. frame_offsets_dev: n_frames+1
 // int64 on the device. cell: cell size (same for all frames). Mode 0 uses the
 // reference's bbox/eps/grid formulas and prime hash (single frame).
+// base_level (dense mode): the points are sorted by cells of cell / 2^base
+// and the table holds levels base .. base + kGridLevels - 1 (cells of cell,
+// 2 cell, ...).
 void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y,
                 const float *z, const int64_t *frame_offsets_dev, int n_frames,
                 size_t n_points, float cell, int mode, long long p1,
-                long long p2, const u64 *n_dev_opt);
+                long long p2, const u64 *n_dev_opt, int base_level = 0);
 
 // Query helpers (queries are SoA; query q belongs to frame qframe(q)).
 struct QuerySet {
@@ -301,11 +314,11 @@ struct TileArgs {
   u64 *open_n;              // device count of open_list
   void *scan_tmp;           // scan_temp_bytes(n_max)
   size_t n_max;             // size of qlevel / qtau
-  cudaEvent_t *level_events;  // null, or 2 per grid level: around each level's kNN kernel
+  cudaEvent_t *level_events;  // null, or 2 per timed kernel (chain levels, cooperative pass)
   bool preset_open;         // qlevel already holds 0 (open) / 0xFF (done) per grid point
-  int lane_levels;          // grid levels of the per-lane kernels (0: all)
+  int lane_levels;          // chain levels of the per-lane kernels (1..kChainLevels; 0: all)
   int coop;                 // cooperative passes (k_knn_coop) before the per-lane kernels
-  u64 *routed;              // optional, [kGridLevels]: queries the cooperative pass routed to each level
+  u64 *routed;              // optional: queries the cooperative pass took
 };
 // false if k has no tile instantiation (use grid_knn then)
 // Normals of the kept points whose SOR neighbour list (TILE_SOR_LIST, ks per

@@ -88,8 +88,9 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
   __shared__ int s_base[4];
   __shared__ int s_staged;
   __shared__ GridFrame s_F;
-  const u64 ngroups = g.n_level[level + 1];
-  const u32 *gstart = g.lstart[level + 1];
+  // groups: the buckets one binary level up
+  const u64 ngroups = g.n_level[level - g.lbase + 1];
+  const u32 *gstart = g.lstart[level - g.lbase + 1];
   const u64 n = *g.n_points;
   const int tid = threadIdx.x;
   const int sh = level;  // level-L cell = fine index >> sh
@@ -99,7 +100,7 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
   for (u64 cb = blockIdx.x; cb < ngroups; cb += gridDim.x) {
     const u32 qs = gstart[cb];
     const u32 qe = (cb + 1 < ngroups) ? gstart[cb + 1] : (u32)n;
-    if (level > 0) {  // only the queries the previous level left open
+    if (level > g.lbase) {  // only the queries the previous level left open
       int any = 0;
       for (u32 base = qs; base < qe; base += TT) {
         const u32 i = base + tid;
@@ -171,7 +172,7 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
     __syncthreads();
     // 3) one thread per open query of this group
     for (u32 qi = qs + tid; qi < qe; qi += TT) {
-      if (level > 0 && qlevel[qi] != level) continue;
+      if (level > g.lbase && qlevel[qi] != level) continue;
       const float4 q = g.pts[qi];
       const u32 qidx = __float_as_uint(q.w);
       if (MODE == TILE_NORMALS && (qidx & kRemovedBit)) continue;
@@ -250,12 +251,13 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
       // K points found), or at level 0 a radius estimated from the own
       // cell's occupancy (surface density), kept under one cell.
       float tb = -1.0f;
-      if (level > 0) {
+      if (level > g.lbase) {
         tb = qtau[qi];
       } else if (a.rfac > 0.0f) {
         const u32 n_own = c_count[(lz * SIDE + ly) * SIDE + lx];
-        const float r = fminf(a.rfac * F.cell * sqrtf((float)K / (float)max(n_own, 1u)),
-                              0.999f * F.cell);
+        const float csb = F.cell * (float)(1 << sh);
+        const float r = fminf(a.rfac * csb * sqrtf((float)K / (float)max(n_own, 1u)),
+                              0.999f * csb);
         tb = r * r;
       }
       bool ok = false;
@@ -282,8 +284,8 @@ __global__ __launch_bounds__(TT, MODE == TILE_SOR_MEAN ? 4 : 3) void k_knn_tile(
         }
       }
       if (!ok) {
-        if (level + 1 < kGridLevels) {
-          qlevel[qi] = (uint8_t)(level + 1);
+        if (level + kChainStep < g.lbase + kChainStep * kChainLevels) {
+          qlevel[qi] = (uint8_t)(level + kChainStep);
           qtau[qi] = tau;
         } else {
           const u32 slot = atomicAdd(a.hard_count, 1u);
@@ -470,13 +472,14 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
       // first pass with a bound: the level below's tau, or at level 0 a
       // radius from the own cell's occupancy (kept under one cell)
       float tb = -1.0f;
-      if (level > 0) {
+      if (level > g.lbase) {
         tb = qtau[pos];
       } else if (a.rfac > 0.0f) {
         u32 st0, n_own;
         cell_run(cx, cy, cz, st0, n_own);
-        const float r = fminf(a.rfac * F.cell * sqrtf((float)K / (float)max(n_own, 1u)),
-                              0.999f * F.cell);
+        const float csb = F.cell * (float)(1 << sh);
+        const float r = fminf(a.rfac * csb * sqrtf((float)K / (float)max(n_own, 1u)),
+                              0.999f * csb);
         tb = r * r;
       }
       bool ok = false;
@@ -507,11 +510,12 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
         // points than that window
         // lane_levels: the levels run by these per-lane kernels; past
         // them the warp kernel (lanes over candidates) takes the query
-        const int last = a.lane_levels > 0 && a.lane_levels < kGridLevels ? a.lane_levels - 1
-                                                                           : kGridLevels - 1;
-        const bool to_warp = level + 1 == last && tau >= 0.0f && a.hard_tau;
+        const int nlev = a.lane_levels > 0 && a.lane_levels < kChainLevels ? a.lane_levels
+                                                                            : kChainLevels;
+        const int last = g.lbase + kChainStep * (nlev - 1);
+        const bool to_warp = level + kChainStep == last && tau >= 0.0f && a.hard_tau;
         if (level < last && !to_warp) {
-          qlevel[pos] = (uint8_t)(level + 1);
+          qlevel[pos] = (uint8_t)(level + kChainStep);
           qtau[pos] = tau;
         } else {
           const u32 slot = atomicAdd(a.hard_count, 1u);
@@ -571,27 +575,27 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
   }
 }
 
-// Cooperative kNN over routed queries. Every grid point is first routed to
-// the finest grid level whose own cell holds at least `min_own` points
-// (k_knn_route), so that a radius from that cell's occupancy is likely to
-// hold K points inside the cell's 27-cell ring. Per level, one warp takes 32
-// consecutive routed queries (a compacted list in grid order, so they lie
-// close together), looks up the union of their rings once (per-warp table,
-// as in k_knn_wt), and every lane takes the bound tb = r^2 with
-// r = rfac * cell * sqrt(K / own-cell count), under one cell. The warp walks
-// only the cells some lane can still use (box distance below that lane's
-// min(tb, K-th key)): 32 candidates of such a cell go up coalesced into a
-// per-warp staging row and every lane tests all of them against its query
-// (broadcast shared-memory reads, all lanes converged). A candidate within
-// tb (and not beyond the lane's K-th key) goes, as its grid position, into
-// the lane's buffer in shared memory; the buffers are merged into the lanes'
-// register lists (insertion network) when one of them fills and at the
-// end, so the warp pays for each lane's insertions once, not for the
-// busiest lane of every batch of 32. Every point with d2 <= tb lies in the
-// lane's tight window of sqrt(tb), inside its ring, and every cell that can
-// hold one is walked, so a lane that found K such points is exact. The
-// others (and warps whose queries span more than the table) move up to the
-// next level's pass, and past the top level to the warp-per-query kernel.
+// Cooperative kNN at the finest chain level. Every grid point whose own
+// cell holds at least `min_own` points is picked (k_knn_route): in such
+// dense cells a radius from the occupancy is likely to hold K points inside
+// the cell's 27-cell ring. One warp takes 32 consecutive picked queries (a
+// compacted list in grid order, so they lie close together), looks up the
+// union of their rings once (per-warp table, as in k_knn_wt), and every
+// lane takes the bound tb = r^2 with r = rfac * cell * sqrt(K / own-cell
+// count), under one cell. The warp walks only the cells some lane can still
+// use (box distance below that lane's min(tb, K-th key)): 32 candidates of
+// such a cell go up coalesced into a per-warp staging row and every lane
+// tests all of them against its query (broadcast shared-memory reads, all
+// lanes converged). A candidate within tb (and not beyond the lane's K-th
+// key) goes, as its grid position, into the lane's buffer in shared memory;
+// the buffers are merged into the lanes' register lists (insertion network)
+// when one of them fills and at the end, so the warp pays for each lane's
+// insertions once, not for the busiest lane of every batch of 32. Every
+// point with d2 <= tb lies in the lane's tight window of sqrt(tb), inside
+// its ring, and every cell that can hold one is walked, so a lane that found
+// K such points is exact. The others (and warps whose queries span more
+// than the table) stay open for the per-lane kernels, like the queries that
+// were not picked.
 constexpr int CP_WARPS = TT / 32;
 constexpr int CP_BUF = 64;  // buffered candidates per lane
 constexpr size_t CP_SMEM = (size_t)CP_WARPS * (WT_CELLS * sizeof(uint2) + 32 * sizeof(float4) +
@@ -638,18 +642,9 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
     bx1 = min(bx1, GX - 1); by1 = min(by1, GY - 1); bz1 = min(bz1, GZ - 1);
     const int wx = bx1 - bx0 + 1, wy = by1 - by0 + 1, wz = bz1 - bz0 + 1;
     const bool use_tab = one_frame && wx > 0 && wy > 0 && wz > 0 && wx * wy * wz <= WT_CELLS;
-    // a query this pass cannot finish: the next level's cooperative pass
-    // (its compaction comes after this kernel), or past the top level the
-    // warp-per-query kernel
-    auto leave_open = [&]() {
-      if (level + 1 < kGridLevels) {
-        qlevel[pos] = (uint8_t)(level + 1);
-      } else {
-        const u32 slot = atomicAdd(a.hard_count, 1u);
-        a.hard[slot] = qidx & 0x7FFFFFFFu;
-        if (a.hard_tau) a.hard_tau[slot] = -1.0f;
-      }
-    };
+    // a query this pass cannot finish: open at this level for the
+    // per-lane kernels' ring
+    auto leave_open = [&]() { qlevel[pos] = (uint8_t)level; };
     if (!use_tab) {
       if (active) leave_open();
       continue;
@@ -788,28 +783,23 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
   }
 }
 
-// the finest grid level whose own cell holds at least min_own points (the
-// top level otherwise), per grid point
+// the cooperative pass takes the grid points whose own cell (chain level
+// lbase) holds at least min_own points (qlevel = kCoopMark); the others are
+// open for the per-lane kernels at that level
+constexpr uint8_t kCoopMark = 0xFE;
 __global__ void k_knn_route(GridView g, const int32_t *frame_of, u32 min_own, uint8_t *qlevel) {
   const u64 n = *g.n_points;
+  const int lb = g.lbase;
   for (u64 pos = blockIdx.x * (u64)blockDim.x + threadIdx.x; pos < n;
        pos += (u64)gridDim.x * blockDim.x) {
     const float4 q = g.pts[pos];
     const u32 qidx = __float_as_uint(q.w) & 0x7FFFFFFFu;
     const GridFrame F = g.frames[frame_of ? frame_of[qidx] : 0];
-    const int cx = cell_axis(q.x, F.min_x, F.cell), cy = cell_axis(q.y, F.min_y, F.cell),
-              cz = cell_axis(q.z, F.min_z, F.cell);
-    int lv = kGridLevels - 1;
-    for (int l = 0; l < kGridLevels - 1; ++l) {
-      u32 st = 0, ct = 0;
-      const int s = l;
-      if (!lookup(g, level_key(g, F, l, cx >> s, cy >> s, cz >> s), st, ct)) ct = 0;
-      if (ct >= min_own) {
-        lv = l;
-        break;
-      }
-    }
-    qlevel[pos] = (uint8_t)lv;
+    const int cx = cell_axis(q.x, F.min_x, F.cell) >> lb, cy = cell_axis(q.y, F.min_y, F.cell) >> lb,
+              cz = cell_axis(q.z, F.min_z, F.cell) >> lb;
+    u32 st = 0, ct = 0;
+    if (!lookup(g, level_key(g, F, lb, cx, cy, cz), st, ct)) ct = 0;
+    qlevel[pos] = ct >= min_own ? kCoopMark : (uint8_t)lb;
   }
 }
 
@@ -834,10 +824,10 @@ template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_in, int blocks,
               uint8_t *qlevel, u32 *stats) {
   TileArgs a = a_in;
-  // cooperative passes first (float-key modes over every grid point): each
-  // point is routed to a level and the warps of each level work on their
-  // queries together; the per-lane kernels then take what stays open, from
-  // their ring pass on (no second bounded pass at level 0)
+  // the cooperative pass first (float-key modes over every grid point): the
+  // points of dense cells, the warps working on 32 queries together; the
+  // per-lane kernels then take what stays open, from their ring pass on (no
+  // second bounded pass at the first chain level)
   const bool coop = a.coop && a.level0_warp && !a.preset_open &&
                     (mode == TILE_SOR_MEAN || mode == TILE_SOR_LIST || mode == TILE_PAIRS_F);
   if (coop) {
@@ -859,43 +849,47 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
     const u32 min_own = (u32)ceilf(rf * rf * (float)K / 0.998f);
     k_knn_route<<<gb, 256, 0, ctx->stream>>>(g, a.frame_of, min_own, qlevel);
     RVP_LAUNCH_CHECK(ctx);
+    k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, kCoopMark, a.open_flags);
+    RVP_LAUNCH_CHECK(ctx);
+    exclusive_scan_u32_to_u64(ctx, a.open_flags, a.open_pos, a.n_max, g.n_points, a.scan_tmp);
+    k_open_scatter<<<gb, 256, 0, ctx->stream>>>(a.open_flags, a.open_pos, g.n_points,
+                                                a.open_list, a.open_n, a.routed);
+    RVP_LAUNCH_CHECK(ctx);
+    cudaEvent_t *ev = a.level_events ? a.level_events + 2 * kChainLevels : nullptr;
+    if (ev) cudaEventRecord(ev[0], ctx->stream);
     const int cblocks = ctx->num_sms * 2;
-    for (int level = 0; level < kGridLevels; ++level) {
-      k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, level, a.open_flags);
-      RVP_LAUNCH_CHECK(ctx);
-      exclusive_scan_u32_to_u64(ctx, a.open_flags, a.open_pos, a.n_max, g.n_points, a.scan_tmp);
-      k_open_scatter<<<gb, 256, 0, ctx->stream>>>(a.open_flags, a.open_pos, g.n_points,
-                                                  a.open_list, a.open_n,
-                                                  a.routed ? a.routed + level : nullptr);
-      RVP_LAUNCH_CHECK(ctx);
-      // certified at this level (levels past 1 share the third counter)
-      u32 *st = stats ? stats + (level < 2 ? level : 2) : nullptr;
-      if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
-      if (mode == TILE_SOR_MEAN)
-        k_knn_coop<K, TILE_SOR_MEAN><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
-            g, a, level, a.open_list, a.open_n, qlevel, a.qtau, st);
-      else if (mode == TILE_SOR_LIST)
-        k_knn_coop<K, TILE_SOR_LIST><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
-            g, a, level, a.open_list, a.open_n, qlevel, a.qtau, st);
-      else
-        k_knn_coop<K, TILE_PAIRS_F><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
-            g, a, level, a.open_list, a.open_n, qlevel, a.qtau, st);
-      RVP_LAUNCH_CHECK(ctx);
-      if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
-    }
-    return;  // nothing stays open: the top level's leftovers are in the hard list
+    if (mode == TILE_SOR_MEAN)
+      k_knn_coop<K, TILE_SOR_MEAN><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
+          g, a, g.lbase, a.open_list, a.open_n, qlevel, a.qtau, stats);
+    else if (mode == TILE_SOR_LIST)
+      k_knn_coop<K, TILE_SOR_LIST><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
+          g, a, g.lbase, a.open_list, a.open_n, qlevel, a.qtau, stats);
+    else
+      k_knn_coop<K, TILE_PAIRS_F><<<cblocks, TT, CP_SMEM, ctx->stream>>>(
+          g, a, g.lbase, a.open_list, a.open_n, qlevel, a.qtau, stats);
+    RVP_LAUNCH_CHECK(ctx);
+    if (ev) cudaEventRecord(ev[1], ctx->stream);
+    // the per-lane kernels take what is open, from the ring pass on
+    a.preset_open = true;
+    a.rfac = 0.0f;
+  } else if (a.level_events) {
+    // no cooperative pass: a zero-length pair in its slot
+    cudaEventRecord(a.level_events[2 * kChainLevels], ctx->stream);
+    cudaEventRecord(a.level_events[2 * kChainLevels + 1], ctx->stream);
   }
-  if (!a.preset_open) RVP_CUDA_TRY(cudaMemsetAsync(qlevel, 0, a.n_max, ctx->stream));
+  if (!a.preset_open)
+    RVP_CUDA_TRY(cudaMemsetAsync(qlevel, (uint8_t)g.lbase, a.n_max, ctx->stream));
+  const int nlev = a.lane_levels > 0 && a.lane_levels < kChainLevels ? a.lane_levels
+                                                                      : kChainLevels;
   if (a.level0_warp) {
-    // barrier-free per-warp kernels at every level; levels > 0 (and level 0
-    // when the caller marked the open queries) read the compacted list of
-    // open queries
+    // barrier-free per-warp kernels at every chain level; the levels past
+    // the first (and the first when the caller marked the open queries)
+    // read the compacted list of open queries
     const int wblocks = ctx->num_sms * 3 * 4;
-    const int levels = a.lane_levels > 0 && a.lane_levels < kGridLevels ? a.lane_levels
-                                                                        : kGridLevels;
-    for (int level = 0; level < levels; ++level) {
+    for (int j = 0; j < nlev; ++j) {
+      const int level = g.lbase + kChainStep * j;
       const u32 *list = nullptr;
-      if (level > 0 || a.preset_open) {
+      if (j > 0 || a.preset_open) {
         const unsigned gb = grid_for(a.n_max, 256, ctx->num_sms * 16);
         k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, level, a.open_flags);
         RVP_LAUNCH_CHECK(ctx);
@@ -905,8 +899,8 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
         RVP_LAUNCH_CHECK(ctx);
         list = a.open_list;
       }
-      u32 *st = stats ? stats + (level < 2 ? level : 2) : nullptr;
-      if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
+      u32 *st = stats ? stats + j : nullptr;
+      if (a.level_events) cudaEventRecord(a.level_events[2 * j], ctx->stream);
       if (mode == TILE_SOR_MEAN)
         k_knn_wt<K, TILE_SOR_MEAN><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                     qlevel, a.qtau, st);
@@ -923,17 +917,18 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
         k_knn_wt<K, TILE_PAIRS><<<wblocks, TT, 0, ctx->stream>>>(g, a, level, list, a.open_n,
                                                                  qlevel, a.qtau, st);
       RVP_LAUNCH_CHECK(ctx);
-      if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
+      if (a.level_events) cudaEventRecord(a.level_events[2 * j + 1], ctx->stream);
     }
-    for (int level = levels; level < kGridLevels && a.level_events; ++level) {
-      cudaEventRecord(a.level_events[2 * level], ctx->stream);  // not run: zero length
-      cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
+    for (int j = nlev; j < kChainLevels && a.level_events; ++j) {
+      cudaEventRecord(a.level_events[2 * j], ctx->stream);  // not run: zero length
+      cudaEventRecord(a.level_events[2 * j + 1], ctx->stream);
     }
     return;
   }
-  for (int level = 0; level < kGridLevels; ++level) {
-    u32 *st = stats ? stats + (level < 2 ? level : 2) : nullptr;
-    if (a.level_events) cudaEventRecord(a.level_events[2 * level], ctx->stream);
+  for (int j = 0; j < kChainLevels; ++j) {
+    const int level = g.lbase + kChainStep * j;
+    u32 *st = stats ? stats + j : nullptr;
+    if (a.level_events) cudaEventRecord(a.level_events[2 * j], ctx->stream);
     if (mode == TILE_SOR_MEAN)
       k_knn_tile<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau,
                                                                    st);
@@ -946,7 +941,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
     else
       k_knn_tile<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, level, qlevel, a.qtau, st);
     RVP_LAUNCH_CHECK(ctx);
-    if (a.level_events) cudaEventRecord(a.level_events[2 * level + 1], ctx->stream);
+    if (a.level_events) cudaEventRecord(a.level_events[2 * j + 1], ctx->stream);
   }
 }
 }  // namespace
@@ -986,7 +981,7 @@ __global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs 
       pz[t] = p.z;
     }
     if (!ok) {
-      a.qlevel[pos] = 0;
+      a.qlevel[pos] = (uint8_t)g.lbase;  // open at the first chain level
       continue;
     }
     a.qlevel[pos] = 0xFF;

@@ -31,7 +31,8 @@ struct rvp_pipeline {
   int max_frames = 0;
   float cell = 0.0f;
   float rfac = 0.9f;
-  int lane_levels = 0;  // grid levels of the per-lane kNN kernels (0: all)
+  int lane_levels = 0;  // chain levels of the per-lane kNN kernels (0: all)
+  int grid_base = 2;    // the grid is sorted by cells of cell / 2^grid_base
   rvp::VoxelWork vw;
   rvp::Grid grid;
   rvp::DevBuf in_x, in_y, in_z, in_offs;
@@ -66,7 +67,7 @@ struct rvp_pipeline {
   // (stage boundaries, then a pair around each grid level's kNN kernel: SOR
   // levels 0-2, normals levels 0-2)
   static constexpr int kStages = 7;
-  static constexpr int kLevelKernels = 2 * rvp::kGridLevels;
+  static constexpr int kLevelKernels = 2 * rvp::kTimedKernels;
   static constexpr int kEventsPerRun = kStages + 1 + 2 * kLevelKernels;
   std::vector<cudaEvent_t> events;  // runs_cap * kEventsPerRun
   int runs_cap = 0, runs_recorded = 0;
@@ -82,12 +83,12 @@ struct rvp_pipeline {
   cudaEvent_t *level_events(int first) {
     if (capturing || runs_cap == 0 || runs_recorded >= runs_cap) return nullptr;
     return &events[(size_t)runs_recorded * kEventsPerRun + kStages + 1 +
-                   first * 2 * rvp::kGridLevels];
+                   first * 2 * rvp::kTimedKernels];
   }
   // a run whose kNN skipped the per-level kernels records zero-length pairs
   void empty_level_events(cudaEvent_t *ev) {
     if (ev)
-      for (int j = 0; j < 2 * rvp::kGridLevels; ++j) cudaEventRecord(ev[j], ctx->stream);
+      for (int j = 0; j < 2 * rvp::kTimedKernels; ++j) cudaEventRecord(ev[j], ctx->stream);
   }
 };
 
@@ -284,10 +285,12 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
                         p->vox_y.as<float>(), p->vox_z.as<float>());
     p->mark(1);
     if (p->record_stages) RVP_CUDA_TRY(cudaEventRecord(p->ev_stage[0], st));
-    // 2) grid over the voxel points of every frame
+    // 2) grid over the voxel points of every frame: cells of `cell` for the
+    //    searches, the points sorted by cells of cell / 4 inside them (so
+    //    that consecutive points, a warp's queries, lie close together)
     rvp::grid_build(ctx, p->grid, p->vox_x.as<float>(), p->vox_y.as<float>(),
                     p->vox_z.as<float>(), vox_offs, n_frames, N, p->cell, rvp::KEY_DENSE, 0, 0,
-                    n_vox);
+                    n_vox, p->grid_base);
     k_frame_ids<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(vox_offs, n_frames, N,
                                                                  p->vox_frame.as<int32_t>());
     RVP_LAUNCH_CHECK(ctx);
@@ -314,7 +317,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles instead
     ta.coop = c.queries_per_warp == 3;         // 3: cooperative passes first
     ta.routed = p->routed.as<u64>();
-    if (ta.coop) RVP_CUDA_TRY(cudaMemsetAsync(ta.routed, 0, 8 * rvp::kGridLevels, st));
+    if (ta.coop) RVP_CUDA_TRY(cudaMemsetAsync(ta.routed, 0, 8, st));
     {
       char *op = p->open.as<char>();
       auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -536,11 +539,11 @@ rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out) {
   return guard(p->ctx, [&] {
     RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
     if (!p->routed.ptr) {
-      for (int l = 0; l < rvp::kGridLevels; ++l) out[l] = 0;
+      *out = 0;
       return;
     }
-    RVP_CUDA_TRY(cudaMemcpyAsync(out, p->routed.ptr, 8 * rvp::kGridLevels,
-                                 cudaMemcpyDeviceToHost, p->ctx->stream));
+    RVP_CUDA_TRY(cudaMemcpyAsync(out, p->routed.ptr, 8, cudaMemcpyDeviceToHost,
+                                 p->ctx->stream));
     RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
   });
 }
@@ -581,7 +584,7 @@ rvp_status rvp_pipeline_set_search_radius_factor(rvp_pipeline *p, float rfac) {
 }
 
 rvp_status rvp_pipeline_set_lane_levels(rvp_pipeline *p, int levels) {
-  if (!p || levels < 0 || levels > rvp::kGridLevels) return RVP_ERR_INVALID_ARG;
+  if (!p || levels < 0 || levels > rvp::kChainLevels) return RVP_ERR_INVALID_ARG;
   p->lane_levels = levels;
   return RVP_OK;
 }

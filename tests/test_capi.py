@@ -75,4 +75,4 @@ def test_python_front_end_imports():
               "rvpoint_b200.sharding", "rvpoint_b200.datasets"):
         importlib.import_module(m)
     from rvpoint_b200 import api
-    assert len(api.Pipeline.LEVEL_KERNELS) == 2 * api.GRID_LEVELS
+    assert len(api.Pipeline.LEVEL_KERNELS) == 2 * len(api.TIMED_KNN)

@@ -458,8 +458,9 @@ def test_pipeline_level_kernel_times(gpu_ctx):
     t = p.stage_times(levels=True)
     assert t["runs"] == 2
     assert t["sor_knn_l0"] > 0 and t["normals_knn_l0"] > 0
-    assert sum(t[f"sor_knn_l{lv}"] for lv in range(5)) <= t["sor_knn"] * 1.001
-    assert (sum(t[f"normals_knn_l{lv}"] for lv in range(5))
+    timed = ("knn_l0", "knn_l1", "knn_l2", "knn_coop")
+    assert sum(t[f"sor_{k}"] for k in timed) <= t["sor_knn"] * 1.001
+    assert (sum(t[f"normals_{k}"] for k in timed)
             <= t["normals_knn"] * 1.001)
 
 
