@@ -334,10 +334,12 @@ RVP_API rvp_status rvp_pipeline_check(rvp_pipeline *p);
  * otherwise). out[1]. */
 RVP_API rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out);
 /* Diagnostics: enable != 0 makes the kNN kernels count which search path
- * settled each query (out16[0..7] SOR, [8..15] normals: fine ring, fine
- * tight window, coarse ring, coarse tight window, whole frame, bounded).
- * Reads (if out16) and clears the counters. */
-RVP_API rvp_status rvp_pipeline_knn_stats(rvp_pipeline *p, int enable, uint32_t *out16);
+ * settled each query: out20[0..7] SOR, [8..15] normals (warp-per-query
+ * kernel: first-level ring, tight window of a bound, second-level ring,
+ * coarser ring, whole frame; per-lane chain levels 1, 2, 3), [16] SOR and
+ * [17] normals settled by the per-thread tight window of a handed-on bound,
+ * [18..19] reserved. Reads (if out20) and clears the counters. */
+RVP_API rvp_status rvp_pipeline_knn_stats(rvp_pipeline *p, int enable, uint32_t *out20);
 /* Host copies of the per-frame voxel and SOR offsets of the last run
  * (n_frames+1 int64 each; either may be NULL). Synchronizes the stream. */
 RVP_API rvp_status rvp_pipeline_frame_offsets(rvp_pipeline *p, int64_t *voxel_offsets,

@@ -780,15 +780,16 @@ class Pipeline:
         check(self.L.rvp_pipeline_check(self.h), self.ctx.h)
 
     # warp kernel: ring at level 0 / tight window / ring at level 1 / ring at
-    # level 2 / whole frame; tile kernel: certified at level 0 / 1 / 2
+    # level 2 / whole frame; tile kernel: certified at level 0 / 1 / 2; plus
+    # "tau_window": the per-thread tight window of a handed-on bound
     PATHS = ("warp_ring0", "warp_tight", "warp_ring1", "warp_ring2", "warp_whole_frame",
              "tile_l0", "tile_l1", "tile_l2")
 
     def knn_stats(self, enable: bool = True) -> dict:
-        out = np.zeros(16, np.uint32)
+        out = np.zeros(20, np.uint32)
         check(self.L.rvp_pipeline_knn_stats(self.h, int(enable), _ptr(out)), self.ctx.h)
-        return {"sor": dict(zip(self.PATHS, map(int, out[:8]))),
-                "normals": dict(zip(self.PATHS, map(int, out[8:16])))}
+        return {"sor": dict(zip(self.PATHS, map(int, out[:8])), tau_window=int(out[16])),
+                "normals": dict(zip(self.PATHS, map(int, out[8:16])), tau_window=int(out[17]))}
 
     def knn_routed(self) -> int:
         """SOR kNN queries the last run's cooperative pass took (0 without it)."""

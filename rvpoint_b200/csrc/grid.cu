@@ -227,6 +227,42 @@ __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__
   }
 }
 
+// The quarter-cell directory of the level-base cells (base 2) of kSubMin to
+// kSubMax points: one warp per cell walks its points (sorted by the 6-bit
+// Morton code of their quarter cell, the key's low bits) and writes, for
+// every code s, the offset of the first point with code >= s to sub_off[st +
+// s] (the cell's own positions: it has at least 64).
+__global__ void k_sub_dir(const u64 *keys, const u32 *lstart0, const u64 *nbuckets,
+                          const u64 *n_dev, uint16_t *sub_off) {
+  const u64 n = *n_dev;
+  const u64 nb = nbuckets[0];
+  const int lane = threadIdx.x & 31;
+  const u64 warps = ((u64)gridDim.x * blockDim.x) >> 5;
+  for (u64 b = ((u64)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += warps) {
+    const u32 st = lstart0[b];
+    const u32 en = b + 1 < nb ? lstart0[b + 1] : (u32)n;
+    const u32 ct = en - st;
+    if (ct < kSubMin || ct > kSubMax) continue;
+    int prev = -1;  // code of the point before this chunk
+    for (u32 i0 = st; i0 < en; i0 += 32) {
+      const u32 i = i0 + lane;
+      const int code = i < en ? (int)(keys[i] & 63u) : 64;
+      int before = __shfl_up_sync(0xffffffffu, code, 1);
+      if (lane == 0) before = prev;
+      // codes (before, code] start at this point
+      if (i < en)
+        for (int s = before + 1; s <= code; ++s) sub_off[st + s] = (uint16_t)(i - st);
+      prev = __shfl_sync(0xffffffffu, code, 31);
+      if (prev == 64) {  // the chunk ran past the cell: the last live code
+        const unsigned live = __ballot_sync(0xffffffffu, i < en);
+        prev = __shfl_sync(0xffffffffu, code, 31 - __clz(live));
+      }
+    }
+    // codes past the last point: the cell's end
+    for (int s = prev + 1 + lane; s < 64; s += 32) sub_off[st + s] = (uint16_t)ct;
+  }
+}
+
 __device__ __forceinline__ void table_put(ulonglong2 *table, u64 mask, u64 key, u64 ent,
                                           int *overflow) {
   u64 slot = mix64(key) & mask;
@@ -302,6 +338,7 @@ void Grid::reserve(size_t n, int nf) {
                  scan_temp_bytes(n_max));
   b_lstart.reserve(al(kHeadLevels * n_max * 4));
   b_pos.reserve(n_max * 4);
+  b_sub.reserve(al(n_max * 2));
   b_misc.reserve(256);
   d_n = b_misc.as<u64>();
   d_nbuckets = d_n + 1;
@@ -330,7 +367,7 @@ void Grid::fit_table(size_t buckets) {
 void Grid::release() {
   b_keys.release(); b_vals.release(); b_pts.release(); b_table.release();
   b_frames.release(); b_begin.release(); b_sort.release(); b_misc.release();
-  b_lstart.release(); b_pos.release();
+  b_lstart.release(); b_pos.release(); b_sub.release();
   n_max = 0; n_frames_max = 0; table_cap = 0;
 }
 
@@ -349,6 +386,7 @@ GridView Grid::view(int mode, long long p1, long long p2) const {
   v.n_points = d_n;
   v.pos_of = b_pos.as<u32>();
   v.lbase = lbase;
+  v.sub_off = mode == KEY_DENSE && lbase == 2 ? b_sub.as<uint16_t>() : nullptr;
   return v;
 }
 
@@ -414,6 +452,11 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
                                (u64)g.table_cap - 1,
                                g.d_nbuckets, g.d_overflow);
   RVP_LAUNCH_CHECK(ctx);
+  if (mode == KEY_DENSE && base == 2) {
+    k_sub_dir<<<sms * 8, 256, 0, st>>>(g.b_keys.as<u64>(), lstart, g.d_nbuckets, n_live,
+                                       g.b_sub.as<uint16_t>());
+    RVP_LAUNCH_CHECK(ctx);
+  }
 }
 
 // ===========================================================================
@@ -590,6 +633,7 @@ __global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int
   const size_t nwarps = ((size_t)gridDim.x * blockDim.x) >> 5;
   const bool two_level = g.mode == KEY_DENSE;
   for (size_t wi = warp; wi < nq; wi += nwarps) {
+    if (q.bound && q.bound[wi] == kTauDone) continue;  // finished by the tau pass
     const u32 qi = query_index(q, wi);
     const int f = q.frame_of ? q.frame_of[qi] : 0;
     const GridFrame F = g.frames[f];
@@ -632,13 +676,15 @@ __global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int
         if (!done) {
           // 2) every point with d2 <= tau lies in the tight window of
           //    sqrt(tau) and there are >= K of them: exact. Scan it at the
-          //    finest level whose window stays small.
+          //    finest level whose window has at most 1024 cells (32 lookup
+          //    rounds), skipping cells beyond the K-th distance: small cells
+          //    keep the scan close to the ball of sqrt(tau)
           const double rt = sqrt((double)tau);
           const int top = two_level ? g.lbase + kGridLevels - 1 : 0;
           for (int lt = two_level ? g.lbase : 0; lt <= top && !done; ++lt) {
             const Window wt = tight_window(F, qx, qy, qz, rt, lt);
             const long long cells = window_cells(wt);
-            if (cells <= (two_level ? (lt == top ? 512 : 125) : 4096)) {
+            if (cells <= (two_level ? (lt == top ? 4096 : 1024) : 4096)) {
               L.init();
               found = 0;
               knn_scan<P>(g, F, f, wt, false, qx, qy, qz, K, bound_of(tau), L, found);

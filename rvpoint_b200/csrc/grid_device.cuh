@@ -174,6 +174,27 @@ __device__ __forceinline__ double coverage(const GridFrame &F, const Window &w, 
   return cov;
 }
 
+// Lower bound on d2(p, q) for any point p of the level-L cell (ux, uy, uz):
+// the gap from q to the cell's box, widened on each side by the rounding
+// slack of the cell function and of the face positions, then shrunk by
+// 1e-5 (the float arithmetic of the bound itself)
+__device__ __forceinline__ float cell_lb2(const GridFrame &F, int level, int ux, int uy, int uz,
+                                          float qx, float qy, float qz) {
+  const float cs = F.cell * (float)(1 << level);
+  const int u[3] = {ux, uy, uz};
+  const float q[3] = {qx, qy, qz};
+  const float mn[3] = {F.min_x, F.min_y, F.min_z};
+  float s = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lo = mn[a] + (float)u[a] * cs;
+    const float sl = 4e-6f * (fabsf(mn[a]) + fabsf(q[a]) + (float)(abs(u[a]) + 2) * cs) + 1e-6f;
+    const float gap = fmaxf(fmaxf(lo - sl - q[a], q[a] - (lo + cs + sl)), 0.0f);
+    s += gap * gap;
+  }
+  return s * (1.0f - 1e-5f);
+}
+
 __device__ __forceinline__ long long window_cells(const Window &w) {
   long long c = 1;
 #pragma unroll
@@ -186,9 +207,14 @@ __device__ __forceinline__ long long window_cells(const Window &w) {
 
 // Walk every candidate of window w (or of the whole frame when brute):
 // fn(float4 p, bool valid) is called by all 32 lanes for each batch of 32.
-template <class Fn>
+// A cell is skipped when skip(cx, cy, cz) (cells of w's level) says so.
+struct NoSkip {
+  __device__ __forceinline__ bool operator()(int, int, int) const { return false; }
+};
+template <class Fn, class Skip = NoSkip>
 __device__ __forceinline__ void for_each_candidate(const GridView &g, const GridFrame &F, int f,
-                                                   const Window &w, bool brute, Fn &&fn) {
+                                                   const Window &w, bool brute, Fn &&fn,
+                                                   Skip skip = Skip()) {
   const int lane = threadIdx.x & 31;
   if (brute) {
     const u64 a = g.frame_pt_begin[f], b = g.frame_pt_begin[f + 1];
@@ -209,7 +235,8 @@ __device__ __forceinline__ void for_each_candidate(const GridView &g, const Grid
       const int cx = w.lo[0] + (int)(j % ncx);
       const int cy = w.lo[1] + (int)((j / ncx) % ncy);
       const int cz = w.lo[2] + (int)(j / ((long long)ncx * ncy));
-      if (!lookup(g, level_key(g, F, w.level, cx, cy, cz), start, count)) count = 0;
+      if (skip(cx, cy, cz) || !lookup(g, level_key(g, F, w.level, cx, cy, cz), start, count))
+        count = 0;
     }
     // flatten: inclusive scan of bucket sizes
     u32 incl = count;
@@ -308,6 +335,12 @@ __device__ __forceinline__ void knn_scan(const GridView &g, const GridFrame &F, 
                                          float qz, int K, u64 bound, WarpList<P> &L,
                                          u32 &found) {
   u64 thr = L.get(K - 1);
+  // cells farther than the current K-th distance (or the bound) are skipped
+  const float bd2 = nbr_d2(bound);
+  auto skip = [&](int cx, int cy, int cz) {
+    const float lim = fminf(nbr_d2(thr), bd2);  // NaN (unfilled list) never skips
+    return cell_lb2(F, w.level, cx, cy, cz, qx, qy, qz) > lim;
+  };
   for_each_candidate(g, F, f, w, brute, [&](float4 p, bool valid) {
     const u32 idx = __float_as_uint(p.w);
     u64 key = ~0ull;
@@ -331,7 +364,7 @@ __device__ __forceinline__ void knn_scan(const GridView &g, const GridFrame &F, 
         thr = L.get(K - 1);
       }
     }
-  });
+  }, skip);
 }
 
 }  // namespace gd

@@ -212,7 +212,13 @@ struct GridView {  // what the query kernels read
   const u64 *n_points;     // number of grid points (device; set by grid_build)
   const u32 *pos_of;       // sorted position of each point (by original index)
   int lbase;               // dense mode: the finest table level (query cell = fine cell << lbase)
+  // lbase == 2: for every level-lbase cell of kSubMin to kSubMax points
+  // (start st), sub_off[st + s] = offset in the cell of the first point of
+  // its s-th quarter cell (s: the 6-bit Morton code of the quarter cell in
+  // the cell; the cell's points are sorted by it); null otherwise
+  const uint16_t *sub_off;
 };
+constexpr u32 kSubMin = 64, kSubMax = 65535;
 
 struct Grid {
   int n_frames_max = 0;
@@ -220,7 +226,8 @@ struct Grid {
   size_t table_cap = 0;
   size_t table_cap_req = 0;    // 0: sized from n_max
   int lbase = 0;               // see GridView::lbase
-  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_lstart, b_pos;
+  DevBuf b_keys, b_vals, b_pts, b_table, b_frames, b_begin, b_sort, b_misc, b_lstart, b_pos,
+      b_sub;
   u64 *d_n = nullptr;          // number of points (device)
   u64 *d_nbuckets = nullptr;   // buckets per level [kHeadLevels] (device)
   int *d_collision = nullptr;  // mode 0: hash collision detected
@@ -328,6 +335,17 @@ bool normals_from_sor_lists(rvp_context *ctx, const GridView &g, const TileArgs 
                             int kn);
 bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
                    int blocks, u32 *stats = nullptr);
+// The hard slots that carry a bound tau (TileArgs::hard, hard_tau; n_hard on
+// the device): one thread per slot scans the tight window of sqrt(tau) at the
+// finest level where it spans at most 27 cells -- exact, since at least K
+// points lie within tau. Done slots get hard_tau = kTauDone (grid_knn skips
+// them). Outputs as the mode's: SOR mean (+ list row), TILE_NORMALS lists by
+// slot (slot_pairs / slot_counts, as KNN_OUT_BY_SLOT), pairs by index.
+// False (nothing launched) if k has no instantiation.
+constexpr float kTauDone = -2.0f;
+bool grid_knn_tau(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
+                  const u64 *n_hard, u64 *slot_pairs = nullptr, int32_t *slot_counts = nullptr,
+                  u32 *stats = nullptr);
 
 // ---------------------------------------------------------------------------
 // voxel grid (voxel.cu)

@@ -575,31 +575,40 @@ __global__ __launch_bounds__(TT, 3) void k_knn_wt(GridView g, TileArgs a, int le
   }
 }
 
-// Cooperative kNN at the finest chain level. Every grid point whose own
-// cell holds at least `min_own` points is picked (k_knn_route): in such
-// dense cells a radius from the occupancy is likely to hold K points inside
-// the cell's 27-cell ring. One warp takes 32 consecutive picked queries (a
+// Cooperative kNN at the first chain level. Every grid point whose own cell
+// holds at least `min_own` points is picked (k_knn_route): in such dense
+// cells a radius from the occupancy is likely to hold K points inside the
+// cell's 27-cell ring. One warp takes 32 consecutive picked queries (a
 // compacted list in grid order, so they lie close together), looks up the
-// union of their rings once (per-warp table, as in k_knn_wt), and every
-// lane takes the bound tb = r^2 with r = rfac * cell * sqrt(K / own-cell
-// count), under one cell. The warp walks only the cells some lane can still
-// use (box distance below that lane's min(tb, K-th key)): 32 candidates of
-// such a cell go up coalesced into a per-warp staging row and every lane
-// tests all of them against its query (broadcast shared-memory reads, all
-// lanes converged). A candidate within tb (and not beyond the lane's K-th
-// key) goes, as its grid position, into the lane's buffer in shared memory;
-// the buffers are merged into the lanes' register lists (insertion network)
-// when one of them fills and at the end, so the warp pays for each lane's
-// insertions once, not for the busiest lane of every batch of 32. Every
-// point with d2 <= tb lies in the lane's tight window of sqrt(tb), inside
-// its ring, and every cell that can hold one is walked, so a lane that found
-// K such points is exact. The others (and warps whose queries span more
-// than the table) stay open for the per-lane kernels, like the queries that
-// were not picked.
+// union of their rings once (per-warp table, as in k_knn_wt), and every lane
+// takes the bound tb = r^2 with r = rfac * cell * sqrt(K / own-cell count),
+// under one cell. The warp walks only the cells some lane can use (box
+// distance below that lane's bound): 32 candidates of such a cell go up
+// coalesced into a per-warp staging row and every lane tests all of them
+// against its query, four at a time (broadcast shared-memory reads, all
+// lanes converged, four independent distance chains). A candidate within
+// the lane's bound goes, as (d2, grid position), into the lane's buffer in
+// shared memory. Every point with d2 <= tb lies in the lane's tight window
+// of sqrt(tb), inside its ring, and every cell that can hold one is walked,
+// so a lane that found K such points is exact.
+//   Selection (float-key SOR modes): at the end the buffer goes through the
+// float insertion network once (sorted K smallest distances: the mean), and
+// the list row takes the positions of the buffered candidates within the
+// K-th distance, each at its rank among those distances; equal distances
+// leave the order (or at the boundary the set) to the scan order, and the
+// row is marked unusable. A buffer about to overflow is cut to its K smallest (and their
+// equals), which then gate what the buffer takes (anything farther cannot be
+// among the K nearest); a lane whose cut cannot free room (many equal
+// distances) gives up and stays open. Feature pairs (TILE_PAIRS_F) need the
+// (d2, index) order: their buffer is merged into a register list with
+// indices beside (insertion network) whenever it fills, and at the end.
+// The queries that stay open (and warps whose queries span more than the
+// table) go to the per-lane kernels, like the queries that were not picked.
 constexpr int CP_WARPS = TT / 32;
-constexpr int CP_BUF = 64;  // buffered candidates per lane
+constexpr int CP_BUF = 48;  // buffered (d2, position) candidates per lane
+constexpr int CP_ILP = 4;   // candidates tested together
 constexpr size_t CP_SMEM = (size_t)CP_WARPS * (WT_CELLS * sizeof(uint2) + 32 * sizeof(float4) +
-                                               CP_BUF * 32 * sizeof(u32));
+                                               CP_BUF * 32 * sizeof(uint2));
 
 template <int K, int MODE>
 __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int level,
@@ -607,17 +616,33 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
                                                     uint8_t *qlevel, float *qtau, u32 *stats) {
   static_assert(MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F,
                 "float-key modes only");
-  constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
+  static_assert(K + CP_ILP <= CP_BUF, "the buffer must hold K candidates and a test group");
+  constexpr bool PAIRS = MODE == TILE_PAIRS_F;
   extern __shared__ __align__(16) unsigned char cp_smem[];
   uint2 (*wtab)[WT_CELLS] = reinterpret_cast<uint2 (*)[WT_CELLS]>(cp_smem);
   float4 (*stage)[32] =
       reinterpret_cast<float4 (*)[32]>(cp_smem + CP_WARPS * WT_CELLS * sizeof(uint2));
-  u32 (*sbuf)[CP_BUF][32] = reinterpret_cast<u32 (*)[CP_BUF][32]>(
+  uint2 (*sbuf)[CP_BUF][32] = reinterpret_cast<uint2 (*)[CP_BUF][32]>(
       cp_smem + CP_WARPS * (WT_CELLS * sizeof(uint2) + 32 * sizeof(float4)));
   const u64 n = *n_list;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const u64 nwarps = (u64)gridDim.x * CP_WARPS;
   const int sh = level;
+  // quarter-cell directories (the cells are of 4 x 4 x 4 fine cells)
+  const bool use_dir = g.sub_off != nullptr && level == 2;
+  // sub_mask[a][m]: the quarter cells of a cell (bits by Morton code) whose
+  // coordinate along axis a is in the 4-bit value set m
+  __shared__ u64 sub_mask[3][16];
+  if (threadIdx.x < 48) {
+    const int ax = threadIdx.x / 16, m = threadIdx.x % 16;
+    u64 bits = 0;
+    for (int c = 0; c < 64; ++c) {
+      const int v = ((c >> ax) & 1) | (((c >> (ax + 3)) & 1) << 1);
+      if ((m >> v) & 1) bits |= 1ull << c;
+    }
+    sub_mask[ax][m] = bits;
+  }
+  __syncthreads();
   for (u64 base = ((u64)blockIdx.x * CP_WARPS + wib) * 32; base < n; base += nwarps * 32) {
     const bool active = base + lane < n;
     const u64 pos = active ? (u64)list[base + lane] : 0;
@@ -662,13 +687,18 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
     const float cs = F.cell * (float)(1 << sh);
     float tb = -1.0f;
     float glx = 0.0f, ghx = 0.0f, gly = 0.0f, ghy = 0.0f, glz = 0.0f, ghz = 0.0f;
+    Window wq;  // the lane's tight window of sqrt(tb) in fine (quarter) cells
+    wq.lo[0] = wq.lo[1] = wq.lo[2] = 1;
+    wq.hi[0] = wq.hi[1] = wq.hi[2] = 0;
     if (active) {
       const u32 n_own = wtab[wib][((cz - bz0) * wy + (cy - by0)) * wx + (cx - bx0)].y;
       const float r = fminf(a.rfac * cs * sqrtf((float)K / (float)max(n_own, 1u)), 0.999f * cs);
       const Window wt = tight_window(F, q.x, q.y, q.z, sqrt((double)(r * r)), level);
       if (wt.lo[0] >= cx - 1 && wt.hi[0] <= cx + 1 && wt.lo[1] >= cy - 1 &&
-          wt.hi[1] <= cy + 1 && wt.lo[2] >= cz - 1 && wt.hi[2] <= cz + 1)
+          wt.hi[1] <= cy + 1 && wt.lo[2] >= cz - 1 && wt.hi[2] <= cz + 1) {
         tb = r * r;
+        if (use_dir) wq = tight_window(F, q.x, q.y, q.z, sqrt((double)(r * r)), 0);
+      }
       const float fx = F.min_x + (float)cx * cs, fy = F.min_y + (float)cy * cs,
                   fz = F.min_z + (float)cz * cs;
       const float slx = 4e-6f * (fabsf(F.min_x) + fabsf(q.x) + (float)(cx + 2) * cs) + 1e-6f;
@@ -682,36 +712,94 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
       ghz = fmaxf(fz + cs - q.z - slz, 0.0f);
     }
     float L[K];
-    u32 I[KV ? K : 1];
+    u32 I[PAIRS ? K : 1];
 #pragma unroll
     for (int j = 0; j < K; ++j) L[j] = INFINITY;
-    float thr = INFINITY;
+    float thr = INFINITY;  // PAIRS: the register list's K-th key
     float tie = -1.0f;
-    u32 found = 0;
-    int cnt = 0;  // buffered candidates of this lane
-    // merge the buffered candidates into the register list, in buffer order
-    auto flush = [&]() {
+    float gate = tb;       // what the buffer takes: d2 <= gate
+    bool seen_k = false;   // K candidates within tb were met (the buffer was cut)
+    int cnt = 0;           // buffered candidates of this lane
+    // PAIRS: merge the buffer into the register list, in buffer order
+    auto merge_pairs = [&]() {
       for (int i = 0; __any_sync(0xffffffffu, i < cnt); ++i) {
         if (i < cnt) {
-          const u32 j = sbuf[wib][i][lane];
-          const float4 p = __ldg(&g.pts[j]);
-          const float key = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
-          if (key < thr) {
-            if constexpr (KV) {
-              // the SOR list keeps grid positions, the feature pairs indices
-              list_insert_kv<K>(L, I, key, MODE == TILE_SOR_LIST ? j : __float_as_uint(p.w));
+          const uint2 b = sbuf[wib][i][lane];
+          const float key = __uint_as_float(b.x);
+          if constexpr (PAIRS) {
+            if (key < thr) {
+              list_insert_kv<K>(L, I, key, b.y);
               if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
-            } else {
-              list_insert<float, K>(L, key);
+              thr = L[K - 1];
+            } else if (key == thr) {
+              tie = key;
             }
-            thr = L[K - 1];
-          } else if constexpr (KV) {
-            if (key == thr) tie = key;
           }
         }
       }
       cnt = 0;
     };
+    // SOR modes: the K smallest buffered distances, sorted (float network)
+    auto select_k = [&]() {
+#pragma unroll
+      for (int j = 0; j < K; ++j) L[j] = INFINITY;
+      for (int i = 0; __any_sync(0xffffffffu, i < cnt); ++i) {
+        if (i < cnt) {
+          const float key = __uint_as_float(sbuf[wib][i][lane].x);
+          if (key < L[K - 1]) list_insert<float, K>(L, key);
+        }
+      }
+    };
+    // SOR modes, a full buffer: keep its K smallest and their equals
+    auto cut = [&]() {
+      const bool full = cnt > CP_BUF - CP_ILP;
+      const int keep_cnt = cnt;
+      if (!full) cnt = 0;  // only the full lanes select
+      select_k();
+      cnt = keep_cnt;
+      if (full) {
+        const float t = L[K - 1];
+        int m = 0;
+        for (int i = 0; i < cnt; ++i) {
+          const uint2 b = sbuf[wib][i][lane];
+          if (__uint_as_float(b.x) <= t) sbuf[wib][m++][lane] = b;
+        }
+        seen_k = true;
+        cnt = m;
+        if (m > CP_BUF - CP_ILP) {  // no room freed: give up (stays open)
+          gate = -1.0f;
+          cnt = 0;
+        } else {
+          gate = t;
+        }
+      }
+    };
+    // test the staged row (m candidates: x, y, z and the grid position in
+    // w; padded to a multiple of CP_ILP with infinitely far points) against
+    // the lane's limit and buffer the hits
+    auto test_row = [&](u32 m, bool need) {
+      const u32 mp = (m + CP_ILP - 1) & ~(u32)(CP_ILP - 1);
+      for (u32 s2 = 0; s2 < mp; s2 += CP_ILP) {
+        // the lane's limit now (the cut and, for pairs, the merge lower it)
+        const float lim = need ? (PAIRS ? fminf(gate, thr) : gate) : -1.0f;
+        float d[CP_ILP];
+        u32 ps[CP_ILP];
+#pragma unroll
+        for (int u = 0; u < CP_ILP; ++u) {
+          const float4 p = stage[wib][s2 + u];
+          d[u] = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+          ps[u] = __float_as_uint(p.w);
+        }
+#pragma unroll
+        for (int u = 0; u < CP_ILP; ++u)
+          if (d[u] <= lim) sbuf[wib][cnt++][lane] = make_uint2(__float_as_uint(d[u]), ps[u]);
+        if (__any_sync(0xffffffffu, cnt > CP_BUF - CP_ILP)) {
+          if constexpr (PAIRS) merge_pairs();
+          else cut();
+        }
+      }
+    };
+    const float4 far4 = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
     for (int t = 0; t < ncells; ++t) {
       const uint2 e = wtab[wib][t];
       if (e.y == 0) continue;
@@ -722,30 +810,96 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
       const float gx = dx < 0 ? glx + (float)(-dx - 1) * cs : (dx > 0 ? ghx + (float)(dx - 1) * cs : 0.0f);
       const float gy = dy < 0 ? gly + (float)(-dy - 1) * cs : (dy > 0 ? ghy + (float)(dy - 1) * cs : 0.0f);
       const float gz = dz < 0 ? glz + (float)(-dz - 1) * cs : (dz > 0 ? ghz + (float)(dz - 1) * cs : 0.0f);
-      const bool need = tb >= 0.0f && (gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) <= fminf(thr, tb);
+      const float lim0 = PAIRS ? fminf(gate, thr) : gate;
+      const bool need = lim0 >= 0.0f && (gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) <= lim0;
       if (!__any_sync(0xffffffffu, need)) continue;
-      for (u32 j0 = 0; j0 < e.y; j0 += 32) {
-        const u32 m = min(32u, e.y - j0);
-        if ((u32)lane < m) stage[wib][lane] = __ldg(&g.pts[e.x + j0 + lane]);
-        __syncwarp();
+      if (use_dir && e.y >= kSubMin && e.y <= kSubMax) {
+        // only the quarter cells inside some needing lane's window: the
+        // union of the lanes' boxes of quarter cells, as a 64-bit mask by
+        // Morton code
+        u64 mk = 0;
         if (need) {
-          for (u32 s2 = 0; s2 < m; ++s2) {
-            const float4 p = stage[wib][s2];
-            const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
-            if (d2 <= tb) {
-              ++found;
-              // a key equal to the K-th still goes in: it marks a tie
-              if (d2 <= thr) sbuf[wib][cnt++][lane] = e.x + j0 + s2;
-            }
+          const int u0[3] = {ux << 2, uy << 2, uz << 2};
+          mk = ~0ull;
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax) {
+            const int lo = max(wq.lo[ax] - u0[ax], 0), hi = min(wq.hi[ax] - u0[ax], 3);
+            const int vm = lo <= hi ? (((2 << hi) - 1) & ~((1 << lo) - 1)) : 0;
+            mk &= sub_mask[ax][vm];
           }
         }
-        __syncwarp();  // the staging row is refilled next
-        if (__any_sync(0xffffffffu, cnt > CP_BUF - 32)) flush();
+        const u64 mask = (u64)__reduce_or_sync(0xffffffffu, (u32)mk) |
+                         ((u64)__reduce_or_sync(0xffffffffu, (u32)(mk >> 32)) << 32);
+        // lane l: quarter cells 2l and 2l + 1 (offsets d0, d1; the next
+        // lane's d0 ends the second)
+        const uint16_t *dir = g.sub_off + e.x;
+        const u32 d0 = dir[2 * lane], d1 = dir[2 * lane + 1];
+        u32 e1 = __shfl_down_sync(0xffffffffu, d0, 1);
+        if (lane == 31) e1 = e.y;
+        const u32 c0 = (mask >> (2 * lane)) & 1 ? d1 - d0 : 0;
+        const u32 c1 = (mask >> (2 * lane + 1)) & 1 ? e1 - d1 : 0;
+        u32 incl = c0 + c1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const u32 ex = incl - c0 - c1;
+        const u32 M = __shfl_sync(0xffffffffu, incl, 31);
+        for (u32 p0 = 0; p0 < M; p0 += 32) {
+          const u32 p = p0 + (u32)lane;
+          // the owning lane: the last with ex <= p
+          int o = 0;
+#pragma unroll
+          for (int st2 = 16; st2; st2 >>= 1) {
+            const u32 v = __shfl_sync(0xffffffffu, ex, o + st2);
+            if (v <= p) o += st2;
+          }
+          const u32 r = p - __shfl_sync(0xffffffffu, ex, o);
+          const u32 c0o = __shfl_sync(0xffffffffu, c0, o);
+          const u32 d0o = __shfl_sync(0xffffffffu, d0, o);
+          const u32 d1o = __shfl_sync(0xffffffffu, d1, o);
+          const u32 m = min(32u, M - p0);
+          if ((u32)lane < m) {
+            const u32 cp = e.x + (r < c0o ? d0o + r : d1o + (r - c0o));
+            const float4 v = __ldg(&g.pts[cp]);
+            stage[wib][lane] = make_float4(v.x, v.y, v.z, __uint_as_float(cp));
+          } else {
+            stage[wib][lane] = far4;
+          }
+          __syncwarp();
+          test_row(m, need);
+          __syncwarp();  // the staging row is refilled next
+        }
+      } else {
+        for (u32 j0 = 0; j0 < e.y; j0 += 32) {
+          const u32 m = min(32u, e.y - j0);
+          if ((u32)lane < m) {
+            const u32 cp = e.x + j0 + lane;
+            const float4 v = __ldg(&g.pts[cp]);
+            stage[wib][lane] = make_float4(v.x, v.y, v.z, __uint_as_float(cp));
+          } else {
+            stage[wib][lane] = far4;
+          }
+          __syncwarp();
+          test_row(m, need);
+          __syncwarp();  // the staging row is refilled next
+        }
       }
     }
-    flush();
+    // the K nearest from what is buffered
+    bool found_k;
+    if constexpr (PAIRS) {
+      // (every candidate within tb went into the buffer: the merged count
+      // plus the rest decides)
+      merge_pairs();
+      found_k = thr < INFINITY;
+    } else {
+      select_k();
+      found_k = gate >= 0.0f && (seen_k || cnt >= K);
+    }
     if (active) {
-      if (found < (u32)K) {
+      if (!found_k) {
         leave_open();
       } else {
         qlevel[pos] = 0xFF;
@@ -753,33 +907,387 @@ __global__ __launch_bounds__(TT, 2) void k_knn_coop(GridView g, TileArgs a, int 
         float sum = 0.0f;
 #pragma unroll
         for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
-        if constexpr (MODE != TILE_PAIRS_F) a.mean[qidx] = fdiv(sum, (float)(K - 1));
-        if constexpr (KV) {
+        if constexpr (!PAIRS) a.mean[qidx] = fdiv(sum, (float)(K - 1));
+        if constexpr (MODE == TILE_SOR_LIST) {
+          // each buffered position within the K-th distance goes to its
+          // rank in the sorted distances (the number below its own). Equal
+          // distances (ranks that collide, or more than K within the K-th
+          // distance) leave the order, or at the boundary the set, to the
+          // scan order instead of the index: the row is marked unusable and
+          // the normal stage searches that point again
+          const float t = L[K - 1];
+          u32 *row = a.sor_list + (size_t)pos * K;
+          int m = 0;
+          for (int i = 0; i < cnt; ++i) {
+            const uint2 b = sbuf[wib][i][lane];
+            const float d = __uint_as_float(b.x);
+            if (d <= t) {
+              int r = 0;
+#pragma unroll
+              for (int j = 0; j < K; ++j) r += L[j] < d ? 1 : 0;
+              if (r < K) row[r] = b.y;
+              ++m;
+            }
+          }
+          bool tied = m != K;
+#pragma unroll
+          for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
+          if (tied)
+            for (int j = 0; j < K; ++j) row[j] = 0xFFFFFFFFu;
+        } else if constexpr (PAIRS) {
           // equal distances leave the order (and at the boundary the set) to
           // the scan order instead of the index: marked for the exact search
           bool tied = tie == L[K - 1];
 #pragma unroll
           for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
-          if constexpr (MODE == TILE_SOR_LIST) {
-            u32 *row = a.sor_list + (size_t)pos * K;
-#pragma unroll
-            for (int j = 0; j < K; ++j) row[j] = tied ? 0xFFFFFFFFu : I[j];
+          if (tied) {
+            const u32 slot = atomicAdd(a.hard_count, 1u);
+            a.hard[slot] = qidx & 0x7FFFFFFFu;
+            if (a.hard_tau) a.hard_tau[slot] = L[K - 1];
           } else {
-            if (tied) {
-              const u32 slot = atomicAdd(a.hard_count, 1u);
-              a.hard[slot] = qidx & 0x7FFFFFFFu;
-              if (a.hard_tau) a.hard_tau[slot] = L[K - 1];
-            } else {
 #pragma unroll
-              for (int j = 0; j < K; ++j)
-                a.pairs[(size_t)qidx * K + j] = pack_nbr(L[j], (int)I[j]);
-              if (a.counts) a.counts[qidx] = K;
-            }
+            for (int j = 0; j < K; ++j)
+              a.pairs[(size_t)qidx * K + j] = pack_nbr(L[j], (int)__float_as_uint(g.pts[I[j]].w));
+            if (a.counts) a.counts[qidx] = K;
           }
         }
       }
     }
     __syncwarp();  // the warp's table and buffers are reused by its next 32 queries
+  }
+}
+
+// Queries the per-lane chain handed on with a bound tau (the K-th distance
+// found in a ring that could not certify it): every point with d2 <= tau
+// lies in the tight window of sqrt(tau), and at least K of them do, so a
+// scan of that window bounded by tau is exact. One thread per hard slot
+// scans the window at the finest table level where it spans at most
+// kTauCells cells (its own lookups: the lanes of a warp sit at different
+// levels and places), skipping cells farther than min(tau, K-th key), when
+// the cells within tau hold at most kTauPoints points. Done slots get tau =
+// kTauDone, which the warp-per-query kernel skips; slots without a bound,
+// with more candidates, and feature lists with tied distances stay for it.
+//   TILE_SOR_MEAN / TILE_SOR_LIST: the mean (and the row of grid positions)
+//   TILE_NORMALS: the (d2, index) list by slot (slot_pairs, slot_counts),
+//                 as the warp kernel's KNN_OUT_BY_SLOT writes it
+//   TILE_PAIRS / TILE_PAIRS_F: the list by original index (a.pairs, a.counts)
+constexpr int kTauCells = 64;     // window cells one thread looks up
+constexpr u32 kTauPoints = 512;   // candidates one thread scans
+
+template <int K, int MODE>
+__global__ __launch_bounds__(TT, 3) void k_knn_tau(GridView g, TileArgs a, const u64 *n_hard,
+                                                   u64 *slot_pairs, int32_t *slot_counts,
+                                                   u32 *stats) {
+  constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
+  constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
+  using Key = typename std::conditional<FKEY, float, u64>::type;
+  const u64 n = *n_hard;
+  for (u64 s = blockIdx.x * (u64)blockDim.x + threadIdx.x; s < n;
+       s += (u64)gridDim.x * blockDim.x) {
+    const float tau = a.hard_tau[s];
+    if (!(tau >= 0.0f)) continue;
+    const u32 qi = a.hard[s];
+    const u32 pos = g.pos_of[qi];
+    const float4 q = g.pts[pos];
+    const GridFrame F = g.frames[a.frame_of ? a.frame_of[qi] : 0];
+    const double rt = sqrt((double)tau);
+    Window w;
+    int level = -1;
+    for (int L = g.lbase; L < g.lbase + kGridLevels; ++L) {
+      w = tight_window(F, q.x, q.y, q.z, rt, L);
+      if (window_cells(w) <= kTauCells) {
+        level = L;
+        break;
+      }
+    }
+    if (level < 0) continue;
+    // the points in cells within tau: past kTauPoints the warp kernel (lanes
+    // over candidates) is faster than one thread
+    {
+      u32 total = 0;
+      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
+        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
+          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+            u32 st, cnt;
+            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) <= tau &&
+                lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt))
+              total += cnt;
+          }
+      if (total > kTauPoints) continue;
+    }
+    const int sh = level;
+    const float cs = F.cell * (float)(1 << sh);
+    const int cx = cell_axis(q.x, F.min_x, F.cell) >> sh, cy = cell_axis(q.y, F.min_y, F.cell) >> sh,
+              cz = cell_axis(q.z, F.min_z, F.cell) >> sh;
+    // distances from q to its own cell's faces, shrunk by the cell
+    // function's rounding slack
+    float glx, ghx, gly, ghy, glz, ghz;
+    {
+      const float fx = F.min_x + (float)cx * cs, fy = F.min_y + (float)cy * cs,
+                  fz = F.min_z + (float)cz * cs;
+      const float slx = 4e-6f * (fabsf(F.min_x) + fabsf(q.x) + (float)(cx + 2) * cs) + 1e-6f;
+      const float sly = 4e-6f * (fabsf(F.min_y) + fabsf(q.y) + (float)(cy + 2) * cs) + 1e-6f;
+      const float slz = 4e-6f * (fabsf(F.min_z) + fabsf(q.z) + (float)(cz + 2) * cs) + 1e-6f;
+      glx = fmaxf(q.x - fx - slx, 0.0f);
+      ghx = fmaxf(fx + cs - q.x - slx, 0.0f);
+      gly = fmaxf(q.y - fy - sly, 0.0f);
+      ghy = fmaxf(fy + cs - q.y - sly, 0.0f);
+      glz = fmaxf(q.z - fz - slz, 0.0f);
+      ghz = fmaxf(fz + cs - q.z - slz, 0.0f);
+    }
+    Key kMax;
+    if constexpr (FKEY) kMax = INFINITY;
+    else kMax = ~0ull;
+    Key L[K];
+#pragma unroll
+    for (int j = 0; j < K; ++j) L[j] = kMax;
+    u32 I[KV ? K : 1];
+    Key thr = kMax;
+    float tie = -1.0f;
+    u32 found = 0;
+    for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
+      for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
+        for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+          // lower bound on the distance from q to the cell (whole cells
+          // between q's cell and it add their edge)
+          const int dx = ux - cx, dy = uy - cy, dz = uz - cz;
+          const float gx = dx < 0 ? glx + (float)(-dx - 1) * cs : (dx > 0 ? ghx + (float)(dx - 1) * cs : 0.0f);
+          const float gy = dy < 0 ? gly + (float)(-dy - 1) * cs : (dy > 0 ? ghy + (float)(dy - 1) * cs : 0.0f);
+          const float gz = dz < 0 ? glz + (float)(-dz - 1) * cs : (dz > 0 ? ghz + (float)(dz - 1) * cs : 0.0f);
+          float thr_d2;
+          if constexpr (FKEY) thr_d2 = thr;
+          else thr_d2 = nbr_d2(thr);
+          if ((gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) > fminf(thr_d2, tau)) continue;
+          u32 st, cnt;
+          if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt)) continue;
+          for (u32 j = 0; j < cnt; ++j) {
+            const float4 p = __ldg(&g.pts[st + j]);
+            const u32 pidx = __float_as_uint(p.w);
+            if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
+            const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+            if (!(d2 <= tau)) continue;
+            ++found;
+            Key key;
+            if constexpr (FKEY) key = d2;
+            else key = pack_nbr(d2, (int)pidx);
+            if (key < thr) {
+              if constexpr (KV) {
+                list_insert_kv<K>(L, I, key, MODE == TILE_SOR_LIST ? st + j : pidx);
+                if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
+              } else {
+                list_insert<Key, K>(L, key);
+              }
+              thr = L[K - 1];
+            } else if constexpr (KV) {
+              if (key == thr) tie = key;
+            }
+          }
+        }
+    if (found < (u32)K) continue;  // not reached with a true bound; the warp kernel decides
+    bool tied = false;
+    if constexpr (KV) {
+      tied = tie == L[K - 1];
+#pragma unroll
+      for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
+    }
+    if constexpr (MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST) {
+      float sum = 0.0f;
+#pragma unroll
+      for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
+      a.mean[qi] = fdiv(sum, (float)(K - 1));
+      if constexpr (MODE == TILE_SOR_LIST) {
+        u32 *row = a.sor_list + (size_t)pos * K;
+#pragma unroll
+        for (int j = 0; j < K; ++j) row[j] = tied ? 0xFFFFFFFFu : I[j];
+      }
+    } else if constexpr (MODE == TILE_NORMALS) {
+#pragma unroll
+      for (int j = 0; j < K; ++j) slot_pairs[(size_t)s * K + j] = L[j];
+      slot_counts[s] = K;
+    } else if constexpr (MODE == TILE_PAIRS_F) {
+      if (tied) continue;  // the exact (d2, index) order from the warp kernel
+#pragma unroll
+      for (int j = 0; j < K; ++j) a.pairs[(size_t)qi * K + j] = pack_nbr(L[j], (int)I[j]);
+      if (a.counts) a.counts[qi] = K;
+    } else {
+#pragma unroll
+      for (int j = 0; j < K; ++j) a.pairs[(size_t)qi * K + j] = L[j];
+      if (a.counts) a.counts[qi] = K;
+    }
+    a.hard_tau[s] = kTauDone;
+    if (stats) atomicAdd(stats, 1u);
+  }
+}
+
+// Adaptive per-thread kNN for the queries the cooperative pass leaves open
+// (sparse cells, and the dense ones it could not finish): one thread per
+// query, no table shared with other lanes. A radius r is estimated from the
+// finest chain level whose own cell holds K points (r = cell * sqrt(K /
+// count), under one cell; the top level's cell when none does). Then,
+// repeatedly: the tight window of r at the finest table level where it
+// spans at most kTauCells cells; a count pass over its cells within r (cell
+// box lower bound) -- fewer than K points: r doubles, nothing scanned; more
+// than kTauPoints: the query goes to the warp kernel (lanes over
+// candidates); else a scan bounded by r^2 (every point with d2 <= r^2 lies in
+// the window), exact when it found K such points, else r grows by sqrt 2.
+// Queries left after kAdaptTries attempts go to the hard list without a
+// bound. Outputs as k_knn_wt's (the SOR mean and list row, the fused
+// normal, or feature pairs; tied lists as there).
+constexpr int kAdaptTries = 8;
+
+template <int K, int MODE>
+__global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
+                                                     const u64 *n_list, u32 *stats) {
+  constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
+  constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
+  using Key = typename std::conditional<FKEY, float, u64>::type;
+  const u64 n = *n_list;
+  const int top = g.lbase + kGridLevels - 1;
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u32 pos = list[i];
+    const float4 q = g.pts[pos];
+    const u32 qidx = __float_as_uint(q.w);
+    if (MODE == TILE_NORMALS && (qidx & kRemovedBit)) continue;
+    const u32 qi = qidx & 0x7FFFFFFFu;
+    const GridFrame F = g.frames[a.frame_of ? a.frame_of[qi] : 0];
+    const int fx = cell_axis(q.x, F.min_x, F.cell), fy = cell_axis(q.y, F.min_y, F.cell),
+              fz = cell_axis(q.z, F.min_z, F.cell);
+    float r = F.cell * (float)(1 << top);
+    for (int L = g.lbase; L <= top; ++L) {
+      u32 st, ct;
+      if (!lookup(g, level_key(g, F, L, fx >> L, fy >> L, fz >> L), st, ct)) ct = 0;
+      if (ct >= (u32)K) {
+        const float cs = F.cell * (float)(1 << L);
+        r = fminf(cs * sqrtf((float)K / (float)ct), cs);
+        break;
+      }
+    }
+    Key kMax;
+    if constexpr (FKEY) kMax = INFINITY;
+    else kMax = ~0ull;
+    Key L[K];
+    u32 I[KV ? K : 1];
+    float tie = -1.0f;
+    bool done = false, punt = false;
+    for (int attempt = 0; attempt < kAdaptTries && !done && !punt; ++attempt) {
+      const float tb = r * r;
+      Window w;
+      int level = -1;
+      for (int Lv = g.lbase; Lv <= top; ++Lv) {
+        w = tight_window(F, q.x, q.y, q.z, sqrt((double)tb), Lv);
+        if (window_cells(w) <= kTauCells) {
+          level = Lv;
+          break;
+        }
+      }
+      if (level < 0) {
+        punt = true;
+        break;
+      }
+      u32 total = 0;
+      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
+        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
+          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+            u32 st, cnt;
+            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) <= tb &&
+                lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt))
+              total += cnt;
+          }
+      if (total < (u32)K) {  // the window cannot hold K points within r
+        r *= 2.0f;
+        continue;
+      }
+      if (total > kTauPoints) {
+        punt = true;
+        break;
+      }
+#pragma unroll
+      for (int j = 0; j < K; ++j) L[j] = kMax;
+      Key thr = kMax;
+      tie = -1.0f;
+      u32 found = 0;
+      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
+        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
+          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+            float thr_d2;
+            if constexpr (FKEY) thr_d2 = thr;
+            else thr_d2 = nbr_d2(thr);
+            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > fminf(thr_d2, tb)) continue;
+            u32 st, cnt;
+            if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt)) continue;
+            for (u32 j = 0; j < cnt; ++j) {
+              const float4 p = __ldg(&g.pts[st + j]);
+              const u32 pidx = __float_as_uint(p.w);
+              if (MODE == TILE_NORMALS && (pidx & kRemovedBit)) continue;
+              const float d2 = dist2(p.x, p.y, p.z, q.x, q.y, q.z);
+              if (!(d2 <= tb)) continue;
+              ++found;
+              Key key;
+              if constexpr (FKEY) key = d2;
+              else key = pack_nbr(d2, (int)pidx);
+              if (key < thr) {
+                if constexpr (KV) {
+                  list_insert_kv<K>(L, I, key, MODE == TILE_SOR_LIST ? st + j : pidx);
+                  if (L[K - 1] == thr) tie = thr;  // evicted a key equal to the boundary
+                } else {
+                  list_insert<Key, K>(L, key);
+                }
+                thr = L[K - 1];
+              } else if constexpr (KV) {
+                if (key == thr) tie = key;
+              }
+            }
+          }
+      if (found >= (u32)K) done = true;
+      else r *= 1.41421356f;
+    }
+    if (!done) {
+      const u32 slot = atomicAdd(a.hard_count, 1u);
+      a.hard[slot] = qi;
+      if (a.hard_tau) a.hard_tau[slot] = -1.0f;
+      continue;
+    }
+    if (stats) atomicAdd(stats, 1u);
+    bool tied = false;
+    if constexpr (KV) {
+      tied = tie == L[K - 1];
+#pragma unroll
+      for (int j = 1; j < K; ++j) tied = tied || L[j] == L[j - 1];
+    }
+    if constexpr (MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST) {
+      float sum = 0.0f;
+#pragma unroll
+      for (int j = 1; j < K; ++j) sum = fadd(sum, __fsqrt_rn(L[j]));
+      a.mean[qi] = fdiv(sum, (float)(K - 1));
+      if constexpr (MODE == TILE_SOR_LIST) {
+        u32 *row = a.sor_list + (size_t)pos * K;
+#pragma unroll
+        for (int j = 0; j < K; ++j) row[j] = tied ? 0xFFFFFFFFu : I[j];
+      }
+    } else if constexpr (MODE == TILE_NORMALS) {
+      float nx, ny, nz;
+      normal_from_keys<K>(a.vx, a.vy, a.vz, L, true, a.iters, q.x, q.y, q.z, a.vpx, a.vpy,
+                          a.vpz, nx, ny, nz);
+      const u64 o = a.out_pos[qi];
+      a.nx[o] = nx;
+      a.ny[o] = ny;
+      a.nz[o] = nz;
+    } else if constexpr (MODE == TILE_PAIRS_F) {
+      if (tied) {  // the exact (d2, index) list from the warp kernel
+        const u32 slot = atomicAdd(a.hard_count, 1u);
+        a.hard[slot] = qi;
+        if (a.hard_tau) a.hard_tau[slot] = L[K - 1];
+      } else {
+#pragma unroll
+        for (int j = 0; j < K; ++j) a.pairs[(size_t)qi * K + j] = pack_nbr(L[j], (int)I[j]);
+        if (a.counts) a.counts[qi] = K;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < K; ++j) a.pairs[(size_t)qi * K + j] = L[j];
+      if (a.counts) a.counts[qi] = K;
+    }
   }
 }
 
@@ -869,13 +1377,42 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
           g, a, g.lbase, a.open_list, a.open_n, qlevel, a.qtau, stats);
     RVP_LAUNCH_CHECK(ctx);
     if (ev) cudaEventRecord(ev[1], ctx->stream);
-    // the per-lane kernels take what is open, from the ring pass on
     a.preset_open = true;
-    a.rfac = 0.0f;
   } else if (a.level_events) {
     // no cooperative pass: a zero-length pair in its slot
     cudaEventRecord(a.level_events[2 * kChainLevels], ctx->stream);
     cudaEventRecord(a.level_events[2 * kChainLevels + 1], ctx->stream);
+  }
+  if (a.coop && a.level0_warp && a.preset_open) {
+    // cooperative mode: what is open (the cooperative pass's leftovers, or
+    // the caller's open queries) goes to the adaptive per-thread kernel,
+    // timed in the first chain slot
+    const unsigned gb = grid_for(a.n_max, 256, ctx->num_sms * 16);
+    k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, g.lbase, a.open_flags);
+    RVP_LAUNCH_CHECK(ctx);
+    exclusive_scan_u32_to_u64(ctx, a.open_flags, a.open_pos, a.n_max, g.n_points, a.scan_tmp);
+    k_open_scatter<<<gb, 256, 0, ctx->stream>>>(a.open_flags, a.open_pos, g.n_points,
+                                                a.open_list, a.open_n);
+    RVP_LAUNCH_CHECK(ctx);
+    if (a.level_events) cudaEventRecord(a.level_events[0], ctx->stream);
+    const int ablocks = ctx->num_sms * 3;
+#define RVP_ADAPT(M) \
+  k_knn_adapt<K, M><<<ablocks, TT, 0, ctx->stream>>>(g, a, a.open_list, a.open_n, stats)
+    if (mode == TILE_SOR_MEAN) RVP_ADAPT(TILE_SOR_MEAN);
+    else if (mode == TILE_SOR_LIST) RVP_ADAPT(TILE_SOR_LIST);
+    else if (mode == TILE_NORMALS) RVP_ADAPT(TILE_NORMALS);
+    else if (mode == TILE_PAIRS_F) RVP_ADAPT(TILE_PAIRS_F);
+    else RVP_ADAPT(TILE_PAIRS);
+#undef RVP_ADAPT
+    RVP_LAUNCH_CHECK(ctx);
+    if (a.level_events) {
+      cudaEventRecord(a.level_events[1], ctx->stream);
+      for (int j = 1; j < kChainLevels; ++j) {  // not run: zero length
+        cudaEventRecord(a.level_events[2 * j], ctx->stream);
+        cudaEventRecord(a.level_events[2 * j + 1], ctx->stream);
+      }
+    }
+    return;
   }
   if (!a.preset_open)
     RVP_CUDA_TRY(cudaMemsetAsync(qlevel, (uint8_t)g.lbase, a.n_max, ctx->stream));
@@ -1008,6 +1545,49 @@ bool normals_from_sor_lists(rvp_context *ctx, const GridView &g, const TileArgs 
     RVP_NSL(8) RVP_NSL(11) RVP_NSL(16) RVP_NSL(17) RVP_NSL(21) RVP_NSL(31) RVP_NSL(32)
     RVP_NSL(33)
 #undef RVP_NSL
+    default: return false;
+  }
+  RVP_LAUNCH_CHECK(ctx);
+  return true;
+}
+
+bool grid_knn_tau(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
+                  const u64 *n_hard, u64 *slot_pairs, int32_t *slot_counts, u32 *stats) {
+  if (g.mode != KEY_DENSE || !a.hard || !a.hard_tau) return false;
+  const int blocks = ctx->num_sms * 3;
+  auto go = [&](auto kc) {
+    constexpr int K = decltype(kc)::value;
+    switch (mode) {
+      case TILE_SOR_MEAN:
+        k_knn_tau<K, TILE_SOR_MEAN><<<blocks, TT, 0, ctx->stream>>>(g, a, n_hard, slot_pairs,
+                                                                    slot_counts, stats);
+        break;
+      case TILE_SOR_LIST:
+        k_knn_tau<K, TILE_SOR_LIST><<<blocks, TT, 0, ctx->stream>>>(g, a, n_hard, slot_pairs,
+                                                                    slot_counts, stats);
+        break;
+      case TILE_NORMALS:
+        k_knn_tau<K, TILE_NORMALS><<<blocks, TT, 0, ctx->stream>>>(g, a, n_hard, slot_pairs,
+                                                                   slot_counts, stats);
+        break;
+      case TILE_PAIRS_F:
+        k_knn_tau<K, TILE_PAIRS_F><<<blocks, TT, 0, ctx->stream>>>(g, a, n_hard, slot_pairs,
+                                                                   slot_counts, stats);
+        break;
+      default:
+        k_knn_tau<K, TILE_PAIRS><<<blocks, TT, 0, ctx->stream>>>(g, a, n_hard, slot_pairs,
+                                                                 slot_counts, stats);
+    }
+  };
+  switch (k) {
+    case 8: go(std::integral_constant<int, 8>()); break;
+    case 11: go(std::integral_constant<int, 11>()); break;
+    case 16: go(std::integral_constant<int, 16>()); break;
+    case 17: go(std::integral_constant<int, 17>()); break;
+    case 21: go(std::integral_constant<int, 21>()); break;
+    case 31: go(std::integral_constant<int, 31>()); break;
+    case 32: go(std::integral_constant<int, 32>()); break;
+    case 33: go(std::integral_constant<int, 33>()); break;
     default: return false;
   }
   RVP_LAUNCH_CHECK(ctx);

@@ -900,6 +900,7 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
                 "kNN tile path unavailable");
     rvp::k_widen32<<<1, 32, 0, st>>>(hard_n, hard_n64);
     RVP_LAUNCH_CHECK(ctx);
+    rvp::grid_knn_tau(ctx, gv, rvp::KF, rvp::TILE_PAIRS_F, ta, hard_n64);
     rvp::QuerySet qh{x, y, z, N, hard_n64, s->frame_of.as<int32_t>(),
                      reinterpret_cast<int32_t *>(hard)};
     qh.bound = hard_tau;

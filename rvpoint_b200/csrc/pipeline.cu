@@ -41,7 +41,7 @@ struct rvp_pipeline {
   rvp::DevBuf sor_aos, sor_x, sor_y, sor_z, sor_offs, sor_frame, sor_src;
   rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
-  rvp::DevBuf stats;  // 16 kNN path counters (diagnostics)
+  rvp::DevBuf stats;  // 20 kNN path counters (diagnostics)
   rvp::DevBuf routed; // SOR queries the cooperative kNN routed to each grid level
   rvp::DevBuf hard;   // queries the tile kernel could not certify (+ counter)
   rvp::DevBuf qlevel; // per grid point: level at which its kNN is still open
@@ -349,6 +349,9 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
       sor_lists = lists;
       k_widen<<<1, 32, 0, st>>>(hard_n, hard_n64);
       RVP_LAUNCH_CHECK(ctx);
+      // the hard queries with a bound: their tight windows, one per thread
+      rvp::grid_knn_tau(ctx, gv, ks, lists ? rvp::TILE_SOR_LIST : rvp::TILE_SOR_MEAN, ta, hard_n64,
+                        nullptr, nullptr, st0 ? st0 + 16 : nullptr);
       rvp::grid_knn(ctx, gv, qh, ks, 0.0f,
                     sor_lists ? reinterpret_cast<u64 *>(p->sor_list.ptr) : nullptr, nullptr, 1,
                     c.block_threads, st0,
@@ -408,6 +411,9 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     }
     k_widen<<<1, 32, 0, st>>>(hard_n, hard_n64);
     RVP_LAUNCH_CHECK(ctx);
+    if (tn_ok)
+      rvp::grid_knn_tau(ctx, gv, kn, rvp::TILE_NORMALS, tn, hard_n64, p->nrm_pairs.as<u64>(),
+                        p->nrm_counts.as<int32_t>(), st0 ? st0 + 17 : nullptr);
     rvp::QuerySet qhn = qh;
     qhn.bound = tn_ok ? hard_tau : nullptr;
     rvp::grid_knn(ctx, gv, qhn, kn, 0.0f, p->nrm_pairs.as<u64>(), p->nrm_counts.as<int32_t>(),
@@ -519,17 +525,17 @@ rvp_status rvp_pipeline_check(rvp_pipeline *p) {
   return RVP_OK;
 }
 
-rvp_status rvp_pipeline_knn_stats(rvp_pipeline *p, int enable, uint32_t *out16) {
+rvp_status rvp_pipeline_knn_stats(rvp_pipeline *p, int enable, uint32_t *out20) {
   if (!p) return RVP_ERR_INVALID_ARG;
   return guard(p->ctx, [&] {
     RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
-    p->stats.reserve(64);
-    if (out16) {
-      RVP_CUDA_TRY(cudaMemcpyAsync(out16, p->stats.ptr, 64, cudaMemcpyDeviceToHost,
+    p->stats.reserve(80);
+    if (out20) {
+      RVP_CUDA_TRY(cudaMemcpyAsync(out20, p->stats.ptr, 80, cudaMemcpyDeviceToHost,
                                    p->ctx->stream));
       RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
     }
-    RVP_CUDA_TRY(cudaMemsetAsync(p->stats.ptr, 0, 64, p->ctx->stream));
+    RVP_CUDA_TRY(cudaMemsetAsync(p->stats.ptr, 0, 80, p->ctx->stream));
     p->stats_on = enable != 0;
   });
 }

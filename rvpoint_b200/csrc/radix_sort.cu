@@ -296,24 +296,67 @@ void radix_sort_pairs(rvp_context *ctx, u64 *keys, u32 *vals, size_t n_max,
 // exclusive scan u32 -> u64 (3 kernels: tile sums, scan of tile sums, apply)
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int SC_TH = 256, SC_IT = 8, SC_TILE = SC_TH * SC_IT;
+// a tile: 256 threads x 16 consecutive items (four 16-byte loads each)
+constexpr int SC_TH = 256, SC_IT = 16, SC_TILE = SC_TH * SC_IT;
 
-__global__ void k_scan_tiles(const u32 *in, size_t n_max, const u64 *n_dev, u64 *tsum) {
+// the thread's 16 items (zero past n): vector loads where the whole run is
+// live and 16-byte aligned
+__device__ __forceinline__ void scan_load(const u32 *in, size_t i0, size_t n, u32 (&v)[SC_IT]) {
+  if (i0 + SC_IT <= n && (reinterpret_cast<uintptr_t>(in + i0) & 15) == 0) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(in + i0);
+#pragma unroll
+    for (int j = 0; j < SC_IT / 4; ++j) {
+      const uint4 t = __ldg(p + j);
+      v[4 * j] = t.x; v[4 * j + 1] = t.y; v[4 * j + 2] = t.z; v[4 * j + 3] = t.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < SC_IT; ++j) v[j] = (i0 + j < n) ? in[i0 + j] : 0u;
+  }
+}
+
+// block-wide exclusive scan of one u64 per thread (warp shuffles, then the
+// warps' totals); returns the exclusive prefix, *total the block's sum
+__device__ __forceinline__ u64 block_exclusive(u64 s, u64 *warp_tot, u64 &total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  u64 incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const u64 t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  u64 before = 0;
+  total = 0;
+#pragma unroll
+  for (int k = 0; k < SC_TH / 32; ++k) {
+    const u64 t = warp_tot[k];
+    if (k < w) before += t;
+    total += t;
+  }
+  return before + incl - s;
+}
+
+__global__ __launch_bounds__(SC_TH) void k_scan_tiles(const u32 *in, size_t n_max,
+                                                      const u64 *n_dev, u64 *tsum) {
   const size_t n = n_dev ? *n_dev : n_max;
   const size_t base = (size_t)blockIdx.x * SC_TILE;
-  u64 s = 0;
-  if (base < n)
-    for (int j = threadIdx.x; j < SC_TILE; j += SC_TH) {
-      const size_t i = base + j;
-      if (i < n) s += in[i];
-    }
+  if (base >= n) return;
+  u32 v[SC_IT];
+  scan_load(in, base + (size_t)threadIdx.x * SC_IT, n, v);
+  u64 s64 = 0;
+#pragma unroll
+  for (int j = 0; j < SC_IT; ++j) s64 += v[j];
   __shared__ u64 sh[SC_TH / 32];
-  u64 v = s;
-  for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  u64 r = s64;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = r;
   __syncthreads();
   if (threadIdx.x == 0) {
     u64 t = 0;
+#pragma unroll
     for (int q = 0; q < SC_TH / 32; ++q) t += sh[q];
     tsum[blockIdx.x] = t;
   }
@@ -346,34 +389,38 @@ __global__ void k_scan_sums(u64 *tsum, size_t nt_max, size_t n_max, const u64 *n
   (void)nt_max;
 }
 
-__global__ void k_scan_apply(const u32 *in, size_t n_max, const u64 *n_dev,
-                             const u64 *tsum, u64 *out) {
+__global__ __launch_bounds__(SC_TH) void k_scan_apply(const u32 *in, size_t n_max,
+                                                      const u64 *n_dev, const u64 *tsum,
+                                                      u64 *out) {
   const size_t n = n_dev ? *n_dev : n_max;
   const size_t base = (size_t)blockIdx.x * SC_TILE;
   if (base >= n) return;
   // thread t owns SC_IT consecutive items
   const size_t i0 = base + (size_t)threadIdx.x * SC_IT;
   u32 v[SC_IT];
+  scan_load(in, i0, n, v);
   u64 s = 0;
 #pragma unroll
-  for (int j = 0; j < SC_IT; ++j) {
-    v[j] = (i0 + j < n) ? in[i0 + j] : 0;
-    s += v[j];
-  }
-  __shared__ u64 sh[SC_TH];
-  sh[threadIdx.x] = s;
-  __syncthreads();
-  for (int off = 1; off < SC_TH; off <<= 1) {
-    u64 t = threadIdx.x >= (unsigned)off ? sh[threadIdx.x - off] : 0;
-    __syncthreads();
-    sh[threadIdx.x] += t;
-    __syncthreads();
-  }
-  u64 run = tsum[blockIdx.x] + sh[threadIdx.x] - s;
+  for (int j = 0; j < SC_IT; ++j) s += v[j];
+  __shared__ u64 warp_tot[SC_TH / 32];
+  u64 total;
+  u64 run = tsum[blockIdx.x] + block_exclusive(s, warp_tot, total);
+  if (i0 + SC_IT <= n && (reinterpret_cast<uintptr_t>(out + i0) & 15) == 0) {
+    ulonglong2 *o = reinterpret_cast<ulonglong2 *>(out + i0);
 #pragma unroll
-  for (int j = 0; j < SC_IT; ++j) {
-    if (i0 + j < n) out[i0 + j] = run;
-    run += v[j];
+    for (int j = 0; j < SC_IT; j += 2) {
+      const u64 a0 = run;
+      run += v[j];
+      const u64 a1 = run;
+      run += v[j + 1];
+      o[j / 2] = make_ulonglong2(a0, a1);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < SC_IT; ++j) {
+      if (i0 + j < n) out[i0 + j] = run;
+      run += v[j];
+    }
   }
 }
 }  // namespace
