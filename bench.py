@@ -436,18 +436,20 @@ def kernel_name(stage: str, coop: bool) -> str:
         return "k_ransac"
     if stage == "sor_knn_coop":
         return "k_knn_coop<17,SOR_LIST> (cells of c)"
+    if coop and stage == "sor_knn_l0":
+        return "k_knn_adapt<17,SOR_LIST> (per-thread windows)"
     cells = {"sor_knn_l0": "c", "sor_knn_l1": "4c", "sor_knn_l2": "16c"}[stage]
     return f"k_knn_wt<17,SOR_LIST> (cells of {cells})"
 
 
-def kernel_units(stage: str, coop: bool, routed, n_vox: int):
-    """Queries one launch of a SOR kNN kernel processes: the cooperative
-    pass, the queries it took; the per-lane kernel on cells of c, every query
-    without the cooperative pass (with it, and on the coarser cells, only the
-    ones left open, a count the line does not carry: not candidates)."""
-    if stage == "sor_knn_coop":
-        return routed if coop else None
-    if stage == "sor_knn_l0" and not coop:
+def kernel_units(stage: str, coop: bool, counts, n_vox: int):
+    """Queries one launch of a SOR kNN kernel processes: in cooperative mode
+    the cooperative pass's and the adaptive kernel's (counts); without it
+    the per-lane kernel on cells of c takes every query (on the coarser
+    cells only the ones left open, a count the line does not carry)."""
+    if coop:
+        return {"sor_knn_coop": counts[0], "sor_knn_l0": counts[1]}.get(stage)
+    if stage == "sor_knn_l0":
         return n_vox
     return None
 
@@ -837,12 +839,13 @@ def main():
     # ---- roofline of the longest kernel timed live (per-level SOR kNN
     # kernels and RANSAC)
     coop = int(pipe.cfg.queries_per_warp) == 3
-    routed = pipe.knn_routed() if coop else None
+    counts = pipe.knn_counts() if coop else None
+    routed = counts[0] if coop else None
     cand = {}
     for k in LEVEL_STAGES + ("ransac",):
         if stages.get(k, 0.0) <= 0.0:
             continue
-        u = None if k == "ransac" else kernel_units(k, coop, routed, n_vox)
+        u = None if k == "ransac" else kernel_units(k, coop, counts, n_vox)
         if k == "ransac" or u:
             cand[k] = u
     dom = max(cand, key=lambda k: stages[k])
@@ -870,7 +873,7 @@ def main():
             "frac": achieved / peak, "traffic": traffic, "kernel": dom_name,
             "stage": dom, "peak_source": peak_src, "queries": cand[dom],
             "algorithmic_bytes_per_launch": alg, "launch_ms": stages[dom],
-            "cooperative_queries": routed}
+            "cooperative_queries": routed, "adaptive_queries": counts[1] if coop else None}
 
     cpu = singles = None
     if world == 1:

@@ -329,9 +329,11 @@ RVP_API rvp_status rvp_pipeline_check(rvp_pipeline *p);
 /* Grid levels of the batched neighbour grid: cells of edge c, 2c, 4c, 8c,
  * 16c (c = the pipeline's cell size). */
 #define RVP_GRID_LEVELS 5
-/* Queries of the SOR kNN the last run's cooperative pass took (points whose
- * own cell holds at least ceil(rfac^2 k) points; queries_per_warp 3; 0
- * otherwise). out[1]. */
+/* Queries of the last run's SOR kNN kernels in cooperative mode
+ * (queries_per_warp 3; zeros otherwise): out[0] the cooperative pass took
+ * (points whose own cell holds at least ceil(rfac^2 k) points), out[1] the
+ * adaptive per-thread kernel took (what the cooperative pass left open).
+ * out[2]. */
 RVP_API rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out);
 /* Diagnostics: enable != 0 makes the kNN kernels count which search path
  * settled each query: out20[0..7] SOR, [8..15] normals (warp-per-query

@@ -793,9 +793,15 @@ class Pipeline:
 
     def knn_routed(self) -> int:
         """SOR kNN queries the last run's cooperative pass took (0 without it)."""
-        out = np.zeros(1, np.uint64)
+        return self.knn_counts()[0]
+
+    def knn_counts(self) -> tuple:
+        """SOR kNN queries of the last run's cooperative pass and of the
+        adaptive per-thread kernel after it (zeros without the cooperative
+        mode)."""
+        out = np.zeros(2, np.uint64)
         check(self.L.rvp_pipeline_knn_routed(self.h, _ptr(out)), self.ctx.h)
-        return int(out[0])
+        return int(out[0]), int(out[1])
 
     def set_timing(self, max_runs: int) -> None:
         check(self.L.rvp_pipeline_set_timing(self.h, int(max_runs)), self.ctx.h)

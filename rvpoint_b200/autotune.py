@@ -47,8 +47,9 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
 
     Two stages: every combination of cell size, kNN kernel mode
     (queries_per_warp: 0 one query per lane at every grid level, 3 a
-    cooperative level-0 pass first), first-pass radius factor and per-lane
-    grid levels at the default block shape; then the block shape of the
+    cooperative pass over dense cells, then one query per thread with its
+    own adaptive window), first-pass radius factor and per-lane grid levels
+    (mode 0 only) at the default block shape; then the block shape of the
     warp-per-query kernel at the best of those."""
     sig = signature(n_points, n_frames, pipe.cfg)
     if cache_file and os.path.exists(cache_file) and not _CACHE:
@@ -61,7 +62,8 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
         _apply(pipe, b)
         return b, []
     leaf = pipe.cfg.leaf_size
-    cells = list(cells) if cells is not None else [leaf * m for m in (3.0, 5.0, 8.0, 10.0, 12.0)]
+    cells = (list(cells) if cells is not None
+             else [leaf * m for m in (3.0, 5.0, 8.0, 10.0, 12.0, 15.0)])
     args = (x, y, z, offsets, n_frames, n_points)
     trials = []
 
@@ -75,10 +77,12 @@ def tune(pipe, x, y, z, offsets, n_frames: int, n_points: int,
             print(f"[autotune] {r}", flush=True)
         return r
 
+    lane_levels = list(lane_levels)
     for c in cells:
         for q in qpws:
             for rf in rfacs:
-                for ll in lane_levels:
+                # the cooperative mode runs no per-lane chain: one level count
+                for ll in (lane_levels[:1] if q == 3 else lane_levels):
                     trial({"cell": c, "block": 0, "qpw": q, "rfac": rf, "lane_levels": ll})
     best = min(trials, key=lambda r: r["ms"])
     for b in blocks:

@@ -158,14 +158,17 @@ __device__ __forceinline__ void atomic_max_f(float *a, float v) {
 struct SortTemp {
   u64 *keys_alt = nullptr;
   u32 *vals_alt = nullptr;
-  u32 *tile_hist = nullptr;    // 256 x tiles(n_max)
-  u32 *global_hist = nullptr;  // 256 digit totals of the current pass
-  int *pass_info = nullptr;    // OR and AND of all keys (2 x u64)
+  u32 *tile_hist = nullptr;    // 256 x tiles(n_max): per-tile digit status words
+  u32 *global_hist = nullptr;  // 8 x 256 digit counts of all keys
+  int *pass_info = nullptr;    // per-pass tile counters
 };
 size_t sort_temp_bytes(size_t n_max);
 void sort_temp_carve(SortTemp &t, void *base, size_t n_max);
 void radix_sort_pairs(rvp_context *ctx, u64 *keys, u32 *vals, size_t n_max,
                       const u64 *n_dev, const SortTemp &t);
+// true once a sort's look-back wait ran out on this device (its output is
+// then wrong); reads a device flag (synchronises the context's stream)
+bool sort_timed_out(rvp_context *ctx);
 
 // exclusive scan of u32/u64 flags -> u64 offsets (scan.cu). n may be on the
 // device. out[n] receives the total. temp: scan_temp_bytes(n_max).
@@ -325,7 +328,7 @@ struct TileArgs {
   bool preset_open;         // qlevel already holds 0 (open) / 0xFF (done) per grid point
   int lane_levels;          // chain levels of the per-lane kernels (1..kChainLevels; 0: all)
   int coop;                 // cooperative passes (k_knn_coop) before the per-lane kernels
-  u64 *routed;              // optional: queries the cooperative pass took
+  u64 *routed;              // optional [2]: queries of the cooperative, adaptive kernels
 };
 // false if k has no tile instantiation (use grid_knn then)
 // Normals of the kept points whose SOR neighbour list (TILE_SOR_LIST, ks per

@@ -1125,18 +1125,20 @@ __global__ __launch_bounds__(TT, 3) void k_knn_tau(GridView g, TileArgs a, const
 // finest chain level whose own cell holds K points (r = cell * sqrt(K /
 // count), under one cell; the top level's cell when none does). Then,
 // repeatedly: the tight window of r at the finest table level where it
-// spans at most kTauCells cells; a count pass over its cells within r (cell
-// box lower bound) -- fewer than K points: r doubles, nothing scanned; more
-// than kTauPoints: the query goes to the warp kernel (lanes over
-// candidates); else a scan bounded by r^2 (every point with d2 <= r^2 lies in
-// the window), exact when it found K such points, else r grows by sqrt 2.
+// spans at most kTauCells cells; from the second attempt on, a count pass
+// over its cells within r (cell box lower bound) -- fewer than K points: r
+// doubles, nothing scanned; more than kTauPoints: the query goes to the warp
+// kernel (lanes over candidates); then a scan bounded by r^2 (every point
+// with d2 <= r^2 lies in the window), exact when it found K such points,
+// else r grows by sqrt 2 (or, past kTauPoints scanned, the warp kernel takes
+// it). Lookups go four at a time (independent table loads in flight).
 // Queries left after kAdaptTries attempts go to the hard list without a
 // bound. Outputs as k_knn_wt's (the SOR mean and list row, the fused
 // normal, or feature pairs; tied lists as there).
 constexpr int kAdaptTries = 8;
 
 template <int K, int MODE>
-__global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
+__global__ __launch_bounds__(TT, 2) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
                                                      const u64 *n_list, u32 *stats) {
   constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
   constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
@@ -1185,37 +1187,40 @@ __global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, con
         punt = true;
         break;
       }
-      u32 total = 0;
-      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
-        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
-          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
-            u32 st, cnt;
-            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) <= tb &&
-                lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt))
-              total += cnt;
-          }
-      if (total < (u32)K) {  // the window cannot hold K points within r
-        r *= 2.0f;
-        continue;
-      }
-      if (total > kTauPoints) {
-        punt = true;
-        break;
+      // the first attempt scans at once (the estimate is mostly generous);
+      // a later one first counts what its window holds within r
+      if (attempt > 0) {
+        u32 total = 0;
+        for_window_cells4(
+            g, F, w,
+            [&](int ux, int uy, int uz) {
+              return cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > tb;
+            },
+            [&](u32, u32 cnt) { total += cnt; });
+        if (total < (u32)K) {  // the window cannot hold K points within r
+          r *= 2.0f;
+          continue;
+        }
+        if (total > kTauPoints) {
+          punt = true;
+          break;
+        }
       }
 #pragma unroll
       for (int j = 0; j < K; ++j) L[j] = kMax;
       Key thr = kMax;
       tie = -1.0f;
-      u32 found = 0;
-      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
-        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
-          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+      u32 found = 0, scanned = 0;
+      for_window_cells4(
+          g, F, w,
+          [&](int ux, int uy, int uz) {
             float thr_d2;
             if constexpr (FKEY) thr_d2 = thr;
             else thr_d2 = nbr_d2(thr);
-            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > fminf(thr_d2, tb)) continue;
-            u32 st, cnt;
-            if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt)) continue;
+            return cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > fminf(thr_d2, tb);
+          },
+          [&](u32 st, u32 cnt) {
+            scanned += cnt;
             for (u32 j = 0; j < cnt; ++j) {
               const float4 p = __ldg(&g.pts[st + j]);
               const u32 pidx = __float_as_uint(p.w);
@@ -1238,8 +1243,9 @@ __global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, con
                 if (key == thr) tie = key;
               }
             }
-          }
+          });
       if (found >= (u32)K) done = true;
+      else if (scanned > kTauPoints) punt = true;  // a dense window: the warp kernel
       else r *= 1.41421356f;
     }
     if (!done) {
@@ -1392,10 +1398,11 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
     RVP_LAUNCH_CHECK(ctx);
     exclusive_scan_u32_to_u64(ctx, a.open_flags, a.open_pos, a.n_max, g.n_points, a.scan_tmp);
     k_open_scatter<<<gb, 256, 0, ctx->stream>>>(a.open_flags, a.open_pos, g.n_points,
-                                                a.open_list, a.open_n);
+                                                a.open_list, a.open_n,
+                                                a.routed ? a.routed + 1 : nullptr);
     RVP_LAUNCH_CHECK(ctx);
     if (a.level_events) cudaEventRecord(a.level_events[0], ctx->stream);
-    const int ablocks = ctx->num_sms * 3;
+    const int ablocks = ctx->num_sms * 2;
 #define RVP_ADAPT(M) \
   k_knn_adapt<K, M><<<ablocks, TT, 0, ctx->stream>>>(g, a, a.open_list, a.open_n, stats)
     if (mode == TILE_SOR_MEAN) RVP_ADAPT(TILE_SOR_MEAN);

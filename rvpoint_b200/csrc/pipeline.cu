@@ -42,7 +42,7 @@ struct rvp_pipeline {
   rvp::DevBuf nrm_pairs, nrm_counts, nx, ny, nz;
   rvp::DevBuf r_model, r_best, r_iters, r_rand;
   rvp::DevBuf stats;  // 20 kNN path counters (diagnostics)
-  rvp::DevBuf routed; // SOR queries the cooperative kNN routed to each grid level
+  rvp::DevBuf routed; // SOR queries of the cooperative and the adaptive kNN kernels
   rvp::DevBuf hard;   // queries the tile kernel could not certify (+ counter)
   rvp::DevBuf qlevel; // per grid point: level at which its kNN is still open
   rvp::DevBuf qtau;   // per grid point: K-th distance bound handed to the next level
@@ -317,7 +317,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     ta.level0_warp = c.queries_per_warp != 2;  // 2: shared-memory tiles instead
     ta.coop = c.queries_per_warp == 3;         // 3: cooperative passes first
     ta.routed = p->routed.as<u64>();
-    if (ta.coop) RVP_CUDA_TRY(cudaMemsetAsync(ta.routed, 0, 8, st));
+    if (ta.coop) RVP_CUDA_TRY(cudaMemsetAsync(ta.routed, 0, 16, st));
     {
       char *op = p->open.as<char>();
       auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
@@ -522,6 +522,13 @@ rvp_status rvp_pipeline_check(rvp_pipeline *p) {
     p->ctx->last_error = "neighbour grid table overflow: refit the tables (rvp_pipeline_fit_tables)";
     return RVP_ERR_CAPACITY;
   }
+  bool sort_to = false;
+  s = guard(p->ctx, [&] { sort_to = rvp::sort_timed_out(p->ctx); });
+  if (s != RVP_OK) return s;
+  if (sort_to) {
+    p->ctx->last_error = "radix sort: a look-back wait ran out (results of that run are wrong)";
+    return RVP_ERR_CUDA;
+  }
   return RVP_OK;
 }
 
@@ -545,10 +552,10 @@ rvp_status rvp_pipeline_knn_routed(rvp_pipeline *p, uint64_t *out) {
   return guard(p->ctx, [&] {
     RVP_CUDA_TRY(cudaSetDevice(p->ctx->device));
     if (!p->routed.ptr) {
-      *out = 0;
+      out[0] = out[1] = 0;
       return;
     }
-    RVP_CUDA_TRY(cudaMemcpyAsync(out, p->routed.ptr, 8, cudaMemcpyDeviceToHost,
+    RVP_CUDA_TRY(cudaMemcpyAsync(out, p->routed.ptr, 16, cudaMemcpyDeviceToHost,
                                  p->ctx->stream));
     RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
   });

@@ -103,13 +103,14 @@ def test_batch_frames_at_tuned_setting(gpu_ctx, bench_frames, bench_oracle):
 
 
 @pytest.mark.parametrize("qpw", [0, 3])
-@pytest.mark.parametrize("cell", [0.3, 0.5, 0.8, 1.0, 1.2])
+@pytest.mark.parametrize("cell", [0.3, 0.5, 0.8, 1.0, 1.2, 1.5])
 @pytest.mark.parametrize("rfac,lane_levels", [(0.7, 3), (1.0, 2)])
 def test_batch_frames_at_every_tuner_setting(gpu_ctx, bench_frames, bench_oracle, cell, rfac,
                                              lane_levels, qpw):
-    """The cells the tuner tries (3, 5, 8, 10, 12 voxel leaves) with both
-    kNN kernel modes (per-lane, cooperative level 0), radius factors and
-    level counts: identical outputs."""
+    """The cells the tuner tries (3, 5, 8, 10, 12, 15 voxel leaves) with both
+    kNN kernel modes (per-lane chain; cooperative pass plus adaptive
+    per-thread windows), radius factors and level counts: identical
+    outputs."""
     from rvpoint_b200 import api
     batch, _ = bench_frames
     p = api.Pipeline(max_points=batch.n, max_frames=batch.n_frames, leaf_size=LEAF, sor_k=SOR_K,
