@@ -601,17 +601,14 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
     t_ptg, (_, bp, it_ptg) = timed(lambda: LR.ransac_frames(be, 10_000, T, targets=tg, ctx=ctx))
     lr = LR.LearnedRansac(scorer)
     cand, coffs = lr.prepare(be)
-    # the feature kNN's kernels: one query per lane, or the cooperative pass
-    # (same features); the faster one serves the learned arm
+    # the feature kNN among each scene's candidates (one block per scene, a
+    # grid of its own in shared memory): its cell size sets only the speed
     knn_modes = {}
-    for cell in (1.0, 1.5, 2.5):
-        for mode, rf in ((0, 1.0), (3, 1.0)):
-            scorer.set_knn(mode, rf)
-            knn_modes[f"cell{cell}_qpw{mode}_rfac{rf}"] = timed(
-                lambda: LR.proposal_features(scorer, be, cand, coffs, cell, lr.scope))[0]
+    for cell in (0.5, 1.0, 1.5, 2.5):
+        knn_modes[f"cell{cell}"] = timed(
+            lambda: LR.proposal_features(scorer, be, cand, coffs, cell, lr.scope))[0]
     best_mode = min(knn_modes, key=knn_modes.get)
-    lr.cell = float(best_mode.split("_")[0][4:])
-    scorer.set_knn(int(best_mode.split("qpw")[1][0]), float(best_mode.split("rfac")[1]))
+    lr.cell = float(best_mode[4:])
     t_l, (_, bl, it_l) = timed(lambda: lr.run(be, cand, coffs, 10_000, T, targets=tg))
     t_f, feat = timed(lambda: LR.proposal_features(scorer, be, cand, coffs, lr.cell, lr.scope))
     t_m, logits = timed(lambda: scorer.forward(feat))

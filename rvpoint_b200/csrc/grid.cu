@@ -647,9 +647,63 @@ __global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int
       const Window w = tight_window(F, qx, qy, qz, (double)radius);
       knn_scan<P>(g, F, f, w, false, qx, qy, qz, K, bound_of(r2), L, found);
     } else {
+      float tb = q.bound ? q.bound[wi] : -1.0f;
+      bool est_done = false;
+      if (tb == kTauEstimate && two_level) {
+        // E) no bound, but a radius estimated from the finest level whose
+        //    own cell holds K points (r = cell * sqrt(K / count), under one
+        //    cell; lanes look the levels up together): the tight window of r
+        //    at the finest level where it spans at most 128 cells, scanned
+        //    bounded by r^2 -- exact when K points lie within r; else r grows
+        //    (by the shortfall) and the window is scanned again
+        tb = -1.0f;  // the rings below, should the estimates run out
+        const int top = g.lbase + kGridLevels - 1;
+        const int fx = cell_axis(qx, F.min_x, F.cell), fy = cell_axis(qy, F.min_y, F.cell),
+                  fz = cell_axis(qz, F.min_z, F.cell);
+        const int lv = g.lbase + lane;
+        u32 ct = 0;
+        if (lv <= top) {
+          u32 st;
+          if (!lookup(g, level_key(g, F, lv, fx >> lv, fy >> lv, fz >> lv), st, ct)) ct = 0;
+        }
+        const unsigned ok = __ballot_sync(0xffffffffu, lv <= top && ct >= (u32)K);
+        const int src = ok ? __ffs(ok) - 1 : 0;
+        const u32 c_src = __shfl_sync(0xffffffffu, ct, src);
+        float r = F.cell * (float)(1 << top);
+        if (ok) {
+          const float cs = F.cell * (float)(1 << (g.lbase + src));
+          r = fminf(cs * sqrtf((float)K / (float)c_src), cs);
+        }
+        for (int attempt = 0; attempt < kEstimateTries && !est_done; ++attempt) {
+          const float t2 = r * r;
+          int lt = -1;
+          Window wt;
+          for (int l = g.lbase; l <= top; ++l) {
+            wt = tight_window(F, qx, qy, qz, sqrt((double)t2), l);
+            if (window_cells(wt) <= 128) {
+              lt = l;
+              break;
+            }
+          }
+          if (lt < 0) break;
+          L.init();
+          found = 0;
+          knn_scan<P>(g, F, f, wt, false, qx, qy, qz, K, bound_of(t2), L, found);
+          if (found >= (u32)K) {
+            est_done = true;
+            path = 0;
+          } else {
+            r *= found > 0 ? fmaxf(1.3f, 1.1f * sqrtf((float)K / (float)found)) : 2.0f;
+          }
+        }
+        if (!est_done) {
+          L.init();
+          found = 0;
+        }
+      }
+      if (!est_done) {
       // 0) a known bound: every point with d2 <= tb lies in the tight window
       //    of sqrt(tb), and there are >= K of them -- scan it directly
-      const float tb = q.bound ? q.bound[wi] : -1.0f;
       Window wr = ring_window(F, qx, qy, qz, 1, g.lbase);
       int lvl = g.lbase;
       if (tb >= 0.0f) {
@@ -700,6 +754,7 @@ __global__ __launch_bounds__(256, 4) void k_knn_warp(GridView g, QuerySet q, int
         knn_scan<P>(g, F, f, wr, true, qx, qy, qz, K, ~0ull - 1, L, found);
         path = 4;
       }
+      }  // !est_done
     }
     const u32 cnt = found < (u32)K ? found : (u32)K;
     if (out_mode == KNN_OUT_SOR_MEAN || out_mode == KNN_OUT_SOR_MEAN_LIST) {

@@ -90,64 +90,6 @@ __device__ __forceinline__ bool lookup(const GridView &g, u64 key, u32 &start, u
   return false;
 }
 
-// Up to four lookups with their first probes in flight together (one
-// thread's cells are independent, so their table loads need not wait for
-// each other); a probe that meets another key continues one slot at a time.
-// Entries u >= m are left empty (count 0).
-__device__ __forceinline__ void lookup4(const GridView &g, const u64 (&key)[4], int m,
-                                        u32 (&start)[4], u32 (&count)[4]) {
-  ulonglong2 e[4];
-  u64 slot[4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    slot[u] = mix64(key[u]) & g.table_mask;
-    e[u] = u < m ? __ldg(&g.table[slot[u]]) : make_ulonglong2(kEmptyKey, 0ull);
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    start[u] = 0;
-    count[u] = 0;
-    u64 probe = 0;
-    while (u < m) {
-      if (e[u].x == key[u]) {
-        start[u] = (u32)(e[u].y & 0xFFFFFFFFull);
-        count[u] = (u32)(e[u].y >> 32);
-        break;
-      }
-      if (e[u].x == kEmptyKey || ++probe > g.table_mask) break;
-      slot[u] = (slot[u] + 1) & g.table_mask;
-      e[u] = __ldg(&g.table[slot[u]]);
-    }
-  }
-}
-
-// Every cell of window w that skip(ux, uy, uz) keeps, looked up four at a
-// time (lookup4), in window order: fn(start, count) for each occupied one.
-template <class Skip, class Fn>
-__device__ __forceinline__ void for_window_cells4(const GridView &g, const GridFrame &F,
-                                                  const Window &w, Skip &&skip, Fn &&fn) {
-  u64 key[4] = {0ull, 0ull, 0ull, 0ull};
-  int m = 0;
-  auto flush = [&]() {
-    u32 st[4], ct[4];
-    lookup4(g, key, m, st, ct);
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (u < m && ct[u]) fn(st[u], ct[u]);
-    m = 0;
-  };
-  for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
-    for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
-      for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
-        if (skip(ux, uy, uz)) continue;
-        const u64 k = level_key(g, F, w.level, ux, uy, uz);
-#pragma unroll
-        for (int u = 0; u < 4; ++u) key[u] = m == u ? k : key[u];  // static indices only
-        if (++m == 4) flush();
-      }
-  if (m) flush();
-}
-
 // Tight window of all cells that can hold a point p with d2(p, q) <= r*r:
 // |p - q| <= r (1 + 3 * 2^-24) per axis for any such p; the bound is padded
 // to r (1 + 1e-6) and rounded outwards, and the cell function is monotone,

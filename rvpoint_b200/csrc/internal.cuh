@@ -158,17 +158,14 @@ __device__ __forceinline__ void atomic_max_f(float *a, float v) {
 struct SortTemp {
   u64 *keys_alt = nullptr;
   u32 *vals_alt = nullptr;
-  u32 *tile_hist = nullptr;    // 256 x tiles(n_max): per-tile digit status words
-  u32 *global_hist = nullptr;  // 8 x 256 digit counts of all keys
-  int *pass_info = nullptr;    // per-pass tile counters
+  u32 *tile_hist = nullptr;    // 256 x tiles(n_max)
+  u32 *global_hist = nullptr;  // 256 digit totals of the current pass
+  int *pass_info = nullptr;    // OR and AND of all keys (2 x u64)
 };
 size_t sort_temp_bytes(size_t n_max);
 void sort_temp_carve(SortTemp &t, void *base, size_t n_max);
 void radix_sort_pairs(rvp_context *ctx, u64 *keys, u32 *vals, size_t n_max,
                       const u64 *n_dev, const SortTemp &t);
-// true once a sort's look-back wait ran out on this device (its output is
-// then wrong); reads a device flag (synchronises the context's stream)
-bool sort_timed_out(rvp_context *ctx);
 
 // exclusive scan of u32/u64 flags -> u64 offsets (scan.cu). n may be on the
 // device. out[n] receives the total. temp: scan_temp_bytes(n_max).
@@ -346,6 +343,12 @@ bool grid_knn_tile(rvp_context *ctx, const GridView &g, int k, int mode, const T
 // slot (slot_pairs / slot_counts, as KNN_OUT_BY_SLOT), pairs by index.
 // False (nothing launched) if k has no instantiation.
 constexpr float kTauDone = -2.0f;
+// a hard slot with hard_tau = kTauEstimate carries no bound: grid_knn
+// estimates a radius from the occupancy of the query's own cells and scans
+// the tight window of it (growing it until K points lie within), before
+// its rings; at most kEstimateTries windows
+constexpr float kTauEstimate = -3.0f;
+constexpr int kEstimateTries = 6;
 bool grid_knn_tau(rvp_context *ctx, const GridView &g, int k, int mode, const TileArgs &a,
                   const u64 *n_hard, u64 *slot_pairs = nullptr, int32_t *slot_counts = nullptr,
                   u32 *stats = nullptr);

@@ -1125,20 +1125,18 @@ __global__ __launch_bounds__(TT, 3) void k_knn_tau(GridView g, TileArgs a, const
 // finest chain level whose own cell holds K points (r = cell * sqrt(K /
 // count), under one cell; the top level's cell when none does). Then,
 // repeatedly: the tight window of r at the finest table level where it
-// spans at most kTauCells cells; from the second attempt on, a count pass
-// over its cells within r (cell box lower bound) -- fewer than K points: r
-// doubles, nothing scanned; more than kTauPoints: the query goes to the warp
-// kernel (lanes over candidates); then a scan bounded by r^2 (every point
-// with d2 <= r^2 lies in the window), exact when it found K such points,
-// else r grows by sqrt 2 (or, past kTauPoints scanned, the warp kernel takes
-// it). Lookups go four at a time (independent table loads in flight).
+// spans at most kTauCells cells; a count pass over its cells within r (cell
+// box lower bound) -- fewer than K points: r doubles, nothing scanned; more
+// than kTauPoints: the query goes to the warp kernel (lanes over
+// candidates); else a scan bounded by r^2 (every point with d2 <= r^2 lies in
+// the window), exact when it found K such points, else r grows by sqrt 2.
 // Queries left after kAdaptTries attempts go to the hard list without a
 // bound. Outputs as k_knn_wt's (the SOR mean and list row, the fused
 // normal, or feature pairs; tied lists as there).
 constexpr int kAdaptTries = 8;
 
 template <int K, int MODE>
-__global__ __launch_bounds__(TT, 2) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
+__global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
                                                      const u64 *n_list, u32 *stats) {
   constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
   constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
@@ -1187,40 +1185,37 @@ __global__ __launch_bounds__(TT, 2) void k_knn_adapt(GridView g, TileArgs a, con
         punt = true;
         break;
       }
-      // the first attempt scans at once (the estimate is mostly generous);
-      // a later one first counts what its window holds within r
-      if (attempt > 0) {
-        u32 total = 0;
-        for_window_cells4(
-            g, F, w,
-            [&](int ux, int uy, int uz) {
-              return cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > tb;
-            },
-            [&](u32, u32 cnt) { total += cnt; });
-        if (total < (u32)K) {  // the window cannot hold K points within r
-          r *= 2.0f;
-          continue;
-        }
-        if (total > kTauPoints) {
-          punt = true;
-          break;
-        }
+      u32 total = 0;
+      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
+        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
+          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+            u32 st, cnt;
+            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) <= tb &&
+                lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt))
+              total += cnt;
+          }
+      if (total < (u32)K) {  // the window cannot hold K points within r
+        r *= 2.0f;
+        continue;
+      }
+      if (total > kTauPoints) {
+        punt = true;
+        break;
       }
 #pragma unroll
       for (int j = 0; j < K; ++j) L[j] = kMax;
       Key thr = kMax;
       tie = -1.0f;
-      u32 found = 0, scanned = 0;
-      for_window_cells4(
-          g, F, w,
-          [&](int ux, int uy, int uz) {
+      u32 found = 0;
+      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
+        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
+          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
             float thr_d2;
             if constexpr (FKEY) thr_d2 = thr;
             else thr_d2 = nbr_d2(thr);
-            return cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > fminf(thr_d2, tb);
-          },
-          [&](u32 st, u32 cnt) {
-            scanned += cnt;
+            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > fminf(thr_d2, tb)) continue;
+            u32 st, cnt;
+            if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt)) continue;
             for (u32 j = 0; j < cnt; ++j) {
               const float4 p = __ldg(&g.pts[st + j]);
               const u32 pidx = __float_as_uint(p.w);
@@ -1243,9 +1238,8 @@ __global__ __launch_bounds__(TT, 2) void k_knn_adapt(GridView g, TileArgs a, con
                 if (key == thr) tie = key;
               }
             }
-          });
+          }
       if (found >= (u32)K) done = true;
-      else if (scanned > kTauPoints) punt = true;  // a dense window: the warp kernel
       else r *= 1.41421356f;
     }
     if (!done) {
@@ -1334,6 +1328,20 @@ __global__ void k_open_scatter(const u32 *flags, const u64 *pos, const u64 *n_de
   }
 }
 
+// the open queries (grid positions) to the hard list without a bound: the
+// warp-per-query kernel estimates their radius (kTauEstimate)
+__global__ void k_open_to_hard(GridView g, const u32 *list, const u64 *n_list, u32 *hard,
+                               u32 *hard_count, float *hard_tau) {
+  const u64 n = *n_list;
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u32 qi = __float_as_uint(g.pts[list[i]].w) & 0x7FFFFFFFu;
+    const u32 slot = atomicAdd(hard_count, 1u);
+    hard[slot] = qi;
+    if (hard_tau) hard_tau[slot] = kTauEstimate;
+  }
+}
+
 template <int K>
 void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_in, int blocks,
               uint8_t *qlevel, u32 *stats) {
@@ -1391,7 +1399,8 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
   }
   if (a.coop && a.level0_warp && a.preset_open) {
     // cooperative mode: what is open (the cooperative pass's leftovers, or
-    // the caller's open queries) goes to the adaptive per-thread kernel,
+    // the caller's open queries) goes to the adaptive per-thread kernel
+    // (normals: to the warp-per-query kernel with an estimated radius),
     // timed in the first chain slot
     const unsigned gb = grid_for(a.n_max, 256, ctx->num_sms * 16);
     k_open_flags<<<gb, 256, 0, ctx->stream>>>(qlevel, g.n_points, g.lbase, a.open_flags);
@@ -1402,15 +1411,23 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
                                                 a.routed ? a.routed + 1 : nullptr);
     RVP_LAUNCH_CHECK(ctx);
     if (a.level_events) cudaEventRecord(a.level_events[0], ctx->stream);
-    const int ablocks = ctx->num_sms * 2;
+    if (mode == TILE_NORMALS && a.hard_tau) {
+      // the normal stage's few open queries sit next to removed points, in
+      // every kind of neighbourhood: the warp-per-query kernel (lanes over
+      // cells and candidates) takes them, with an estimated radius
+      k_open_to_hard<<<gb, 256, 0, ctx->stream>>>(g, a.open_list, a.open_n, a.hard,
+                                                  a.hard_count, a.hard_tau);
+    } else {
+      const int ablocks = ctx->num_sms * 3;
 #define RVP_ADAPT(M) \
   k_knn_adapt<K, M><<<ablocks, TT, 0, ctx->stream>>>(g, a, a.open_list, a.open_n, stats)
-    if (mode == TILE_SOR_MEAN) RVP_ADAPT(TILE_SOR_MEAN);
-    else if (mode == TILE_SOR_LIST) RVP_ADAPT(TILE_SOR_LIST);
-    else if (mode == TILE_NORMALS) RVP_ADAPT(TILE_NORMALS);
-    else if (mode == TILE_PAIRS_F) RVP_ADAPT(TILE_PAIRS_F);
-    else RVP_ADAPT(TILE_PAIRS);
+      if (mode == TILE_SOR_MEAN) RVP_ADAPT(TILE_SOR_MEAN);
+      else if (mode == TILE_SOR_LIST) RVP_ADAPT(TILE_SOR_LIST);
+      else if (mode == TILE_NORMALS) RVP_ADAPT(TILE_NORMALS);
+      else if (mode == TILE_PAIRS_F) RVP_ADAPT(TILE_PAIRS_F);
+      else RVP_ADAPT(TILE_PAIRS);
 #undef RVP_ADAPT
+    }
     RVP_LAUNCH_CHECK(ctx);
     if (a.level_events) {
       cudaEventRecord(a.level_events[1], ctx->stream);

@@ -166,6 +166,215 @@ __global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t 
   }
 }
 
+// Feature neighbourhoods among one scene's candidates (a few thousand
+// points at most): one block per scene keeps its candidates in shared
+// memory, sorted into a small grid of its own (counting sort over at most
+// CK_CELLS cells of at least the given cell size), and every query, one per
+// thread, takes the exact KF nearest by rings of cells around its own cell
+// (the own cell, then shells at Chebyshev distance 1, 2, ...) until the KF-th
+// distance lies inside the covered box (its distance to every face that has
+// cells beyond it, less a rounding slack) or the box covers the grid; the
+// queries go in cell order, so a warp's lanes walk the same cells. Keys
+// are packed (d2, index), so the list is the exact (d2, index) order the
+// grid kNN gives; d2 is computed as there. A scene of more than CK_MAX
+// candidates is searched by brute force over global memory (exact, slow;
+// not reached with the proposal's candidate counts).
+constexpr int CK_MAX = 2048, CK_CELLS = 2048, CK_TH = 256;
+constexpr size_t CK_SMEM = (size_t)CK_MAX * 16 + (size_t)(2 * CK_CELLS + 1) * 4 + CK_MAX * 2;
+
+__device__ __forceinline__ void insert_u64(u64 (&L)[KF], u64 key) {
+#pragma unroll
+  for (int j = KF - 1; j > 0; --j) {
+    const u64 a = L[j - 1], b = L[j];
+    L[j] = key < a ? a : (key < b ? key : b);
+  }
+  L[0] = key < L[0] ? key : L[0];
+}
+
+__global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
+                                                    const float *__restrict__ y,
+                                                    const float *__restrict__ z,
+                                                    const int64_t *offs, int n_frames,
+                                                    float cell, u64 *pairs, int32_t *counts) {
+  extern __shared__ __align__(16) unsigned char ck_smem[];
+  float4 *sp = reinterpret_cast<float4 *>(ck_smem);                // sorted points
+  u32 *cstart = reinterpret_cast<u32 *>(sp + CK_MAX);             // CK_CELLS + 1
+  u32 *cursor = cstart + CK_CELLS + 1;                            // CK_CELLS
+  uint16_t *cellof = reinterpret_cast<uint16_t *>(cursor + CK_CELLS);  // CK_MAX
+  __shared__ float s_bb[3];
+  __shared__ float s_wmn[CK_TH / 32][3], s_wmx[CK_TH / 32][3];
+  __shared__ int s_dim[3];
+  __shared__ float s_cell;
+  const int tid = threadIdx.x;
+  for (int f = blockIdx.x; f < n_frames; f += gridDim.x) {
+    const int64_t a = offs[f], b = offs[f + 1];
+    const int m = (int)(b - a);
+    if (m <= 0) continue;
+    if (m > CK_MAX) {  // brute force over global memory
+      for (int i = tid; i < m; i += CK_TH) {
+        const float qx = x[a + i], qy = y[a + i], qz = z[a + i];
+        u64 L[KF];
+#pragma unroll
+        for (int j = 0; j < KF; ++j) L[j] = ~0ull;
+        for (int t = 0; t < m; ++t) {
+          const u64 key = pack_nbr(dist2(x[a + t], y[a + t], z[a + t], qx, qy, qz), (int)(a + t));
+          if (key < L[KF - 1]) insert_u64(L, key);
+        }
+#pragma unroll
+        for (int j = 0; j < KF; ++j) pairs[(size_t)(a + i) * KF + j] = L[j];
+        counts[a + i] = min(m, KF);
+      }
+      continue;
+    }
+    // bounding box
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = tid; i < m; i += CK_TH) {
+      const float v[3] = {x[a + i], y[a + i], z[a + i]};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        mn[k] = fminf(mn[k], v[k]);
+        mx[k] = fmaxf(mx[k], v[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      for (int o = 16; o; o >>= 1) {
+        mn[k] = fminf(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+        mx[k] = fmaxf(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+      }
+    // the block's min / max through a per-warp table
+    if ((tid & 31) == 0)
+      for (int k = 0; k < 3; ++k) {
+        s_wmn[tid >> 5][k] = mn[k];
+        s_wmx[tid >> 5][k] = mx[k];
+      }
+    __syncthreads();
+    if (tid == 0) {
+      float bmn[3] = {INFINITY, INFINITY, INFINITY}, bmx[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (int w = 0; w < CK_TH / 32; ++w)
+        for (int k = 0; k < 3; ++k) {
+          bmn[k] = fminf(bmn[k], s_wmn[w][k]);
+          bmx[k] = fmaxf(bmx[k], s_wmx[w][k]);
+        }
+      // the grid: cells of at least `cell`, at most CK_CELLS of them
+      float c = cell;
+      int d[3];
+      for (int it = 0; it < 64; ++it) {
+        long long tot = 1;
+        for (int k = 0; k < 3; ++k) {
+          d[k] = (int)floorf((bmx[k] - bmn[k]) / c) + 1;
+          d[k] = max(d[k], 1);
+          tot *= d[k];
+        }
+        if (tot <= CK_CELLS) break;
+        c *= 1.26f;
+      }
+      for (int k = 0; k < 3; ++k) {
+        s_bb[k] = bmn[k];
+        s_dim[k] = d[k];
+      }
+      s_cell = c;
+    }
+    __syncthreads();
+    const float c = s_cell, ic = 1.0f / c;
+    const int GX = s_dim[0], GY = s_dim[1], GZ = s_dim[2];
+    const float mnx = s_bb[0], mny = s_bb[1], mnz = s_bb[2];
+    auto cax = [&](float v, float m0, int G) { return min(max((int)((v - m0) * ic), 0), G - 1); };
+    // counting sort into the cells
+    for (int j = tid; j < CK_CELLS; j += CK_TH) cursor[j] = 0;
+    __syncthreads();
+    for (int i = tid; i < m; i += CK_TH) {
+      const int cid = (cax(z[a + i], mnz, GZ) * GY + cax(y[a + i], mny, GY)) * GX +
+                      cax(x[a + i], mnx, GX);
+      cellof[i] = (uint16_t)cid;
+      atomicAdd(&cursor[cid], 1u);
+    }
+    __syncthreads();
+    if (tid < 32) {  // exclusive scan of the cell counts (one warp)
+      u32 run = 0;
+      for (int base = 0; base < CK_CELLS; base += 32) {
+        const u32 v = cursor[base + tid];
+        u32 incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const u32 t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (tid >= o) incl += t;
+        }
+        cstart[base + tid] = run + incl - v;
+        run += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (tid == 0) cstart[CK_CELLS] = run;
+    }
+    __syncthreads();
+    for (int j = tid; j < CK_CELLS; j += CK_TH) cursor[j] = cstart[j];
+    __syncthreads();
+    for (int i = tid; i < m; i += CK_TH) {
+      const u32 p = atomicAdd(&cursor[cellof[i]], 1u);
+      sp[p] = make_float4(x[a + i], y[a + i], z[a + i], __int_as_float((int)(a + i)));
+    }
+    __syncthreads();
+    // queries, in cell order (the lanes of a warp work on neighbouring
+    // points: the same cells, the same ring counts)
+    for (int i = tid; i < m; i += CK_TH) {
+      const float4 qp = sp[i];
+      const float qx = qp.x, qy = qp.y, qz = qp.z;
+      const int64_t qo = __float_as_int(qp.w);  // its index in the candidate cloud
+      const int cx = cax(qx, mnx, GX), cy = cax(qy, mny, GY), cz = cax(qz, mnz, GZ);
+      u64 L[KF];
+#pragma unroll
+      for (int j = 0; j < KF; ++j) L[j] = ~0ull;
+      int found = 0;
+      // rounding slack of the cell function and the face positions
+      const float sl = 4e-6f * (fabsf(mnx) + fabsf(mny) + fabsf(mnz) + fabsf(qx) + fabsf(qy) +
+                                fabsf(qz) + (float)(GX + GY + GZ + 3) * c) + 1e-6f;
+      for (int r = 0;; ++r) {
+        for (int dz = -r; dz <= r; ++dz) {
+          const int uz = cz + dz;
+          if (uz < 0 || uz >= GZ) continue;
+          for (int dy = -r; dy <= r; ++dy) {
+            const int uy = cy + dy;
+            if (uy < 0 || uy >= GY) continue;
+            const bool edge = dz == -r || dz == r || dy == -r || dy == r;
+            for (int dx = -r; dx <= r; dx += (edge ? 1 : 2 * r)) {
+              const int ux = cx + dx;
+              if (ux >= 0 && ux < GX) {
+                const int cid = (uz * GY + uy) * GX + ux;
+                for (u32 t = cstart[cid]; t < cstart[cid + 1]; ++t) {
+                  const float4 p = sp[t];
+                  const u64 key =
+                      pack_nbr(dist2(p.x, p.y, p.z, qx, qy, qz), __float_as_int(p.w));
+                  ++found;
+                  if (key < L[KF - 1]) insert_u64(L, key);
+                }
+              }
+              if (r == 0) break;
+            }
+          }
+        }
+        // the box of rings 0..r: all points found, or the KF-th inside it
+        const bool all = cx - r <= 0 && cy - r <= 0 && cz - r <= 0 && cx + r >= GX - 1 &&
+                         cy + r >= GY - 1 && cz + r >= GZ - 1;
+        if (all) break;
+        if (found >= KF) {
+          float cov = INFINITY;
+          if (cx - r > 0) cov = fminf(cov, qx - (mnx + (float)(cx - r) * c));
+          if (cx + r < GX - 1) cov = fminf(cov, (mnx + (float)(cx + r + 1) * c) - qx);
+          if (cy - r > 0) cov = fminf(cov, qy - (mny + (float)(cy - r) * c));
+          if (cy + r < GY - 1) cov = fminf(cov, (mny + (float)(cy + r + 1) * c) - qy);
+          if (cz - r > 0) cov = fminf(cov, qz - (mnz + (float)(cz - r) * c));
+          if (cz + r < GZ - 1) cov = fminf(cov, (mnz + (float)(cz + r + 1) * c) - qz);
+          cov -= sl;
+          if (cov > 0.0f && nbr_d2(L[KF - 1]) < cov * cov * (1.0f - 1e-5f)) break;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < KF; ++j) pairs[(size_t)qo * KF + j] = L[j];
+      counts[qo] = min(m, KF);
+    }
+    __syncthreads();  // the shared arrays are reused by the next scene
+  }
+}
+
 __global__ void k_mark_cand(const u32 *cand, size_t n_cand, size_t n, uint8_t *is_cand) {
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n_cand;
        t += (size_t)gridDim.x * blockDim.x)
@@ -919,8 +1128,10 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
                                const int64_t *cand_offsets_dev, size_t n_cand, int neighbours,
                                float *features) {
   if (!s) return RVP_ERR_INVALID_ARG;
-  if (neighbours == 0) return features_impl(s, x, y, z, frame_offsets_dev, n_frames, n_points,
-                                            cell_size, cand, n_cand, features);
+  if (neighbours == 0)  // the batched grid kNN, in the mode rvp_scorer_set_knn chose
+    return features_impl(s, x, y, z, frame_offsets_dev, n_frames, n_points, cell_size, cand,
+                         n_cand, features, 0, s->knn_coop ? s->knn_rfac : 1.0f,
+                         s->knn_coop != 0);
   if (neighbours != 1 || !cand || !cand_offsets_dev) return RVP_ERR_INVALID_ARG;
   // neighbourhoods among the candidates only: their coordinates, frame by
   // frame, become the cloud of the grid search
@@ -936,13 +1147,29 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
     RVP_LAUNCH_CHECK(ctx);
   });
   if (st != RVP_OK) return st;
-  const float *gx = s->cand_xyz.as<float>();
-  // sparse clouds: after one per-lane level the warp kernel is cheaper, and
-  // the first pass bounded by the own cell's occupancy rarely certifies a
-  // query there (it scans the ring at once)
-  return features_impl(s, gx, gx + n_cand, gx + 2 * n_cand, cand_offsets_dev, n_frames, n_cand,
-                       cell_size, nullptr, n_cand, features, 1,
-                       s->knn_coop ? s->knn_rfac : 0.0f, s->knn_coop != 0);
+  // one block per scene: its candidates' neighbourhoods in shared memory
+  // (no global grid, sort or table)
+  return sguard(ctx, [&] {
+    RVP_REQUIRE(cell_size > 0.0f, "cell_size must be > 0");
+    RVP_REQUIRE(n_frames >= 1 && n_frames <= s->max_frames, "n_frames out of range");
+    const float *gx = s->cand_xyz.as<float>();
+    static bool attr[64] = {false};
+    if (ctx->device < 64 && !attr[ctx->device]) {
+      RVP_CUDA_TRY(cudaFuncSetAttribute(rvp::k_cand_knn,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)rvp::CK_SMEM));
+      attr[ctx->device] = true;
+    }
+    const unsigned blocks = (unsigned)std::min(n_frames, ctx->num_sms * 8);
+    rvp::k_cand_knn<<<blocks, rvp::CK_TH, rvp::CK_SMEM, ctx->stream>>>(
+        gx, gx + n_cand, gx + 2 * n_cand, cand_offsets_dev, n_frames, cell_size,
+        s->pairs.as<u64>(), s->counts.as<int32_t>());
+    RVP_LAUNCH_CHECK(ctx);
+    rvp::k_features<<<rvp::grid_for(n_cand, 256, ctx->num_sms * 16), 256, 0, ctx->stream>>>(
+        gx, gx + n_cand, gx + 2 * n_cand, s->pairs.as<u64>(), s->counts.as<int32_t>(), nullptr,
+        n_cand, n_cand, features);
+    RVP_LAUNCH_CHECK(ctx);
+  });
 }
 
 rvp_status rvp_scorer_set_knn(rvp_scorer *s, int queries_per_warp, float rfac) {

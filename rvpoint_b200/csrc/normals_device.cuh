@@ -12,53 +12,46 @@
 namespace rvp {
 namespace nd {
 
+// One Jacobi rotation of the reference's loop body on the pair (P, Q), with
+// every index static so that A and V stay in registers.
+template <int P, int Q>
+__device__ __forceinline__ void jacobi_rotate_ref(float (&A)[3][3], float (&V)[3][3]) {
+  const float app = A[P][P], aqq = A[Q][Q], apq = A[P][Q];
+  const float phi = fmul(0.5f, atan2f(fmul(2.0f, apq), fsub(app, aqq)));
+  const float c = cosf(phi), s = sinf(phi);
+  const float cc = fmul(c, c), ss = fmul(s, s), s2c = fmul(fmul(2.0f, s), c);
+  // c*c*app - 2*s*c*apq + s*s*aqq ; s*s*app + 2*s*c*apq + c*c*aqq
+  A[P][P] = fadd(fsub(fmul(cc, app), fmul(s2c, apq)), fmul(ss, aqq));
+  A[Q][Q] = fadd(fadd(fmul(ss, app), fmul(s2c, apq)), fmul(cc, aqq));
+  A[P][Q] = 0.0f;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const float vip = V[r][P], viq = V[r][Q];
+    V[r][P] = fsub(fmul(c, vip), fmul(s, viq));
+    V[r][Q] = fadd(fmul(s, vip), fmul(c, viq));
+  }
+}
+
 // The reference's Jacobi loop: each iteration rotates the pair with the
 // largest upper off-diagonal |A[p][q]| (first of equals), which it reads from
-// the upper triangle only; the lower triangle is never read. The pair is
-// picked by selects, not branches (lanes of a warp pick different pairs), so
-// each iteration evaluates one angle and one rotation per lane; the
-// arithmetic on the picked values is the reference's.
+// the upper triangle only; the lower triangle is never read.
 __device__ __forceinline__ void eigen_smallest_ref(float A[3][3], int iters, float &nx, float &ny, float &nz) {
-  float m00 = A[0][0], m11 = A[1][1], m22 = A[2][2];
-  float m01 = A[0][1], m02 = A[0][2], m12 = A[1][2];
+  float (&M)[3][3] = *reinterpret_cast<float (*)[3][3]>(A);
   float V[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
   for (int it = 0; it < iters; ++it) {
-    // 0: (0,1), 1: (0,2), 2: (1,2)
-    int pq = 0;
-    float max_off = fabsf(m01);
-    if (fabsf(m02) > max_off) { pq = 1; max_off = fabsf(m02); }
-    if (fabsf(m12) > max_off) pq = 2;
-    const float app = pq == 2 ? m11 : m00;
-    const float aqq = pq == 0 ? m11 : m22;
-    const float apq = pq == 0 ? m01 : (pq == 1 ? m02 : m12);
-    const float phi = fmul(0.5f, atan2f(fmul(2.0f, apq), fsub(app, aqq)));
-    float s, c;
-    sincosf(phi, &s, &c);
-    const float cc = fmul(c, c), ss = fmul(s, s), s2c = fmul(fmul(2.0f, s), c);
-    // c*c*app - 2*s*c*apq + s*s*aqq ; s*s*app + 2*s*c*apq + c*c*aqq
-    const float npp = fadd(fsub(fmul(cc, app), fmul(s2c, apq)), fmul(ss, aqq));
-    const float nqq = fadd(fadd(fmul(ss, app), fmul(s2c, apq)), fmul(cc, aqq));
-    m00 = pq != 2 ? npp : m00;
-    m11 = pq == 2 ? npp : (pq == 0 ? nqq : m11);
-    m22 = pq != 0 ? nqq : m22;
-    m01 = pq == 0 ? 0.0f : m01;
-    m02 = pq == 1 ? 0.0f : m02;
-    m12 = pq == 2 ? 0.0f : m12;
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      const float vip = pq == 2 ? V[r][1] : V[r][0];
-      const float viq = pq == 0 ? V[r][1] : V[r][2];
-      const float np = fsub(fmul(c, vip), fmul(s, viq));
-      const float nq = fadd(fmul(s, vip), fmul(c, viq));
-      V[r][0] = pq != 2 ? np : V[r][0];
-      V[r][1] = pq == 2 ? np : (pq == 0 ? nq : V[r][1]);
-      V[r][2] = pq != 0 ? nq : V[r][2];
-    }
+    int pq = 0;  // 0: (0,1), 1: (0,2), 2: (1,2)
+    float max_off = fabsf(M[0][1]);
+    if (fabsf(M[0][2]) > max_off) { pq = 1; max_off = fabsf(M[0][2]); }
+    if (fabsf(M[1][2]) > max_off) pq = 2;
+    if (pq == 0) jacobi_rotate_ref<0, 1>(M, V);
+    else if (pq == 1) jacobi_rotate_ref<0, 2>(M, V);
+    else jacobi_rotate_ref<1, 2>(M, V);
   }
+  float d0 = M[0][0], d1 = M[1][1], d2 = M[2][2];
   int m = 0;
-  float dm = m00;
-  if (m11 < dm) { m = 1; dm = m11; }
-  if (m22 < dm) m = 2;
+  float dm = d0;
+  if (d1 < dm) { m = 1; dm = d1; }
+  if (d2 < dm) m = 2;
   nx = m == 0 ? V[0][0] : (m == 1 ? V[0][1] : V[0][2]);
   ny = m == 0 ? V[1][0] : (m == 1 ? V[1][1] : V[1][2]);
   nz = m == 0 ? V[2][0] : (m == 1 ? V[2][1] : V[2][2]);

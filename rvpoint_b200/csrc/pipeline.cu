@@ -522,13 +522,6 @@ rvp_status rvp_pipeline_check(rvp_pipeline *p) {
     p->ctx->last_error = "neighbour grid table overflow: refit the tables (rvp_pipeline_fit_tables)";
     return RVP_ERR_CAPACITY;
   }
-  bool sort_to = false;
-  s = guard(p->ctx, [&] { sort_to = rvp::sort_timed_out(p->ctx); });
-  if (s != RVP_OK) return s;
-  if (sort_to) {
-    p->ctx->last_error = "radix sort: a look-back wait ran out (results of that run are wrong)";
-    return RVP_ERR_CUDA;
-  }
   return RVP_OK;
 }
 

@@ -1,20 +1,11 @@
-// Stable LSD radix sort of (u64 key, u32 value) pairs for sm_100a, one
-// kernel per 8-bit digit (single-pass "onesweep" style).
+// Stable LSD radix sort of (u64 key, u32 value) pairs for sm_100a.
 //
-// First one kernel counts all eight digits of every key (8 x 256 global
-// counters, warp-aggregated with __match_any_sync). A digit is live unless
-// one value holds all n keys; dead digits cost nothing, so a 64-bit key with
-// 30 live bits costs 4 passes. Each pass then takes tiles of 4096 keys in
-// the order its blocks start (a tile id from an atomic counter, so every
-// tile a block waits for has started), ranks the tile's keys stably in
-// registers and shared memory (per-warp __match_any_sync counts), publishes
-// its per-digit counts, and finds the keys before it in earlier tiles by
-// looking back over their published counts and prefixes (decoupled
-// look-back; every wait is bounded, and a wait that runs out sets an error
-// flag instead of hanging). The tile is reordered in shared memory and
-// written out one digit run at a time (coalesced). The key count lives in
-// device memory and nothing returns to the host, so a sort can sit in a
-// graph.
+// Per live 8-bit digit: (1) tile histogram, (2) per-digit scan over tiles,
+// (3) tile-local stable ranking with __match_any_sync, reorder in shared
+// memory, coalesced scatter of each digit run. A digit is live when the keys
+// differ in it (global OR ^ AND of all keys), so a 64-bit key with 30 live
+// bits costs 4 passes. Pass kernels read the key count and the live mask from
+// device memory; nothing returns to the host, so a sort can sit in a graph.
 #include "internal.cuh"
 
 namespace rvp {
@@ -25,81 +16,145 @@ constexpr int ITEMS = 16;
 constexpr int TILE = TH * ITEMS;  // 4096 keys per tile
 constexpr int WARPS = TH / 32;
 constexpr int CHUNK = TILE / WARPS;  // 512 keys per warp, in order
-// tile status word: flag in the top two bits, a count below
-constexpr u32 ST_AGG = 1u << 30, ST_PRE = 2u << 30, ST_VAL = (1u << 30) - 1;
-constexpr int SPIN_LIMIT = 1 << 21;  // look-back polls of one status word
-__device__ int g_sort_timeout;       // a look-back wait ran out (results wrong)
 
 __host__ __device__ inline size_t tiles_for(size_t n) { return (n + TILE - 1) / TILE; }
 
 inline size_t al(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// the eight digit histograms of all keys (ghist[pass * 256 + digit])
-__global__ __launch_bounds__(TH) void k_digit_hist(const u64 *__restrict__ keys, size_t n_max,
-                                                   const u64 *__restrict__ n_dev, u32 *ghist) {
-  __shared__ u32 h[8][256];
-  for (int j = threadIdx.x; j < 8 * 256; j += TH) (&h[0][0])[j] = 0;
-  __syncthreads();
+__device__ __forceinline__ u64 live_mask(const u64 *orand) {
+  return orand[0] ^ orand[1];
+}
+__device__ __forceinline__ bool pass_live(u64 live, int pass) {
+  return ((live >> (8 * pass)) & 0xFFull) != 0;
+}
+// buffer holding the input of `pass`: parity of live passes below it
+__device__ __forceinline__ int pass_src(u64 live, int pass) {
+  int c = 0;
+  for (int q = 0; q < pass; ++q) c += pass_live(live, q) ? 1 : 0;
+  return c & 1;
+}
+
+__global__ void k_orand(const u64 *__restrict__ keys, size_t n_max,
+                        const u64 *__restrict__ n_dev, u64 *orand) {
   const size_t n = n_dev ? *n_dev : n_max;
-  const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1;
-  const size_t stride = (size_t)gridDim.x * TH;
-  for (size_t i0 = (size_t)blockIdx.x * TH + (threadIdx.x & ~31); i0 < n; i0 += stride) {
-    const size_t i = i0 + lane;
+  u64 o = 0, a = ~0ull;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const u64 k = keys[i];
+    o |= k;
+    a &= k;
+  }
+  unsigned olo = __reduce_or_sync(0xffffffffu, (unsigned)o);
+  unsigned ohi = __reduce_or_sync(0xffffffffu, (unsigned)(o >> 32));
+  unsigned alo = __reduce_and_sync(0xffffffffu, (unsigned)a);
+  unsigned ahi = __reduce_and_sync(0xffffffffu, (unsigned)(a >> 32));
+  if ((threadIdx.x & 31) == 0) {
+    atomicOr(&orand[0], ((u64)ohi << 32) | olo);
+    atomicAnd(&orand[1], ((u64)ahi << 32) | alo);
+  }
+}
+
+__global__ __launch_bounds__(TH) void k_hist(const u64 *k0, const u64 *k1,
+                                            size_t n_max, const u64 *n_dev,
+                                            const u64 *orand, int pass,
+                                            u32 *tile_hist, size_t t_max) {
+  const u64 live = live_mask(orand);
+  if (!pass_live(live, pass)) return;
+  const u64 *kin = pass_src(live, pass) ? k1 : k0;
+  const size_t n = n_dev ? *n_dev : n_max;
+  const size_t base = (size_t)blockIdx.x * TILE;
+  if (base >= n) return;
+  __shared__ u32 h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int shift = 8 * pass;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r = 0; r < ITEMS; ++r) {
+    const size_t i = base + (size_t)w * CHUNK + (size_t)r * 32 + lane;
     const bool valid = i < n;
     const unsigned vm = __ballot_sync(0xffffffffu, valid);
     if (valid) {
-      const u64 k = keys[i];
-#pragma unroll
-      for (int p = 0; p < 8; ++p) {
-        const unsigned d = (unsigned)((k >> (8 * p)) & 0xFF);
-        const unsigned m = __match_any_sync(vm, d);
-        if ((m & lt) == 0) atomicAdd(&h[p][d], __popc(m));
-      }
+      const unsigned d = (unsigned)((kin[i] >> shift) & 0xFF);
+      const unsigned m = __match_any_sync(vm, d);
+      if ((m & ((1u << lane) - 1)) == 0) atomicAdd(&h[d], __popc(m));
     }
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < 8 * 256; j += TH) {
-    const u32 c = (&h[0][0])[j];
-    if (c) atomicAdd(&ghist[j], c);
-  }
+  tile_hist[(size_t)threadIdx.x * t_max + blockIdx.x] = h[threadIdx.x];
 }
 
-// pass p is live unless one digit value holds all n keys (all 256 threads
-// of the block call it)
-__device__ __forceinline__ bool pass_live_dev(const u32 *ghist, int pass, u32 n) {
-  return !__syncthreads_or(ghist[pass * 256 + threadIdx.x] == n);
-}
-
-__global__ __launch_bounds__(TH) void k_onesweep(u64 *k0, u32 *v0, u64 *k1, u32 *v1,
-                                                size_t n_max, const u64 *n_dev,
-                                                const u32 *ghist, int pass, u32 *status,
-                                                u32 *tile_counter) {
+// block d: exclusive scan over the live tiles of digit d, in place; totals[d].
+__global__ __launch_bounds__(TH) void k_scan_digit(u32 *tile_hist, size_t t_max,
+                                                  size_t n_max, const u64 *n_dev,
+                                                  const u64 *orand, int pass,
+                                                  u32 *totals) {
+  if (!pass_live(live_mask(orand), pass)) return;
   const size_t n = n_dev ? *n_dev : n_max;
-  if (n == 0) return;
-  // live passes below this one decide which buffer holds its input
-  int src = 0;
-  for (int q = 0; q < pass; ++q) src ^= pass_live_dev(ghist, q, (u32)n) ? 1 : 0;
-  if (!pass_live_dev(ghist, pass, (u32)n)) return;
+  const size_t T = tiles_for(n);
+  u32 *row = tile_hist + (size_t)blockIdx.x * t_max;
+  const size_t per = (T + TH - 1) / TH;
+  const size_t a = threadIdx.x * per;
+  const size_t b = a + per < T ? a + per : T;
+  u32 s = 0;
+  for (size_t t = a; t < b; ++t) s += row[t];
+  __shared__ u32 sh[TH];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int off = 1; off < TH; off <<= 1) {
+    u32 v = threadIdx.x >= off ? sh[threadIdx.x - off] : 0;
+    __syncthreads();
+    sh[threadIdx.x] += v;
+    __syncthreads();
+  }
+  u32 run = sh[threadIdx.x] - s;
+  for (size_t t = a; t < b; ++t) {
+    const u32 c = row[t];
+    row[t] = run;
+    run += c;
+  }
+  if (threadIdx.x == TH - 1) totals[blockIdx.x] = sh[TH - 1];
+}
+
+__global__ __launch_bounds__(TH) void k_scatter(u64 *k0, u32 *v0, u64 *k1, u32 *v1,
+                                               size_t n_max, const u64 *n_dev,
+                                               const u64 *orand, int pass,
+                                               const u32 *tile_scan, size_t t_max,
+                                               const u32 *totals) {
+  const u64 live = live_mask(orand);
+  if (!pass_live(live, pass)) return;
+  const int src = pass_src(live, pass);
   const u64 *kin = src ? k1 : k0;
   const u32 *vin = src ? v1 : v0;
   u64 *kout = src ? k0 : k1;
   u32 *vout = src ? v0 : v1;
+  const size_t n = n_dev ? *n_dev : n_max;
+  const size_t base = (size_t)blockIdx.x * TILE;
+  if (base >= n) return;
 
   extern __shared__ __align__(16) unsigned char smem[];
-  u64 *skeys = reinterpret_cast<u64 *>(smem);          // TILE
-  u32 *svals = reinterpret_cast<u32 *>(skeys + TILE);  // TILE
-  u32 *wh = svals + TILE;                              // WARPS * 256
-  u32 *dstart = wh + WARPS * 256;                      // 256: tile-local digit starts
-  u32 *gbase = dstart + 256;                           // 256: global start of the tile's run
-  __shared__ u32 s_tile;
+  u64 *skeys = reinterpret_cast<u64 *>(smem);                 // TILE
+  u32 *svals = reinterpret_cast<u32 *>(skeys + TILE);         // TILE
+  u32 *wh = svals + TILE;                                     // WARPS*256
+  u32 *dstart = wh + WARPS * 256;                             // 256
+  u32 *gbase = dstart + 256;                                  // 256
+
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-  if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
   for (int j = tid; j < WARPS * 256; j += TH) wh[j] = 0;
+  // digit bases over the whole key set: exclusive scan of totals
+  {
+    u32 t = totals[tid];
+    dstart[tid] = t;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {
+      u32 v = tid >= off ? dstart[tid - off] : 0;
+      __syncthreads();
+      dstart[tid] += v;
+      __syncthreads();
+    }
+    gbase[tid] = dstart[tid] - t + tile_scan[(size_t)tid * t_max + blockIdx.x];
+  }
   __syncthreads();
-  const u32 tile = s_tile;
-  const size_t base = (size_t)tile * TILE;
-  if (base >= n) return;  // (block-uniform)
+
   const int shift = 8 * pass;
   const unsigned lt = (1u << lane) - 1;
   u64 key[ITEMS];
@@ -112,7 +167,6 @@ __global__ __launch_bounds__(TH) void k_onesweep(u64 *k0, u32 *v0, u64 *k1, u32 
     key[r] = valid ? kin[i] : 0;
     val[r] = valid ? vin[i] : 0;
   }
-  // stable ranks inside each warp's chunk, counts per warp and digit
 #pragma unroll
   for (int r = 0; r < ITEMS; ++r) {
     const size_t i = base + (size_t)w * CHUNK + (size_t)r * 32 + lane;
@@ -130,64 +184,23 @@ __global__ __launch_bounds__(TH) void k_onesweep(u64 *k0, u32 *v0, u64 *k1, u32 
     __syncwarp();
   }
   __syncthreads();
-  // thread tid = digit: exclusive over warps; the tile's count of the digit
-  u32 cnt = 0;
-  for (int q = 0; q < WARPS; ++q) {
-    const u32 c = wh[q * 256 + tid];
-    wh[q * 256 + tid] = cnt;
-    cnt += c;
-  }
-  // publish this tile's count, then look back for the keys of this digit in
-  // earlier tiles
-  volatile u32 *st = status;
-  st[(size_t)tile * 256 + tid] = (tile == 0 ? ST_PRE : ST_AGG) | cnt;
-  u32 before = 0;
-  if (tile > 0) {
-    long long t = (long long)tile - 1;
-    int spins = 0;
-    while (t >= 0) {
-      const u32 v = st[(size_t)t * 256 + tid];
-      if (v & ST_PRE) {
-        before += v & ST_VAL;
-        break;
-      }
-      if (v & ST_AGG) {
-        before += v & ST_VAL;
-        --t;
-        continue;
-      }
-      if (++spins > SPIN_LIMIT) {  // never published: give up, flag it
-        g_sort_timeout = 1;
-        break;
-      }
-      __nanosleep(64);
+  {  // per digit: exclusive over warps, then tile-local digit starts
+    u32 run = 0;
+    for (int q = 0; q < WARPS; ++q) {
+      const u32 c = wh[q * 256 + tid];
+      wh[q * 256 + tid] = run;
+      run += c;
     }
-    st[(size_t)tile * 256 + tid] = ST_PRE | (before + cnt);
-  }
-  // global start of this tile's run of the digit: keys of smaller digits
-  // (exclusive prefix of the digit counts) plus this digit's earlier keys
-  {
-    const u32 t_all = ghist[pass * 256 + tid];
-    dstart[tid] = t_all;
+    __syncthreads();
+    dstart[tid] = run;
     __syncthreads();
     for (int off = 1; off < 256; off <<= 1) {
-      const u32 v = tid >= off ? dstart[tid - off] : 0;
+      u32 v = tid >= off ? dstart[tid - off] : 0;
       __syncthreads();
       dstart[tid] += v;
       __syncthreads();
     }
-    gbase[tid] = dstart[tid] - t_all + before;
-    __syncthreads();
-    // tile-local digit starts: exclusive prefix of the tile's counts
-    dstart[tid] = cnt;
-    __syncthreads();
-    for (int off = 1; off < 256; off <<= 1) {
-      const u32 v = tid >= off ? dstart[tid - off] : 0;
-      __syncthreads();
-      dstart[tid] += v;
-      __syncthreads();
-    }
-    dstart[tid] -= cnt;
+    dstart[tid] -= run;
   }
   __syncthreads();
 #pragma unroll
@@ -201,8 +214,8 @@ __global__ __launch_bounds__(TH) void k_onesweep(u64 *k0, u32 *v0, u64 *k1, u32 
     }
   }
   __syncthreads();
-  const size_t c_all = (n - base) < (size_t)TILE ? (n - base) : (size_t)TILE;
-  for (int j = tid; j < (int)c_all; j += TH) {
+  const size_t cnt = (n - base) < (size_t)TILE ? (n - base) : (size_t)TILE;
+  for (int j = tid; j < (int)cnt; j += TH) {
     const u64 k = skeys[j];
     const unsigned d = (unsigned)((k >> shift) & 0xFF);
     const size_t dst = (size_t)gbase[d] + (size_t)(j - (int)dstart[d]);
@@ -211,13 +224,13 @@ __global__ __launch_bounds__(TH) void k_onesweep(u64 *k0, u32 *v0, u64 *k1, u32 
   }
 }
 
-__global__ void k_copy_back(u64 *k0, u32 *v0, const u64 *k1, const u32 *v1, size_t n_max,
-                            const u64 *n_dev, const u32 *ghist) {
-  const size_t n = n_dev ? *n_dev : n_max;
-  if (n == 0) return;
+__global__ void k_copy_back(u64 *k0, u32 *v0, const u64 *k1, const u32 *v1,
+                            size_t n_max, const u64 *n_dev, const u64 *orand) {
+  const u64 live = live_mask(orand);
   int c = 0;
-  for (int q = 0; q < 8; ++q) c ^= pass_live_dev(ghist, q, (u32)n) ? 1 : 0;
-  if (c == 0) return;
+  for (int q = 0; q < 8; ++q) c += pass_live(live, q) ? 1 : 0;
+  if ((c & 1) == 0) return;
+  const size_t n = n_dev ? *n_dev : n_max;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     k0[i] = k1[i];
@@ -225,13 +238,13 @@ __global__ void k_copy_back(u64 *k0, u32 *v0, const u64 *k1, const u32 *v1, size
   }
 }
 
-constexpr size_t kSweepSmem =
+constexpr size_t kScatterSmem =
     (size_t)TILE * 8 + (size_t)TILE * 4 + (size_t)WARPS * 256 * 4 + 256 * 4 * 2;
 }  // namespace
 
 size_t sort_temp_bytes(size_t n_max) {
   const size_t T = tiles_for(n_max) > 0 ? tiles_for(n_max) : 1;
-  return al(n_max * 8) + al(n_max * 4) + al(256 * T * 4) + al(8 * 256 * 4) + al(64);
+  return al(n_max * 8) + al(n_max * 4) + al(256 * T * 4) + al(256 * 4) + al(64);
 }
 
 void sort_temp_carve(SortTemp &t, void *base, size_t n_max) {
@@ -239,47 +252,44 @@ void sort_temp_carve(SortTemp &t, void *base, size_t n_max) {
   char *p = static_cast<char *>(base);
   t.keys_alt = reinterpret_cast<u64 *>(p); p += al(n_max * 8);
   t.vals_alt = reinterpret_cast<u32 *>(p); p += al(n_max * 4);
-  t.tile_hist = reinterpret_cast<u32 *>(p); p += al(256 * T * 4);   // tile status words
-  t.global_hist = reinterpret_cast<u32 *>(p); p += al(8 * 256 * 4);  // digit counts
-  t.pass_info = reinterpret_cast<int *>(p);                          // 8 tile counters
+  t.tile_hist = reinterpret_cast<u32 *>(p); p += al(256 * T * 4);
+  t.global_hist = reinterpret_cast<u32 *>(p); p += al(256 * 4);  // digit totals
+  t.pass_info = reinterpret_cast<int *>(p);                      // or/and words
 }
 
 void radix_sort_pairs(rvp_context *ctx, u64 *keys, u32 *vals, size_t n_max,
                       const u64 *n_dev, const SortTemp &t) {
   if (n_max == 0) return;
-  RVP_REQUIRE(n_max < ST_VAL, "radix sort: more than 2^30 - 1 keys");
   static bool attr_set[64] = {false};
   int dev = ctx->device;
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    RVP_CUDA_TRY(cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSweepSmem));
+    RVP_CUDA_TRY(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kScatterSmem));
     attr_set[dev] = true;
   }
   const size_t T = tiles_for(n_max);
-  u32 *counters = reinterpret_cast<u32 *>(t.pass_info);
-  RVP_CUDA_TRY(cudaMemsetAsync(t.global_hist, 0, 8 * 256 * 4, ctx->stream));
-  RVP_CUDA_TRY(cudaMemsetAsync(counters, 0, 8 * 4, ctx->stream));
-  k_digit_hist<<<grid_for(n_max, TH, ctx->num_sms * 4), TH, 0, ctx->stream>>>(keys, n_max, n_dev,
-                                                                              t.global_hist);
+  u64 *orand = reinterpret_cast<u64 *>(t.pass_info);
+  RVP_CUDA_TRY(cudaMemsetAsync(orand, 0x00, 8, ctx->stream));
+  RVP_CUDA_TRY(cudaMemsetAsync(orand + 1, 0xFF, 8, ctx->stream));
+  k_orand<<<grid_for(n_max, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(keys, n_max, n_dev,
+                                                                           orand);
   RVP_LAUNCH_CHECK(ctx);
   for (int pass = 0; pass < 8; ++pass) {
-    RVP_CUDA_TRY(cudaMemsetAsync(t.tile_hist, 0, T * 256 * 4, ctx->stream));
-    k_onesweep<<<(unsigned)T, TH, kSweepSmem, ctx->stream>>>(keys, vals, t.keys_alt, t.vals_alt,
-                                                             n_max, n_dev, t.global_hist, pass,
-                                                             t.tile_hist, counters + pass);
+    k_hist<<<(unsigned)T, TH, 0, ctx->stream>>>(keys, t.keys_alt, n_max, n_dev, orand, pass,
+                                                t.tile_hist, T);
+    RVP_LAUNCH_CHECK(ctx);
+    k_scan_digit<<<256, TH, 0, ctx->stream>>>(t.tile_hist, T, n_max, n_dev, orand, pass,
+                                             t.global_hist);
+    RVP_LAUNCH_CHECK(ctx);
+    k_scatter<<<(unsigned)T, TH, kScatterSmem, ctx->stream>>>(keys, vals, t.keys_alt,
+                                                             t.vals_alt, n_max, n_dev, orand,
+                                                             pass, t.tile_hist, T,
+                                                             t.global_hist);
     RVP_LAUNCH_CHECK(ctx);
   }
   k_copy_back<<<grid_for(n_max, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
-      keys, vals, t.keys_alt, t.vals_alt, n_max, n_dev, t.global_hist);
+      keys, vals, t.keys_alt, t.vals_alt, n_max, n_dev, orand);
   RVP_LAUNCH_CHECK(ctx);
-}
-
-bool sort_timed_out(rvp_context *ctx) {
-  int v = 0;
-  RVP_CUDA_TRY(cudaMemcpyFromSymbolAsync(&v, g_sort_timeout, sizeof(int), 0,
-                                         cudaMemcpyDeviceToHost, ctx->stream));
-  RVP_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  return v != 0;
 }
 
 // ---------------------------------------------------------------------------

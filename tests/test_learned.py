@@ -198,17 +198,20 @@ def test_features_among_candidates_equal_features_of_their_subcloud(gpu_ctx):
     s = PlaneScorer(b.n, 3, ctx=gpu_ctx)
     cand = torch.from_numpy(cand_h.view(np.int32)).cuda()
     coffs = torch.from_numpy(coffs_h).cuda()
-    f1 = s.features(b, 1.0, cand, coffs, among_candidates=True).cpu().numpy()
-    f2 = s.features(DeviceBatch.from_host(sub), 1.0).cpu().numpy()
-    assert np.array_equal(f1.view(np.int32), f2.view(np.int32))
-    # the cooperative first pass of the kNN finds the same neighbours
+    sb = DeviceBatch.from_host(sub)
+    f2 = s.features(sb, 1.0).cpu().numpy()
+    # among the candidates: one block per scene, its own grid in shared memory
+    for cell in (0.5, 1.0, 2.5):
+        f1 = s.features(b, cell, cand, coffs, among_candidates=True).cpu().numpy()
+        assert np.array_equal(f1.view(np.int32), f2.view(np.int32)), cell
+    # the batched grid kNN over the subcloud in its cooperative mode (dense
+    # cells together, the rest one query per thread) finds the same neighbours
     for rfac in (0.7, 1.0, 2.0):
         for cell in (1.0, 2.5):
             s.set_knn(3, rfac)
-            f3 = s.features(b, cell, cand, coffs, among_candidates=True).cpu().numpy()
+            f3 = s.features(sb, cell).cpu().numpy()
             s.set_knn(0)
-            f4 = s.features(b, cell, cand, coffs, among_candidates=True).cpu().numpy()
-            assert np.array_equal(f3.view(np.int32), f4.view(np.int32)), (rfac, cell)
+            assert np.array_equal(f3.view(np.int32), f2.view(np.int32)), (rfac, cell)
     s.close()
 
 
