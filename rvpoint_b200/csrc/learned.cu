@@ -173,7 +173,8 @@ __global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t 
 // thread, takes the exact KF nearest by rings of cells around its own cell
 // (the own cell, then shells at Chebyshev distance 1, 2, ...) until the KF-th
 // distance lies inside the covered box (its distance to every face that has
-// cells beyond it, less a rounding slack) or the box covers the grid; the
+// cells beyond it, less a rounding slack) or the box covers the grid,
+// skipping cells whose box lies beyond the KF-th distance so far; the
 // queries go in cell order, so a warp's lanes walk the same cells. Keys
 // are packed (d2, index), so the list is the exact (d2, index) order the
 // grid kNN gives; d2 is computed as there. A scene of more than CK_MAX
@@ -337,7 +338,18 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
             const bool edge = dz == -r || dz == r || dy == -r || dy == r;
             for (int dx = -r; dx <= r; dx += (edge ? 1 : 2 * r)) {
               const int ux = cx + dx;
-              if (ux >= 0 && ux < GX) {
+              // a cell whose box lies beyond the current KF-th distance
+              // holds nothing for the list (skipped once the list is full)
+              bool near = ux >= 0 && ux < GX;
+              if (near && r > 0) {
+                const float lx = mnx + (float)ux * c, ly = mny + (float)uy * c,
+                            lz = mnz + (float)uz * c;
+                const float gx = fmaxf(fmaxf(lx - sl - qx, qx - (lx + c + sl)), 0.0f);
+                const float gy = fmaxf(fmaxf(ly - sl - qy, qy - (ly + c + sl)), 0.0f);
+                const float gz = fmaxf(fmaxf(lz - sl - qz, qz - (lz + c + sl)), 0.0f);
+                near = !((gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) > nbr_d2(L[KF - 1]));
+              }
+              if (near) {
                 const int cid = (uz * GY + uy) * GX + ux;
                 for (u32 t = cstart[cid]; t < cstart[cid + 1]; ++t) {
                   const float4 p = sp[t];
