@@ -335,7 +335,7 @@ void Grid::reserve(size_t n, int nf) {
   b_begin.reserve(al((n_frames_max + 1) * 8));
   b_sort.reserve(sort_temp_bytes(n_max) + al(kHeadLevels * n_max * 4) +
                  al(kHeadLevels * (n_max + 1) * 8) +
-                 scan_temp_bytes(n_max));
+                 kHeadLevels * scan_temp_bytes(n_max));
   b_lstart.reserve(al(kHeadLevels * n_max * 4));
   b_pos.reserve(n_max * 4);
   b_sub.reserve(al(n_max * 2));
@@ -437,9 +437,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   k_heads<<<gb, 256, 0, st>>>(g.b_keys.as<u64>(), nm, n_live, levels, base, heads);
   RVP_LAUNCH_CHECK(ctx);
   // bucket_of[L][i] = number of level-L heads before i (the bucket id of a head)
-  for (int L = 0; L < levels; ++L)
-    exclusive_scan_u32_to_u64(ctx, heads + (size_t)L * nm, bucket_of + (size_t)L * (nm + 1), nm,
-                              n_live, scan_tmp);
+  exclusive_scan_u32_to_u64_batch(ctx, heads, nm, bucket_of, nm + 1, levels, nm, n_live,
+                                  scan_tmp);
   RVP_CUDA_TRY(cudaMemsetAsync(g.b_table.ptr, 0xFF, g.table_cap * 16, st));
   // buckets per level, collision, overflow
   RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 8 * kHeadLevels + 8, st));

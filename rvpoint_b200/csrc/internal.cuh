@@ -172,6 +172,11 @@ void radix_sort_pairs(rvp_context *ctx, u64 *keys, u32 *vals, size_t n_max,
 size_t scan_temp_bytes(size_t n_max);
 void exclusive_scan_u32_to_u64(rvp_context *ctx, const u32 *in, u64 *out,
                                size_t n_max, const u64 *n_dev, void *temp);
+// `batch` such scans at once (array b at in + b in_stride, out + b
+// out_stride, elements); temp: batch * scan_temp_bytes(n_max)
+void exclusive_scan_u32_to_u64_batch(rvp_context *ctx, const u32 *in, size_t in_stride, u64 *out,
+                                     size_t out_stride, int batch, size_t n_max,
+                                     const u64 *n_dev, void *temp);
 
 // ---------------------------------------------------------------------------
 // cell grid (grid.cu)

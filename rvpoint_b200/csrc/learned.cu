@@ -167,8 +167,9 @@ __global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t 
 }
 
 // Feature neighbourhoods among one scene's candidates (a few thousand
-// points at most): one block per scene keeps its candidates in shared
-// memory, sorted into a small grid of its own (counting sort over at most
+// points at most): each of CK_SLICES blocks per scene keeps the scene's
+// candidates in shared memory (and answers a share of its queries), sorted
+// into a small grid of its own (counting sort over at most
 // CK_CELLS cells of at least the given cell size), and every query, one per
 // thread, takes the exact KF nearest by rings of cells around its own cell
 // (the own cell, then shells at Chebyshev distance 1, 2, ...) until the KF-th
@@ -181,6 +182,14 @@ __global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t 
 // candidates is searched by brute force over global memory (exact, slow;
 // not reached with the proposal's candidate counts).
 constexpr int CK_MAX = 2048, CK_CELLS = 2048, CK_TH = 256;
+constexpr int CK_SLICES = 4;  // blocks per scene (each builds the scene's grid)
+// the 26 cells around a cell, nearest first: 6 faces, 12 edges, 8 corners
+__constant__ signed char kNbr26[26][3] = {
+    {-1, 0, 0},  {1, 0, 0},   {0, -1, 0},  {0, 1, 0},   {0, 0, -1},  {0, 0, 1},
+    {-1, -1, 0}, {1, -1, 0},  {-1, 1, 0},  {1, 1, 0},   {-1, 0, -1}, {1, 0, -1},
+    {-1, 0, 1},  {1, 0, 1},   {0, -1, -1}, {0, 1, -1},  {0, -1, 1},  {0, 1, 1},
+    {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {-1, -1, 1}, {1, -1, 1},
+    {-1, 1, 1},  {1, 1, 1}};
 constexpr size_t CK_SMEM = (size_t)CK_MAX * 16 + (size_t)(2 * CK_CELLS + 1) * 4 + CK_MAX * 2;
 
 __device__ __forceinline__ void insert_u64(u64 (&L)[KF], u64 key) {
@@ -207,12 +216,15 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
   __shared__ int s_dim[3];
   __shared__ float s_cell;
   const int tid = threadIdx.x;
-  for (int f = blockIdx.x; f < n_frames; f += gridDim.x) {
+  // work items: (scene, slice); each of a scene's CK_SLICES blocks builds
+  // the scene's grid and answers every CK_SLICES-th run of CK_TH queries
+  for (int item = blockIdx.x; item < n_frames * CK_SLICES; item += gridDim.x) {
+    const int f = item / CK_SLICES, slice = item % CK_SLICES;
     const int64_t a = offs[f], b = offs[f + 1];
     const int m = (int)(b - a);
     if (m <= 0) continue;
     if (m > CK_MAX) {  // brute force over global memory
-      for (int i = tid; i < m; i += CK_TH) {
+      for (int i = tid + slice * CK_TH; i < m; i += CK_SLICES * CK_TH) {
         const float qx = x[a + i], qy = y[a + i], qz = z[a + i];
         u64 L[KF];
 #pragma unroll
@@ -316,7 +328,7 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
     __syncthreads();
     // queries, in cell order (the lanes of a warp work on neighbouring
     // points: the same cells, the same ring counts)
-    for (int i = tid; i < m; i += CK_TH) {
+    for (int i = tid + slice * CK_TH; i < m; i += CK_SLICES * CK_TH) {
       const float4 qp = sp[i];
       const float qx = qp.x, qy = qp.y, qz = qp.z;
       const int64_t qo = __float_as_int(qp.w);  // its index in the candidate cloud
@@ -328,40 +340,39 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
       // rounding slack of the cell function and the face positions
       const float sl = 4e-6f * (fabsf(mnx) + fabsf(mny) + fabsf(mnz) + fabsf(qx) + fabsf(qy) +
                                 fabsf(qz) + (float)(GX + GY + GZ + 3) * c) + 1e-6f;
+      // one cell: skipped when its box lies beyond the current KF-th
+      // distance (once the list is full), else its points tested
+      auto visit = [&](int ux, int uy, int uz, bool test_box) {
+        if (ux < 0 || ux >= GX || uy < 0 || uy >= GY || uz < 0 || uz >= GZ) return;
+        if (test_box) {
+          const float lx = mnx + (float)ux * c, ly = mny + (float)uy * c,
+                      lz = mnz + (float)uz * c;
+          const float gx = fmaxf(fmaxf(lx - sl - qx, qx - (lx + c + sl)), 0.0f);
+          const float gy = fmaxf(fmaxf(ly - sl - qy, qy - (ly + c + sl)), 0.0f);
+          const float gz = fmaxf(fmaxf(lz - sl - qz, qz - (lz + c + sl)), 0.0f);
+          if ((gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) > nbr_d2(L[KF - 1])) return;
+        }
+        const int cid = (uz * GY + uy) * GX + ux;
+        for (u32 t = cstart[cid]; t < cstart[cid + 1]; ++t) {
+          const float4 p = sp[t];
+          const u64 key = pack_nbr(dist2(p.x, p.y, p.z, qx, qy, qz), __float_as_int(p.w));
+          ++found;
+          if (key < L[KF - 1]) insert_u64(L, key);
+        }
+      };
       for (int r = 0;; ++r) {
-        for (int dz = -r; dz <= r; ++dz) {
-          const int uz = cz + dz;
-          if (uz < 0 || uz >= GZ) continue;
-          for (int dy = -r; dy <= r; ++dy) {
-            const int uy = cy + dy;
-            if (uy < 0 || uy >= GY) continue;
-            const bool edge = dz == -r || dz == r || dy == -r || dy == r;
-            for (int dx = -r; dx <= r; dx += (edge ? 1 : 2 * r)) {
-              const int ux = cx + dx;
-              // a cell whose box lies beyond the current KF-th distance
-              // holds nothing for the list (skipped once the list is full)
-              bool near = ux >= 0 && ux < GX;
-              if (near && r > 0) {
-                const float lx = mnx + (float)ux * c, ly = mny + (float)uy * c,
-                            lz = mnz + (float)uz * c;
-                const float gx = fmaxf(fmaxf(lx - sl - qx, qx - (lx + c + sl)), 0.0f);
-                const float gy = fmaxf(fmaxf(ly - sl - qy, qy - (ly + c + sl)), 0.0f);
-                const float gz = fmaxf(fmaxf(lz - sl - qz, qz - (lz + c + sl)), 0.0f);
-                near = !((gx * gx + gy * gy + gz * gz) * (1.0f - 1e-5f) > nbr_d2(L[KF - 1]));
-              }
-              if (near) {
-                const int cid = (uz * GY + uy) * GX + ux;
-                for (u32 t = cstart[cid]; t < cstart[cid + 1]; ++t) {
-                  const float4 p = sp[t];
-                  const u64 key =
-                      pack_nbr(dist2(p.x, p.y, p.z, qx, qy, qz), __float_as_int(p.w));
-                  ++found;
-                  if (key < L[KF - 1]) insert_u64(L, key);
-                }
-              }
-              if (r == 0) break;
+        if (r == 0) {
+          visit(cx, cy, cz, false);
+        } else if (r == 1) {  // nearest first: faces, edges, corners
+          for (int t = 0; t < 26; ++t)
+            visit(cx + kNbr26[t][0], cy + kNbr26[t][1], cz + kNbr26[t][2], true);
+        } else {
+          for (int dz = -r; dz <= r; ++dz)
+            for (int dy = -r; dy <= r; ++dy) {
+              const bool edge = dz == -r || dz == r || dy == -r || dy == r;
+              for (int dx = -r; dx <= r; dx += (edge ? 1 : 2 * r))
+                visit(cx + dx, cy + dy, cz + dz, true);
             }
-          }
         }
         // the box of rings 0..r: all points found, or the KF-th inside it
         const bool all = cx - r <= 0 && cy - r <= 0 && cz - r <= 0 && cx + r >= GX - 1 &&
@@ -1172,7 +1183,7 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
                                         (int)rvp::CK_SMEM));
       attr[ctx->device] = true;
     }
-    const unsigned blocks = (unsigned)std::min(n_frames, ctx->num_sms * 8);
+    const unsigned blocks = (unsigned)std::min(n_frames * rvp::CK_SLICES, ctx->num_sms * 8);
     rvp::k_cand_knn<<<blocks, rvp::CK_TH, rvp::CK_SMEM, ctx->stream>>>(
         gx, gx + n_cand, gx + 2 * n_cand, cand_offsets_dev, n_frames, cell_size,
         s->pairs.as<u64>(), s->counts.as<int32_t>());

@@ -338,8 +338,12 @@ __device__ __forceinline__ u64 block_exclusive(u64 s, u64 *warp_tot, u64 &total)
   return before + incl - s;
 }
 
+// (batched scans: blockIdx.y picks the array; strides in elements)
 __global__ __launch_bounds__(SC_TH) void k_scan_tiles(const u32 *in, size_t n_max,
-                                                      const u64 *n_dev, u64 *tsum) {
+                                                      const u64 *n_dev, u64 *tsum,
+                                                      size_t in_stride, size_t ts_stride) {
+  in += blockIdx.y * in_stride;
+  tsum += blockIdx.y * ts_stride;
   const size_t n = n_dev ? *n_dev : n_max;
   const size_t base = (size_t)blockIdx.x * SC_TILE;
   if (base >= n) return;
@@ -363,7 +367,9 @@ __global__ __launch_bounds__(SC_TH) void k_scan_tiles(const u32 *in, size_t n_ma
 }
 
 __global__ void k_scan_sums(u64 *tsum, size_t nt_max, size_t n_max, const u64 *n_dev,
-                            u64 *out) {
+                            u64 *out, size_t out_stride, size_t ts_stride) {
+  tsum += blockIdx.x * ts_stride;
+  out += blockIdx.x * out_stride;
   const size_t n = n_dev ? *n_dev : n_max;
   const size_t nt = (n + SC_TILE - 1) / SC_TILE;
   __shared__ u64 sh[1024];
@@ -391,7 +397,11 @@ __global__ void k_scan_sums(u64 *tsum, size_t nt_max, size_t n_max, const u64 *n
 
 __global__ __launch_bounds__(SC_TH) void k_scan_apply(const u32 *in, size_t n_max,
                                                       const u64 *n_dev, const u64 *tsum,
-                                                      u64 *out) {
+                                                      u64 *out, size_t in_stride,
+                                                      size_t out_stride, size_t ts_stride) {
+  in += blockIdx.y * in_stride;
+  out += blockIdx.y * out_stride;
+  tsum += blockIdx.y * ts_stride;
   const size_t n = n_dev ? *n_dev : n_max;
   const size_t base = (size_t)blockIdx.x * SC_TILE;
   if (base >= n) return;
@@ -431,14 +441,23 @@ size_t scan_temp_bytes(size_t n_max) {
 
 void exclusive_scan_u32_to_u64(rvp_context *ctx, const u32 *in, u64 *out, size_t n_max,
                                const u64 *n_dev, void *temp) {
+  exclusive_scan_u32_to_u64_batch(ctx, in, 0, out, 0, 1, n_max, n_dev, temp);
+}
+
+void exclusive_scan_u32_to_u64_batch(rvp_context *ctx, const u32 *in, size_t in_stride, u64 *out,
+                                     size_t out_stride, int batch, size_t n_max,
+                                     const u64 *n_dev, void *temp) {
   const size_t nt = (n_max + SC_TILE - 1) / SC_TILE;
+  const size_t ts_stride = scan_temp_bytes(n_max) / 8;
   u64 *tsum = static_cast<u64 *>(temp);
-  const unsigned g = (unsigned)(nt > 0 ? nt : 1);
-  k_scan_tiles<<<g, SC_TH, 0, ctx->stream>>>(in, n_max, n_dev, tsum);
+  const dim3 g((unsigned)(nt > 0 ? nt : 1), (unsigned)batch);
+  k_scan_tiles<<<g, SC_TH, 0, ctx->stream>>>(in, n_max, n_dev, tsum, in_stride, ts_stride);
   RVP_LAUNCH_CHECK(ctx);
-  k_scan_sums<<<1, 1024, 0, ctx->stream>>>(tsum, nt, n_max, n_dev, out);
+  k_scan_sums<<<(unsigned)batch, 1024, 0, ctx->stream>>>(tsum, nt, n_max, n_dev, out, out_stride,
+                                                        ts_stride);
   RVP_LAUNCH_CHECK(ctx);
-  k_scan_apply<<<g, SC_TH, 0, ctx->stream>>>(in, n_max, n_dev, tsum, out);
+  k_scan_apply<<<g, SC_TH, 0, ctx->stream>>>(in, n_max, n_dev, tsum, out, in_stride, out_stride,
+                                             ts_stride);
   RVP_LAUNCH_CHECK(ctx);
 }
 
