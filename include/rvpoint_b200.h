@@ -320,8 +320,10 @@ typedef struct {
 } rvp_pipeline_outputs;
 RVP_API rvp_status rvp_pipeline_outputs_get(rvp_pipeline *p, rvp_pipeline_outputs *o);
 /* Re-size the neighbour grid's bucket table to the bucket count of the last
- * run (with 2x headroom and load <= 0.4) so it stays resident in L2. Call
- * after a first run, before capturing a graph. */
+ * run (with 25% headroom, 2.5 slots per bucket rounded up to a power of two)
+ * so it stays resident in L2. Call after a first run, before capturing a
+ * graph; a later batch with more buckets than that makes rvp_pipeline_check
+ * report RVP_ERR_CAPACITY (refit then). */
 RVP_API rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p);
 /* RVP_ERR_CAPACITY if the last run's bucket table overflowed (results of
  * that run are then incomplete); synchronizes the stream. */

@@ -1077,7 +1077,7 @@ rvp_status features_impl(rvp_scorer *s, const float *x, const float *y, const fl
       RVP_CUDA_TRY(cudaStreamSynchronize(st));
       size_t tot = 0;
       for (int l = 0; l < rvp::kGridLevels; ++l) tot += (size_t)nb[l];
-      s->grid.fit_table(tot * 2);
+      s->grid.fit_table(tot + tot / 4);
       s->fitted_points = N;
       s->fitted_cell = cell_size;
       rvp::grid_build(ctx, s->grid, x, y, z, frame_offsets_dev, n_frames, N, cell_size,

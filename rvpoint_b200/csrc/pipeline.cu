@@ -501,10 +501,12 @@ rvp_status rvp_pipeline_fit_tables(rvp_pipeline *p) {
     RVP_CUDA_TRY(cudaMemcpyAsync(nb, p->grid.d_nbuckets, 8 * rvp::kHeadLevels, cudaMemcpyDeviceToHost,
                                  p->ctx->stream));
     RVP_CUDA_TRY(cudaStreamSynchronize(p->ctx->stream));
-    // headroom for batches whose scenes occupy more cells than this one
+    // a quarter of headroom for batches whose scenes occupy more cells than
+    // this one; the table (2.5 slots per bucket, rounded up to a power of
+    // two) then stays inside L2, where every probe of the kNN kernels lands
     size_t tot = 0;
     for (int l = 0; l < rvp::kGridLevels; ++l) tot += (size_t)nb[l];
-    p->grid.fit_table(tot * 2);
+    p->grid.fit_table(tot + tot / 4);
   });
 }
 
