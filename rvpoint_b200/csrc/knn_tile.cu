@@ -1125,11 +1125,13 @@ __global__ __launch_bounds__(TT, 3) void k_knn_tau(GridView g, TileArgs a, const
 // finest chain level whose own cell holds K points (r = cell * sqrt(K /
 // count), under one cell; the top level's cell when none does). Then,
 // repeatedly: the tight window of r at the finest table level where it
-// spans at most kTauCells cells; a count pass over its cells within r (cell
-// box lower bound) -- fewer than K points: r doubles, nothing scanned; more
-// than kTauPoints: the query goes to the warp kernel (lanes over
-// candidates); else a scan bounded by r^2 (every point with d2 <= r^2 lies in
-// the window), exact when it found K such points, else r grows by sqrt 2.
+// spans at most kTauCells cells; from the second attempt on, a count pass
+// over its cells within r (cell box lower bound) -- fewer than K points: r
+// doubles, nothing scanned; more than kTauPoints: the query goes to the warp
+// kernel (lanes over candidates); then a scan bounded by r^2 (every point
+// with d2 <= r^2 lies in the window; a scan that would pass kTauPoints
+// candidates stops and the warp kernel takes the query), exact when it
+// found K such points, else r grows by sqrt 2.
 // Queries left after kAdaptTries attempts go to the hard list without a
 // bound. Outputs as k_knn_wt's (the SOR mean and list row, the fused
 // normal, or feature pairs; tied lists as there).
@@ -1185,37 +1187,47 @@ __global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, con
         punt = true;
         break;
       }
-      u32 total = 0;
-      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
-        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
-          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
-            u32 st, cnt;
-            if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) <= tb &&
-                lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt))
-              total += cnt;
-          }
-      if (total < (u32)K) {  // the window cannot hold K points within r
-        r *= 2.0f;
-        continue;
-      }
-      if (total > kTauPoints) {
-        punt = true;
-        break;
+      // from the second attempt on, a count pass first (the first radius
+      // is mostly generous enough, so its window is scanned at once)
+      if (attempt > 0) {
+        u32 total = 0;
+        for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
+          for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
+            for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+              u32 st, cnt;
+              if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) <= tb &&
+                  lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt))
+                total += cnt;
+            }
+        if (total < (u32)K) {  // the window cannot hold K points within r
+          r *= 2.0f;
+          continue;
+        }
+        if (total > kTauPoints) {
+          punt = true;
+          break;
+        }
       }
 #pragma unroll
       for (int j = 0; j < K; ++j) L[j] = kMax;
       Key thr = kMax;
       tie = -1.0f;
-      u32 found = 0;
-      for (int uz = w.lo[2]; uz <= w.hi[2]; ++uz)
-        for (int uy = w.lo[1]; uy <= w.hi[1]; ++uy)
-          for (int ux = w.lo[0]; ux <= w.hi[0]; ++ux) {
+      u32 found = 0, scanned = 0;
+      for (int uz = w.lo[2]; uz <= w.hi[2] && !punt; ++uz)
+        for (int uy = w.lo[1]; uy <= w.hi[1] && !punt; ++uy)
+          for (int ux = w.lo[0]; ux <= w.hi[0] && !punt; ++ux) {
             float thr_d2;
             if constexpr (FKEY) thr_d2 = thr;
             else thr_d2 = nbr_d2(thr);
             if (cell_lb2(F, level, ux, uy, uz, q.x, q.y, q.z) > fminf(thr_d2, tb)) continue;
             u32 st, cnt;
             if (!lookup(g, level_key(g, F, level, ux, uy, uz), st, cnt)) continue;
+            // a dense window: the warp kernel (lanes over candidates)
+            if (scanned + cnt > kTauPoints) {
+              punt = true;
+              break;
+            }
+            scanned += cnt;
             for (u32 j = 0; j < cnt; ++j) {
               const float4 p = __ldg(&g.pts[st + j]);
               const u32 pidx = __float_as_uint(p.w);
@@ -1239,6 +1251,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, con
               }
             }
           }
+      if (punt) break;
       if (found >= (u32)K) done = true;
       else r *= 1.41421356f;
     }
