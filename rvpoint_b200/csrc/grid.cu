@@ -201,7 +201,8 @@ __global__ void k_heads(const u64 *keys, size_t n_max, const u64 *n_dev, int lev
 }
 
 __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__ y,
-                          const float *__restrict__ z, const u32 *vals, const u32 *heads,
+                          const float *__restrict__ z, const float *__restrict__ aos,
+                          const u32 *vals, const u32 *heads,
                           const u64 *bucket_of, size_t n_max, const u64 *n_dev, int levels,
                           float4 *pts, u32 *lstart, const GridFrame *frames, int mode,
                           int *collision, u32 *pos_of) {
@@ -209,7 +210,16 @@ __global__ void k_reorder(const float *__restrict__ x, const float *__restrict__
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const u32 v = vals[i];
-    const float px = x[v], py = y[v], pz = z[v];
+    float px, py, pz;
+    if (aos) {
+      px = aos[3 * (size_t)v];
+      py = aos[3 * (size_t)v + 1];
+      pz = aos[3 * (size_t)v + 2];
+    } else {
+      px = x[v];
+      py = y[v];
+      pz = z[v];
+    }
     pts[i] = make_float4(px, py, pz, __uint_as_float(v));
     pos_of[v] = (u32)i;
     for (int L = 0; L < levels; ++L)
@@ -392,7 +402,8 @@ GridView Grid::view(int mode, long long p1, long long p2) const {
 
 void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const float *z,
                 const int64_t *offs, int n_frames, size_t n_points, float cell, int mode,
-                long long p1, long long p2, const u64 *n_dev_opt, int base_level) {
+                long long p1, long long p2, const u64 *n_dev_opt, int base_level,
+                const float *xyz_aos) {
   g.reserve(n_points, n_frames);
   const int base = mode == KEY_DENSE ? base_level : 0;
   g.lbase = base;
@@ -442,7 +453,8 @@ void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y, const
   RVP_CUDA_TRY(cudaMemsetAsync(g.b_table.ptr, 0xFF, g.table_cap * 16, st));
   // buckets per level, collision, overflow
   RVP_CUDA_TRY(cudaMemsetAsync(g.d_nbuckets, 0, 8 * kHeadLevels + 8, st));
-  k_reorder<<<gb, 256, 0, st>>>(x, y, z, g.b_vals.as<u32>(), heads, bucket_of, nm, n_live, levels,
+  k_reorder<<<gb, 256, 0, st>>>(x, y, z, xyz_aos, g.b_vals.as<u32>(), heads, bucket_of, nm,
+                                n_live, levels,
                                 g.b_pts.as<float4>(), lstart, frames, mode, g.d_collision,
                                 g.b_pos.as<u32>());
   RVP_LAUNCH_CHECK(ctx);

@@ -249,11 +249,13 @@ struct Grid {
 // reference's bbox/eps/grid formulas and prime hash (single frame).
 // base_level (dense mode): the points are sorted by cells of cell / 2^base
 // and the table holds levels base .. base + kGridLevels - 1 (cells of cell,
-// 2 cell, ...).
+// 2 cell, ...). xyz_aos (optional): the same points interleaved x, y, z
+// (one 12-byte gather per point when the grid records are written).
 void grid_build(rvp_context *ctx, Grid &g, const float *x, const float *y,
                 const float *z, const int64_t *frame_offsets_dev, int n_frames,
                 size_t n_points, float cell, int mode, long long p1,
-                long long p2, const u64 *n_dev_opt, int base_level = 0);
+                long long p2, const u64 *n_dev_opt, int base_level = 0,
+                const float *xyz_aos = nullptr);
 
 // Query helpers (queries are SoA; query q belongs to frame qframe(q)).
 struct QuerySet {

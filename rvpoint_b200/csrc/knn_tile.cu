@@ -1125,7 +1125,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_tau(GridView g, TileArgs a, const
 // finest chain level whose own cell holds K points (r = cell * sqrt(K /
 // count), under one cell; the top level's cell when none does). Then,
 // repeatedly: the tight window of r at the finest table level where it
-// spans at most kTauCells cells; from the second attempt on, a count pass
+// spans at most kAdaptCells cells; from the second attempt on, a count pass
 // over its cells within r (cell box lower bound) -- fewer than K points: r
 // doubles, nothing scanned; more than kTauPoints: the query goes to the warp
 // kernel (lanes over candidates); then a scan bounded by r^2 (every point
@@ -1136,6 +1136,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_tau(GridView g, TileArgs a, const
 // bound. Outputs as k_knn_wt's (the SOR mean and list row, the fused
 // normal, or feature pairs; tied lists as there).
 constexpr int kAdaptTries = 8;
+constexpr int kAdaptCells = 27;  // window cells one thread looks up
 
 template <int K, int MODE>
 __global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
@@ -1178,7 +1179,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, con
       int level = -1;
       for (int Lv = g.lbase; Lv <= top; ++Lv) {
         w = tight_window(F, q.x, q.y, q.z, sqrt((double)tb), Lv);
-        if (window_cells(w) <= kTauCells) {
+        if (window_cells(w) <= kAdaptCells) {
           level = Lv;
           break;
         }
@@ -1531,7 +1532,7 @@ namespace {
 // consecutive rows) and its neighbours' float4 grid records (spatially close,
 // so mostly cached), whose index word carries the removed flag.
 template <int KN>
-__global__ __launch_bounds__(256) void k_normals_sor_lists(GridView g, TileArgs a, int ks) {
+__global__ __launch_bounds__(256, 4) void k_normals_sor_lists(GridView g, TileArgs a, int ks) {
   const u64 n = *g.n_points;
   for (u64 pos = blockIdx.x * (u64)blockDim.x + threadIdx.x; pos < n;
        pos += (u64)gridDim.x * blockDim.x) {

@@ -290,7 +290,7 @@ rvp_status rvp_pipeline_run_device(rvp_pipeline *p, const float *x, const float 
     //    that consecutive points, a warp's queries, lie close together)
     rvp::grid_build(ctx, p->grid, p->vox_x.as<float>(), p->vox_y.as<float>(),
                     p->vox_z.as<float>(), vox_offs, n_frames, N, p->cell, rvp::KEY_DENSE, 0, 0,
-                    n_vox, p->grid_base);
+                    n_vox, p->grid_base, p->vox_aos.as<float>());
     k_frame_ids<<<rvp::grid_for(N, 256, sms * 16), 256, 0, st>>>(vox_offs, n_frames, N,
                                                                  p->vox_frame.as<int32_t>());
     RVP_LAUNCH_CHECK(ctx);
