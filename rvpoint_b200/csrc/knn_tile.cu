@@ -1139,7 +1139,7 @@ constexpr int kAdaptTries = 8;
 constexpr int kAdaptCells = 27;  // window cells one thread looks up
 
 template <int K, int MODE>
-__global__ __launch_bounds__(TT, 3) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
+__global__ __launch_bounds__(TT, 4) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
                                                      const u64 *n_list, u32 *stats) {
   constexpr bool FKEY = MODE == TILE_SOR_MEAN || MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
   constexpr bool KV = MODE == TILE_SOR_LIST || MODE == TILE_PAIRS_F;
@@ -1432,7 +1432,7 @@ void launch_k(rvp_context *ctx, const GridView &g, int mode, const TileArgs &a_i
       k_open_to_hard<<<gb, 256, 0, ctx->stream>>>(g, a.open_list, a.open_n, a.hard,
                                                   a.hard_count, a.hard_tau);
     } else {
-      const int ablocks = ctx->num_sms * 3;
+      const int ablocks = ctx->num_sms * 4;
 #define RVP_ADAPT(M) \
   k_knn_adapt<K, M><<<ablocks, TT, 0, ctx->stream>>>(g, a, a.open_list, a.open_n, stats)
       if (mode == TILE_SOR_MEAN) RVP_ADAPT(TILE_SOR_MEAN);
