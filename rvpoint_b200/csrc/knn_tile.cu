@@ -1136,7 +1136,7 @@ __global__ __launch_bounds__(TT, 3) void k_knn_tau(GridView g, TileArgs a, const
 // bound. Outputs as k_knn_wt's (the SOR mean and list row, the fused
 // normal, or feature pairs; tied lists as there).
 constexpr int kAdaptTries = 8;
-constexpr int kAdaptCells = 27;  // window cells one thread looks up
+constexpr int kAdaptCells = 64;  // window cells one thread looks up
 
 template <int K, int MODE>
 __global__ __launch_bounds__(TT, 4) void k_knn_adapt(GridView g, TileArgs a, const u32 *list,
