@@ -168,8 +168,8 @@ __global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t 
 
 // Feature neighbourhoods among one scene's candidates (a few thousand
 // points at most): each of CK_SLICES blocks per scene keeps the scene's
-// candidates in shared memory (and answers a share of its queries), sorted
-// into a small grid of its own (counting sort over at most
+// candidates in shared memory (and answers the queries whose index in the
+// scene is its slice modulo CK_SLICES), sorted into a small grid of its own (counting sort over at most
 // CK_CELLS cells of at least the given cell size), and every query, one per
 // thread, takes the exact KF nearest by rings of cells around its own cell
 // (the own cell, then shells at Chebyshev distance 1, 2, ...) until the KF-th
@@ -213,6 +213,8 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
   uint16_t *cellof = reinterpret_cast<uint16_t *>(cursor + CK_CELLS);  // CK_MAX
   __shared__ float s_bb[3];
   __shared__ float s_wmn[CK_TH / 32][3], s_wmx[CK_TH / 32][3];
+  __shared__ int s_wsum[CK_TH / 32];
+  __shared__ int s_nq;
   __shared__ int s_dim[3];
   __shared__ float s_cell;
   const int tid = threadIdx.x;
@@ -326,10 +328,48 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
       sp[p] = make_float4(x[a + i], y[a + i], z[a + i], __int_as_float((int)(a + i)));
     }
     __syncthreads();
-    // queries, in cell order (the lanes of a warp work on neighbouring
-    // points: the same cells, the same ring counts)
-    for (int i = tid + slice * CK_TH; i < m; i += CK_SLICES * CK_TH) {
-      const float4 qp = sp[i];
+    // this block's queries: the candidates whose index in the scene is
+    // slice modulo CK_SLICES (a partition that does not depend on the order
+    // the scatter left inside a cell, which differs between the scene's
+    // blocks), listed in cell order (the lanes of a warp work on
+    // neighbouring points: the same cells, the same ring counts)
+    uint16_t *qlist = cellof;  // free once the points are in place
+    {
+      constexpr int PER = CK_MAX / CK_TH;  // sorted positions per thread
+      int cnt = 0;
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int t = tid * PER + u;
+        cnt += t < m && (__float_as_int(sp[t].w) - (int)a) % CK_SLICES == slice ? 1 : 0;
+      }
+      // block exclusive scan of the counts (warp shuffles, then warp totals)
+      const int lane = tid & 31, wid = tid >> 5;
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      if (lane == 31) s_wsum[wid] = incl;
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int k = 0; k < CK_TH / 32; ++k) {
+        if (k < wid) before += s_wsum[k];
+        total += s_wsum[k];
+      }
+      int o = before + incl - cnt;
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int t = tid * PER + u;
+        if (t < m && (__float_as_int(sp[t].w) - (int)a) % CK_SLICES == slice)
+          qlist[o++] = (uint16_t)t;
+      }
+      if (tid == 0) s_nq = total;
+      __syncthreads();
+    }
+    const int nq = s_nq;
+    for (int j = tid; j < nq; j += CK_TH) {
+      const float4 qp = sp[qlist[j]];
       const float qx = qp.x, qy = qp.y, qz = qp.z;
       const int64_t qo = __float_as_int(qp.w);  // its index in the candidate cloud
       const int cx = cax(qx, mnx, GX), cy = cax(qy, mny, GY), cz = cax(qz, mnz, GZ);
