@@ -604,7 +604,7 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
     # the feature kNN among each scene's candidates (one block per scene, a
     # grid of its own in shared memory): its cell size sets only the speed
     knn_modes = {}
-    for cell in (0.5, 1.0, 1.5, 2.5):
+    for cell in (1.0, 1.5, 2.0, 2.5):
         knn_modes[f"cell{cell}"] = timed(
             lambda: LR.proposal_features(scorer, be, cand, coffs, cell, lr.scope))[0]
     best_mode = min(knn_modes, key=knn_modes.get)

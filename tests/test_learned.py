@@ -204,18 +204,20 @@ def test_features_among_candidates_equal_features_of_their_subcloud(gpu_ctx):
     for cell in (0.5, 1.0, 2.5):
         f1 = s.features(b, cell, cand, coffs, among_candidates=True).cpu().numpy()
         assert np.array_equal(f1.view(np.int32), f2.view(np.int32)), cell
-    # the bench's scene generator at its candidate count, cell 1.0 m (about
-    # one candidate per cell: rings of two and three cells), twice in a row
+    # the bench's scene generator at its candidate count, twice in a row at
+    # each cell: 1.0 m (about one candidate per cell: rings of two and three
+    # cells), 2.0 and 2.5 m (about 5 and 8 candidates per cell: mostly
+    # finished at ring 1, a few queries on ring 2)
     ev = D.plane_batch(n_scenes=16, seed=D.SEED_BASE + 4)
     be = DeviceBatch.from_host(ev)
     ch, co = candidates(be.offsets_host, 1024, 11)
     se = PlaneScorer(be.n, 16, ctx=gpu_ctx)
     ref = se.features(DeviceBatch.from_host(D.Batch(ev.x[ch], ev.y[ch], ev.z[ch], co)),
                       1.0).cpu().numpy()
-    for _ in range(2):
-        fe = se.features(be, 1.0, torch.from_numpy(ch.view(np.int32)).cuda(),
+    for cell in (1.0, 1.0, 2.0, 2.0, 2.5, 2.5):
+        fe = se.features(be, cell, torch.from_numpy(ch.view(np.int32)).cuda(),
                          torch.from_numpy(co).cuda(), among_candidates=True).cpu().numpy()
-        assert np.array_equal(fe.view(np.int32), ref.view(np.int32))
+        assert np.array_equal(fe.view(np.int32), ref.view(np.int32)), cell
     se.close()
     # the batched grid kNN over the subcloud in its cooperative mode (dense
     # cells together, the rest one query per thread) finds the same neighbours
