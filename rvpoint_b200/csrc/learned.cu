@@ -182,7 +182,7 @@ __global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t 
 // candidates is searched by brute force over global memory (exact, slow;
 // not reached with the proposal's candidate counts).
 constexpr int CK_MAX = 2048, CK_CELLS = 2048, CK_TH = 256;
-constexpr int CK_SLICES = 4;  // blocks per scene (each builds the scene's grid)
+constexpr int CK_SLICES = 2;  // blocks per scene (each builds the scene's grid)
 // the 26 cells around a cell, nearest first: 6 faces, 12 edges, 8 corners
 __constant__ signed char kNbr26[26][3] = {
     {-1, 0, 0},  {1, 0, 0},   {0, -1, 0},  {0, 1, 0},   {0, 0, -1},  {0, 0, 1},
