@@ -168,9 +168,10 @@ __global__ void k_frame_of(const int64_t *offs, int n_frames, size_t n, int32_t 
 
 // Feature neighbourhoods among one scene's candidates (a few thousand
 // points at most): each of CK_SLICES blocks per scene keeps the scene's
-// candidates in shared memory (and answers the queries whose index in the
-// scene is its slice modulo CK_SLICES), sorted into a small grid of its own (counting sort over at most
-// CK_CELLS cells of at least the given cell size), and every query, one per
+// candidates in shared memory, sorted into a small grid of its own
+// (counting sort over at most CK_CELLS cells of at least the given cell
+// size), and answers the queries of a run of whole cells (about one
+// CK_SLICES-th of them, in cell order); every query, one per
 // thread, takes the exact KF nearest by rings of cells around its own cell
 // (the own cell, then shells at Chebyshev distance 1, 2, ...) until the KF-th
 // distance lies inside the covered box (its distance to every face that has
@@ -213,13 +214,11 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
   uint16_t *cellof = reinterpret_cast<uint16_t *>(cursor + CK_CELLS);  // CK_MAX
   __shared__ float s_bb[3];
   __shared__ float s_wmn[CK_TH / 32][3], s_wmx[CK_TH / 32][3];
-  __shared__ int s_wsum[CK_TH / 32];
-  __shared__ int s_nq;
   __shared__ int s_dim[3];
   __shared__ float s_cell;
   const int tid = threadIdx.x;
   // work items: (scene, slice); each of a scene's CK_SLICES blocks builds
-  // the scene's grid and answers every CK_SLICES-th run of CK_TH queries
+  // the scene's grid and answers its slice's run of cells
   for (int item = blockIdx.x; item < n_frames * CK_SLICES; item += gridDim.x) {
     const int f = item / CK_SLICES, slice = item % CK_SLICES;
     const int64_t a = offs[f], b = offs[f + 1];
@@ -328,48 +327,26 @@ __global__ __launch_bounds__(CK_TH) void k_cand_knn(const float *__restrict__ x,
       sp[p] = make_float4(x[a + i], y[a + i], z[a + i], __int_as_float((int)(a + i)));
     }
     __syncthreads();
-    // this block's queries: the candidates whose index in the scene is
-    // slice modulo CK_SLICES (a partition that does not depend on the order
-    // the scatter left inside a cell, which differs between the scene's
-    // blocks), listed in cell order (the lanes of a warp work on
-    // neighbouring points: the same cells, the same ring counts)
-    uint16_t *qlist = cellof;  // free once the points are in place
-    {
-      constexpr int PER = CK_MAX / CK_TH;  // sorted positions per thread
-      int cnt = 0;
-#pragma unroll
-      for (int u = 0; u < PER; ++u) {
-        const int t = tid * PER + u;
-        cnt += t < m && (__float_as_int(sp[t].w) - (int)a) % CK_SLICES == slice ? 1 : 0;
+    // this block's queries: a run of whole cells in cell order, from the
+    // start of the cell holding sorted position slice * m / CK_SLICES to
+    // that of the next slice (the cell starts are the same in every block
+    // of the scene, while the order inside a cell is not: whole cells keep
+    // the split exact); a warp's lanes work on neighbouring points, the same
+    // cells, the same ring counts
+    auto slice_start = [&](int k) -> int {
+      if (k <= 0) return 0;
+      if (k >= CK_SLICES) return m;
+      const u32 pos = (u32)((long long)k * m / CK_SLICES);
+      int lo = 0, hi = CK_CELLS - 1;  // the last cell starting at or before pos
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cstart[mid] <= pos) lo = mid; else hi = mid - 1;
       }
-      // block exclusive scan of the counts (warp shuffles, then warp totals)
-      const int lane = tid & 31, wid = tid >> 5;
-      int incl = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      if (lane == 31) s_wsum[wid] = incl;
-      __syncthreads();
-      int before = 0, total = 0;
-      for (int k = 0; k < CK_TH / 32; ++k) {
-        if (k < wid) before += s_wsum[k];
-        total += s_wsum[k];
-      }
-      int o = before + incl - cnt;
-#pragma unroll
-      for (int u = 0; u < PER; ++u) {
-        const int t = tid * PER + u;
-        if (t < m && (__float_as_int(sp[t].w) - (int)a) % CK_SLICES == slice)
-          qlist[o++] = (uint16_t)t;
-      }
-      if (tid == 0) s_nq = total;
-      __syncthreads();
-    }
-    const int nq = s_nq;
-    for (int j = tid; j < nq; j += CK_TH) {
-      const float4 qp = sp[qlist[j]];
+      return (int)cstart[lo];
+    };
+    const int q0 = slice_start(slice), q1 = slice_start(slice + 1);
+    for (int j = q0 + tid; j < q1; j += CK_TH) {
+      const float4 qp = sp[j];
       const float qx = qp.x, qy = qp.y, qz = qp.z;
       const int64_t qo = __float_as_int(qp.w);  // its index in the candidate cloud
       const int cx = cax(qx, mnx, GX), cy = cax(qy, mny, GY), cz = cax(qz, mnz, GZ);
