@@ -601,8 +601,9 @@ def learned_leg(ctx, n_scenes: int, n_train: int, reps: int = 3) -> dict:
     t_ptg, (_, bp, it_ptg) = timed(lambda: LR.ransac_frames(be, 10_000, T, targets=tg, ctx=ctx))
     lr = LR.LearnedRansac(scorer)
     cand, coffs = lr.prepare(be)
-    # the feature kNN among each scene's candidates (one block per scene, a
-    # grid of its own in shared memory): its cell size sets only the speed
+    # the feature kNN among each scene's candidates (two blocks per scene,
+    # each with the scene's grid in shared memory): its cell size sets only
+    # the speed
     knn_modes = {}
     for cell in (1.0, 1.5, 2.0, 2.5):
         knn_modes[f"cell{cell}"] = timed(

@@ -1187,8 +1187,8 @@ rvp_status rvp_scorer_features(rvp_scorer *s, const float *x, const float *y, co
     RVP_LAUNCH_CHECK(ctx);
   });
   if (st != RVP_OK) return st;
-  // one block per scene: its candidates' neighbourhoods in shared memory
-  // (no global grid, sort or table)
+  // CK_SLICES blocks per scene, each with the scene's candidates in shared
+  // memory (no global grid, sort or table)
   return sguard(ctx, [&] {
     RVP_REQUIRE(cell_size > 0.0f, "cell_size must be > 0");
     RVP_REQUIRE(n_frames >= 1 && n_frames <= s->max_frames, "n_frames out of range");

@@ -200,7 +200,8 @@ def test_features_among_candidates_equal_features_of_their_subcloud(gpu_ctx):
     coffs = torch.from_numpy(coffs_h).cuda()
     sb = DeviceBatch.from_host(sub)
     f2 = s.features(sb, 1.0).cpu().numpy()
-    # among the candidates: one block per scene, its own grid in shared memory
+    # among the candidates: two blocks per scene, each with the scene's grid
+    # in shared memory
     for cell in (0.5, 1.0, 2.5):
         f1 = s.features(b, cell, cand, coffs, among_candidates=True).cpu().numpy()
         assert np.array_equal(f1.view(np.int32), f2.view(np.int32)), cell
